@@ -1,0 +1,293 @@
+#!/usr/bin/env python
+"""Benchmark of the FP64 uniform-patch D-Claw step on B200.
+
+Workload (default): the 4096 x 4096 random-field case -- dx 0.5 m, seeded
+Gaussian random terrain (spectral slope -3, 5 m RMS) on a 20 deg tilt, 32
+seeded paraboloid sources (~70% of cells dry), reference material
+parameters, order 2 + transverse corrections + MC limiter, wall boundaries.
+Synthetic data generated here from a seed.
+
+A "step" is one full patch step (ghost fill, b4step2, step2 sweeps, update,
+src2, Courant number, next dt). Metric: cell-updates/s (interior cells x
+steps / time). `value` is measured with CUDA events on the launching stream
+with the state resident in HBM (the 672 MB state is larger than L2, so no
+flush is needed); `e2e` goes through the public patch-step API with host
+buffers: each step copies the state from pinned host memory to the device,
+runs the step and copies the new state and the Courant number back.
+
+--impl reference times the CPU restatement of the reference Fortran
+(oracle/, OpenMP over all host cores) on the same workload, one full step
+per timed step.
+
+Multi-GPU (torchrun): every rank advances its own patch (independent
+replicas, weak scaling); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+BYTES_PER_CELL_UPDATE = 88  # read 5 state + 1 bed, write 5 state (FP64)
+METRIC = "cell-updates/sec on 1 B200 (plain vs batched); gradient/forward time ratio"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=4096)
+    ap.add_argument("--dx", type=float, default=0.5)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--json-out", default="")
+    return ap.parse_args()
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in Path(self.path).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_case(args, rank=0):
+    from dclaw_b200 import workloads as W
+
+    return W.random_field_case(n=args.size, dx=args.dx, seed=args.seed + rank)
+
+
+def cpu_baseline(args, case, steps):
+    """Oracle (CPU restatement) on `steps` full steps of the same case."""
+    from oracle import Oracle
+
+    o = Oracle()
+    cores = o.threads(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    r = o.run(case.params, case.q, case.b, case.dx, case.dy, steps, case.dt_initial, parallel=True)
+    el = time.perf_counter() - t0
+    cells = case.mx * case.my * steps
+    return {"value": cells / el, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+            "sample": f"first {steps} steps of the {case.mx}x{case.my} workload from its initial state "
+                      f"({el:.1f} s, OpenMP, oracle/dclaw_oracle.cpp)", "status": r["status"]}
+
+
+def run_reference(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    case = make_case(args)
+    from oracle import Oracle
+
+    o = Oracle()
+    cores = o.threads(os.cpu_count() or 1)
+    # warm-up steps advance the state; the timed steps continue from it
+    r = o.run(case.params, case.q, case.b, case.dx, case.dy, args.warmup, case.dt_initial, parallel=True)
+    dt_next = float(r["dt"][-1]) if args.warmup else case.dt_initial
+    t0 = time.perf_counter()
+    r2 = o.run(case.params, r["q"], case.b, case.dx, case.dy, args.steps, dt_next, parallel=True)
+    el = time.perf_counter() - t0
+    cells = case.mx * case.my * args.steps
+    v = cells / el
+    line = {"metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"random_field_{case.mx}x{case.my}_dx{case.dx}", "steps_per_sample": 1,
+                       "threads": cores},
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} full steps of the {case.mx}x{case.my} workload after "
+                                       f"{args.warmup} warm-up steps (oracle/dclaw_oracle.cpp, OpenMP)"},
+            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "status": r2["status"]}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_info()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(dev)
+    from dclaw_b200 import _lib
+    from dclaw_b200.solver import PatchStepper
+
+    case = make_case(args, rank)
+    q = torch.tensor(case.q, device=dev)
+    b = torch.tensor(case.b, device=dev)
+    st = PatchStepper(q, b, case.params, case.dx, case.dy)
+    st.init_clock(case.dt_initial)
+    cells = case.mx * case.my
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up (also advances the flow past its first, mostly static, steps)
+    st.step(args.warmup)
+    barrier()
+    sampler = ClockSampler(dev.index)
+    sampler.start()
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    st.step(args.steps)
+    e1.record(stream)
+    barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    ms_t = torch.tensor([ms], device=dev)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    status = st.status()
+    value = cells * args.steps * world / (ms / 1000.0)
+
+    # ---- end to end through the public patch-step API with host buffers ----
+    e2e_ms = None
+    h2d = d2h = 0
+    if args.e2e_steps > 0:
+        qh = st.state().cpu().pin_memory()
+        cfl_h = torch.zeros(8, dtype=torch.float64).pin_memory()
+        barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.e2e_steps):
+            st.qa.copy_(qh, non_blocking=True)           # that step's input state, host -> device
+            st.step(1)
+            qh.copy_(st.state(), non_blocking=True)      # the new state, device -> host
+            cfl_h.copy_(st.clock, non_blocking=True)     # Courant number and next dt
+        f1.record(stream)
+        barrier()
+        e2e_ms = f0.elapsed_time(f1)
+        e_t = torch.tensor([e2e_ms], device=dev)
+        if world > 1:
+            dist.all_reduce(e_t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(e_t.item())
+        h2d = qh.numel() * 8
+        d2h = qh.numel() * 8 + cfl_h.numel() * 8
+
+    peak, peak_kind = load_peaks()
+    achieved = BYTES_PER_CELL_UPDATE * cells / (ms / 1000.0 / args.steps) / 1e9
+    out = None
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": {"workload": f"random_field_{case.mx}x{case.my}_dx{case.dx}",
+                          "cells_per_gpu": cells, "parallelism": f"replicas{world}",
+                          "l2": "state 672 MB > L2, no flush", "order": case.params.order,
+                          "transverse_waves": case.params.transverse_waves, "limiter": "MC"},
+               "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "traffic": None,
+                            "kernel": "whole fused step (88 B/cell-update algorithmic)",
+                            "peak_source": peak_kind},
+               "clocks": clocks, "gpu_launches": 8 * args.steps, "status": status}
+        if e2e_ms is not None:
+            out["e2e"] = {"value": cells * args.e2e_steps * world / (e2e_ms / 1000.0), "unit": "cell-updates/s",
+                          "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                          "api": "PatchStepper.step with pinned host state in/out every step"}
+    if world > 1:
+        dist.barrier()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args, case, args.cpu_steps)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+        if args.json_out:
+            Path(args.json_out).write_text(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,509 @@
+// kernels.cu -- CUDA kernels (sm_100a, FP64) and the C ABI of include/dclaw_b200.h.
+//
+// One launch per stage of stages.cuh, all on the caller's stream, all
+// reading dt from the device-resident clock so that a sequence of steps can
+// be captured in a CUDA graph. The Courant number is max-reduced with warp
+// shuffles, one shared-memory pass per block and one 64-bit atomicMax per
+// block on the order-preserving bit pattern of a non-negative double.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "stages.cuh"
+
+namespace dclaw {
+
+constexpr int TPB = 256;
+
+__device__ __forceinline__ double warp_max(double v) {
+    for (int o = 16; o > 0; o >>= 1) {
+        double w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w > v ? w : v;
+    }
+    return v;
+}
+
+// block-wide max of a non-negative value into *acc (bit pattern of a double)
+__device__ __forceinline__ void block_max_to(double v, unsigned long long* acc) {
+    __shared__ double red[TPB / 32];
+    v = warp_max(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        double x = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
+        x = warp_max(x);
+        if (lane == 0 && x > 0.0) atomicMax(acc, (unsigned long long)__double_as_longlong(x));
+    }
+}
+
+__device__ __forceinline__ void flag_status(dclaw_clock* clk, int code) { atomicCAS(&clk->status, 0, code); }
+
+// ---- fused step (interior layout) -----------------------------------------
+__global__ void __launch_bounds__(TPB) k_b4(dclaw_params P, Geom g, const double* __restrict__ q_in,
+                                            const double* __restrict__ b, Work W, dclaw_clock* clk) {
+    const long long n = (long long)g.PX * g.PY;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
+    if (stage_b4(P, g, q_in, b, W, i, j)) flag_status(clk, DCLAW_ERR_NAN);
+}
+
+__global__ void __launch_bounds__(TPB) k_taudir(dclaw_params P, Geom g, Work W, int inner_only) {
+    const long long n = (long long)g.PX * g.PY;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
+    if (inner_only && (i < 0 || j < 0 || i > g.mx + 1 || j > g.my + 1)) return;
+    stage_taudir(P, g, W, i, j);
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(TPB) k_riemann(dclaw_params P, Geom g, Work W, dclaw_clock* clk,
+                                                 uint32_t* __restrict__ brlog) {
+    // DIR 0: rows r = 0..my+1, interfaces i = 0..mx+2 (x fastest)
+    // DIR 1: interfaces k = 0..my+2, columns c = 0..mx+1 (column fastest)
+    const int nfast = DIR == 0 ? g.mx + 3 : g.mx + 2;
+    const int nslow = DIR == 0 ? g.my + 2 : g.my + 3;
+    const long long n = (long long)nfast * nslow;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double cflv = 0.0;
+    if (idx < n) {
+        int a = (int)(idx % nfast), s = (int)(idx / nfast);
+        int r = DIR == 0 ? s : a;   // slice
+        int i = DIR == 0 ? a : s;   // interface along the slice
+        const int nlen = DIR == 0 ? g.mx : g.my;
+        uint32_t bits = 0;
+        double smax = stage_riemann<DIR>(P, g, W, r, i, &bits);
+        if (i >= 1 && i <= nlen + 1) {
+            const double dt = clk->dt;
+            const double dtdx = DIR == 0 ? dt / g.dx : dt / g.dy;
+            cflv = dtdx * smax;
+            if (brlog) {
+                size_t off = DIR == 0 ? (size_t)r * (g.mx + 1) + (size_t)(i - 1)
+                                      : (size_t)(g.my + 2) * (g.mx + 1) + (size_t)r * (g.my + 1) + (size_t)(i - 1);
+                brlog[off] = bits;
+            }
+        }
+        if (!(cflv == cflv)) cflv = 0.0;
+    }
+    block_max_to(cflv, reinterpret_cast<unsigned long long*>(&clk->cfl_bits));
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(TPB) k_flux(dclaw_params P, Geom g, Work W, const dclaw_clock* clk,
+                                              uint32_t* __restrict__ brlog) {
+    // DIR 0: rows 0..my+1, interfaces 1..mx+1; DIR 1: interfaces 1..my+1, columns 0..mx+1
+    const int nfast = DIR == 0 ? g.mx + 1 : g.mx + 2;
+    const int nslow = DIR == 0 ? g.my + 2 : g.my + 1;
+    const long long n = (long long)nfast * nslow;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    int a = (int)(idx % nfast), s = (int)(idx / nfast);
+    int r = DIR == 0 ? s : a;
+    int i = DIR == 0 ? a + 1 : s + 1;
+    const double dt = clk->dt;
+    const double dtdx = DIR == 0 ? dt / g.dx : dt / g.dy;
+    uint32_t bits = 0;
+    stage_flux<DIR>(P, g, W, r, i, dtdx, brlog ? &bits : nullptr);
+    if (brlog) {
+        size_t off = DIR == 0 ? (size_t)r * (g.mx + 1) + (size_t)(i - 1)
+                              : (size_t)(g.my + 2) * (g.mx + 1) + (size_t)r * (g.my + 1) + (size_t)(i - 1);
+        brlog[off] |= bits;
+    }
+}
+
+__global__ void __launch_bounds__(TPB) k_final(dclaw_params P, Geom g, Work W, double* __restrict__ q_out,
+                                               dclaw_clock* clk) {
+    const long long n = (long long)g.mx * g.my;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    int i = (int)(idx % g.mx) + 1, j = (int)(idx / g.mx) + 1;
+    if (stage_finalize(P, g, W, q_out, i, j, clk->dt)) flag_status(clk, DCLAW_ERR_NAN);
+}
+
+__global__ void k_tick(dclaw_params P, dclaw_clock* clk) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double cfl = __longlong_as_double((long long)clk->cfl_bits);
+    double dt = clk->dt;
+    clk->cfl = cfl;
+    clk->dt_last = dt;
+    clk->t = clk->t + dt;
+    clk->nsteps = clk->nsteps + 1;
+    double dtn = clk->fixed_dt ? dt : tick_next_dt(P, dt, cfl);
+    if (clk->t_final > 0.0) dtn = fmax2(fmin2(dtn, clk->t_final - clk->t), 0.0);
+    clk->dt = dtn;
+    clk->cfl_bits = 0ull;
+}
+
+__global__ void k_clock_init(dclaw_clock* clk, double t, double dt, double t_final, int fixed_dt) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    clk->t = t;
+    clk->t_final = t_final;
+    clk->dt = t_final > 0.0 ? fmax2(fmin2(dt, t_final - t), 0.0) : dt;
+    clk->cfl = 0.0;
+    clk->dt_last = 0.0;
+    clk->cfl_bits = 0ull;
+    clk->nsteps = 0;
+    clk->blocks_done = 0;
+    clk->status = 0;
+    clk->fixed_dt = fixed_dt;
+}
+
+// ---- patch calls (padded layout) ------------------------------------------
+__global__ void __launch_bounds__(TPB) k_bc2amr(dclaw_params P, int mx, int my, double* q) {
+    // one thread per padded cell; ghost cells read their source interior cell
+    const int PX = mx + 4, PY = my + 4;
+    const size_t npad = (size_t)PX * PY;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)npad) return;
+    int i = (int)(idx % PX) - 1, j = (int)(idx / PX) - 1;
+    if (i >= 1 && i <= mx && j >= 1 && j <= my) return;
+    int si = i, sj = j;
+    bool fu = false, fv = false;
+    if (i < 1) { if (P.bc_lower[0] == DCLAW_BC_WALL) { si = 1 - i; fu = true; } else si = 1; }
+    else if (i > mx) { if (P.bc_upper[0] == DCLAW_BC_WALL) { si = 2 * mx + 1 - i; fu = true; } else si = mx; }
+    if (j < 1) { if (P.bc_lower[1] == DCLAW_BC_WALL) { sj = 1 - j; fv = true; } else sj = 1; }
+    else if (j > my) { if (P.bc_upper[1] == DCLAW_BC_WALL) { sj = 2 * my + 1 - j; fv = true; } else sj = my; }
+    const size_t d = (size_t)(j + 1) * PX + (size_t)(i + 1);
+    const size_t s = (size_t)(sj + 1) * PX + (size_t)(si + 1);
+    for (int m = 0; m < 5; ++m) {
+        double v = q[(size_t)m * npad + s];
+        if ((m == 1 && fu) || (m == 2 && fv)) v = -v;
+        q[(size_t)m * npad + d] = v;
+    }
+}
+
+__global__ void __launch_bounds__(TPB) k_setaux(dclaw_params P, int mx, int my, double* aux) {
+    const int PX = mx + 4, PY = my + 4;
+    const size_t npad = (size_t)PX * PY;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)npad) return;
+    int i = (int)(idx % PX) - 1, j = (int)(idx / PX) - 1;
+    int ii = i < 1 ? 1 : (i > mx ? mx : i);
+    int jj = j < 1 ? 1 : (j > my ? my : j);
+    aux[idx] = aux[(size_t)(jj + 1) * PX + (size_t)(ii + 1)];
+    aux[npad + idx] = P.phi;
+    aux[2 * npad + idx] = P.theta_input;
+    aux[3 * npad + idx] = 0.0;
+    aux[4 * npad + idx] = 0.0;
+    aux[5 * npad + idx] = 0.0;
+}
+
+__global__ void __launch_bounds__(TPB) k_b4_padded(dclaw_params P, int mx, int my, double* q, dclaw_clock* clk) {
+    const int PX = mx + 4, PY = my + 4;
+    const size_t npad = (size_t)PX * PY;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)npad) return;
+    double h = q[idx], hu = q[npad + idx], hv = q[2 * npad + idx], hm = q[3 * npad + idx], p = q[4 * npad + idx];
+    if (clk && ((h != h) || (hu != hu) || (hv != hv) || (hm != hm) || (p != p))) flag_status(clk, DCLAW_ERR_NAN);
+    double u, v, m;
+    qfix(P, h, hu, hv, hm, p, u, v, m, P.grav);
+    if (h > 0.0) {
+        double s = sqrt((sq(hu) + sq(hv))) / h;
+        if (s > P.speed_limit) {
+            double sratio = P.speed_limit / s;
+            hu = hu * sratio;
+            hv = hv * sratio;
+        }
+    }
+    q[idx] = h; q[npad + idx] = hu; q[2 * npad + idx] = hv; q[3 * npad + idx] = hm; q[4 * npad + idx] = p;
+}
+
+__global__ void __launch_bounds__(TPB) k_update_padded(Geom g, Work W, double dt, double* q, double* fluxes,
+                                                       dclaw_clock* clk) {
+    const long long n = (long long)g.mx * g.my;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    int i = (int)(idx % g.mx) + 1, j = (int)(idx / g.mx) + 1;
+    double qn[5], fl[20];
+    bool nan = stage_update(g, W, i, j, dt, qn, fluxes ? fl : nullptr);
+    if (nan && clk) flag_status(clk, DCLAW_ERR_NAN);
+    const size_t pc = pidx(g, i, j);
+    for (int m = 0; m < 5; ++m) q[(size_t)m * W.npad + pc] = qn[m];
+    if (fluxes) {
+        const size_t np = W.npad;
+        for (int m = 0; m < 5; ++m) {
+            fluxes[(size_t)(0 + m) * np + pidx(g, i + 1, j)] = fl[m];
+            fluxes[(size_t)(5 + m) * np + pc] = fl[5 + m];
+            fluxes[(size_t)(10 + m) * np + pidx(g, i, j + 1)] = fl[10 + m];
+            fluxes[(size_t)(15 + m) * np + pc] = fl[15 + m];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(TPB) k_src2_padded(dclaw_params P, int mx, int my, double dt, double* q) {
+    const long long n = (long long)mx * my;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    const int PX = mx + 4, PY = my + 4;
+    const size_t npad = (size_t)PX * PY;
+    int i = (int)(idx % mx) + 1, j = (int)(idx / mx) + 1;
+    const size_t pc = (size_t)(j + 1) * PX + (size_t)(i + 1);
+    double a = q[pc], b = q[npad + pc], c = q[2 * npad + pc], d = q[3 * npad + pc], e = q[4 * npad + pc];
+    src2_cell(P, P.phi, dt, a, b, c, d, e);
+    q[pc] = a; q[npad + pc] = b; q[2 * npad + pc] = c; q[3 * npad + pc] = d; q[4 * npad + pc] = e;
+}
+
+__global__ void __launch_bounds__(TPB) k_wave_speed(dclaw_params P, int mx, int my, const double* __restrict__ q,
+                                                   unsigned long long* acc) {
+    const long long n = (long long)mx * my;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (idx < n) {
+        double h = q[idx];
+        if (h > P.dry_tolerance) {
+            double u = q[n + idx] / h, w = q[2 * n + idx] / h;
+            v = sqrt(sq(u) + sq(w)) + sqrt(P.grav * h);
+        }
+        if (!(v == v)) v = 0.0;
+    }
+    block_max_to(v, acc);
+}
+
+__global__ void k_cfl_from_bits(dclaw_clock* clk) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) clk->cfl = __longlong_as_double((long long)clk->cfl_bits);
+}
+
+// ---- host helpers ----------------------------------------------------------
+inline unsigned nblocks(long long n) { return (unsigned)((n + TPB - 1) / TPB); }
+
+inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+struct Layout {
+    size_t npad, nxi, nyi;
+    size_t off_qB, off_bP, off_td, off_wx, off_wy, off_fx, off_fy, total;
+};
+
+inline Layout layout(int mx, int my) {
+    Layout L;
+    L.npad = (size_t)(mx + 4) * (my + 4);
+    L.nxi = (size_t)(mx + 3) * (my + 2);
+    L.nyi = (size_t)(my + 3) * (mx + 2);
+    size_t o = 0;
+    L.off_qB = o; o += align256(5 * L.npad * 8);
+    L.off_bP = o; o += align256(L.npad * 8);
+    L.off_td = o; o += align256(3 * L.npad * 8);
+    L.off_wx = o; o += align256((size_t)NW * L.nxi * 8);
+    L.off_wy = o; o += align256((size_t)NW * L.nyi * 8);
+    L.off_fx = o; o += align256((size_t)NF * L.nxi * 8);
+    L.off_fy = o; o += align256((size_t)NF * L.nyi * 8);
+    L.total = o;
+    return L;
+}
+
+inline Work make_work(void* base, const Layout& L) {
+    char* b = (char*)base;
+    Work W;
+    W.qB = (double*)(b + L.off_qB);
+    W.bP = (double*)(b + L.off_bP);
+    W.td = (double*)(b + L.off_td);
+    W.wx = (double*)(b + L.off_wx);
+    W.wy = (double*)(b + L.off_wy);
+    W.fx = (double*)(b + L.off_fx);
+    W.fy = (double*)(b + L.off_fy);
+    W.npad = L.npad;
+    W.nxi = L.nxi;
+    W.nyi = L.nyi;
+    return W;
+}
+
+inline int cuda_status() {
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? DCLAW_OK : DCLAW_ERR_CUDA;
+}
+
+inline bool sizes_ok(int mx, int my) {
+    return mx >= 2 && my >= 2 && (long long)(mx + 4) * (my + 4) < (1LL << 40);
+}
+
+}  // namespace dclaw
+
+using namespace dclaw;
+
+extern "C" {
+
+int dclaw_abi_version(void) { return DCLAW_ABI_VERSION; }
+
+const char* dclaw_error_string(int code) {
+    switch (code) {
+        case DCLAW_OK: return "ok";
+        case DCLAW_ERR_ARG: return "invalid argument";
+        case DCLAW_ERR_UNSUPPORTED: return "unsupported option";
+        case DCLAW_ERR_NAN: return "NaN in the state";
+        case DCLAW_ERR_CUDA: return "CUDA error";
+        case DCLAW_ERR_WORKSPACE: return "workspace too small";
+        case DCLAW_ERR_TOO_LARGE: return "size beyond the fixed limit";
+        default: return "unknown error";
+    }
+}
+
+void dclaw_params_default(dclaw_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->grav = 9.81;
+    p->dry_tolerance = 1.0e-3;
+    p->speed_limit = 1.0e6;
+    p->friction_forcing = 0;
+    p->dd_manning = 0;
+    p->manning_coefficient = 0.0;
+    p->friction_depth = 1.0e6;
+    p->manning_max = 0.06;
+    p->rho_s = 2700.0;
+    p->rho_f = 1000.0;
+    p->m_crit = 0.64;
+    p->m0 = 0.62;
+    p->mref = 0.60;
+    p->kref = 1.0e-10;
+    p->phi = 32.0 * 3.14159265358979323846 / 180.0;
+    p->delta = 0.01;
+    p->mu = 0.005;
+    p->alpha_c = 0.01;
+    p->c1 = 1.0;
+    p->sigma_0 = 1.0e3;
+    p->theta_input = 0.0;
+    p->src2method = 0;
+    p->alphamethod = 0;
+    p->rarecorrectortest = 0;
+    p->order = 2;
+    p->transverse_waves = 2;
+    p->limiter = 4;
+    p->bc_lower[0] = p->bc_lower[1] = DCLAW_BC_WALL;
+    p->bc_upper[0] = p->bc_upper[1] = DCLAW_BC_WALL;
+    p->cfl_desired = 0.9;
+    p->cfl_max = 1.0;
+    p->dt_max = 1.0e99;
+}
+
+int dclaw_params_check(const dclaw_params* p) {
+    if (!p) return DCLAW_ERR_ARG;
+    if (p->bed_normal != 0 || p->entrainment != 0 || p->segregation != 0 || p->curvature != 0)
+        return DCLAW_ERR_UNSUPPORTED;
+    if (p->src2method < -1 || p->src2method > 1) return DCLAW_ERR_UNSUPPORTED;
+    if (p->alphamethod != 0 && p->alphamethod != 1) return DCLAW_ERR_ARG;
+    if (p->order != 1 && p->order != 2) return DCLAW_ERR_ARG;
+    if (p->transverse_waves < 0 || p->transverse_waves > 2) return DCLAW_ERR_ARG;
+    if (p->limiter < 0 || p->limiter > 5) return DCLAW_ERR_ARG;
+    for (int k = 0; k < 2; ++k) {
+        if (p->bc_lower[k] != DCLAW_BC_WALL && p->bc_lower[k] != DCLAW_BC_EXTRAP) return DCLAW_ERR_ARG;
+        if (p->bc_upper[k] != DCLAW_BC_WALL && p->bc_upper[k] != DCLAW_BC_EXTRAP) return DCLAW_ERR_ARG;
+    }
+    if (!(p->grav > 0.0) || !(p->dry_tolerance > 0.0) || !(p->rho_f > 0.0) || !(p->rho_s > 0.0)) return DCLAW_ERR_ARG;
+    if (!(p->alpha_c > 0.0) || !(p->cfl_desired > 0.0) || !(p->dt_max > 0.0)) return DCLAW_ERR_ARG;
+    return DCLAW_OK;
+}
+
+size_t dclaw_workspace_bytes(int mx, int my) {
+    if (!sizes_ok(mx, my)) return 0;
+    return layout(mx, my).total;
+}
+
+int dclaw_clock_init(dclaw_clock* clock, double t, double dt, double t_final, int fixed_dt, void* stream) {
+    if (!clock) return DCLAW_ERR_ARG;
+    k_clock_init<<<1, 32, 0, (cudaStream_t)stream>>>(clock, t, dt, t_final, fixed_dt);
+    return cuda_status();
+}
+
+int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int my, double dx, double dy,
+               const dclaw_params* p, dclaw_clock* clock, void* work, size_t work_bytes, uint32_t* branch_log,
+               void* stream) {
+    if (!q_in || !q_out || !b || !p || !clock || !work || q_in == q_out) return DCLAW_ERR_ARG;
+    if (!sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0)) return DCLAW_ERR_ARG;
+    int rc = dclaw_params_check(p);
+    if (rc) return rc;
+    Layout L = layout(mx, my);
+    if (work_bytes < L.total) return DCLAW_ERR_WORKSPACE;
+    cudaStream_t s = (cudaStream_t)stream;
+    Geom g{mx, my, mx + 4, my + 4, dx, dy};
+    Work W = make_work(work, L);
+    const dclaw_params P = *p;
+    k_b4<<<nblocks((long long)L.npad), TPB, 0, s>>>(P, g, q_in, b, W, clock);
+    k_taudir<<<nblocks((long long)L.npad), TPB, 0, s>>>(P, g, W, 0);
+    k_riemann<0><<<nblocks((long long)L.nxi), TPB, 0, s>>>(P, g, W, clock, branch_log);
+    k_riemann<1><<<nblocks((long long)(mx + 2) * (my + 3)), TPB, 0, s>>>(P, g, W, clock, branch_log);
+    k_flux<0><<<nblocks((long long)(mx + 1) * (my + 2)), TPB, 0, s>>>(P, g, W, clock, branch_log);
+    k_flux<1><<<nblocks((long long)(mx + 2) * (my + 1)), TPB, 0, s>>>(P, g, W, clock, branch_log);
+    k_final<<<nblocks((long long)mx * my), TPB, 0, s>>>(P, g, W, q_out, clock);
+    k_tick<<<1, 32, 0, s>>>(P, clock);
+    return cuda_status();
+}
+
+int dclaw_bc2amr(double* q, int mx, int my, int mbc, const dclaw_params* p, void* stream) {
+    if (!q || !p || mbc != 2 || !sizes_ok(mx, my)) return DCLAW_ERR_ARG;
+    int rc = dclaw_params_check(p);
+    if (rc) return rc;
+    k_bc2amr<<<nblocks((long long)(mx + 4) * (my + 4)), TPB, 0, (cudaStream_t)stream>>>(*p, mx, my, q);
+    return cuda_status();
+}
+
+int dclaw_setaux(double* aux, int mx, int my, int mbc, const dclaw_params* p, void* stream) {
+    if (!aux || !p || mbc != 2 || !sizes_ok(mx, my)) return DCLAW_ERR_ARG;
+    k_setaux<<<nblocks((long long)(mx + 4) * (my + 4)), TPB, 0, (cudaStream_t)stream>>>(*p, mx, my, aux);
+    return cuda_status();
+}
+
+int dclaw_b4step2(double* q, double* aux, int mx, int my, int mbc, double dx, double dy, double t, double dt,
+                  const dclaw_params* p, dclaw_clock* clock, void* stream) {
+    (void)t; (void)dt;
+    if (!q || !aux || !p || mbc != 2 || !sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0)) return DCLAW_ERR_ARG;
+    int rc = dclaw_params_check(p);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t npad = (size_t)(mx + 4) * (my + 4);
+    k_b4_padded<<<nblocks((long long)npad), TPB, 0, s>>>(*p, mx, my, q, clock);
+    Geom g{mx, my, mx + 4, my + 4, dx, dy};
+    Work W{};
+    W.qB = q;
+    W.bP = aux;
+    W.td = aux + 3 * npad;
+    W.npad = npad;
+    k_taudir<<<nblocks((long long)npad), TPB, 0, s>>>(*p, g, W, 1);
+    return cuda_status();
+}
+
+int dclaw_step2(double* q, const double* aux, int mx, int my, int mbc, double dx, double dy, double dt,
+                const dclaw_params* p, dclaw_clock* clock, double* fluxes, void* work, size_t work_bytes,
+                void* stream) {
+    if (!q || !aux || !p || !clock || !work || mbc != 2 || !sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0))
+        return DCLAW_ERR_ARG;
+    int rc = dclaw_params_check(p);
+    if (rc) return rc;
+    Layout L = layout(mx, my);
+    if (work_bytes < L.total) return DCLAW_ERR_WORKSPACE;
+    cudaStream_t s = (cudaStream_t)stream;
+    Geom g{mx, my, mx + 4, my + 4, dx, dy};
+    Work W = make_work(work, L);
+    W.qB = q;
+    W.bP = const_cast<double*>(aux);
+    W.td = const_cast<double*>(aux) + 3 * L.npad;
+    // the kernels read dt from the clock: use a clock set to this dt
+    k_clock_init<<<1, 32, 0, s>>>(clock, 0.0, dt, 0.0, 1);
+    const dclaw_params P = *p;
+    k_riemann<0><<<nblocks((long long)L.nxi), TPB, 0, s>>>(P, g, W, clock, nullptr);
+    k_riemann<1><<<nblocks((long long)(mx + 2) * (my + 3)), TPB, 0, s>>>(P, g, W, clock, nullptr);
+    k_flux<0><<<nblocks((long long)(mx + 1) * (my + 2)), TPB, 0, s>>>(P, g, W, clock, nullptr);
+    k_flux<1><<<nblocks((long long)(mx + 2) * (my + 1)), TPB, 0, s>>>(P, g, W, clock, nullptr);
+    k_update_padded<<<nblocks((long long)mx * my), TPB, 0, s>>>(g, W, dt, q, fluxes, clock);
+    k_cfl_from_bits<<<1, 32, 0, s>>>(clock);
+    return cuda_status();
+}
+
+int dclaw_src2(double* q, const double* aux, int mx, int my, int mbc, double dx, double dy, double t, double dt,
+               const dclaw_params* p, void* stream) {
+    (void)aux; (void)dx; (void)dy; (void)t;
+    if (!q || !p || mbc != 2 || !sizes_ok(mx, my)) return DCLAW_ERR_ARG;
+    int rc = dclaw_params_check(p);
+    if (rc) return rc;
+    k_src2_padded<<<nblocks((long long)mx * my), TPB, 0, (cudaStream_t)stream>>>(*p, mx, my, dt, q);
+    return cuda_status();
+}
+
+int dclaw_max_wave_speed(const double* q, int mx, int my, const dclaw_params* p, double* smax, void* stream) {
+    if (!q || !p || !smax || !sizes_ok(mx, my)) return DCLAW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaMemsetAsync(smax, 0, sizeof(double), s);
+    k_wave_speed<<<nblocks((long long)mx * my), TPB, 0, s>>>(*p, mx, my, q, (unsigned long long*)smax);
+    return cuda_status();
+}
+
+}  // extern "C"

@@ -1,0 +1,173 @@
+/*
+ * dclaw_b200.h -- C ABI of the B200 (sm_100a) D-Claw uniform-patch time step.
+ *
+ * The step is D-Claw's single-level patch update: b4step2 (admissibility,
+ * speed limit, static-friction directions), step2/flux2 (augmented f-wave
+ * Riemann solves, MC wave limiting, transverse propagation, flux
+ * accumulation, Courant number) and src2 (Coulomb/viscous friction,
+ * pore-pressure and solid-fraction relaxation), all in FP64.
+ *
+ * Conventions shared by every entry point
+ *   - All array arguments are DEVICE pointers unless stated otherwise;
+ *     `const dclaw_params*` is always a HOST pointer (copied into the launch).
+ *   - State is structure-of-arrays, 5 planes in the order h, hu, hv, hm, pb.
+ *     The segregation (h*chi) and bed-change fields of the 7-field Fortran
+ *     state are identically zero when segregation = 0 and entrainment = 0,
+ *     which is the only configuration accepted, so they are not stored.
+ *   - Patch-call layout ("padded"): each plane holds (mx+2*mbc)*(my+2*mbc)
+ *     doubles, x fastest; cell (i,j) with Fortran index i in 1-mbc..mx+mbc,
+ *     j in 1-mbc..my+mbc lives at [(j-1+mbc)*(mx+2*mbc) + (i-1+mbc)].
+ *     mbc must be 2.
+ *   - Fused layout ("interior"): each plane holds mx*my doubles, x fastest;
+ *     ghost cells are produced on the fly from the boundary conditions.
+ *   - aux planes (padded layout): 0 b (bed), 1 phi, 2 theta, 3 fsphi,
+ *     4 taudir_x, 5 taudir_y -- the first six D-Claw aux fields of a
+ *     Cartesian run (digclaw_module.f90:96-110).
+ *   - Every call is asynchronous on `stream` (a cudaStream_t, NULL = legacy
+ *     default stream). The return code reports argument errors found on the
+ *     host and CUDA launch errors; numerical errors (NaN in the state) are
+ *     reported through the device status word of dclaw_clock.
+ *   - The library never allocates device memory on these paths: callers
+ *     pass a workspace of dclaw_workspace_bytes() bytes.
+ */
+#ifndef DCLAW_B200_H
+#define DCLAW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DCLAW_ABI_VERSION 1
+
+/* return / status codes */
+#define DCLAW_OK 0
+#define DCLAW_ERR_ARG 1          /* bad size, pointer or parameter */
+#define DCLAW_ERR_UNSUPPORTED 2  /* option not implemented (bed_normal=1, ...) */
+#define DCLAW_ERR_NAN 3          /* NaN found in the state (check4nans) */
+#define DCLAW_ERR_CUDA 4         /* CUDA launch / runtime error */
+#define DCLAW_ERR_WORKSPACE 5    /* workspace too small */
+#define DCLAW_ERR_TOO_LARGE 6    /* size beyond a fixed limit */
+
+/* boundary condition codes (clawdata.bc_lower / bc_upper) */
+#define DCLAW_BC_EXTRAP 1
+#define DCLAW_BC_WALL 3
+
+/*
+ * Parameters. Names follow the reference's setrun data classes:
+ * geo_data (grav, dry_tolerance, speed_limit, friction_*), DClawInputData
+ * (src/python/dclaw/data.py:315-351) and clawdata (order, transverse_waves,
+ * limiter, cfl_*, dt_*, bc_*). Angles are in RADIANS here (set_dig converts
+ * degrees, digclaw_module.f90:135-136).
+ */
+typedef struct dclaw_params {
+    /* geo_data */
+    double grav;
+    double dry_tolerance;
+    double speed_limit;
+    int32_t friction_forcing;     /* Manning friction in src2 (src2.f90:271-289) */
+    int32_t dd_manning;
+    double manning_coefficient;
+    double friction_depth;
+    double manning_max;
+    /* dclaw_data */
+    double rho_s, rho_f, m_crit, m0, mref, kref;
+    double phi;                   /* basal friction angle, radians */
+    double delta, mu, alpha_c, c1, sigma_0;
+    double theta_input;           /* radians; only used with bed_normal = 1 */
+    int32_t src2method;           /* -1, 0 or 1 (2 = FE_4quad: not accepted) */
+    int32_t alphamethod;          /* 0 or 1 */
+    int32_t rarecorrectortest;    /* 0/1 */
+    int32_t bed_normal;           /* must be 0 */
+    int32_t entrainment;          /* must be 0 */
+    int32_t segregation;          /* must be 0 */
+    int32_t curvature;            /* must be 0 */
+    /* clawdata */
+    int32_t order;                /* method(2): 1 or 2 */
+    int32_t transverse_waves;     /* method(3): 0, 1 or 2 */
+    int32_t limiter;              /* mthlim for every wave: 0 none,1 minmod,2 superbee,3 van Leer,4 MC,5 Beam-Warming */
+    int32_t bc_lower[2];          /* x, y */
+    int32_t bc_upper[2];          /* x, y */
+    double cfl_desired;
+    double cfl_max;
+    double dt_max;
+} dclaw_params;
+
+/*
+ * Device-resident clock of a run: the Courant number of the last step and
+ * the dt chosen for the next one by the tick rule
+ *   dt_next = min(dt * cfl_desired / cfl, dt_max)   (cfl > 0; dt_max else),
+ * clipped so that t never passes t_final when t_final > 0
+ * (tick.f:490-526 and the time clamp of the step-function API).
+ */
+typedef struct dclaw_clock {
+    double t;            /* simulated time after the last step */
+    double dt;           /* dt the next step will use */
+    double cfl;          /* Courant number of the last step (cflgrid) */
+    double dt_last;      /* dt the last step used */
+    double t_final;      /* <= 0: no clamp */
+    uint64_t cfl_bits;   /* internal accumulator (order-preserving bits) */
+    uint32_t nsteps;     /* steps taken */
+    uint32_t blocks_done;/* internal counter */
+    int32_t status;      /* DCLAW_OK or DCLAW_ERR_NAN */
+    int32_t fixed_dt;    /* 1: keep dt constant (no tick rule) */
+} dclaw_clock;
+
+/* ---- library info and parameters ---------------------------------------- */
+int dclaw_abi_version(void);
+const char* dclaw_error_string(int code);
+/* reference defaults (data.py:315-351, geo_data, clawdata) with config-0 style numerics */
+void dclaw_params_default(dclaw_params* p);
+/* host-side validation; returns DCLAW_OK, DCLAW_ERR_ARG or DCLAW_ERR_UNSUPPORTED */
+int dclaw_params_check(const dclaw_params* p);
+/* bytes of device workspace the step entry points need for an mx x my patch */
+size_t dclaw_workspace_bytes(int mx, int my);
+
+/* ---- step2-style patch calls (padded layout, mbc = 2) -------------------
+ * Replace the Fortran patch step of stepgrid: bc2amr (GeoClaw, called before
+ * the step), b4step2 (src/2d/dig/b4step2.f90:7), step2 + stepgrid's
+ * flux-differencing update (GeoClaw step2.f90, driving flux2fw.f:8-11 with
+ * rpn2_dclaw.f:24 / rpt2_dclaw.f:16) and src2 (src/2d/dig/src2.f90:27).
+ */
+/* fill the two ghost rings of q from the boundary conditions (bc2amr) */
+int dclaw_bc2amr(double* q, int mx, int my, int mbc, const dclaw_params* p, void* stream);
+/* fill aux for a new patch: ghost bed = nearest interior bed (setaux.f90:155-184),
+ * phi/theta uniform, fsphi/taudir zero (setaux.f90:195-198,268-281) */
+int dclaw_setaux(double* aux, int mx, int my, int mbc, const dclaw_params* p, void* stream);
+/* b4step2: qfix + bdif clamp on all cells, speed limit, calc_taudir (aux 3..5) */
+int dclaw_b4step2(double* q, double* aux, int mx, int my, int mbc, double dx, double dy,
+                  double t, double dt, const dclaw_params* p, dclaw_clock* clock, void* stream);
+/* step2 + update: q <- q - dt/dx (fm(i+1)-fp(i)) - dt/dy (gm(j+1)-gp(j)) on the interior;
+ * the patch Courant number is max-reduced into clock->cfl_bits/cfl.
+ * fluxes (nullable): 20 padded planes fm[5], fp[5], gm[5], gp[5]. */
+int dclaw_step2(double* q, const double* aux, int mx, int my, int mbc, double dx, double dy,
+                double dt, const dclaw_params* p, dclaw_clock* clock, double* fluxes,
+                void* work, size_t work_bytes, void* stream);
+/* src2: friction + m/pb relaxation on interior cells */
+int dclaw_src2(double* q, const double* aux, int mx, int my, int mbc, double dx, double dy,
+               double t, double dt, const dclaw_params* p, void* stream);
+
+/* ---- fused uniform-patch step (interior layout) -------------------------
+ * One full step (bc2amr + b4step2 + step2 + update + src2 + Courant number)
+ * from q_in to q_out (distinct buffers). dt is read from clock->dt; after
+ * the step clock holds t += dt, cfl, nsteps += 1 and the next dt (tick rule
+ * unless clock->fixed_dt). phi is the uniform basal friction angle
+ * (p->phi). branch_log (nullable) receives per-interface branch bits:
+ * x interfaces [(my+2) rows][(mx+1)], then y interfaces [(mx+2) cols][(my+1)].
+ */
+int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int my,
+               double dx, double dy, const dclaw_params* p, dclaw_clock* clock,
+               void* work, size_t work_bytes, uint32_t* branch_log, void* stream);
+/* initialise a device clock: t, dt, t_final, fixed_dt; counters cleared */
+int dclaw_clock_init(dclaw_clock* clock, double t, double dt, double t_final, int fixed_dt,
+                     void* stream);
+/* max over cells of |u|+sqrt(g h) (interior layout) written to *smax (device double) */
+int dclaw_max_wave_speed(const double* q, int mx, int my, const dclaw_params* p, double* smax,
+                         void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DCLAW_B200_H */

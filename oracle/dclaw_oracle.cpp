@@ -1,0 +1,1535 @@
+/*
+ * dclaw_oracle.cpp -- TEST INFRASTRUCTURE, NOT PRODUCT CODE.
+ *
+ * CPU restatement (C++17, FP64, glibc libm, no FMA contraction) of D-Claw's
+ * uniform-patch time step, written to follow the reference Fortran line by
+ * line so that the CUDA kernels can be checked against it. Only the tests,
+ * the smoke check and the CPU-baseline leg of the benchmark may load it.
+ *
+ * Sources restated (paths inside the youryugi/dclaw project):
+ *   src/2d/dig/digclaw_module.f90  qfix :285, qfix_cmass :353, setvars :394,
+ *                                  calc_taudir :500
+ *   src/2d/dig/b4step2.f90         b4step2 :7
+ *   src/2d/dig/rpn2_dclaw.f        rpn2 :24
+ *   src/2d/dig/riemannsolvers_dclaw.f  riemann_dig2_aug_sswave_ez :3,
+ *                                  riemanntype :526
+ *   src/2d/dig/rpt2_dclaw.f        rpt2 :16
+ *   src/2d/dig/flux2fw.f           flux2 :8
+ *   src/2d/dig/src2.f90            src2 :27
+ *   src/2d/dig/mp_update.f90       mp_update_relax_Dclaw4 :710
+ *   src/2d/dig/setaux.f90          ghost bed :155-184, aux defaults :195-198,268-281
+ *   src/2d/dig/tick.f              dt update :490-526
+ * Clawpack pieces that the reference links from an unpinned Clawpack
+ * checkout (src/2d/dig/Makefile.dclaw:108,130,132; not in the reference
+ * tree) are restated from the published wave-propagation method
+ * (LeVeque 2002, "Finite Volume Methods for Hyperbolic Problems",
+ * ch. 6.9/6.12 wave limiters, ch. 21 transverse propagation, f-waves):
+ *   step2 sweep/accumulation order and the stepgrid update, the wave
+ *   limiter (inlinelimiter), bc2amr wall/extrapolation ghost cells.
+ *
+ * Parity status: no output of the reference Fortran exists for this path
+ * (no Fortran compiler, no Clawpack, no committed fort.q files), so this
+ * restatement is pinned only by the closed-form known-answer tests that the
+ * reference's own test suites define (tests/eigenstructure_check/check.py:65,80,97-118,
+ * differentiable_dclaw/tests/test_lake_at_rest.py:42). Beyond those KATs
+ * parity is unpinned.
+ *
+ * Layout: the Fortran arrays q(7, 1-mbc:mx+mbc, 1-mbc:my+mbc) and
+ * aux(10, ...) are kept (field fastest), mbc = 2.
+ */
+#include "../include/dclaw_b200.h"
+
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr int MEQN = 7;
+constexpr int MAUX = 10;
+constexpr int MWAVES = 5;
+constexpr int MBC = 2;
+// q indices (digclaw_module.f90:96-102), 1-based as in Fortran
+constexpr int I_H = 1, I_HU = 2, I_HV = 3, I_HM = 4, I_PB = 5, I_HCHI = 6, I_BDIF = 7;
+// aux indices for a Cartesian run (digclaw_module.f90:83-110)
+constexpr int I_PHI = 2, I_THETA = 3, I_FSPHI = 4, I_TAUDIR_X = 5, I_TAUDIR_Y = 6;
+
+// branch bits, shared meaning with the CUDA path
+constexpr uint32_t BR_DRY = 1u << 0, BR_WALL = 1u << 1, BR_SONIC = 1u << 2, BR_STATIC = 1u << 3,
+                   BR_WET4 = 1u << 4, BR_REVERT_L = 1u << 5, BR_RPT1 = 1u << 6, BR_RPT2 = 1u << 7;
+inline uint32_t br_lim(int mw, uint32_t code) { return code << (8 + 3 * (mw - 1)); }
+inline uint32_t br_up(int mw) { return 1u << (23 + (mw - 1)); }
+
+inline double sq(double x) { return x * x; }
+// Fortran MAX/MIN with two arguments
+inline double fmax2(double a, double b) { return a > b ? a : b; }
+inline double fmin2(double a, double b) { return a < b ? a : b; }
+// Fortran SIGN(a,b) for reals: |a| with the sign bit of b
+inline double fsign(double a, double b) { return std::copysign(std::fabs(a), b); }
+
+struct Model {
+    dclaw_params p;
+    double phi;      // module variable `phi`, overwritten by calc_taudir (digclaw_module.f90:557)
+    double kappa;    // earth pressure coefficient, hard-coded 1 (digclaw_module.f90:113)
+};
+
+// ---------------------------------------------------------------------------
+// digclaw_module.f90:285-345
+void qfix(const Model& M, double& h, double& hu, double& hv, double& hm, double& p, double& hchi,
+          double& u, double& v, double& m, double& chi, double& rho, double gz) {
+    const dclaw_params& P = M.p;
+    if (h <= P.dry_tolerance) {
+        h = 0.0; hu = 0.0; hv = 0.0; hm = 0.0; p = 0.0; hchi = 0.0;
+        u = 0.0; v = 0.0; m = 0.0; chi = 0.0; rho = 0.0;
+        return;
+    }
+    u = hu / h;
+    v = hv / h;
+    m = hm / h;
+    chi = hchi / h;
+    m = fmax2(m, 0.0);
+    m = fmin2(m, 1.0);
+    hm = h * m;
+    chi = fmax2(chi, 0.0);
+    chi = fmin2(chi, 1.0);
+    hchi = h * chi;
+    rho = P.rho_s * m + (1.0 - m) * P.rho_f;
+    double pmax = rho * gz * h;
+    p = fmax2(0.0, p);
+    p = fmin2(pmax, p);
+}
+
+// digclaw_module.f90:353-387
+void qfix_cmass(const Model& M, double& h, double& m, double& p, double& rho, double& p_exc,
+                double& hu, double& hv, double& hm, double u, double v, double rhoh, double gz) {
+    const dclaw_params& P = M.p;
+    m = fmax2(m, 0.0);
+    m = fmin2(m, 1.0);
+    rho = m * (P.rho_s - P.rho_f) + P.rho_f;
+    h = rhoh / rho;
+    double p_exc_max = rhoh * gz - P.rho_f * h * gz;
+    double p_exc_min = 0.0 - P.rho_f * h * gz;
+    p_exc = fmax2(p_exc_min, p_exc);
+    p_exc = fmin2(p_exc_max, p_exc);
+    p = P.rho_f * gz * h + p_exc;
+    hu = h * u;
+    hv = h * v;
+    hm = h * m;
+}
+
+// digclaw_module.f90:394-491 (segregation = 0: kr_chi = 1)
+void setvars(const Model& M, double h, double u, double v, double m, double p, double /*chi*/,
+             double gz, double& rho, double& kperm, double& alphainv, double& m_eq,
+             double& tanpsi, double& tau) {
+    const dclaw_params& P = M.p;
+    rho = m * (P.rho_s - P.rho_f) + P.rho_f;
+    double kr_chi = 1.0;
+    kperm = kr_chi * P.kref * std::exp(-(m - P.mref) / (0.04));
+    double sig_eff = fmax2(0.0, rho * gz * h - p);
+    double sig_0 = 0.0;
+    if (P.alphamethod == 0) {
+        sig_0 = P.sigma_0;
+    } else if (P.alphamethod == 1) {
+        sig_0 = 0.50 * P.alpha_c * P.rho_f * (P.rho_s - P.rho_f) * gz * h / rho;
+    }
+    alphainv = m * (sig_eff + sig_0) / P.alpha_c;
+    double vnorm = std::sqrt(sq(u) + sq(v));
+    double shear;
+    if (h > P.dry_tolerance) shear = 2.0 * vnorm / h;
+    else shear = 0.0;
+    double Nden = P.rho_s * sq(shear * P.delta) + sig_eff;
+    double Nnum = P.mu * shear;
+    if (Nnum <= 0.0) m_eq = P.m_crit;
+    else m_eq = P.m_crit * (std::sqrt(Nden) / (std::sqrt(Nden) + std::sqrt(Nnum)));
+    tanpsi = P.c1 * (m - m_eq);
+    double psi = std::atan(P.c1 * (m - m_eq));
+    tau = sig_eff * std::tan(M.phi + psi);
+    tau = tau * 0.5 * (1.0 + std::tanh(100.0 * (m - 0.1)));
+}
+
+// ---------------------------------------------------------------------------
+struct Patch {
+    int mx, my;
+    std::vector<double> q;    // q(7, 1-mbc:mx+mbc, 1-mbc:my+mbc)
+    std::vector<double> aux;  // aux(10, ...)
+    Patch(int mx_, int my_) : mx(mx_), my(my_),
+        q((size_t)MEQN * (mx_ + 2 * MBC) * (my_ + 2 * MBC), 0.0),
+        aux((size_t)MAUX * (mx_ + 2 * MBC) * (my_ + 2 * MBC), 0.0) {}
+    size_t cell(int i, int j) const {
+        return (size_t)(j + MBC - 1) * (mx + 2 * MBC) + (size_t)(i + MBC - 1);
+    }
+    double& Q(int m, int i, int j) { return q[cell(i, j) * MEQN + (m - 1)]; }
+    double& A(int m, int i, int j) { return aux[cell(i, j) * MAUX + (m - 1)]; }
+};
+
+// digclaw_module.f90:500-719 (bed_normal = 0: theta = 0, gz = grav)
+void calc_taudir(Model& M, Patch& pt, double dx, double dy) {
+    const dclaw_params& P = M.p;
+    const int mx = pt.mx, my = pt.my;
+    const double dry = P.dry_tolerance;
+    double gz = P.grav;
+    for (int j = 2 - MBC; j <= my + MBC - 1; ++j) {
+        for (int i = 2 - MBC; i <= mx + MBC - 1; ++i) {
+            double theta = 0.0;
+            double u, v, m, chi, rho;
+            double h = pt.Q(I_H, i, j), hu = pt.Q(I_HU, i, j), hv = pt.Q(I_HV, i, j);
+            double hm = pt.Q(I_HM, i, j), p = pt.Q(I_PB, i, j), hchi = pt.Q(I_HCHI, i, j);
+            qfix(M, h, hu, hv, hm, p, hchi, u, v, m, chi, rho, gz);
+            double b = pt.A(1, i, j) - pt.Q(I_BDIF, i, j);
+            double eta = h + b;
+            M.phi = pt.A(I_PHI, i, j);
+
+            double uX, vX, mX, chiX, rhoX;
+            double hL = pt.Q(I_H, i - 1, j), huL = pt.Q(I_HU, i - 1, j), hvL = pt.Q(I_HV, i - 1, j);
+            double hmL = pt.Q(I_HM, i - 1, j), pL = pt.Q(I_PB, i - 1, j), hchiL = pt.Q(I_HCHI, i - 1, j);
+            qfix(M, hL, huL, hvL, hmL, pL, hchiL, uX, vX, mX, chiX, rhoX, gz);
+            double bL = pt.A(1, i - 1, j) - pt.Q(I_BDIF, i - 1, j);
+            double etaL = hL + bL;
+            if (hL < dry) etaL = fmin2(etaL, eta);
+
+            double hR = pt.Q(I_H, i + 1, j), huR = pt.Q(I_HU, i + 1, j), hvR = pt.Q(I_HV, i + 1, j);
+            double hmR = pt.Q(I_HM, i + 1, j), pR = pt.Q(I_PB, i + 1, j), hchiR = pt.Q(I_HCHI, i + 1, j);
+            qfix(M, hR, huR, hvR, hmR, pR, hchiR, uX, vX, mX, chiX, rhoX, gz);
+            double bR = pt.A(1, i + 1, j) - pt.Q(I_BDIF, i + 1, j);
+            double etaR = hR + bR;
+            if (hR < dry) etaR = fmin2(etaR, eta);
+
+            double hB = pt.Q(I_H, i, j - 1), huB = pt.Q(I_HU, i, j - 1), hvB = pt.Q(I_HV, i, j - 1);
+            double hmB = pt.Q(I_HM, i, j - 1), pB = pt.Q(I_PB, i, j - 1), hchiB = pt.Q(I_HCHI, i, j - 1);
+            qfix(M, hB, huB, hvB, hmB, pB, hchiB, uX, vX, mX, chiX, rhoX, gz);
+            double bB = pt.A(1, i, j - 1) - pt.Q(I_BDIF, i, j - 1);
+            double etaB = hB + bB;
+            if (hB < dry) etaB = fmin2(etaB, eta);
+
+            double hT = pt.Q(I_H, i, j + 1), huT = pt.Q(I_HU, i, j + 1), hvT = pt.Q(I_HV, i, j + 1);
+            double hmT = pt.Q(I_HM, i, j + 1), pT = pt.Q(I_PB, i, j + 1), hchiT = pt.Q(I_HCHI, i, j + 1);
+            qfix(M, hT, huT, hvT, hmT, pT, hchiT, uX, vX, mX, chiX, rhoX, gz);
+            double bT = pt.A(1, i, j + 1) - pt.Q(I_BDIF, i, j + 1);
+            double etaT = hT + bT;
+            if (hT < dry) etaT = fmin2(etaT, eta);
+
+            if (h < dry) {
+                eta = fmin2(etaL, eta);
+                eta = fmin2(etaB, eta);
+            }
+            if ((h + hL + hB + hR + hT) < dry) {
+                pt.A(I_TAUDIR_X, i, j) = 0.0;
+                pt.A(I_TAUDIR_Y, i, j) = 0.0;
+                pt.A(I_FSPHI, i, j) = 0.0;
+                continue;
+            }
+            double kperm, alphainv, m_eq, tanpsi, tau;
+            setvars(M, h, u, v, m, p, chi, gz, rho, kperm, alphainv, m_eq, tanpsi, tau);
+
+            double FxL = -gz * 0.5 * (h + hL) * (eta - etaL) / (dx) + gz * 0.5 * (h + hL) * std::sin(theta);
+            double FyL = -gz * 0.5 * (h + hB) * (eta - etaB) / (dy);
+            double FxR = -gz * 0.5 * (h + hR) * (etaR - eta) / (dx) + gz * 0.5 * (h + hR) * std::sin(theta);
+            double FyR = -gz * 0.5 * (h + hT) * (etaT - eta) / (dy);
+            double Fx, Fy;
+            if (FxL * FxR > 0.0) Fx = fsign(fmin2(std::fabs(FxL), std::fabs(FxR)), FxL);
+            else Fx = 0.0;
+            if (FyL * FyR > 0.0) Fy = fsign(fmin2(std::fabs(FyL), std::fabs(FyR)), FyL);
+            else Fy = 0.0;
+
+            double hvnorm = std::sqrt(sq(hu) + sq(hv));
+            if (hvnorm > 0.0) {
+                pt.A(I_TAUDIR_X, i, j) = -dx * hu / hvnorm;
+                pt.A(I_TAUDIR_Y, i, j) = -dy * hv / hvnorm;
+                double dot = fmin2(fmax2(0.0, Fx * hu), fmax2(0.0, Fy * hv));
+                if (dot > 0.0) {
+                    double Fproj = dot / hvnorm;
+                    pt.A(I_FSPHI, i, j) = fmin2(1.0, Fproj * rho / fmax2(tau, 1.0e-16));
+                } else {
+                    pt.A(I_FSPHI, i, j) = 0.0;
+                }
+            } else {
+                if ((sq(FxL) + sq(Fy)) > 0.0) pt.A(I_TAUDIR_X, i, j) = -dx * FxL / std::sqrt(sq(FxL) + sq(Fy));
+                else pt.A(I_TAUDIR_X, i, j) = dx * 1.0;
+                if ((sq(Fx) + sq(FyL)) > 0.0) pt.A(I_TAUDIR_Y, i, j) = -dy * FyL / std::sqrt(sq(Fx) + sq(FyL));
+                else pt.A(I_TAUDIR_Y, i, j) = dy * 1.0;
+                if ((sq(pt.A(I_TAUDIR_Y, i, j)) + sq(pt.A(I_TAUDIR_X, i, j))) > 0.0) pt.A(I_FSPHI, i, j) = 1.0;
+                else pt.A(I_FSPHI, i, j) = 0.0;
+            }
+        }
+    }
+}
+
+// b4step2.f90:7-113 (check4nans is reported by the driver; setaux is not re-run:
+// the bed is static, aux_finalized >= 2)
+void b4step2(Model& M, Patch& pt, double dx, double dy) {
+    const dclaw_params& P = M.p;
+    const int mx = pt.mx, my = pt.my;
+    double gz = P.grav;
+    for (int j = 1 - MBC; j <= my + MBC; ++j) {
+        for (int i = 1 - MBC; i <= mx + MBC; ++i) {
+            double u, v, m, chi, rho;
+            qfix(M, pt.Q(I_H, i, j), pt.Q(I_HU, i, j), pt.Q(I_HV, i, j), pt.Q(I_HM, i, j),
+                 pt.Q(I_PB, i, j), pt.Q(I_HCHI, i, j), u, v, m, chi, rho, gz);
+            pt.Q(I_BDIF, i, j) = fmax2(pt.Q(I_BDIF, i, j), 0.0);
+        }
+    }
+    for (int j = 1 - MBC; j <= my + MBC; ++j) {
+        for (int i = 1 - MBC; i <= mx + MBC; ++i) {
+            if (pt.Q(1, i, j) > 0.0) {
+                double s = std::sqrt((sq(pt.Q(2, i, j)) + sq(pt.Q(3, i, j)))) / pt.Q(1, i, j);
+                if (s > P.speed_limit) {
+                    double sratio = P.speed_limit / s;
+                    pt.Q(2, i, j) = pt.Q(2, i, j) * sratio;
+                    pt.Q(3, i, j) = pt.Q(3, i, j) * sratio;
+                }
+            }
+        }
+    }
+    calc_taudir(M, pt, dx, dy);
+}
+
+// ---------------------------------------------------------------------------
+// riemannsolvers_dclaw.f:526-637
+void riemanntype(double hL, double hR, double uL, double uR, double& hm, double& s1m, double& s2m,
+                 bool& rare1, bool& rare2, int maxiter, double drytol, double g) {
+    double h_min = fmin2(hR, hL);
+    double h_max = fmax2(hR, hL);
+    double delu = uR - uL;
+    double um, u1m, u2m, h0, F0, slope, dfdh, gL, gR;
+    (void)um;
+    if (h_min <= drytol) {
+        hm = 0.0;
+        um = 0.0;
+        s1m = uR + uL - 2.0 * std::sqrt(g * hR) + 2.0 * std::sqrt(g * hL);
+        s2m = uR + uL - 2.0 * std::sqrt(g * hR) + 2.0 * std::sqrt(g * hL);
+        if (hL <= 0.0) { rare2 = true; rare1 = false; }
+        else { rare1 = true; rare2 = false; }
+    } else {
+        double F_min = delu + 2.0 * (std::sqrt(g * h_min) - std::sqrt(g * h_max));
+        double F_max = delu + (h_max - h_min) * (std::sqrt(.5 * g * (h_max + h_min) / (h_max * h_min)));
+        if (F_min > 0.0) {
+            hm = (1.0 / (16.0 * g)) * sq(fmax2(0.0, -delu + 2.0 * (std::sqrt(g * hL) + std::sqrt(g * hR))));
+            um = fsign(1.0, hm) * (uL + 2.0 * (std::sqrt(g * hL) - std::sqrt(g * hm)));
+            s1m = uL + 2.0 * std::sqrt(g * hL) - 3.0 * std::sqrt(g * hm);
+            s2m = uR - 2.0 * std::sqrt(g * hR) + 3.0 * std::sqrt(g * hm);
+            rare1 = true;
+            rare2 = true;
+        } else if (F_max <= 0.0) {
+            h0 = h_max;
+            for (int iter = 1; iter <= maxiter; ++iter) {
+                gL = std::sqrt(.5 * g * (1 / h0 + 1 / hL));
+                gR = std::sqrt(.5 * g * (1 / h0 + 1 / hR));
+                F0 = delu + (h0 - hL) * gL + (h0 - hR) * gR;
+                dfdh = gL - g * (h0 - hL) / (4.0 * (sq(h0)) * gL) + gR - g * (h0 - hR) / (4.0 * (sq(h0)) * gR);
+                slope = 2.0 * std::sqrt(h0) * dfdh;
+                h0 = sq(std::sqrt(h0) - F0 / slope);
+            }
+            hm = h0;
+            u1m = uL - (hm - hL) * std::sqrt((.5 * g) * (1 / hm + 1 / hL));
+            u2m = uR + (hm - hR) * std::sqrt((.5 * g) * (1 / hm + 1 / hR));
+            um = .5 * (u1m + u2m);
+            s1m = u1m - std::sqrt(g * hm);
+            s2m = u2m + std::sqrt(g * hm);
+            rare1 = false;
+            rare2 = false;
+        } else {
+            h0 = h_min;
+            for (int iter = 1; iter <= maxiter; ++iter) {
+                F0 = delu + 2.0 * (std::sqrt(g * h0) - std::sqrt(g * h_max))
+                     + (h0 - h_min) * std::sqrt(.5 * g * (1.0 / h0 + 1.0 / h_min));
+                slope = (F_max - F0) / (h_max - h_min);
+                h0 = h0 - F0 / slope;
+            }
+            hm = h0;
+            if (hL > hR) {
+                um = uL + 2.0 * std::sqrt(g * hL) - 2.0 * std::sqrt(g * hm);
+                s1m = uL + 2.0 * std::sqrt(g * hL) - 3.0 * std::sqrt(g * hm);
+                s2m = uL + 2.0 * std::sqrt(g * hL) - std::sqrt(g * hm);
+                rare1 = true;
+                rare2 = false;
+            } else {
+                s2m = uR - 2.0 * std::sqrt(g * hR) + 3.0 * std::sqrt(g * hm);
+                s1m = uR - 2.0 * std::sqrt(g * hR) + std::sqrt(g * hm);
+                um = uR - 2.0 * std::sqrt(g * hR) + 2.0 * std::sqrt(g * hm);
+                rare2 = true;
+                rare1 = false;
+            }
+        }
+    }
+}
+
+// riemannsolvers_dclaw.f:3-521. fw[m][mw] holds fw(m+1, mw+1).
+void riemann_dig2_aug_sswave_ez(Model& M, double hL, double hR, double huL, double huR,
+        double hvL, double hvR, double hmL, double hmR, double pL, double pR, double bL, double bR,
+        double uL, double uR, double vL, double vR, double mL, double mR, double thetaL, double thetaR,
+        double sw[3], double fw[6][3], bool wallprob, double taudirL, double taudirR,
+        double chiL, double chiR, double fsL, double fsR, uint32_t* br) {
+    const dclaw_params& P = M.p;
+    const double grav = P.grav;
+    const double kappa = M.kappa;
+    bool delta_huvm_revert = true;
+    double drytol = P.dry_tolerance;
+    double veltol2 = 0.0;
+    double criticaltol = fmax2(drytol * grav, 1e-6);
+    double criticaltol_2 = std::sqrt(criticaltol);
+
+    double gzL = grav * std::cos(thetaL);
+    double gzR = grav * std::cos(thetaR);
+    double theta = 0.5 * (thetaL + thetaR);
+    double gz = grav * std::cos(theta);
+    double alpha_seg = 1.0 - 0.0; // beta_seg = 0 (segregation off)
+
+    double rhoL, rhoR, tauL, tauR, kperm, alphainv, m_eq, tanpsi, h, v, mbar;
+    (void)v; (void)mbar;
+    if (hL >= drytol && hR >= drytol) {
+        setvars(M, hL, uL, vL, mL, pL, chiL, gzL, rhoL, kperm, alphainv, m_eq, tanpsi, tauL);
+        setvars(M, hR, uR, vR, mR, pR, chiR, gzR, rhoR, kperm, alphainv, m_eq, tanpsi, tauR);
+        h = 0.5 * (hL + hR);
+        v = 0.5 * (vL + vR);
+        mbar = 0.5 * (mL + mR);
+    } else if (hL >= drytol) {
+        setvars(M, hL, uL, vL, mL, pL, chiL, gzL, rhoL, kperm, alphainv, m_eq, tanpsi, tauL);
+        setvars(M, hL, uL, vL, mL, pL, chiL, gzL, rhoR, kperm, alphainv, m_eq, tanpsi, tauR);
+        tauR = 0.5 * tauL;
+        h = 0.5 * hL;
+        v = vL;
+        mbar = mL;
+    } else {
+        setvars(M, hR, uR, vR, mR, pR, chiR, gzR, rhoL, kperm, alphainv, m_eq, tanpsi, tauL);
+        setvars(M, hR, uR, vR, mR, pR, chiR, gzR, rhoR, kperm, alphainv, m_eq, tanpsi, tauR);
+        tauL = 0.5 * tauR;
+        h = 0.5 * hR;
+        v = vR;
+        mbar = mR;
+    }
+    tauL = fsL * tauL;
+    tauR = fsR * tauR;
+    double rho = 0.5 * (rhoL + rhoR);
+    double tau = 0.5 * (tauL + tauR);
+    (void)tau;
+    double gamma = 0.0, gammaL = 0.0, gammaR = 0.0;
+    if (P.src2method == -1) {
+        gamma = P.rho_f / rho;
+        gammaL = P.rho_f / rhoL;
+        gammaR = P.rho_f / rhoR;
+    } else if (P.src2method >= 0 && P.src2method <= 2) {
+        gamma = 0.25 * (P.rho_f + 3.0 * rho) / rho;
+        gammaL = 0.25 * (P.rho_f + 3.0 * rhoL) / rhoL;
+        gammaR = 0.25 * (P.rho_f + 3.0 * rhoR) / rhoR;
+    }
+    double eps = kappa + (1.0 - kappa) * gamma;
+    double geps = gz * eps;
+
+    double sL = uL - std::sqrt(geps * hL);
+    double sR = uR + std::sqrt(geps * hR);
+    double uhat = (std::sqrt(hL) * uL + std::sqrt(hR) * uR) / (std::sqrt(hR) + std::sqrt(hL));
+    double chat = std::sqrt(geps * 0.5 * (hR + hL));
+    double sRoe1 = uhat - chat;
+    double sRoe2 = uhat + chat;
+    double sE1 = fmin2(sL, sRoe1);
+    double sE2 = fmax2(sR, sRoe2);
+    sw[0] = sE1;
+    sw[2] = sE2;
+    double u = uhat;
+
+    double hm, s1m, s2m;
+    bool rare1, rare2;
+    riemanntype(hL, hR, uL, uR, hm, s1m, s2m, rare1, rare2, 1, drytol, geps);
+    sw[0] = fmin2(sw[0], s2m);
+    sw[2] = fmax2(sw[2], s1m);
+    sw[1] = 0.5 * (sw[2] + sw[0]);
+
+    double hstarHLL = fmax2((huL - huR + sE2 * hR - sE1 * hL) / (sE2 - sE1), 0.0);
+    bool rarecorrector = false;
+    if (P.rarecorrectortest) {
+        double sdelta = sw[2] - sw[0];
+        double raremin = 0.5;
+        double raremax = 0.9;
+        if (rare1 && sE1 * s1m < 0.0) raremin = 0.2;
+        if (rare2 && sE2 * s2m < 0.0) raremin = 0.2;
+        if (rare1 || rare2) {
+            double rare1st = 3.0 * (std::sqrt(geps * hL) - std::sqrt(geps * hm));
+            double rare2st = 3.0 * (std::sqrt(geps * hR) - std::sqrt(geps * hm));
+            if (fmax2(rare1st, rare2st) > raremin * sdelta && fmax2(rare1st, rare2st) < raremax * sdelta) {
+                rarecorrector = true;
+                if (rare1st > rare2st) sw[1] = s1m;
+                else if (rare2st > rare1st) sw[1] = s2m;
+                else sw[1] = 0.5 * (s1m + s2m);
+            }
+        }
+        if (hstarHLL < fmin2(hL, hR) / 5.0) rarecorrector = false;
+    }
+
+    double delb = (bR - bL);
+    double hbar = 0.5 * (hL + hR);
+    double s1s2bar = 0.25 * sq(uL + uR) - gz * hbar;
+    double s1s2tilde = fmax2(0.0, uL * uR) - gz * hbar;
+
+    bool sonic = false;
+    if (std::fabs(s1s2bar) <= criticaltol) sonic = true;
+    else if (s1s2bar * s1s2tilde <= sq(criticaltol)) sonic = true;
+    else if (s1s2bar * sE1 * sE2 <= sq(criticaltol)) sonic = true;
+    else if (fmin2(std::fabs(sE1), std::fabs(sE2)) < criticaltol_2) sonic = true;
+    else if (sE1 < criticaltol_2 && s1m > -criticaltol_2) sonic = true;
+    else if (sE2 > -criticaltol_2 && s2m < criticaltol_2) sonic = true;
+    else if ((uL + std::sqrt(geps * hL)) * (uR + std::sqrt(geps * hR)) < 0.0) sonic = true;
+    else if ((uL - std::sqrt(geps * hL)) * (uR - std::sqrt(geps * hR)) < 0.0) sonic = true;
+    if (sonic && br) *br |= BR_SONIC;
+
+    double source2dx;
+    if (sonic) source2dx = -gz * hbar * delb;
+    else source2dx = -gz * hbar * delb * s1s2tilde / s1s2bar;
+    source2dx = fmin2(source2dx, gz * fmax2(-hL * delb, -hR * delb));
+    source2dx = fmax2(source2dx, gz * fmin2(-hL * delb, -hR * delb));
+    if (std::fabs(u) <= veltol2) source2dx = -hbar * gz * delb;
+
+    double deldelh;
+    if (sonic) deldelh = -delb;
+    else deldelh = delb * gz * hbar / s1s2bar;
+    if (sE1 < -criticaltol && sE2 > criticaltol) {
+        deldelh = fmin2(deldelh, hstarHLL * (sE2 - sE1) / sE2);
+        deldelh = fmax2(deldelh, hstarHLL * (sE2 - sE1) / sE1);
+    } else if (sE1 >= criticaltol) {
+        deldelh = fmin2(deldelh, hstarHLL * (sE2 - sE1) / sE1);
+        deldelh = fmax2(deldelh, -hL);
+    } else if (sE2 <= -criticaltol) {
+        deldelh = fmin2(deldelh, hR);
+        deldelh = fmax2(deldelh, hstarHLL * (sE2 - sE1) / sE2);
+    }
+
+    double R[3][3];  // R(0:2, 1:3) -> R[row][mw-1]
+    R[0][1] = 0.0; R[1][1] = 0.0; R[2][1] = 1.0;
+    int cwavetype = 1;
+    R[0][0] = 1.0; R[1][0] = sw[0]; R[2][0] = sq(sw[0]);
+    R[0][2] = 1.0; R[1][2] = sw[2]; R[2][2] = sq(sw[2]);
+    if (rarecorrector) {
+        R[0][1] = 1.0; R[1][1] = sw[1]; R[2][1] = sq(sw[1]);
+        cwavetype = 2;
+    }
+
+    double del[5];
+    del[0] = hR - hL - deldelh;
+    del[1] = huR - huL;
+    del[2] = hR * sq(uR) + 0.5 * kappa * gz * sq(hR) - (hL * sq(uL) + 0.5 * kappa * gz * sq(hL));
+    del[2] = del[2] + (1.0 - kappa) * h * (pR - pL) / rho;
+    del[3] = pR - pL - gamma * rho * gz * deldelh;
+    del[4] = -gamma * rho * gz * u * (hR - hL) + gamma * rho * gz * del[1] + u * (pR - pL);
+
+    double vnorm = std::sqrt(sq(uR) + sq(uL) + sq(vR) + sq(vL));
+    bool is_static = false;
+    double tausource;
+    if (vnorm > 0.0) {
+        tausource = 0.0;
+    } else if (0.5 * std::fabs(taudirR * tauR / rhoR + tauL * taudirR / rhoL) > std::fabs(del[2] - source2dx)) {
+        tausource = del[2] - source2dx;
+        del[1] = 0.0;
+        del[0] = 0.0;
+        del[3] = 0.0;
+        del[4] = 0.0;
+        is_static = true;
+    } else {
+        tausource = 0.5 * ((taudirR * tauR / rhoR) + (tauL * taudirR / rhoL));
+        tausource = fsign(tausource, del[2] - source2dx);
+    }
+    (void)taudirL;
+    if (is_static && br) *br |= BR_STATIC;
+    if (wallprob) tausource = 0.0;
+    del[2] = del[2] - source2dx - tausource;
+
+    double theta1, theta2, theta3;
+    if (sw[0] >= 0.0) { theta1 = thetaR; theta2 = thetaR; theta3 = thetaR; }
+    else if (sw[2] <= 0.0) { theta1 = thetaL; theta2 = thetaL; theta3 = thetaL; }
+    else if (sw[1] >= 0.0) { theta1 = thetaL; theta2 = thetaR; theta3 = thetaR; }
+    else { theta1 = thetaL; theta2 = thetaL; theta3 = thetaR; }
+    (void)theta2;
+
+    double a = sw[0], b = sw[1], c = sw[2];
+    double beta[3];
+    if (cwavetype == 1) {
+        beta[0] = (c * del[0] - del[1]) / (c - a);
+        beta[1] = a * c * del[0] - (a + c) * del[1] + del[2];
+        beta[2] = (del[1] - a * del[0]) / (c - a);
+    } else {
+        beta[0] = (b * c * del[0] - (b + c) * del[1] + del[2]) / (sq(a) - a * b - a * c + b * c);
+        beta[1] = (-a * c * del[0] + (a + c) * del[1] - del[2]) / (a * b - a * c - sq(b) + b * c);
+        beta[2] = (a * b * del[0] - (a + b) * del[1] + del[2]) / (a * b - a * c - b * c + sq(c));
+    }
+
+    for (int mw = 0; mw < 3; ++mw)
+        for (int m = 0; m < 2; ++m) fw[m][mw] = beta[mw] * R[m + 1][mw];
+
+    fw[3][0] = fw[0][0] * mL;
+    fw[3][2] = fw[0][2] * mR;
+    fw[3][1] = hmR * uR - hmL * uL - fw[3][0] - fw[3][2];
+
+    fw[2][0] = fw[0][0] * vL;
+    fw[2][2] = fw[0][2] * vR;
+    fw[2][1] = hvR * uR - hvL * uL - fw[2][0] - fw[2][2];
+
+    fw[4][0] = fw[0][0] * gammaL * rhoL * grav * std::cos(theta1);
+    fw[4][2] = fw[0][2] * gammaR * rhoR * grav * std::cos(theta3);
+    fw[4][1] = del[4] - fw[4][2] - fw[4][0];
+
+    double seg_L = chiL * hL * uL * (1.0 + (1.0 - alpha_seg) * (1.0 - chiL));
+    double seg_R = chiR * hR * uR * (1.0 + (1.0 - alpha_seg) * (1.0 - chiR));
+    fw[5][0] = fw[0][0] * chiL * (1.0 + (1.0 - alpha_seg) * (1.0 - chiL));
+    fw[5][2] = fw[0][2] * chiR * (1.0 + (1.0 - alpha_seg) * (1.0 - chiR));
+    fw[5][1] = seg_R - seg_L - fw[5][0] - fw[5][2];
+
+    if (delta_huvm_revert) {
+        double hustar_interface = huL + fw[0][0];
+        if (!is_static) {
+            double u_interface = hustar_interface / hstarHLL;
+            del[4] = -gamma * rho * gz * u_interface * (hR - hL) + gamma * rho * gz * del[1]
+                     + u_interface * (pR - pL);
+            fw[4][1] = del[4] - fw[4][2] - fw[4][0];
+        }
+        if (hustar_interface <= 0.0) {
+            if (br) *br |= BR_REVERT_L;
+            fw[2][0] = fw[2][0] + fw[2][1];
+            fw[3][0] = fw[3][0] + fw[3][1];
+            fw[4][0] = fw[4][0] + fw[4][1];
+            fw[5][0] = fw[5][0] + fw[5][1];
+        } else {
+            fw[2][2] = fw[2][2] + fw[2][1];
+            fw[3][2] = fw[3][2] + fw[3][1];
+            fw[4][2] = fw[4][2] + fw[4][1];
+            fw[5][2] = fw[5][2] + fw[5][1];
+        }
+        fw[2][1] = 0.0;
+        fw[3][1] = 0.0;
+        fw[4][1] = 0.0;
+        fw[5][1] = 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 1-D slice storage with Fortran bounds 1-mbc:mx+mbc
+struct Slice {
+    int n;  // number of cells in the slice interior (mx or my)
+    std::vector<double> q1d;     // (meqn, 1-mbc:n+mbc)
+    std::vector<double> aux1, aux2, aux3;  // (maux, ...)
+    std::vector<double> dtdx1d;
+    std::vector<double> fwave;   // (meqn, mwaves, ...)
+    std::vector<double> s;       // (mwaves, ...)
+    std::vector<double> amdq, apdq, bmasdq, bpasdq, cqxx;
+    std::vector<double> faddm, faddp, gaddm, gaddp;  // gadd: (meqn, ..., 2)
+    std::vector<uint32_t> br;    // branch bits per interface 1..n+1 (index i-1)
+    explicit Slice(int n_) : n(n_) {
+        size_t L = (size_t)n_ + 2 * MBC;
+        q1d.assign(MEQN * L, 0.0);
+        aux1.assign(MAUX * L, 0.0); aux2.assign(MAUX * L, 0.0); aux3.assign(MAUX * L, 0.0);
+        dtdx1d.assign(L, 0.0);
+        fwave.assign((size_t)MEQN * MWAVES * L, 0.0);
+        s.assign(MWAVES * L, 0.0);
+        amdq.assign(MEQN * L, 0.0); apdq.assign(MEQN * L, 0.0);
+        bmasdq.assign(MEQN * L, 0.0); bpasdq.assign(MEQN * L, 0.0);
+        cqxx.assign(MEQN * L, 0.0);
+        faddm.assign(MEQN * L, 0.0); faddp.assign(MEQN * L, 0.0);
+        gaddm.assign(MEQN * L * 2, 0.0); gaddp.assign(MEQN * L * 2, 0.0);
+        br.assign((size_t)n_ + 1, 0u);
+    }
+    size_t L() const { return (size_t)n + 2 * MBC; }
+    size_t ix(int i) const { return (size_t)(i + MBC - 1); }
+    double& Q(int m, int i) { return q1d[ix(i) * MEQN + (m - 1)]; }
+    double& A1(int m, int i) { return aux1[ix(i) * MAUX + (m - 1)]; }
+    double& A2(int m, int i) { return aux2[ix(i) * MAUX + (m - 1)]; }
+    double& A3(int m, int i) { return aux3[ix(i) * MAUX + (m - 1)]; }
+    double& DT(int i) { return dtdx1d[ix(i)]; }
+    double& FW(int m, int mw, int i) { return fwave[(ix(i) * MWAVES + (mw - 1)) * MEQN + (m - 1)]; }
+    double& S(int mw, int i) { return s[ix(i) * MWAVES + (mw - 1)]; }
+    double& AM(int m, int i) { return amdq[ix(i) * MEQN + (m - 1)]; }
+    double& AP(int m, int i) { return apdq[ix(i) * MEQN + (m - 1)]; }
+    double& BM(int m, int i) { return bmasdq[ix(i) * MEQN + (m - 1)]; }
+    double& BP(int m, int i) { return bpasdq[ix(i) * MEQN + (m - 1)]; }
+    double& CQ(int m, int i) { return cqxx[ix(i) * MEQN + (m - 1)]; }
+    double& FM(int m, int i) { return faddm[ix(i) * MEQN + (m - 1)]; }
+    double& FP(int m, int i) { return faddp[ix(i) * MEQN + (m - 1)]; }
+    double& GM(int m, int i, int side) { return gaddm[((size_t)(side - 1) * L() + ix(i)) * MEQN + (m - 1)]; }
+    double& GP(int m, int i, int side) { return gaddp[((size_t)(side - 1) * L() + ix(i)) * MEQN + (m - 1)]; }
+    uint32_t* BR(int i) { return (i >= 1 && i <= n + 1) ? &br[(size_t)(i - 1)] : nullptr; }
+};
+
+// rpn2_dclaw.f:24-392 (ql = qr = q1d, auxl = auxr = aux2; q1d is mutated by qfix)
+void rpn2(Model& M, int ixy, Slice& sl) {
+    const dclaw_params& P = M.p;
+    const int mx = sl.n;
+    double gmod = P.grav;
+    int waves = 3;
+    double drytol = P.dry_tolerance;
+    for (int i = 2 - MBC; i <= mx + MBC; ++i) {
+        for (int mw = 1; mw <= MWAVES; ++mw) {
+            sl.S(mw, i) = 0.0;
+            for (int m = 1; m <= MEQN; ++m) sl.FW(m, mw, i) = 0.0;
+        }
+        double sw[3] = {0.0, 0.0, 0.0};
+        double fw[6][3];
+        for (int m = 0; m < 6; ++m) for (int mw = 0; mw < 3; ++mw) fw[m][mw] = 0.0;
+        uint32_t* br = sl.BR(i);
+
+        if (sl.Q(I_H, i - 1) <= drytol && sl.Q(I_H, i) <= drytol) {
+            if (br) *br |= BR_DRY;
+            continue;
+        }
+        int mhu, nhv;
+        double taudirR, taudirL;
+        if (ixy == 1) {
+            mhu = I_HU; nhv = I_HV;
+            taudirR = sl.A2(I_TAUDIR_X, i);
+            taudirL = sl.A2(I_TAUDIR_X, i - 1);
+        } else {
+            mhu = I_HV; nhv = I_HU;
+            taudirR = sl.A2(I_TAUDIR_Y, i);
+            taudirL = sl.A2(I_TAUDIR_Y, i - 1);
+        }
+        double fsL = sl.A2(I_FSPHI, i - 1);
+        double fsR = sl.A2(I_FSPHI, i);
+        double thetaL = 0.0, thetaR = 0.0;
+        double gzL = P.grav, gzR = P.grav;
+
+        double uR, vR, mR, chiR, rhoR, uL, vL, mL, chiL, rhoL;
+        qfix(M, sl.Q(I_H, i), sl.Q(mhu, i), sl.Q(nhv, i), sl.Q(I_HM, i), sl.Q(I_PB, i), sl.Q(I_HCHI, i),
+             uR, vR, mR, chiR, rhoR, gzR);
+        qfix(M, sl.Q(I_H, i - 1), sl.Q(mhu, i - 1), sl.Q(nhv, i - 1), sl.Q(I_HM, i - 1), sl.Q(I_PB, i - 1),
+             sl.Q(I_HCHI, i - 1), uL, vL, mL, chiL, rhoL, gzL);
+
+        double hL = sl.Q(I_H, i - 1), hR = sl.Q(I_H, i);
+        double huL = sl.Q(mhu, i - 1), huR = sl.Q(mhu, i);
+        double hvL = sl.Q(nhv, i - 1), hvR = sl.Q(nhv, i);
+        double hmL = sl.Q(I_HM, i - 1), hmR = sl.Q(I_HM, i);
+        double pL = sl.Q(I_PB, i - 1), pR = sl.Q(I_PB, i);
+        double bL = sl.A2(1, i - 1) - sl.Q(I_BDIF, i - 1);
+        double bR = sl.A2(1, i) - sl.Q(I_BDIF, i);
+        double chiHL = sl.Q(I_HCHI, i - 1), chiHR = sl.Q(I_HCHI, i);
+        (void)chiHL; (void)chiHR;
+
+        double wall[3] = {1.0, 1.0, 1.0};
+        bool wallprob = false;
+        double hstar, s1m, s2m, hstartest;
+        bool rare1, rare2;
+        if (hR <= drytol) {
+            hR = 0.0;
+            pR = 0.0;
+            mR = mL;
+            chiR = chiL;
+            riemanntype(hL, hL, uL, -uL, hstar, s1m, s2m, rare1, rare2, 1, drytol, gmod);
+            hstartest = fmax2(hL, hstar);
+            if (hstartest + bL < bR) {
+                wall[1] = 0.0;
+                wall[2] = 0.0;
+                wallprob = true;
+                hR = hL; huR = -huL; hvR = hvL; hmR = hmL; bR = bL;
+                uR = -uL; vR = vL; mR = mL; pR = pL; chiHR = chiHL; chiR = chiL;
+            }
+        } else if (hL <= drytol) {
+            hL = 0.0;
+            pL = 0.0;
+            mL = mR;
+            chiL = chiR;
+            riemanntype(hR, hR, -uR, uR, hstar, s1m, s2m, rare1, rare2, 1, drytol, gmod);
+            hstartest = fmax2(hR, hstar);
+            if (hstartest + bR < bL) {
+                wall[0] = 0.0;
+                wall[1] = 0.0;
+                wallprob = true;
+                hL = hR; huL = -huR; hvL = hvR; hmL = hmR; mL = mR; bL = bR;
+                uL = -uR; vL = vR; pL = pR; chiHL = chiHR; chiL = chiR;
+            }
+        }
+        if (wallprob && br) *br |= BR_WALL;
+
+        riemann_dig2_aug_sswave_ez(M, hL, hR, huL, huR, hvL, hvR, hmL, hmR, pL, pR, bL, bR, uL, uR, vL,
+                                   vR, mL, mR, thetaL, thetaR, sw, fw, wallprob, taudirL, taudirR, chiL,
+                                   chiR, fsL, fsR, br);
+        for (int mw = 0; mw < 3; ++mw) {
+            sw[mw] = sw[mw] * wall[mw];
+            for (int m = 0; m < 6; ++m) fw[m][mw] = fw[m][mw] * wall[mw];
+        }
+        sl.S(1, i) = sw[0];
+        sl.S(2, i) = sw[1];
+        sl.S(3, i) = sw[1];
+        sl.S(4, i) = sw[1];
+        sl.S(5, i) = sw[2];
+
+        sl.FW(I_H, 1, i) = fw[0][0];
+        sl.FW(mhu, 1, i) = fw[1][0];
+        sl.FW(nhv, 1, i) = fw[2][0];
+        sl.FW(I_HM, 1, i) = fw[3][0];
+        sl.FW(I_PB, 1, i) = fw[4][0];
+        sl.FW(I_HCHI, 1, i) = fw[5][0];
+
+        sl.FW(I_H, 5, i) = fw[0][2];
+        sl.FW(mhu, 5, i) = fw[1][2];
+        sl.FW(nhv, 5, i) = fw[2][2];
+        sl.FW(I_HM, 5, i) = fw[3][2];
+        sl.FW(I_PB, 5, i) = fw[4][2];
+        sl.FW(I_HCHI, 5, i) = fw[5][2];
+
+        sl.FW(I_H, 2, i) = fw[0][1];
+        sl.FW(mhu, 2, i) = fw[1][1];
+        sl.FW(nhv, 2, i) = fw[2][1];
+        sl.FW(I_HM, 2, i) = 0.0;
+        sl.FW(I_PB, 2, i) = 0.0;
+        sl.FW(I_HCHI, 2, i) = fw[5][1];
+
+        sl.FW(I_H, 3, i) = 0.0;
+        sl.FW(mhu, 3, i) = 0.0;
+        sl.FW(nhv, 3, i) = 0.0;
+        sl.FW(I_HM, 3, i) = fw[3][1];
+        sl.FW(I_PB, 3, i) = 0.0;
+        sl.FW(I_HCHI, 3, i) = 0.0;
+
+        sl.FW(I_H, 4, i) = 0.0;
+        sl.FW(mhu, 4, i) = 0.0;
+        sl.FW(nhv, 4, i) = 0.0;
+        sl.FW(I_HM, 4, i) = 0.0;
+        sl.FW(I_PB, 4, i) = fw[4][1];
+        sl.FW(I_HCHI, 4, i) = 0.0;
+    }
+    // fluctuations (rpn2_dclaw.f:347-379); mcapa = 0
+    std::fill(sl.amdq.begin(), sl.amdq.end(), 0.0);
+    std::fill(sl.apdq.begin(), sl.apdq.end(), 0.0);
+    for (int i = 2 - MBC; i <= mx + MBC; ++i) {
+        for (int mw = 1; mw <= MWAVES; ++mw) {
+            if (sl.S(mw, i) < 0.0) {
+                for (int m = 1; m <= MEQN; ++m) sl.AM(m, i) = sl.AM(m, i) + sl.FW(m, mw, i);
+            } else if (sl.S(mw, i) > 0.0) {
+                for (int m = 1; m <= MEQN; ++m) sl.AP(m, i) = sl.AP(m, i) + sl.FW(m, mw, i);
+            }
+        }
+    }
+}
+
+// Wave limiter (Clawpack inlinelimiter, restated from LeVeque 2002 sec. 6.9, 6.12):
+// for each wave family, theta = <W_upwind, W_i> / <W_i, W_i> with the upwind
+// neighbour chosen by the sign of the speed (s > 0: left, else right), computed
+// from the unlimited waves; W_i <- phi(theta) W_i at interfaces 1..mx+1.
+void limiter(const Model& M, Slice& sl) {
+    const int mx = sl.n;
+    const int mth = M.p.limiter;
+    if (mth == 0) return;
+    for (int mw = 1; mw <= MWAVES; ++mw) {
+        double dotr = 0.0;
+        for (int i = 0; i <= mx + 1; ++i) {
+            double wnorm2 = 0.0;
+            double dotl = dotr;
+            dotr = 0.0;
+            for (int m = 1; m <= MEQN; ++m) {
+                wnorm2 = wnorm2 + sq(sl.FW(m, mw, i));
+                dotr = dotr + sl.FW(m, mw, i) * sl.FW(m, mw, i + 1);
+            }
+            if (i == 0) continue;
+            if (wnorm2 == 0.0) continue;
+            uint32_t* br = sl.BR(i);
+            double r;
+            if (sl.S(mw, i) > 0.0) {
+                r = dotl / wnorm2;
+                if (br) *br |= br_up(mw);
+            } else {
+                r = dotr / wnorm2;
+            }
+            double wlimitr;
+            uint32_t code;
+            switch (mth) {
+                case 1: wlimitr = fmax2(0.0, fmin2(1.0, r)); code = wlimitr == 0.0 ? 1u : 2u; break;
+                case 2: wlimitr = fmax2(fmax2(0.0, fmin2(1.0, 2.0 * r)), fmin2(2.0, r));
+                        code = wlimitr == 0.0 ? 1u : 2u; break;
+                case 3: wlimitr = (r + std::fabs(r)) / (1.0 + std::fabs(r)); code = wlimitr == 0.0 ? 1u : 2u; break;
+                case 4: {
+                    double c = (1.0 + r) / 2.0;
+                    wlimitr = fmax2(0.0, fmin2(fmin2(c, 2.0), 2.0 * r));
+                    code = wlimitr == 0.0 ? 1u : (wlimitr == c ? 2u : (wlimitr == 2.0 ? 3u : 4u));
+                    break;
+                }
+                default: wlimitr = r; code = 2u; break;
+            }
+            if (br) *br |= br_lim(mw, code);
+            for (int m = 1; m <= MEQN; ++m) sl.FW(m, mw, i) = wlimitr * sl.FW(m, mw, i);
+        }
+    }
+}
+
+// rpt2_dclaw.f:16-266 (Cartesian, bed_normal = 0)
+void rpt2(const Model& M, int ixy, int imp, Slice& sl, std::vector<double>& asdq) {
+    const dclaw_params& P = M.p;
+    const int mx = sl.n;
+    int mu, mv;
+    if (ixy == 1) { mu = I_HU; mv = I_HV; } else { mu = I_HV; mv = I_HU; }
+    std::fill(sl.bmasdq.begin(), sl.bmasdq.end(), 0.0);
+    std::fill(sl.bpasdq.begin(), sl.bpasdq.end(), 0.0);
+    double g = P.grav;
+    auto AS = [&](int m, int i) -> double { return asdq[sl.ix(i) * MEQN + (m - 1)]; };
+    for (int i = 2 - MBC; i <= mx + MBC; ++i) {
+        double h;
+        if (imp == 1) h = sl.Q(I_H, i - 1);
+        else h = sl.Q(I_H, i);
+        if (h <= P.dry_tolerance) continue;
+        double u, v, m, p, chi, eta, topo1, topo3;
+        if (imp == 1) {
+            u = sl.Q(mu, i - 1) / h;
+            v = sl.Q(mv, i - 1) / h;
+            m = sl.Q(I_HM, i - 1) / h;
+            p = sl.Q(I_PB, i - 1);
+            chi = sl.Q(I_HCHI, i - 1) / h;
+            eta = h + sl.A2(1, i - 1) - sl.Q(I_BDIF, i - 1);
+            topo1 = sl.A1(1, i - 1);
+            topo3 = sl.A3(1, i - 1);
+        } else {
+            u = sl.Q(mu, i) / h;
+            v = sl.Q(mv, i) / h;
+            m = sl.Q(I_HM, i) / h;
+            p = sl.Q(I_PB, i);
+            chi = sl.Q(I_HCHI, i) / h;
+            eta = h + sl.A2(1, i) - sl.Q(I_BDIF, i);
+            topo1 = sl.A1(1, i);
+            topo3 = sl.A3(1, i);
+        }
+        (void)p;
+        double rho = m * P.rho_s + (1.0 - m) * P.rho_f;
+        double gamma = 0.0;
+        if (P.src2method == -1) gamma = P.rho_f / rho;
+        else if (P.src2method >= 0 && P.src2method <= 2) gamma = 0.25 * (P.rho_f + 3.0 * rho) / rho;
+        if (eta < fmin2(topo1, topo3)) continue;
+        uint32_t* br = sl.BR(i);
+        if (br) *br |= (imp == 1 ? BR_RPT1 : BR_RPT2);
+        double dxdcp = 1.0, dxdcm = 1.0;
+        double s[3];
+        s[0] = v - std::sqrt(g * h);
+        s[1] = v;
+        s[2] = v + std::sqrt(g * h);
+        double delf1 = AS(I_H, i), delf2 = AS(mu, i), delf3 = AS(mv, i), delf4 = AS(I_HM, i),
+               delf5 = AS(I_PB, i), delf6 = AS(I_HCHI, i);
+        (void)delf4; (void)delf5; (void)delf6;
+        double beta[3];
+        beta[0] = (s[2] * delf1 - delf3) / (s[2] - s[0]);
+        beta[1] = -u * delf1 + delf2;
+        beta[2] = (delf3 - s[0] * delf1) / (s[2] - s[0]);
+        double r[6][3];
+        r[0][0] = 1.0; r[1][0] = u; r[2][0] = s[0]; r[3][0] = m; r[4][0] = gamma * rho * g; r[5][0] = chi;
+        r[0][2] = 1.0; r[1][2] = u; r[2][2] = s[2]; r[3][2] = m; r[4][2] = gamma * rho * g; r[5][2] = chi;
+        r[0][1] = 0.0; r[1][1] = 1.0; r[2][1] = 0.0; r[3][1] = 0.0; r[4][1] = 0.0; r[5][1] = 0.0;
+        const int comp[6] = {I_H, mu, mv, I_HM, I_PB, I_HCHI};
+        for (int mw = 0; mw < 3; ++mw) {
+            if ((s[mw] < 0.0) && (eta >= topo1)) {
+                for (int k = 0; k < 6; ++k)
+                    sl.BM(comp[k], i) = sl.BM(comp[k], i) + dxdcm * s[mw] * beta[mw] * r[k][mw];
+            } else if ((s[mw] > 0.0) && (eta >= topo3)) {
+                for (int k = 0; k < 6; ++k)
+                    sl.BP(comp[k], i) = sl.BP(comp[k], i) + dxdcp * s[mw] * beta[mw] * r[k][mw];
+            }
+        }
+    }
+}
+
+// flux2fw.f:8-286 (Cartesian, relimit = .false.)
+void flux2(Model& M, int ixy, Slice& sl, double& cfl1d) {
+    const dclaw_params& P = M.p;
+    const int mx = sl.n;
+    const int method2 = P.order, method3 = P.transverse_waves;
+    std::fill(sl.faddm.begin(), sl.faddm.end(), 0.0);
+    std::fill(sl.faddp.begin(), sl.faddp.end(), 0.0);
+    std::fill(sl.gaddm.begin(), sl.gaddm.end(), 0.0);
+    std::fill(sl.gaddp.begin(), sl.gaddp.end(), 0.0);
+    rpn2(M, ixy, sl);
+    for (int i = 1 - MBC + 1; i <= mx + MBC - 1; ++i) {
+        for (int m = 1; m <= MEQN; ++m) {
+            sl.FP(m, i) = sl.FP(m, i) - sl.AP(m, i);
+            sl.FM(m, i) = sl.FM(m, i) + sl.AM(m, i);
+        }
+    }
+    cfl1d = 0.0;
+    for (int mw = 1; mw <= MWAVES; ++mw)
+        for (int i = 1; i <= mx + 1; ++i)
+            cfl1d = fmax2(fmax2(cfl1d, sl.DT(i) * sl.S(mw, i)), -sl.DT(i - 1) * sl.S(mw, i));
+    if (method2 != 1) {
+        limiter(M, sl);
+        for (int i = 1; i <= mx + 1; ++i) {
+            sl.DT(i - 1) = 0.5 * (sl.DT(i - 1) + sl.DT(i));
+            double hleft2 = sl.Q(1, i - 2), hleft = sl.Q(1, i - 1), hright = sl.Q(1, i), hright2 = sl.Q(1, i + 1);
+            bool wet4 = hleft * hright * hleft2 * hright2 > 0.0;
+            if (wet4) { uint32_t* br = sl.BR(i); if (br) *br |= BR_WET4; }
+            for (int m = 1; m <= MEQN; ++m) {
+                sl.CQ(m, i) = 0.0;
+                if (wet4) {
+                    for (int mw = 1; mw <= MWAVES; ++mw)
+                        sl.CQ(m, i) = sl.CQ(m, i) + fsign(1.0, sl.S(mw, i))
+                                      * (1.0 - std::fabs(sl.S(mw, i)) * sl.DT(i - 1)) * sl.FW(m, mw, i);
+                }
+                sl.FM(m, i) = sl.FM(m, i) + 0.5 * sl.CQ(m, i);
+                sl.FP(m, i) = sl.FP(m, i) + 0.5 * sl.CQ(m, i);
+            }
+        }
+    }
+    if (method3 == 0) return;
+    if (method2 > 1 && method3 == 2) {
+        for (int i = 1; i <= mx + 1; ++i)
+            for (int m = 1; m <= MEQN; ++m) {
+                sl.AM(m, i) = sl.AM(m, i) + sl.CQ(m, i);
+                sl.AP(m, i) = sl.AP(m, i) - sl.CQ(m, i);
+            }
+    }
+    rpt2(M, ixy, 1, sl, sl.amdq);
+    for (int i = 1; i <= mx + 1; ++i)
+        for (int m = 1; m <= MEQN; ++m) {
+            double gupdate = 0.5 * sl.DT(i - 1) * sl.BM(m, i);
+            sl.GM(m, i - 1, 1) = sl.GM(m, i - 1, 1) - gupdate;
+            sl.GP(m, i - 1, 1) = sl.GP(m, i - 1, 1) - gupdate;
+            gupdate = 0.5 * sl.DT(i - 1) * sl.BP(m, i);
+            sl.GM(m, i - 1, 2) = sl.GM(m, i - 1, 2) - gupdate;
+            sl.GP(m, i - 1, 2) = sl.GP(m, i - 1, 2) - gupdate;
+        }
+    rpt2(M, ixy, 2, sl, sl.apdq);
+    for (int i = 1; i <= mx + 1; ++i)
+        for (int m = 1; m <= MEQN; ++m) {
+            double gupdate = 0.5 * sl.DT(i - 1) * sl.BM(m, i);
+            sl.GM(m, i, 1) = sl.GM(m, i, 1) - gupdate;
+            sl.GP(m, i, 1) = sl.GP(m, i, 1) - gupdate;
+            gupdate = 0.5 * sl.DT(i - 1) * sl.BP(m, i);
+            sl.GM(m, i, 2) = sl.GM(m, i, 2) - gupdate;
+            sl.GP(m, i, 2) = sl.GP(m, i, 2) - gupdate;
+        }
+}
+
+// Flux arrays fm, fp, gm, gp (meqn, 1-mbc:mx+mbc, 1-mbc:my+mbc)
+struct Fluxes {
+    int mx, my;
+    std::vector<double> fm, fp, gm, gp;
+    Fluxes(int mx_, int my_) : mx(mx_), my(my_) {
+        size_t n = (size_t)MEQN * (mx_ + 2 * MBC) * (my_ + 2 * MBC);
+        fm.assign(n, 0.0); fp.assign(n, 0.0); gm.assign(n, 0.0); gp.assign(n, 0.0);
+    }
+    size_t at(int m, int i, int j) const {
+        return ((size_t)(j + MBC - 1) * (mx + 2 * MBC) + (size_t)(i + MBC - 1)) * MEQN + (m - 1);
+    }
+};
+
+void load_xslice(Patch& pt, Slice& sl, int j, double dtdx) {
+    const int mx = pt.mx;
+    for (int i = 1 - MBC; i <= mx + MBC; ++i) {
+        for (int m = 1; m <= MEQN; ++m) sl.Q(m, i) = pt.Q(m, i, j);
+        sl.DT(i) = dtdx;
+        for (int m = 1; m <= MAUX; ++m) {
+            sl.A1(m, i) = pt.A(m, i, j - 1);
+            sl.A2(m, i) = pt.A(m, i, j);
+            sl.A3(m, i) = pt.A(m, i, j + 1);
+        }
+    }
+    std::fill(sl.br.begin(), sl.br.end(), 0u);
+}
+
+void load_yslice(Patch& pt, Slice& sl, int i, double dtdy) {
+    const int my = pt.my;
+    for (int j = 1 - MBC; j <= my + MBC; ++j) {
+        for (int m = 1; m <= MEQN; ++m) sl.Q(m, j) = pt.Q(m, i, j);
+        sl.DT(j) = dtdy;
+        for (int m = 1; m <= MAUX; ++m) {
+            sl.A1(m, j) = pt.A(m, i - 1, j);
+            sl.A2(m, j) = pt.A(m, i, j);
+            sl.A3(m, j) = pt.A(m, i + 1, j);
+        }
+    }
+    std::fill(sl.br.begin(), sl.br.end(), 0u);
+}
+
+// GeoClaw step2 (restated): x-sweeps over rows 0..my+1, then y-sweeps over
+// columns 0..mx+1, accumulating each slice's fadd/gadd into fm, fp, gm, gp in
+// sweep order. Literal serial version.
+double step2_serial(Model& M, Patch& pt, Fluxes& F, double dx, double dy, double dt,
+                    uint32_t* xlog, uint32_t* ylog) {
+    const int mx = pt.mx, my = pt.my;
+    double cflgrid = 0.0;
+    double dtdx = dt / dx, dtdy = dt / dy;
+    std::fill(F.fm.begin(), F.fm.end(), 0.0);
+    std::fill(F.fp.begin(), F.fp.end(), 0.0);
+    std::fill(F.gm.begin(), F.gm.end(), 0.0);
+    std::fill(F.gp.begin(), F.gp.end(), 0.0);
+    Slice sx(mx);
+    for (int j = 0; j <= my + 1; ++j) {
+        load_xslice(pt, sx, j, dtdx);
+        double cfl1d;
+        flux2(M, 1, sx, cfl1d);
+        cflgrid = fmax2(cflgrid, cfl1d);
+        for (int i = 1; i <= mx + 1; ++i)
+            for (int m = 1; m <= MEQN; ++m) {
+                F.fm[F.at(m, i, j)] += sx.FM(m, i);
+                F.fp[F.at(m, i, j)] += sx.FP(m, i);
+                F.gm[F.at(m, i, j)] += sx.GM(m, i, 1);
+                F.gp[F.at(m, i, j)] += sx.GP(m, i, 1);
+                F.gm[F.at(m, i, j + 1)] += sx.GM(m, i, 2);
+                F.gp[F.at(m, i, j + 1)] += sx.GP(m, i, 2);
+            }
+        if (xlog) std::memcpy(xlog + (size_t)j * (mx + 1), sx.br.data(), sizeof(uint32_t) * (mx + 1));
+    }
+    Slice sy(my);
+    for (int i = 0; i <= mx + 1; ++i) {
+        load_yslice(pt, sy, i, dtdy);
+        double cfl1d;
+        flux2(M, 2, sy, cfl1d);
+        cflgrid = fmax2(cflgrid, cfl1d);
+        for (int j = 1; j <= my + 1; ++j)
+            for (int m = 1; m <= MEQN; ++m) {
+                F.gm[F.at(m, i, j)] += sy.FM(m, j);
+                F.gp[F.at(m, i, j)] += sy.FP(m, j);
+                F.fm[F.at(m, i, j)] += sy.GM(m, j, 1);
+                F.fp[F.at(m, i, j)] += sy.GP(m, j, 1);
+                F.fm[F.at(m, i + 1, j)] += sy.GM(m, j, 2);
+                F.fp[F.at(m, i + 1, j)] += sy.GP(m, j, 2);
+            }
+        if (ylog) std::memcpy(ylog + (size_t)i * (my + 1), sy.br.data(), sizeof(uint32_t) * (my + 1));
+    }
+    return cflgrid;
+}
+
+// Same arithmetic, same per-element summation order, split into phases that
+// OpenMP can run concurrently: every sum keeps the operand order of the
+// serial sweep (x-sweep row j-1 before row j, y-sweep column i-1 before i).
+double step2_parallel(Model& M, Patch& pt, Fluxes& F, double dx, double dy, double dt,
+                      uint32_t* xlog, uint32_t* ylog) {
+    const int mx = pt.mx, my = pt.my;
+    double dtdx = dt / dx, dtdy = dt / dy;
+    const size_t LX = (size_t)mx + 2 * MBC, LY = (size_t)my + 2 * MBC;
+    // per-slice transverse increments, side 1 and side 2 (gaddm == gaddp)
+    std::vector<double> Gx((size_t)(my + 2) * 2 * LX * MEQN);
+    std::vector<double> cflx(my + 2), cfly(mx + 2);
+    std::fill(F.fm.begin(), F.fm.end(), 0.0);
+    std::fill(F.fp.begin(), F.fp.end(), 0.0);
+    std::fill(F.gm.begin(), F.gm.end(), 0.0);
+    std::fill(F.gp.begin(), F.gp.end(), 0.0);
+#pragma omp parallel
+    {
+        Slice sx(mx);
+        Model Mt = M;
+#pragma omp for schedule(dynamic, 4)
+        for (int j = 0; j <= my + 1; ++j) {
+            load_xslice(pt, sx, j, dtdx);
+            double cfl1d;
+            flux2(Mt, 1, sx, cfl1d);
+            cflx[j] = cfl1d;
+            for (int i = 1; i <= mx + 1; ++i)
+                for (int m = 1; m <= MEQN; ++m) {
+                    F.fm[F.at(m, i, j)] = 0.0 + sx.FM(m, i);
+                    F.fp[F.at(m, i, j)] = 0.0 + sx.FP(m, i);
+                    Gx[(((size_t)j * 2 + 0) * LX + sx.ix(i)) * MEQN + (m - 1)] = sx.GM(m, i, 1);
+                    Gx[(((size_t)j * 2 + 1) * LX + sx.ix(i)) * MEQN + (m - 1)] = sx.GM(m, i, 2);
+                }
+            if (xlog) std::memcpy(xlog + (size_t)j * (mx + 1), sx.br.data(), sizeof(uint32_t) * (mx + 1));
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j <= my + 2; ++j)
+        for (int i = 1; i <= mx + 1; ++i)
+            for (int m = 1; m <= MEQN; ++m) {
+                double acc = 0.0;
+                if (j - 1 >= 0) acc = acc + Gx[((((size_t)(j - 1)) * 2 + 1) * LX + (size_t)(i + MBC - 1)) * MEQN + (m - 1)];
+                if (j <= my + 1) acc = acc + Gx[(((size_t)j * 2 + 0) * LX + (size_t)(i + MBC - 1)) * MEQN + (m - 1)];
+                F.gm[F.at(m, i, j)] = acc;
+                F.gp[F.at(m, i, j)] = acc;
+            }
+    std::vector<double>().swap(Gx);
+    std::vector<double> Gy((size_t)(mx + 2) * 2 * LY * MEQN);
+#pragma omp parallel
+    {
+        Slice sy(my);
+        Model Mt = M;
+#pragma omp for schedule(dynamic, 4)
+        for (int i = 0; i <= mx + 1; ++i) {
+            load_yslice(pt, sy, i, dtdy);
+            double cfl1d;
+            flux2(Mt, 2, sy, cfl1d);
+            cfly[i] = cfl1d;
+            for (int j = 1; j <= my + 1; ++j)
+                for (int m = 1; m <= MEQN; ++m) {
+                    F.gm[F.at(m, i, j)] += sy.FM(m, j);
+                    F.gp[F.at(m, i, j)] += sy.FP(m, j);
+                    Gy[(((size_t)i * 2 + 0) * LY + sy.ix(j)) * MEQN + (m - 1)] = sy.GM(m, j, 1);
+                    Gy[(((size_t)i * 2 + 1) * LY + sy.ix(j)) * MEQN + (m - 1)] = sy.GM(m, j, 2);
+                }
+            if (ylog) std::memcpy(ylog + (size_t)i * (my + 1), sy.br.data(), sizeof(uint32_t) * (my + 1));
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int j = 1; j <= my + 1; ++j)
+        for (int i = 0; i <= mx + 2; ++i)
+            for (int m = 1; m <= MEQN; ++m) {
+                double fm = F.fm[F.at(m, i, j)], fp = F.fp[F.at(m, i, j)];
+                if (i - 1 >= 0) {
+                    double g2 = Gy[((((size_t)(i - 1)) * 2 + 1) * LY + (size_t)(j + MBC - 1)) * MEQN + (m - 1)];
+                    fm = fm + g2;
+                    fp = fp + g2;
+                }
+                if (i <= mx + 1) {
+                    double g1 = Gy[(((size_t)i * 2 + 0) * LY + (size_t)(j + MBC - 1)) * MEQN + (m - 1)];
+                    fm = fm + g1;
+                    fp = fp + g1;
+                }
+                F.fm[F.at(m, i, j)] = fm;
+                F.fp[F.at(m, i, j)] = fp;
+            }
+    double cflgrid = 0.0;
+    for (int j = 0; j <= my + 1; ++j) cflgrid = fmax2(cflgrid, cflx[j]);
+    for (int i = 0; i <= mx + 1; ++i) cflgrid = fmax2(cflgrid, cfly[i]);
+    return cflgrid;
+}
+
+// GeoClaw stepgrid flux-differencing update (mcapa = 0)
+void update(Patch& pt, const Fluxes& F, double dx, double dy, double dt) {
+    const int mx = pt.mx, my = pt.my;
+    double dtdx = dt / dx, dtdy = dt / dy;
+#pragma omp parallel for schedule(static)
+    for (int j = 1; j <= my; ++j)
+        for (int i = 1; i <= mx; ++i)
+            for (int m = 1; m <= MEQN; ++m)
+                pt.Q(m, i, j) = pt.Q(m, i, j) - dtdx * (F.fm[F.at(m, i + 1, j)] - F.fp[F.at(m, i, j)])
+                                - dtdy * (F.gm[F.at(m, i, j + 1)] - F.gp[F.at(m, i, j)]);
+}
+
+// mp_update.f90:710-789
+void mp_update_relax_Dclaw4(Model& M, double dt, double& h, double& u, double& v, double& m,
+                            double& p, double& chi, double rhoh, double gz) {
+    const dclaw_params& P = M.p;
+    double rho, kperm, alphainv, m_eq, tanpsi, tau;
+    setvars(M, h, u, v, m, p, chi, gz, rho, kperm, alphainv, m_eq, tanpsi, tau);
+    double hu = h * u, hv = h * v, hm = h * m, hchi = h * chi;
+    double vnorm = std::sqrt(sq(hu) + sq(hv)) / h;
+    p = p - dt * 3.0 * vnorm * tanpsi * alphainv / h;
+    qfix(M, h, hu, hv, hm, p, hchi, u, v, m, chi, rho, gz);
+    double zeta = 3.0 * alphainv / (h * 2.0) + (rho - P.rho_f) * P.rho_f * gz / (4.0 * rho);
+    double krate = -zeta * 2.0 * kperm / (h * fmax2(P.mu, 1.0e-16));
+    double p_eq = P.rho_f * h * gz;
+    p = p_eq + (p - p_eq) * std::exp(krate * dt);
+    double p_exc = p - P.rho_f * gz * h;
+    qfix_cmass(M, h, m, p, rho, p_exc, hu, hv, hm, u, v, rhoh, gz);
+    double D = -2.0 * (kperm / (P.mu * h)) * p_exc;
+    krate = D * (rho - P.rho_f) / rhoh;
+    hm = hm * std::exp(-dt * D * P.rho_f / (rhoh));
+    if (P.src2method == 0) {
+        h = h + h * krate * dt;
+        hchi = h * chi;
+        hu = hu * std::exp(dt * krate);
+        hv = hv * std::exp(dt * krate);
+        qfix(M, h, hu, hv, hm, p, hchi, u, v, m, chi, rho, gz);
+    } else if (P.src2method == 1) {
+        h = (rhoh - hm * (P.rho_s - P.rho_f)) / P.rho_f;
+        hu = h * u;
+        hv = h * v;
+        hchi = h * chi;
+        qfix(M, h, hu, hv, hm, p, hchi, u, v, m, chi, rho, gz);
+    }
+}
+
+// src2.f90:27-306 (bed_normal = 0, curvature = 0, entrainment = 0)
+void src2(Model& M, Patch& pt, double dt) {
+    const dclaw_params& P = M.p;
+    const int mx = pt.mx, my = pt.my;
+    double coeffmanning = P.friction_forcing ? P.manning_coefficient : 0.0;
+    double gz = P.grav;
+    double gx = 0.0;
+#pragma omp parallel for schedule(static)
+    for (int j = 1; j <= my; ++j) {
+        Model Mt = M;
+        for (int i = 1; i <= mx; ++i) {
+            double h = pt.Q(I_H, i, j);
+            if (h <= P.dry_tolerance) {
+                pt.Q(I_H, i, j) = 0.0; pt.Q(I_HU, i, j) = 0.0; pt.Q(I_HV, i, j) = 0.0;
+                pt.Q(I_HM, i, j) = 0.0; pt.Q(I_PB, i, j) = 0.0; pt.Q(I_HCHI, i, j) = 0.0;
+                continue;
+            }
+            double hu = pt.Q(I_HU, i, j), hv = pt.Q(I_HV, i, j), hm = pt.Q(I_HM, i, j);
+            double p = pt.Q(I_PB, i, j), hchi = pt.Q(I_HCHI, i, j);
+            double rhoh = hm * P.rho_s + (h - hm) * P.rho_f;
+            if (hm < 0.0) continue;
+            double u, v, m, chi, rho;
+            qfix(Mt, h, hu, hv, hm, p, hchi, u, v, m, chi, rho, gz);
+            double kperm, alphainv, m_eq, tanpsi, tau;
+            setvars(Mt, h, u, v, m, p, chi, gz, rho, kperm, alphainv, m_eq, tanpsi, tau);
+            double hvnorm0 = std::sqrt(sq(hu) + sq(hv));
+            double vnorm = hvnorm0 / h;
+            if (hvnorm0 > 0.0) {
+                vnorm = fmax2(0.0, vnorm - dt * tau / rhoh);
+                vnorm = vnorm * std::exp(-(1.0 - m) * 2.0 * P.mu * dt / (h * rhoh));
+                double hvnorm = h * vnorm;
+                hu = hvnorm * hu / hvnorm0 + gx * h * dt;
+                hv = hvnorm * hv / hvnorm0;
+                u = hu / h;
+                v = hv / h;
+                vnorm = std::sqrt(sq(u) + sq(v));
+            }
+            setvars(Mt, h, u, v, m, p, chi, gz, rho, kperm, alphainv, m_eq, tanpsi, tau);
+            if (P.src2method == -1) {
+                hu = h * u; hv = h * v; hm = h * m; hchi = h * chi;
+            } else {
+                mp_update_relax_Dclaw4(Mt, dt, h, u, v, m, p, chi, rhoh, gz);
+                hu = h * u; hv = h * v; hm = h * m; hchi = h * chi;
+            }
+            if (h <= P.dry_tolerance) {
+                pt.Q(I_H, i, j) = 0.0; pt.Q(I_HU, i, j) = 0.0; pt.Q(I_HV, i, j) = 0.0;
+                pt.Q(I_HM, i, j) = 0.0; pt.Q(I_PB, i, j) = 0.0; pt.Q(I_HCHI, i, j) = 0.0;
+                continue;
+            }
+            setvars(Mt, h, u, v, m, p, chi, gz, rho, kperm, alphainv, m_eq, tanpsi, tau);
+            if (P.friction_forcing && coeffmanning > 0.0) {
+                if (h <= P.friction_depth) {
+                    double cm = coeffmanning;
+                    if (P.dd_manning)
+                        cm = P.manning_max + (P.manning_coefficient - P.manning_max) * 0.5
+                             * (1.0 + std::tanh(300.0 * (h - 0.05)));
+                    double beta = 1.0;
+                    double gamma = beta * std::sqrt(sq(hu) + sq(hv)) * (gz * sq(cm)) / (std::pow(h, 7.0 / 3.0));
+                    double dgamma = 1.0 + dt * gamma;
+                    hu = hu / dgamma;
+                    hv = hv / dgamma;
+                    qfix(Mt, h, hu, hv, hm, p, hchi, u, v, m, chi, rho, gz);
+                }
+            }
+            pt.Q(I_H, i, j) = h; pt.Q(I_HU, i, j) = hu; pt.Q(I_HV, i, j) = hv;
+            pt.Q(I_HM, i, j) = hm; pt.Q(I_PB, i, j) = p; pt.Q(I_HCHI, i, j) = hchi;
+        }
+    }
+}
+
+// GeoClaw bc2amr (restated): per side, wall = mirror with the normal momentum
+// negated, extrapolation = copy of the nearest interior cell; x sides first
+// (all rows), then y sides (all columns, corners included).
+void bc2amr(const dclaw_params& P, Patch& pt) {
+    const int mx = pt.mx, my = pt.my;
+    for (int j = 1 - MBC; j <= my + MBC; ++j) {
+        for (int k = 1; k <= MBC; ++k) {
+            int gi = 1 - k;  // left ghost
+            int si = (P.bc_lower[0] == DCLAW_BC_WALL) ? k : 1;
+            for (int m = 1; m <= MEQN; ++m) pt.Q(m, gi, j) = pt.Q(m, si, j);
+            if (P.bc_lower[0] == DCLAW_BC_WALL) pt.Q(I_HU, gi, j) = -pt.Q(I_HU, gi, j);
+            gi = mx + k;
+            si = (P.bc_upper[0] == DCLAW_BC_WALL) ? mx + 1 - k : mx;
+            for (int m = 1; m <= MEQN; ++m) pt.Q(m, gi, j) = pt.Q(m, si, j);
+            if (P.bc_upper[0] == DCLAW_BC_WALL) pt.Q(I_HU, gi, j) = -pt.Q(I_HU, gi, j);
+        }
+    }
+    for (int i = 1 - MBC; i <= mx + MBC; ++i) {
+        for (int k = 1; k <= MBC; ++k) {
+            int gj = 1 - k;
+            int sj = (P.bc_lower[1] == DCLAW_BC_WALL) ? k : 1;
+            for (int m = 1; m <= MEQN; ++m) pt.Q(m, i, gj) = pt.Q(m, i, sj);
+            if (P.bc_lower[1] == DCLAW_BC_WALL) pt.Q(I_HV, i, gj) = -pt.Q(I_HV, i, gj);
+            gj = my + k;
+            sj = (P.bc_upper[1] == DCLAW_BC_WALL) ? my + 1 - k : my;
+            for (int m = 1; m <= MEQN; ++m) pt.Q(m, i, gj) = pt.Q(m, i, sj);
+            if (P.bc_upper[1] == DCLAW_BC_WALL) pt.Q(I_HV, i, gj) = -pt.Q(I_HV, i, gj);
+        }
+    }
+}
+
+// setaux.f90:155-198,268-281 for a bed given on the interior
+void setaux(const dclaw_params& P, Patch& pt, const double* b_interior) {
+    const int mx = pt.mx, my = pt.my;
+    for (int j = 1 - MBC; j <= my + MBC; ++j)
+        for (int i = 1 - MBC; i <= mx + MBC; ++i) {
+            int ii = i < 1 ? 1 : (i > mx ? mx : i);
+            int jj = j < 1 ? 1 : (j > my ? my : j);
+            for (int m = 1; m <= MAUX; ++m) pt.A(m, i, j) = 0.0;
+            pt.A(1, i, j) = b_interior[(size_t)(jj - 1) * mx + (ii - 1)];
+            pt.A(I_PHI, i, j) = P.phi;
+            pt.A(I_THETA, i, j) = P.theta_input;
+        }
+}
+
+bool has_nan(Patch& pt) {
+    for (double x : pt.q) if (std::isnan(x)) return true;
+    return false;
+}
+
+// tick.f:490-526 with stepgrid's dtnew = dt*cfl_desired/cflgrid
+double next_dt(const dclaw_params& P, double dt, double cfl) {
+    double dtnew = cfl > 0.0 ? dt * P.cfl_desired / cfl : 1.0e300;
+    return fmin2(dtnew, P.dt_max);
+}
+
+void put_state(Patch& pt, const double* q_soa) {
+    const int mx = pt.mx, my = pt.my;
+    const size_t plane = (size_t)mx * my;
+    for (int j = 1; j <= my; ++j)
+        for (int i = 1; i <= mx; ++i) {
+            size_t c = (size_t)(j - 1) * mx + (i - 1);
+            for (int m = 1; m <= 5; ++m) pt.Q(m, i, j) = q_soa[(m - 1) * plane + c];
+            pt.Q(I_HCHI, i, j) = 0.0;
+            pt.Q(I_BDIF, i, j) = 0.0;
+        }
+}
+
+void get_state(Patch& pt, double* q_soa) {
+    const int mx = pt.mx, my = pt.my;
+    const size_t plane = (size_t)mx * my;
+    for (int j = 1; j <= my; ++j)
+        for (int i = 1; i <= mx; ++i) {
+            size_t c = (size_t)(j - 1) * mx + (i - 1);
+            for (int m = 1; m <= 5; ++m) q_soa[(m - 1) * plane + c] = pt.Q(m, i, j);
+        }
+}
+
+// padded SoA (5 or 6 planes) <-> AoS patch arrays
+void put_padded_q(Patch& pt, const double* q) {
+    const size_t plane = (size_t)(pt.mx + 2 * MBC) * (pt.my + 2 * MBC);
+    for (size_t c = 0; c < plane; ++c) {
+        for (int m = 0; m < 5; ++m) pt.q[c * MEQN + m] = q[m * plane + c];
+        pt.q[c * MEQN + 5] = 0.0;
+        pt.q[c * MEQN + 6] = 0.0;
+    }
+}
+void get_padded_q(Patch& pt, double* q) {
+    const size_t plane = (size_t)(pt.mx + 2 * MBC) * (pt.my + 2 * MBC);
+    for (size_t c = 0; c < plane; ++c)
+        for (int m = 0; m < 5; ++m) q[m * plane + c] = pt.q[c * MEQN + m];
+}
+void put_padded_aux(Patch& pt, const double* aux) {
+    const size_t plane = (size_t)(pt.mx + 2 * MBC) * (pt.my + 2 * MBC);
+    for (size_t c = 0; c < plane; ++c) {
+        for (int m = 0; m < MAUX; ++m) pt.aux[c * MAUX + m] = 0.0;
+        for (int m = 0; m < 6; ++m) pt.aux[c * MAUX + m] = aux[m * plane + c];
+    }
+}
+void get_padded_aux(Patch& pt, double* aux) {
+    const size_t plane = (size_t)(pt.mx + 2 * MBC) * (pt.my + 2 * MBC);
+    for (size_t c = 0; c < plane; ++c)
+        for (int m = 0; m < 6; ++m) aux[m * plane + c] = pt.aux[c * MAUX + m];
+}
+
+Model make_model(const dclaw_params* p) {
+    Model M;
+    M.p = *p;
+    M.phi = p->phi;
+    M.kappa = 1.0;
+    return M;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_version(void) { return 1; }
+
+int oracle_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
+
+/*
+ * Run nsteps full steps (bc2amr, b4step2, step2, update, src2, tick) on an
+ * mx x my interior state q (5 SoA planes, in/out) over bed b (mx*my).
+ * dt_hist/cfl_hist (nullable) receive each step's dt and Courant number.
+ * fixed_dt != 0 keeps dt constant. t_final > 0 clips dt so t <= t_final.
+ * parallel != 0 uses the OpenMP step2 (bit-identical to the serial one).
+ * xlog/ylog (nullable): branch bits of the LAST step, sized
+ * (my+2)*(mx+1) and (mx+2)*(my+1).
+ * Returns 0, or 3 if a NaN appeared (the step where it appeared is not taken).
+ */
+int oracle_run(const dclaw_params* prm, int mx, int my, double dx, double dy, double* q,
+               const double* b, int nsteps, double dt_initial, double t_final, int fixed_dt,
+               int parallel, double* dt_hist, double* cfl_hist, uint32_t* xlog, uint32_t* ylog,
+               double* t_out) {
+    Model M = make_model(prm);
+    Patch pt(mx, my);
+    put_state(pt, q);
+    setaux(M.p, pt, b);
+    Fluxes F(mx, my);
+    double t = 0.0, dt = dt_initial;
+    int status = 0;
+    for (int n = 0; n < nsteps; ++n) {
+        double dtn = dt;
+        if (t_final > 0.0) dtn = fmax2(fmin2(dtn, t_final - t), 0.0);
+        bc2amr(M.p, pt);
+        if (has_nan(pt)) { status = 3; break; }
+        b4step2(M, pt, dx, dy);
+        bool last = (n == nsteps - 1);
+        double cfl = parallel ? step2_parallel(M, pt, F, dx, dy, dtn, last ? xlog : nullptr, last ? ylog : nullptr)
+                              : step2_serial(M, pt, F, dx, dy, dtn, last ? xlog : nullptr, last ? ylog : nullptr);
+        update(pt, F, dx, dy, dtn);
+        src2(M, pt, dtn);
+        if (dt_hist) dt_hist[n] = dtn;
+        if (cfl_hist) cfl_hist[n] = cfl;
+        t = t + dtn;
+        if (!fixed_dt) dt = next_dt(M.p, dtn, cfl);
+    }
+    get_state(pt, q);
+    if (t_out) *t_out = t;
+    return status;
+}
+
+/* Patch-call oracles on the padded SoA layout (5 q planes, 6 aux planes). */
+int oracle_bc2amr(const dclaw_params* prm, int mx, int my, double* q) {
+    Patch pt(mx, my);
+    put_padded_q(pt, q);
+    bc2amr(*prm, pt);
+    get_padded_q(pt, q);
+    return 0;
+}
+
+int oracle_setaux(const dclaw_params* prm, int mx, int my, const double* b_interior, double* aux) {
+    Patch pt(mx, my);
+    setaux(*prm, pt, b_interior);
+    get_padded_aux(pt, aux);
+    return 0;
+}
+
+int oracle_b4step2(const dclaw_params* prm, int mx, int my, double dx, double dy, double* q, double* aux) {
+    Model M = make_model(prm);
+    Patch pt(mx, my);
+    put_padded_q(pt, q);
+    put_padded_aux(pt, aux);
+    b4step2(M, pt, dx, dy);
+    get_padded_q(pt, q);
+    get_padded_aux(pt, aux);
+    return 0;
+}
+
+/* step2 + update; fluxes (nullable) = 20 padded planes fm[5],fp[5],gm[5],gp[5] */
+int oracle_step2(const dclaw_params* prm, int mx, int my, double dx, double dy, double dt, double* q,
+                 const double* aux, double* cflgrid, double* fluxes, int parallel, uint32_t* xlog,
+                 uint32_t* ylog) {
+    Model M = make_model(prm);
+    Patch pt(mx, my);
+    put_padded_q(pt, q);
+    put_padded_aux(pt, aux);
+    Fluxes F(mx, my);
+    double cfl = parallel ? step2_parallel(M, pt, F, dx, dy, dt, xlog, ylog)
+                          : step2_serial(M, pt, F, dx, dy, dt, xlog, ylog);
+    update(pt, F, dx, dy, dt);
+    get_padded_q(pt, q);
+    if (cflgrid) *cflgrid = cfl;
+    if (fluxes) {
+        const size_t plane = (size_t)(mx + 2 * MBC) * (my + 2 * MBC);
+        for (size_t c = 0; c < plane; ++c)
+            for (int m = 0; m < 5; ++m) {
+                fluxes[(0 * 5 + m) * plane + c] = F.fm[c * MEQN + m];
+                fluxes[(1 * 5 + m) * plane + c] = F.fp[c * MEQN + m];
+                fluxes[(2 * 5 + m) * plane + c] = F.gm[c * MEQN + m];
+                fluxes[(3 * 5 + m) * plane + c] = F.gp[c * MEQN + m];
+            }
+    }
+    return 0;
+}
+
+int oracle_src2(const dclaw_params* prm, int mx, int my, double dt, double* q, const double* aux) {
+    Model M = make_model(prm);
+    Patch pt(mx, my);
+    put_padded_q(pt, q);
+    put_padded_aux(pt, aux);
+    src2(M, pt, dt);
+    get_padded_q(pt, q);
+    return 0;
+}
+
+/* pointwise closures, for unit tests */
+void oracle_qfix(const dclaw_params* prm, double* s /* h,hu,hv,hm,p,hchi in/out */, double* prim /* u,v,m,chi,rho */) {
+    Model M = make_model(prm);
+    qfix(M, s[0], s[1], s[2], s[3], s[4], s[5], prim[0], prim[1], prim[2], prim[3], prim[4], prm->grav);
+}
+void oracle_setvars(const dclaw_params* prm, const double* in /* h,u,v,m,p,chi */, double* out /* rho,kperm,alphainv,m_eq,tanpsi,tau */) {
+    Model M = make_model(prm);
+    setvars(M, in[0], in[1], in[2], in[3], in[4], in[5], prm->grav, out[0], out[1], out[2], out[3], out[4], out[5]);
+}
+
+}  // extern "C"

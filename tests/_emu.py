@@ -1,0 +1,50 @@
+"""TEST INFRASTRUCTURE: host build of the CUDA stage functions (tests/emu)."""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from dclaw_b200.params import CParams
+
+HERE = Path(__file__).resolve().parent / "emu"
+SRC = HERE / "emu_step.cpp"
+LIB = HERE / "libemu.so"
+CSRC = Path(__file__).resolve().parents[1] / "dclaw_b200" / "csrc"
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_up = ctypes.POINTER(ctypes.c_uint32)
+
+
+def build() -> Path:
+    deps = [SRC, *CSRC.glob("*.cuh")]
+    if LIB.exists() and all(d.stat().st_mtime <= LIB.stat().st_mtime for d in deps):
+        return LIB
+    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
+                    str(SRC), "-o", str(LIB)], check=True)
+    return LIB
+
+
+class Emu:
+    def __init__(self):
+        self.lib = ctypes.CDLL(str(build()))
+        self.lib.emu_run.restype = ctypes.c_int
+        self.lib.emu_run.argtypes = [ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                     ctypes.c_double, _dp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_int, _dp, _dp, _up, _dp]
+
+    def run(self, p, q, b, dx, dy, nsteps, dt_initial, t_final=0.0, fixed_dt=False):
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        _, my, mx = q.shape
+        dth = np.zeros(max(nsteps, 1))
+        cfh = np.zeros(max(nsteps, 1))
+        br = np.zeros((my + 2) * (mx + 1) + (mx + 2) * (my + 1), dtype=np.uint32)
+        t = np.zeros(1)
+        cp = p.to_c()
+        st = self.lib.emu_run(ctypes.byref(cp), mx, my, dx, dy, q.ctypes.data_as(_dp), b.ctypes.data_as(_dp),
+                              nsteps, dt_initial, t_final, int(fixed_dt), dth.ctypes.data_as(_dp),
+                              cfh.ctypes.data_as(_dp), br.ctypes.data_as(_up), t.ctypes.data_as(_dp))
+        return dict(q=q, dt=dth[:nsteps], cfl=cfh[:nsteps], status=st, br=br, t=float(t[0]))

@@ -1,0 +1,79 @@
+// emu_step.cpp -- TEST INFRASTRUCTURE: runs the CUDA step's stage functions
+// (dclaw_b200/csrc/stages.cuh) on the host, in the kernels' launch order, so
+// that the CPU test suite can check the device arithmetic against the oracle
+// bit for bit (both sides use glibc libm and no FMA contraction here; on the
+// GPU only CUDA's exp/atan/tan/tanh differ). This is not a product path.
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+#include "../../dclaw_b200/csrc/stages.cuh"
+
+using namespace dclaw;
+
+extern "C" int emu_run(const dclaw_params* P, int mx, int my, double dx, double dy, double* q, const double* b,
+                       int nsteps, double dt_initial, double t_final, int fixed_dt, double* dt_hist,
+                       double* cfl_hist, uint32_t* brlog, double* t_out) {
+    Geom g{mx, my, mx + 4, my + 4, dx, dy};
+    size_t npad = (size_t)(mx + 4) * (my + 4), nxi = (size_t)(mx + 3) * (my + 2), nyi = (size_t)(my + 3) * (mx + 2);
+    std::vector<double> qB(5 * npad), bP(npad), td(3 * npad), wx(NW * nxi), wy(NW * nyi), fx(NF * nxi), fy(NF * nyi);
+    Work W{qB.data(), bP.data(), td.data(), wx.data(), wy.data(), fx.data(), fy.data(), npad, nxi, nyi};
+    std::vector<double> qa(q, q + 5 * (size_t)mx * my), qb(5 * (size_t)mx * my);
+    double t = 0.0, dt = t_final > 0.0 ? fmax2(fmin2(dt_initial, t_final), 0.0) : dt_initial;
+    int status = 0;
+    for (int n = 0; n < nsteps; ++n) {
+        const bool last = n == nsteps - 1;
+        uint32_t* br = (last && brlog) ? brlog : nullptr;
+        for (int j = -1; j <= my + 2; ++j)
+            for (int i = -1; i <= mx + 2; ++i)
+                if (stage_b4(*P, g, qa.data(), b, W, i, j)) status = DCLAW_ERR_NAN;
+        if (status) break;
+        for (int j = -1; j <= my + 2; ++j)
+            for (int i = -1; i <= mx + 2; ++i) stage_taudir(*P, g, W, i, j);
+        double cfl = 0.0;
+        for (int r = 0; r <= my + 1; ++r)
+            for (int i = 0; i <= mx + 2; ++i) {
+                uint32_t bits = 0;
+                double s = stage_riemann<0>(*P, g, W, r, i, &bits);
+                if (i >= 1 && i <= mx + 1) {
+                    cfl = fmax2(cfl, (dt / dx) * s);
+                    if (br) br[(size_t)r * (mx + 1) + (i - 1)] = bits;
+                }
+            }
+        for (int c = 0; c <= mx + 1; ++c)
+            for (int k = 0; k <= my + 2; ++k) {
+                uint32_t bits = 0;
+                double s = stage_riemann<1>(*P, g, W, c, k, &bits);
+                if (k >= 1 && k <= my + 1) {
+                    cfl = fmax2(cfl, (dt / dy) * s);
+                    if (br) br[(size_t)(my + 2) * (mx + 1) + (size_t)c * (my + 1) + (k - 1)] = bits;
+                }
+            }
+        for (int r = 0; r <= my + 1; ++r)
+            for (int i = 1; i <= mx + 1; ++i) {
+                uint32_t bits = 0;
+                stage_flux<0>(*P, g, W, r, i, dt / dx, br ? &bits : nullptr);
+                if (br) br[(size_t)r * (mx + 1) + (i - 1)] |= bits;
+            }
+        for (int c = 0; c <= mx + 1; ++c)
+            for (int k = 1; k <= my + 1; ++k) {
+                uint32_t bits = 0;
+                stage_flux<1>(*P, g, W, c, k, dt / dy, br ? &bits : nullptr);
+                if (br) br[(size_t)(my + 2) * (mx + 1) + (size_t)c * (my + 1) + (k - 1)] |= bits;
+            }
+        for (int j = 1; j <= my; ++j)
+            for (int i = 1; i <= mx; ++i)
+                if (stage_finalize(*P, g, W, qb.data(), i, j, dt)) status = DCLAW_ERR_NAN;
+        qa.swap(qb);
+        if (dt_hist) dt_hist[n] = dt;
+        if (cfl_hist) cfl_hist[n] = cfl;
+        t = t + dt;
+        double dtn = fixed_dt ? dt : tick_next_dt(*P, dt, cfl);
+        if (t_final > 0.0) dtn = fmax2(fmin2(dtn, t_final - t), 0.0);
+        dt = dtn;
+        if (status) break;
+    }
+    memcpy(q, qa.data(), sizeof(double) * 5 * (size_t)mx * my);
+    if (t_out) *t_out = t;
+    return status;
+}

@@ -1,0 +1,256 @@
+"""Parity of the CUDA step (through the C ABI) with the oracle.
+
+Bar: the dry/wet mask (h == 0) and every per-interface branch bit (dry
+skip, wall problem, sonic, static friction, middle-wave merge side, 4-cell
+wet check, limiter regime and upwind side of each wave family, transverse
+splits) of the last step are bit-identical; state fields agree to 1e-12
+relative (max |gpu - oracle| over the field / max |oracle|) on short runs and
+1e-10 after 1000 steps. The remaining differences come only from CUDA's
+exp/atan/tan/tanh, which may round differently from glibc by an ulp.
+"""
+import numpy as np
+import pytest
+import torch
+
+from dclaw_b200 import workloads as W
+from dclaw_b200.params import DClawParams
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_run(c, n, fixed_dt=False, dt=None):
+    from dclaw_b200.solver import PatchStepper
+
+    dev = torch.device("cuda:0")
+    st = PatchStepper(torch.tensor(c.q, device=dev), torch.tensor(c.b, device=dev), c.params, c.dx, c.dy,
+                      branch_log=True)
+    st.init_clock(c.dt_initial if dt is None else dt, fixed_dt=fixed_dt)
+    hist = torch.zeros((n, 4), dtype=torch.float64, device=dev)
+    st.step(n, history=hist)
+    torch.cuda.synchronize()
+    return dict(q=st.state().cpu().numpy(), hist=hist.cpu().numpy(),
+                br=st.brlog.cpu().numpy().view(np.uint32), status=st.status())
+
+
+def rel_err(a, b):
+    return max(np.abs(a[m] - b[m]).max() / max(np.abs(b[m]).max(), 1e-300) for m in range(5))
+
+
+def check(c, n, tol, oracle, fixed_dt=False):
+    g = gpu_run(c, n, fixed_dt)
+    o = oracle.run(c.params, c.q, c.b, c.dx, c.dy, n, c.dt_initial, fixed_dt=fixed_dt, branch_log=True)
+    assert g["status"] == 0 and o["status"] == 0
+    assert np.array_equal(g["q"][0] == 0.0, o["q"][0] == 0.0), "dry/wet mask differs"
+    br_o = np.concatenate([o["xlog"].ravel(), o["ylog"].ravel()])
+    nd = int((g["br"] != br_o).sum())
+    assert nd == 0, f"{nd} interfaces took a different branch"
+    assert rel_err(g["q"], o["q"]) <= tol
+    assert np.allclose(g["hist"][:, 3], o["dt"], rtol=tol, atol=0)
+    assert np.allclose(g["hist"][:, 2], o["cfl"], rtol=tol, atol=0)
+    return g, o
+
+
+def test_slope_runout_short(cuda_device, oracle):
+    check(W.slope_runout(), 20, 1e-12, oracle)
+
+
+@pytest.mark.parametrize("variant", ["order1", "transverse1", "minmod", "extrap", "src2m1", "swe", "alpha1",
+                                     "manning", "speed_limit"])
+def test_variants(cuda_device, oracle, variant):
+    kw = {"order1": dict(order=1, transverse_waves=0), "transverse1": dict(transverse_waves=1),
+          "minmod": dict(limiter=1), "extrap": dict(bc_lower=("extrap", "wall"), bc_upper=("extrap", "extrap")),
+          "src2m1": dict(src2method=1), "swe": dict(src2method=-1), "alpha1": dict(alphamethod=1),
+          "manning": dict(friction_forcing=True, manning_coefficient=0.025),
+          "speed_limit": dict(speed_limit=2.0)}[variant]
+    base = W.slope_runout(n=96)
+    c = W.Case(base.name, base.q, base.b, base.dx, base.dy, base.params.replace(**kw), 0, base.dt_initial)
+    check(c, 40, 1e-12, oracle)
+
+
+def test_random_field_small(cuda_device, oracle):
+    check(W.random_field_case(n=256, dx=0.5, seed=5), 30, 1e-12, oracle)
+
+
+def test_slope_runout_1000_steps(cuda_device, oracle):
+    """The 200 x 200 slope-runout case over its full 1000 steps."""
+    check(W.slope_runout(), 1000, 1e-10, oracle)
+
+
+def test_kats_on_gpu(cuda_device):
+    # contact wave (tests/eigenstructure_check/check.py:65,80)
+    c = W.contact_wave()
+    from dclaw_b200.solver import PatchStepper
+
+    dev = cuda_device
+    st = PatchStepper(torch.tensor(c.q, device=dev), torch.tensor(c.b, device=dev), c.params, c.dx, c.dy)
+    st.init_clock(c.dt_initial, t_final=2.0)
+    st.step(420)
+    q = st.state().cpu().numpy()
+    assert abs(st.read_clock().t - 2.0) < 1e-12
+    h = q[0]
+    u = np.where(h > 1e-6, q[1] / np.where(h > 1e-6, h, 1.0), 0.0)
+    assert np.abs(u).max() <= 1e-9 and h.max() - h.min() <= 1e-9
+    # lake at rest (differentiable_dclaw/tests/test_lake_at_rest.py:42)
+    c = W.lake_at_rest()
+    st = PatchStepper(torch.tensor(c.q, device=dev), torch.tensor(c.b, device=dev), c.params, c.dx, c.dy)
+    st.init_clock(c.dt_initial, t_final=60.0)
+    st.step(400)
+    q = st.state().cpu().numpy()
+    wet = q[0] > 0.01
+    assert np.abs(np.where(wet, q[1] / np.maximum(q[0], 1e-9), 0.0)).max() < 1e-8
+    assert np.abs(np.where(wet, q[0] + c.b - 5.0, 0.0)).max() < 1e-8
+    # dam front bound (check.py:97-118)
+    c = W.dam_front()
+    st = PatchStepper(torch.tensor(c.q, device=dev), torch.tensor(c.b, device=dev), c.params, c.dx, c.dy)
+    st.init_clock(c.dt_initial, t_final=1.0)
+    st.step(400)
+    h = st.state().cpu().numpy()[0][c.my // 2]
+    x = (np.arange(c.mx) + 0.5) * c.dx
+    assert x[h > 1e-3].max() <= 5.0 + 2.0 * np.sqrt(9.81 * 2.0) * 1.0 + 0.1
+
+
+def test_patch_calls(cuda_device, oracle):
+    """bc2amr, setaux, b4step2, step2 (+fluxes, cflgrid), src2 through the patch API."""
+    from dclaw_b200.patch import Patch
+
+    c = W.slope_runout(n=80)
+    mx, my = c.mx, c.my
+    p = c.params
+    dev = cuda_device
+    qpad = np.zeros((5, my + 4, mx + 4))
+    qpad[:, 2:-2, 2:-2] = c.q
+    # evolve a few steps on the oracle to get a moving state
+    r = oracle.run(p, c.q, c.b, c.dx, c.dy, 15, c.dt_initial)
+    qpad[:, 2:-2, 2:-2] = r["q"]
+    P = Patch(p, mx, my)
+    qg = torch.tensor(qpad, device=dev)
+    P.bc2amr(qg)
+    qo = oracle.bc2amr(p, qpad)
+    assert np.array_equal(qg.cpu().numpy(), qo)
+    auxo = oracle.setaux(p, c.b)
+    auxg = torch.zeros((6, my + 4, mx + 4), dtype=torch.float64, device=dev)
+    auxg[0, 2:-2, 2:-2] = torch.tensor(c.b, device=dev)
+    P.setaux(auxg)
+    assert np.array_equal(auxg.cpu().numpy(), auxo)
+    P.b4step2(qg, auxg, c.dx, c.dy)
+    qo, auxo = oracle.b4step2(p, qo, auxo, c.dx, c.dy)
+    assert np.array_equal(qg.cpu().numpy()[0] == 0, qo[0] == 0)
+    assert rel_err(qg.cpu().numpy(), qo) <= 1e-14
+    a_g, a_o = auxg.cpu().numpy(), auxo
+    assert np.array_equal(a_g[3] > 0, a_o[3] > 0)
+    assert np.abs(a_g[3:] - a_o[3:]).max() <= 1e-12
+    dt = float(r["dt"][-1])
+    fl = torch.zeros((20, my + 4, mx + 4), dtype=torch.float64, device=dev)
+    cfl_g = P.step2(qg, auxg, c.dx, c.dy, dt, fluxes=fl)
+    so = oracle.step2(p, qo, auxo, c.dx, c.dy, dt, fluxes=True)
+    assert abs(cfl_g - so["cfl"]) <= 1e-13 * so["cfl"]
+    assert rel_err(qg.cpu().numpy(), so["q"]) <= 1e-12
+    flg = fl.cpu().numpy()
+    # compare the flux entries the update uses
+    for k, (di, dj) in enumerate([(1, 0), (0, 0), (0, 1), (0, 0)]):
+        for m in range(5):
+            a = flg[5 * k + m, 2 + dj:2 + dj + my, 2 + di:2 + di + mx]
+            b = so["fluxes"][5 * k + m, 2 + dj:2 + dj + my, 2 + di:2 + di + mx]
+            assert np.abs(a - b).max() <= 1e-12 * max(np.abs(b).max(), 1e-30)
+    P.src2(qg, auxg, c.dx, c.dy, 0.0, dt)
+    qs = oracle.src2(p, so["q"], auxo, dt)
+    assert rel_err(qg.cpu().numpy(), qs) <= 1e-12
+    assert P.status() == 0
+
+
+def test_graph_replay_matches_eager(cuda_device):
+    from dclaw_b200.solver import PatchStepper
+
+    c = W.random_field_case(n=192, dx=0.5, seed=11)
+    dev = cuda_device
+    a = PatchStepper(torch.tensor(c.q, device=dev), torch.tensor(c.b, device=dev), c.params, c.dx, c.dy)
+    a.init_clock(c.dt_initial)
+    a.step(12)
+    b = PatchStepper(torch.tensor(c.q, device=dev), torch.tensor(c.b, device=dev), c.params, c.dx, c.dy)
+    b.init_clock(c.dt_initial)
+    b.capture(4)
+    b.replay(3)
+    torch.cuda.synchronize()
+    assert torch.equal(a.state(), b.state())
+    ca, cb = a.read_clock(), b.read_clock()
+    assert ca.t == cb.t and ca.dt == cb.dt and cb.nsteps == 12
+
+
+def test_full_size_window(cuda_device, oracle):
+    """4096 x 4096 run (fixed dt) against the oracle on a window: with a fixed
+    dt a cell depends only on cells within 4 per step, so the window's core
+    must agree although the oracle sees walls at the window edges."""
+    from dclaw_b200.solver import PatchStepper
+
+    c = W.random_field_case(n=4096, dx=0.5, seed=0)
+    dev = cuda_device
+    n, dt = 8, 0.02
+    st = PatchStepper(torch.tensor(c.q, device=dev), torch.tensor(c.b, device=dev), c.params, c.dx, c.dy)
+    st.init_clock(dt, fixed_dt=True)
+    st.step(n)
+    assert st.status() == 0
+    qg = st.state()
+    # a window around the wettest 256 x 256 block
+    h = torch.tensor(c.q[0], device=dev)
+    blk = torch.nn.functional.avg_pool2d(h[None, None], 256, 256)[0, 0]
+    jb, ib = divmod(int(torch.argmax(blk)), blk.shape[1])
+    j0, i0 = jb * 256, ib * 256
+    win = slice(j0, j0 + 256), slice(i0, i0 + 256)
+    o = oracle.run(c.params, c.q[:, win[0], win[1]], c.b[win[0], win[1]], c.dx, c.dy, n, dt, fixed_dt=True)
+    m = 4 * n + 4
+    g = qg[:, j0 + m:j0 + 256 - m, i0 + m:i0 + 256 - m].cpu().numpy()
+    oo = o["q"][:, m:256 - m, m:256 - m]
+    assert (g[0] > 0).sum() > 1000
+    assert np.array_equal(g[0] == 0, oo[0] == 0)
+    assert rel_err(g, oo) <= 1e-12
+
+
+def test_nan_reported_as_status(cuda_device):
+    from dclaw_b200.solver import PatchStepper
+
+    c = W.slope_runout(n=32)
+    q = c.q.copy()
+    q[4, 5, 5] = np.nan
+    st = PatchStepper(torch.tensor(q, device=cuda_device), torch.tensor(c.b, device=cuda_device), c.params,
+                      c.dx, c.dy)
+    st.init_clock(c.dt_initial)
+    st.step(1)
+    assert st.status() == 3
+
+
+def test_all_dry_stays_dry(cuda_device):
+    from dclaw_b200.solver import PatchStepper
+
+    c = W.slope_runout(n=32)
+    q = np.zeros_like(c.q)
+    st = PatchStepper(torch.tensor(q, device=cuda_device), torch.tensor(c.b, device=cuda_device), c.params,
+                      c.dx, c.dy)
+    st.init_clock(0.1)
+    st.step(3)
+    assert torch.count_nonzero(st.state()) == 0 and st.read_clock().cfl == 0.0
+
+
+def test_step_function_api(cuda_device, oracle):
+    """step / cfl_dt / rollout / rollout_peak with the port's (5, nx, ny) shapes."""
+    from dclaw_b200 import solver as S
+
+    c = W.slope_runout(n=64)
+    dev = cuda_device
+    q0 = torch.tensor(c.q, device=dev).permute(0, 2, 1).contiguous()  # (5, nx, ny)
+    b = torch.tensor(c.b, device=dev).t().contiguous()
+    grid = S.Grid(nx=64, ny=64, dx=c.dx, dy=c.dy)
+    p = c.params
+    q1 = S.step(q0, b, p, grid, 0.05)
+    o = oracle.run(p, c.q, c.b, c.dx, c.dy, 1, 0.05, fixed_dt=True)
+    assert rel_err(q1.permute(0, 2, 1).cpu().numpy(), o["q"]) <= 1e-12
+    dt = float(S.cfl_dt(q0, p, grid, 0.4))
+    h = c.q[0]
+    wet = h > 1e-3
+    smax = np.max(np.sqrt(9.81 * h[wet]))
+    assert abs(dt - 0.4 * c.dx / smax) <= 1e-12 * dt
+    qf, t, states, times = S.rollout(q0, b, p, grid, t_final=2.0, cfl=0.9, n_steps=40)
+    assert states.shape == (40, 5, 64, 64) and float(t) <= 2.0 + 1e-12
+    assert torch.equal(states[-1], qf)
+    qp, tp, hmax = S.rollout_peak(q0, b, p, grid, t_final=2.0, cfl=0.9, n_steps=40)
+    assert torch.equal(qp, qf) and hmax.shape == (64, 64)
+    assert torch.all(hmax >= qf[0]) and torch.all(hmax >= q0[0])

@@ -1,0 +1,52 @@
+"""The C-ABI library loads and exports every entry point of include/dclaw_b200.h
+(host-side calls only: no device work on the CPU runner)."""
+import ctypes
+import re
+from pathlib import Path
+
+from dclaw_b200 import _lib
+from dclaw_b200.params import CParams, DClawParams
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "dclaw_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"\b(dclaw_[a-z0-9_]+)\s*\(", text)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = declared_functions()
+    assert len(names) >= 12
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) <= set(_lib.SIGNATURES) | {"dclaw_step_noalloc"}
+
+
+def test_host_side_helpers():
+    lib = _lib.load()
+    assert lib.dclaw_abi_version() == 1
+    p = CParams()
+    lib.dclaw_params_default(ctypes.byref(p))
+    assert p.grav == 9.81 and p.limiter == 4 and p.order == 2
+    assert lib.dclaw_params_check(ctypes.byref(p)) == 0
+    mine = DClawParams().to_c()
+    assert lib.dclaw_params_check(ctypes.byref(mine)) == 0
+    bad = DClawParams(bed_normal=1).to_c()
+    assert lib.dclaw_params_check(ctypes.byref(bad)) == 2
+    bad = DClawParams(src2method=2).to_c()
+    assert lib.dclaw_params_check(ctypes.byref(bad)) == 2
+    bad = DClawParams(order=3).to_c()
+    assert lib.dclaw_params_check(ctypes.byref(bad)) == 1
+    assert lib.dclaw_workspace_bytes(1, 10) == 0
+    assert lib.dclaw_workspace_bytes(4096, 4096) > 0
+    assert lib.dclaw_error_string(3) == b"NaN in the state"
+
+
+def test_ctypes_struct_matches_header_size():
+    # dclaw_params: 8 doubles + 2 int32 + ... checked by field offsets of the ctypes image
+    assert ctypes.sizeof(CParams) % 8 == 0
+    assert CParams.bc_lower.offset % 4 == 0

@@ -1,0 +1,80 @@
+"""The oracle against the known-answer tests of the reference's own suites.
+
+Pins the CPU restatement (oracle/dclaw_oracle.cpp) to the closed-form
+criteria of tests/eigenstructure_check/check.py:65,80,97-118 (contact-wave
+preservation, dry dam-break front bound) and
+differentiable_dclaw/tests/test_lake_at_rest.py:42 (well-balancing, 1e-8).
+"""
+import numpy as np
+
+from dclaw_b200 import workloads as W
+
+
+def test_contact_wave_kat(oracle):
+    c = W.contact_wave()
+    r = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 420, c.dt_initial, t_final=2.0)
+    assert r["status"] == 0
+    assert abs(r["t"] - 2.0) < 1e-12
+    q = r["q"]
+    h = q[0]
+    u = np.where(h > 1e-6, q[1] / np.where(h > 1e-6, h, 1.0), 0.0)
+    assert np.abs(u).max() <= 1e-9           # check.py:65
+    assert h.max() - h.min() <= 1e-9         # check.py:65
+    j = c.my // 2
+    x = -5.0 + (np.arange(c.mx) + 0.5) * c.dx
+    m0 = c.q[3][j] / c.q[0][j]
+    m1 = np.where(h[j] > 1e-6, q[3][j] / h[j], 0.0)
+    # the interface: first cell of the m = 0.60 side, before and after
+    i0 = np.argmax(m0 > 0.575)
+    i1 = np.argmax(m1 > 0.575)
+    assert abs(x[i1] - x[i0]) <= 1e-6        # check.py:80
+
+
+def test_dam_front_kat(oracle):
+    c = W.dam_front()
+    for T in (0.2, 0.5, 1.0):
+        r = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 400, c.dt_initial, t_final=T)
+        assert r["status"] == 0 and abs(r["t"] - T) < 1e-12
+        h = r["q"][0][c.my // 2]
+        x = (np.arange(c.mx) + 0.5) * c.dx
+        wet = h > 1e-3
+        front = x[wet].max() if wet.any() else 5.0
+        assert front <= 5.0 + 2.0 * np.sqrt(9.81 * 2.0) * T + 0.1   # check.py:97-118
+        assert front > 5.0 + 0.5 * np.sqrt(9.81 * 2.0) * T          # the front does move
+
+
+def test_lake_at_rest_kat(oracle):
+    c = W.lake_at_rest()
+    r = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 400, c.dt_initial, t_final=60.0)
+    q = r["q"]
+    wet = q[0] > 0.01
+    max_u = np.abs(np.where(wet, q[1] / np.maximum(q[0], 1e-9), 0.0)).max()
+    eta_dev = np.abs(np.where(wet, q[0] + c.b - 5.0, 0.0)).max()
+    assert max_u < 1e-8 and eta_dev < 1e-8                    # test_lake_at_rest.py:42
+    assert np.all(q[0][c.b > 5.01] < 1e-6)                     # the island stays dry
+
+
+def test_serial_and_parallel_step2_agree(oracle):
+    c = W.slope_runout()
+    a = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 25, c.dt_initial, parallel=False, branch_log=True)
+    b = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 25, c.dt_initial, parallel=True, branch_log=True)
+    assert np.array_equal(a["q"], b["q"])
+    assert np.array_equal(a["dt"], b["dt"]) and np.array_equal(a["cfl"], b["cfl"])
+    assert np.array_equal(a["xlog"], b["xlog"]) and np.array_equal(a["ylog"], b["ylog"])
+
+
+def test_pointwise_qfix_and_setvars(oracle):
+    from dclaw_b200.params import DClawParams
+
+    p = DClawParams()
+    s, prim = oracle.qfix(p, [2.0, 1.0, -0.5, 1.3, 5.0e4, 0.0])
+    assert s[3] == 2.0 * (1.3 / 2.0) and prim[2] == 1.3 / 2.0
+    rho = 2700.0 * prim[2] + (1 - prim[2]) * 1000.0
+    assert s[4] == min(max(0.0, 5.0e4), rho * 9.81 * 2.0)
+    s, prim = oracle.qfix(p, [5e-4, 1.0, 1.0, 1.0, 1.0, 0.0])
+    assert np.all(s == 0) and np.all(prim == 0)
+    out = oracle.setvars(p, [1.0, 0.0, 0.0, 0.6, 0.8 * 1000 * 9.81, 0.0])
+    rho, kperm, alphainv, m_eq, tanpsi, tau = out
+    assert rho == 0.6 * (2700.0 - 1000.0) + 1000.0
+    assert m_eq == 0.64 and abs(tanpsi - (0.6 - 0.64)) < 1e-15
+    assert kperm == 1e-10 * np.exp(-(0.6 - 0.6) / 0.04)
