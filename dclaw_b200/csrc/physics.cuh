@@ -4,8 +4,9 @@
 // keeps the operand order of the Fortran (left-to-right, as gfortran -O
 // evaluates it) and the library is compiled with --fmad=false, so additions
 // and products round exactly as on the host; sqrt and division are IEEE
-// correctly rounded on the GPU as on x86-64. Only exp/atan/tan/tanh/pow come
-// from CUDA's libm and may differ from glibc by an ulp.
+// correctly rounded on the GPU as on x86-64. The elementary functions (exp,
+// atan, tan, tanh, h^(7/3)) are the project's own deterministic versions in
+// elementary.cuh, so the device returns the same bits as a host build.
 //
 // Reference map (paths in the youryugi/dclaw tree):
 //   qfix          src/2d/dig/digclaw_module.f90:285-345
@@ -31,6 +32,8 @@
 // host build of the same stage code (used only by the CPU emulation test)
 #define DC_HD inline
 #endif
+
+#include "elementary.cuh"
 
 namespace dclaw {
 
@@ -116,7 +119,7 @@ DC_HD SetVars setvars(const dclaw_params& P, double phi, double h, double u, dou
     SetVars o;
     o.rho = m * (P.rho_s - P.rho_f) + P.rho_f;
     double kr_chi = 1.0;
-    if (NEED_ALL) o.kperm = kr_chi * P.kref * exp(-(m - P.mref) / (0.04));
+    if (NEED_ALL) o.kperm = kr_chi * P.kref * em::d_exp(-(m - P.mref) / (0.04));
     else o.kperm = 0.0;
     double sig_eff = fmax2(0.0, o.rho * gz * h - p);
     double sig_0 = 0.0;
@@ -132,9 +135,9 @@ DC_HD SetVars setvars(const dclaw_params& P, double phi, double h, double u, dou
     if (Nnum <= 0.0) o.m_eq = P.m_crit;
     else o.m_eq = P.m_crit * (sqrt(Nden) / (sqrt(Nden) + sqrt(Nnum)));
     o.tanpsi = P.c1 * (m - o.m_eq);
-    double psi = atan(P.c1 * (m - o.m_eq));
-    double tau = sig_eff * tan(phi + psi);
-    o.tau = tau * 0.5 * (1.0 + tanh(100.0 * (m - 0.1)));
+    double psi = em::d_atan(P.c1 * (m - o.m_eq));
+    double tau = sig_eff * em::d_tan(phi + psi);
+    o.tau = tau * 0.5 * (1.0 + em::d_tanh(100.0 * (m - 0.1)));
     return o;
 }
 
@@ -546,15 +549,15 @@ DC_HD void mp_update_relax(const dclaw_params& P, double phi, double dt, double&
     double zeta = 3.0 * sv.alphainv / (h * 2.0) + (rho - P.rho_f) * P.rho_f * gz / (4.0 * rho);
     double krate = -zeta * 2.0 * sv.kperm / (h * fmax2(P.mu, 1.0e-16));
     double p_eq = P.rho_f * h * gz;
-    p = p_eq + (p - p_eq) * exp(krate * dt);
+    p = p_eq + (p - p_eq) * em::d_exp(krate * dt);
     double p_exc = p - P.rho_f * gz * h;
     qfix_cmass(P, h, m, p, rho, p_exc, hu, hv, hm, u, v, rhoh, gz);
     double D = -2.0 * (sv.kperm / (P.mu * h)) * p_exc;
     krate = D * (rho - P.rho_f) / rhoh;
-    hm = hm * exp(-dt * D * P.rho_f / (rhoh));
+    hm = hm * em::d_exp(-dt * D * P.rho_f / (rhoh));
     if (P.src2method == 0) {
         h = h + h * krate * dt;
-        double e = exp(dt * krate);
+        double e = em::d_exp(dt * krate);
         hu = hu * e;
         hv = hv * e;
         qfix(P, h, hu, hv, hm, p, u, v, m, gz);
@@ -586,7 +589,7 @@ DC_HD void src2_cell(const dclaw_params& P, double phi, double dt, double& qh, d
     double vnorm = hvnorm0 / h;
     if (hvnorm0 > 0.0) {
         vnorm = fmax2(0.0, vnorm - dt * sv.tau / rhoh);
-        vnorm = vnorm * exp(-(1.0 - m) * 2.0 * P.mu * dt / (h * rhoh));
+        vnorm = vnorm * em::d_exp(-(1.0 - m) * 2.0 * P.mu * dt / (h * rhoh));
         double hvnorm = h * vnorm;
         hu = hvnorm * hu / hvnorm0 + gx * h * dt;
         hv = hvnorm * hv / hvnorm0;
@@ -607,9 +610,9 @@ DC_HD void src2_cell(const dclaw_params& P, double phi, double dt, double& qh, d
         if (h <= P.friction_depth) {
             double cm = P.manning_coefficient;
             if (P.dd_manning)
-                cm = P.manning_max + (P.manning_coefficient - P.manning_max) * 0.5 * (1.0 + tanh(300.0 * (h - 0.05)));
+                cm = P.manning_max + (P.manning_coefficient - P.manning_max) * 0.5 * (1.0 + em::d_tanh(300.0 * (h - 0.05)));
             double beta = 1.0;
-            double gamma = beta * sqrt(sq(hu) + sq(hv)) * (gz * sq(cm)) / (pow(h, 7.0 / 3.0));
+            double gamma = beta * sqrt(sq(hu) + sq(hv)) * (gz * sq(cm)) / (em::d_pow_7_3(h));
             double dgamma = 1.0 + dt * gamma;
             hu = hu / dgamma;
             hv = hv / dgamma;

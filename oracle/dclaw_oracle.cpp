@@ -38,6 +38,7 @@
  * aux(10, ...) are kept (field fastest), mbc = 2.
  */
 #include "../include/dclaw_b200.h"
+#include "../dclaw_b200/csrc/elementary.cuh"
 
 #include <cmath>
 #include <cstdint>
@@ -66,6 +67,16 @@ inline uint32_t br_lim(int mw, uint32_t code) { return code << (8 + 3 * (mw - 1)
 inline uint32_t br_up(int mw) { return 1u << (23 + (mw - 1)); }
 
 inline double sq(double x) { return x * x; }
+
+// Elementary functions. Default: glibc libm, as gfortran on x86-64 Linux
+// links it. Portable mode: the deterministic functions the CUDA step uses
+// (dclaw_b200/csrc/elementary.cuh), for bit-exact GPU/oracle comparisons.
+int g_portable_libm = 0;
+inline double E_exp(double x) { return g_portable_libm ? dclaw::em::d_exp(x) : std::exp(x); }
+inline double E_atan(double x) { return g_portable_libm ? dclaw::em::d_atan(x) : std::atan(x); }
+inline double E_tan(double x) { return g_portable_libm ? dclaw::em::d_tan(x) : std::tan(x); }
+inline double E_tanh(double x) { return g_portable_libm ? dclaw::em::d_tanh(x) : std::tanh(x); }
+inline double E_pow73(double x) { return g_portable_libm ? dclaw::em::d_pow_7_3(x) : std::pow(x, 7.0 / 3.0); }
 // Fortran MAX/MIN with two arguments
 inline double fmax2(double a, double b) { return a > b ? a : b; }
 inline double fmin2(double a, double b) { return a < b ? a : b; }
@@ -129,7 +140,7 @@ void setvars(const Model& M, double h, double u, double v, double m, double p, d
     const dclaw_params& P = M.p;
     rho = m * (P.rho_s - P.rho_f) + P.rho_f;
     double kr_chi = 1.0;
-    kperm = kr_chi * P.kref * std::exp(-(m - P.mref) / (0.04));
+    kperm = kr_chi * P.kref * E_exp(-(m - P.mref) / (0.04));
     double sig_eff = fmax2(0.0, rho * gz * h - p);
     double sig_0 = 0.0;
     if (P.alphamethod == 0) {
@@ -147,9 +158,9 @@ void setvars(const Model& M, double h, double u, double v, double m, double p, d
     if (Nnum <= 0.0) m_eq = P.m_crit;
     else m_eq = P.m_crit * (std::sqrt(Nden) / (std::sqrt(Nden) + std::sqrt(Nnum)));
     tanpsi = P.c1 * (m - m_eq);
-    double psi = std::atan(P.c1 * (m - m_eq));
-    tau = sig_eff * std::tan(M.phi + psi);
-    tau = tau * 0.5 * (1.0 + std::tanh(100.0 * (m - 0.1)));
+    double psi = E_atan(P.c1 * (m - m_eq));
+    tau = sig_eff * E_tan(M.phi + psi);
+    tau = tau * 0.5 * (1.0 + E_tanh(100.0 * (m - 0.1)));
 }
 
 // ---------------------------------------------------------------------------
@@ -1196,17 +1207,17 @@ void mp_update_relax_Dclaw4(Model& M, double dt, double& h, double& u, double& v
     double zeta = 3.0 * alphainv / (h * 2.0) + (rho - P.rho_f) * P.rho_f * gz / (4.0 * rho);
     double krate = -zeta * 2.0 * kperm / (h * fmax2(P.mu, 1.0e-16));
     double p_eq = P.rho_f * h * gz;
-    p = p_eq + (p - p_eq) * std::exp(krate * dt);
+    p = p_eq + (p - p_eq) * E_exp(krate * dt);
     double p_exc = p - P.rho_f * gz * h;
     qfix_cmass(M, h, m, p, rho, p_exc, hu, hv, hm, u, v, rhoh, gz);
     double D = -2.0 * (kperm / (P.mu * h)) * p_exc;
     krate = D * (rho - P.rho_f) / rhoh;
-    hm = hm * std::exp(-dt * D * P.rho_f / (rhoh));
+    hm = hm * E_exp(-dt * D * P.rho_f / (rhoh));
     if (P.src2method == 0) {
         h = h + h * krate * dt;
         hchi = h * chi;
-        hu = hu * std::exp(dt * krate);
-        hv = hv * std::exp(dt * krate);
+        hu = hu * E_exp(dt * krate);
+        hv = hv * E_exp(dt * krate);
         qfix(M, h, hu, hv, hm, p, hchi, u, v, m, chi, rho, gz);
     } else if (P.src2method == 1) {
         h = (rhoh - hm * (P.rho_s - P.rho_f)) / P.rho_f;
@@ -1246,7 +1257,7 @@ void src2(Model& M, Patch& pt, double dt) {
             double vnorm = hvnorm0 / h;
             if (hvnorm0 > 0.0) {
                 vnorm = fmax2(0.0, vnorm - dt * tau / rhoh);
-                vnorm = vnorm * std::exp(-(1.0 - m) * 2.0 * P.mu * dt / (h * rhoh));
+                vnorm = vnorm * E_exp(-(1.0 - m) * 2.0 * P.mu * dt / (h * rhoh));
                 double hvnorm = h * vnorm;
                 hu = hvnorm * hu / hvnorm0 + gx * h * dt;
                 hv = hvnorm * hv / hvnorm0;
@@ -1272,9 +1283,9 @@ void src2(Model& M, Patch& pt, double dt) {
                     double cm = coeffmanning;
                     if (P.dd_manning)
                         cm = P.manning_max + (P.manning_coefficient - P.manning_max) * 0.5
-                             * (1.0 + std::tanh(300.0 * (h - 0.05)));
+                             * (1.0 + E_tanh(300.0 * (h - 0.05)));
                     double beta = 1.0;
-                    double gamma = beta * std::sqrt(sq(hu) + sq(hv)) * (gz * sq(cm)) / (std::pow(h, 7.0 / 3.0));
+                    double gamma = beta * std::sqrt(sq(hu) + sq(hv)) * (gz * sq(cm)) / (E_pow73(h));
                     double dgamma = 1.0 + dt * gamma;
                     hu = hu / dgamma;
                     hv = hv / dgamma;
@@ -1405,6 +1416,23 @@ Model make_model(const dclaw_params* p) {
 extern "C" {
 
 int oracle_version(void) { return 1; }
+
+/* 0: glibc libm (default), 1: the project's portable elementary functions */
+int oracle_set_libm(int portable) {
+    g_portable_libm = portable ? 1 : 0;
+    return g_portable_libm;
+}
+
+double oracle_elementary(int which, double x) {
+    switch (which) {
+        case 0: return dclaw::em::d_exp(x);
+        case 1: return dclaw::em::d_atan(x);
+        case 2: return dclaw::em::d_tan(x);
+        case 3: return dclaw::em::d_tanh(x);
+        case 4: return dclaw::em::d_pow_7_3(x);
+        default: return 0.0;
+    }
+}
 
 int oracle_threads(int n) {
 #ifdef _OPENMP

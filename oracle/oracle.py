@@ -31,7 +31,8 @@ def lib_path() -> Path:
 
 def build(force: bool = False) -> Path:
     """Compile the oracle into oracle/liboracle.so (g++, OpenMP)."""
-    if _LIB.exists() and not force and _LIB.stat().st_mtime >= SRC.stat().st_mtime:
+    deps = [SRC, HERE.parent / "dclaw_b200" / "csrc" / "elementary.cuh", HERE.parent / "include" / "dclaw_b200.h"]
+    if _LIB.exists() and not force and all(_LIB.stat().st_mtime >= d.stat().st_mtime for d in deps):
         return _LIB
     cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC",
            "-shared", str(SRC), "-o", str(_LIB) + ".tmp"]
@@ -67,16 +68,32 @@ class Oracle:
         L.oracle_step2.argtypes = [ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _dp, ctypes.c_int, _up, _up]
         L.oracle_src2.argtypes = [ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp]
+        L.oracle_set_libm.restype = ctypes.c_int
+        L.oracle_set_libm.argtypes = [ctypes.c_int]
+        L.oracle_elementary.restype = ctypes.c_double
+        L.oracle_elementary.argtypes = [ctypes.c_int, ctypes.c_double]
         L.oracle_qfix.argtypes = [ctypes.POINTER(CParams), _dp, _dp]
         L.oracle_setvars.argtypes = [ctypes.POINTER(CParams), _dp, _dp]
 
     def threads(self, n: int = 0) -> int:
         return self.lib.oracle_threads(n)
 
+    def set_libm(self, libm: str) -> None:
+        """'glibc' (default; gfortran on x86-64 Linux links glibc's libm) or
+        'portable' (the deterministic elementary functions the CUDA step uses)."""
+        if libm not in ("glibc", "portable"):
+            raise ValueError(libm)
+        self.lib.oracle_set_libm(1 if libm == "portable" else 0)
+
+    def elementary(self, name: str, x: float) -> float:
+        """The portable elementary function `name` (exp, atan, tan, tanh, pow73) at x."""
+        return self.lib.oracle_elementary(["exp", "atan", "tan", "tanh", "pow73"].index(name), float(x))
+
     def run(self, p: DClawParams, q: np.ndarray, b: np.ndarray, dx: float, dy: float, nsteps: int,
             dt_initial: float, t_final: float = 0.0, fixed_dt: bool = False, parallel: bool = True,
-            branch_log: bool = False):
+            branch_log: bool = False, libm: str = "glibc"):
         """Advance q (5, my, mx) by nsteps; returns dict(q, dt, cfl, t, status, xlog, ylog)."""
+        self.set_libm(libm)
         q = np.ascontiguousarray(q, dtype=np.float64).copy()
         b = np.ascontiguousarray(b, dtype=np.float64)
         _, my, mx = q.shape
@@ -108,7 +125,8 @@ class Oracle:
         self.lib.oracle_setaux(ctypes.byref(cp), mx, my, _ptr(b), _ptr(aux))
         return aux
 
-    def b4step2(self, p: DClawParams, q: np.ndarray, aux: np.ndarray, dx: float, dy: float):
+    def b4step2(self, p: DClawParams, q: np.ndarray, aux: np.ndarray, dx: float, dy: float, libm: str = "glibc"):
+        self.set_libm(libm)
         q = np.ascontiguousarray(q, dtype=np.float64).copy()
         aux = np.ascontiguousarray(aux, dtype=np.float64).copy()
         my, mx = q.shape[1] - 4, q.shape[2] - 4
@@ -117,7 +135,8 @@ class Oracle:
         return q, aux
 
     def step2(self, p: DClawParams, q: np.ndarray, aux: np.ndarray, dx: float, dy: float, dt: float,
-              parallel: bool = False, fluxes: bool = False, branch_log: bool = False):
+              parallel: bool = False, fluxes: bool = False, branch_log: bool = False, libm: str = "glibc"):
+        self.set_libm(libm)
         q = np.ascontiguousarray(q, dtype=np.float64).copy()
         aux = np.ascontiguousarray(aux, dtype=np.float64)
         my, mx = q.shape[1] - 4, q.shape[2] - 4
@@ -130,7 +149,8 @@ class Oracle:
                               int(parallel), _ptr(xlog, _up), _ptr(ylog, _up))
         return dict(q=q, cfl=float(cfl[0]), fluxes=fl, xlog=xlog, ylog=ylog)
 
-    def src2(self, p: DClawParams, q: np.ndarray, aux: np.ndarray, dt: float) -> np.ndarray:
+    def src2(self, p: DClawParams, q: np.ndarray, aux: np.ndarray, dt: float, libm: str = "glibc") -> np.ndarray:
+        self.set_libm(libm)
         q = np.ascontiguousarray(q, dtype=np.float64).copy()
         aux = np.ascontiguousarray(aux, dtype=np.float64)
         my, mx = q.shape[1] - 4, q.shape[2] - 4

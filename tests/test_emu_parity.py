@@ -1,7 +1,7 @@
 """The CUDA step's stage arithmetic (dclaw_b200/csrc/stages.cuh) run on the
 host against the oracle: bit-identical state, dt/Courant histories and
-branch bits. Host libm is glibc on both sides here, so any difference is a
-logic or operation-order error in the device code."""
+branch bits. The oracle runs with the same portable elementary functions as
+the device code, so any difference is a logic or operation-order error."""
 import numpy as np
 import pytest
 
@@ -16,7 +16,7 @@ def emu():
 
 
 def _cmp(oracle, emu, c, n):
-    r1 = oracle.run(c.params, c.q, c.b, c.dx, c.dy, n, c.dt_initial, branch_log=True)
+    r1 = oracle.run(c.params, c.q, c.b, c.dx, c.dy, n, c.dt_initial, branch_log=True, libm="portable")
     r2 = emu.run(c.params, c.q, c.b, c.dx, c.dy, n, c.dt_initial)
     br1 = np.concatenate([r1["xlog"].ravel(), r1["ylog"].ravel()])
     assert r1["status"] == r2["status"] == 0

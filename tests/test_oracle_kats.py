@@ -6,13 +6,18 @@ preservation, dry dam-break front bound) and
 differentiable_dclaw/tests/test_lake_at_rest.py:42 (well-balancing, 1e-8).
 """
 import numpy as np
+import pytest
 
 from dclaw_b200 import workloads as W
 
 
-def test_contact_wave_kat(oracle):
+LIBMS = ["glibc", "portable"]
+
+
+@pytest.mark.parametrize("libm", LIBMS)
+def test_contact_wave_kat(oracle, libm):
     c = W.contact_wave()
-    r = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 420, c.dt_initial, t_final=2.0)
+    r = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 420, c.dt_initial, t_final=2.0, libm=libm)
     assert r["status"] == 0
     assert abs(r["t"] - 2.0) < 1e-12
     q = r["q"]
@@ -30,10 +35,11 @@ def test_contact_wave_kat(oracle):
     assert abs(x[i1] - x[i0]) <= 1e-6        # check.py:80
 
 
-def test_dam_front_kat(oracle):
+@pytest.mark.parametrize("libm", LIBMS)
+def test_dam_front_kat(oracle, libm):
     c = W.dam_front()
     for T in (0.2, 0.5, 1.0):
-        r = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 400, c.dt_initial, t_final=T)
+        r = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 400, c.dt_initial, t_final=T, libm=libm)
         assert r["status"] == 0 and abs(r["t"] - T) < 1e-12
         h = r["q"][0][c.my // 2]
         x = (np.arange(c.mx) + 0.5) * c.dx
@@ -43,9 +49,10 @@ def test_dam_front_kat(oracle):
         assert front > 5.0 + 0.5 * np.sqrt(9.81 * 2.0) * T          # the front does move
 
 
-def test_lake_at_rest_kat(oracle):
+@pytest.mark.parametrize("libm", LIBMS)
+def test_lake_at_rest_kat(oracle, libm):
     c = W.lake_at_rest()
-    r = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 400, c.dt_initial, t_final=60.0)
+    r = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 400, c.dt_initial, t_final=60.0, libm=libm)
     q = r["q"]
     wet = q[0] > 0.01
     max_u = np.abs(np.where(wet, q[1] / np.maximum(q[0], 1e-9), 0.0)).max()
@@ -78,3 +85,15 @@ def test_pointwise_qfix_and_setvars(oracle):
     assert rho == 0.6 * (2700.0 - 1000.0) + 1000.0
     assert m_eq == 0.64 and abs(tanpsi - (0.6 - 0.64)) < 1e-15
     assert kperm == 1e-10 * np.exp(-(0.6 - 0.6) / 0.04)
+
+
+def test_libm_sensitivity_one_step(oracle):
+    """One step with glibc vs the portable elementary functions: the states
+    agree to 1e-13, the dry/wet masks exactly."""
+    c = W.slope_runout()
+    r0 = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 30, c.dt_initial, libm="glibc")
+    a = oracle.run(c.params, r0["q"], c.b, c.dx, c.dy, 1, 0.1, fixed_dt=True, libm="glibc")
+    b = oracle.run(c.params, r0["q"], c.b, c.dx, c.dy, 1, 0.1, fixed_dt=True, libm="portable")
+    assert np.array_equal(a["q"][0] == 0, b["q"][0] == 0)
+    for m in range(5):
+        assert np.abs(a["q"][m] - b["q"][m]).max() <= 1e-13 * np.abs(a["q"][m]).max()
