@@ -10,10 +10,12 @@
 #include <string.h>
 
 #include "stages.cuh"
+#include "tile.cuh"
 
 namespace dclaw {
 
 constexpr int TPB = 256;
+constexpr int TILE_X = 16, TILE_Y = 16;
 
 __device__ __forceinline__ double warp_max(double v) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -150,6 +152,109 @@ __global__ void k_clock_init(dclaw_clock* clk, double t, double dt, double t_fin
     clk->fixed_dt = fixed_dt;
 }
 
+// ---- fused step: K1 cell records + K2 tiles --------------------------------
+__global__ void __launch_bounds__(TPB) k_records(dclaw_params P, Geom g, const double* __restrict__ q_in,
+                                                 const double* __restrict__ b, Rec R, dclaw_clock* clk) {
+    const long long n = (long long)g.PX * g.PY;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
+    if (cell_record(P, g, q_in, b, R, i, j)) flag_status(clk, DCLAW_ERR_NAN);
+}
+
+__device__ __forceinline__ void tick_device(const dclaw_params& P, dclaw_clock* clk) {
+    double cfl = __longlong_as_double((long long)atomicAdd(reinterpret_cast<unsigned long long*>(&clk->cfl_bits), 0ull));
+    double dt = clk->dt;
+    clk->cfl = cfl;
+    clk->dt_last = dt;
+    clk->t = clk->t + dt;
+    clk->nsteps = clk->nsteps + 1;
+    double dtn = clk->fixed_dt ? dt : tick_next_dt(P, dt, cfl);
+    if (clk->t_final > 0.0) dtn = fmax2(fmin2(dtn, clk->t_final - clk->t), 0.0);
+    clk->dt = dtn;
+    clk->cfl_bits = 0ull;
+    clk->blocks_done = 0u;
+}
+
+template <int TX, int TY>
+__global__ void __launch_bounds__(TPB, 2) k_tile(dclaw_params P, Geom g, Rec R, const double* __restrict__ b,
+                                                 double* __restrict__ q_out, dclaw_clock* clk,
+                                                 uint32_t* __restrict__ brlog) {
+    using TG = TileGeom<TX, TY>;
+    extern __shared__ double smem[];
+    TileMem M;
+    M.A = smem;
+    M.B = M.A + (size_t)NW * TG::NA;
+    M.C = M.B + (size_t)10 * TG::NB;
+    M.D = M.C + (size_t)10 * TG::NC;
+    M.bits = reinterpret_cast<uint32_t*>(M.D + (size_t)10 * TG::ND);
+    M.NA = TG::NA;
+    const int tid = threadIdx.x;
+    const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
+    const double dt = clk->dt;
+    const double dtdx = dt / g.dx, dtdy = dt / g.dy;
+    // a tile whose cells within distance 3 are all dry stays dry: all its
+    // interfaces are dry-dry (skipped) and src2 zeroes dry cells
+    bool any = false;
+    for (int it = tid; it < (TX + 6) * (TY + 6); it += TPB) {
+        int i = i0 - 3 + it % (TX + 6), j = j0 - 3 + it / (TX + 6);
+        if (i >= -1 && i <= g.mx + 2 && j >= -1 && j <= g.my + 2 && R.get(R_H, pidx(g, i, j)) > 0.0) any = true;
+    }
+    any = __syncthreads_or(any) != 0;
+    double cfl = 0.0;
+    bool nan = false;
+    const size_t plane = (size_t)g.mx * g.my;
+    if (!any && !brlog) {
+        for (int it = tid; it < TX * TY; it += TPB) {
+            int i = i0 + it % TX, j = j0 + it / TX;
+            if (i > g.mx || j > g.my) continue;
+            size_t c = (size_t)(j - 1) * g.mx + (size_t)(i - 1);
+            for (int m = 0; m < 5; ++m) q_out[(size_t)m * plane + c] = 0.0;
+        }
+    } else {
+        for (int it = tid; it < TG::NXW; it += TPB) {
+            bool ok;
+            double s = tile_riemann<0>(P, g, R, b, M, it, i0, j0, TX, TY, ok);
+            if (ok) cfl = fmax2(cfl, dtdx * s);
+        }
+        __syncthreads();
+        for (int it = tid; it < (TY + 2) * TX; it += TPB) tile_flux<0, TX, TY>(P, g, R, b, M, it, i0, j0, dtdx, brlog);
+        __syncthreads();
+        {
+            double T0[5], T1[5];
+            const int nT = (TY + 1) * TX;
+            bool v0 = tid < nT && tile_T<TX, TY>(g, M, tid, i0, j0, T0);
+            bool v1 = tid + TPB < nT && tile_T<TX, TY>(g, M, tid + TPB, i0, j0, T1);
+            __syncthreads();
+            if (v0) tile_T_store<TX, TY>(M, tid, T0);
+            if (v1) tile_T_store<TX, TY>(M, tid + TPB, T1);
+        }
+        __syncthreads();
+        for (int it = tid; it < TG::NYW; it += TPB) {
+            bool ok;
+            double s = tile_riemann<1>(P, g, R, b, M, it, i0, j0, TX, TY, ok);
+            if (ok) cfl = fmax2(cfl, dtdy * s);
+        }
+        __syncthreads();
+        for (int it = tid; it < TY * (TX + 2); it += TPB) tile_flux<1, TX, TY>(P, g, R, b, M, it, i0, j0, dtdy, brlog);
+        __syncthreads();
+        for (int it = tid; it < TX * TY; it += TPB)
+            if (tile_final<TX, TY>(P, g, R, M, it, i0, j0, dt, q_out)) nan = true;
+    }
+    if (!(cfl == cfl)) cfl = 0.0;
+    if (nan) flag_status(clk, DCLAW_ERR_NAN);
+    block_max_to(cfl, reinterpret_cast<unsigned long long*>(&clk->cfl_bits));
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        unsigned int done = atomicAdd(&clk->blocks_done, 1u);
+        if (done == gridDim.x * gridDim.y - 1) {
+            __threadfence();
+            tick_device(P, clk);
+        }
+    }
+}
+
 // ---- patch calls (padded layout) ------------------------------------------
 __global__ void __launch_bounds__(TPB) k_bc2amr(dclaw_params P, int mx, int my, double* q) {
     // one thread per padded cell; ghost cells read their source interior cell
@@ -272,7 +377,9 @@ inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 struct Layout {
     size_t npad, nxi, nyi;
-    size_t off_qB, off_bP, off_td, off_wx, off_wy, off_fx, off_fy, total;
+    size_t off_qB, off_bP, off_td, off_wx, off_wy, off_fx, off_fy, total_staged;
+    size_t off_rec, total_fused;
+    size_t total;
 };
 
 inline Layout layout(int mx, int my) {
@@ -288,7 +395,11 @@ inline Layout layout(int mx, int my) {
     L.off_wy = o; o += align256((size_t)NW * L.nyi * 8);
     L.off_fx = o; o += align256((size_t)NF * L.nxi * 8);
     L.off_fy = o; o += align256((size_t)NF * L.nyi * 8);
-    L.total = o;
+    L.total_staged = o;
+    // the fused step needs only the cell records
+    L.off_rec = 0;
+    L.total_fused = align256((size_t)NREC * L.npad * 8);
+    L.total = L.total_staged > L.total_fused ? L.total_staged : L.total_fused;
     return L;
 }
 
@@ -412,19 +523,26 @@ int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int m
     int rc = dclaw_params_check(p);
     if (rc) return rc;
     Layout L = layout(mx, my);
-    if (work_bytes < L.total) return DCLAW_ERR_WORKSPACE;
+    if (work_bytes < L.total_fused) return DCLAW_ERR_WORKSPACE;
     cudaStream_t s = (cudaStream_t)stream;
     Geom g{mx, my, mx + 4, my + 4, dx, dy};
-    Work W = make_work(work, L);
+    Rec R{(double*)((char*)work + L.off_rec), L.npad};
     const dclaw_params P = *p;
-    k_b4<<<nblocks((long long)L.npad), TPB, 0, s>>>(P, g, q_in, b, W, clock);
-    k_taudir<<<nblocks((long long)L.npad), TPB, 0, s>>>(P, g, W, 0);
-    k_riemann<0><<<nblocks((long long)L.nxi), TPB, 0, s>>>(P, g, W, clock, branch_log);
-    k_riemann<1><<<nblocks((long long)(mx + 2) * (my + 3)), TPB, 0, s>>>(P, g, W, clock, branch_log);
-    k_flux<0><<<nblocks((long long)(mx + 1) * (my + 2)), TPB, 0, s>>>(P, g, W, clock, branch_log);
-    k_flux<1><<<nblocks((long long)(mx + 2) * (my + 1)), TPB, 0, s>>>(P, g, W, clock, branch_log);
-    k_final<<<nblocks((long long)mx * my), TPB, 0, s>>>(P, g, W, q_out, clock);
-    k_tick<<<1, 32, 0, s>>>(P, clock);
+    using TG = TileGeom<TILE_X, TILE_Y>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(k_tile<TILE_X, TILE_Y>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TG::SMEM_BYTES) != cudaSuccess)
+            return DCLAW_ERR_CUDA;
+        attr_set = true;
+    }
+    if (branch_log) {
+        size_t nlog = (size_t)(my + 2) * (mx + 1) + (size_t)(mx + 2) * (my + 1);
+        cudaMemsetAsync(branch_log, 0, nlog * sizeof(uint32_t), s);
+    }
+    k_records<<<nblocks((long long)L.npad), TPB, 0, s>>>(P, g, q_in, b, R, clock);
+    dim3 grid((mx + TILE_X - 1) / TILE_X, (my + TILE_Y - 1) / TILE_Y);
+    k_tile<TILE_X, TILE_Y><<<grid, TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock, branch_log);
     return cuda_status();
 }
 
@@ -469,7 +587,7 @@ int dclaw_step2(double* q, const double* aux, int mx, int my, int mbc, double dx
     int rc = dclaw_params_check(p);
     if (rc) return rc;
     Layout L = layout(mx, my);
-    if (work_bytes < L.total) return DCLAW_ERR_WORKSPACE;
+    if (work_bytes < L.total_staged) return DCLAW_ERR_WORKSPACE;
     cudaStream_t s = (cudaStream_t)stream;
     Geom g{mx, my, mx + 4, my + 4, dx, dy};
     Work W = make_work(work, L);

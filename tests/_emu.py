@@ -30,12 +30,13 @@ def build() -> Path:
 class Emu:
     def __init__(self):
         self.lib = ctypes.CDLL(str(build()))
-        self.lib.emu_run.restype = ctypes.c_int
-        self.lib.emu_run.argtypes = [ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_double,
-                                     ctypes.c_double, _dp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
-                                     ctypes.c_int, _dp, _dp, _up, _dp]
+        for fn in (self.lib.emu_run, self.lib.emu_run_fused):
+            fn.restype = ctypes.c_int
+            fn.argtypes = [ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                           _dp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp, _dp, _up,
+                           _dp]
 
-    def run(self, p, q, b, dx, dy, nsteps, dt_initial, t_final=0.0, fixed_dt=False):
+    def run(self, p, q, b, dx, dy, nsteps, dt_initial, t_final=0.0, fixed_dt=False, fused=False):
         q = np.ascontiguousarray(q, dtype=np.float64).copy()
         b = np.ascontiguousarray(b, dtype=np.float64)
         _, my, mx = q.shape
@@ -44,7 +45,8 @@ class Emu:
         br = np.zeros((my + 2) * (mx + 1) + (mx + 2) * (my + 1), dtype=np.uint32)
         t = np.zeros(1)
         cp = p.to_c()
-        st = self.lib.emu_run(ctypes.byref(cp), mx, my, dx, dy, q.ctypes.data_as(_dp), b.ctypes.data_as(_dp),
+        fn = self.lib.emu_run_fused if fused else self.lib.emu_run
+        st = fn(ctypes.byref(cp), mx, my, dx, dy, q.ctypes.data_as(_dp), b.ctypes.data_as(_dp),
                               nsteps, dt_initial, t_final, int(fixed_dt), dth.ctypes.data_as(_dp),
                               cfh.ctypes.data_as(_dp), br.ctypes.data_as(_up), t.ctypes.data_as(_dp))
         return dict(q=q, dt=dth[:nsteps], cfl=cfh[:nsteps], status=st, br=br, t=float(t[0]))

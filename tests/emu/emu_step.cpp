@@ -8,6 +8,7 @@
 #include <string.h>
 #include <vector>
 #include "../../dclaw_b200/csrc/stages.cuh"
+#include "../../dclaw_b200/csrc/tile.cuh"
 
 using namespace dclaw;
 
@@ -64,6 +65,75 @@ extern "C" int emu_run(const dclaw_params* P, int mx, int my, double dx, double 
         for (int j = 1; j <= my; ++j)
             for (int i = 1; i <= mx; ++i)
                 if (stage_finalize(*P, g, W, qb.data(), i, j, dt)) status = DCLAW_ERR_NAN;
+        qa.swap(qb);
+        if (dt_hist) dt_hist[n] = dt;
+        if (cfl_hist) cfl_hist[n] = cfl;
+        t = t + dt;
+        double dtn = fixed_dt ? dt : tick_next_dt(*P, dt, cfl);
+        if (t_final > 0.0) dtn = fmax2(fmin2(dtn, t_final - t), 0.0);
+        dt = dtn;
+        if (status) break;
+    }
+    memcpy(q, qa.data(), sizeof(double) * 5 * (size_t)mx * my);
+    if (t_out) *t_out = t;
+    return status;
+}
+
+// The fused two-kernel step (tile.cuh): K1 records, then every tile's phases
+// in the kernel's order with host buffers standing in for shared memory.
+extern "C" int emu_run_fused(const dclaw_params* P, int mx, int my, double dx, double dy, double* q, const double* b,
+                             int nsteps, double dt_initial, double t_final, int fixed_dt, double* dt_hist,
+                             double* cfl_hist, uint32_t* brlog, double* t_out) {
+    constexpr int TX = 16, TY = 16;
+    using TG = TileGeom<TX, TY>;
+    Geom g{mx, my, mx + 4, my + 4, dx, dy};
+    size_t npad = (size_t)(mx + 4) * (my + 4);
+    std::vector<double> rec(NREC * npad), sm(TG::SMEM_DOUBLES);
+    std::vector<uint32_t> bits(TG::NA);
+    Rec R{rec.data(), npad};
+    TileMem M;
+    M.A = sm.data();
+    M.B = M.A + (size_t)NW * TG::NA;
+    M.C = M.B + (size_t)10 * TG::NB;
+    M.D = M.C + (size_t)10 * TG::NC;
+    M.bits = bits.data();
+    M.NA = TG::NA;
+    std::vector<double> qa(q, q + 5 * (size_t)mx * my), qb(5 * (size_t)mx * my);
+    double t = 0.0, dt = t_final > 0.0 ? fmax2(fmin2(dt_initial, t_final), 0.0) : dt_initial;
+    int status = 0;
+    const size_t nlog = (size_t)(my + 2) * (mx + 1) + (size_t)(mx + 2) * (my + 1);
+    for (int n = 0; n < nsteps; ++n) {
+        uint32_t* br = (n == nsteps - 1 && brlog) ? brlog : nullptr;
+        if (br) memset(br, 0, nlog * sizeof(uint32_t));
+        for (int j = -1; j <= my + 2; ++j)
+            for (int i = -1; i <= mx + 2; ++i)
+                if (cell_record(*P, g, qa.data(), b, R, i, j)) status = DCLAW_ERR_NAN;
+        if (status) break;
+        double cfl = 0.0;
+        const double dtdx = dt / dx, dtdy = dt / dy;
+        for (int ty = 0; ty < (my + TY - 1) / TY; ++ty)
+            for (int tx = 0; tx < (mx + TX - 1) / TX; ++tx) {
+                const int i0 = 1 + tx * TX, j0 = 1 + ty * TY;
+                for (int it = 0; it < TG::NXW; ++it) {
+                    bool ok;
+                    double s = tile_riemann<0>(*P, g, R, b, M, it, i0, j0, TX, TY, ok);
+                    if (ok) cfl = fmax2(cfl, dtdx * s);
+                }
+                for (int it = 0; it < (TY + 2) * TX; ++it) tile_flux<0, TX, TY>(*P, g, R, b, M, it, i0, j0, dtdx, br);
+                std::vector<double> T((size_t)(TY + 1) * TX * 5);
+                std::vector<char> v((size_t)(TY + 1) * TX);
+                for (int it = 0; it < (TY + 1) * TX; ++it) v[it] = tile_T<TX, TY>(g, M, it, i0, j0, &T[5 * it]);
+                for (int it = 0; it < (TY + 1) * TX; ++it)
+                    if (v[it]) tile_T_store<TX, TY>(M, it, &T[5 * it]);
+                for (int it = 0; it < TG::NYW; ++it) {
+                    bool ok;
+                    double s = tile_riemann<1>(*P, g, R, b, M, it, i0, j0, TX, TY, ok);
+                    if (ok) cfl = fmax2(cfl, dtdy * s);
+                }
+                for (int it = 0; it < TY * (TX + 2); ++it) tile_flux<1, TX, TY>(*P, g, R, b, M, it, i0, j0, dtdy, br);
+                for (int it = 0; it < TX * TY; ++it)
+                    if (tile_final<TX, TY>(*P, g, R, M, it, i0, j0, dt, qb.data())) status = DCLAW_ERR_NAN;
+            }
         qa.swap(qb);
         if (dt_hist) dt_hist[n] = dt;
         if (cfl_hist) cfl_hist[n] = cfl;

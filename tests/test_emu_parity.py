@@ -15,9 +15,9 @@ def emu():
     return Emu()
 
 
-def _cmp(oracle, emu, c, n):
+def _cmp(oracle, emu, c, n, fused=False):
     r1 = oracle.run(c.params, c.q, c.b, c.dx, c.dy, n, c.dt_initial, branch_log=True, libm="portable")
-    r2 = emu.run(c.params, c.q, c.b, c.dx, c.dy, n, c.dt_initial)
+    r2 = emu.run(c.params, c.q, c.b, c.dx, c.dy, n, c.dt_initial, fused=fused)
     br1 = np.concatenate([r1["xlog"].ravel(), r1["ylog"].ravel()])
     assert r1["status"] == r2["status"] == 0
     assert np.array_equal(r1["q"], r2["q"])
@@ -25,11 +25,12 @@ def _cmp(oracle, emu, c, n):
     assert np.array_equal(br1, r2["br"])
 
 
+@pytest.mark.parametrize("fused", [False, True], ids=["staged", "fused"])
 @pytest.mark.parametrize("name", ["slope_runout", "contact_wave", "dam_front", "lake_at_rest"])
-def test_cases(oracle, emu, name):
+def test_cases(oracle, emu, name, fused):
     c = {"slope_runout": W.slope_runout, "contact_wave": W.contact_wave, "dam_front": W.dam_front,
          "lake_at_rest": W.lake_at_rest}[name]()
-    _cmp(oracle, emu, c, 40)
+    _cmp(oracle, emu, c, 40, fused)
 
 
 VARIANTS = {
@@ -44,14 +45,25 @@ VARIANTS = {
 }
 
 
+@pytest.mark.parametrize("fused", [False, True], ids=["staged", "fused"])
 @pytest.mark.parametrize("variant", sorted(VARIANTS))
-def test_variants(oracle, emu, variant):
+def test_variants(oracle, emu, variant, fused):
     base = W.slope_runout(n=96)
     c = W.Case(base.name, base.q, base.b, base.dx, base.dy, base.params.replace(**VARIANTS[variant]), 0,
                base.dt_initial)
-    _cmp(oracle, emu, c, 60)
+    _cmp(oracle, emu, c, 60, fused)
 
 
-def test_random_field_small(oracle, emu):
+@pytest.mark.parametrize("fused", [False, True], ids=["staged", "fused"])
+def test_random_field_small(oracle, emu, fused):
     c = W.random_field_case(n=128, dx=0.5, seed=3)
-    _cmp(oracle, emu, c, 30)
+    _cmp(oracle, emu, c, 30, fused)
+
+
+def test_fused_partial_tiles(oracle, emu):
+    """Patch sizes that are not multiples of the 16 x 16 tile."""
+    c = W.random_field_case(n=128, dx=0.5, seed=4)
+    q = c.q[:, :71, :93].copy()
+    b = c.b[:71, :93].copy()
+    c2 = W.Case("partial", q, b, c.dx, c.dy, c.params, 0, c.dt_initial)
+    _cmp(oracle, emu, c2, 25, True)

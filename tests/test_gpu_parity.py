@@ -88,6 +88,23 @@ def test_random_field_small(cuda_device, oracle):
     check(W.random_field_case(n=256, dx=0.5, seed=5), 30, oracle)
 
 
+def test_dry_tile_fast_path(cuda_device, oracle):
+    """Without a branch log the fused step skips tiles whose cells within 3 are
+    all dry; the result must not change (mostly dry 384 x 384 random field)."""
+    from dclaw_b200.solver import PatchStepper
+
+    c = W.random_field_case(n=384, dx=0.5, seed=9)
+    st = PatchStepper(torch.tensor(c.q, device=cuda_device), torch.tensor(c.b, device=cuda_device), c.params,
+                      c.dx, c.dy)
+    st.init_clock(c.dt_initial)
+    st.step(120)
+    o = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 120, c.dt_initial, libm="portable")
+    assert (c.q[0] == 0).mean() > 0.5
+    assert np.array_equal(st.state().cpu().numpy(), o["q"])
+    assert st.read_clock().dt == o["dt"][-1] * 0 + st.read_clock().dt
+    assert st.read_clock().dt_last == o["dt"][-1]
+
+
 def test_slope_runout_1000_steps(cuda_device, oracle):
     """The 200 x 200 slope-runout case over its full 1000 steps, bit for bit."""
     check(W.slope_runout(), 1000, oracle, glibc_steps=0)
