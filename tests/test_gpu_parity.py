@@ -101,7 +101,6 @@ def test_dry_tile_fast_path(cuda_device, oracle):
     o = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 120, c.dt_initial, libm="portable")
     assert (c.q[0] == 0).mean() > 0.5
     assert np.array_equal(st.state().cpu().numpy(), o["q"])
-    assert st.read_clock().dt == o["dt"][-1] * 0 + st.read_clock().dt
     assert st.read_clock().dt_last == o["dt"][-1]
 
 
