@@ -424,6 +424,22 @@ inline int cuda_status() {
     return e == cudaSuccess ? DCLAW_OK : DCLAW_ERR_CUDA;
 }
 
+// the tile kernel's dynamic shared memory above 48 KB must be opted into
+// once per device (function attributes belong to the device's context)
+constexpr int MAX_DEVICES = 64;
+inline int ensure_tile_smem_attr() {
+    static bool done[MAX_DEVICES] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return DCLAW_ERR_CUDA;
+    if (!done[dev]) {
+        if (cudaFuncSetAttribute(k_tile<TILE_X, TILE_Y>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TileGeom<TILE_X, TILE_Y>::SMEM_BYTES) != cudaSuccess)
+            return DCLAW_ERR_CUDA;
+        done[dev] = true;
+    }
+    return DCLAW_OK;
+}
+
 inline bool sizes_ok(int mx, int my) {
     return mx >= 2 && my >= 2 && (long long)(mx + 4) * (my + 4) < (1LL << 40);
 }
@@ -529,13 +545,7 @@ int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int m
     Rec R{(double*)((char*)work + L.off_rec), L.npad};
     const dclaw_params P = *p;
     using TG = TileGeom<TILE_X, TILE_Y>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        if (cudaFuncSetAttribute(k_tile<TILE_X, TILE_Y>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)TG::SMEM_BYTES) != cudaSuccess)
-            return DCLAW_ERR_CUDA;
-        attr_set = true;
-    }
+    if (ensure_tile_smem_attr() != DCLAW_OK) return DCLAW_ERR_CUDA;
     if (branch_log) {
         size_t nlog = (size_t)(my + 2) * (mx + 1) + (size_t)(mx + 2) * (my + 1);
         cudaMemsetAsync(branch_log, 0, nlog * sizeof(uint32_t), s);

@@ -80,16 +80,13 @@ DC_HD bool cell_record(const dclaw_params& P, const Geom& g, const double* __res
     const size_t plane = (size_t)mx * my;
     const size_t c = (size_t)(sj - 1) * mx + (size_t)(si - 1);
     const size_t pi = pidx(g, i, j);
+    // every field is read: a NaN anywhere in the state is reported, as the
+    // reference's check4nans does before b4step2
     double h = q_in[c];
-    bool nan = (h != h);
-    double hu = 0.0, hv = 0.0, hm = 0.0, p = 0.0;
+    double hu = q_in[plane + c], hv = q_in[2 * plane + c], hm = q_in[3 * plane + c], p = q_in[4 * plane + c];
+    bool nan = (h != h) || (hu != hu) || (hv != hv) || (hm != hm) || (p != p);
     bool wet = h > P.dry_tolerance;
     if (wet) {
-        hu = q_in[plane + c];
-        hv = q_in[2 * plane + c];
-        hm = q_in[3 * plane + c];
-        p = q_in[4 * plane + c];
-        nan = nan || (hu != hu) || (hv != hv) || (hm != hm) || (p != p);
         if (flip_u) hu = -hu;
         if (flip_v) hv = -hv;
         double u, v, m;
@@ -102,6 +99,8 @@ DC_HD bool cell_record(const dclaw_params& P, const Geom& g, const double* __res
         }
     } else {
         h = 0.0;
+        hu = 0.0;
+        hv = 0.0;
     }
     R.put(R_H, pi, h);
     double fs = 0.0, tdx = 0.0, tdy = 0.0;
