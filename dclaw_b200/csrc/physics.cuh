@@ -35,6 +35,14 @@
 
 #include "elementary.cuh"
 
+// Large device routines can be compiled out of line (-DDCLAW_OUTLINE_BIG)
+// to shrink the tile kernel's code; inline is the default.
+#if defined(__CUDACC__) && defined(DCLAW_OUTLINE_BIG)
+#define DC_BIG __host__ __device__ __noinline__
+#else
+#define DC_BIG DC_HD
+#endif
+
 namespace dclaw {
 
 // branch bits recorded per interface (same meaning as the oracle's)
@@ -114,7 +122,7 @@ struct SetVars {
 
 // setvars with segregation = 0 (kr_chi = 1). `phi` is the basal friction angle.
 template <bool NEED_ALL>
-DC_HD SetVars setvars(const dclaw_params& P, double phi, double h, double u, double v,
+DC_BIG SetVars setvars(const dclaw_params& P, double phi, double h, double u, double v,
                                            double m, double p, double gz) {
     SetVars o;
     o.rho = m * (P.rho_s - P.rho_f) + P.rho_f;
@@ -247,7 +255,7 @@ struct Side {
 // L and R carry setvars (rho, tau) of their states; the mirrored ghost of a
 // wall problem has the same closures as its source because setvars depends
 // on the velocity only through u^2 + v^2.
-DC_HD Waves riemann_solve(const dclaw_params& P, Side L, Side R, uint32_t* br) {
+DC_BIG Waves riemann_solve(const dclaw_params& P, Side L, Side R, uint32_t* br) {
     const double grav = P.grav;
     const double drytol = P.dry_tolerance;
     double wall1 = 1.0, wall2 = 1.0, wall3 = 1.0;
@@ -481,7 +489,7 @@ DC_HD Waves riemann_solve(const dclaw_params& P, Side L, Side R, uint32_t* br) {
 // b = its bed, topo1/topo3 = bed of the neighbours below/above in the
 // transverse direction. asdq in (h, n, t, hm, p). Outputs bm/bp in the same
 // order. Returns false when the split is skipped.
-DC_HD bool rpt2_split(const dclaw_params& P, double h, double hn, double ht, double hm,
+DC_BIG bool rpt2_split(const dclaw_params& P, double h, double hn, double ht, double hm,
                                           double b, double topo1, double topo3, const double asdq[5],
                                           double bm[5], double bp[5]) {
     for (int k = 0; k < 5; ++k) { bm[k] = 0.0; bp[k] = 0.0; }
@@ -570,7 +578,7 @@ DC_HD void mp_update_relax(const dclaw_params& P, double phi, double dt, double&
 }
 
 // src2 on one interior cell (in place on the 5 conserved fields)
-DC_HD void src2_cell(const dclaw_params& P, double phi, double dt, double& qh, double& qhu,
+DC_BIG void src2_cell(const dclaw_params& P, double phi, double dt, double& qh, double& qhu,
                                           double& qhv, double& qhm, double& qp) {
     double h = qh;
     if (h <= P.dry_tolerance) {
