@@ -635,3 +635,52 @@ int dclaw_max_wave_speed(const double* q, int mx, int my, const dclaw_params* p,
 }
 
 }  // extern "C"
+
+// ---- allocation-free variant of the fused step ------------------------------
+// Scratch for the per-cell records of one patch of at most
+// NOALLOC_MAX_CELLS padded cells, in a fixed device array of this library
+// (NREC * 2^18 doubles = 28 MiB per device). Host code must not use the
+// symbol as an address: it is a host-side stand-in; the device address is
+// looked up once per device with cudaGetSymbolAddress.
+namespace dclaw {
+constexpr size_t NOALLOC_MAX_CELLS = (size_t)1 << 18;
+static __device__ __align__(256) double g_noalloc_scratch[(size_t)NREC * NOALLOC_MAX_CELLS];
+static double* g_noalloc_addr[MAX_DEVICES] = {};
+}  // namespace dclaw
+
+extern "C" {
+
+size_t dclaw_step_noalloc_max_cells(void) { return dclaw::NOALLOC_MAX_CELLS; }
+
+int dclaw_step_noalloc(const double* q_in, double* q_out, const double* b, int mx, int my, double dx, double dy,
+                       const dclaw_params* p, dclaw_clock* clock, void* stream) {
+    if (!q_in || !q_out || !b || !p || !clock || q_in == q_out) return DCLAW_ERR_ARG;
+    if (!sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0)) return DCLAW_ERR_ARG;
+    if ((size_t)(mx + 4) * (size_t)(my + 4) > NOALLOC_MAX_CELLS) return DCLAW_ERR_TOO_LARGE;
+    int rc = dclaw_params_check(p);
+    if (rc) return rc;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return DCLAW_ERR_CUDA;
+    if (!g_noalloc_addr[dev]) {
+        // set-up on first use on this device (this device is current here)
+        void* addr = nullptr;
+        if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return DCLAW_ERR_CUDA;
+        g_noalloc_addr[dev] = static_cast<double*>(addr);
+    }
+    if (ensure_tile_smem_attr() != DCLAW_OK) return DCLAW_ERR_CUDA;
+    // every record plane a tile reads is written by k_records in the same
+    // call (h, fsphi and taudir for every padded cell, the other planes for
+    // every wet cell, the only cells whose other planes are read), so the
+    // previous call's contents need no clearing
+    cudaStream_t s = (cudaStream_t)stream;
+    Geom g{mx, my, mx + 4, my + 4, dx, dy};
+    const size_t npad = (size_t)(mx + 4) * (my + 4);
+    Rec R{g_noalloc_addr[dev], npad};
+    const dclaw_params P = *p;
+    k_records<<<nblocks((long long)npad), TPB, 0, s>>>(P, g, q_in, b, R, clock);
+    dim3 grid((mx + TILE_X - 1) / TILE_X, (my + TILE_Y - 1) / TILE_Y);
+    k_tile<TILE_X, TILE_Y><<<grid, TPB, TileGeom<TILE_X, TILE_Y>::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock, nullptr);
+    return cuda_status();
+}
+
+}  // extern "C"

@@ -160,6 +160,28 @@ int dclaw_src2(double* q, const double* aux, int mx, int my, int mbc, double dx,
 int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int my,
                double dx, double dy, const dclaw_params* p, dclaw_clock* clock,
                void* work, size_t work_bytes, uint32_t* branch_log, void* stream);
+/* Allocation-free variant of dclaw_step. No counterpart in the reference:
+ * it exists for callers that drive the step from code with no device
+ * allocator of their own -- a Fortran time loop bound through iso_c_binding
+ * (gfortran has no CUDA allocation API), or a host application that owns all
+ * device memory and hands the step only the state it already holds -- and so
+ * cannot size and keep the workspace dclaw_step needs. Its scratch (the
+ * per-cell records) lives in a fixed 28 MiB device array inside the library,
+ * which every GPU that loads the library keeps until the process exits; the
+ * patch is limited to (mx+4)*(my+4) <= 262144 padded cells (e.g. 508 x 508),
+ * larger patches return DCLAW_ERR_TOO_LARGE without launching anything.
+ * It never calls cudaMalloc/cudaFree. The first call on a device looks up
+ * the array's device address (with that device current) and should come
+ * before any stream capture on that device. All calls on a device share the
+ * one array: calls whose work overlaps on the GPU (different streams, or
+ * different host threads without ordering) race and must not be issued.
+ * Arguments and results are those of dclaw_step without the workspace and
+ * the branch log. */
+int dclaw_step_noalloc(const double* q_in, double* q_out, const double* b, int mx, int my,
+                       double dx, double dy, const dclaw_params* p, dclaw_clock* clock,
+                       void* stream);
+/* largest patch (padded cells) dclaw_step_noalloc accepts */
+size_t dclaw_step_noalloc_max_cells(void);
 /* initialise a device clock: t, dt, t_final, fixed_dt; counters cleared */
 int dclaw_clock_init(dclaw_clock* clock, double t, double dt, double t_final, int fixed_dt,
                      void* stream);

@@ -23,7 +23,7 @@ def test_library_exports_every_declared_symbol():
     assert len(names) >= 12
     for n in names:
         assert hasattr(lib, n), n
-    assert set(names) <= set(_lib.SIGNATURES) | {"dclaw_step_noalloc"}
+    assert set(names) <= set(_lib.SIGNATURES)
 
 
 def test_host_side_helpers():
