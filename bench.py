@@ -262,9 +262,9 @@ def run_ours(args):
                           "transverse_waves": case.params.transverse_waves, "limiter": "MC"},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": None,
-                            "kernel": "fused step k_records + k_tile (88 B/cell-update algorithmic)",
+                            "kernel": "fused step k_records + k_tile + k_src2_cells (88 B/cell-update algorithmic)",
                             "peak_source": peak_kind},
-               "clocks": clocks, "gpu_launches": 2 * args.steps, "status": status}
+               "clocks": clocks, "gpu_launches": 3 * args.steps, "status": status}
         if e2e_ms is not None:
             out["e2e"] = {"value": cells * args.e2e_steps * world / (e2e_ms / 1000.0), "unit": "cell-updates/s",
                           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -15,7 +15,19 @@
 namespace dclaw {
 
 constexpr int TPB = 256;
-constexpr int TILE_X = 16, TILE_Y = 16;
+// tile of the fused step: with 16 x 14 the flux phases of k_tile fit in one
+// round of 256 threads (256 and 252 cells) and the solves in two
+#ifndef DCLAW_TILE_X
+#define DCLAW_TILE_X 16
+#endif
+#ifndef DCLAW_TILE_Y
+#define DCLAW_TILE_Y 14
+#endif
+// src2 in its own per-cell kernel (1) or as the tile kernel's last phase (0)
+#ifndef DCLAW_SRC2_KERNEL
+#define DCLAW_SRC2_KERNEL 1
+#endif
+constexpr int TILE_X = DCLAW_TILE_X, TILE_Y = DCLAW_TILE_Y;
 
 __device__ __forceinline__ double warp_max(double v) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -176,7 +188,20 @@ __device__ __forceinline__ void tick_device(const dclaw_params& P, dclaw_clock* 
     clk->blocks_done = 0u;
 }
 
-template <int TX, int TY>
+// the block finishing last (after its Courant-number atomic) runs the tick
+__device__ __forceinline__ void last_block_tick(const dclaw_params& P, dclaw_clock* clk) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned int done = atomicAdd(&clk->blocks_done, 1u);
+        if (done == gridDim.x * gridDim.y - 1) {
+            __threadfence();
+            tick_device(P, clk);
+        }
+    }
+}
+
+template <int TX, int TY, bool WITH_SRC2>
 __global__ void __launch_bounds__(TPB, 2) k_tile(dclaw_params P, Geom g, Rec R, const double* __restrict__ b,
                                                  double* __restrict__ q_out, dclaw_clock* clk,
                                                  uint32_t* __restrict__ brlog) {
@@ -239,20 +264,22 @@ __global__ void __launch_bounds__(TPB, 2) k_tile(dclaw_params P, Geom g, Rec R, 
         for (int it = tid; it < TY * (TX + 2); it += TPB) tile_flux<1, TX, TY>(P, g, R, b, M, it, i0, j0, dtdy, brlog);
         __syncthreads();
         for (int it = tid; it < TX * TY; it += TPB)
-            if (tile_final<TX, TY>(P, g, R, M, it, i0, j0, dt, q_out)) nan = true;
+            if (tile_final<TX, TY, WITH_SRC2>(P, g, R, M, it, i0, j0, dt, q_out)) nan = true;
     }
     if (!(cfl == cfl)) cfl = 0.0;
     if (nan) flag_status(clk, DCLAW_ERR_NAN);
     block_max_to(cfl, reinterpret_cast<unsigned long long*>(&clk->cfl_bits));
-    __syncthreads();
-    if (tid == 0) {
-        __threadfence();
-        unsigned int done = atomicAdd(&clk->blocks_done, 1u);
-        if (done == gridDim.x * gridDim.y - 1) {
-            __threadfence();
-            tick_device(P, clk);
-        }
-    }
+    if (WITH_SRC2) last_block_tick(P, clk);
+}
+
+// src2 of every interior cell from the updated state; the last block
+// applies the tick rule
+__global__ void __launch_bounds__(TPB) k_src2_cells(dclaw_params P, Geom g, const double* __restrict__ q_star,
+                                                    double* __restrict__ q_out, dclaw_clock* clk) {
+    const long long n = (long long)g.mx * g.my;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < n) cell_src2(P, g, clk->dt, q_star, q_out, (size_t)idx);
+    last_block_tick(P, clk);
 }
 
 // ---- patch calls (padded layout) ------------------------------------------
@@ -378,7 +405,7 @@ inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 struct Layout {
     size_t npad, nxi, nyi;
     size_t off_qB, off_bP, off_td, off_wx, off_wy, off_fx, off_fy, total_staged;
-    size_t off_rec, total_fused;
+    size_t off_rec, off_qstar, total_fused;
     size_t total;
 };
 
@@ -396,9 +423,10 @@ inline Layout layout(int mx, int my) {
     L.off_fx = o; o += align256((size_t)NF * L.nxi * 8);
     L.off_fy = o; o += align256((size_t)NF * L.nyi * 8);
     L.total_staged = o;
-    // the fused step needs only the cell records
+    // the fused step needs the cell records and the updated state before src2
     L.off_rec = 0;
-    L.total_fused = align256((size_t)NREC * L.npad * 8);
+    L.off_qstar = align256((size_t)NREC * L.npad * 8);
+    L.total_fused = L.off_qstar + align256((size_t)5 * mx * my * 8);
     L.total = L.total_staged > L.total_fused ? L.total_staged : L.total_fused;
     return L;
 }
@@ -432,8 +460,11 @@ inline int ensure_tile_smem_attr() {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return DCLAW_ERR_CUDA;
     if (!done[dev]) {
-        if (cudaFuncSetAttribute(k_tile<TILE_X, TILE_Y>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)TileGeom<TILE_X, TILE_Y>::SMEM_BYTES) != cudaSuccess)
+        const int bytes = (int)TileGeom<TILE_X, TILE_Y>::SMEM_BYTES;
+        if (cudaFuncSetAttribute(k_tile<TILE_X, TILE_Y, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 bytes) != cudaSuccess ||
+            cudaFuncSetAttribute(k_tile<TILE_X, TILE_Y, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 bytes) != cudaSuccess)
             return DCLAW_ERR_CUDA;
         done[dev] = true;
     }
@@ -552,7 +583,13 @@ int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int m
     }
     k_records<<<nblocks((long long)L.npad), TPB, 0, s>>>(P, g, q_in, b, R, clock);
     dim3 grid((mx + TILE_X - 1) / TILE_X, (my + TILE_Y - 1) / TILE_Y);
-    k_tile<TILE_X, TILE_Y><<<grid, TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock, branch_log);
+    if (DCLAW_SRC2_KERNEL) {
+        double* qstar = (double*)((char*)work + L.off_qstar);
+        k_tile<TILE_X, TILE_Y, false><<<grid, TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, qstar, clock, branch_log);
+        k_src2_cells<<<nblocks((long long)mx * my), TPB, 0, s>>>(P, g, qstar, q_out, clock);
+    } else {
+        k_tile<TILE_X, TILE_Y, true><<<grid, TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock, branch_log);
+    }
     return cuda_status();
 }
 
@@ -679,7 +716,8 @@ int dclaw_step_noalloc(const double* q_in, double* q_out, const double* b, int m
     const dclaw_params P = *p;
     k_records<<<nblocks((long long)npad), TPB, 0, s>>>(P, g, q_in, b, R, clock);
     dim3 grid((mx + TILE_X - 1) / TILE_X, (my + TILE_Y - 1) / TILE_Y);
-    k_tile<TILE_X, TILE_Y><<<grid, TPB, TileGeom<TILE_X, TILE_Y>::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock, nullptr);
+    k_tile<TILE_X, TILE_Y, true><<<grid, TPB, TileGeom<TILE_X, TILE_Y>::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock,
+                                                                                     nullptr);
     return cuda_status();
 }
 

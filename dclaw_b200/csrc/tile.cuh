@@ -530,8 +530,10 @@ DC_HD void tile_T_store(const TileMem& M, int item, const double T[5]) {
     for (int m = 0; m < 5; ++m) slot[m] = T[m];
 }
 
-// update + src2 of tile cell (i, j); returns true on NaN
-template <int TX, int TY>
+// flux-differencing update of tile cell (i, j), written to q_out (interior
+// layout); with WITH_SRC2 the cell's src2 follows in the same thread,
+// otherwise q_out holds the updated state before src2. Returns true on NaN.
+template <int TX, int TY, bool WITH_SRC2>
 DC_HD bool tile_final(const dclaw_params& P, const Geom& g, const Rec& R, const TileMem& M, int item, int i0,
                       int j0, double dt, double* __restrict__ q_out) {
     int i = i0 + item % TX, j = j0 + item / TX;
@@ -561,11 +563,31 @@ DC_HD bool tile_final(const dclaw_params& P, const Geom& g, const Rec& R, const 
         qn[m] = qb[m] - dtdx * (fm - fp) - dtdy * (gm - gp);
     }
     bool nan = (qn[0] != qn[0]) || (qn[1] != qn[1]) || (qn[2] != qn[2]) || (qn[3] != qn[3]) || (qn[4] != qn[4]);
-    src2_cell(P, P.phi, dt, qn[0], qn[1], qn[2], qn[3], qn[4]);
+    if (WITH_SRC2) src2_cell(P, P.phi, dt, qn[0], qn[1], qn[2], qn[3], qn[4]);
     const size_t plane = (size_t)g.mx * g.my;
     const size_t c = (size_t)(j - 1) * g.mx + (size_t)(i - 1);
     for (int m = 0; m < 5; ++m) q_out[(size_t)m * plane + c] = qn[m];
     return nan;
+}
+
+// src2 of interior cell c (0-based linear index) from the updated state
+// q_star to q_out (interior layout)
+DC_HD void cell_src2(const dclaw_params& P, const Geom& g, double dt, const double* __restrict__ q_star,
+                     double* __restrict__ q_out, size_t c) {
+    const size_t plane = (size_t)g.mx * g.my;
+    double h = q_star[c];
+    if (h <= P.dry_tolerance) {
+        for (int m = 0; m < 5; ++m) q_out[(size_t)m * plane + c] = 0.0;
+        return;
+    }
+    double a = h, b = q_star[plane + c], cc = q_star[2 * plane + c], d = q_star[3 * plane + c],
+           e = q_star[4 * plane + c];
+    src2_cell(P, P.phi, dt, a, b, cc, d, e);
+    q_out[c] = a;
+    q_out[plane + c] = b;
+    q_out[2 * plane + c] = cc;
+    q_out[3 * plane + c] = d;
+    q_out[4 * plane + c] = e;
 }
 
 }  // namespace dclaw

@@ -35,8 +35,10 @@ class Emu:
             fn.argtypes = [ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                            _dp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp, _dp, _up,
                            _dp]
+        self.lib.emu_run_fused.argtypes = self.lib.emu_run_fused.argtypes + [ctypes.c_int] * 3
 
-    def run(self, p, q, b, dx, dy, nsteps, dt_initial, t_final=0.0, fixed_dt=False, fused=False):
+    def run(self, p, q, b, dx, dy, nsteps, dt_initial, t_final=0.0, fixed_dt=False, fused=False, tile=(16, 14),
+            src2_in_tile=False):
         q = np.ascontiguousarray(q, dtype=np.float64).copy()
         b = np.ascontiguousarray(b, dtype=np.float64)
         _, my, mx = q.shape
@@ -45,8 +47,9 @@ class Emu:
         br = np.zeros((my + 2) * (mx + 1) + (mx + 2) * (my + 1), dtype=np.uint32)
         t = np.zeros(1)
         cp = p.to_c()
-        fn = self.lib.emu_run_fused if fused else self.lib.emu_run
-        st = fn(ctypes.byref(cp), mx, my, dx, dy, q.ctypes.data_as(_dp), b.ctypes.data_as(_dp),
-                              nsteps, dt_initial, t_final, int(fixed_dt), dth.ctypes.data_as(_dp),
-                              cfh.ctypes.data_as(_dp), br.ctypes.data_as(_up), t.ctypes.data_as(_dp))
+        args = [ctypes.byref(cp), mx, my, dx, dy, q.ctypes.data_as(_dp), b.ctypes.data_as(_dp), nsteps, dt_initial,
+                t_final, int(fixed_dt), dth.ctypes.data_as(_dp), cfh.ctypes.data_as(_dp), br.ctypes.data_as(_up),
+                t.ctypes.data_as(_dp)]
+        st = self.lib.emu_run_fused(*args, *tile, int(src2_in_tile)) if fused else self.lib.emu_run(*args)
+        assert st >= 0, "tile size not instantiated in the emulation"
         return dict(q=q, dt=dth[:nsteps], cfl=cfh[:nsteps], status=st, br=br, t=float(t[0]))

@@ -81,10 +81,10 @@ extern "C" int emu_run(const dclaw_params* P, int mx, int my, double dx, double 
 
 // The fused two-kernel step (tile.cuh): K1 records, then every tile's phases
 // in the kernel's order with host buffers standing in for shared memory.
-extern "C" int emu_run_fused(const dclaw_params* P, int mx, int my, double dx, double dy, double* q, const double* b,
-                             int nsteps, double dt_initial, double t_final, int fixed_dt, double* dt_hist,
-                             double* cfl_hist, uint32_t* brlog, double* t_out) {
-    constexpr int TX = 16, TY = 16;
+template <int TX, int TY>
+static int run_fused(const dclaw_params* P, int mx, int my, double dx, double dy, double* q, const double* b,
+                     int nsteps, double dt_initial, double t_final, int fixed_dt, double* dt_hist,
+                     double* cfl_hist, uint32_t* brlog, double* t_out, bool src2_in_tile) {
     using TG = TileGeom<TX, TY>;
     Geom g{mx, my, mx + 4, my + 4, dx, dy};
     size_t npad = (size_t)(mx + 4) * (my + 4);
@@ -98,7 +98,7 @@ extern "C" int emu_run_fused(const dclaw_params* P, int mx, int my, double dx, d
     M.D = M.C + (size_t)10 * TG::NC;
     M.bits = bits.data();
     M.NA = TG::NA;
-    std::vector<double> qa(q, q + 5 * (size_t)mx * my), qb(5 * (size_t)mx * my);
+    std::vector<double> qa(q, q + 5 * (size_t)mx * my), qb(5 * (size_t)mx * my), qs(5 * (size_t)mx * my);
     double t = 0.0, dt = t_final > 0.0 ? fmax2(fmin2(dt_initial, t_final), 0.0) : dt_initial;
     int status = 0;
     const size_t nlog = (size_t)(my + 2) * (mx + 1) + (size_t)(mx + 2) * (my + 1);
@@ -131,9 +131,14 @@ extern "C" int emu_run_fused(const dclaw_params* P, int mx, int my, double dx, d
                     if (ok) cfl = fmax2(cfl, dtdy * s);
                 }
                 for (int it = 0; it < TY * (TX + 2); ++it) tile_flux<1, TX, TY>(*P, g, R, b, M, it, i0, j0, dtdy, br);
-                for (int it = 0; it < TX * TY; ++it)
-                    if (tile_final<TX, TY>(*P, g, R, M, it, i0, j0, dt, qb.data())) status = DCLAW_ERR_NAN;
+                for (int it = 0; it < TX * TY; ++it) {
+                    bool nan = src2_in_tile ? tile_final<TX, TY, true>(*P, g, R, M, it, i0, j0, dt, qb.data())
+                                            : tile_final<TX, TY, false>(*P, g, R, M, it, i0, j0, dt, qs.data());
+                    if (nan) status = DCLAW_ERR_NAN;
+                }
             }
+        if (!src2_in_tile)
+            for (size_t c = 0; c < (size_t)mx * my; ++c) cell_src2(*P, g, dt, qs.data(), qb.data(), c);
         qa.swap(qb);
         if (dt_hist) dt_hist[n] = dt;
         if (cfl_hist) cfl_hist[n] = cfl;
@@ -146,4 +151,18 @@ extern "C" int emu_run_fused(const dclaw_params* P, int mx, int my, double dx, d
     memcpy(q, qa.data(), sizeof(double) * 5 * (size_t)mx * my);
     if (t_out) *t_out = t;
     return status;
+}
+
+extern "C" int emu_run_fused(const dclaw_params* P, int mx, int my, double dx, double dy, double* q, const double* b,
+                             int nsteps, double dt_initial, double t_final, int fixed_dt, double* dt_hist,
+                             double* cfl_hist, uint32_t* brlog, double* t_out, int tx, int ty, int src2_in_tile) {
+#define DCLAW_EMU_TILE(X, Y)                                                                              \
+    if (tx == X && ty == Y)                                                                              \
+        return run_fused<X, Y>(P, mx, my, dx, dy, q, b, nsteps, dt_initial, t_final, fixed_dt, dt_hist, \
+                               cfl_hist, brlog, t_out, src2_in_tile != 0);
+    DCLAW_EMU_TILE(16, 16)
+    DCLAW_EMU_TILE(16, 14)
+    DCLAW_EMU_TILE(13, 14)
+    DCLAW_EMU_TILE(8, 8)
+    return -1;
 }

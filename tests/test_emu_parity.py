@@ -60,10 +60,17 @@ def test_random_field_small(oracle, emu, fused):
     _cmp(oracle, emu, c, 30, fused)
 
 
-def test_fused_partial_tiles(oracle, emu):
-    """Patch sizes that are not multiples of the 16 x 16 tile."""
+@pytest.mark.parametrize("src2_in_tile", [False, True])
+@pytest.mark.parametrize("tile", [(13, 14), (16, 16), (16, 14), (8, 8)])
+def test_fused_tile_shapes_and_partial_tiles(oracle, emu, tile, src2_in_tile):
+    """Tile shapes of the fused step on a patch whose sizes are not multiples
+    of the tile."""
     c = W.random_field_case(n=128, dx=0.5, seed=4)
     q = c.q[:, :71, :93].copy()
     b = c.b[:71, :93].copy()
     c2 = W.Case("partial", q, b, c.dx, c.dy, c.params, 0, c.dt_initial)
-    _cmp(oracle, emu, c2, 25, True)
+    r1 = oracle.run(c2.params, c2.q, c2.b, c2.dx, c2.dy, 25, c2.dt_initial, branch_log=True, libm="portable")
+    r2 = emu.run(c2.params, c2.q, c2.b, c2.dx, c2.dy, 25, c2.dt_initial, fused=True, tile=tile,
+                 src2_in_tile=src2_in_tile)
+    assert np.array_equal(r1["q"], r2["q"])
+    assert np.array_equal(np.concatenate([r1["xlog"].ravel(), r1["ylog"].ravel()]), r2["br"])
