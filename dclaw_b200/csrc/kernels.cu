@@ -23,6 +23,10 @@ constexpr int TPB = 256;
 #ifndef DCLAW_TILE_Y
 #define DCLAW_TILE_Y 14
 #endif
+// resident tile CTAs per SM the register allocation is sized for
+#ifndef DCLAW_TILE_MINBLOCKS
+#define DCLAW_TILE_MINBLOCKS 2
+#endif
 // src2 in its own per-cell kernel (1) or as the tile kernel's last phase (0)
 #ifndef DCLAW_SRC2_KERNEL
 #define DCLAW_SRC2_KERNEL 1
@@ -202,7 +206,7 @@ __device__ __forceinline__ void last_block_tick(const dclaw_params& P, dclaw_clo
 }
 
 template <int TX, int TY, bool WITH_SRC2>
-__global__ void __launch_bounds__(TPB, 2) k_tile(dclaw_params P, Geom g, Rec R, const double* __restrict__ b,
+__global__ void __launch_bounds__(TPB, DCLAW_TILE_MINBLOCKS) k_tile(dclaw_params P, Geom g, Rec R, const double* __restrict__ b,
                                                  double* __restrict__ q_out, dclaw_clock* clk,
                                                  uint32_t* __restrict__ brlog) {
     using TG = TileGeom<TX, TY>;
@@ -212,19 +216,23 @@ __global__ void __launch_bounds__(TPB, 2) k_tile(dclaw_params P, Geom g, Rec R, 
     M.B = M.A + (size_t)NW * TG::NA;
     M.C = M.B + (size_t)10 * TG::NB;
     M.D = M.C + (size_t)10 * TG::NC;
-    M.bits = reinterpret_cast<uint32_t*>(M.D + (size_t)10 * TG::ND);
+    M.H = M.D + (size_t)10 * TG::ND;
+    M.Bd = M.H + TG::NHB;
+    M.bits = reinterpret_cast<uint32_t*>(M.Bd + TG::NHB);
     M.NA = TG::NA;
     const int tid = threadIdx.x;
     const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
+    M.hi0 = i0 - 3;
+    M.hj0 = j0 - 3;
+    M.hw = TX + 6;
     const double dt = clk->dt;
     const double dtdx = dt / g.dx, dtdy = dt / g.dy;
-    // a tile whose cells within distance 3 are all dry stays dry: all its
-    // interfaces are dry-dry (skipped) and src2 zeroes dry cells
+    // stage h and bed of the cells within 3 of the tile; a tile whose cells
+    // within distance 3 are all dry stays dry: all its interfaces are
+    // dry-dry (skipped) and src2 zeroes dry cells
     bool any = false;
-    for (int it = tid; it < (TX + 6) * (TY + 6); it += TPB) {
-        int i = i0 - 3 + it % (TX + 6), j = j0 - 3 + it / (TX + 6);
-        if (i >= -1 && i <= g.mx + 2 && j >= -1 && j <= g.my + 2 && R.get(R_H, pidx(g, i, j)) > 0.0) any = true;
-    }
+    for (int it = tid; it < TG::NHB; it += TPB)
+        if (tile_stage_hb(g, R, b, M, it)) any = true;
     any = __syncthreads_or(any) != 0;
     double cfl = 0.0;
     bool nan = false;
@@ -237,32 +245,31 @@ __global__ void __launch_bounds__(TPB, 2) k_tile(dclaw_params P, Geom g, Rec R, 
             for (int m = 0; m < 5; ++m) q_out[(size_t)m * plane + c] = 0.0;
         }
     } else {
-        for (int it = tid; it < TG::NXW; it += TPB) {
-            bool ok;
-            double s = tile_riemann<0>(P, g, R, b, M, it, i0, j0, TX, TY, ok);
-            if (ok) cfl = fmax2(cfl, dtdx * s);
-        }
-        __syncthreads();
-        for (int it = tid; it < (TY + 2) * TX; it += TPB) tile_flux<0, TX, TY>(P, g, R, b, M, it, i0, j0, dtdx, brlog);
-        __syncthreads();
-        {
-            double T0[5], T1[5];
-            const int nT = (TY + 1) * TX;
-            bool v0 = tid < nT && tile_T<TX, TY>(g, M, tid, i0, j0, T0);
-            bool v1 = tid + TPB < nT && tile_T<TX, TY>(g, M, tid + TPB, i0, j0, T1);
+        // the two sweeps share one copy of the solver, limiter and rpt2 code
+#pragma unroll 1
+        for (int dir = 0; dir < 2; ++dir) {
+            const int nsolve = dir == 0 ? TG::NXW : TG::NYW;
+            const double dtd = dir == 0 ? dtdx : dtdy;
+            for (int it = tid; it < nsolve; it += TPB) {
+                bool ok;
+                double s = tile_riemann(P, g, R, M, dir, it, i0, j0, TX, TY, ok);
+                if (ok) cfl = fmax2(cfl, dtd * s);
+            }
             __syncthreads();
-            if (v0) tile_T_store<TX, TY>(M, tid, T0);
-            if (v1) tile_T_store<TX, TY>(M, tid + TPB, T1);
+            const int ncell = dir == 0 ? (TY + 2) * TX : TY * (TX + 2);
+            for (int it = tid; it < ncell; it += TPB) tile_flux<TX, TY>(P, g, R, M, dir, it, i0, j0, dtd, brlog);
+            __syncthreads();
+            if (dir == 0) {
+                double T0[5], T1[5];
+                const int nT = (TY + 1) * TX;
+                bool v0 = tid < nT && tile_T<TX, TY>(g, M, tid, i0, j0, T0);
+                bool v1 = tid + TPB < nT && tile_T<TX, TY>(g, M, tid + TPB, i0, j0, T1);
+                __syncthreads();
+                if (v0) tile_T_store<TX, TY>(M, tid, T0);
+                if (v1) tile_T_store<TX, TY>(M, tid + TPB, T1);
+                __syncthreads();
+            }
         }
-        __syncthreads();
-        for (int it = tid; it < TG::NYW; it += TPB) {
-            bool ok;
-            double s = tile_riemann<1>(P, g, R, b, M, it, i0, j0, TX, TY, ok);
-            if (ok) cfl = fmax2(cfl, dtdy * s);
-        }
-        __syncthreads();
-        for (int it = tid; it < TY * (TX + 2); it += TPB) tile_flux<1, TX, TY>(P, g, R, b, M, it, i0, j0, dtdy, brlog);
-        __syncthreads();
         for (int it = tid; it < TX * TY; it += TPB)
             if (tile_final<TX, TY, WITH_SRC2>(P, g, R, M, it, i0, j0, dt, q_out)) nan = true;
     }

@@ -183,15 +183,55 @@ DC_HD bool cell_record(const dclaw_params& P, const Geom& g, const double* __res
     return nan;
 }
 
+// ---------------------------------------------------------------------------
+template <int TX, int TY>
+struct TileGeom {
+    static constexpr int NA = (TY + 2) * (TX + 3) > (TX + 2) * (TY + 3) ? (TY + 2) * (TX + 3) : (TX + 2) * (TY + 3);
+    static constexpr int NXW = (TY + 2) * (TX + 3);   // x solves: rows j0-1..j0+TY, ifaces i0-1..i0+TX+1
+    static constexpr int NYW = (TX + 2) * (TY + 3);   // y solves: cols i0-1..i0+TX, ifaces j0-1..j0+TY+1
+    static constexpr int NB = TY * (TX + 1);          // x-fluxes of tile rows, ifaces i0..i0+TX
+    static constexpr int NC = (TY + 2) * TX;          // G1x/G2x rows j0-1..j0+TY (then T/gm/gp rows j0..j0+TY)
+    static constexpr int ND = (TX + 2) * TY;          // G1y/G2y cols i0-1..i0+TX, rows j0..j0+TY-1
+    static constexpr int NHB = (TX + 6) * (TY + 6);    // h and bed of cells within 3 of the tile
+    static constexpr size_t SMEM_DOUBLES = (size_t)NW * NA + 10 * NB + 10 * NC + 10 * ND + 2 * NHB;
+    static constexpr size_t SMEM_BYTES = SMEM_DOUBLES * 8 + 4 * (size_t)NA;
+};
+
+struct TileMem {
+    double* A;   // NW planes of NA
+    double* B;   // [NB][10]
+    double* C;   // [NC][10]
+    double* D;   // [ND][10]
+    double* H;   // record h of cells (i0-3..i0+TX+2) x (j0-3..j0+TY+2)
+    double* Bd;  // bed of the same cells
+    uint32_t* bits;  // NA Riemann branch bits of the current sweep
+    int NA;
+    int hi0, hj0, hw;  // origin and width of the H/Bd block
+    DC_HD double h(int i, int j) const { return H[(j - hj0) * hw + (i - hi0)]; }
+    DC_HD double bed(int i, int j) const { return Bd[(j - hj0) * hw + (i - hi0)]; }
+};
+
+// stage record h and bed of block item `it` (cells within 3 of the tile);
+// returns whether the cell is wet. Cells outside the padded patch are never
+// read and are left unset.
+DC_HD bool tile_stage_hb(const Geom& g, const Rec& R, const double* b_in, const TileMem& M, int it) {
+    int i = M.hi0 + it % M.hw, j = M.hj0 + it / M.hw;
+    if (i < -1 || i > g.mx + 2 || j < -1 || j > g.my + 2) return false;
+    double h = R.get(R_H, pidx(g, i, j));
+    M.H[it] = h;
+    M.Bd[it] = bed_at(g, b_in, i, j);
+    return h > 0.0;
+}
+
 // Solver side of a record cell after one (A1) or two (A2) qfix passes
-DC_HD Side rec_side(const dclaw_params& P, const Rec& R, const Geom& g, const double* b_in, int i, int j,
-                    int dir, bool twice) {
+DC_HD Side rec_side(const dclaw_params& P, const Rec& R, const Geom& g, const TileMem& M, int i, int j, int dir,
+                    bool twice) {
     const size_t pi = pidx(g, i, j);
     Side s;
-    s.b = bed_at(g, b_in, i, j);
+    s.b = M.bed(i, j);
     s.fs = R.get(R_FS, pi);
     s.taudir = R.get(dir == 0 ? R_TDX : R_TDY, pi);
-    double h = R.get(R_H, pi);
+    double h = M.h(i, j);
     if (h <= P.dry_tolerance) {
         s.h = 0.0; s.hn = 0.0; s.ht = 0.0; s.hm = 0.0; s.p = 0.0;
         s.un = 0.0; s.ut = 0.0; s.m = 0.0; s.rho_sv = 0.0; s.tau_sv = 0.0;
@@ -224,66 +264,43 @@ DC_HD Side rec_side(const dclaw_params& P, const Rec& R, const Geom& g, const do
     return s;
 }
 
-// ---------------------------------------------------------------------------
-template <int TX, int TY>
-struct TileGeom {
-    static constexpr int NA = (TY + 2) * (TX + 3) > (TX + 2) * (TY + 3) ? (TY + 2) * (TX + 3) : (TX + 2) * (TY + 3);
-    static constexpr int NXW = (TY + 2) * (TX + 3);   // x solves: rows j0-1..j0+TY, ifaces i0-1..i0+TX+1
-    static constexpr int NYW = (TX + 2) * (TY + 3);   // y solves: cols i0-1..i0+TX, ifaces j0-1..j0+TY+1
-    static constexpr int NB = TY * (TX + 1);          // x-fluxes of tile rows, ifaces i0..i0+TX
-    static constexpr int NC = (TY + 2) * TX;          // G1x/G2x rows j0-1..j0+TY (then T/gm/gp rows j0..j0+TY)
-    static constexpr int ND = (TX + 2) * TY;          // G1y/G2y cols i0-1..i0+TX, rows j0..j0+TY-1
-    static constexpr size_t SMEM_DOUBLES = (size_t)NW * NA + 10 * NB + 10 * NC + 10 * ND;
-    static constexpr size_t SMEM_BYTES = SMEM_DOUBLES * 8 + 4 * (size_t)NA;
-};
-
-struct TileMem {
-    double* A;   // NW planes of NA
-    double* B;   // [NB][10]
-    double* C;   // [NC][10]
-    double* D;   // [ND][10]
-    uint32_t* bits;  // NA Riemann branch bits of the current sweep
-    int NA;
-};
-
-// expand a stored solve into q-ordered 5-vectors
-template <int DIR>
-DC_HD void tile_waves(const TileMem& M, int item, double s[3], double W1[5], double W2[5], double W5[5]) {
+// expand a stored solve into q-ordered 5-vectors (dir 0: normal = hu,
+// tangential = hv; dir 1: normal = hv, tangential = hu)
+DC_HD void tile_waves(const TileMem& M, int dir, int item, double s[3], double W1[5], double W2[5], double W5[5]) {
     double v[NW];
     for (int k = 0; k < NW; ++k) v[k] = M.A[(size_t)k * M.NA + item];
     s[0] = v[W_S1]; s[1] = v[W_S2]; s[2] = v[W_S5];
-    const int cn = DIR == 0 ? 1 : 2, ct = DIR == 0 ? 2 : 1;
-    W1[0] = v[W_1H]; W1[cn] = v[W_1N]; W1[ct] = v[W_1T]; W1[3] = v[W_1M]; W1[4] = v[W_1P];
-    W2[0] = v[W_2H]; W2[cn] = v[W_2N]; W2[ct] = 0.0; W2[3] = 0.0; W2[4] = 0.0;
-    W5[0] = v[W_5H]; W5[cn] = v[W_5N]; W5[ct] = v[W_5T]; W5[3] = v[W_5M]; W5[4] = v[W_5P];
+    const bool y = dir != 0;
+    W1[0] = v[W_1H]; W1[1] = y ? v[W_1T] : v[W_1N]; W1[2] = y ? v[W_1N] : v[W_1T]; W1[3] = v[W_1M]; W1[4] = v[W_1P];
+    W2[0] = v[W_2H]; W2[1] = y ? 0.0 : v[W_2N]; W2[2] = y ? v[W_2N] : 0.0; W2[3] = 0.0; W2[4] = 0.0;
+    W5[0] = v[W_5H]; W5[1] = y ? v[W_5T] : v[W_5N]; W5[2] = y ? v[W_5N] : v[W_5T]; W5[3] = v[W_5M]; W5[4] = v[W_5P];
 }
 
-// Riemann solve of sweep DIR for tile-local item (slice s, interface k).
-// DIR 0: s = row r, k = x-interface; DIR 1: s = column c, k = y-interface.
-// Returns max |s| (0 for skipped items), *valid tells whether the item lies
-// in the patch; *cfl_ok whether it counts for the Courant number.
-template <int DIR>
-DC_HD double tile_riemann(const dclaw_params& P, const Geom& g, const Rec& R, const double* b_in,
-                          const TileMem& M, int item, int i0, int j0, int TX, int TY, bool& cfl_ok) {
+// Riemann solve of sweep `dir` for tile-local item (slice s, interface k).
+// dir 0: s = row r, k = x-interface; dir 1: s = column c, k = y-interface.
+// Returns max |s| (0 for skipped items); cfl_ok tells whether the item
+// counts for the Courant number.
+DC_HD double tile_riemann(const dclaw_params& P, const Geom& g, const Rec& R, const TileMem& M, int dir,
+                          int item, int i0, int j0, int TX, int TY, bool& cfl_ok) {
     int sl, k;
-    if (DIR == 0) { sl = j0 - 1 + item / (TX + 3); k = i0 - 1 + item % (TX + 3); }
+    if (dir == 0) { sl = j0 - 1 + item / (TX + 3); k = i0 - 1 + item % (TX + 3); }
     else { sl = i0 - 1 + item % (TX + 2); k = j0 - 1 + item / (TX + 2); }
-    const int nslice = DIR == 0 ? g.my : g.mx, nlen = DIR == 0 ? g.mx : g.my;
+    const int nslice = dir == 0 ? g.my : g.mx, nlen = dir == 0 ? g.mx : g.my;
     cfl_ok = false;
     Waves w;
     uint32_t bits = 0;
     if (sl < 0 || sl > nslice + 1 || k < 0 || k > nlen + 2) {
         zero_waves(w);
     } else {
-        int iL = DIR == 0 ? k - 1 : sl, jL = DIR == 0 ? sl : k - 1;
-        int iR = DIR == 0 ? k : sl, jR = DIR == 0 ? sl : k;
-        double hL0 = R.get(R_H, pidx(g, iL, jL)), hR0 = R.get(R_H, pidx(g, iR, jR));
+        int iL = dir == 0 ? k - 1 : sl, jL = dir == 0 ? sl : k - 1;
+        int iR = dir == 0 ? k : sl, jR = dir == 0 ? sl : k;
+        double hL0 = M.h(iL, jL), hR0 = M.h(iR, jR);
         if (hL0 <= P.dry_tolerance && hR0 <= P.dry_tolerance) {
             zero_waves(w);
             bits |= BR_DRY;
         } else {
-            Side Rs = rec_side(P, R, g, b_in, iR, jR, DIR, false);
-            Side Ls = rec_side(P, R, g, b_in, iL, jL, DIR, k - 1 >= 0);
+            Side Rs = rec_side(P, R, g, M, iR, jR, dir, false);
+            Side Ls = rec_side(P, R, g, M, iL, jL, dir, k - 1 >= 0);
             w = riemann_solve(P, Ls, Rs, &bits);
         }
         cfl_ok = k >= 1 && k <= nlen + 1;
@@ -295,11 +312,11 @@ DC_HD double tile_riemann(const dclaw_params& P, const Geom& g, const Rec& R, co
     return fmax2(fmax2(fabs(w.s1), fabs(w.s2)), fabs(w.s5));
 }
 
-// A2 state (h, hn, ht, hm) of a record cell and its bed
-DC_HD void rec_a2(const dclaw_params& P, const Rec& R, const Geom& g, int i, int j, int dir, double& h,
-                  double& hn, double& ht, double& hm) {
+// A2 state (h, hn, ht, hm) of a record cell
+DC_HD void rec_a2(const dclaw_params& P, const Rec& R, const Geom& g, const TileMem& M, int i, int j, int dir,
+                  double& h, double& hn, double& ht, double& hm) {
     const size_t pi = pidx(g, i, j);
-    h = R.get(R_H, pi);
+    h = M.h(i, j);
     if (h <= P.dry_tolerance) { h = 0.0; hn = 0.0; ht = 0.0; hm = 0.0; return; }
     double hu = R.get(R_HU, pi), hv = R.get(R_HV, pi);
     hn = dir == 0 ? hu : hv;
@@ -309,12 +326,11 @@ DC_HD void rec_a2(const dclaw_params& P, const Rec& R, const Geom& g, int i, int
 
 // limited waves + fluctuations at one interface (local position `pos` in
 // the sweep's item grid; neighbours at pos-1, pos+1). Returns wet4.
-template <int DIR>
-DC_HD bool iface_limited(const dclaw_params& P, const TileMem& M, int item_m, int item, int item_p,
+DC_HD bool iface_limited(const dclaw_params& P, const TileMem& M, int dir, int item_m, int item, int item_p,
                          const double hcells[4], double dtdx, double amdq[5], double apdq[5], double cqxx[5],
                          uint32_t* bits) {
     double s[3], W1[5], W2[5], W5[5];
-    tile_waves<DIR>(M, item, s, W1, W2, W5);
+    tile_waves(M, dir, item, s, W1, W2, W5);
     for (int m = 0; m < 5; ++m) {
         double am = 0.0, ap = 0.0;
         if (s[0] < 0.0) am = am + W1[m]; else if (s[0] > 0.0) ap = ap + W1[m];
@@ -328,8 +344,8 @@ DC_HD bool iface_limited(const dclaw_params& P, const TileMem& M, int item_m, in
     if (P.order != 1) {
         if (P.limiter != 0) {
             double sm[3], Wm1[5], Wm2[5], Wm5[5], sp[3], Wp1[5], Wp2[5], Wp5[5];
-            tile_waves<DIR>(M, item_m, sm, Wm1, Wm2, Wm5);
-            tile_waves<DIR>(M, item_p, sp, Wp1, Wp2, Wp5);
+            tile_waves(M, dir, item_m, sm, Wm1, Wm2, Wm5);
+            tile_waves(M, dir, item_p, sp, Wp1, Wp2, Wp5);
             limit_family(P.limiter, 1, s[0], Wm1, W1, Wp1, bits);
             limit_family(P.limiter, 2, s[1], Wm2, W2, Wp2, bits);
             limit_family(P.limiter, 5, s[2], Wm5, W5, Wp5, bits);
@@ -353,20 +369,18 @@ DC_HD bool iface_limited(const dclaw_params& P, const TileMem& M, int item_m, in
 }
 
 // transverse split (rpt2) of one fluctuation with the Jacobian of cell (ci, cj)
-template <int DIR>
-DC_HD bool split_cell(const dclaw_params& P, const Rec& R, const Geom& g, const double* b_in, int ci, int cj,
-                      const double src[5], double half, double Um[5], double Up[5]) {
-    const int cn = DIR == 0 ? 1 : 2, ct = DIR == 0 ? 2 : 1;
+DC_HD bool split_cell(const dclaw_params& P, const Rec& R, const Geom& g, const TileMem& M, int dir, int ci,
+                      int cj, const double src[5], double half, double Um[5], double Up[5]) {
+    const bool y = dir != 0;
     double h, hn, ht, hm;
-    rec_a2(P, R, g, ci, cj, DIR, h, hn, ht, hm);
+    rec_a2(P, R, g, M, ci, cj, dir, h, hn, ht, hm);
     double topo1, topo3;
-    if (DIR == 0) { topo1 = bed_at(g, b_in, ci, cj - 1); topo3 = bed_at(g, b_in, ci, cj + 1); }
-    else { topo1 = bed_at(g, b_in, ci - 1, cj); topo3 = bed_at(g, b_in, ci + 1, cj); }
-    double asdq[5] = {src[0], src[cn], src[ct], src[3], src[4]}, bm[5], bp[5];
-    bool done = rpt2_split(P, h, hn, ht, hm, bed_at(g, b_in, ci, cj), topo1, topo3, asdq, bm, bp);
-    double bmq[5] = {bm[0], 0.0, 0.0, bm[3], bm[4]}, bpq[5] = {bp[0], 0.0, 0.0, bp[3], bp[4]};
-    bmq[cn] = bm[1]; bmq[ct] = bm[2];
-    bpq[cn] = bp[1]; bpq[ct] = bp[2];
+    if (!y) { topo1 = M.bed(ci, cj - 1); topo3 = M.bed(ci, cj + 1); }
+    else { topo1 = M.bed(ci - 1, cj); topo3 = M.bed(ci + 1, cj); }
+    double asdq[5] = {src[0], y ? src[2] : src[1], y ? src[1] : src[2], src[3], src[4]}, bm[5], bp[5];
+    bool done = rpt2_split(P, h, hn, ht, hm, M.bed(ci, cj), topo1, topo3, asdq, bm, bp);
+    double bmq[5] = {bm[0], y ? bm[2] : bm[1], y ? bm[1] : bm[2], bm[3], bm[4]};
+    double bpq[5] = {bp[0], y ? bp[2] : bp[1], y ? bp[1] : bp[2], bp[3], bp[4]};
     for (int m = 0; m < 5; ++m) {
         Um[m] = half * bmq[m];
         Up[m] = half * bpq[m];
@@ -388,32 +402,30 @@ DC_HD size_t ylog_off(const Geom& g, int c, int k) {
     return (size_t)(g.my + 2) * (g.mx + 1) + (size_t)c * (g.my + 1) + (size_t)(k - 1);
 }
 
-// Sweep flux phase for one cell of the sweep (DIR 0: cell (c, r) of rows
-// j0-1..j0+TY, columns i0..i0+TX-1; DIR 1: cell (c, j) of columns
+// Sweep flux phase for one cell of the sweep (dir 0: cell (c, r) of rows
+// j0-1..j0+TY, columns i0..i0+TX-1; dir 1: cell (c, j) of columns
 // i0-1..i0+TX, rows j0..j0+TY-1). Computes the fluxes of its own interface
 // (and of the next one for the last cell), and the cell's transverse
 // increments G1 = (0 - U1m(next iface)) - U2m(own iface), G2 likewise.
-template <int DIR, int TX, int TY>
-DC_HD void tile_flux(const dclaw_params& P, const Geom& g, const Rec& R, const double* b_in, const TileMem& M,
-                     int item, int i0, int j0, double dtdx, uint32_t* log) {
+template <int TX, int TY>
+DC_HD void tile_flux(const dclaw_params& P, const Geom& g, const Rec& R, const TileMem& M, int dir, int item,
+                     int i0, int j0, double dtdx, uint32_t* log) {
     int c, r;  // cell column / row
-    if (DIR == 0) { r = j0 - 1 + item / TX; c = i0 + item % TX; }
+    if (dir == 0) { r = j0 - 1 + item / TX; c = i0 + item % TX; }
     else { c = i0 - 1 + item % (TX + 2); r = j0 + item / (TX + 2); }
     const int mx = g.mx, my = g.my;
-    if (c < (DIR == 0 ? 1 : 0) || c > (DIR == 0 ? mx : mx + 1)) return;
-    if (r < (DIR == 0 ? 0 : 1) || r > (DIR == 0 ? my + 1 : my)) return;
+    if (c < (dir == 0 ? 1 : 0) || c > (dir == 0 ? mx : mx + 1)) return;
+    if (r < (dir == 0 ? 0 : 1) || r > (dir == 0 ? my + 1 : my)) return;
     // position along the sweep and the item-grid index of an interface
-    const int a = DIR == 0 ? c : r;                 // this cell along the sweep
-    const int nlen = DIR == 0 ? mx : my;
+    const int a = dir == 0 ? c : r;                 // this cell along the sweep
+    const int nlen = dir == 0 ? mx : my;
     auto witem = [&](int k) -> int {
-        return DIR == 0 ? (r - (j0 - 1)) * (TX + 3) + (k - (i0 - 1)) : (k - (j0 - 1)) * (TX + 2) + (c - (i0 - 1));
+        return dir == 0 ? (r - (j0 - 1)) * (TX + 3) + (k - (i0 - 1)) : (k - (j0 - 1)) * (TX + 2) + (c - (i0 - 1));
     };
-    auto hcell = [&](int aa) -> double {
-        return DIR == 0 ? R.get(R_H, pidx(g, aa, r)) : R.get(R_H, pidx(g, c, aa));
-    };
+    auto hcell = [&](int aa) -> double { return dir == 0 ? M.h(aa, r) : M.h(c, aa); };
     const double half = 0.5 * dtdx;
-    const bool last = DIR == 0 ? (c == (i0 + TX - 1 < mx ? i0 + TX - 1 : mx)) : (r == (j0 + TY - 1 < my ? j0 + TY - 1 : my));
-    const bool in_tile = DIR == 0 ? (r >= j0 && r <= j0 + TY - 1 && r <= my) : (c >= i0 && c <= i0 + TX - 1 && c <= mx);
+    const bool last = dir == 0 ? (c == (i0 + TX - 1 < mx ? i0 + TX - 1 : mx)) : (r == (j0 + TY - 1 < my ? j0 + TY - 1 : my));
+    const bool in_tile = dir == 0 ? (r >= j0 && r <= j0 + TY - 1 && r <= my) : (c >= i0 && c <= i0 + TX - 1 && c <= mx);
     uint32_t b_own = 0, b_next = 0;
     uint32_t* pb_own = log ? &b_own : nullptr;
     uint32_t* pb_next = log ? &b_next : nullptr;
@@ -421,8 +433,8 @@ DC_HD void tile_flux(const dclaw_params& P, const Geom& g, const Rec& R, const d
     double am0[5], ap0[5], cq0[5], am1[5], ap1[5], cq1[5];
     double h0[4] = {hcell(a - 2), hcell(a - 1), hcell(a), hcell(a + 1)};
     double h1[4] = {h0[1], h0[2], h0[3], hcell(a + 2)};
-    iface_limited<DIR>(P, M, witem(a - 1), witem(a), witem(a + 1), h0, dtdx, am0, ap0, cq0, pb_own);
-    iface_limited<DIR>(P, M, witem(a), witem(a + 1), witem(a + 2), h1, dtdx, am1, ap1, cq1, pb_next);
+    iface_limited(P, M, dir, witem(a - 1), witem(a), witem(a + 1), h0, dtdx, am0, ap0, cq0, pb_own);
+    iface_limited(P, M, dir, witem(a), witem(a + 1), witem(a + 2), h1, dtdx, am1, ap1, cq1, pb_next);
     const bool ord2 = P.order != 1;
     auto fadd = [&](const double* am, const double* ap, const double* cq, double fm[5], double fp[5]) {
         for (int m = 0; m < 5; ++m) {
@@ -436,7 +448,7 @@ DC_HD void tile_flux(const dclaw_params& P, const Geom& g, const Rec& R, const d
     };
     if (in_tile) {
         double fm[5], fp[5];
-        if (DIR == 0) {
+        if (dir == 0) {
             fadd(am0, ap0, cq0, fm, fp);
             double* dst = M.B + (size_t)((r - j0) * (TX + 1) + (c - i0)) * 10;
             for (int m = 0; m < 5; ++m) { dst[m] = fm[m]; dst[5 + m] = fp[m]; }
@@ -475,8 +487,8 @@ DC_HD void tile_flux(const dclaw_params& P, const Geom& g, const Rec& R, const d
             src1[m] = fold ? am1[m] + cq1[m] : am1[m];   // A-dq at the next interface (imp = 1)
             src2[m] = fold ? ap0[m] - cq0[m] : ap0[m];   // A+dq at the own interface (imp = 2)
         }
-        bool d1 = split_cell<DIR>(P, R, g, b_in, c, r, src1, half, U1m, U1p);
-        bool d2 = split_cell<DIR>(P, R, g, b_in, c, r, src2, half, U2m, U2p);
+        bool d1 = split_cell(P, R, g, M, dir, c, r, src1, half, U1m, U1p);
+        bool d2 = split_cell(P, R, g, M, dir, c, r, src2, half, U2m, U2p);
         if (d1) b_next |= BR_RPT1;
         if (d2) b_own |= BR_RPT2;
         if (log) {
@@ -485,31 +497,31 @@ DC_HD void tile_flux(const dclaw_params& P, const Geom& g, const Rec& R, const d
             if (a == 1) {   // imp = 1 at interface 1 uses cell 0
                 double s0[5];
                 double amx[5], apx[5], cqx[5], hx[4] = {hcell(-1), hcell(0), hcell(1), hcell(2)};
-                iface_limited<DIR>(P, M, witem(0), witem(1), witem(2), hx, dtdx, amx, apx, cqx, nullptr);
+                iface_limited(P, M, dir, witem(0), witem(1), witem(2), hx, dtdx, amx, apx, cqx, nullptr);
                 for (int m = 0; m < 5; ++m) s0[m] = fold ? amx[m] + cqx[m] : amx[m];
-                int ci = DIR == 0 ? 0 : c, cj = DIR == 0 ? r : 0;
-                if (split_cell<DIR>(P, R, g, b_in, ci, cj, s0, half, Xm, Xp)) b_own |= BR_RPT1;
+                int ci = dir == 0 ? 0 : c, cj = dir == 0 ? r : 0;
+                if (split_cell(P, R, g, M, dir, ci, cj, s0, half, Xm, Xp)) b_own |= BR_RPT1;
             }
             if (a == nlen) {   // imp = 2 at interface n+1 uses cell n+1
                 double s0[5];
                 for (int m = 0; m < 5; ++m) s0[m] = fold ? ap1[m] - cq1[m] : ap1[m];
-                int ci = DIR == 0 ? a + 1 : c, cj = DIR == 0 ? r : a + 1;
-                if (split_cell<DIR>(P, R, g, b_in, ci, cj, s0, half, Xm, Xp)) b_next |= BR_RPT2;
+                int ci = dir == 0 ? a + 1 : c, cj = dir == 0 ? r : a + 1;
+                if (split_cell(P, R, g, M, dir, ci, cj, s0, half, Xm, Xp)) b_next |= BR_RPT2;
             }
         }
     }
-    double* G = DIR == 0 ? M.C + (size_t)((r - (j0 - 1)) * TX + (c - i0)) * 10
+    double* G = dir == 0 ? M.C + (size_t)((r - (j0 - 1)) * TX + (c - i0)) * 10
                          : M.D + (size_t)((r - j0) * (TX + 2) + (c - (i0 - 1))) * 10;
     for (int m = 0; m < 5; ++m) {
         G[m] = (0.0 - U1m[m]) - U2m[m];
         G[5 + m] = (0.0 - U1p[m]) - U2p[m];
     }
     if (log) {
-        const int s = DIR == 0 ? r : c;
+        const int s = dir == 0 ? r : c;
         if (a >= 1 && a <= nlen + 1)
-            bits_or(log, DIR == 0 ? xlog_off(g, s, a) : ylog_off(g, s, a), b_own | M.bits[witem(a)]);
+            bits_or(log, dir == 0 ? xlog_off(g, s, a) : ylog_off(g, s, a), b_own | M.bits[witem(a)]);
         if (a + 1 >= 1 && a + 1 <= nlen + 1)
-            bits_or(log, DIR == 0 ? xlog_off(g, s, a + 1) : ylog_off(g, s, a + 1), b_next | M.bits[witem(a + 1)]);
+            bits_or(log, dir == 0 ? xlog_off(g, s, a + 1) : ylog_off(g, s, a + 1), b_next | M.bits[witem(a + 1)]);
     }
 }
 
@@ -541,7 +553,7 @@ DC_HD bool tile_final(const dclaw_params& P, const Geom& g, const Rec& R, const 
     const double dtdx = dt / g.dx, dtdy = dt / g.dy;
     const size_t pc = pidx(g, i, j);
     double qb[5];
-    qb[0] = R.get(R_H, pc);
+    qb[0] = M.h(i, j);
     if (qb[0] > 0.0) {
         qb[1] = R.get(R_HU, pc); qb[2] = R.get(R_HV, pc); qb[3] = R.get(R_HM, pc); qb[4] = R.get(R_P, pc);
     } else {

@@ -96,8 +96,11 @@ static int run_fused(const dclaw_params* P, int mx, int my, double dx, double dy
     M.B = M.A + (size_t)NW * TG::NA;
     M.C = M.B + (size_t)10 * TG::NB;
     M.D = M.C + (size_t)10 * TG::NC;
+    M.H = M.D + (size_t)10 * TG::ND;
+    M.Bd = M.H + TG::NHB;
     M.bits = bits.data();
     M.NA = TG::NA;
+    M.hw = TX + 6;
     std::vector<double> qa(q, q + 5 * (size_t)mx * my), qb(5 * (size_t)mx * my), qs(5 * (size_t)mx * my);
     double t = 0.0, dt = t_final > 0.0 ? fmax2(fmin2(dt_initial, t_final), 0.0) : dt_initial;
     int status = 0;
@@ -114,23 +117,27 @@ static int run_fused(const dclaw_params* P, int mx, int my, double dx, double dy
         for (int ty = 0; ty < (my + TY - 1) / TY; ++ty)
             for (int tx = 0; tx < (mx + TX - 1) / TX; ++tx) {
                 const int i0 = 1 + tx * TX, j0 = 1 + ty * TY;
-                for (int it = 0; it < TG::NXW; ++it) {
-                    bool ok;
-                    double s = tile_riemann<0>(*P, g, R, b, M, it, i0, j0, TX, TY, ok);
-                    if (ok) cfl = fmax2(cfl, dtdx * s);
+                M.hi0 = i0 - 3;
+                M.hj0 = j0 - 3;
+                for (int it = 0; it < TG::NHB; ++it) tile_stage_hb(g, R, b, M, it);
+                for (int dir = 0; dir < 2; ++dir) {
+                    const int nsolve = dir == 0 ? TG::NXW : TG::NYW;
+                    const double dtd = dir == 0 ? dtdx : dtdy;
+                    for (int it = 0; it < nsolve; ++it) {
+                        bool ok;
+                        double s = tile_riemann(*P, g, R, M, dir, it, i0, j0, TX, TY, ok);
+                        if (ok) cfl = fmax2(cfl, dtd * s);
+                    }
+                    const int ncell = dir == 0 ? (TY + 2) * TX : TY * (TX + 2);
+                    for (int it = 0; it < ncell; ++it) tile_flux<TX, TY>(*P, g, R, M, dir, it, i0, j0, dtd, br);
+                    if (dir == 0) {
+                        std::vector<double> T((size_t)(TY + 1) * TX * 5);
+                        std::vector<char> v((size_t)(TY + 1) * TX);
+                        for (int it = 0; it < (TY + 1) * TX; ++it) v[it] = tile_T<TX, TY>(g, M, it, i0, j0, &T[5 * it]);
+                        for (int it = 0; it < (TY + 1) * TX; ++it)
+                            if (v[it]) tile_T_store<TX, TY>(M, it, &T[5 * it]);
+                    }
                 }
-                for (int it = 0; it < (TY + 2) * TX; ++it) tile_flux<0, TX, TY>(*P, g, R, b, M, it, i0, j0, dtdx, br);
-                std::vector<double> T((size_t)(TY + 1) * TX * 5);
-                std::vector<char> v((size_t)(TY + 1) * TX);
-                for (int it = 0; it < (TY + 1) * TX; ++it) v[it] = tile_T<TX, TY>(g, M, it, i0, j0, &T[5 * it]);
-                for (int it = 0; it < (TY + 1) * TX; ++it)
-                    if (v[it]) tile_T_store<TX, TY>(M, it, &T[5 * it]);
-                for (int it = 0; it < TG::NYW; ++it) {
-                    bool ok;
-                    double s = tile_riemann<1>(*P, g, R, b, M, it, i0, j0, TX, TY, ok);
-                    if (ok) cfl = fmax2(cfl, dtdy * s);
-                }
-                for (int it = 0; it < TY * (TX + 2); ++it) tile_flux<1, TX, TY>(*P, g, R, b, M, it, i0, j0, dtdy, br);
                 for (int it = 0; it < TX * TY; ++it) {
                     bool nan = src2_in_tile ? tile_final<TX, TY, true>(*P, g, R, M, it, i0, j0, dt, qb.data())
                                             : tile_final<TX, TY, false>(*P, g, R, M, it, i0, j0, dt, qs.data());
