@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--json-out", default="")
+    ap.add_argument("--ensemble-members", type=int, default=256,
+                    help="members of the batched flume ensemble measured beside the plain step (0: skip)")
+    ap.add_argument("--ensemble-steps", type=int, default=10)
     return ap.parse_args()
 
 
@@ -177,6 +180,82 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def ensemble_bench(args, dev):
+    """Batched flume ensemble (uneven channels, per-member parameters and dt)
+    against looping the plain patch step over its members. Both forms run the
+    same members from the same state for the same number of steps; the
+    batched form replays one captured CUDA graph of the persistent ensemble
+    kernels after autotuning, the looped form calls the plain step member by
+    member (eagerly, and captured into one CUDA graph of all its launches)."""
+    import torch
+
+    from dclaw_b200 import workloads as W
+    from dclaw_b200.ensemble import EnsembleStepper, Member
+    from dclaw_b200.solver import PatchStepper
+
+    K = max(2, args.ensemble_steps + args.ensemble_steps % 2)
+    cases = W.flume_ensemble(n=args.ensemble_members, seed=args.seed)
+    members = [Member(c.q, c.b, c.params, c.dx, c.dy, c.dt_initial) for c in cases]
+    cells = sum(c.mx * c.my for c in cases)
+    ens = EnsembleStepper(members, dev)
+    tune = ens.autotune(steps=2)
+    ens.step(args.warmup)
+    ens.capture(K)
+    ens.replay(1)
+    torch.cuda.synchronize()
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    ms_b = timed(lambda: ens.replay(1))
+    status_b = ens.status()
+    del ens
+    steppers = []
+    for m in members:
+        ps = PatchStepper(torch.from_numpy(m.q).to(dev), torch.from_numpy(m.b).to(dev), m.params, m.dx, m.dy)
+        ps.init_clock(m.dt_initial)
+        steppers.append(ps)
+    for _ in range(args.warmup):
+        for ps in steppers:
+            ps.step(1)
+
+    def loop_eager():
+        for _ in range(K):
+            for ps in steppers:
+                ps.step(1)
+
+    ms_le = timed(loop_eager)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            for _ in range(K // 2):
+                for ps in steppers:
+                    ps._launch(ps.qa, ps.qb)
+                for ps in steppers:
+                    ps._launch(ps.qb, ps.qa)
+    torch.cuda.current_stream().wait_stream(s)
+    g.replay()
+    ms_lg = timed(g.replay)
+    del g
+    v_b = cells * K / (ms_b / 1000.0)
+    return {"workload": f"flume_ensemble_{len(members)}_dx0.05", "members": len(members), "cells": cells,
+            "steps": K, "value": v_b, "unit": "cell-updates/s", "ms_per_step": ms_b / K,
+            "looped_eager": {"value": cells * K / (ms_le / 1000.0), "ms_per_step": ms_le / K},
+            "looped_graph": {"value": cells * K / (ms_lg / 1000.0), "ms_per_step": ms_lg / K},
+            "vs_looped_eager": ms_le / ms_b, "vs_looped_graph": ms_lg / ms_b,
+            "autotune": {k: tune[k] for k in ("tile_shape", "tile_ctas_per_sm", "ms")},
+            "gpu_launches": 3 * K, "status_nonzero": sum(1 for x in status_b if x)}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -271,6 +350,10 @@ def run_ours(args):
                           "api": "PatchStepper.step with pinned host state in/out every step"}
     if world > 1:
         dist.barrier()
+    if rank == 0 and world == 1 and args.ensemble_members > 0:
+        del st
+        torch.cuda.empty_cache()
+        out["batched"] = ensemble_bench(args, dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args, case, args.cpu_steps)
     if rank == 0:

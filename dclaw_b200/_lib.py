@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes
 from pathlib import Path
 
-from .params import CClock, CParams
+from .params import CBatch, CClock, CMember, CParams
 
 LIB_DIR = Path(__file__).resolve().parent / "lib"
 LIB_PATH = LIB_DIR / "libdclaw_b200.so"
@@ -37,6 +37,10 @@ SIGNATURES = {
     "dclaw_max_wave_speed": (_int, [_vp, _int, _int, _pp, _vp, _vp]),
     "dclaw_step_noalloc": (_int, [_vp, _vp, _vp, _int, _int, _dbl, _dbl, _pp, _vp, _vp]),
     "dclaw_step_noalloc_max_cells": (_sz, []),
+    "dclaw_batch_tile_shapes": (_int, [_vp, _vp, _int]),
+    "dclaw_batch_layout": (_int, [_int, _vp, _vp, _vp, _vp, _int, ctypes.POINTER(CMember), ctypes.POINTER(CBatch)]),
+    "dclaw_step_batched": (_int, [ctypes.POINTER(CBatch), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dclaw_batch_reset": (_int, [ctypes.POINTER(CBatch), _vp, _vp]),
 }
 
 _lib = None

@@ -15,6 +15,7 @@
 namespace dclaw {
 
 constexpr int TPB = 256;
+constexpr int MAX_DEVICES = 64;
 // tile of the fused step: with 16 x 14 the flux phases of k_tile fit in one
 // round of 256 threads (256 and 252 cells) and the solves in two
 #ifndef DCLAW_TILE_X
@@ -205,12 +206,14 @@ __device__ __forceinline__ void last_block_tick(const dclaw_params& P, dclaw_clo
     }
 }
 
+// One tile of the fused step (all threads of the CTA call it). smem holds
+// TileGeom<TX,TY>::SMEM_BYTES. Returns this thread's Courant-number
+// contribution; *nan is set when an updated state holds a NaN.
 template <int TX, int TY, bool WITH_SRC2>
-__global__ void __launch_bounds__(TPB, DCLAW_TILE_MINBLOCKS) k_tile(dclaw_params P, Geom g, Rec R, const double* __restrict__ b,
-                                                 double* __restrict__ q_out, dclaw_clock* clk,
-                                                 uint32_t* __restrict__ brlog) {
+__device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g, const Rec& R,
+                                            const double* __restrict__ b, double* __restrict__ q_out, double dt,
+                                            int i0, int j0, double* smem, uint32_t* __restrict__ brlog, bool& nan) {
     using TG = TileGeom<TX, TY>;
-    extern __shared__ double smem[];
     TileMem M;
     M.A = smem;
     M.B = M.A + (size_t)NW * TG::NA;
@@ -221,11 +224,9 @@ __global__ void __launch_bounds__(TPB, DCLAW_TILE_MINBLOCKS) k_tile(dclaw_params
     M.bits = reinterpret_cast<uint32_t*>(M.Bd + TG::NHB);
     M.NA = TG::NA;
     const int tid = threadIdx.x;
-    const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
     M.hi0 = i0 - 3;
     M.hj0 = j0 - 3;
     M.hw = TX + 6;
-    const double dt = clk->dt;
     const double dtdx = dt / g.dx, dtdy = dt / g.dy;
     // stage h and bed of the cells within 3 of the tile; a tile whose cells
     // within distance 3 are all dry stays dry: all its interfaces are
@@ -235,7 +236,7 @@ __global__ void __launch_bounds__(TPB, DCLAW_TILE_MINBLOCKS) k_tile(dclaw_params
         if (tile_stage_hb(g, R, b, M, it)) any = true;
     any = __syncthreads_or(any) != 0;
     double cfl = 0.0;
-    bool nan = false;
+    nan = false;
     const size_t plane = (size_t)g.mx * g.my;
     if (!any && !brlog) {
         for (int it = tid; it < TX * TY; it += TPB) {
@@ -274,6 +275,17 @@ __global__ void __launch_bounds__(TPB, DCLAW_TILE_MINBLOCKS) k_tile(dclaw_params
             if (tile_final<TX, TY, WITH_SRC2>(P, g, R, M, it, i0, j0, dt, q_out)) nan = true;
     }
     if (!(cfl == cfl)) cfl = 0.0;
+    return cfl;
+}
+
+template <int TX, int TY, bool WITH_SRC2>
+__global__ void __launch_bounds__(TPB, DCLAW_TILE_MINBLOCKS) k_tile(dclaw_params P, Geom g, Rec R, const double* __restrict__ b,
+                                                 double* __restrict__ q_out, dclaw_clock* clk,
+                                                 uint32_t* __restrict__ brlog) {
+    extern __shared__ double smem[];
+    const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
+    bool nan;
+    double cfl = tile_body<TX, TY, WITH_SRC2>(P, g, R, b, q_out, clk->dt, i0, j0, smem, brlog, nan);
     if (nan) flag_status(clk, DCLAW_ERR_NAN);
     block_max_to(cfl, reinterpret_cast<unsigned long long*>(&clk->cfl_bits));
     if (WITH_SRC2) last_block_tick(P, clk);
@@ -287,6 +299,181 @@ __global__ void __launch_bounds__(TPB) k_src2_cells(dclaw_params P, Geom g, cons
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx < n) cell_src2(P, g, clk->dt, q_star, q_out, (size_t)idx);
     last_block_tick(P, clk);
+}
+
+// ---- batched ensemble -------------------------------------------------------
+constexpr int NBATCH_SHAPES = 3;
+__host__ __device__ constexpr int batch_tx(int k) { return k == 0 ? 16 : (k == 1 ? 13 : 16); }
+__host__ __device__ constexpr int batch_ty(int k) { return k == 0 ? 14 : (k == 1 ? 14 : 16); }
+
+// index of the member owning global chunk/tile `x` (largest k with first[k] <= x)
+template <typename F>
+__device__ __forceinline__ int find_member(int n, uint32_t x, F first) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (first(mid) <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// copy member m's table entry and parameters into shared memory (whole CTA)
+__device__ __forceinline__ void load_member(const dclaw_member* __restrict__ mem, const dclaw_params* __restrict__ prm,
+                                            int m, dclaw_member& sM, dclaw_params& sP) {
+    const int nM = (int)(sizeof(dclaw_member) / 4), nP = (int)(sizeof(dclaw_params) / 4);
+    for (int k = threadIdx.x; k < nM + nP; k += blockDim.x) {
+        if (k < nM) reinterpret_cast<int*>(&sM)[k] = reinterpret_cast<const int*>(mem + m)[k];
+        else reinterpret_cast<int*>(&sP)[k - nM] = reinterpret_cast<const int*>(prm + m)[k - nM];
+    }
+}
+
+__global__ void __launch_bounds__(TPB) k_records_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
+                                                       const dclaw_params* __restrict__ prm, dclaw_clock* clocks,
+                                                       const double* __restrict__ q_in, const double* __restrict__ b,
+                                                       double* __restrict__ work, unsigned int* counters) {
+    __shared__ dclaw_member sM;
+    __shared__ dclaw_params sP;
+    __shared__ int s_m;
+    if (blockIdx.x == 0 && threadIdx.x == 0) counters[0] = 0u;  // the tile queue of this step
+    int cur = -1;
+    for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+        if (threadIdx.x == 0) s_m = find_member(nmem, ch, [&](int k) { return mem[k].rchunk0; });
+        __syncthreads();
+        const int m = s_m;
+        if (m != cur) {
+            load_member(mem, prm, m, sM, sP);
+            __syncthreads();
+            cur = m;
+        }
+        const Geom g{sM.mx, sM.my, sM.mx + 4, sM.my + 4, sM.dx, sM.dy};
+        const size_t npad = (size_t)g.PX * g.PY;
+        const Rec R{work + sM.rec_off, npad};
+        const size_t idx = (size_t)(ch - sM.rchunk0) * TPB + threadIdx.x;
+        if (idx < npad) {
+            int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
+            if (cell_record(sP, g, q_in + sM.q_off, b + sM.b_off, R, i, j)) flag_status(clocks + m, DCLAW_ERR_NAN);
+        }
+        __syncthreads();
+    }
+}
+
+template <int TX, int TY>
+__global__ void __launch_bounds__(TPB, 2) k_tile_batch(int nmem, uint32_t ntiles, const dclaw_member* __restrict__ mem,
+                                                       const dclaw_params* __restrict__ prm, dclaw_clock* clocks,
+                                                       const double* __restrict__ b, double* __restrict__ work,
+                                                       unsigned int* counters) {
+    extern __shared__ double smem[];
+    __shared__ dclaw_member sM;
+    __shared__ dclaw_params sP;
+    __shared__ unsigned int s_t;
+    __shared__ int s_m;
+    __shared__ double red[TPB / 32];
+    int cur = -1;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            s_t = atomicAdd(counters, 1u);
+            s_m = s_t < ntiles ? find_member(nmem, s_t, [&](int k) { return mem[k].tile0; }) : -1;
+        }
+        __syncthreads();
+        const unsigned int t = s_t;
+        const int m = s_m;
+        if (t >= ntiles) break;
+        if (m != cur) {
+            load_member(mem, prm, m, sM, sP);
+            __syncthreads();
+            cur = m;
+        }
+        const Geom g{sM.mx, sM.my, sM.mx + 4, sM.my + 4, sM.dx, sM.dy};
+        const Rec R{work + sM.rec_off, (size_t)g.PX * g.PY};
+        const unsigned int lt = t - sM.tile0;
+        const int i0 = 1 + (int)(lt % sM.ntiles_x) * TX, j0 = 1 + (int)(lt / sM.ntiles_x) * TY;
+        bool nan;
+        double cfl = tile_body<TX, TY, false>(sP, g, R, b + sM.b_off, work + sM.qs_off, clocks[m].dt, i0, j0, smem,
+                                              nullptr, nan);
+        if (nan) flag_status(clocks + m, DCLAW_ERR_NAN);
+        // block max of this tile's Courant number into member m's clock
+        cfl = warp_max(cfl);
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        if (lane == 0) red[wid] = cfl;
+        __syncthreads();
+        if (wid == 0) {
+            double x = lane < TPB / 32 ? red[lane] : 0.0;
+            x = warp_max(x);
+            if (lane == 0 && x > 0.0)
+                atomicMax(reinterpret_cast<unsigned long long*>(&clocks[m].cfl_bits),
+                          (unsigned long long)__double_as_longlong(x));
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(TPB) k_src2_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
+                                                    const dclaw_params* __restrict__ prm, dclaw_clock* clocks,
+                                                    double* __restrict__ q_out, const double* __restrict__ work) {
+    __shared__ dclaw_member sM;
+    __shared__ dclaw_params sP;
+    __shared__ int s_m;
+    int cur = -1;
+    for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+        if (threadIdx.x == 0) s_m = find_member(nmem, ch, [&](int k) { return mem[k].schunk0; });
+        __syncthreads();
+        const int m = s_m;
+        if (m != cur) {
+            load_member(mem, prm, m, sM, sP);
+            __syncthreads();
+            cur = m;
+        }
+        const Geom g{sM.mx, sM.my, sM.mx + 4, sM.my + 4, sM.dx, sM.dy};
+        const size_t n = (size_t)g.mx * g.my;
+        const size_t idx = (size_t)(ch - sM.schunk0) * TPB + threadIdx.x;
+        const double dt = clocks[m].dt;
+        if (idx < n) cell_src2(sP, g, dt, work + sM.qs_off, q_out + sM.q_off, idx);
+        // the last finished chunk of member m applies its tick
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            unsigned int done = atomicAdd(&clocks[m].blocks_done, 1u);
+            if (done == sM.nschunks - 1) {
+                __threadfence();
+                tick_device(sP, clocks + m);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <int TX, int TY>
+inline int batch_tile_attr() {
+    static bool done[MAX_DEVICES] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return DCLAW_ERR_CUDA;
+    if (!done[dev]) {
+        if (cudaFuncSetAttribute(k_tile_batch<TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TileGeom<TX, TY>::SMEM_BYTES) != cudaSuccess)
+            return DCLAW_ERR_CUDA;
+        done[dev] = true;
+    }
+    return DCLAW_OK;
+}
+
+template <int TX, int TY>
+inline int launch_tile_batch(const dclaw_batch* B, const dclaw_member* mem, const dclaw_params* prm, dclaw_clock* clocks,
+                             const double* b, double* work, unsigned int* counters, int nsm, cudaStream_t s) {
+    if (batch_tile_attr<TX, TY>() != DCLAW_OK) return DCLAW_ERR_CUDA;
+    unsigned grid = (unsigned)(nsm * (B->tile_ctas_per_sm > 0 ? B->tile_ctas_per_sm : 2));
+    if (grid > B->ntiles) grid = B->ntiles > 0 ? B->ntiles : 1;
+    k_tile_batch<TX, TY><<<grid, TPB, TileGeom<TX, TY>::SMEM_BYTES, s>>>(B->nmembers, B->ntiles, mem, prm, clocks, b,
+                                                                        work, counters);
+    return DCLAW_OK;
+}
+
+inline int sm_count() {
+    static int n[MAX_DEVICES] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return 0;
+    if (!n[dev]) cudaDeviceGetAttribute(&n[dev], cudaDevAttrMultiProcessorCount, dev);
+    return n[dev];
 }
 
 // ---- patch calls (padded layout) ------------------------------------------
@@ -461,7 +648,6 @@ inline int cuda_status() {
 
 // the tile kernel's dynamic shared memory above 48 KB must be opted into
 // once per device (function attributes belong to the device's context)
-constexpr int MAX_DEVICES = 64;
 inline int ensure_tile_smem_attr() {
     static bool done[MAX_DEVICES] = {};
     int dev = 0;
@@ -725,6 +911,105 @@ int dclaw_step_noalloc(const double* q_in, double* q_out, const double* b, int m
     dim3 grid((mx + TILE_X - 1) / TILE_X, (my + TILE_Y - 1) / TILE_Y);
     k_tile<TILE_X, TILE_Y, true><<<grid, TPB, TileGeom<TILE_X, TILE_Y>::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock,
                                                                                      nullptr);
+    return cuda_status();
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int dclaw_batch_tile_shapes(int32_t* tx, int32_t* ty, int max) {
+    int n = 0;
+    for (int k = 0; k < NBATCH_SHAPES && k < max; ++k, ++n) {
+        if (tx) tx[k] = batch_tx(k);
+        if (ty) ty[k] = batch_ty(k);
+    }
+    return n;
+}
+
+int dclaw_batch_layout(int n, const int32_t* mx, const int32_t* my, const double* dx, const double* dy,
+                       int tile_shape, dclaw_member* members, dclaw_batch* batch) {
+    if (n <= 0 || !mx || !my || !dx || !dy || !members || !batch) return DCLAW_ERR_ARG;
+    if (tile_shape < 0 || tile_shape >= NBATCH_SHAPES) return DCLAW_ERR_ARG;
+    const int TX = batch_tx(tile_shape), TY = batch_ty(tile_shape);
+    uint64_t q = 0, bb = 0, w = 0;
+    uint32_t tiles = 0, rch = 0, sch = 0;
+    for (int k = 0; k < n; ++k) {
+        if (!sizes_ok(mx[k], my[k]) || !(dx[k] > 0.0) || !(dy[k] > 0.0)) return DCLAW_ERR_ARG;
+        dclaw_member& M = members[k];
+        memset(&M, 0, sizeof(M));
+        M.mx = mx[k];
+        M.my = my[k];
+        M.dx = dx[k];
+        M.dy = dy[k];
+        const uint64_t cells = (uint64_t)mx[k] * my[k];
+        const uint64_t npad = (uint64_t)(mx[k] + 4) * (my[k] + 4);
+        M.q_off = q;
+        q += 5 * cells;
+        M.b_off = bb;
+        bb += cells;
+        M.rec_off = w;
+        w += (uint64_t)NREC * npad;
+        M.qs_off = w;
+        w += 5 * cells;
+        w = (w + 31) & ~(uint64_t)31;  // 256-byte alignment of every member's block
+        M.ntiles_x = (uint32_t)((mx[k] + TX - 1) / TX);
+        M.ntiles = M.ntiles_x * (uint32_t)((my[k] + TY - 1) / TY);
+        M.tile0 = tiles;
+        tiles += M.ntiles;
+        M.nrchunks = (uint32_t)((npad + TPB - 1) / TPB);
+        M.rchunk0 = rch;
+        rch += M.nrchunks;
+        M.nschunks = (uint32_t)((cells + TPB - 1) / TPB);
+        M.schunk0 = sch;
+        sch += M.nschunks;
+    }
+    memset(batch, 0, sizeof(*batch));
+    batch->nmembers = n;
+    batch->tile_shape = tile_shape;
+    batch->tile_ctas_per_sm = 2;
+    batch->cell_ctas_per_sm = 8;
+    batch->ntiles = tiles;
+    batch->nrchunks = rch;
+    batch->nschunks = sch;
+    batch->q_doubles = q;
+    batch->b_doubles = bb;
+    batch->work_bytes = w * 8 + 256;  // + work-queue counters
+    return DCLAW_OK;
+}
+
+int dclaw_batch_reset(const dclaw_batch* batch, void* work, void* stream) {
+    if (!batch || !work) return DCLAW_ERR_ARG;
+    unsigned int* counters = (unsigned int*)((char*)work + (batch->work_bytes - 256));
+    cudaMemsetAsync(counters, 0, 256, (cudaStream_t)stream);
+    return cuda_status();
+}
+
+int dclaw_step_batched(const dclaw_batch* batch, const dclaw_member* members, const dclaw_params* params,
+                       dclaw_clock* clocks, const double* q_in, double* q_out, const double* b, void* work,
+                       void* stream) {
+    if (!batch || !members || !params || !clocks || !q_in || !q_out || !b || !work || q_in == q_out)
+        return DCLAW_ERR_ARG;
+    if (batch->nmembers <= 0 || batch->tile_shape < 0 || batch->tile_shape >= NBATCH_SHAPES) return DCLAW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nsm = sm_count();
+    if (nsm <= 0) return DCLAW_ERR_CUDA;
+    double* w = (double*)work;
+    unsigned int* counters = (unsigned int*)((char*)work + (batch->work_bytes - 256));
+    const int cpsm = batch->cell_ctas_per_sm > 0 ? batch->cell_ctas_per_sm : 8;
+    unsigned g1 = (unsigned)(nsm * cpsm);
+    if (g1 > batch->nrchunks) g1 = batch->nrchunks;
+    k_records_batch<<<g1, TPB, 0, s>>>(batch->nmembers, batch->nrchunks, members, params, clocks, q_in, b, w, counters);
+    int rc = DCLAW_OK;
+    switch (batch->tile_shape) {
+        case 0: rc = launch_tile_batch<batch_tx(0), batch_ty(0)>(batch, members, params, clocks, b, w, counters, nsm, s); break;
+        case 1: rc = launch_tile_batch<batch_tx(1), batch_ty(1)>(batch, members, params, clocks, b, w, counters, nsm, s); break;
+        default: rc = launch_tile_batch<batch_tx(2), batch_ty(2)>(batch, members, params, clocks, b, w, counters, nsm, s); break;
+    }
+    if (rc != DCLAW_OK) return rc;
+    unsigned g3 = (unsigned)(nsm * cpsm);
+    if (g3 > batch->nschunks) g3 = batch->nschunks;
+    k_src2_batch<<<g3, TPB, 0, s>>>(batch->nmembers, batch->nschunks, members, params, clocks, q_out, w);
     return cuda_status();
 }
 

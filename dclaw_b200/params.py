@@ -78,6 +78,32 @@ class CClock(ctypes.Structure):
 CLOCK_DOUBLES = ctypes.sizeof(CClock) // 8  # the clock is kept in a float64 tensor
 
 
+class CMember(ctypes.Structure):
+    """ctypes image of `dclaw_member` (one ensemble member's table entry)."""
+
+    _fields_ = [
+        ("mx", ctypes.c_int32), ("my", ctypes.c_int32),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+        ("q_off", ctypes.c_uint64), ("b_off", ctypes.c_uint64),
+        ("rec_off", ctypes.c_uint64), ("qs_off", ctypes.c_uint64),
+        ("tile0", ctypes.c_uint32), ("ntiles_x", ctypes.c_uint32), ("ntiles", ctypes.c_uint32),
+        ("rchunk0", ctypes.c_uint32), ("nrchunks", ctypes.c_uint32),
+        ("schunk0", ctypes.c_uint32), ("nschunks", ctypes.c_uint32), ("pad_", ctypes.c_uint32),
+    ]
+
+
+class CBatch(ctypes.Structure):
+    """ctypes image of `dclaw_batch` (an ensemble's totals and launch choices)."""
+
+    _fields_ = [
+        ("nmembers", ctypes.c_int32), ("tile_shape", ctypes.c_int32),
+        ("tile_ctas_per_sm", ctypes.c_int32), ("cell_ctas_per_sm", ctypes.c_int32),
+        ("ntiles", ctypes.c_uint32), ("nrchunks", ctypes.c_uint32), ("nschunks", ctypes.c_uint32),
+        ("pad_", ctypes.c_uint32),
+        ("q_doubles", ctypes.c_uint64), ("b_doubles", ctypes.c_uint64), ("work_bytes", ctypes.c_uint64),
+    ]
+
+
 @dataclasses.dataclass
 class DClawParams:
     """D-Claw parameters for one run (or one ensemble member).

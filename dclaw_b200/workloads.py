@@ -183,3 +183,39 @@ def lake_at_rest(params: DClawParams | None = None) -> Case:
     q = np.stack([h, z, z, h * m, 1000.0 * 9.81 * h])
     q = _admissible(q, p)
     return Case("lake_at_rest", q, b, dx, dx, p, 0, 0.01)
+
+
+# ---- flume ensembles (batched particle-filter case) -------------------------
+def flume_member(width: int, length: int, dx: float, params: DClawParams, slope_deg: float = 31.0,
+                 runout_frac: float = 0.25, block_len: float = 3.0, block_h: float = 1.0, p_ratio: float = 0.8):
+    """One channel: `length` cells along x at dx, `width` cells across; a
+    planar slope of slope_deg down to a horizontal runout over the last
+    runout_frac of the length; a rectangular release block block_len m long
+    and block_h m high at the head (3 m^2 per metre of width: the cross
+    section of a 6 m^3 release in a 2 m wide flume), at rest."""
+    x = (np.arange(length) + 0.5) * dx
+    L = length * dx
+    xb = (1.0 - runout_frac) * L
+    b1 = math.tan(math.radians(slope_deg)) * np.maximum(xb - x, 0.0)
+    b = np.broadcast_to(b1[None, :], (width, length)).copy()
+    h1 = np.where((x >= 0.5) & (x < 0.5 + block_len), block_h, 0.0)
+    h = np.broadcast_to(h1[None, :], (width, length)).copy()
+    q = state_from(h, np.full_like(h, params.m0), params, p_ratio)
+    return q, b
+
+
+def flume_ensemble(n: int = 256, seed: int = 0, dx: float = 0.05, width_range=(32, 128),
+                   length_range=(1024, 4096), nsteps: int = 2000):
+    """n flume members of uneven sizes with per-member parameters drawn from
+    the priors phi U[28, 40] deg, log10 k0 U[-11, -8], m0 U[0.55, 0.65],
+    alpha U[0.005, 0.05]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        w = int(rng.integers(width_range[0], width_range[1] + 1))
+        L = int(rng.integers(length_range[0], length_range[1] + 1))
+        p = DClawParams(phi=float(rng.uniform(28.0, 40.0)), kref=float(10.0 ** rng.uniform(-11.0, -8.0)),
+                        m0=float(rng.uniform(0.55, 0.65)), alpha_c=float(rng.uniform(0.005, 0.05)))
+        q, b = flume_member(w, L, dx, p)
+        out.append(Case(f"flume_{w}x{L}", q, b, dx, dx, p, nsteps, 1.0e-3))
+    return out

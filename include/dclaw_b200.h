@@ -182,6 +182,63 @@ int dclaw_step_noalloc(const double* q_in, double* q_out, const double* b, int m
                        void* stream);
 /* largest patch (padded cells) dclaw_step_noalloc accepts */
 size_t dclaw_step_noalloc_max_cells(void);
+/* ---- batched ensemble -------------------------------------------------------
+ * An ensemble of independent uniform patches of uneven sizes, each with its
+ * own parameters and its own clock (the particle-filter use of the
+ * reference's differentiable port: one simulation per particle,
+ * gradient_particle_filter/pf_flume/flume_model.py:129-179, vmapped in
+ * pf_flume/inference.py:96-108). All members advance together: one step of
+ * the ensemble is three launches of persistent kernels (cell records, a
+ * dynamic work queue over every member's tiles, src2 + each member's tick),
+ * so a sequence of ensemble steps captures into one CUDA graph.
+ * Member m's state is 5 planes [5][my][mx] at q_off in the state arenas; its
+ * bed is [my][mx] at b_off in the bed arena. */
+typedef struct dclaw_member {
+    int32_t mx, my;
+    double dx, dy;
+    uint64_t q_off;       /* doubles into the state arenas */
+    uint64_t b_off;       /* doubles into the bed arena */
+    uint64_t rec_off;     /* doubles into the workspace: per-cell records */
+    uint64_t qs_off;      /* doubles into the workspace: state before src2 */
+    uint32_t tile0;       /* first tile of the member in the ensemble's tile list */
+    uint32_t ntiles_x;    /* tiles along x */
+    uint32_t ntiles;      /* tiles of the member */
+    uint32_t rchunk0;     /* first 256-cell chunk of the member's padded cells */
+    uint32_t nrchunks;
+    uint32_t schunk0;     /* first 256-cell chunk of the member's interior cells */
+    uint32_t nschunks;
+    uint32_t pad_;
+} dclaw_member;
+
+typedef struct dclaw_batch {
+    int32_t nmembers;
+    int32_t tile_shape;        /* index into dclaw_batch_tile_shapes() */
+    int32_t tile_ctas_per_sm;  /* persistent tile CTAs per SM (1 or 2) */
+    int32_t cell_ctas_per_sm;  /* persistent CTAs per SM of the cell kernels */
+    uint32_t ntiles;           /* tiles of all members (for tile_shape) */
+    uint32_t nrchunks, nschunks;
+    uint32_t pad_;
+    uint64_t q_doubles;        /* size of one state arena */
+    uint64_t b_doubles;        /* size of the bed arena */
+    uint64_t work_bytes;       /* workspace size */
+} dclaw_batch;
+
+/* tile shapes compiled for the ensemble kernels; returns how many (<= max) */
+int dclaw_batch_tile_shapes(int32_t* tx, int32_t* ty, int max);
+/* host-side layout of n members (sizes and spacings in host arrays): fills
+ * members[0..n) (host array) and *batch for the given tile shape */
+int dclaw_batch_layout(int n, const int32_t* mx, const int32_t* my, const double* dx, const double* dy,
+                       int tile_shape, dclaw_member* members, dclaw_batch* batch);
+/* one step of every member. batch: host; members, params, clocks: DEVICE
+ * arrays of nmembers; q_in / q_out: distinct state arenas; b: bed arena;
+ * work: batch->work_bytes (the tile queue counter inside it must be zero
+ * before the first step: dclaw_batch_reset). */
+int dclaw_step_batched(const dclaw_batch* batch, const dclaw_member* members, const dclaw_params* params,
+                       dclaw_clock* clocks, const double* q_in, double* q_out, const double* b, void* work,
+                       void* stream);
+/* zero the ensemble's work-queue counters (before the first step) */
+int dclaw_batch_reset(const dclaw_batch* batch, void* work, void* stream);
+
 /* initialise a device clock: t, dt, t_final, fixed_dt; counters cleared */
 int dclaw_clock_init(dclaw_clock* clock, double t, double dt, double t_final, int fixed_dt,
                      void* stream);
