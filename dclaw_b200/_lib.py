@@ -41,6 +41,10 @@ SIGNATURES = {
     "dclaw_batch_layout": (_int, [_int, _vp, _vp, _vp, _vp, _int, ctypes.POINTER(CMember), ctypes.POINTER(CBatch)]),
     "dclaw_step_batched": (_int, [ctypes.POINTER(CBatch), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dclaw_batch_reset": (_int, [ctypes.POINTER(CBatch), _vp, _vp]),
+    "dclaw_adjoint_workspace_bytes": (_sz, [_int, _int]),
+    "dclaw_adjoint_supported": (_int, [_pp]),
+    "dclaw_step_adjoint": (_int, [_vp, _vp, _int, _int, _dbl, _dbl, _vp, _pp, _vp, _vp, _vp, _vp, _sz, _vp,
+                                  _vp]),
 }
 
 _lib = None

@@ -1,0 +1,222 @@
+"""Reverse-mode gradients of runs of the uniform-patch step.
+
+The reference's differentiable port takes gradients with `jax.grad` through
+`rollout_peak(..., checkpoint_block=k)`, whose nested `jax.checkpoint` scans
+keep about n/k + k states (differentiable_dclaw/dclaw_jax/solver.py:357-388,
+differentiable_dclaw/tests/test_reverse_mode.py:37-49). Here the step is the
+reference Fortran's (the fused CUDA step of `solver.PatchStepper`) and its
+reverse is hand-written (`dclaw_step_adjoint` of the C ABI, one launch
+sequence per step), wrapped in a `torch.autograd.Function` with the same
+sqrt(N) time checkpointing:
+
+* forward: run the fused step, record each step's dt on the device, keep the
+  state every k steps (k = ceil(sqrt(n_steps)) unless given) and the states
+  the caller asked for;
+* backward: for each block of k steps, last block first, recompute its
+  states from its checkpoint with the recorded dts (bit-identical, so every
+  branch is the one the forward took), then run the step adjoint backwards
+  through the block, adding the caller's output gradients as it passes them.
+
+Time steps are data: the dt of each step (chosen by D-Claw's tick rule from
+the previous Courant number, or fixed) is recorded in the forward pass and
+not differentiated. Gradients flow to the initial state and to the material
+parameters theta = (phi [deg], kref, alpha_c, mu).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from typing import Sequence
+
+import torch
+
+from . import _lib
+from .params import DClawParams
+from .solver import PatchStepper
+
+THETA_NAMES = ("phi", "kref", "alpha_c", "mu")
+_DEG = math.pi / 180.0
+
+
+def theta_of(params: DClawParams, device=None) -> torch.Tensor:
+    """(phi [deg], kref, alpha_c, mu) of a parameter set as a float64 tensor."""
+    return torch.tensor([params.phi, params.kref, params.alpha_c, params.mu], dtype=torch.float64, device=device)
+
+
+def with_theta(params: DClawParams, theta) -> DClawParams:
+    vals = [float(v) for v in (theta.tolist() if torch.is_tensor(theta) else theta)]
+    return params.replace(**dict(zip(THETA_NAMES, vals)))
+
+
+class StepAdjoint:
+    """The adjoint of one step of a fixed patch (bed, parameters, sizes).
+
+    vjp(q_in, dt, lam_out, lam_in, pbar): lam_in = (dS/dq)^T lam_out and
+    pbar += (dS/dtheta)^T lam_out with phi in radians; dt is a one-element
+    float64 device tensor (the step's dt); all arrays are (5, my, mx).
+    """
+
+    def __init__(self, b: torch.Tensor, params: DClawParams, dx: float, dy: float):
+        self.lib = _lib.load()
+        self.cp = params.to_c()
+        _lib.check(self.lib.dclaw_adjoint_supported(ctypes.byref(self.cp)), "adjoint options")
+        self.b = b.contiguous()
+        self.my, self.mx = self.b.shape
+        self.dx, self.dy = float(dx), float(dy)
+        self.work_bytes = self.lib.dclaw_adjoint_workspace_bytes(self.mx, self.my)
+        if self.work_bytes == 0:
+            raise _lib.DClawError("invalid patch size")
+        self.work = torch.empty(self.work_bytes, dtype=torch.uint8, device=b.device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=b.device)
+
+    def vjp(self, q_in: torch.Tensor, dt: torch.Tensor, lam_out: torch.Tensor, lam_in: torch.Tensor,
+            pbar: torch.Tensor) -> None:
+        rc = self.lib.dclaw_step_adjoint(_lib.ptr(q_in), _lib.ptr(self.b), self.mx, self.my, self.dx, self.dy,
+                                         _lib.ptr(dt), ctypes.byref(self.cp), _lib.ptr(lam_out), _lib.ptr(lam_in),
+                                         _lib.ptr(pbar), _lib.ptr(self.work), self.work_bytes,
+                                         _lib.ptr(self.status), _lib.stream_ptr())
+        _lib.check(rc, "dclaw_step_adjoint")
+
+    def check_status(self) -> None:
+        _lib.check(int(self.status.item()), "adjoint step")
+
+
+def _block(n_steps: int, checkpoint_block: int | None) -> int:
+    if checkpoint_block is None:
+        return max(1, math.ceil(math.sqrt(n_steps)))
+    if checkpoint_block < 1:
+        raise ValueError("checkpoint_block must be >= 1")
+    return int(checkpoint_block)
+
+
+class _Rollout(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, q0, theta, b, params, dx, dy, n_steps, out_steps, dt0, fixed_dt, t_final, checkpoint_block,
+                dt_schedule):
+        prm = with_theta(params, theta.detach().cpu())
+        st = PatchStepper(q0.detach(), b, prm, dx, dy)
+        if dt_schedule is not None:
+            st.init_clock(0.0, fixed_dt=True)
+        else:
+            st.init_clock(float(dt0), t_final=float(t_final), fixed_dt=bool(fixed_dt))
+        k = _block(n_steps, checkpoint_block)
+        dts = torch.empty(n_steps, dtype=torch.float64, device=q0.device)
+        ckpt = []
+        outs = torch.empty((len(out_steps),) + tuple(q0.shape), dtype=q0.dtype, device=q0.device)
+        where = {}
+        for idx, n in enumerate(out_steps):
+            where.setdefault(n, []).append(idx)
+        for idx in where.get(0, []):
+            outs[idx].copy_(q0)
+        for n in range(n_steps):
+            if n % k == 0:
+                ckpt.append(st.state().clone())
+            if dt_schedule is not None:
+                st.clock[1:2].copy_(dt_schedule[n:n + 1])
+            st.step(1)
+            dts[n:n + 1].copy_(st.clock[3:4])   # dt the step used
+            for idx in where.get(n + 1, []):
+                outs[idx].copy_(st.state())
+        _lib.check(st.status(), "rollout forward")
+        ctx.save_for_backward(b, dts)
+        ctx.ckpt = ckpt
+        ctx.meta = (prm, float(dx), float(dy), int(n_steps), tuple(out_steps), k)
+        return outs
+
+    @staticmethod
+    def backward(ctx, g_out):
+        b, dts = ctx.saved_tensors
+        prm, dx, dy, n_steps, out_steps, k = ctx.meta
+        dev = b.device
+        shape = ctx.ckpt[0].shape
+        where = {}
+        for idx, n in enumerate(out_steps):
+            where.setdefault(n, []).append(idx)
+        adj = StepAdjoint(b, prm, dx, dy)
+        fw = PatchStepper(ctx.ckpt[0], b, prm, dx, dy)
+        fw.init_clock(0.0, fixed_dt=True)
+        lam = torch.zeros(shape, dtype=torch.float64, device=dev)
+        lam2 = torch.empty_like(lam)
+        pbar = torch.zeros(4, dtype=torch.float64, device=dev)
+        seg = torch.empty((k,) + tuple(shape), dtype=torch.float64, device=dev)
+        g_out = g_out.contiguous() if g_out is not None else None
+        nblocks = len(ctx.ckpt)
+        for s in reversed(range(nblocks)):
+            n0 = s * k
+            n1 = min(n0 + k, n_steps)
+            # recompute the block's states n0 .. n1-1 with the recorded dts
+            seg[0].copy_(ctx.ckpt[s])
+            fw.qa.copy_(ctx.ckpt[s])
+            for n in range(n0 + 1, n1):
+                fw.clock[1:2].copy_(dts[n - 1:n])
+                fw.step(1)
+                seg[n - n0].copy_(fw.state())
+            for n in range(n1, n0, -1):
+                if g_out is not None:
+                    for idx in where.get(n, []):
+                        lam.add_(g_out[idx])
+                adj.vjp(seg[n - 1 - n0], dts[n - 1:n], lam, lam2, pbar)
+                lam, lam2 = lam2, lam
+        if g_out is not None:
+            for idx in where.get(0, []):
+                lam.add_(g_out[idx])
+        _lib.check(fw.status(), "rollout recompute")
+        adj.check_status()
+        scale = torch.tensor([_DEG, 1.0, 1.0, 1.0], dtype=torch.float64, device=dev)
+        return lam, pbar * scale, None, None, None, None, None, None, None, None, None, None, None
+
+
+def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b: torch.Tensor, params: DClawParams, dx: float,
+                   dy: float, n_steps: int, out_steps: Sequence[int], dt0: float, fixed_dt: bool = False,
+                   t_final: float = 0.0, checkpoint_block: int | None = None,
+                   dt_schedule: torch.Tensor | None = None) -> torch.Tensor:
+    """Differentiable run of n_steps fused steps on one patch.
+
+    q0: (5, my, mx) float64 CUDA tensor (x fastest), theta: (4,) float64
+    tensor (phi [deg], kref, alpha_c, mu) overriding those fields of params,
+    b: (my, mx). Returns the states after each step count in out_steps
+    (0 = q0), shape (len(out_steps), 5, my, mx). dt0 is the first dt; with
+    fixed_dt every step uses it, otherwise the tick rule picks the next dt
+    from the Courant number (clipped at t_final when t_final > 0). Gradients
+    reach q0 and theta through the hand-written step adjoint with sqrt(N)
+    checkpointing (checkpoint_block steps per block, default ceil(sqrt(n))).
+    dt_schedule (n_steps,) float64 device tensor: replay these dts instead
+    (dt0, fixed_dt and t_final are then ignored) -- e.g. the dts of an
+    earlier adaptive run, for finite-difference checks at a fixed schedule.
+    """
+    for n in out_steps:
+        if not 0 <= n <= n_steps:
+            raise ValueError(f"output step {n} outside 0..{n_steps}")
+    if dt_schedule is not None:
+        if dt_schedule.shape != (n_steps,) or dt_schedule.dtype != torch.float64 or not dt_schedule.is_cuda:
+            raise ValueError("dt_schedule must be a (n_steps,) float64 CUDA tensor")
+        dt_schedule = dt_schedule.contiguous()
+    return _Rollout.apply(q0, theta, b.contiguous(), params, dx, dy, int(n_steps), tuple(int(n) for n in out_steps),
+                          float(dt0), bool(fixed_dt), float(t_final), checkpoint_block, dt_schedule)
+
+
+def last_dts(out: torch.Tensor) -> torch.Tensor:
+    """The per-step dts recorded by the rollout that produced `out`."""
+    fn = out.grad_fn
+    if fn is None or not hasattr(fn, "saved_tensors"):
+        raise ValueError("not the output of a differentiable rollout")
+    return fn.saved_tensors[1]
+
+
+def initial_state(h0: torch.Tensor, m0: torch.Tensor, params: DClawParams, p_ratio: float = 0.8) -> torch.Tensor:
+    """Differentiable (5, my, mx) state at rest from a depth field and a solid
+    fraction (scalar or field): hm = h m, pb = p_ratio rho_f g h, then the
+    admissibility clip of qfix (digclaw_module.f90:285-345; init_ptype = 3
+    style pore pressure, qinit.f90:264-285). Dry cells (h <= dry_tolerance)
+    are zero."""
+    wet = h0 > params.dry_tolerance
+    hs = torch.where(wet, h0, torch.ones_like(h0))
+    m = torch.clamp((h0 * m0) / hs, 0.0, 1.0)
+    rho = params.rho_s * m + (1.0 - m) * params.rho_f
+    pb = torch.minimum(torch.clamp(p_ratio * params.rho_f * params.grav * h0, min=0.0), rho * params.grav * h0)
+    z = torch.zeros_like(h0)
+    q = torch.stack([h0, z, z, h0 * m, pb])
+    return torch.where(wet.unsqueeze(0), q, torch.zeros_like(q))
+
+
+__all__ = ["StepAdjoint", "rollout_states", "theta_of", "with_theta", "initial_state", "last_dts", "THETA_NAMES"]

@@ -445,7 +445,6 @@ DC_HD bool riemann_solve_b(const dclaw_params& P, const Side& L, const Side& R, 
     RType rt = riemanntype(hL, hR, uL, uR, drytol, geps);
     double sw1 = fmin2(sE1, rt.s2m);
     double sw3 = fmax2(sE2, rt.s1m);
-    double sw2 = 0.5 * (sw3 + sw1);
     double Dd = sE2 - sE1;
     double Qh = (huL - huR + sE2 * hR - sE1 * hL) / Dd;
     double hstarHLL = fmax2(Qh, 0.0);
@@ -815,9 +814,10 @@ DC_HD void zero_cellb(CellB& c) {
     c.fs = c.taudir = c.b = 0.0;
 }
 
-// load_side reverse (see load_side): Side adjoint -> cell adjoint
-DC_HD void load_side_b(const dclaw_params& P, const Work& W, size_t pi, int comp_n, int comp_t, bool twice,
-                       const SideB& sb, CellB& cb, double* pbar) {
+// load_side reverse (see load_side): Side adjoint -> cell adjoint, with
+// setvars' partial derivatives read from the record (svrec_cell)
+DC_HD void load_side_b_sv(const dclaw_params& P, const Work& W, const double* __restrict__ sv, size_t pi,
+                          int comp_n, int comp_t, bool twice, const SideB& sb, CellB& cb, double* pbar) {
     cb.b += sb.b;
     cb.fs += sb.fs;
     cb.taudir += sb.taudir;
@@ -829,15 +829,18 @@ DC_HD void load_side_b(const dclaw_params& P, const Work& W, size_t pi, int comp
     double p0 = W.qB[4 * W.npad + pi];
     double hm1 = hm0, p1 = p0, m1;
     qfix_mp(P, h, hm1, p1, m1, P.grav);
-    double hm = hm1, p = p1, m = m1;
-    if (twice) qfix_mp(P, h, hm, p, m, P.grav);
     double un = hn / h, ut = ht / h;
-    SetVars ob{};
-    ob.rho = sb.rho_sv;
-    ob.tau = sb.tau_sv;
-    double phib = 0.0, hb = sb.h, unb = sb.un, utb = sb.ut, mb = sb.m, pb = sb.p;
-    setvars_b<false>(P, P.phi, h, un, ut, m, p, P.grav, ob, phib, hb, unb, utb, mb, pb, pbar);
-    pbar[PB_PHI] += phib;
+    const double* r = sv + (size_t)(twice ? SV_N : 0) * W.npad + pi;
+    const size_t np = W.npad;
+    const double tb = sb.tau_sv;
+    const int kn = comp_n == 1 ? SV_DU : SV_DV, kt = comp_n == 1 ? SV_DV : SV_DU;
+    double hb = sb.h + tb * r[SV_DH * np];
+    double unb = sb.un + tb * r[(size_t)kn * np];
+    double utb = sb.ut + tb * r[(size_t)kt * np];
+    double mb = sb.m + (tb * r[SV_DM * np] + sb.rho_sv * (P.rho_s - P.rho_f));
+    double pb = sb.p + tb * r[SV_DP * np];
+    pbar[PB_PHI] += tb * r[SV_DPHI * np];
+    pbar[PB_MU] += tb * r[SV_DMU * np];
     double hnb = sb.hn + unb / h, htb = sb.ht + utb / h;
     hb -= unb * un / h + utb * ut / h;
     double hmb = sb.hm;
@@ -853,19 +856,47 @@ DC_HD void load_side_b(const dclaw_params& P, const Work& W, size_t pi, int comp
     cb.q[4] += pb;
 }
 
+// setvars record of padded cell pi: for the rpn2 states A1 and A2, tau and
+// its partial derivatives (the reverse of setvars for a unit tau adjoint)
+DC_HD void svrec_cell(const dclaw_params& P, const Work& W, double* __restrict__ sv, size_t pi) {
+    const size_t np = W.npad;
+    const double h = W.qB[pi];
+    if (h <= P.dry_tolerance) return;  // dry sides never read their record
+    const double u = W.qB[np + pi] / h, v = W.qB[2 * np + pi] / h;
+    double hm = W.qB[3 * np + pi], p = W.qB[4 * np + pi], m;
+    for (int a = 0; a < 2; ++a) {
+        qfix_mp(P, h, hm, p, m, P.grav);
+        SetVars s = setvars<false>(P, P.phi, h, u, v, m, p, P.grav);
+        SetVars ob{};
+        ob.tau = 1.0;
+        double phib = 0.0, hb = 0.0, ub = 0.0, vb = 0.0, mb = 0.0, pb = 0.0;
+        double pl[NPB] = {0.0, 0.0, 0.0, 0.0};
+        setvars_b<false>(P, P.phi, h, u, v, m, p, P.grav, ob, phib, hb, ub, vb, mb, pb, pl);
+        double* o = sv + (size_t)(a * SV_N) * np + pi;
+        o[SV_TAU * np] = s.tau;
+        o[SV_DH * np] = hb;
+        o[SV_DU * np] = ub;
+        o[SV_DV * np] = vb;
+        o[SV_DM * np] = mb;
+        o[SV_DP * np] = pb;
+        o[SV_DPHI * np] = phib;
+        o[SV_DMU * np] = pl[PB_MU];
+    }
+}
+
 // Stage C reverse: interface i of slice r; wb = adjoint of its 15 stored
 // values (W_* order). Accumulates into the cell adjoints of L and R.
 // Returns false when the interface has no adjoint form (rare-wave corrector).
 template <int DIR>
-DC_HD bool stage_riemann_b(const dclaw_params& P, const Geom& g, const Work& W, int r, int i, const double* wbv,
-                           CellB& Lc, CellB& Rc, double* pbar) {
+DC_HD bool stage_riemann_b(const dclaw_params& P, const Geom& g, const Work& W, const double* __restrict__ sv,
+                           int r, int i, const double* wbv, CellB& Lc, CellB& Rc, double* pbar) {
     size_t pL, pR;
     if (DIR == 0) { pL = pidx(g, i - 1, r); pR = pidx(g, i, r); }
     else { pL = pidx(g, r, i - 1); pR = pidx(g, r, i); }
     const int cn = DIR == 0 ? 1 : 2, ct = DIR == 0 ? 2 : 1;
     if (W.qB[pL] <= P.dry_tolerance && W.qB[pR] <= P.dry_tolerance) return true;
-    Side R = load_side(P, W, pR, cn, ct, false, 1 + DIR);
-    Side L = load_side(P, W, pL, cn, ct, i - 1 >= 0, 1 + DIR);
+    Side R = load_side_sv(P, W, sv, pR, cn, ct, false, 1 + DIR);
+    Side L = load_side_sv(P, W, sv, pL, cn, ct, i - 1 >= 0, 1 + DIR);
     Waves wb;
     wb.s1 = wbv[W_S1]; wb.s2 = wbv[W_S2]; wb.s5 = wbv[W_S5];
     wb.w1h = wbv[W_1H]; wb.w1n = wbv[W_1N]; wb.w1t = wbv[W_1T]; wb.w1m = wbv[W_1M]; wb.w1p = wbv[W_1P];
@@ -875,8 +906,8 @@ DC_HD bool stage_riemann_b(const dclaw_params& P, const Geom& g, const Work& W, 
     zero_sideb(Lb);
     zero_sideb(Rb);
     if (!riemann_solve_b(P, L, R, wb, Lb, Rb)) return false;
-    load_side_b(P, W, pR, cn, ct, false, Rb, Rc, pbar);
-    load_side_b(P, W, pL, cn, ct, i - 1 >= 0, Lb, Lc, pbar);
+    load_side_b_sv(P, W, sv, pR, cn, ct, false, Rb, Rc, pbar);
+    load_side_b_sv(P, W, sv, pL, cn, ct, i - 1 >= 0, Lb, Lc, pbar);
     return true;
 }
 
@@ -1673,6 +1704,8 @@ DC_HD void stage_b4_b(const dclaw_params& P, const Geom& g, const double* __rest
 // The adjoint of one whole step, as per-item stages over the staged forward
 // intermediates (Work, recomputed from the step's input state):
 //
+//   R  adj_item_svrec    padded cell     setvars records of the rpn2 states
+//                                        (after the forward stages A, B)
 //   E  adj_item_src2     interior cell   src2 and the update: adjoint of the
 //                                        updated state (lamq)
 //   D  adj_item_flux     interface       flux differencing, 2nd-order
@@ -1698,7 +1731,13 @@ struct AdjWork {
     double* ycb;   // NCB y-interface planes
     double* tdq;   // NTD padded planes
     double* qsb;   // 5 padded planes
+    double* sv;    // NSV padded planes: setvars records (svrec_cell)
 };
+
+// padded cell (i, j), i in -1..mx+2, j in -1..my+2: setvars records
+DC_HD void adj_item_svrec(const dclaw_params& P, const Geom& g, const Work& W, const AdjWork& A, int i, int j) {
+    svrec_cell(P, W, A.sv, pidx(g, i, j));
+}
 
 DC_HD void adj_item_src2(const dclaw_params& P, const Geom& g, const Work& W, const AdjWork& A,
                          const double* __restrict__ lam_out, int i, int j, double dt, double* pbar) {
@@ -1750,7 +1789,7 @@ DC_HD bool adj_item_riemann(const dclaw_params& P, const Geom& g, const Work& W,
     CellB Lc, Rc;
     zero_cellb(Lc);
     zero_cellb(Rc);
-    bool ok = stage_riemann_b<DIR>(P, g, W, r, i, wb, Lc, Rc, pbar);
+    bool ok = stage_riemann_b<DIR>(P, g, W, A.sv, r, i, wb, Lc, Rc, pbar);
     double* dst = DIR == 0 ? A.xcb : A.ycb;
     const size_t oi = at(i);
     for (int k = 0; k < 5; ++k) {

@@ -11,6 +11,7 @@
 
 #include "stages.cuh"
 #include "tile.cuh"
+#include "workspace.cuh"
 
 namespace dclaw {
 
@@ -594,51 +595,21 @@ __global__ void k_cfl_from_bits(dclaw_clock* clk) {
 // ---- host helpers ----------------------------------------------------------
 inline unsigned nblocks(long long n) { return (unsigned)((n + TPB - 1) / TPB); }
 
-inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
-
-struct Layout {
-    size_t npad, nxi, nyi;
-    size_t off_qB, off_bP, off_td, off_wx, off_wy, off_fx, off_fy, total_staged;
+struct Layout : StagedLayout {
+    size_t total_staged;
     size_t off_rec, off_qstar, total_fused;
-    size_t total;
 };
 
 inline Layout layout(int mx, int my) {
     Layout L;
-    L.npad = (size_t)(mx + 4) * (my + 4);
-    L.nxi = (size_t)(mx + 3) * (my + 2);
-    L.nyi = (size_t)(my + 3) * (mx + 2);
-    size_t o = 0;
-    L.off_qB = o; o += align256(5 * L.npad * 8);
-    L.off_bP = o; o += align256(L.npad * 8);
-    L.off_td = o; o += align256(3 * L.npad * 8);
-    L.off_wx = o; o += align256((size_t)NW * L.nxi * 8);
-    L.off_wy = o; o += align256((size_t)NW * L.nyi * 8);
-    L.off_fx = o; o += align256((size_t)NF * L.nxi * 8);
-    L.off_fy = o; o += align256((size_t)NF * L.nyi * 8);
-    L.total_staged = o;
+    static_cast<StagedLayout&>(L) = staged_layout(mx, my);
+    L.total_staged = L.StagedLayout::total;
     // the fused step needs the cell records and the updated state before src2
     L.off_rec = 0;
     L.off_qstar = align256((size_t)NREC * L.npad * 8);
     L.total_fused = L.off_qstar + align256((size_t)5 * mx * my * 8);
     L.total = L.total_staged > L.total_fused ? L.total_staged : L.total_fused;
     return L;
-}
-
-inline Work make_work(void* base, const Layout& L) {
-    char* b = (char*)base;
-    Work W;
-    W.qB = (double*)(b + L.off_qB);
-    W.bP = (double*)(b + L.off_bP);
-    W.td = (double*)(b + L.off_td);
-    W.wx = (double*)(b + L.off_wx);
-    W.wy = (double*)(b + L.off_wy);
-    W.fx = (double*)(b + L.off_fx);
-    W.fy = (double*)(b + L.off_fy);
-    W.npad = L.npad;
-    W.nxi = L.nxi;
-    W.nyi = L.nyi;
-    return W;
 }
 
 inline int cuda_status() {

@@ -213,11 +213,51 @@ DC_HD Side load_side(const dclaw_params& P, const Work& W, size_t pi, int comp_n
     return s;
 }
 
+// Per-cell setvars records of the two rpn2 states (A1: qfix once, A2:
+// twice) of a wet padded cell, SV_N planes per state (padded layout): tau and
+// its partial derivatives in (h, u, v, m, p, phi, mu), u = hu/h, v = hv/h.
+// setvars reads the velocity only through u^2 + v^2, so the record serves
+// both sweep directions. Written by the adjoint's record stage.
+constexpr int SV_N = 8;
+constexpr int NSV = 2 * SV_N;
+enum { SV_TAU = 0, SV_DH, SV_DU, SV_DV, SV_DM, SV_DP, SV_DPHI, SV_DMU };
+
+// load_side with tau read from the record instead of recomputed (same bits)
+DC_HD Side load_side_sv(const dclaw_params& P, const Work& W, const double* __restrict__ sv, size_t pi,
+                        int comp_n, int comp_t, bool twice, int taudir_plane) {
+    Side s;
+    double h = W.qB[pi];
+    s.b = W.bP[pi];
+    s.fs = W.td[pi];
+    s.taudir = W.td[(size_t)taudir_plane * W.npad + pi];
+    if (h <= P.dry_tolerance) {
+        s.h = 0.0; s.hn = 0.0; s.ht = 0.0; s.hm = 0.0; s.p = 0.0;
+        s.un = 0.0; s.ut = 0.0; s.m = 0.0;
+        s.rho_sv = 0.0; s.tau_sv = 0.0;
+        return s;
+    }
+    double hn = W.qB[(size_t)comp_n * W.npad + pi];
+    double ht = W.qB[(size_t)comp_t * W.npad + pi];
+    double hm = W.qB[3 * W.npad + pi];
+    double p = W.qB[4 * W.npad + pi];
+    double m;
+    qfix_mp(P, h, hm, p, m, P.grav);
+    if (twice) qfix_mp(P, h, hm, p, m, P.grav);
+    s.h = h; s.hn = hn; s.ht = ht; s.hm = hm; s.p = p; s.m = m;
+    s.un = hn / h;
+    s.ut = ht / h;
+    s.rho_sv = m * (P.rho_s - P.rho_f) + P.rho_f;
+    s.tau_sv = sv[(size_t)((twice ? SV_N : 0) + SV_TAU) * W.npad + pi];
+    return s;
+}
+
 // Stage C. Interface `i` (0..n+2) of slice `r` (x: row 0..my+1; y: column
 // 0..mx+1). Writes the compact waves; returns max |s| over the waves for the
-// Courant number and ORs branch bits into *br (nullable).
+// Courant number and ORs branch bits into *br (nullable). sv (nullable):
+// setvars records to read tau from instead of recomputing it.
 template <int DIR>
-DC_HD double stage_riemann(const dclaw_params& P, const Geom& g, const Work& W, int r, int i, uint32_t* br) {
+DC_HD double stage_riemann(const dclaw_params& P, const Geom& g, const Work& W, int r, int i, uint32_t* br,
+                           const double* __restrict__ sv = nullptr) {
     size_t pL, pR, oi;
     double* wv;
     size_t nplane;
@@ -234,8 +274,9 @@ DC_HD double stage_riemann(const dclaw_params& P, const Geom& g, const Work& W, 
         zero_waves(w);
         if (br) *br |= BR_DRY;
     } else {
-        Side R = load_side(P, W, pR, cn, ct, false, 1 + DIR);
-        Side L = load_side(P, W, pL, cn, ct, i - 1 >= 0, 1 + DIR);
+        Side R = sv ? load_side_sv(P, W, sv, pR, cn, ct, false, 1 + DIR) : load_side(P, W, pR, cn, ct, false, 1 + DIR);
+        Side L = sv ? load_side_sv(P, W, sv, pL, cn, ct, i - 1 >= 0, 1 + DIR)
+                    : load_side(P, W, pL, cn, ct, i - 1 >= 0, 1 + DIR);
         w = riemann_solve(P, L, R, br);
     }
     const double vals[NW] = {w.s1, w.s2, w.s5, w.w1h, w.w1n, w.w1t, w.w1m, w.w1p,

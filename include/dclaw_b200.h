@@ -239,6 +239,31 @@ int dclaw_step_batched(const dclaw_batch* batch, const dclaw_member* members, co
 /* zero the ensemble's work-queue counters (before the first step) */
 int dclaw_batch_reset(const dclaw_batch* batch, void* work, void* stream);
 
+/* ---- adjoint of one step ----------------------------------------------------
+ * The reference has no adjoint of the Fortran step; its differentiable port
+ * takes gradients with jax.grad through checkpointed scans
+ * (differentiable_dclaw/dclaw_jax/solver.py:357-388,
+ * differentiable_dclaw/tests/test_reverse_mode.py:37-49). This is the
+ * hand-written reverse of the same step as dclaw_step, for the gradient of
+ * a loss over a run of steps.
+ *
+ * lam_in = (dS/dq)^T lam_out, where S is one step of size *dt (a DEVICE
+ * double; dt is data, not differentiated) from q_in (interior layout, 5
+ * planes) over bed b. pbar (DEVICE, 4 doubles, ACCUMULATED) receives
+ * (dS/dtheta)^T lam_out for theta = (phi [radians], kref, alpha_c, mu).
+ * At branches (dry tolerance, limiter regimes, wall and static-friction
+ * tests, min/max picks) the adjoint follows the branch the forward step
+ * took. Results are bit-reproducible (no atomics in the sums). status
+ * (DEVICE int32, nullable) receives DCLAW_ERR_NAN if q_in holds a NaN.
+ * work: dclaw_adjoint_workspace_bytes(mx, my) bytes. */
+size_t dclaw_adjoint_workspace_bytes(int mx, int my);
+/* DCLAW_OK when the options have an adjoint form; DCLAW_ERR_UNSUPPORTED for
+ * the rare-wave corrector test and for Manning friction */
+int dclaw_adjoint_supported(const dclaw_params* p);
+int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, double dx, double dy,
+                       const double* dt, const dclaw_params* p, const double* lam_out, double* lam_in,
+                       double* pbar, void* work, size_t work_bytes, int32_t* status, void* stream);
+
 /* initialise a device clock: t, dt, t_final, fixed_dt; counters cleared */
 int dclaw_clock_init(dclaw_clock* clock, double t, double dt, double t_final, int fixed_dt,
                      void* stream);

@@ -420,8 +420,10 @@ int adj_step_vjp(const dclaw_params* P, int mx, int my, double dx, double dy, co
     forward_stages(*P, g, q, b, H, dt);
     const Work& W = H.W;
     std::vector<double> lamq(5 * (size_t)mx * my), xfb(NFB * W.nxi), yfb(NFB * W.nyi), xcb(NCB * W.nxi),
-        ycb(NCB * W.nyi), tdq(NTD * W.npad), qsb(5 * W.npad);
-    AdjWork A{lamq.data(), xfb.data(), yfb.data(), xcb.data(), ycb.data(), tdq.data(), qsb.data()};
+        ycb(NCB * W.nyi), tdq(NTD * W.npad), qsb(5 * W.npad), sv(NSV * W.npad);
+    AdjWork A{lamq.data(), xfb.data(), yfb.data(), xcb.data(), ycb.data(), tdq.data(), qsb.data(), sv.data()};
+    for (int j = -1; j <= my + 2; ++j)
+        for (int i = -1; i <= mx + 2; ++i) adj_item_svrec(*P, g, W, A, i, j);
     for (int j = 1; j <= my; ++j)
         for (int i = 1; i <= mx; ++i) adj_item_src2(*P, g, W, A, lam_out, i, j, dt, pbar);
     for (int r = 0; r <= my + 1; ++r)

@@ -1,0 +1,255 @@
+"""The step adjoint on the GPU (dclaw_step_adjoint through the C ABI) and the
+differentiable rollout with sqrt(N) checkpointing.
+
+1. One step: the CUDA adjoint against the host build of the same reverse
+   routines (tests/adj), which are checked against central finite
+   differences on the CPU runner: the state adjoint bit for bit, the
+   parameter adjoints (summed in another order) to 1e-12 relative, over wet,
+   dry, resting, boundary, order, transverse, limiter and src2 variants.
+2. Runs of steps: gradients of a loss over several output states with
+   respect to the initial state and the material parameters against
+   central finite differences of the CUDA forward run at the same dt
+   schedule (fixed, and replayed from an adaptive run), to 1e-6 relative.
+3. Checkpointing: every checkpoint block length gives the same bits.
+4. The loss at gauge points over output times, with the gradient reaching
+   the initial depth field and the solid fraction through the differentiable
+   initial state, against finite differences.
+"""
+import numpy as np
+import pytest
+import torch
+
+from dclaw_b200 import workloads as W
+from dclaw_b200.adjoint import StepAdjoint, last_dts, rollout_states, theta_of
+from dclaw_b200.params import DClawParams
+
+from .test_adjoint_cpu import CASES, _case
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def host_adj():
+    from ._adj import Adj
+
+    return Adj()
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_step_adjoint_matches_host_build(cuda_device, host_adj, name):
+    p, q, b = _case(**CASES[name])
+    dx, dt = 1.0, 0.02
+    rng = np.random.default_rng(100)
+    lam = rng.standard_normal(q.shape)
+    li_h, pb_h = host_adj.vjp(p, q, b, dx, dx, dt, lam)
+    dev = cuda_device
+    adj = StepAdjoint(torch.tensor(b, device=dev), p, dx, dx)
+    lam_in = torch.empty(q.shape, dtype=torch.float64, device=dev)
+    pbar = torch.zeros(4, dtype=torch.float64, device=dev)
+    dtt = torch.tensor([dt], dtype=torch.float64, device=dev)
+    adj.vjp(torch.tensor(q, device=dev), dtt, torch.tensor(lam, device=dev), lam_in, pbar)
+    torch.cuda.synchronize()
+    adj.check_status()
+    li = lam_in.cpu().numpy()
+    assert np.array_equal(li, li_h), f"max |diff| {np.abs(li - li_h).max():.3e}"
+    pb = pbar.cpu().numpy()
+    assert np.allclose(pb, pb_h, rtol=1e-12, atol=1e-300), (pb, pb_h)
+    # a second call gives the same bits (no atomics in the sums)
+    pbar2 = torch.zeros(4, dtype=torch.float64, device=dev)
+    lam_in2 = torch.empty_like(lam_in)
+    adj.vjp(torch.tensor(q, device=dev), dtt, torch.tensor(lam, device=dev), lam_in2, pbar2)
+    assert torch.equal(lam_in, lam_in2) and torch.equal(pbar, pbar2)
+
+
+def _small_flow(seed=1, mx=24, my=20, dry_frac=0.25):
+    """A moving wet patch with a dry region, on a sloping bed."""
+    p, q, b = _case(seed=seed, mx=mx, my=my, dry_frac=0.0)
+    X, Y = np.meshgrid(np.arange(mx), np.arange(my))
+    dry = (X + 0.7 * Y) > (1.0 - dry_frac) * (mx + 0.7 * my)
+    q[:, dry] = 0.0
+    return p, q, b
+
+
+def _loss_weights(q, n_out, seed=5):
+    """Random weights scaled by each field's magnitude, so every field's
+    terms are O(1) and the loss's rounding stays far below its derivatives."""
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal((n_out,) + q.shape)
+    sc = np.abs(q).reshape(5, -1).max(1)
+    return w / sc[None, :, None, None]
+
+
+def _fd(f, eps0=1e-6, agree=1e-5, tries=5):
+    """Central difference (f(e) - f(-e)) / 2e and its uncertainty.
+
+    Estimates at e, 2e and 4e are compared; where they disagree by more than
+    `agree` a kink of the forward map lies within the step (limiter regimes,
+    the dry tolerance and min/max picks put kinks within 1e-6 relative of
+    ordinary states, and a step that straddles one measures a chord, not the
+    derivative the adjoint gives), so e is halved. Returns (estimate at e,
+    spread of the three estimates) for the first step that settles, else for
+    the one with the smallest spread. Truncation error is far below the
+    spread, which measures the estimate's rounding noise: every perturbed
+    run rounds its elementary functions afresh, step after step, and that
+    noise divided by e grows as e shrinks."""
+    def cd(e):
+        return (f(e) - f(-e)) / (2 * e)
+
+    e = eps0
+    vals = {2 * e: cd(2 * e), 4 * e: cd(4 * e)}
+    best = None
+    for _ in range(tries):
+        vals[e] = cd(e)
+        three = [vals[e], vals[2 * e], vals[4 * e]]
+        spread = max(three) - min(three)
+        if best is None or spread < best[1]:
+            best = (vals[e], spread)
+        if spread <= agree * abs(vals[e]):
+            break
+        e *= 0.5
+    return best
+
+
+def _close(ad, fd, what, rtol=1e-6):
+    est, noise = fd
+    assert abs(ad - est) <= rtol * abs(est) + noise, f"{what}: AD {ad:.12e} FD {est:.12e} (noise {noise:.2e})"
+
+
+def _run_loss(q0, theta, b, p, dx, n, outs, wts, **kw):
+    o = rollout_states(q0, theta, b, p, dx, dx, n, outs, **kw)
+    return (o * wts).sum(), o
+
+
+@pytest.mark.parametrize("mode", ["fixed", "adaptive"])
+def test_rollout_gradient_matches_finite_differences(cuda_device, mode):
+    dev = cuda_device
+    p, qn, bn = _small_flow()
+    if mode == "adaptive":
+        # tick rule at Courant number 0.4: at 0.9 the run's rounding noise,
+        # amplified over 16 large steps, leaves the finite differences of
+        # the small parameters (kref, mu) uncertain by ~5e-6 relative
+        p = p.replace(cfl_desired=0.4)
+    dx = 1.0
+    n, outs = 16, [4, 9, 16]
+    q0 = torch.tensor(qn, device=dev, requires_grad=True)
+    b = torch.tensor(bn, device=dev)
+    theta = theta_of(p, dev).requires_grad_(True)
+    wts = torch.tensor(_loss_weights(qn, len(outs)), device=dev)
+    kw = dict(dt0=0.02, fixed_dt=True) if mode == "fixed" else dict(dt0=0.02, fixed_dt=False)
+    L, o = _run_loss(q0, theta, b, p, dx, n, outs, wts, **kw)
+    sched = last_dts(o).clone()
+    L.backward()
+    gq, gt = q0.grad.clone(), theta.grad.clone()
+    assert torch.isfinite(gq).all() and torch.isfinite(gt).all()
+
+    def Lf(qq, th):
+        with torch.no_grad():
+            return float(_run_loss(qq, th, b, p, dx, n, outs, wts, dt0=0.0, dt_schedule=sched)[0])
+
+    # initial state: a direction over wet cells only (dry cells stay dry)
+    rng = np.random.default_rng(7)
+    d = rng.standard_normal(qn.shape) * (np.abs(qn) + 1e-3)
+    d[:, qn[0] <= 10 * p.dry_tolerance] = 0.0
+    d = torch.tensor(d, device=dev)
+    q00, th0 = q0.detach(), theta.detach()
+    _close(float((gq * d).sum()), _fd(lambda e: Lf(q00 + e * d, th0)), "state")
+    # parameters, one at a time
+    for k, scale in enumerate([1.0, p.kref, p.alpha_c, p.mu]):
+        e = torch.zeros(4, dtype=torch.float64, device=dev)
+        e[k] = scale
+        _close(float(gt[k]) * scale, _fd(lambda h: Lf(q00, th0 + h * e), eps0=4e-6), f"theta[{k}]")
+
+
+def test_checkpoint_block_gives_identical_gradients(cuda_device):
+    dev = cuda_device
+    p, qn, bn = _small_flow(seed=2)
+    b = torch.tensor(bn, device=dev)
+    n, outs = 23, [0, 5, 11, 23]
+    wts = torch.tensor(_loss_weights(qn, len(outs), seed=9), device=dev)
+    res = []
+    for blk in (1, 3, 5, 23, None):
+        q0 = torch.tensor(qn, device=dev, requires_grad=True)
+        theta = theta_of(p, dev).requires_grad_(True)
+        L, _ = _run_loss(q0, theta, b, p, 1.0, n, outs, wts, dt0=0.02, checkpoint_block=blk)
+        L.backward()
+        res.append((float(L), q0.grad.clone(), theta.grad.clone()))
+    for r in res[1:]:
+        assert r[0] == res[0][0]
+        assert torch.equal(r[1], res[0][1])
+        assert torch.equal(r[2], res[0][2])
+
+
+def test_gauge_loss_gradient(cuda_device):
+    """Loss over gauge cells and output times against a target run at other
+    parameters (the shape of the 512 x 512 gradient case); the gradient
+    reaches the window's depth field per cell, a solid fraction m0 that sets
+    hm = h m0, and theta. The window starts from a flow in motion (40 steps
+    after release from rest): from rest, calc_taudir's static-friction
+    switch (factor of safety 0 or 1, digclaw_module.f90:500-719) makes the
+    loss jump under any perturbation, and no finite difference is defined."""
+    from oracle import Oracle
+
+    dev = cuda_device
+    n_cells, pre, n = 40, 40, 30
+    bn = W.random_terrain(n_cells, 1.0, seed=7)
+    p = DClawParams()
+    X, Y = np.meshgrid(np.arange(n_cells) + 0.5, np.arange(n_cells) + 0.5)
+    h0n = np.maximum(1.5 * (1.0 - ((X - 20) ** 2 + (Y - 20) ** 2) / 10.0**2), 0.0)
+    q_rest = W.state_from(h0n, np.full_like(h0n, 0.62), p, 0.8)
+    qp = Oracle().run(p, q_rest, bn, 1.0, 1.0, pre, 0.05, libm="portable")["q"]
+    b = torch.tensor(bn, device=dev)
+    outs = list(range(3, n + 1, 3))
+    rng = np.random.default_rng(11)
+    gi_t = torch.tensor(rng.integers(10, 30, size=8), device=dev)
+    gj_t = torch.tensor(rng.integers(10, 30, size=8), device=dev)
+    qpt = torch.tensor(qp, device=dev)
+    wet = qpt[0] > p.dry_tolerance
+
+    def start(h, m0):
+        return torch.stack([h, qpt[1], qpt[2], torch.where(wet, h * m0, 0.0), qpt[4]])
+
+    def run(h, m0, theta, sched=None):
+        kw = dict(dt0=0.0, dt_schedule=sched) if sched is not None else dict(dt0=0.05)
+        o = rollout_states(start(h, m0), theta, b, p, 1.0, 1.0, n, outs, **kw)
+        return o[:, 0, gj_t, gi_t], o
+
+    with torch.no_grad():
+        target, _ = run(qpt[0], torch.tensor(0.6, dtype=torch.float64, device=dev),
+                        theta_of(p.replace(phi=30.0, kref=3e-10), dev))
+    h = qpt[0].clone().requires_grad_(True)
+    m0 = torch.tensor(0.62, dtype=torch.float64, device=dev, requires_grad=True)
+    theta = theta_of(p, dev).requires_grad_(True)
+    g, o = run(h, m0, theta)
+    L = ((g - target) ** 2).sum()
+    sched = last_dts(o).clone()
+    L.backward()
+    assert float(L.detach()) > 0.0
+
+    def Lf(hh, mm, th):
+        with torch.no_grad():
+            gg, _ = run(hh, mm, th, sched)
+            return float(((gg - target) ** 2).sum())
+
+    h00, m00, th0 = h.detach(), m0.detach(), theta.detach()
+    d = torch.tensor(np.where(qp[0] > 0.2, rng.standard_normal(qp[0].shape), 0.0), device=dev)
+    _close(float((h.grad * d).sum()), _fd(lambda e: Lf(h00 + e * d, m00, th0)), "h")
+    _close(float(m0.grad), _fd(lambda e: Lf(h00, m00 + e, th0), eps0=4e-6), "m0")
+    # this loss hardly feels the material parameters over 30 steps (relative
+    # sensitivities ~1e-3 of the depth's), so their finite differences carry
+    # ~1e-4 relative rounding noise; theta is checked at 1e-6 in
+    # test_rollout_gradient_matches_finite_differences
+    for k, scale in enumerate([1.0, p.kref, p.alpha_c, p.mu]):
+        e = torch.zeros(4, dtype=torch.float64, device=dev)
+        e[k] = scale
+        _close(float(theta.grad[k]) * scale, _fd(lambda hh: Lf(h00, m00, th0 + hh * e), eps0=4e-6), f"theta[{k}]",
+               rtol=1e-4)
+
+
+def test_unsupported_options_are_refused(cuda_device):
+    from dclaw_b200 import _lib
+
+    b = torch.zeros((8, 8), dtype=torch.float64, device=cuda_device)
+    with pytest.raises(_lib.DClawError):
+        StepAdjoint(b, DClawParams(rarecorrectortest=True), 1.0, 1.0)
+    with pytest.raises(_lib.DClawError):
+        StepAdjoint(b, DClawParams(friction_forcing=True, manning_coefficient=0.03), 1.0, 1.0)
