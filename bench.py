@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -59,6 +60,9 @@ def parse():
     ap.add_argument("--ensemble-members", type=int, default=256,
                     help="members of the batched flume ensemble measured beside the plain step (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=10)
+    ap.add_argument("--grad-steps", type=int, default=500,
+                    help="steps of the 512 x 512 gradient case measured beside the plain step (0: skip)")
+    ap.add_argument("--checkpoint-block", type=int, default=0, help="0: ceil(sqrt(steps))")
     return ap.parse_args()
 
 
@@ -256,6 +260,78 @@ def ensemble_bench(args, dev):
             "gpu_launches": 3 * K, "status_nonzero": sum(1 for x in status_b if x)}
 
 
+def gradient_bench(args, dev):
+    """Gradient of a gauge loss over a 500-step run of the 512 x 512 case
+    with respect to (phi, kref, m0, alpha_c) and the initial depth of every
+    cell, by the hand-written step adjoint with sqrt(N) checkpointing,
+    against the forward solve of the same run. Both are timed with CUDA
+    events on the launching stream; the gradient's time covers its forward
+    pass (with checkpoints), the loss and the whole backward pass."""
+    import torch
+
+    from dclaw_b200 import workloads as W
+    from dclaw_b200.adjoint import initial_state, rollout_states, theta_of
+    from dclaw_b200.solver import PatchStepper
+
+    c = W.gradient_case(nsteps=args.grad_steps)
+    p = c.params
+    b = torch.tensor(c.b, device=dev)
+    gj = torch.tensor(c.gauges[:, 0], device=dev)
+    gi = torch.tensor(c.gauges[:, 1], device=dev)
+    h0 = torch.tensor(c.h0, device=dev)
+    blk = args.checkpoint_block or None
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        return e
+
+    def gauges(h, m0, theta):
+        q0 = initial_state(h, m0, p)
+        o = rollout_states(q0, theta, b, p, c.dx, c.dx, c.nsteps, c.out_steps, c.dt_initial, checkpoint_block=blk)
+        return o[:, 0, gj, gi]
+
+    with torch.no_grad():
+        target = gauges(h0, torch.tensor(c.m0, dtype=torch.float64, device=dev), theta_of(c.true_params, dev))
+    # forward solve of the same run (plain fused steps)
+    q0 = initial_state(h0, torch.tensor(c.m0, dtype=torch.float64, device=dev), p)
+    fwd_ms = []
+    for _ in range(2):
+        st = PatchStepper(q0, b, p, c.dx, c.dx)
+        st.init_clock(c.dt_initial)
+        torch.cuda.synchronize()
+        e0 = ev()
+        st.step(c.nsteps)
+        e1 = ev()
+        torch.cuda.synchronize()
+        fwd_ms.append(e0.elapsed_time(e1))
+    del st
+    grad_ms = []
+    for _ in range(2):
+        h = h0.clone().requires_grad_(True)
+        m0 = torch.tensor(c.m0, dtype=torch.float64, device=dev, requires_grad=True)
+        theta = theta_of(p, dev).requires_grad_(True)
+        torch.cuda.synchronize()
+        torch.cuda.reset_peak_memory_stats(dev)
+        e0 = ev()
+        loss = ((gauges(h, m0, theta) - target) ** 2).sum()
+        loss.backward()
+        e1 = ev()
+        torch.cuda.synchronize()
+        grad_ms.append(e0.elapsed_time(e1))
+    f, g = min(fwd_ms), min(grad_ms)
+    k = blk or math.ceil(math.sqrt(c.nsteps))
+    mx, my = c.b.shape[1], c.b.shape[0]
+    return {"workload": f"gauge_loss_{mx}x{my}_dx{c.dx}_{c.nsteps}steps", "gauges": len(c.gauges),
+            "output_times": len(c.out_steps), "checkpoint_block": k, "forward_ms": f, "gradient_ms": g,
+            "gradient_over_forward": g / f, "loss": float(loss.detach()),
+            "grad": {"phi_deg": float(theta.grad[0]), "kref": float(theta.grad[1]), "m0": float(m0.grad),
+                     "alpha_c": float(theta.grad[2]), "h0_l2": float(h.grad.norm())},
+            "peak_mem_gb": torch.cuda.max_memory_allocated(dev) / 1e9,
+            "gpu_launches": {"adjoint_per_step": 16, "recompute_per_step": 3, "forward_per_step": 3},
+            "note": "dt of each step chosen by the tick rule in the forward pass and replayed, not differentiated"}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -354,6 +430,8 @@ def run_ours(args):
         del st
         torch.cuda.empty_cache()
         out["batched"] = ensemble_bench(args, dev)
+    if rank == 0 and world == 1 and args.grad_steps > 0:
+        out["gradient"] = gradient_bench(args, dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args, case, args.cpu_steps)
     if rank == 0:

@@ -32,7 +32,7 @@ namespace adj {
 #endif
 // resident blocks per SM the heavy reverse kernels' registers are sized for
 #ifndef DCLAW_ADJ_MINB
-#define DCLAW_ADJ_MINB 1
+#define DCLAW_ADJ_MINB 4
 #endif
 constexpr int ATPB = DCLAW_ADJ_TPB;
 constexpr int NWARP = ATPB / 32;

@@ -219,3 +219,41 @@ def flume_ensemble(n: int = 256, seed: int = 0, dx: float = 0.05, width_range=(3
         q, b = flume_member(w, L, dx, p)
         out.append(Case(f"flume_{w}x{L}", q, b, dx, dx, p, nsteps, 1.0e-3))
     return out
+
+
+# ---- gradient case -----------------------------------------------------------
+@dataclasses.dataclass
+class GradientCase:
+    """Loss over gauge cells and output times for the gradient benchmark."""
+
+    b: np.ndarray            # (my, mx)
+    h0: np.ndarray           # (my, mx) initial depth
+    m0: float                # solid fraction of the initial mass
+    params: DClawParams      # parameters the gradient is taken at
+    true_params: DClawParams  # parameters of the synthetic target run
+    gauges: np.ndarray       # (n_gauges, 2) cell indices (j, i)
+    out_steps: list          # step counts at which the gauges are read
+    nsteps: int
+    dx: float
+    dt_initial: float
+
+
+def gradient_case(n: int = 512, dx: float = 1.0, seed: int = 7, nsteps: int = 500, n_gauges: int = 64,
+                  n_out: int = 50) -> GradientCase:
+    """512 x 512, dx 1 m: the random terrain of the 4096 x 4096 case at this
+    seed, paraboloid sources (one uniform solid fraction m0 = 0.62), 64
+    seeded gauge cells among the cells the initial mass covers or borders,
+    read at 50 evenly spaced output steps over 500 steps. The target comes
+    from the same solver at perturbed true parameters (phi 30 deg, kref
+    3e-10, alpha_c 0.015)."""
+    p = DClawParams()
+    b = random_terrain(n, dx, seed)
+    src = paraboloid_sources(n, dx, seed, params=p)
+    h0 = src[0]
+    rng = np.random.default_rng(seed + 2000)
+    near = np.argwhere(np.maximum.reduce([np.roll(h0, s, a) for a in (0, 1) for s in (-8, 0, 8)]) > 0)
+    gauges = near[rng.choice(len(near), size=n_gauges, replace=False)]
+    every = max(1, nsteps // n_out)
+    out_steps = list(range(every, nsteps + 1, every))[:n_out]
+    true = p.replace(phi=30.0, kref=3.0e-10, alpha_c=0.015)
+    return GradientCase(b, h0, 0.62, p, true, gauges, out_steps, nsteps, dx, 0.05)
