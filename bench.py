@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--grad-steps", type=int, default=500,
                     help="steps of the 512 x 512 gradient case measured beside the plain step (0: skip)")
     ap.add_argument("--checkpoint-block", type=int, default=0, help="0: ceil(sqrt(steps))")
+    ap.add_argument("--only", default="", choices=["", "batched", "gradient"],
+                    help="run one side measurement alone and print its object (profiling runs)")
     return ap.parse_args()
 
 
@@ -442,9 +444,20 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_only(args):
+    import torch
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    out = ensemble_bench(args, dev) if args.only == "batched" else gradient_bench(args, dev)
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.only:
+        run_only(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -223,6 +223,8 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
     M.H = M.D + (size_t)10 * TG::ND;
     M.Bd = M.H + TG::NHB;
     M.bits = reinterpret_cast<uint32_t*>(M.Bd + TG::NHB);
+    M.list = reinterpret_cast<int*>(M.bits + TG::NA);
+    M.nlist = M.list + TG::NA;
     M.NA = TG::NA;
     const int tid = threadIdx.x;
     M.hi0 = i0 - 3;
@@ -252,9 +254,34 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
         for (int dir = 0; dir < 2; ++dir) {
             const int nsolve = dir == 0 ? TG::NXW : TG::NYW;
             const double dtd = dir == 0 ? dtdx : dtdy;
-            for (int it = tid; it < nsolve; it += TPB) {
+            // Items that need a solve are gathered into a dense list first,
+            // so that every warp of the solve loop is full of them: wet
+            // interfaces cluster in space, and handing items out by index
+            // leaves warps of dry items idle at the barrier while others
+            // solve twice. The other items store zero waves here. Each
+            // item writes only its own slots and the Courant number is a
+            // max, so the list's order changes no result.
+            if (tid == 0) *M.nlist = 0;
+            __syncthreads();
+            const int lane = tid & 31;
+            for (int it0 = 0; it0 < nsolve; it0 += TPB) {
+                const int it = it0 + tid;
+                bool need = it < nsolve && tile_needs_solve(P, g, M, dir, it, i0, j0, TX);
+                if (it < nsolve && !need) {
+                    bool ok;
+                    tile_riemann(P, g, R, M, dir, it, i0, j0, TX, TY, ok);
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, need);
+                int base = 0;
+                if (lane == 0 && bal) base = atomicAdd(M.nlist, __popc(bal));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (need) M.list[base + __popc(bal & ((1u << lane) - 1u))] = it;
+            }
+            __syncthreads();
+            const int nneed = *M.nlist;
+            for (int w = tid; w < nneed; w += TPB) {
                 bool ok;
-                double s = tile_riemann(P, g, R, M, dir, it, i0, j0, TX, TY, ok);
+                double s = tile_riemann(P, g, R, M, dir, M.list[w], i0, j0, TX, TY, ok);
                 if (ok) cfl = fmax2(cfl, dtd * s);
             }
             __syncthreads();

@@ -194,7 +194,9 @@ struct TileGeom {
     static constexpr int ND = (TX + 2) * TY;          // G1y/G2y cols i0-1..i0+TX, rows j0..j0+TY-1
     static constexpr int NHB = (TX + 6) * (TY + 6);    // h and bed of cells within 3 of the tile
     static constexpr size_t SMEM_DOUBLES = (size_t)NW * NA + 10 * NB + 10 * NC + 10 * ND + 2 * NHB;
-    static constexpr size_t SMEM_BYTES = SMEM_DOUBLES * 8 + 4 * (size_t)NA;
+    // + branch bits of the sweep's items, the list of items that need a
+    // solve, and its length
+    static constexpr size_t SMEM_BYTES = SMEM_DOUBLES * 8 + 4 * (size_t)NA + 4 * (size_t)NA + 16;
 };
 
 struct TileMem {
@@ -205,6 +207,8 @@ struct TileMem {
     double* H;   // record h of cells (i0-3..i0+TX+2) x (j0-3..j0+TY+2)
     double* Bd;  // bed of the same cells
     uint32_t* bits;  // NA Riemann branch bits of the current sweep
+    int* list;       // NA: items of the current sweep that need a solve
+    int* nlist;      // length of the list
     int NA;
     int hi0, hj0, hw;  // origin and width of the H/Bd block
     DC_HD double h(int i, int j) const { return H[(j - hj0) * hw + (i - hi0)]; }
@@ -274,6 +278,21 @@ DC_HD void tile_waves(const TileMem& M, int dir, int item, double s[3], double W
     W1[0] = v[W_1H]; W1[1] = y ? v[W_1T] : v[W_1N]; W1[2] = y ? v[W_1N] : v[W_1T]; W1[3] = v[W_1M]; W1[4] = v[W_1P];
     W2[0] = v[W_2H]; W2[1] = y ? 0.0 : v[W_2N]; W2[2] = y ? v[W_2N] : 0.0; W2[3] = 0.0; W2[4] = 0.0;
     W5[0] = v[W_5H]; W5[1] = y ? v[W_5T] : v[W_5N]; W5[2] = y ? v[W_5N] : v[W_5T]; W5[3] = v[W_5M]; W5[4] = v[W_5P];
+}
+
+// Whether item `item` of sweep `dir` needs a Riemann solve (inside the
+// patch and not dry-dry); tile_riemann handles every other item with a
+// store of zero waves.
+DC_HD bool tile_needs_solve(const dclaw_params& P, const Geom& g, const TileMem& M, int dir, int item, int i0,
+                            int j0, int TX) {
+    int sl, k;
+    if (dir == 0) { sl = j0 - 1 + item / (TX + 3); k = i0 - 1 + item % (TX + 3); }
+    else { sl = i0 - 1 + item % (TX + 2); k = j0 - 1 + item / (TX + 2); }
+    const int nslice = dir == 0 ? g.my : g.mx, nlen = dir == 0 ? g.mx : g.my;
+    if (sl < 0 || sl > nslice + 1 || k < 0 || k > nlen + 2) return false;
+    int iL = dir == 0 ? k - 1 : sl, jL = dir == 0 ? sl : k - 1;
+    int iR = dir == 0 ? k : sl, jR = dir == 0 ? sl : k;
+    return !(M.h(iL, jL) <= P.dry_tolerance && M.h(iR, jR) <= P.dry_tolerance);
 }
 
 // Riemann solve of sweep `dir` for tile-local item (slice s, interface k).
