@@ -21,6 +21,9 @@
 //   tan   Cody & Waite reduction by pi/2 (three-part split), Taylor series of
 //         sin and cos on |r| <= pi/4, tan = s/c or -c/s by quadrant.
 //   h^(7/3) = h^2 * cbrt(h), cbrt by Newton iteration from an exponent guess.
+//   log   x = 2^k f with f in [sqrt(1/2), sqrt(2)); log f = 2 atanh(s),
+//         s = (f - 1)/(f + 1) (f - 1 exact), by the Taylor series of atanh
+//         on |s| <= 0.1716; log x = k ln2_hi + (k ln2_lo + log f).
 // The constants were produced with 80-digit decimal arithmetic.
 #pragma once
 #include <stdint.h>
@@ -239,6 +242,46 @@ DC_HD double d_tan(double x) {
     cp = cp * r2 + IF4;
     double c = 1.0 + r2 * (-0.5 + r2 * cp);
     return (k & 1) ? -c / s : s / c;
+}
+
+// natural logarithm (src2method 2's substep bounds)
+DC_HD double d_log(double x) {
+    if (!(x == x)) return x + x;
+    if (x < 0.0) return bits2d(0x7ff8000000000000ull);
+    if (x == 0.0) return bits2d(0xfff0000000000000ull);
+    if (x > 1.7976931348623157e308) return x;
+    uint64_t b = d2bits(x);
+    int e = (int)((b >> 52) & 0x7ff);
+    int k = 0;
+    if (e == 0) {  // subnormal: scale into the normal range
+        b = d2bits(x * 18014398509481984.0);  // 2^54
+        e = (int)((b >> 52) & 0x7ff);
+        k = -54;
+    }
+    k += e - 1023;
+    double f = bits2d((b & 0x000fffffffffffffull) | 0x3ff0000000000000ull);  // [1, 2)
+    if (f > 1.4142135623730951) {
+        f = f * 0.5;
+        k += 1;
+    }
+    double s = (f - 1.0) / (f + 1.0);
+    double z = s * s;
+    double q = 0.07407407407407407;  // 2/27, then 2/(2n+1) down to 2/3
+    q = q * z + 0.08;
+    q = q * z + 0.08695652173913043;
+    q = q * z + 0.09523809523809523;
+    q = q * z + 0.10526315789473684;
+    q = q * z + 0.11764705882352941;
+    q = q * z + 0.13333333333333333;
+    q = q * z + 0.15384615384615385;
+    q = q * z + 0.18181818181818182;
+    q = q * z + 0.2222222222222222;
+    q = q * z + 0.2857142857142857;
+    q = q * z + 0.4;
+    q = q * z + 0.6666666666666666;
+    double lf = 2.0 * s + s * (z * q);
+    double kd = (double)k;
+    return kd * LN2_HI + (kd * LN2_LO + lf);
 }
 
 // h^(7/3) for h > 0 (Manning friction)

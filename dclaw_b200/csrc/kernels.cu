@@ -728,8 +728,10 @@ int dclaw_params_check(const dclaw_params* p) {
     if (!p) return DCLAW_ERR_ARG;
     if (p->bed_normal != 0 || p->entrainment != 0 || p->segregation != 0 || p->curvature != 0)
         return DCLAW_ERR_UNSUPPORTED;
-    if (p->src2method < -1 || p->src2method > 1) return DCLAW_ERR_UNSUPPORTED;
+    if (p->src2method < -1 || p->src2method > 2) return DCLAW_ERR_UNSUPPORTED;
     if (p->alphamethod != 0 && p->alphamethod != 1) return DCLAW_ERR_ARG;
+    // the setrun writer's parameter conflict check (src/python/dclaw/data.py:362-365)
+    if (p->src2method == 2 && p->alphamethod < 1) return DCLAW_ERR_ARG;
     if (p->order != 1 && p->order != 2) return DCLAW_ERR_ARG;
     if (p->transverse_waves < 0 || p->transverse_waves > 2) return DCLAW_ERR_ARG;
     if (p->limiter < 0 || p->limiter > 5) return DCLAW_ERR_ARG;

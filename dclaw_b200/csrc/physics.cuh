@@ -17,6 +17,7 @@
 //                 inundation set-up of src/2d/dig/rpn2_dclaw.f:124-272
 //   rpt2_split    src/2d/dig/rpt2_dclaw.f:78-263
 //   src2_cell     src/2d/dig/src2.f90:100-300 + mp_update.f90:710-789
+//   mp_update_fe4quad  src/2d/dig/mp_update.f90:38-707 (src2method 2)
 //
 // The hchi (segregation) and bdif (bed change) components are identically
 // zero for the accepted configurations; their contributions are the exact
@@ -577,6 +578,181 @@ DC_HD void mp_update_relax(const dclaw_params& P, double phi, double dt, double&
     }
 }
 
+// mp_update_FE_4quad (mp_update.f90:38-707), src2method 2: one substep of
+// the quadrant-wise explicit integration of (m, p_exc) on the rho h = const
+// manifold; returns the time the substep covered. Where the reference reads
+// dtm unassigned (branch vnorm == 0 or m == m_eq, mp_update.f90:225-249),
+// dtm = dtr, the whole remaining time.
+DC_BIG double mp_update_fe4quad(const dclaw_params& P, double phi, double dtr, double& h, double u, double v,
+                                double& m, double& p, double rhoh, double gz) {
+    const double rs = P.rho_s, rf = P.rho_f, mu = P.mu;
+    const double vnorm = sqrt(sq(u) + sq(v));
+    SetVars sv = setvars<true>(P, phi, h, u, v, m, p, gz);
+    const double h0 = h, m_0 = m;
+    const double rho0 = m_0 * (rs - rf) + rf;
+    const double p_eq0 = rf * gz * h0;
+    const double p_exc0 = p - p_eq0;
+    const double km0 = ((2.0 * sv.kperm * (rho0 * rho0)) / (mu * (rhoh * rhoh)));
+    const double c_d0 = -3.0 * vnorm * (sv.alphainv * rho0 / (rhoh)) * sv.tanpsi;
+    double kp0 = (sv.kperm / (h0 * mu)) * (3.0 * sv.alphainv * rho0 / rhoh - 1.5 * rf * gz * h0 * (rho0 - rf) / rhoh);
+    kp0 = fmax2(kp0, 1.0e-3);
+    double rho, p_exc, hu, hv, hm;
+    if (m == 0.0) {
+        p_exc = p_exc0 * em::d_exp(-kp0 * dtr);
+        qfix_cmass(P, h, m, p, rho, p_exc, hu, hv, hm, u, v, rhoh, gz);
+        return dtr;
+    }
+    const double m_eq = sv.m_eq;
+    if ((fabs(p_exc0 / (rf * gz * h0)) < 1.0e-12) && (fabs(m - m_eq) < 1.0e-12)) return dtr;
+    if ((vnorm == 0.0) || (m == m_eq)) {
+        const double dtm = dtr;
+        p_exc = p_exc0 * em::d_exp(-kp0 * dtm);
+        if (!((m == m_eq) && (m < 0.3))) m = m_0 * em::d_exp(km0 * p_exc * dtm);
+        qfix_cmass(P, h, m, p, rho, p_exc, hu, hv, hm, u, v, rhoh, gz);
+        return dtm;
+    }
+    // critical point (m_c, p_eq_c) by fixed-point iteration
+    double m_c = P.m_crit;
+    double rho_c = m_c * (rs - rf) + rf;
+    double h_c = rhoh / rho_c;
+    double p_eq_c = rf * gz * h_c;
+    const double shear = 2.0 * vnorm / h0;
+    int iter;
+    double normc = 0.0;
+    for (iter = 1; iter <= 100; ++iter) {
+        const double m_c0 = m_c, p_eq_c0 = p_eq_c;
+        rho_c = m_c * (rs - rf) + rf;
+        h_c = rhoh / rho_c;
+        p_eq_c = rf * gz * h_c;
+        const double sig_c = fmax2(rhoh * gz - p_eq_c, 0.0);
+        const double Nd = rs * sq(shear * P.delta) + sig_c;
+        const double Nn = mu * shear;
+        m_c = P.m_crit * (sqrt(Nd) / (sqrt(Nd) + sqrt(Nn)));
+        normc = sq(1.0e2 * (m_c - m_c0)) + sq(1.0e-3 * (p_eq_c - p_eq_c0));
+        if (normc < 1.0e-16) break;
+    }
+    if ((iter >= 100) && (normc > 1.0)) m_c = P.m_crit;
+    rho_c = m_c * (rs - rf) + rf;
+    h_c = rhoh / rho_c;
+    p_eq_c = rf * gz * h_c;
+    int quad0 = 0;
+    if ((m < m_c) && (p >= p_eq_c)) quad0 = 1;
+    else if ((m >= m_c) && (p > p_eq_c)) quad0 = 2;
+    else if ((m > m_c) && (p <= p_eq_c)) quad0 = 3;
+    else if ((m <= m_c) && (p < p_eq_c)) quad0 = 4;
+    if (quad0 == 0) return 0.0;
+    // p_exc(t) = (1/kp0) ((kp0 p_exc0 - c_d0) e^{-kp0 t} + c_d0)
+    auto pexc_at = [&](double t) { return (1.0 / kp0) * ((kp0 * p_exc0 - c_d0) * em::d_exp(-kp0 * t) + c_d0); };
+    double dtm, dtp, dts, p_exc_ave;
+    if (quad0 == 1) {
+        if (p_exc0 < -1.0e-3 * rhoh * gz) {  // region 1A
+            if (c_d0 > 0.0) dtp = -(1.0 / kp0) * em::d_log(c_d0 / (c_d0 - kp0 * p_exc0));
+            else dtp = dtr;
+            dtm = em::d_log(0.98) / (kp0 * p_exc0);
+            dts = fmin2(fmin2(dtr, dtp), dtm);
+            dts = fmax2(dts, 0.0);
+            p_exc = pexc_at(dts);
+            m = m_0 * em::d_exp(dts * km0 * p_exc);
+        } else if ((-kp0 * p_exc0 + c_d0) > 0.0) {  // region 1B
+            if ((c_d0 / kp0) > (rhoh * gz - p_eq_c))
+                dtp = fmin2(dtr, -(1.0 / kp0) * em::d_log((-kp0 * rhoh * gz + kp0 * p_eq_c + c_d0) / (-kp0 * p_exc0 + c_d0)));
+            else
+                dtp = dtr;
+            p_exc = pexc_at(dtp);
+            p_exc_ave = 0.5 * (p_exc + p_exc0);
+            if (p_exc_ave <= 0.0) dtm = dtr;
+            else if ((km0 * p_exc_ave * m_0) < 1.0e-99) dtm = dtp;
+            else dtm = fmin2(dtp, (m_eq - m_0) / (km0 * p_exc_ave * m_0));
+            m = m_0 + km0 * m_0 * p_exc_ave * dtm;
+            dts = dtm;
+        } else if (c_d0 > 0.0) {  // region 1C, left of m_eq
+            dtp = dtr;
+            if ((km0 * p_exc0 * m_0) > 1.0e-99) dtm = (m_c - m_0) / (km0 * p_exc0 * m_0);
+            else dtm = dtp;
+            dts = fmin2(dtm, dtp);
+            dts = fmax2(dts, 0.0);
+            m = m_0 + km0 * m_0 * p_exc0 * dts;
+            p_exc = pexc_at(dts);
+        } else {  // region 1C, right of m_eq
+            dts = dtr;
+            dtp = dtr;
+            if ((km0 * p_exc0 * m_0) > 1.0e-99) dts = fmin2(dtr, (m_c - m_0) / (km0 * p_exc0 * m_0));
+            if ((kp0 * p_exc0 - c_d0) != 0.0) {
+                if ((-kp0 * p_eq0 - c_d0) / (kp0 * p_exc0 - c_d0) > 1.0e-99)
+                    dtp = fmin2(dtr, -(1.0 / kp0) * em::d_log((c_d0) / (c_d0 - kp0 * p_exc0)));
+            }
+            dts = fmin2(dts, dtp);
+            dts = fmax2(dts, 0.0);
+            m = m_0 + km0 * m_0 * p_exc0 * dts;
+            p_exc = pexc_at(dts);
+        }
+    } else if (quad0 == 2) {
+        dtp = dtr;
+        if ((c_d0 - kp0 * (p_eq_c - p_eq0)) / (c_d0 - kp0 * p_exc0) > 1.0e-99)
+            dtp = fmin2(dtr, -(1.0 / kp0) * em::d_log((c_d0 - kp0 * (p_eq_c - p_eq0)) / (c_d0 - kp0 * p_exc0)));
+        dtm = dtp;
+        if (km0 * p_exc0 * m_0 > 1.0e-99) dtm = fmin2(dtp, (fmin2(1.0 - m_0, 0.02) / (km0 * p_exc0 * m_0)));
+        dts = fmin2(dtp, dtm);
+        p_exc = pexc_at(dts);
+        m = m_0 + km0 * m_0 * p_exc * dts;
+    } else if (quad0 == 3) {
+        if (p_exc0 > 1.0e-3 * rhoh * gz) {  // region 3A
+            dtp = dtr;
+            if ((c_d0 / (-kp0 * p_exc0 + c_d0)) > 1.0e-99)
+                dtp = fmin2(dtr, -(1.0 / kp0) * em::d_log(c_d0 / (c_d0 - kp0 * p_exc0)));
+            dtm = dtp;
+            if ((km0 * p_exc0 * m_0) > 1.0e-99) dtm = fmin2(dtp, (fmin2(1.0 - m_0, 0.02)) / (km0 * p_exc0 * m_0));
+            p_exc = pexc_at(dtp);
+            m = m_0 + km0 * m_0 * 0.5 * (p_exc0 + p_exc) * dtm;
+            dts = dtp;
+        } else if ((-kp0 * p_exc0 + c_d0) < 0.0) {  // region 3B
+            dtp = dtr;
+            if (c_d0 / kp0 < -p_eq0) {
+                if (((c_d0 + kp0 * p_eq0) / (-kp0 * p_exc0 + c_d0)) > 1.0e-99)
+                    dtp = fmin2(dtr, -(1.0 / kp0) * em::d_log((c_d0 + kp0 * p_eq0) / (-kp0 * p_exc0 + c_d0)));
+            }
+            p_exc = pexc_at(dtp);
+            p_exc_ave = 0.5 * (p_exc + p_exc0);
+            if (p_exc_ave > 0.0) {
+                dtm = fmin2(dtr, (0.02) / (km0 * p_exc_ave * m_0));
+            } else {
+                const double m_lower = m_eq + fmax2(0.0, (1.0 / 3.0) * kp0 * h0 * (-p_exc_ave) / (vnorm * sv.alphainv));
+                dtm = fmin2(dtr, (m_lower - m_0) / (km0 * p_exc_ave * m_0));
+            }
+            m = m_0 + km0 * m_0 * p_exc_ave * dtm;
+            dts = dtm;
+        } else if (c_d0 < 0.0) {  // region 3C, between the p-nullcline and m_eq
+            dtp = dtr;
+            dtm = dtr;
+            if (-(km0 * p_exc0 * m_0) > 1.0e-99) dtm = (m_c - m_0) / (km0 * p_exc0 * m_0);
+            dts = fmin2(dtp, dtm);
+            dts = fmax2(dts, 0.0);
+            p_exc = pexc_at(dts);
+            m = m_0 + km0 * m_0 * p_exc0 * dts;
+        } else {  // region 3C, left of m_eq
+            dtm = dtr;
+            dtp = dtr;
+            if ((km0 * p_exc0 * m_0) > 1.0e-99) dtm = (m_c - m_0) / (km0 * p_exc0 * m_0);
+            if ((-c_d0 / (kp0 * p_exc0 - c_d0)) > 1.0e-99) dtp = -(1.0 / kp0) * em::d_log(c_d0 / (c_d0 - kp0 * p_exc0));
+            dts = fmin2(dtp, dtm);
+            dts = fmax2(dts, 0.0);
+            p_exc = pexc_at(dts);
+            m = m_0 + km0 * m_0 * p_exc0 * dts;
+        }
+    } else {  // quad0 == 4
+        dtp = dtr;
+        if ((c_d0 - kp0 * (p_eq_c - p_eq0)) / (c_d0 - kp0 * p_exc0) > 1.0e-99)
+            dtp = fmin2(dtr, -(1.0 / kp0) * em::d_log((c_d0 - kp0 * (p_eq_c - p_eq0)) / (c_d0 - kp0 * p_exc0)));
+        dtm = em::d_log(0.98) / (kp0 * p_exc0);
+        dts = fmin2(dtr, fmin2(dtp, dtm));
+        p_exc = pexc_at(dts);
+        m = m_0 * em::d_exp(dts * km0 * 0.5 * (p_exc0 + p_exc));
+        dts = dtp;  // the reference reports dtp as the time covered
+    }
+    qfix_cmass(P, h, m, p, rho, p_exc, hu, hv, hm, u, v, rhoh, gz);
+    return dts;
+}
+
 // src2 on one interior cell (in place on the 5 conserved fields)
 DC_BIG void src2_cell(const dclaw_params& P, double phi, double dt, double& qh, double& qhu,
                                           double& qhv, double& qhm, double& qp) {
@@ -606,6 +782,20 @@ DC_BIG void src2_cell(const dclaw_params& P, double phi, double dt, double& qh, 
     }
     if (P.src2method == -1) {
         hu = h * u; hv = h * v; hm = h * m;
+    } else if (P.src2method == 2) {
+        // src2.f90:206-229: substeps until dt is covered, at most 100
+        double dtremaining = dt;
+        int itercount = 0;
+        while (dtremaining > 1.0e-99) {
+            const double dtk = mp_update_fe4quad(P, phi, dtremaining, h, u, v, m, p, rhoh, gz);
+            dtremaining = dtremaining - dtk;
+            itercount = itercount + 1;
+            if (dtk == 0.0) break;
+            if (h < P.dry_tolerance) break;
+            if (itercount >= 100) break;
+        }
+        hu = h * u; hv = h * v; hm = h * m;
+        qfix(P, h, hu, hv, hm, p, u, v, m, gz);
     } else {
         mp_update_relax(P, phi, dt, h, u, v, m, p, rhoh, gz);
         hu = h * u; hv = h * v; hm = h * m;

@@ -77,7 +77,7 @@ typedef struct dclaw_params {
     double phi;                   /* basal friction angle, radians */
     double delta, mu, alpha_c, c1, sigma_0;
     double theta_input;           /* radians; only used with bed_normal = 1 */
-    int32_t src2method;           /* -1, 0 or 1 (2 = FE_4quad: not accepted) */
+    int32_t src2method;           /* -1 (no m/p source), 0, 1 (mp_update_relax_Dclaw4) or 2 (mp_update_FE_4quad) */
     int32_t alphamethod;          /* 0 or 1 */
     int32_t rarecorrectortest;    /* 0/1 */
     int32_t bed_normal;           /* must be 0 */

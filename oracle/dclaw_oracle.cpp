@@ -16,7 +16,7 @@
  *   src/2d/dig/rpt2_dclaw.f        rpt2 :16
  *   src/2d/dig/flux2fw.f           flux2 :8
  *   src/2d/dig/src2.f90            src2 :27
- *   src/2d/dig/mp_update.f90       mp_update_relax_Dclaw4 :710
+ *   src/2d/dig/mp_update.f90       mp_update_relax_Dclaw4 :710, mp_update_FE_4quad :38
  *   src/2d/dig/setaux.f90          ghost bed :155-184, aux defaults :195-198,268-281
  *   src/2d/dig/tick.f              dt update :490-526
  * Clawpack pieces that the reference links from an unpinned Clawpack
@@ -77,6 +77,7 @@ inline double E_atan(double x) { return g_portable_libm ? dclaw::em::d_atan(x) :
 inline double E_tan(double x) { return g_portable_libm ? dclaw::em::d_tan(x) : std::tan(x); }
 inline double E_tanh(double x) { return g_portable_libm ? dclaw::em::d_tanh(x) : std::tanh(x); }
 inline double E_pow73(double x) { return g_portable_libm ? dclaw::em::d_pow_7_3(x) : std::pow(x, 7.0 / 3.0); }
+inline double E_log(double x) { return g_portable_libm ? dclaw::em::d_log(x) : std::log(x); }
 // Fortran MAX/MIN with two arguments
 inline double fmax2(double a, double b) { return a > b ? a : b; }
 inline double fmin2(double a, double b) { return a < b ? a : b; }
@@ -1228,6 +1229,230 @@ void mp_update_relax_Dclaw4(Model& M, double dt, double& h, double& u, double& v
     }
 }
 
+// mp_update.f90:38-707 (src2method 2), debug output omitted. One substep of
+// the quadrant-wise explicit integration of (m, p_exc) on the rho h = const
+// manifold; dtk receives the time the substep covered.
+// Defined choice: in the branch vnorm == 0 or m == m_eq (mp_update.f90:225-249)
+// the reference reads dtm before any assignment (undefined); here dtm = dtr,
+// the whole remaining time, which the surrounding comments describe.
+void mp_update_FE_4quad(Model& M, double dt, double& h, double u, double v, double& m, double& p,
+                        double chi, double rhoh, double gz, double& dtk) {
+    const dclaw_params& P = M.p;
+    const double rho_s = P.rho_s, rho_f = P.rho_f, mu = P.mu, m_crit = P.m_crit, delta = P.delta;
+    double vnorm = std::sqrt(sq(u) + sq(v));
+    double rho, kperm, alphainv, m_eq, tanpsi, tau;
+    setvars(M, h, u, v, m, p, chi, gz, rho, kperm, alphainv, m_eq, tanpsi, tau);
+    double h0 = h;
+    double m_0 = m;
+    double rho0 = m_0 * (rho_s - rho_f) + rho_f;
+    double p0 = p;
+    double p_eq0 = rho_f * gz * h0;
+    double p_exc0 = p0 - p_eq0;
+    dtk = 0.0;
+    double dtr = dt;
+    int quad0 = 0;
+    double km0 = ((2.0 * kperm * (rho0 * rho0)) / (mu * (rhoh * rhoh)));
+    double c_d0 = -3.0 * vnorm * (alphainv * rho0 / (rhoh)) * tanpsi;
+    double kp0 = (kperm / (h0 * mu)) * (3.0 * alphainv * rho0 / rhoh - 1.5 * rho_f * gz * h0 * (rho0 - rho_f) / rhoh);
+    kp0 = fmax2(kp0, 1.0e-3);
+    double hu, hv, hm, p_exc;
+    if (m == 0.0) {
+        p_exc = p_exc0 * E_exp(-kp0 * dtr);
+        qfix_cmass(M, h, m, p, rho, p_exc, hu, hv, hm, u, v, rhoh, gz);
+        dtk = dtr;
+        return;
+    }
+    if ((std::fabs(p_exc0 / (rho_f * gz * h0)) < 1.0e-12) && (std::fabs(m - m_eq) < 1.0e-12)) {
+        dtk = dtr;
+        return;
+    }
+    double dtm, dtp, dts, p_exc_ave;
+    if ((vnorm == 0.0) || (m == m_eq)) {
+        dtm = dtr;  // defined choice (see above)
+        p_exc = p_exc0 * E_exp(-kp0 * dtm);
+        if ((m == m_eq) && (m < 0.3)) {
+        } else {
+            m = m_0 * E_exp(km0 * p_exc * dtm);
+        }
+        qfix_cmass(M, h, m, p, rho, p_exc, hu, hv, hm, u, v, rhoh, gz);
+        dtk = dtm;
+        return;
+    }
+    double m_c = m_crit;
+    double rho_c = m_c * (rho_s - rho_f) + rho_f;
+    double h_c = rhoh / rho_c;
+    double p_eq_c = rho_f * gz * h_c;
+    double shear = 2.0 * vnorm / h0;
+    const double convtol = 1.0e-16;
+    const int itermax = 100;
+    int iter;
+    double normc = 0.0;
+    for (iter = 1; iter <= itermax; ++iter) {
+        double m_c0 = m_c;
+        double p_eq_c0 = p_eq_c;
+        rho_c = m_c * (rho_s - rho_f) + rho_f;
+        h_c = rhoh / rho_c;
+        p_eq_c = rho_f * gz * h_c;
+        double sig_c = fmax2(rhoh * gz - p_eq_c, 0.0);
+        double Nd = rho_s * sq(shear * delta) + sig_c;
+        double Nn = mu * shear;
+        m_c = m_crit * (std::sqrt(Nd) / (std::sqrt(Nd) + std::sqrt(Nn)));
+        normc = sq(1.0e2 * (m_c - m_c0)) + sq(1.0e-3 * (p_eq_c - p_eq_c0));
+        if (normc < convtol) break;
+    }
+    if ((iter >= itermax) && (normc > 1.0)) {
+        m_c = m_crit;
+        rho_c = m_c * (rho_s - rho_f) + rho_f;
+        h_c = rhoh / rho_c;
+        p_eq_c = rho_f * gz * h_c;
+    } else {
+        rho_c = m_c * (rho_s - rho_f) + rho_f;
+        h_c = rhoh / rho_c;
+        p_eq_c = rho_f * gz * h_c;
+    }
+    if ((m < m_c) && (p >= p_eq_c)) quad0 = 1;
+    else if ((m >= m_c) && (p > p_eq_c)) quad0 = 2;
+    else if ((m > m_c) && (p <= p_eq_c)) quad0 = 3;
+    else if ((m <= m_c) && (p < p_eq_c)) quad0 = 4;
+    switch (quad0) {
+        case 1:
+            if (p_exc0 < -1.0e-3 * rhoh * gz) {  // region 1A
+                if (c_d0 > 0.0) dtp = -(1.0 / kp0) * E_log(c_d0 / (c_d0 - kp0 * p_exc0));
+                else dtp = dtr;
+                dtm = E_log(0.98) / (kp0 * p_exc0);
+                dts = fmin2(fmin2(dtr, dtp), dtm);
+                dts = fmax2(dts, 0.0);
+                p_exc = (1.0 / kp0) * ((kp0 * p_exc0 - c_d0) * E_exp(-kp0 * dts) + c_d0);
+                m = m_0 * E_exp(dts * km0 * p_exc);
+            } else if ((-kp0 * p_exc0 + c_d0) > 0.0) {  // region 1B
+                if ((c_d0 / kp0) > (rhoh * gz - p_eq_c))
+                    dtp = fmin2(dtr, -(1.0 / kp0) * E_log((-kp0 * rhoh * gz + kp0 * p_eq_c + c_d0) / (-kp0 * p_exc0 + c_d0)));
+                else
+                    dtp = dtr;
+                p_exc = (1.0 / kp0) * ((kp0 * p_exc0 - c_d0) * E_exp(-kp0 * dtp) + c_d0);
+                p_exc_ave = 0.5 * (p_exc + p_exc0);
+                if (p_exc_ave <= 0.0) {
+                    dtm = dtr;
+                    m = m_0 * E_exp(km0 * 0.5 * (p_exc + p_exc0) * dtm);
+                } else {
+                    if ((km0 * p_exc_ave * m_0) < 1.0e-99) dtm = dtp;
+                    else dtm = fmin2(dtp, (m_eq - m_0) / (km0 * p_exc_ave * m_0));
+                }
+                m = m_0 + km0 * m_0 * p_exc_ave * dtm;
+                dts = dtm;
+            } else {  // region 1C
+                if (c_d0 > 0.0) {
+                    dtp = dtr;
+                    if ((km0 * p_exc0 * m_0) > 1.0e-99) dtm = (m_c - m_0) / (km0 * p_exc0 * m_0);
+                    else dtm = dtp;
+                    dts = fmin2(dtm, dtp);
+                    dts = fmax2(dts, 0.0);
+                    m = m_0 + km0 * m_0 * p_exc0 * dts;
+                    p_exc = (1.0 / kp0) * ((kp0 * p_exc0 - c_d0) * E_exp(-kp0 * dts) + c_d0);
+                } else {
+                    dts = dtr;
+                    dtp = dtr;
+                    if ((km0 * p_exc0 * m_0) > 1.0e-99) dts = fmin2(dtr, (m_c - m_0) / (km0 * p_exc0 * m_0));
+                    if ((kp0 * p_exc0 - c_d0) != 0.0) {
+                        if ((-kp0 * p_eq0 - c_d0) / (kp0 * p_exc0 - c_d0) > 1.0e-99)
+                            dtp = fmin2(dtr, -(1.0 / kp0) * E_log((c_d0) / (c_d0 - kp0 * p_exc0)));
+                    }
+                    dts = fmin2(dts, dtp);
+                    dts = fmax2(dts, 0.0);
+                    m = m_0 + km0 * m_0 * p_exc0 * dts;
+                    p_exc = (1.0 / kp0) * ((kp0 * p_exc0 - c_d0) * E_exp(-kp0 * dts) + c_d0);
+                }
+            }
+            qfix_cmass(M, h, m, p, rho, p_exc, hu, hv, hm, u, v, rhoh, gz);
+            dtk = dts;
+            dtr = dtr - dts;
+            break;
+        case 2:
+            dtp = dtr;
+            if ((c_d0 - kp0 * (p_eq_c - p_eq0)) / (c_d0 - kp0 * p_exc0) > 1.0e-99)
+                dtp = fmin2(dtr, -(1.0 / kp0) * E_log((c_d0 - kp0 * (p_eq_c - p_eq0)) / (c_d0 - kp0 * p_exc0)));
+            dtm = dtp;
+            if (km0 * p_exc0 * m_0 > 1.0e-99)
+                dtm = fmin2(dtp, (fmin2(1.0 - m_0, 0.02) / (km0 * p_exc0 * m_0)));
+            dts = fmin2(dtp, dtm);
+            p_exc = (1.0 / kp0) * ((kp0 * p_exc0 - c_d0) * E_exp(-kp0 * dts) + c_d0);
+            m = m_0 + km0 * m_0 * p_exc * dts;
+            qfix_cmass(M, h, m, p, rho, p_exc, hu, hv, hm, u, v, rhoh, gz);
+            dtk = dts;
+            dtr = dtr - dts;
+            break;
+        case 3:
+            if (p_exc0 > 1.0e-3 * rhoh * gz) {  // region 3A
+                dtp = dtr;
+                if ((c_d0 / (-kp0 * p_exc0 + c_d0)) > 1.0e-99)
+                    dtp = fmin2(dtr, -(1.0 / kp0) * E_log(c_d0 / (c_d0 - kp0 * p_exc0)));
+                dtm = dtp;
+                if ((km0 * p_exc0 * m_0) > 1.0e-99)
+                    dtm = fmin2(dtp, (fmin2(1.0 - m_0, 0.02)) / (km0 * p_exc0 * m_0));
+                p_exc = (1.0 / kp0) * ((kp0 * p_exc0 - c_d0) * E_exp(-kp0 * dtp) + c_d0);
+                m = m_0 + km0 * m_0 * 0.5 * (p_exc0 + p_exc) * dtm;
+                dts = dtp;
+            } else if ((-kp0 * p_exc0 + c_d0) < 0.0) {  // region 3B
+                if (c_d0 / kp0 < -p_eq0) {
+                    dtp = dtr;
+                    if (((c_d0 + kp0 * p_eq0) / (-kp0 * p_exc0 + c_d0)) > 1.0e-99)
+                        dtp = fmin2(dtr, -(1.0 / kp0) * E_log((c_d0 + kp0 * p_eq0) / (-kp0 * p_exc0 + c_d0)));
+                } else {
+                    dtp = dtr;
+                }
+                p_exc = (1.0 / kp0) * ((kp0 * p_exc0 - c_d0) * E_exp(-kp0 * dtp) + c_d0);
+                p_exc_ave = 0.5 * (p_exc + p_exc0);
+                if (p_exc_ave > 0.0) {
+                    dtm = fmin2(dtr, (0.02) / (km0 * p_exc_ave * m_0));
+                } else {
+                    double m_lower = m_eq + fmax2(0.0, (1.0 / 3.0) * kp0 * h0 * (-p_exc_ave) / (vnorm * alphainv));
+                    dtm = fmin2(dtr, (m_lower - m_0) / (km0 * p_exc_ave * m_0));
+                }
+                m = m_0 + km0 * m_0 * p_exc_ave * dtm;
+                dts = dtm;
+            } else {  // region 3C
+                if (c_d0 < 0.0) {
+                    dtp = dtr;
+                    dtm = dtr;
+                    if (-(km0 * p_exc0 * m_0) > 1.0e-99) dtm = (m_c - m_0) / (km0 * p_exc0 * m_0);
+                    dts = fmin2(dtp, dtm);
+                    dts = fmax2(dts, 0.0);
+                    p_exc = (1.0 / kp0) * ((kp0 * p_exc0 - c_d0) * E_exp(-kp0 * dts) + c_d0);
+                    m = m_0 + km0 * m_0 * p_exc0 * dts;
+                } else {
+                    dtm = dtr;
+                    dtp = dtr;
+                    if ((km0 * p_exc0 * m_0) > 1.0e-99) dtm = (m_c - m_0) / (km0 * p_exc0 * m_0);
+                    if ((-c_d0 / (kp0 * p_exc0 - c_d0)) > 1.0e-99)
+                        dtp = -(1.0 / kp0) * E_log(c_d0 / (c_d0 - kp0 * p_exc0));
+                    dts = fmin2(dtp, dtm);
+                    dts = fmax2(dts, 0.0);
+                    p_exc = (1.0 / kp0) * ((kp0 * p_exc0 - c_d0) * E_exp(-kp0 * dts) + c_d0);
+                    m = m_0 + km0 * m_0 * p_exc0 * dts;
+                }
+            }
+            qfix_cmass(M, h, m, p, rho, p_exc, hu, hv, hm, u, v, rhoh, gz);
+            dtk = dts;
+            dtr = dtr - dts;
+            break;
+        case 4:
+            dtp = dtr;
+            if ((c_d0 - kp0 * (p_eq_c - p_eq0)) / (c_d0 - kp0 * p_exc0) > 1.0e-99)
+                dtp = fmin2(dtr, -(1.0 / kp0) * E_log((c_d0 - kp0 * (p_eq_c - p_eq0)) / (c_d0 - kp0 * p_exc0)));
+            dtm = E_log(0.98) / (kp0 * p_exc0);
+            dts = fmin2(dtr, fmin2(dtp, dtm));
+            p_exc = (1.0 / kp0) * ((kp0 * p_exc0 - c_d0) * E_exp(-kp0 * dts) + c_d0);
+            m = m_0 * E_exp(dts * km0 * 0.5 * (p_exc0 + p_exc));
+            dts = dtp;
+            qfix_cmass(M, h, m, p, rho, p_exc, hu, hv, hm, u, v, rhoh, gz);
+            dtk = dts;
+            dtr = dtr - dts;
+            break;
+        default:
+            break;
+    }
+}
+
 // src2.f90:27-306 (bed_normal = 0, curvature = 0, entrainment = 0)
 void src2(Model& M, Patch& pt, double dt) {
     const dclaw_params& P = M.p;
@@ -1268,6 +1493,22 @@ void src2(Model& M, Patch& pt, double dt) {
             setvars(Mt, h, u, v, m, p, chi, gz, rho, kperm, alphainv, m_eq, tanpsi, tau);
             if (P.src2method == -1) {
                 hu = h * u; hv = h * v; hm = h * m; hchi = h * chi;
+            } else if (P.src2method == 2) {
+                // src2.f90:206-229: substeps until dt is covered (<= 100)
+                double dtremaining = dt;
+                const int itercountmax = 100;
+                int itercount = 0;
+                while (dtremaining > 1.0e-99) {
+                    double dtk;
+                    mp_update_FE_4quad(Mt, dtremaining, h, u, v, m, p, chi, rhoh, gz, dtk);
+                    dtremaining = dtremaining - dtk;
+                    itercount = itercount + 1;
+                    if (dtk == 0.0) break;
+                    if (h < P.dry_tolerance) break;
+                    if (itercount >= itercountmax) break;
+                }
+                hu = h * u; hv = h * v; hm = h * m; hchi = h * chi;
+                qfix(Mt, h, hu, hv, hm, p, hchi, u, v, m, chi, rho, gz);
             } else {
                 mp_update_relax_Dclaw4(Mt, dt, h, u, v, m, p, chi, rhoh, gz);
                 hu = h * u; hv = h * v; hm = h * m; hchi = h * chi;
@@ -1430,6 +1671,7 @@ double oracle_elementary(int which, double x) {
         case 2: return dclaw::em::d_tan(x);
         case 3: return dclaw::em::d_tanh(x);
         case 4: return dclaw::em::d_pow_7_3(x);
+        case 5: return dclaw::em::d_log(x);
         default: return 0.0;
     }
 }

@@ -86,8 +86,8 @@ class Oracle:
         self.lib.oracle_set_libm(1 if libm == "portable" else 0)
 
     def elementary(self, name: str, x: float) -> float:
-        """The portable elementary function `name` (exp, atan, tan, tanh, pow73) at x."""
-        return self.lib.oracle_elementary(["exp", "atan", "tan", "tanh", "pow73"].index(name), float(x))
+        """The portable elementary function `name` (exp, atan, tan, tanh, pow73, log) at x."""
+        return self.lib.oracle_elementary(["exp", "atan", "tan", "tanh", "pow73", "log"].index(name), float(x))
 
     def run(self, p: DClawParams, q: np.ndarray, b: np.ndarray, dx: float, dy: float, nsteps: int,
             dt_initial: float, t_final: float = 0.0, fixed_dt: bool = False, parallel: bool = True,

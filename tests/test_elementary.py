@@ -20,6 +20,7 @@ CASES = {
     "tan": (np.tan, [(-1.5, 1.5), (-0.8, 0.8), (-100.0, 100.0)]),
     "tanh": (np.tanh, [(-25.0, 25.0), (-0.6, 0.6), (-1e-6, 1e-6), (-60.0, 60.0)]),
     "pow73": (lambda x: np.power(x, np.longdouble(7) / 3), [(1e-3, 10.0), (1e-6, 1e3)]),
+    "log": (np.log, [(1e-300, 1e300), (0.5, 2.0), (0.9, 1.1), (1e-3, 1e3)]),
 }
 
 
@@ -30,7 +31,7 @@ def test_accuracy(oracle, name):
     worst = 0.0
     for lo, hi in ranges:
         xs = rng.uniform(lo, hi, 4000)
-        if name == "pow73":
+        if name in ("pow73", "log"):
             xs = np.exp(rng.uniform(np.log(lo), np.log(hi), 4000))
         got = np.array([oracle.elementary(name, x) for x in xs])
         ref = fn(xs.astype(np.longdouble))
@@ -46,6 +47,8 @@ def test_special_values(oracle):
     assert e("tanh", 30.0) == 1.0 and e("tanh", -30.0) == -1.0 and e("tanh", 1e-20) == 1e-20
     assert e("atan", 0.0) == 0.0 and abs(e("atan", 1e300) - np.pi / 2) < 1e-16
     assert e("tan", 0.0) == 0.0
+    assert e("log", 1.0) == 0.0 and np.isinf(e("log", 0.0)) and e("log", 0.0) < 0 and np.isnan(e("log", -1.0))
+    assert e("log", 2.0) == np.log(2.0) and abs(e("log", 5e-324) - np.log(5e-324)) < 1e-12
     # tanh(100 (m - 0.1)) saturates to exactly 1 for debris (m > 0.32) as glibc's does
     for m in (0.33, 0.55, 0.64, 1.0):
         assert e("tanh", 100.0 * (m - 0.1)) == 1.0 == np.tanh(100.0 * (m - 0.1))

@@ -38,6 +38,7 @@ VARIANTS = {
     "minmod": dict(limiter=1), "superbee": dict(limiter=2), "vanleer": dict(limiter=3), "nolimiter": dict(limiter=0),
     "extrap": dict(bc_lower=("extrap", "wall"), bc_upper=("extrap", "extrap")),
     "src2m1": dict(src2method=1), "swe": dict(src2method=-1), "alpha1": dict(alphamethod=1),
+    "src2m2": dict(src2method=2, alphamethod=1),
     "rarecorrector": dict(rarecorrectortest=True),
     "manning": dict(friction_forcing=True, manning_coefficient=0.025),
     "dd_manning": dict(friction_forcing=True, manning_coefficient=0.025, dd_manning=True),

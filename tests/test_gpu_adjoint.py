@@ -172,7 +172,7 @@ def test_checkpoint_block_gives_identical_gradients(cuda_device):
         theta = theta_of(p, dev).requires_grad_(True)
         L, _ = _run_loss(q0, theta, b, p, 1.0, n, outs, wts, dt0=0.02, checkpoint_block=blk)
         L.backward()
-        res.append((float(L), q0.grad.clone(), theta.grad.clone()))
+        res.append((float(L.detach()), q0.grad.clone(), theta.grad.clone()))
     for r in res[1:]:
         assert r[0] == res[0][0]
         assert torch.equal(r[1], res[0][1])

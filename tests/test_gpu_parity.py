@@ -72,11 +72,12 @@ def test_slope_runout_short(cuda_device, oracle):
 
 
 @pytest.mark.parametrize("variant", ["order1", "transverse1", "minmod", "extrap", "src2m1", "swe", "alpha1",
-                                     "manning", "speed_limit"])
+                                     "src2m2", "manning", "speed_limit"])
 def test_variants(cuda_device, oracle, variant):
     kw = {"order1": dict(order=1, transverse_waves=0), "transverse1": dict(transverse_waves=1),
           "minmod": dict(limiter=1), "extrap": dict(bc_lower=("extrap", "wall"), bc_upper=("extrap", "extrap")),
           "src2m1": dict(src2method=1), "swe": dict(src2method=-1), "alpha1": dict(alphamethod=1),
+          "src2m2": dict(src2method=2, alphamethod=1),
           "manning": dict(friction_forcing=True, manning_coefficient=0.025),
           "speed_limit": dict(speed_limit=2.0)}[variant]
     base = W.slope_runout(n=96)
@@ -290,3 +291,26 @@ def test_step_function_api(cuda_device, oracle):
     qp, tp, hmax = S.rollout_peak(q0, b, p, grid, t_final=2.0, cfl=0.9, n_steps=40)
     assert torch.equal(qp, qf) and hmax.shape == (64, 64)
     assert torch.all(hmax >= qf[0]) and torch.all(hmax >= q0[0])
+
+
+@pytest.mark.parametrize("dt", [0.01, 0.05, 0.5])
+def test_src2method2_patch_call(cuda_device, oracle, dt):
+    """src2 with mp_update_FE_4quad (src2method 2) through the patch call, on
+    states spread over the four (m, p) quadrants: bit for bit against the
+    oracle with the same elementary functions, 1e-12 against glibc's."""
+    from dclaw_b200.patch import Patch
+
+    from .test_oracle_kats import _quadrant_states
+
+    p = DClawParams(src2method=2, alphamethod=1)
+    q = _quadrant_states(p, n=64, seed=33)
+    n = q.shape[1] - 4
+    aux = np.zeros((6,) + q.shape[1:])
+    P = Patch(p, n, n)
+    qg = torch.tensor(q, device=cuda_device)
+    P.src2(qg, torch.tensor(aux, device=cuda_device), 1.0, 1.0, 0.0, dt)
+    got = qg.cpu().numpy()
+    want = oracle.src2(p, q, aux, dt, libm="portable")
+    assert np.array_equal(got, want), f"max |diff| {np.abs(got - want).max():.3e}"
+    ref = oracle.src2(p, q, aux, dt, libm="glibc")
+    assert rel_err(ref, got) <= 1e-12

@@ -37,8 +37,13 @@ def test_host_side_helpers():
     assert lib.dclaw_params_check(ctypes.byref(mine)) == 0
     bad = DClawParams(bed_normal=1).to_c()
     assert lib.dclaw_params_check(ctypes.byref(bad)) == 2
-    bad = DClawParams(src2method=2).to_c()
+    bad = DClawParams(src2method=3).to_c()
     assert lib.dclaw_params_check(ctypes.byref(bad)) == 2
+    # src2method 2 needs alphamethod 1, as the reference's setrun writer demands
+    bad = DClawParams(src2method=2).to_c()
+    assert lib.dclaw_params_check(ctypes.byref(bad)) == 1
+    ok = DClawParams(src2method=2, alphamethod=1).to_c()
+    assert lib.dclaw_params_check(ctypes.byref(ok)) == 0
     bad = DClawParams(order=3).to_c()
     assert lib.dclaw_params_check(ctypes.byref(bad)) == 1
     assert lib.dclaw_workspace_bytes(1, 10) == 0

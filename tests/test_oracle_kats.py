@@ -97,3 +97,39 @@ def test_libm_sensitivity_one_step(oracle):
     assert np.array_equal(a["q"][0] == 0, b["q"][0] == 0)
     for m in range(5):
         assert np.abs(a["q"][m] - b["q"][m]).max() <= 1e-13 * np.abs(a["q"][m]).max()
+
+
+def _quadrant_states(p, n=48, seed=21):
+    """Padded (5, n+4, n+4) states spread over the (m, p) plane of
+    mp_update_FE_4quad: m either side of m_crit, pore pressure from 0 to
+    above lithostatic, speeds from rest to 6 m/s, depths 5 cm to 2 m."""
+    rng = np.random.default_rng(seed)
+    h = rng.uniform(0.05, 2.0, (n + 4, n + 4))
+    m = rng.uniform(0.40, 0.72, (n + 4, n + 4))
+    rho = p.rho_s * m + (1.0 - m) * p.rho_f
+    pb = rng.uniform(0.0, 1.1, (n + 4, n + 4)) * rho * p.grav * h
+    sp = np.where(rng.random((n + 4, n + 4)) < 0.15, 0.0, rng.uniform(0.0, 6.0, (n + 4, n + 4)))
+    ang = rng.uniform(0.0, 2 * np.pi, (n + 4, n + 4))
+    return np.stack([h, h * sp * np.cos(ang), h * sp * np.sin(ang), h * m, pb])
+
+
+@pytest.mark.parametrize("libm", LIBMS)
+def test_src2method2_keeps_rho_h(oracle, libm):
+    """src2method 2 integrates m and p on the rho h = const manifold
+    (mp_update.f90:13-16,30-33): every wet cell's rho h is unchanged by src2
+    to rounding, while m and p move."""
+    from dclaw_b200.params import DClawParams
+
+    p = DClawParams(src2method=2, alphamethod=1)
+    q = _quadrant_states(p)
+    aux = np.zeros((6,) + q.shape[1:])
+    out = oracle.src2(p, q, aux, 0.05, libm=libm)
+    inner = (slice(None), slice(2, -2), slice(2, -2))
+    qi, qo = q[inner], out[inner]
+    rhoh0 = qi[3] * p.rho_s + (qi[0] - qi[3]) * p.rho_f
+    rhoh1 = qo[3] * p.rho_s + (qo[0] - qo[3]) * p.rho_f
+    wet = qo[0] > p.dry_tolerance
+    assert wet.mean() > 0.95
+    assert np.abs(rhoh1 - rhoh0)[wet].max() <= 1e-12 * rhoh0[wet].max()
+    assert np.abs(qo[3] / qo[0] - qi[3] / qi[0])[wet].max() > 1e-4     # m moved
+    assert np.abs(qo[4] - qi[4])[wet].max() > 1.0                       # p moved
