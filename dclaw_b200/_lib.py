@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes
 from pathlib import Path
 
-from .params import CBatch, CClock, CMember, CParams
+from .params import CAdjBatch, CAdjMember, CBatch, CClock, CMember, CParams
 
 LIB_DIR = Path(__file__).resolve().parent / "lib"
 LIB_PATH = LIB_DIR / "libdclaw_b200.so"
@@ -45,6 +45,10 @@ SIGNATURES = {
     "dclaw_adjoint_supported": (_int, [_pp]),
     "dclaw_step_adjoint": (_int, [_vp, _vp, _int, _int, _dbl, _dbl, _vp, _pp, _vp, _vp, _vp, _vp, _sz, _vp,
                                   _vp]),
+    "dclaw_adjoint_batch_layout": (_int, [_int, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(CAdjMember),
+                                          ctypes.POINTER(CAdjBatch)]),
+    "dclaw_step_adjoint_batched": (_int, [ctypes.POINTER(CAdjBatch), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                          _vp, _vp]),
 }
 
 _lib = None

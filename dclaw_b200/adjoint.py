@@ -28,6 +28,7 @@ import ctypes
 import math
 from typing import Sequence
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -219,4 +220,162 @@ def initial_state(h0: torch.Tensor, m0: torch.Tensor, params: DClawParams, p_rat
     return torch.where(wet.unsqueeze(0), q, torch.zeros_like(q))
 
 
-__all__ = ["StepAdjoint", "rollout_states", "theta_of", "with_theta", "initial_state", "last_dts", "THETA_NAMES"]
+__all__ = ["StepAdjoint", "rollout_states", "theta_of", "with_theta", "initial_state", "last_dts", "THETA_NAMES",
+           "EnsembleStepAdjoint", "ensemble_rollout_states", "ensemble_last_dts"]
+
+
+# ---- ensembles -----------------------------------------------------------------
+class EnsembleStepAdjoint:
+    """The adjoint of one ensemble step (every member of an `EnsembleStepper`'s
+    layout at once): lam_in = (dS/dq)^T lam_out on the state arenas, and
+    pbar[k] += (dS_k/dtheta_k)^T lam_out_k per member (phi in radians).
+    dts: (n,) float64 device tensor, member k's dt."""
+
+    def __init__(self, stepper, params_dev: torch.Tensor | None = None):
+        from .params import CAdjBatch, CAdjMember
+
+        self.lib = _lib.load()
+        st = stepper
+        self.n = st.n
+        for m in st.members:
+            _lib.check(self.lib.dclaw_adjoint_supported(ctypes.byref(m.params.to_c())), "adjoint options")
+        q_off = np.array([st.cm[k].q_off for k in range(self.n)], dtype=np.uint64)
+        b_off = np.array([st.cm[k].b_off for k in range(self.n)], dtype=np.uint64)
+        self.am = (CAdjMember * self.n)()
+        self.batch = CAdjBatch()
+        _lib.check(self.lib.dclaw_adjoint_batch_layout(self.n, st.mx.ctypes.data, st.my.ctypes.data,
+                                                       st.dxs.ctypes.data, st.dys.ctypes.data, q_off.ctypes.data,
+                                                       b_off.ctypes.data, self.am, ctypes.byref(self.batch)),
+                   "adjoint batch layout")
+        dev = st.device
+        self.members_dev = torch.frombuffer(bytearray(bytes(self.am)), dtype=torch.uint8).to(dev)
+        self.params = st.params if params_dev is None else params_dev
+        self.bed = st.bed
+        self.work = torch.empty(self.batch.work_bytes, dtype=torch.uint8, device=dev)
+        self.status = torch.zeros(self.n, dtype=torch.int32, device=dev)
+
+    def vjp(self, q_in: torch.Tensor, dts: torch.Tensor, lam_out: torch.Tensor, lam_in: torch.Tensor,
+            pbar: torch.Tensor) -> None:
+        rc = self.lib.dclaw_step_adjoint_batched(ctypes.byref(self.batch), _lib.ptr(self.members_dev),
+                                                 _lib.ptr(self.params), _lib.ptr(dts), _lib.ptr(q_in),
+                                                 _lib.ptr(self.bed), _lib.ptr(lam_out), _lib.ptr(lam_in),
+                                                 _lib.ptr(pbar), _lib.ptr(self.work), _lib.ptr(self.status),
+                                                 _lib.stream_ptr())
+        _lib.check(rc, "dclaw_step_adjoint_batched")
+
+    def check_status(self) -> None:
+        for k, st in enumerate(self.status.tolist()):
+            _lib.check(int(st), f"ensemble adjoint, member {k}")
+
+
+def _ensemble(members, theta, fixed_dt: bool):
+    from .ensemble import EnsembleStepper, Member
+
+    th = theta.detach().cpu().tolist()
+    mem = [Member(m.q, m.b, with_theta(m.params, th[k]), m.dx, m.dy, m.dt_initial, m.t_final)
+           for k, m in enumerate(members)]
+    return EnsembleStepper(mem, theta.device, fixed_dt=fixed_dt)
+
+
+def _clock_field(st, k: int) -> torch.Tensor:
+    from .params import CLOCK_DOUBLES
+
+    return st.clocks.view(st.n, CLOCK_DOUBLES)[:, k]
+
+
+class _EnsembleRollout(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, q0, theta, members, n_steps, out_steps, checkpoint_block, fixed_dt, dt_schedule):
+        st = _ensemble(members, theta, fixed_dt or dt_schedule is not None)
+        st.qa.copy_(q0.detach())
+        k = _block(n_steps, checkpoint_block)
+        dts = torch.empty((n_steps, st.n), dtype=torch.float64, device=q0.device)
+        outs = torch.empty((len(out_steps),) + tuple(q0.shape), dtype=q0.dtype, device=q0.device)
+        where = {}
+        for idx, n in enumerate(out_steps):
+            where.setdefault(n, []).append(idx)
+        for idx in where.get(0, []):
+            outs[idx].copy_(q0)
+        ckpt = []
+        for n in range(n_steps):
+            if n % k == 0:
+                ckpt.append(st.qa.clone())
+            if dt_schedule is not None:
+                _clock_field(st, 1).copy_(dt_schedule[n])
+            st.step(1)
+            dts[n].copy_(_clock_field(st, 3))
+            for idx in where.get(n + 1, []):
+                outs[idx].copy_(st.qa)
+        for kk, s in enumerate(st.status()):
+            _lib.check(s, f"ensemble rollout, member {kk}")
+        ctx.save_for_backward(dts)
+        ctx.ckpt = ckpt
+        ctx.meta = (members, theta.detach(), int(n_steps), tuple(out_steps), k)
+        return outs
+
+    @staticmethod
+    def backward(ctx, g_out):
+        (dts,) = ctx.saved_tensors
+        members, theta, n_steps, out_steps, k = ctx.meta
+        dev = dts.device
+        where = {}
+        for idx, n in enumerate(out_steps):
+            where.setdefault(n, []).append(idx)
+        fw = _ensemble(members, theta, True)
+        adj = EnsembleStepAdjoint(fw)
+        lam = torch.zeros_like(fw.qa)
+        lam2 = torch.zeros_like(lam)   # arena gaps between members stay zero
+        pbar = torch.zeros((fw.n, 4), dtype=torch.float64, device=dev)
+        seg = torch.empty((k,) + tuple(fw.qa.shape), dtype=torch.float64, device=dev)
+        g_out = g_out.contiguous() if g_out is not None else None
+        for s in reversed(range(len(ctx.ckpt))):
+            n0 = s * k
+            n1 = min(n0 + k, n_steps)
+            seg[0].copy_(ctx.ckpt[s])
+            fw.qa.copy_(ctx.ckpt[s])
+            for n in range(n0 + 1, n1):
+                _clock_field(fw, 1).copy_(dts[n - 1])
+                fw.step(1)
+                seg[n - n0].copy_(fw.qa)
+            for n in range(n1, n0, -1):
+                if g_out is not None:
+                    for idx in where.get(n, []):
+                        lam.add_(g_out[idx])
+                adj.vjp(seg[n - 1 - n0], dts[n - 1], lam, lam2, pbar)
+                lam, lam2 = lam2, lam
+        if g_out is not None:
+            for idx in where.get(0, []):
+                lam.add_(g_out[idx])
+        for kk, st in enumerate(fw.status()):
+            _lib.check(st, f"ensemble recompute, member {kk}")
+        adj.check_status()
+        scale = torch.tensor([_DEG, 1.0, 1.0, 1.0], dtype=torch.float64, device=dev)
+        return lam, pbar * scale, None, None, None, None, None, None
+
+
+def ensemble_rollout_states(q0: torch.Tensor, theta: torch.Tensor, members, n_steps: int, out_steps,
+                            checkpoint_block: int | None = None, fixed_dt: bool = False,
+                            dt_schedule: torch.Tensor | None = None) -> torch.Tensor:
+    """Differentiable run of an ensemble (the batched form of `rollout_states`).
+
+    members: list of `ensemble.Member` (bed, parameters, spacing, first dt;
+    their q only sets the layout); q0: the state arena of an
+    `EnsembleStepper` over them (float64 CUDA tensor, member k at its q_off);
+    theta: (n, 4) float64 tensor, row k = (phi [deg], kref, alpha_c, mu) of
+    member k. Returns the arenas after each step count in out_steps, shape
+    (len(out_steps), arena size). Every member keeps its own dt (tick rule,
+    or fixed; dt_schedule (n_steps, n) replays recorded dts). The backward
+    pass runs the batched step adjoint with sqrt(N) checkpointing.
+    """
+    for n in out_steps:
+        if not 0 <= n <= n_steps:
+            raise ValueError(f"output step {n} outside 0..{n_steps}")
+    if dt_schedule is not None and dt_schedule.shape != (n_steps, len(members)):
+        raise ValueError("dt_schedule must be (n_steps, n_members)")
+    return _EnsembleRollout.apply(q0, theta, list(members), int(n_steps), tuple(int(n) for n in out_steps),
+                                  checkpoint_block, bool(fixed_dt), dt_schedule)
+
+
+def ensemble_last_dts(out: torch.Tensor) -> torch.Tensor:
+    """The (n_steps, n_members) dts recorded by the ensemble rollout that produced `out`."""
+    return out.grad_fn.saved_tensors[0]

@@ -37,15 +37,15 @@ namespace adj {
 constexpr int ATPB = DCLAW_ADJ_TPB;
 constexpr int NWARP = ATPB / 32;
 
-inline unsigned nblk(long long n) { return (unsigned)((n + ATPB - 1) / ATPB); }
+__host__ __device__ inline unsigned nblk(long long n) { return (unsigned)((n + ATPB - 1) / ATPB); }
 
 __device__ __forceinline__ void flag(int32_t* st, int code) {
     if (st) atomicCAS(st, 0, code);
 }
 
 // Sum of the block's per-thread parameter adjoints, in a fixed order, into
-// part[blockIdx.x * NPB + k]. Every thread of the block must call it.
-__device__ __forceinline__ void block_pbar(const double* pb, double* __restrict__ part) {
+// dst[0..NPB). Every thread of the block must call it.
+__device__ __forceinline__ void block_pbar(const double* pb, double* __restrict__ dst) {
     __shared__ double red[NPB][NWARP];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
@@ -58,7 +58,7 @@ __device__ __forceinline__ void block_pbar(const double* pb, double* __restrict_
     if (threadIdx.x < NPB) {
         double s = 0.0;
         for (int w = 0; w < NWARP; ++w) s += red[threadIdx.x][w];
-        part[(size_t)blockIdx.x * NPB + threadIdx.x] = s;
+        dst[threadIdx.x] = s;
     }
 }
 
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_rv_src2(dclaw_params P
         int i = (int)(idx % g.mx) + 1, j = (int)(idx / g.mx) + 1;
         adj_item_src2(P, g, W, A, lam_out, i, j, *dtp, pb);
     }
-    block_pbar(pb, part);
+    block_pbar(pb, part + (size_t)blockIdx.x * NPB);
 }
 
 template <int DIR>
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_rv_riemann(dclaw_param
         int r = DIR == 0 ? s : a, i = DIR == 0 ? a : s;
         if (!adj_item_riemann<DIR>(P, g, W, A, r, i, pb)) flag(status, DCLAW_ERR_UNSUPPORTED);
     }
-    block_pbar(pb, part);
+    block_pbar(pb, part + (size_t)blockIdx.x * NPB);
 }
 
 __global__ void __launch_bounds__(ATPB) k_rv_taudir(dclaw_params P, Geom g, Work W, AdjWork A,
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(ATPB) k_rv_taudir(dclaw_params P, Geom g, Work
         int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
         adj_item_taudir(P, g, W, A, i, j, pb);
     }
-    block_pbar(pb, part);
+    block_pbar(pb, part + (size_t)blockIdx.x * NPB);
 }
 
 __global__ void __launch_bounds__(ATPB) k_rv_b4(dclaw_params P, Geom g, Work W, AdjWork A,
@@ -209,7 +209,7 @@ struct AdjLayout {
     size_t total;
 };
 
-inline AdjLayout adj_layout(int mx, int my) {
+__host__ __device__ inline AdjLayout adj_layout(int mx, int my) {
     AdjLayout L;
     L.S = staged_layout(mx, my);
     L.nb_src2 = nblk((long long)mx * my);
@@ -233,6 +233,176 @@ inline AdjLayout adj_layout(int mx, int my) {
 
 inline bool adj_sizes_ok(int mx, int my) {
     return mx >= 2 && my >= 2 && (long long)(mx + 4) * (my + 4) < (1LL << 40);
+}
+
+// ---- ensembles: the same stages over the chunks of every member -------------
+enum { SP_PAD = 0, SP_INT, SP_RX, SP_RY, SP_FX, SP_FY, NSPACE };
+enum {
+    OP_FW_B4, OP_FW_TAUDIR, OP_FW_SVREC, OP_FW_RX, OP_FW_RY, OP_FW_FX, OP_FW_FY,
+    OP_RV_SRC2, OP_RV_FX, OP_RV_FY, OP_RV_RX, OP_RV_RY, OP_RV_TAUDIR, OP_RV_B4, OP_RV_GATHER
+};
+
+template <int OP>
+struct OpTraits;
+#define DC_OP(op, space, pb) \
+    template <>              \
+    struct OpTraits<op> {    \
+        static constexpr int SPACE = space; \
+        static constexpr bool PBAR = pb;    \
+    };
+DC_OP(OP_FW_B4, SP_PAD, false)
+DC_OP(OP_FW_TAUDIR, SP_PAD, false)
+DC_OP(OP_FW_SVREC, SP_PAD, false)
+DC_OP(OP_FW_RX, SP_RX, false)
+DC_OP(OP_FW_RY, SP_RY, false)
+DC_OP(OP_FW_FX, SP_FX, false)
+DC_OP(OP_FW_FY, SP_FY, false)
+DC_OP(OP_RV_SRC2, SP_INT, true)
+DC_OP(OP_RV_FX, SP_FX, false)
+DC_OP(OP_RV_FY, SP_FY, false)
+DC_OP(OP_RV_RX, SP_RX, true)
+DC_OP(OP_RV_RY, SP_RY, true)
+DC_OP(OP_RV_TAUDIR, SP_PAD, true)
+DC_OP(OP_RV_B4, SP_PAD, false)
+DC_OP(OP_RV_GATHER, SP_INT, false)
+#undef DC_OP
+
+__host__ __device__ inline long long space_items(int sp, int mx, int my) {
+    switch (sp) {
+        case SP_PAD: return (long long)(mx + 4) * (my + 4);
+        case SP_INT: return (long long)mx * my;
+        case SP_RX: return (long long)(mx + 3) * (my + 2);
+        case SP_RY: return (long long)(mx + 2) * (my + 3);
+        case SP_FX: return (long long)(mx + 1) * (my + 2);
+        default: return (long long)(mx + 2) * (my + 1);
+    }
+}
+
+struct BatchArgs {
+    int nmem;
+    const dclaw_adj_member* mem;
+    const dclaw_params* prm;
+    const double* dt;
+    const double* q;
+    const double* b;
+    const double* lam_out;
+    double* lam_in;
+    char* work;
+    int32_t* status;
+};
+
+// One stage over the chunks of all members (grid-stride; every thread of a
+// block runs the same number of iterations, so the barriers are uniform).
+template <int OP>
+__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_adj_batch(BatchArgs a, uint32_t nchunks) {
+    constexpr int SP = OpTraits<OP>::SPACE;
+    __shared__ dclaw_adj_member sM;
+    __shared__ dclaw_params sP;
+    __shared__ int s_m;
+    int cur = -1;
+    for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = a.nmem - 1;
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (a.mem[mid].chunk0[SP] <= ch) lo = mid;
+                else hi = mid - 1;
+            }
+            s_m = lo;
+        }
+        __syncthreads();
+        const int m = s_m;
+        if (m != cur) {
+            const int nM = (int)(sizeof(dclaw_adj_member) / 4), nP = (int)(sizeof(dclaw_params) / 4);
+            for (int k = threadIdx.x; k < nM + nP; k += blockDim.x) {
+                if (k < nM) reinterpret_cast<int*>(&sM)[k] = reinterpret_cast<const int*>(a.mem + m)[k];
+                else reinterpret_cast<int*>(&sP)[k - nM] = reinterpret_cast<const int*>(a.prm + m)[k - nM];
+            }
+            __syncthreads();
+            cur = m;
+        }
+        const int mx = sM.mx, my = sM.my;
+        const Geom g{mx, my, mx + 4, my + 4, sM.dx, sM.dy};
+        const AdjLayout L = adj_layout(mx, my);
+        char* base = a.work + sM.work_off;
+        const Work W = make_work(base, L.S);
+        const AdjWork A{(double*)(base + L.off_lamq), (double*)(base + L.off_xfb), (double*)(base + L.off_yfb),
+                        (double*)(base + L.off_xcb), (double*)(base + L.off_ycb), (double*)(base + L.off_tdq),
+                        (double*)(base + L.off_qsb), (double*)(base + L.off_sv)};
+        const uint32_t lch = ch - sM.chunk0[SP];
+        const long long idx = (long long)lch * ATPB + threadIdx.x;
+        const double* q_in = a.q + sM.q_off;
+        double pb[NPB] = {0.0, 0.0, 0.0, 0.0};
+        if (idx < space_items(SP, mx, my)) {
+            const double dt = a.dt[m];
+            if (SP == SP_PAD) {
+                const int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
+                if (OP == OP_FW_B4) {
+                    if (stage_b4(sP, g, q_in, a.b + sM.b_off, W, i, j) && a.status) atomicCAS(a.status + m, 0, DCLAW_ERR_NAN);
+                } else if (OP == OP_FW_TAUDIR) {
+                    stage_taudir(sP, g, W, i, j);
+                } else if (OP == OP_FW_SVREC) {
+                    adj_item_svrec(sP, g, W, A, i, j);
+                } else if (OP == OP_RV_TAUDIR) {
+                    adj_item_taudir(sP, g, W, A, i, j, pb);
+                } else if (OP == OP_RV_B4) {
+                    adj_item_b4(sP, g, W, A, q_in, i, j);
+                }
+            } else if (SP == SP_INT) {
+                const int i = (int)(idx % mx) + 1, j = (int)(idx / mx) + 1;
+                if (OP == OP_RV_SRC2) adj_item_src2(sP, g, W, A, a.lam_out + sM.q_off, i, j, dt, pb);
+                else if (OP == OP_RV_GATHER) adj_item_gather(sP, g, A, W, a.lam_in + sM.q_off, i, j);
+            } else if (SP == SP_RX || SP == SP_RY) {
+                const int nfast = SP == SP_RX ? mx + 3 : mx + 2;
+                const int af = (int)(idx % nfast), as = (int)(idx / nfast);
+                const int r = SP == SP_RX ? as : af, i = SP == SP_RX ? af : as;
+                constexpr int DIR = SP == SP_RX ? 0 : 1;
+                if (OP == OP_FW_RX || OP == OP_FW_RY) {
+                    stage_riemann<DIR>(sP, g, W, r, i, nullptr, A.sv);
+                } else {
+                    if (!adj_item_riemann<DIR>(sP, g, W, A, r, i, pb) && a.status)
+                        atomicCAS(a.status + m, 0, DCLAW_ERR_UNSUPPORTED);
+                }
+            } else {
+                const int nfast = SP == SP_FX ? mx + 1 : mx + 2;
+                const int af = (int)(idx % nfast), as = (int)(idx / nfast);
+                const int r = SP == SP_FX ? as : af, i = SP == SP_FX ? af + 1 : as + 1;
+                constexpr int DIR = SP == SP_FX ? 0 : 1;
+                if (OP == OP_FW_FX || OP == OP_FW_FY) stage_flux<DIR>(sP, g, W, r, i, DIR == 0 ? dt / g.dx : dt / g.dy, nullptr);
+                else adj_item_flux<DIR>(sP, g, W, A, r, i, dt);
+            }
+        }
+        if (OpTraits<OP>::PBAR) {
+            // the member's block partials, in the single-patch call's order
+            double* part = (double*)(base + L.off_part);
+            const long long off = OP == OP_RV_SRC2 ? 0
+                                  : OP == OP_RV_RX ? L.nb_src2
+                                  : OP == OP_RV_RY ? L.nb_src2 + L.nb_rx
+                                                   : L.nb_src2 + L.nb_rx + L.nb_ry;
+            block_pbar(pb, part + (size_t)(off + lch) * NPB);
+        }
+        __syncthreads();
+    }
+}
+
+// pbar[4 m + k] += member m's partials, summed as k_rv_pbar sums them
+__global__ void __launch_bounds__(ATPB) k_adj_batch_pbar(BatchArgs a, double* __restrict__ pbar) {
+    __shared__ double red[NPB][ATPB];
+    const int m = blockIdx.x;
+    const dclaw_adj_member M = a.mem[m];
+    const AdjLayout L = adj_layout(M.mx, M.my);
+    const double* part = (const double*)(a.work + M.work_off + L.off_part);
+    for (int k = 0; k < NPB; ++k) {
+        double s = 0.0;
+        for (long long b = threadIdx.x; b < L.nparts; b += ATPB) s += part[b * NPB + k];
+        red[k][threadIdx.x] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < NPB) {
+        double s = 0.0;
+        for (int t = 0; t < ATPB; ++t) s += red[threadIdx.x][t];
+        pbar[(size_t)m * NPB + threadIdx.x] += s;
+    }
 }
 
 }  // namespace adj
@@ -301,6 +471,77 @@ int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, doub
     k_rv_b4<<<nblk(npad), ATPB, 0, s>>>(P, g, W, A, q_in);
     k_rv_gather<<<nblk(nint), ATPB, 0, s>>>(P, g, W, A, lam_in);
     k_rv_pbar<<<1, ATPB, 0, s>>>(part, L.nparts, pbar);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? DCLAW_OK : DCLAW_ERR_CUDA;
+}
+
+int dclaw_adjoint_batch_layout(int n, const int32_t* mx, const int32_t* my, const double* dx, const double* dy,
+                               const uint64_t* q_off, const uint64_t* b_off, dclaw_adj_member* members,
+                               dclaw_adj_batch* batch) {
+    if (n <= 0 || !mx || !my || !dx || !dy || !q_off || !b_off || !members || !batch) return DCLAW_ERR_ARG;
+    uint64_t w = 0;
+    uint64_t nch[NSPACE] = {0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < n; ++k) {
+        if (!adj_sizes_ok(mx[k], my[k]) || !(dx[k] > 0.0) || !(dy[k] > 0.0)) return DCLAW_ERR_ARG;
+        dclaw_adj_member& M = members[k];
+        M.mx = mx[k];
+        M.my = my[k];
+        M.dx = dx[k];
+        M.dy = dy[k];
+        M.q_off = q_off[k];
+        M.b_off = b_off[k];
+        M.work_off = w;
+        w += align256(adj_layout(mx[k], my[k]).total);
+        for (int sp = 0; sp < NSPACE; ++sp) {
+            const uint64_t c = nblk(space_items(sp, mx[k], my[k]));
+            if (nch[sp] + c > 0xffffffffull) return DCLAW_ERR_TOO_LARGE;
+            M.chunk0[sp] = (uint32_t)nch[sp];
+            M.nchunk[sp] = (uint32_t)c;
+            nch[sp] += c;
+        }
+    }
+    batch->nmembers = n;
+    batch->chunk_items = ATPB;
+    for (int sp = 0; sp < NSPACE; ++sp) batch->nchunks[sp] = (uint32_t)nch[sp];
+    batch->work_bytes = w;
+    return DCLAW_OK;
+}
+
+int dclaw_step_adjoint_batched(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
+                               const dclaw_params* params, const double* dt, const double* q_in, const double* b,
+                               const double* lam_out, double* lam_in, double* pbar, void* work, int32_t* status,
+                               void* stream) {
+    if (!batch || !members || !params || !dt || !q_in || !b || !lam_out || !lam_in || !pbar || !work)
+        return DCLAW_ERR_ARG;
+    if (batch->nmembers <= 0 || batch->chunk_items != (uint32_t)ATPB || lam_in == lam_out) return DCLAW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    BatchArgs a{batch->nmembers, members, params, dt, q_in, b, lam_out, lam_in, (char*)work, status};
+    // persistent grids: a few blocks per SM, capped by the chunks of the space
+    auto grid = [&](int sp) -> unsigned {
+        uint32_t c = batch->nchunks[sp];
+        uint32_t cap = (uint32_t)nsm * 8u;
+        return c < cap ? (c ? c : 1u) : cap;
+    };
+#define DC_LAUNCH(op) k_adj_batch<op><<<grid(OpTraits<op>::SPACE), ATPB, 0, s>>>(a, batch->nchunks[OpTraits<op>::SPACE])
+    DC_LAUNCH(OP_FW_B4);
+    DC_LAUNCH(OP_FW_TAUDIR);
+    DC_LAUNCH(OP_FW_SVREC);
+    DC_LAUNCH(OP_FW_RX);
+    DC_LAUNCH(OP_FW_RY);
+    DC_LAUNCH(OP_FW_FX);
+    DC_LAUNCH(OP_FW_FY);
+    DC_LAUNCH(OP_RV_SRC2);
+    DC_LAUNCH(OP_RV_FX);
+    DC_LAUNCH(OP_RV_FY);
+    DC_LAUNCH(OP_RV_RX);
+    DC_LAUNCH(OP_RV_RY);
+    DC_LAUNCH(OP_RV_TAUDIR);
+    DC_LAUNCH(OP_RV_B4);
+    DC_LAUNCH(OP_RV_GATHER);
+#undef DC_LAUNCH
+    k_adj_batch_pbar<<<batch->nmembers, ATPB, 0, s>>>(a, pbar);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DCLAW_OK : DCLAW_ERR_CUDA;
 }

@@ -16,6 +16,11 @@
 namespace dclaw {
 
 constexpr int TPB = 256;
+// threads per CTA of the single-patch tile kernel
+#ifndef DCLAW_TILE_TPB
+#define DCLAW_TILE_TPB 256
+#endif
+constexpr int TILE_TPB = DCLAW_TILE_TPB;
 constexpr int MAX_DEVICES = 64;
 // tile of the fused step: with 16 x 14 the flux phases of k_tile fit in one
 // round of 256 threads (256 and 252 cells) and the solves in two
@@ -45,7 +50,7 @@ __device__ __forceinline__ double warp_max(double v) {
 
 // block-wide max of a non-negative value into *acc (bit pattern of a double)
 __device__ __forceinline__ void block_max_to(double v, unsigned long long* acc) {
-    __shared__ double red[TPB / 32];
+    __shared__ double red[32];
     v = warp_max(v);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 0) red[wid] = v;
@@ -210,7 +215,7 @@ __device__ __forceinline__ void last_block_tick(const dclaw_params& P, dclaw_clo
 // One tile of the fused step (all threads of the CTA call it). smem holds
 // TileGeom<TX,TY>::SMEM_BYTES. Returns this thread's Courant-number
 // contribution; *nan is set when an updated state holds a NaN.
-template <int TX, int TY, bool WITH_SRC2>
+template <int TX, int TY, bool WITH_SRC2, int NT>
 __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g, const Rec& R,
                                             const double* __restrict__ b, double* __restrict__ q_out, double dt,
                                             int i0, int j0, double* smem, uint32_t* __restrict__ brlog, bool& nan) {
@@ -235,14 +240,14 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
     // within distance 3 are all dry stays dry: all its interfaces are
     // dry-dry (skipped) and src2 zeroes dry cells
     bool any = false;
-    for (int it = tid; it < TG::NHB; it += TPB)
+    for (int it = tid; it < TG::NHB; it += NT)
         if (tile_stage_hb(g, R, b, M, it)) any = true;
     any = __syncthreads_or(any) != 0;
     double cfl = 0.0;
     nan = false;
     const size_t plane = (size_t)g.mx * g.my;
     if (!any && !brlog) {
-        for (int it = tid; it < TX * TY; it += TPB) {
+        for (int it = tid; it < TX * TY; it += NT) {
             int i = i0 + it % TX, j = j0 + it / TX;
             if (i > g.mx || j > g.my) continue;
             size_t c = (size_t)(j - 1) * g.mx + (size_t)(i - 1);
@@ -264,7 +269,7 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
             if (tid == 0) *M.nlist = 0;
             __syncthreads();
             const int lane = tid & 31;
-            for (int it0 = 0; it0 < nsolve; it0 += TPB) {
+            for (int it0 = 0; it0 < nsolve; it0 += NT) {
                 const int it = it0 + tid;
                 bool need = it < nsolve && tile_needs_solve(P, g, M, dir, it, i0, j0, TX);
                 if (it < nsolve && !need) {
@@ -279,27 +284,27 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
             }
             __syncthreads();
             const int nneed = *M.nlist;
-            for (int w = tid; w < nneed; w += TPB) {
+            for (int w = tid; w < nneed; w += NT) {
                 bool ok;
                 double s = tile_riemann(P, g, R, M, dir, M.list[w], i0, j0, TX, TY, ok);
                 if (ok) cfl = fmax2(cfl, dtd * s);
             }
             __syncthreads();
             const int ncell = dir == 0 ? (TY + 2) * TX : TY * (TX + 2);
-            for (int it = tid; it < ncell; it += TPB) tile_flux<TX, TY>(P, g, R, M, dir, it, i0, j0, dtd, brlog);
+            for (int it = tid; it < ncell; it += NT) tile_flux<TX, TY>(P, g, R, M, dir, it, i0, j0, dtd, brlog);
             __syncthreads();
             if (dir == 0) {
                 double T0[5], T1[5];
                 const int nT = (TY + 1) * TX;
                 bool v0 = tid < nT && tile_T<TX, TY>(g, M, tid, i0, j0, T0);
-                bool v1 = tid + TPB < nT && tile_T<TX, TY>(g, M, tid + TPB, i0, j0, T1);
+                bool v1 = tid + NT < nT && tile_T<TX, TY>(g, M, tid + NT, i0, j0, T1);
                 __syncthreads();
                 if (v0) tile_T_store<TX, TY>(M, tid, T0);
-                if (v1) tile_T_store<TX, TY>(M, tid + TPB, T1);
+                if (v1) tile_T_store<TX, TY>(M, tid + NT, T1);
                 __syncthreads();
             }
         }
-        for (int it = tid; it < TX * TY; it += TPB)
+        for (int it = tid; it < TX * TY; it += NT)
             if (tile_final<TX, TY, WITH_SRC2>(P, g, R, M, it, i0, j0, dt, q_out)) nan = true;
     }
     if (!(cfl == cfl)) cfl = 0.0;
@@ -307,13 +312,13 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
 }
 
 template <int TX, int TY, bool WITH_SRC2>
-__global__ void __launch_bounds__(TPB, DCLAW_TILE_MINBLOCKS) k_tile(dclaw_params P, Geom g, Rec R, const double* __restrict__ b,
+__global__ void __launch_bounds__(TILE_TPB, DCLAW_TILE_MINBLOCKS) k_tile(dclaw_params P, Geom g, Rec R, const double* __restrict__ b,
                                                  double* __restrict__ q_out, dclaw_clock* clk,
                                                  uint32_t* __restrict__ brlog) {
     extern __shared__ double smem[];
     const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
     bool nan;
-    double cfl = tile_body<TX, TY, WITH_SRC2>(P, g, R, b, q_out, clk->dt, i0, j0, smem, brlog, nan);
+    double cfl = tile_body<TX, TY, WITH_SRC2, TILE_TPB>(P, g, R, b, q_out, clk->dt, i0, j0, smem, brlog, nan);
     if (nan) flag_status(clk, DCLAW_ERR_NAN);
     block_max_to(cfl, reinterpret_cast<unsigned long long*>(&clk->cfl_bits));
     if (WITH_SRC2) last_block_tick(P, clk);
@@ -417,7 +422,7 @@ __global__ void __launch_bounds__(TPB, 2) k_tile_batch(int nmem, uint32_t ntiles
         const unsigned int lt = t - sM.tile0;
         const int i0 = 1 + (int)(lt % sM.ntiles_x) * TX, j0 = 1 + (int)(lt / sM.ntiles_x) * TY;
         bool nan;
-        double cfl = tile_body<TX, TY, false>(sP, g, R, b + sM.b_off, work + sM.qs_off, clocks[m].dt, i0, j0, smem,
+        double cfl = tile_body<TX, TY, false, TPB>(sP, g, R, b + sM.b_off, work + sM.qs_off, clocks[m].dt, i0, j0, smem,
                                               nullptr, nan);
         if (nan) flag_status(clocks + m, DCLAW_ERR_NAN);
         // block max of this tile's Courant number into member m's clock
@@ -778,10 +783,10 @@ int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int m
     dim3 grid((mx + TILE_X - 1) / TILE_X, (my + TILE_Y - 1) / TILE_Y);
     if (DCLAW_SRC2_KERNEL) {
         double* qstar = (double*)((char*)work + L.off_qstar);
-        k_tile<TILE_X, TILE_Y, false><<<grid, TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, qstar, clock, branch_log);
+        k_tile<TILE_X, TILE_Y, false><<<grid, TILE_TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, qstar, clock, branch_log);
         k_src2_cells<<<nblocks((long long)mx * my), TPB, 0, s>>>(P, g, qstar, q_out, clock);
     } else {
-        k_tile<TILE_X, TILE_Y, true><<<grid, TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock, branch_log);
+        k_tile<TILE_X, TILE_Y, true><<<grid, TILE_TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock, branch_log);
     }
     return cuda_status();
 }
@@ -909,7 +914,7 @@ int dclaw_step_noalloc(const double* q_in, double* q_out, const double* b, int m
     const dclaw_params P = *p;
     k_records<<<nblocks((long long)npad), TPB, 0, s>>>(P, g, q_in, b, R, clock);
     dim3 grid((mx + TILE_X - 1) / TILE_X, (my + TILE_Y - 1) / TILE_Y);
-    k_tile<TILE_X, TILE_Y, true><<<grid, TPB, TileGeom<TILE_X, TILE_Y>::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock,
+    k_tile<TILE_X, TILE_Y, true><<<grid, TILE_TPB, TileGeom<TILE_X, TILE_Y>::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock,
                                                                                      nullptr);
     return cuda_status();
 }

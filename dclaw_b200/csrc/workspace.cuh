@@ -10,16 +10,22 @@
 #include <stddef.h>
 #include "stages.cuh"
 
+#if defined(__CUDACC__)
+#define WS_HD __host__ __device__ inline
+#else
+#define WS_HD inline
+#endif
+
 namespace dclaw {
 
-inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+WS_HD size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 struct StagedLayout {
     size_t npad, nxi, nyi;
     size_t off_qB, off_bP, off_td, off_wx, off_wy, off_fx, off_fy, total;
 };
 
-inline StagedLayout staged_layout(int mx, int my) {
+WS_HD StagedLayout staged_layout(int mx, int my) {
     StagedLayout L;
     L.npad = (size_t)(mx + 4) * (my + 4);
     L.nxi = (size_t)(mx + 3) * (my + 2);
@@ -36,7 +42,7 @@ inline StagedLayout staged_layout(int mx, int my) {
     return L;
 }
 
-inline Work make_work(void* base, const StagedLayout& L) {
+WS_HD Work make_work(void* base, const StagedLayout& L) {
     char* b = (char*)base;
     Work W;
     W.qB = (double*)(b + L.off_qB);

@@ -65,9 +65,10 @@ class EnsembleStepper:
         self.fixed_dt = fixed_dt
         self._layout(tile_shape)
         # arenas
-        self.qa = torch.empty(self.batch.q_doubles, dtype=torch.float64, device=self.device)
-        self.qb = torch.empty_like(self.qa)
-        self.bed = torch.empty(self.batch.b_doubles, dtype=torch.float64, device=self.device)
+        # zeroed: the alignment gaps between members are never written
+        self.qa = torch.zeros(self.batch.q_doubles, dtype=torch.float64, device=self.device)
+        self.qb = torch.zeros_like(self.qa)
+        self.bed = torch.zeros(self.batch.b_doubles, dtype=torch.float64, device=self.device)
         for k, m in enumerate(members):
             o, c = self.cm[k].q_off, int(self.mx[k]) * int(self.my[k])
             self.qa[o:o + 5 * c].copy_(torch.from_numpy(np.ascontiguousarray(m.q, dtype=np.float64).ravel()))

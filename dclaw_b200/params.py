@@ -104,6 +104,26 @@ class CBatch(ctypes.Structure):
     ]
 
 
+class CAdjMember(ctypes.Structure):
+    """ctypes image of `dclaw_adj_member` (one ensemble member of the adjoint)."""
+
+    _fields_ = [
+        ("mx", ctypes.c_int32), ("my", ctypes.c_int32),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+        ("q_off", ctypes.c_uint64), ("b_off", ctypes.c_uint64), ("work_off", ctypes.c_uint64),
+        ("chunk0", ctypes.c_uint32 * 6), ("nchunk", ctypes.c_uint32 * 6),
+    ]
+
+
+class CAdjBatch(ctypes.Structure):
+    """ctypes image of `dclaw_adj_batch`."""
+
+    _fields_ = [
+        ("nmembers", ctypes.c_int32), ("chunk_items", ctypes.c_uint32), ("nchunks", ctypes.c_uint32 * 6),
+        ("work_bytes", ctypes.c_uint64),
+    ]
+
+
 @dataclasses.dataclass
 class DClawParams:
     """D-Claw parameters for one run (or one ensemble member).

@@ -264,6 +264,49 @@ int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, doub
                        const double* dt, const dclaw_params* p, const double* lam_out, double* lam_in,
                        double* pbar, void* work, size_t work_bytes, int32_t* status, void* stream);
 
+/* ---- adjoint of one step of an ensemble ---------------------------------------
+ * The reference differentiates its particle filters member by member with
+ * jax.jacfwd / jax.grad under jax.vmap (gradient_particle_filter/pf_flume/
+ * inference.py:96-108). Here the adjoint of one step of every member of an
+ * ensemble of uneven patches runs as one sequence of 16 launches, each a
+ * grid-stride loop over the chunks of all members' items. Each member has its
+ * own parameters, dt and parameter adjoints; member k's results equal those of
+ * dclaw_step_adjoint on member k alone, bit for bit.
+ * Item spaces (chunk0 / nchunk index): 0 padded cells, 1 interior cells,
+ * 2 x-interface solves, 3 y-interface solves, 4 x-interface fluxes, 5 y-interface
+ * fluxes. */
+typedef struct dclaw_adj_member {
+    int32_t mx, my;
+    double dx, dy;
+    uint64_t q_off;        /* doubles into the state and adjoint arenas ([5][my][mx]) */
+    uint64_t b_off;        /* doubles into the bed arena */
+    uint64_t work_off;     /* bytes into the batch's adjoint workspace (256-aligned) */
+    uint32_t chunk0[6];    /* first chunk of the member in each item space */
+    uint32_t nchunk[6];    /* chunks of the member in each item space */
+} dclaw_adj_member;
+
+typedef struct dclaw_adj_batch {
+    int32_t nmembers;
+    uint32_t chunk_items;  /* items per chunk (threads per block) */
+    uint32_t nchunks[6];   /* chunks of all members per item space */
+    uint64_t work_bytes;   /* adjoint workspace of the whole batch */
+} dclaw_adj_batch;
+
+/* host-side layout: members[0..n) (host array) from sizes, spacings and the
+ * members' offsets in the state / bed arenas (host arrays, in doubles) */
+int dclaw_adjoint_batch_layout(int n, const int32_t* mx, const int32_t* my, const double* dx, const double* dy,
+                               const uint64_t* q_off, const uint64_t* b_off, dclaw_adj_member* members,
+                               dclaw_adj_batch* batch);
+/* batch: host; members, params, dt (one per member), status (one int32 per
+ * member, nullable), pbar (4 per member, accumulated): DEVICE arrays.
+ * q_in, lam_out, lam_in: state-shaped arenas; b: bed arena; work:
+ * batch->work_bytes. Members whose options have no adjoint form get
+ * DCLAW_ERR_UNSUPPORTED in their status word. */
+int dclaw_step_adjoint_batched(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
+                               const dclaw_params* params, const double* dt, const double* q_in, const double* b,
+                               const double* lam_out, double* lam_in, double* pbar, void* work, int32_t* status,
+                               void* stream);
+
 /* initialise a device clock: t, dt, t_final, fixed_dt; counters cleared */
 int dclaw_clock_init(dclaw_clock* clock, double t, double dt, double t_final, int fixed_dt,
                      void* stream);

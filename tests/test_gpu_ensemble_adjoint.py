@@ -1,0 +1,91 @@
+"""The batched step adjoint (dclaw_step_adjoint_batched through the C ABI)
+and the differentiable ensemble rollout, against the single-patch adjoint
+member by member: the batched launches run the same reverse stages on every
+member's own layout, parameters and dt, so state and parameter adjoints are
+bit-identical to dclaw_step_adjoint on each member alone, and so are whole
+checkpointed gradients. The single-patch adjoint is checked against finite
+differences in test_gpu_adjoint.py."""
+import numpy as np
+import pytest
+import torch
+
+from dclaw_b200 import workloads as W
+from dclaw_b200.adjoint import (EnsembleStepAdjoint, StepAdjoint, ensemble_rollout_states, rollout_states,
+                                theta_of)
+from dclaw_b200.ensemble import EnsembleStepper, Member
+
+pytestmark = pytest.mark.gpu
+
+
+def _members(seed=5):
+    """Uneven members, each with its own parameters and first dt; all in motion
+    after a few steps of their release."""
+    out = []
+    for c in W.flume_ensemble(n=3, seed=seed, width_range=(6, 20), length_range=(40, 90)):
+        out.append(Member(c.q, c.b, c.params, c.dx, c.dy, 2.0e-3))
+    rf = W.random_field_case(n=40, dx=0.5, seed=seed + 1)
+    p = rf.params.replace(bc_lower=("wall", "extrap"), bc_upper=("extrap", "wall"), transverse_waves=1,
+                          phi=34.0, kref=2e-10)
+    out.append(Member(rf.q, rf.b, p, rf.dx, rf.dy, 0.01))
+    rf2 = W.random_field_case(n=32, dx=0.5, seed=seed + 2)
+    out.append(Member(rf2.q[:, :21, :].copy(), rf2.b[:21, :].copy(), rf2.params.replace(order=1, limiter=1),
+                      0.5, 0.25, 0.005))
+    return out
+
+
+def _advance(members, dev, n=12):
+    """The members' states after n steps (moving flows) as new members."""
+    ens = EnsembleStepper(members, dev)
+    ens.step(n)
+    return [Member(ens.state(k).cpu().numpy(), m.b, m.params, m.dx, m.dy, m.dt_initial)
+            for k, m in enumerate(members)]
+
+
+def test_batched_step_adjoint_matches_single_patch(cuda_device):
+    dev = cuda_device
+    members = _advance(_members(), dev)
+    ens = EnsembleStepper(members, dev)
+    adj = EnsembleStepAdjoint(ens)
+    rng = np.random.default_rng(3)
+    lam = torch.tensor(rng.standard_normal(ens.qa.numel()), device=dev)
+    dts = torch.tensor([0.004 + 0.001 * k for k in range(ens.n)], dtype=torch.float64, device=dev)
+    lam_in = torch.zeros_like(lam)
+    pbar = torch.zeros((ens.n, 4), dtype=torch.float64, device=dev)
+    adj.vjp(ens.qa, dts, lam, lam_in, pbar)
+    torch.cuda.synchronize()
+    adj.check_status()
+    for k, m in enumerate(members):
+        o, c = ens.cm[k].q_off, m.q.size
+        sa = StepAdjoint(torch.tensor(m.b, device=dev), m.params, m.dx, m.dy)
+        li = torch.empty(m.q.shape, dtype=torch.float64, device=dev)
+        pb = torch.zeros(4, dtype=torch.float64, device=dev)
+        sa.vjp(ens.qa[o:o + c].view(m.q.shape), dts[k:k + 1], lam[o:o + c].view(m.q.shape).contiguous(), li, pb)
+        assert torch.equal(lam_in[o:o + c].view(m.q.shape), li), f"member {k}: state adjoint differs"
+        assert torch.equal(pbar[k], pb), f"member {k}: parameter adjoint differs"
+
+
+def test_ensemble_gradient_matches_single_patch_gradients(cuda_device):
+    """Per-member losses over output times; the batched checkpointed gradient
+    equals each member's unbatched rollout_states gradient, bit for bit."""
+    dev = cuda_device
+    members = _advance(_members(seed=9), dev, n=8)
+    ens = EnsembleStepper(members, dev)
+    n, outs = 14, [3, 7, 14]
+    q0 = ens.qa.clone().requires_grad_(True)
+    theta = torch.stack([theta_of(m.params, dev) for m in members]).requires_grad_(True)
+    rng = np.random.default_rng(4)
+    wts = torch.tensor(rng.standard_normal((len(outs), ens.qa.numel())), device=dev)
+    o = ensemble_rollout_states(q0, theta, members, n, outs, checkpoint_block=4)
+    L = (o * wts).sum()
+    L.backward()
+    for k, m in enumerate(members):
+        off, c = ens.cm[k].q_off, m.q.size
+        qk = torch.tensor(m.q, device=dev, requires_grad=True)
+        tk = theta_of(m.params, dev).requires_grad_(True)
+        ok = rollout_states(qk, tk, torch.tensor(m.b, device=dev), m.params, m.dx, m.dy, n, outs,
+                            m.dt_initial, checkpoint_block=5)
+        Lk = (ok * wts[:, off:off + c].view((len(outs),) + m.q.shape)).sum()
+        Lk.backward()
+        assert torch.equal(o.detach()[:, off:off + c].view(ok.shape), ok.detach()), f"member {k}: states"
+        assert torch.equal(q0.grad[off:off + c].view(m.q.shape), qk.grad), f"member {k}: state gradient"
+        assert torch.equal(theta.grad[k], tk.grad), f"member {k}: parameter gradient"
