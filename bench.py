@@ -63,7 +63,11 @@ def parse():
     ap.add_argument("--grad-steps", type=int, default=500,
                     help="steps of the 512 x 512 gradient case measured beside the plain step (0: skip)")
     ap.add_argument("--checkpoint-block", type=int, default=0, help="0: ceil(sqrt(steps))")
-    ap.add_argument("--only", default="", choices=["", "batched", "gradient"],
+    ap.add_argument("--bgrad-members", type=int, default=64,
+                    help="members of the batched-gradient channel case (0: skip)")
+    ap.add_argument("--bgrad-steps", type=int, default=200,
+                    help="steps of the batched-gradient case (the case is defined over 800)")
+    ap.add_argument("--only", default="", choices=["", "batched", "gradient", "batched_gradient"],
                     help="run one side measurement alone and print its object (profiling runs)")
     return ap.parse_args()
 
@@ -288,10 +292,12 @@ def gradient_bench(args, dev):
         e.record()
         return e
 
+    sel = gj * c.b.shape[1] + gi            # depth plane entries of the gauge cells
+
     def gauges(h, m0, theta):
         q0 = initial_state(h, m0, p)
-        o = rollout_states(q0, theta, b, p, c.dx, c.dx, c.nsteps, c.out_steps, c.dt_initial, checkpoint_block=blk)
-        return o[:, 0, gj, gi]
+        return rollout_states(q0, theta, b, p, c.dx, c.dx, c.nsteps, c.out_steps, c.dt_initial,
+                              checkpoint_block=blk, select=sel)
 
     with torch.no_grad():
         target = gauges(h0, torch.tensor(c.m0, dtype=torch.float64, device=dev), theta_of(c.true_params, dev))
@@ -332,6 +338,111 @@ def gradient_bench(args, dev):
             "peak_mem_gb": torch.cuda.max_memory_allocated(dev) / 1e9,
             "gpu_launches": {"adjoint_per_step": 16, "recompute_per_step": 3, "forward_per_step": 3},
             "note": "dt of each step chosen by the tick rule in the forward pass and replayed, not differentiated"}
+
+
+def batched_gradient_bench(args, dev):
+    """Per-member gradients over an ensemble of uneven channels: each member's
+    gauge loss (16 centreline gauges x 50 output times against a target run
+    at its own perturbed parameters) differentiated with respect to its four
+    material parameters, its solid fraction m0 and its release-block volume,
+    by the batched step adjoint with sqrt(N) checkpointing. Timed against the
+    batched forward solve of the same run; both with CUDA events. The
+    unbatched reference times rollout_states gradients of the first two
+    members one after the other."""
+    import torch
+
+    from dclaw_b200 import workloads as W
+    from dclaw_b200.adjoint import ensemble_rollout_states, initial_state, rollout_states, theta_of
+    from dclaw_b200.ensemble import EnsembleStepper, Member
+
+    c = W.batched_gradient_case(n=args.bgrad_members, nsteps=args.bgrad_steps)
+    n = len(c.members)
+    members = [Member(m.q, m.b, m.params, m.dx, m.dy, m.dt_initial) for m in c.members]
+    ens = EnsembleStepper(members, dev)
+    total = ens.qa.numel()
+    offs = [int(ens.cm[k].q_off) for k in range(n)]
+    masks = [torch.tensor(mk, device=dev) for mk in c.block_masks]
+    gidx = []
+    for k, m in enumerate(c.members):
+        mx = m.q.shape[2]
+        gidx += [offs[k] + int(j) * mx + int(i) for j, i in c.gauges[k]]
+    gidx = torch.tensor(gidx, device=dev)
+
+    def arena(H, m0):
+        pieces, pos = [], 0
+        for k, m in enumerate(c.members):
+            if offs[k] > pos:
+                pieces.append(torch.zeros(offs[k] - pos, dtype=torch.float64, device=dev))
+            qk = initial_state(H[k] * masks[k], m0[k], m.params)
+            pieces.append(qk.reshape(-1))
+            pos = offs[k] + qk.numel()
+        if pos < total:
+            pieces.append(torch.zeros(total - pos, dtype=torch.float64, device=dev))
+        return torch.cat(pieces)
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        return e
+
+    ones = torch.ones(n, dtype=torch.float64, device=dev)
+    m0s = torch.tensor([m.params.m0 for m in c.members], dtype=torch.float64, device=dev)
+    th_true = torch.stack([theta_of(p, dev) for p in c.true_params])
+    with torch.no_grad():
+        target = ensemble_rollout_states(arena(ones, m0s), th_true, members, c.nsteps, c.out_steps, select=gidx)
+    # forward solve of the same run (batched fused steps)
+    q0 = arena(ones, m0s).detach()
+    fwd = []
+    for _ in range(2):
+        st = EnsembleStepper(members, dev)
+        st.qa.copy_(q0)
+        torch.cuda.synchronize()
+        e0 = ev()
+        st.step(c.nsteps)
+        e1 = ev()
+        torch.cuda.synchronize()
+        fwd.append(e0.elapsed_time(e1))
+        del st
+    H = ones.clone().requires_grad_(True)
+    m0 = m0s.clone().requires_grad_(True)
+    theta = torch.stack([theta_of(m.params, dev) for m in c.members]).requires_grad_(True)
+    torch.cuda.synchronize()
+    torch.cuda.reset_peak_memory_stats(dev)
+    e0 = ev()
+    out = ensemble_rollout_states(arena(H, m0), theta, members, c.nsteps, c.out_steps, select=gidx)
+    loss = ((out - target) ** 2).sum()
+    loss.backward()
+    e1 = ev()
+    torch.cuda.synchronize()
+    grad_ms = e0.elapsed_time(e1)
+    peak = torch.cuda.max_memory_allocated(dev) / 1e9
+    # unbatched: the first two members' gradients, one patch at a time
+    unb = 0.0
+    for k in range(min(2, n)):
+        m = c.members[k]
+        b = torch.tensor(m.b, device=dev)
+        tk = theta_of(m.params, dev).requires_grad_(True)
+        qk = initial_state(masks[k].clone(), torch.tensor(m.params.m0, dtype=torch.float64, device=dev), m.params)
+        selk = torch.tensor([int(j) * m.q.shape[2] + int(i) for j, i in c.gauges[k]], device=dev)
+        tgt = target[:, k * 16:(k + 1) * 16]
+        torch.cuda.synchronize()
+        f0 = ev()
+        ok = rollout_states(qk, tk, b, m.params, m.dx, m.dy, c.nsteps, c.out_steps, m.dt_initial, select=selk)
+        ((ok - tgt) ** 2).sum().backward()
+        f1 = ev()
+        torch.cuda.synchronize()
+        unb += f0.elapsed_time(f1)
+    cells = sum(m.q.shape[1] * m.q.shape[2] for m in c.members)
+    area = torch.tensor(c.block_area, dtype=torch.float64, device=dev)
+    return {"workload": f"channels_{n}x1024_w128-256_dx0.05_{c.nsteps}steps", "members": n, "cells": cells,
+            "steps": c.nsteps, "forward_ms": min(fwd), "gradient_ms": grad_ms,
+            "gradient_over_forward": grad_ms / min(fwd), "unbatched_first2_gradient_ms": unb,
+            "batched_gradient_ms_per_member": grad_ms / n, "peak_mem_gb": peak,
+            "grad_member0": {"phi_deg": float(theta.grad[0, 0]), "kref": float(theta.grad[0, 1]),
+                             "alpha_c": float(theta.grad[0, 2]), "mu": float(theta.grad[0, 3]),
+                             "m0": float(m0.grad[0]), "block_volume": float(H.grad[0] / area[0])},
+            "gpu_launches": {"adjoint_per_step": 16, "recompute_per_step": 3, "forward_per_step": 3},
+            "note": "every member's dt from its own tick rule, recorded and replayed, not differentiated"}
 
 
 def run_ours(args):
@@ -434,6 +545,8 @@ def run_ours(args):
         out["batched"] = ensemble_bench(args, dev)
     if rank == 0 and world == 1 and args.grad_steps > 0:
         out["gradient"] = gradient_bench(args, dev)
+    if rank == 0 and world == 1 and args.bgrad_members > 0 and args.bgrad_steps > 0:
+        out["batched_gradient"] = batched_gradient_bench(args, dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args, case, args.cpu_steps)
     if rank == 0:
@@ -449,7 +562,8 @@ def run_only(args):
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    out = ensemble_bench(args, dev) if args.only == "batched" else gradient_bench(args, dev)
+    fn = {"batched": ensemble_bench, "gradient": gradient_bench, "batched_gradient": batched_gradient_bench}
+    out = fn[args.only](args, dev)
     print(json.dumps(out), flush=True)
 
 

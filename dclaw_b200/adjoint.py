@@ -93,7 +93,7 @@ def _block(n_steps: int, checkpoint_block: int | None) -> int:
 class _Rollout(torch.autograd.Function):
     @staticmethod
     def forward(ctx, q0, theta, b, params, dx, dy, n_steps, out_steps, dt0, fixed_dt, t_final, checkpoint_block,
-                dt_schedule):
+                dt_schedule, select):
         prm = with_theta(params, theta.detach().cpu())
         st = PatchStepper(q0.detach(), b, prm, dx, dy)
         if dt_schedule is not None:
@@ -103,12 +103,14 @@ class _Rollout(torch.autograd.Function):
         k = _block(n_steps, checkpoint_block)
         dts = torch.empty(n_steps, dtype=torch.float64, device=q0.device)
         ckpt = []
-        outs = torch.empty((len(out_steps),) + tuple(q0.shape), dtype=q0.dtype, device=q0.device)
+        oshape = tuple(q0.shape) if select is None else tuple(select.shape)
+        outs = torch.empty((len(out_steps),) + oshape, dtype=q0.dtype, device=q0.device)
+        pick = (lambda t: t) if select is None else (lambda t: t.reshape(-1)[select])
         where = {}
         for idx, n in enumerate(out_steps):
             where.setdefault(n, []).append(idx)
         for idx in where.get(0, []):
-            outs[idx].copy_(q0)
+            outs[idx].copy_(pick(q0.detach()))
         for n in range(n_steps):
             if n % k == 0:
                 ckpt.append(st.state().clone())
@@ -117,10 +119,11 @@ class _Rollout(torch.autograd.Function):
             st.step(1)
             dts[n:n + 1].copy_(st.clock[3:4])   # dt the step used
             for idx in where.get(n + 1, []):
-                outs[idx].copy_(st.state())
+                outs[idx].copy_(pick(st.state()))
         _lib.check(st.status(), "rollout forward")
         ctx.save_for_backward(b, dts)
         ctx.ckpt = ckpt
+        ctx.select = select
         ctx.meta = (prm, float(dx), float(dy), int(n_steps), tuple(out_steps), k)
         return outs
 
@@ -141,6 +144,14 @@ class _Rollout(torch.autograd.Function):
         pbar = torch.zeros(4, dtype=torch.float64, device=dev)
         seg = torch.empty((k,) + tuple(shape), dtype=torch.float64, device=dev)
         g_out = g_out.contiguous() if g_out is not None else None
+        sel = ctx.select
+
+        def add_out(idx):
+            if sel is None:
+                lam.add_(g_out[idx])
+            else:
+                lam.view(-1).index_add_(0, sel.reshape(-1), g_out[idx].reshape(-1))
+
         nblocks = len(ctx.ckpt)
         for s in reversed(range(nblocks)):
             n0 = s * k
@@ -155,22 +166,22 @@ class _Rollout(torch.autograd.Function):
             for n in range(n1, n0, -1):
                 if g_out is not None:
                     for idx in where.get(n, []):
-                        lam.add_(g_out[idx])
+                        add_out(idx)
                 adj.vjp(seg[n - 1 - n0], dts[n - 1:n], lam, lam2, pbar)
                 lam, lam2 = lam2, lam
         if g_out is not None:
             for idx in where.get(0, []):
-                lam.add_(g_out[idx])
+                add_out(idx)
         _lib.check(fw.status(), "rollout recompute")
         adj.check_status()
         scale = torch.tensor([_DEG, 1.0, 1.0, 1.0], dtype=torch.float64, device=dev)
-        return lam, pbar * scale, None, None, None, None, None, None, None, None, None, None, None
+        return lam, pbar * scale, None, None, None, None, None, None, None, None, None, None, None, None
 
 
 def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b: torch.Tensor, params: DClawParams, dx: float,
                    dy: float, n_steps: int, out_steps: Sequence[int], dt0: float, fixed_dt: bool = False,
                    t_final: float = 0.0, checkpoint_block: int | None = None,
-                   dt_schedule: torch.Tensor | None = None) -> torch.Tensor:
+                   dt_schedule: torch.Tensor | None = None, select: torch.Tensor | None = None) -> torch.Tensor:
     """Differentiable run of n_steps fused steps on one patch.
 
     q0: (5, my, mx) float64 CUDA tensor (x fastest), theta: (4,) float64
@@ -184,6 +195,9 @@ def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b: torch.Tensor, param
     dt_schedule (n_steps,) float64 device tensor: replay these dts instead
     (dt0, fixed_dt and t_final are then ignored) -- e.g. the dts of an
     earlier adaptive run, for finite-difference checks at a fixed schedule.
+    select (int64 CUDA tensor of flat indices into the (5, my, mx) state):
+    return only these entries at each output step, shape (len(out_steps),
+    *select.shape) -- e.g. gauge cells' depths -- instead of whole states.
     """
     for n in out_steps:
         if not 0 <= n <= n_steps:
@@ -193,7 +207,7 @@ def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b: torch.Tensor, param
             raise ValueError("dt_schedule must be a (n_steps,) float64 CUDA tensor")
         dt_schedule = dt_schedule.contiguous()
     return _Rollout.apply(q0, theta, b.contiguous(), params, dx, dy, int(n_steps), tuple(int(n) for n in out_steps),
-                          float(dt0), bool(fixed_dt), float(t_final), checkpoint_block, dt_schedule)
+                          float(dt0), bool(fixed_dt), float(t_final), checkpoint_block, dt_schedule, select)
 
 
 def last_dts(out: torch.Tensor) -> torch.Tensor:
@@ -285,17 +299,19 @@ def _clock_field(st, k: int) -> torch.Tensor:
 
 class _EnsembleRollout(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, q0, theta, members, n_steps, out_steps, checkpoint_block, fixed_dt, dt_schedule):
+    def forward(ctx, q0, theta, members, n_steps, out_steps, checkpoint_block, fixed_dt, dt_schedule, select):
         st = _ensemble(members, theta, fixed_dt or dt_schedule is not None)
         st.qa.copy_(q0.detach())
         k = _block(n_steps, checkpoint_block)
         dts = torch.empty((n_steps, st.n), dtype=torch.float64, device=q0.device)
-        outs = torch.empty((len(out_steps),) + tuple(q0.shape), dtype=q0.dtype, device=q0.device)
+        oshape = tuple(q0.shape) if select is None else tuple(select.shape)
+        outs = torch.empty((len(out_steps),) + oshape, dtype=q0.dtype, device=q0.device)
+        pick = (lambda t: t) if select is None else (lambda t: t[select])
         where = {}
         for idx, n in enumerate(out_steps):
             where.setdefault(n, []).append(idx)
         for idx in where.get(0, []):
-            outs[idx].copy_(q0)
+            outs[idx].copy_(pick(q0.detach()))
         ckpt = []
         for n in range(n_steps):
             if n % k == 0:
@@ -305,11 +321,12 @@ class _EnsembleRollout(torch.autograd.Function):
             st.step(1)
             dts[n].copy_(_clock_field(st, 3))
             for idx in where.get(n + 1, []):
-                outs[idx].copy_(st.qa)
+                outs[idx].copy_(pick(st.qa))
         for kk, s in enumerate(st.status()):
             _lib.check(s, f"ensemble rollout, member {kk}")
         ctx.save_for_backward(dts)
         ctx.ckpt = ckpt
+        ctx.select = select
         ctx.meta = (members, theta.detach(), int(n_steps), tuple(out_steps), k)
         return outs
 
@@ -328,6 +345,14 @@ class _EnsembleRollout(torch.autograd.Function):
         pbar = torch.zeros((fw.n, 4), dtype=torch.float64, device=dev)
         seg = torch.empty((k,) + tuple(fw.qa.shape), dtype=torch.float64, device=dev)
         g_out = g_out.contiguous() if g_out is not None else None
+        sel = ctx.select
+
+        def add_out(idx):
+            if sel is None:
+                lam.add_(g_out[idx])
+            else:
+                lam.index_add_(0, sel.reshape(-1), g_out[idx].reshape(-1))
+
         for s in reversed(range(len(ctx.ckpt))):
             n0 = s * k
             n1 = min(n0 + k, n_steps)
@@ -340,22 +365,22 @@ class _EnsembleRollout(torch.autograd.Function):
             for n in range(n1, n0, -1):
                 if g_out is not None:
                     for idx in where.get(n, []):
-                        lam.add_(g_out[idx])
+                        add_out(idx)
                 adj.vjp(seg[n - 1 - n0], dts[n - 1], lam, lam2, pbar)
                 lam, lam2 = lam2, lam
         if g_out is not None:
             for idx in where.get(0, []):
-                lam.add_(g_out[idx])
+                add_out(idx)
         for kk, st in enumerate(fw.status()):
             _lib.check(st, f"ensemble recompute, member {kk}")
         adj.check_status()
         scale = torch.tensor([_DEG, 1.0, 1.0, 1.0], dtype=torch.float64, device=dev)
-        return lam, pbar * scale, None, None, None, None, None, None
+        return lam, pbar * scale, None, None, None, None, None, None, None
 
 
 def ensemble_rollout_states(q0: torch.Tensor, theta: torch.Tensor, members, n_steps: int, out_steps,
                             checkpoint_block: int | None = None, fixed_dt: bool = False,
-                            dt_schedule: torch.Tensor | None = None) -> torch.Tensor:
+                            dt_schedule: torch.Tensor | None = None, select: torch.Tensor | None = None) -> torch.Tensor:
     """Differentiable run of an ensemble (the batched form of `rollout_states`).
 
     members: list of `ensemble.Member` (bed, parameters, spacing, first dt;
@@ -364,8 +389,10 @@ def ensemble_rollout_states(q0: torch.Tensor, theta: torch.Tensor, members, n_st
     theta: (n, 4) float64 tensor, row k = (phi [deg], kref, alpha_c, mu) of
     member k. Returns the arenas after each step count in out_steps, shape
     (len(out_steps), arena size). Every member keeps its own dt (tick rule,
-    or fixed; dt_schedule (n_steps, n) replays recorded dts). The backward
-    pass runs the batched step adjoint with sqrt(N) checkpointing.
+    or fixed; dt_schedule (n_steps, n) replays recorded dts). select (int64
+    CUDA tensor of arena indices): return only these entries per output
+    step (gauges) instead of whole arenas. The backward pass runs the
+    batched step adjoint with sqrt(N) checkpointing.
     """
     for n in out_steps:
         if not 0 <= n <= n_steps:
@@ -373,7 +400,7 @@ def ensemble_rollout_states(q0: torch.Tensor, theta: torch.Tensor, members, n_st
     if dt_schedule is not None and dt_schedule.shape != (n_steps, len(members)):
         raise ValueError("dt_schedule must be (n_steps, n_members)")
     return _EnsembleRollout.apply(q0, theta, list(members), int(n_steps), tuple(int(n) for n in out_steps),
-                                  checkpoint_block, bool(fixed_dt), dt_schedule)
+                                  checkpoint_block, bool(fixed_dt), dt_schedule, select)
 
 
 def ensemble_last_dts(out: torch.Tensor) -> torch.Tensor:

@@ -257,3 +257,45 @@ def gradient_case(n: int = 512, dx: float = 1.0, seed: int = 7, nsteps: int = 50
     out_steps = list(range(every, nsteps + 1, every))[:n_out]
     true = p.replace(phi=30.0, kref=3.0e-10, alpha_c=0.015)
     return GradientCase(b, h0, 0.62, p, true, gauges, out_steps, nsteps, dx, 0.05)
+
+
+@dataclasses.dataclass
+class BatchedGradientCase:
+    """Per-member gauge losses over an ensemble of channels."""
+
+    members: list            # Case per member (q at the members' own release block)
+    true_params: list        # DClawParams per member for the synthetic targets
+    block_masks: list        # (my, mx) 0/1 masks of the release blocks
+    block_area: list         # m^2 of each release block
+    gauges: list             # (16, 2) cell indices (j, i) per member, along the centreline
+    out_steps: list
+    nsteps: int
+
+
+def batched_gradient_case(n: int = 64, seed: int = 11, length: int = 1024, width_range=(128, 256),
+                          dx: float = 0.05, n_gauges: int = 16, nsteps: int = 800, n_out: int = 50):
+    """n channels of `length` x U[width_range] cells at dx on a 31 deg slope with a
+    horizontal runout (the flume members of the ensemble case), each with its
+    own parameters from the priors (phi U[28, 40] deg, log10 k0 U[-11, -8],
+    m0 U[0.55, 0.65], alpha U[0.005, 0.05]) and a 3 m x 1 m release block;
+    16 gauges along each centreline from below the block to the runout, read
+    at n_out evenly spaced output steps. Each member's target comes from the
+    same solver at its own perturbed parameters (phi + 1.5 deg, kref x 2,
+    alpha_c x 1.3)."""
+    rng = np.random.default_rng(seed)
+    members, true, masks, areas, gauges = [], [], [], [], []
+    for _ in range(n):
+        w = int(rng.integers(width_range[0], width_range[1] + 1))
+        p = DClawParams(phi=float(rng.uniform(28.0, 40.0)), kref=float(10.0 ** rng.uniform(-11.0, -8.0)),
+                        m0=float(rng.uniform(0.55, 0.65)), alpha_c=float(rng.uniform(0.005, 0.05)))
+        q, b = flume_member(w, length, dx, p)
+        mask = (q[0] > 0.0).astype(np.float64)
+        members.append(Case(f"channel_{w}x{length}", q, b, dx, dx, p, nsteps, 1.0e-3))
+        true.append(p.replace(phi=p.phi + 1.5, kref=2.0 * p.kref, alpha_c=1.3 * p.alpha_c))
+        masks.append(mask)
+        areas.append(float(mask.sum()) * dx * dx)
+        xi = np.linspace(int(4.0 / dx), int(0.9 * length), n_gauges).astype(int)
+        gauges.append(np.stack([np.full(n_gauges, w // 2), xi], axis=1))
+    every = max(1, nsteps // n_out)
+    out_steps = list(range(every, nsteps + 1, every))[:n_out]
+    return BatchedGradientCase(members, true, masks, areas, gauges, out_steps, nsteps)

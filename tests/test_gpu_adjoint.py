@@ -253,3 +253,27 @@ def test_unsupported_options_are_refused(cuda_device):
         StepAdjoint(b, DClawParams(rarecorrectortest=True), 1.0, 1.0)
     with pytest.raises(_lib.DClawError):
         StepAdjoint(b, DClawParams(friction_forcing=True, manning_coefficient=0.03), 1.0, 1.0)
+
+
+def test_select_outputs_give_the_same_gradient(cuda_device):
+    """Returning only selected entries (gauges) at the output steps gives the
+    gradient of the same loss computed from whole output states."""
+    dev = cuda_device
+    p, qn, bn = _small_flow(seed=3)
+    b = torch.tensor(bn, device=dev)
+    n, outs = 12, [4, 8, 12]
+    rng = np.random.default_rng(6)
+    sel = torch.tensor(rng.choice(qn.size, size=40, replace=False), device=dev)
+    res = []
+    for use_sel in (False, True):
+        q0 = torch.tensor(qn, device=dev, requires_grad=True)
+        theta = theta_of(p, dev).requires_grad_(True)
+        if use_sel:
+            o = rollout_states(q0, theta, b, p, 1.0, 1.0, n, outs, 0.02, select=sel)
+        else:
+            o = rollout_states(q0, theta, b, p, 1.0, 1.0, n, outs, 0.02).reshape(len(outs), -1)[:, sel]
+        L = (o ** 2).sum()
+        L.backward()
+        res.append((o.detach(), q0.grad.clone(), theta.grad.clone()))
+    assert torch.equal(res[0][0], res[1][0])
+    assert torch.equal(res[0][1], res[1][1]) and torch.equal(res[0][2], res[1][2])

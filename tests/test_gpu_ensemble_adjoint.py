@@ -89,3 +89,26 @@ def test_ensemble_gradient_matches_single_patch_gradients(cuda_device):
         assert torch.equal(o.detach()[:, off:off + c].view(ok.shape), ok.detach()), f"member {k}: states"
         assert torch.equal(q0.grad[off:off + c].view(m.q.shape), qk.grad), f"member {k}: state gradient"
         assert torch.equal(theta.grad[k], tk.grad), f"member {k}: parameter gradient"
+
+
+def test_ensemble_select_outputs(cuda_device):
+    """Selected arena entries at the output steps give the gradient of the same
+    loss computed from whole output arenas."""
+    dev = cuda_device
+    members = _advance(_members(seed=2), dev, n=6)
+    ens = EnsembleStepper(members, dev)
+    rng = np.random.default_rng(8)
+    sel = torch.tensor(np.concatenate([ens.cm[k].q_off + rng.choice(m.q.size, 10, replace=False)
+                                       for k, m in enumerate(members)]), device=dev)
+    res = []
+    for use_sel in (False, True):
+        q0 = ens.qa.clone().requires_grad_(True)
+        theta = torch.stack([theta_of(m.params, dev) for m in members]).requires_grad_(True)
+        if use_sel:
+            o = ensemble_rollout_states(q0, theta, members, 9, [3, 9], select=sel)
+        else:
+            o = ensemble_rollout_states(q0, theta, members, 9, [3, 9])[:, sel]
+        (o ** 2).sum().backward()
+        res.append((o.detach(), q0.grad.clone(), theta.grad.clone()))
+    for a, b in zip(res[0], res[1]):
+        assert torch.equal(a, b)
