@@ -64,6 +64,34 @@ __device__ __forceinline__ void block_max_to(double v, unsigned long long* acc) 
 
 __device__ __forceinline__ void flag_status(dclaw_clock* clk, int code) { atomicCAS(&clk->status, 0, code); }
 
+// ---- tile activity flags ------------------------------------------------------
+// A tile is active in a step when a cell within distance 3 of it is wet after
+// b4step2 (the cells whose records the tile reads). k_records writes the
+// step's number into the flag of every tile a wet padded cell makes active;
+// a tile whose flag holds another number has only dry-dry interfaces and
+// dry cells, so the tile kernel skips it and src2 writes its cells' zeros.
+// Stale numbers from earlier runs can only mark a dry tile active, which
+// costs time and changes no result.
+__device__ __forceinline__ int fdiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+__device__ __forceinline__ void mark_tiles(uint32_t* __restrict__ tflag, uint32_t epoch, int i, int j, int TX, int TY,
+                                           int ntx, int nty) {
+    // tile t covers i0 = 1 + t TX .. i0 + TX - 1 and reads i0 - 3 .. i0 + TX + 2
+    int x0 = fdiv(i - TX - 3 + TX - 1, TX), x1 = fdiv(i + 2, TX);
+    int y0 = fdiv(j - TY - 3 + TY - 1, TY), y1 = fdiv(j + 2, TY);
+    if (x0 < 0) x0 = 0;
+    if (y0 < 0) y0 = 0;
+    if (x1 > ntx - 1) x1 = ntx - 1;
+    if (y1 > nty - 1) y1 = nty - 1;
+    for (int ty = y0; ty <= y1; ++ty)
+        for (int tx = x0; tx <= x1; ++tx) tflag[ty * ntx + tx] = epoch;
+}
+
+__device__ __forceinline__ bool tile_active(const uint32_t* __restrict__ tflag, uint32_t epoch, int i, int j, int TX,
+                                            int TY, int ntx) {
+    return !tflag || tflag[((j - 1) / TY) * ntx + (i - 1) / TX] == epoch;
+}
+
 // ---- fused step (interior layout) -----------------------------------------
 __global__ void __launch_bounds__(TPB) k_b4(dclaw_params P, Geom g, const double* __restrict__ q_in,
                                             const double* __restrict__ b, Work W, dclaw_clock* clk) {
@@ -177,12 +205,16 @@ __global__ void k_clock_init(dclaw_clock* clk, double t, double dt, double t_fin
 
 // ---- fused step: K1 cell records + K2 tiles --------------------------------
 __global__ void __launch_bounds__(TPB) k_records(dclaw_params P, Geom g, const double* __restrict__ q_in,
-                                                 const double* __restrict__ b, Rec R, dclaw_clock* clk) {
+                                                 const double* __restrict__ b, Rec R, dclaw_clock* clk,
+                                                 uint32_t* __restrict__ tflag) {
     const long long n = (long long)g.PX * g.PY;
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n) return;
     int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
     if (cell_record(P, g, q_in, b, R, i, j)) flag_status(clk, DCLAW_ERR_NAN);
+    if (tflag && R.get(R_H, pidx(g, i, j)) > 0.0)
+        mark_tiles(tflag, clk->nsteps + 1u, i, j, TILE_X, TILE_Y, (g.mx + TILE_X - 1) / TILE_X,
+                   (g.my + TILE_Y - 1) / TILE_Y);
 }
 
 __device__ __forceinline__ void tick_device(const dclaw_params& P, dclaw_clock* clk) {
@@ -218,7 +250,8 @@ __device__ __forceinline__ void last_block_tick(const dclaw_params& P, dclaw_clo
 template <int TX, int TY, bool WITH_SRC2, int NT>
 __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g, const Rec& R,
                                             const double* __restrict__ b, double* __restrict__ q_out, double dt,
-                                            int i0, int j0, double* smem, uint32_t* __restrict__ brlog, bool& nan) {
+                                            int i0, int j0, double* smem, uint32_t* __restrict__ brlog, bool& nan,
+                                            bool active = true) {
     using TG = TileGeom<TX, TY>;
     TileMem M;
     M.A = smem;
@@ -236,6 +269,21 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
     M.hj0 = j0 - 3;
     M.hw = TX + 6;
     const double dtdx = dt / g.dx, dtdy = dt / g.dy;
+    if (!active) {
+        // flagged inactive: with src2 in this kernel its cells' zeros are
+        // written here, otherwise src2's kernel writes them
+        nan = false;
+        if (WITH_SRC2) {
+            const size_t plane = (size_t)g.mx * g.my;
+            for (int it = tid; it < TX * TY; it += NT) {
+                int i = i0 + it % TX, j = j0 + it / TX;
+                if (i > g.mx || j > g.my) continue;
+                size_t c = (size_t)(j - 1) * g.mx + (size_t)(i - 1);
+                for (int m = 0; m < 5; ++m) q_out[(size_t)m * plane + c] = 0.0;
+            }
+        }
+        return 0.0;
+    }
     // stage h and bed of the cells within 3 of the tile; a tile whose cells
     // within distance 3 are all dry stays dry: all its interfaces are
     // dry-dry (skipped) and src2 zeroes dry cells
@@ -314,11 +362,12 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
 template <int TX, int TY, bool WITH_SRC2>
 __global__ void __launch_bounds__(TILE_TPB, DCLAW_TILE_MINBLOCKS) k_tile(dclaw_params P, Geom g, Rec R, const double* __restrict__ b,
                                                  double* __restrict__ q_out, dclaw_clock* clk,
-                                                 uint32_t* __restrict__ brlog) {
+                                                 uint32_t* __restrict__ brlog, const uint32_t* __restrict__ tflag) {
     extern __shared__ double smem[];
     const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
+    const bool active = !tflag || brlog || tflag[blockIdx.y * gridDim.x + blockIdx.x] == clk->nsteps + 1u;
     bool nan;
-    double cfl = tile_body<TX, TY, WITH_SRC2, TILE_TPB>(P, g, R, b, q_out, clk->dt, i0, j0, smem, brlog, nan);
+    double cfl = tile_body<TX, TY, WITH_SRC2, TILE_TPB>(P, g, R, b, q_out, clk->dt, i0, j0, smem, brlog, nan, active);
     if (nan) flag_status(clk, DCLAW_ERR_NAN);
     block_max_to(cfl, reinterpret_cast<unsigned long long*>(&clk->cfl_bits));
     if (WITH_SRC2) last_block_tick(P, clk);
@@ -327,10 +376,19 @@ __global__ void __launch_bounds__(TILE_TPB, DCLAW_TILE_MINBLOCKS) k_tile(dclaw_p
 // src2 of every interior cell from the updated state; the last block
 // applies the tick rule
 __global__ void __launch_bounds__(TPB) k_src2_cells(dclaw_params P, Geom g, const double* __restrict__ q_star,
-                                                    double* __restrict__ q_out, dclaw_clock* clk) {
+                                                    double* __restrict__ q_out, dclaw_clock* clk,
+                                                    const uint32_t* __restrict__ tflag) {
     const long long n = (long long)g.mx * g.my;
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx < n) cell_src2(P, g, clk->dt, q_star, q_out, (size_t)idx);
+    if (idx < n) {
+        const int i = (int)(idx % g.mx) + 1, j = (int)(idx / g.mx) + 1;
+        if (tile_active(tflag, clk->nsteps + 1u, i, j, TILE_X, TILE_Y, (g.mx + TILE_X - 1) / TILE_X)) {
+            cell_src2(P, g, clk->dt, q_star, q_out, (size_t)idx);
+        } else {
+            const size_t plane = (size_t)g.mx * g.my;
+            for (int m = 0; m < 5; ++m) q_out[(size_t)m * plane + (size_t)idx] = 0.0;
+        }
+    }
     last_block_tick(P, clk);
 }
 
@@ -361,33 +419,30 @@ __device__ __forceinline__ void load_member(const dclaw_member* __restrict__ mem
     }
 }
 
+// Every thread finds its chunk's member by binary search over the member
+// table (read through the cache; all threads of a block share the chunk, so
+// the search is uniform) and reads the member's entry and parameters in
+// place: no shared-memory broadcast and no barrier per chunk.
 __global__ void __launch_bounds__(TPB) k_records_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
                                                        const dclaw_params* __restrict__ prm, dclaw_clock* clocks,
                                                        const double* __restrict__ q_in, const double* __restrict__ b,
-                                                       double* __restrict__ work, unsigned int* counters) {
-    __shared__ dclaw_member sM;
-    __shared__ dclaw_params sP;
-    __shared__ int s_m;
+                                                       double* __restrict__ work, unsigned int* counters,
+                                                       uint32_t* __restrict__ tflag, int TX, int TY) {
     if (blockIdx.x == 0 && threadIdx.x == 0) counters[0] = 0u;  // the tile queue of this step
-    int cur = -1;
     for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-        if (threadIdx.x == 0) s_m = find_member(nmem, ch, [&](int k) { return mem[k].rchunk0; });
-        __syncthreads();
-        const int m = s_m;
-        if (m != cur) {
-            load_member(mem, prm, m, sM, sP);
-            __syncthreads();
-            cur = m;
-        }
-        const Geom g{sM.mx, sM.my, sM.mx + 4, sM.my + 4, sM.dx, sM.dy};
+        const int m = find_member(nmem, ch, [&](int k) { return mem[k].rchunk0; });
+        const dclaw_member& M = mem[m];
+        const Geom g{M.mx, M.my, M.mx + 4, M.my + 4, M.dx, M.dy};
         const size_t npad = (size_t)g.PX * g.PY;
-        const Rec R{work + sM.rec_off, npad};
-        const size_t idx = (size_t)(ch - sM.rchunk0) * TPB + threadIdx.x;
+        const Rec R{work + M.rec_off, npad};
+        const size_t idx = (size_t)(ch - M.rchunk0) * TPB + threadIdx.x;
         if (idx < npad) {
             int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
-            if (cell_record(sP, g, q_in + sM.q_off, b + sM.b_off, R, i, j)) flag_status(clocks + m, DCLAW_ERR_NAN);
+            if (cell_record(prm[m], g, q_in + M.q_off, b + M.b_off, R, i, j)) flag_status(clocks + m, DCLAW_ERR_NAN);
+            if (R.get(R_H, pidx(g, i, j)) > 0.0)
+                mark_tiles(tflag + M.tile0, clocks[m].nsteps + 1u, i, j, TX, TY, (int)M.ntiles_x,
+                           (int)(M.ntiles / M.ntiles_x));
         }
-        __syncthreads();
     }
 }
 
@@ -395,7 +450,7 @@ template <int TX, int TY>
 __global__ void __launch_bounds__(TPB, 2) k_tile_batch(int nmem, uint32_t ntiles, const dclaw_member* __restrict__ mem,
                                                        const dclaw_params* __restrict__ prm, dclaw_clock* clocks,
                                                        const double* __restrict__ b, double* __restrict__ work,
-                                                       unsigned int* counters) {
+                                                       unsigned int* counters, const uint32_t* __restrict__ tflag) {
     extern __shared__ double smem[];
     __shared__ dclaw_member sM;
     __shared__ dclaw_params sP;
@@ -412,6 +467,11 @@ __global__ void __launch_bounds__(TPB, 2) k_tile_batch(int nmem, uint32_t ntiles
         const unsigned int t = s_t;
         const int m = s_m;
         if (t >= ntiles) break;
+        // inactive tiles (no wet cell within 3): src2 writes their zeros
+        if (tflag[t] != clocks[m].nsteps + 1u) {
+            __syncthreads();
+            continue;
+        }
         if (m != cur) {
             load_member(mem, prm, m, sM, sP);
             __syncthreads();
@@ -442,38 +502,31 @@ __global__ void __launch_bounds__(TPB, 2) k_tile_batch(int nmem, uint32_t ntiles
 }
 
 __global__ void __launch_bounds__(TPB) k_src2_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
-                                                    const dclaw_params* __restrict__ prm, dclaw_clock* clocks,
-                                                    double* __restrict__ q_out, const double* __restrict__ work) {
-    __shared__ dclaw_member sM;
-    __shared__ dclaw_params sP;
-    __shared__ int s_m;
-    int cur = -1;
+                                                    const dclaw_params* __restrict__ prm, const dclaw_clock* clocks,
+                                                    double* __restrict__ q_out, const double* __restrict__ work,
+                                                    const uint32_t* __restrict__ tflag, int TX, int TY) {
     for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-        if (threadIdx.x == 0) s_m = find_member(nmem, ch, [&](int k) { return mem[k].schunk0; });
-        __syncthreads();
-        const int m = s_m;
-        if (m != cur) {
-            load_member(mem, prm, m, sM, sP);
-            __syncthreads();
-            cur = m;
-        }
-        const Geom g{sM.mx, sM.my, sM.mx + 4, sM.my + 4, sM.dx, sM.dy};
+        const int m = find_member(nmem, ch, [&](int k) { return mem[k].schunk0; });
+        const dclaw_member& M = mem[m];
+        const Geom g{M.mx, M.my, M.mx + 4, M.my + 4, M.dx, M.dy};
         const size_t n = (size_t)g.mx * g.my;
-        const size_t idx = (size_t)(ch - sM.schunk0) * TPB + threadIdx.x;
-        const double dt = clocks[m].dt;
-        if (idx < n) cell_src2(sP, g, dt, work + sM.qs_off, q_out + sM.q_off, idx);
-        // the last finished chunk of member m applies its tick
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            __threadfence();
-            unsigned int done = atomicAdd(&clocks[m].blocks_done, 1u);
-            if (done == sM.nschunks - 1) {
-                __threadfence();
-                tick_device(sP, clocks + m);
+        const size_t idx = (size_t)(ch - M.schunk0) * TPB + threadIdx.x;
+        if (idx < n) {
+            const int i = (int)(idx % g.mx) + 1, j = (int)(idx / g.mx) + 1;
+            if (tile_active(tflag + M.tile0, clocks[m].nsteps + 1u, i, j, TX, TY, (int)M.ntiles_x)) {
+                cell_src2(prm[m], g, clocks[m].dt, work + M.qs_off, q_out + M.q_off, idx);
+            } else {
+                for (int f = 0; f < 5; ++f) q_out[M.q_off + (size_t)f * n + idx] = 0.0;
             }
         }
-        __syncthreads();
     }
+}
+
+// every member's tick, after its src2
+__global__ void __launch_bounds__(TPB) k_tick_batch(int nmem, const dclaw_params* __restrict__ prm,
+                                                    dclaw_clock* clocks) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < nmem) tick_device(prm[m], clocks + m);
 }
 
 template <int TX, int TY>
@@ -492,12 +545,13 @@ inline int batch_tile_attr() {
 
 template <int TX, int TY>
 inline int launch_tile_batch(const dclaw_batch* B, const dclaw_member* mem, const dclaw_params* prm, dclaw_clock* clocks,
-                             const double* b, double* work, unsigned int* counters, int nsm, cudaStream_t s) {
+                             const double* b, double* work, unsigned int* counters, const uint32_t* tflag, int nsm,
+                             cudaStream_t s) {
     if (batch_tile_attr<TX, TY>() != DCLAW_OK) return DCLAW_ERR_CUDA;
     unsigned grid = (unsigned)(nsm * (B->tile_ctas_per_sm > 0 ? B->tile_ctas_per_sm : 2));
     if (grid > B->ntiles) grid = B->ntiles > 0 ? B->ntiles : 1;
     k_tile_batch<TX, TY><<<grid, TPB, TileGeom<TX, TY>::SMEM_BYTES, s>>>(B->nmembers, B->ntiles, mem, prm, clocks, b,
-                                                                        work, counters);
+                                                                        work, counters, tflag);
     return DCLAW_OK;
 }
 
@@ -629,7 +683,7 @@ inline unsigned nblocks(long long n) { return (unsigned)((n + TPB - 1) / TPB); }
 
 struct Layout : StagedLayout {
     size_t total_staged;
-    size_t off_rec, off_qstar, total_fused;
+    size_t off_rec, off_qstar, off_tflag, total_fused;
 };
 
 inline Layout layout(int mx, int my) {
@@ -639,7 +693,9 @@ inline Layout layout(int mx, int my) {
     // the fused step needs the cell records and the updated state before src2
     L.off_rec = 0;
     L.off_qstar = align256((size_t)NREC * L.npad * 8);
-    L.total_fused = L.off_qstar + align256((size_t)5 * mx * my * 8);
+    L.off_tflag = L.off_qstar + align256((size_t)5 * mx * my * 8);
+    const size_t ntiles = (size_t)((mx + TILE_X - 1) / TILE_X) * (size_t)((my + TILE_Y - 1) / TILE_Y);
+    L.total_fused = L.off_tflag + align256(ntiles * 4);
     L.total = L.total_staged > L.total_fused ? L.total_staged : L.total_fused;
     return L;
 }
@@ -779,14 +835,17 @@ int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int m
         size_t nlog = (size_t)(my + 2) * (mx + 1) + (size_t)(mx + 2) * (my + 1);
         cudaMemsetAsync(branch_log, 0, nlog * sizeof(uint32_t), s);
     }
-    k_records<<<nblocks((long long)L.npad), TPB, 0, s>>>(P, g, q_in, b, R, clock);
+    uint32_t* tflag = (uint32_t*)((char*)work + L.off_tflag);
+    k_records<<<nblocks((long long)L.npad), TPB, 0, s>>>(P, g, q_in, b, R, clock, tflag);
     dim3 grid((mx + TILE_X - 1) / TILE_X, (my + TILE_Y - 1) / TILE_Y);
     if (DCLAW_SRC2_KERNEL) {
         double* qstar = (double*)((char*)work + L.off_qstar);
-        k_tile<TILE_X, TILE_Y, false><<<grid, TILE_TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, qstar, clock, branch_log);
-        k_src2_cells<<<nblocks((long long)mx * my), TPB, 0, s>>>(P, g, qstar, q_out, clock);
+        k_tile<TILE_X, TILE_Y, false><<<grid, TILE_TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, qstar, clock, branch_log,
+                                                                             tflag);
+        k_src2_cells<<<nblocks((long long)mx * my), TPB, 0, s>>>(P, g, qstar, q_out, clock, tflag);
     } else {
-        k_tile<TILE_X, TILE_Y, true><<<grid, TILE_TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock, branch_log);
+        k_tile<TILE_X, TILE_Y, true><<<grid, TILE_TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock, branch_log,
+                                                                            tflag);
     }
     return cuda_status();
 }
@@ -912,10 +971,10 @@ int dclaw_step_noalloc(const double* q_in, double* q_out, const double* b, int m
     const size_t npad = (size_t)(mx + 4) * (my + 4);
     Rec R{g_noalloc_addr[dev], npad};
     const dclaw_params P = *p;
-    k_records<<<nblocks((long long)npad), TPB, 0, s>>>(P, g, q_in, b, R, clock);
+    k_records<<<nblocks((long long)npad), TPB, 0, s>>>(P, g, q_in, b, R, clock, nullptr);
     dim3 grid((mx + TILE_X - 1) / TILE_X, (my + TILE_Y - 1) / TILE_Y);
     k_tile<TILE_X, TILE_Y, true><<<grid, TILE_TPB, TileGeom<TILE_X, TILE_Y>::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock,
-                                                                                     nullptr);
+                                                                                     nullptr, nullptr);
     return cuda_status();
 }
 
@@ -979,7 +1038,8 @@ int dclaw_batch_layout(int n, const int32_t* mx, const int32_t* my, const double
     batch->nschunks = sch;
     batch->q_doubles = q;
     batch->b_doubles = bb;
-    batch->work_bytes = w * 8 + 256;  // + work-queue counters
+    // + the tile activity flags, then the work-queue counters
+    batch->work_bytes = w * 8 + align256((size_t)tiles * 4) + 256;
     return DCLAW_OK;
 }
 
@@ -1001,20 +1061,24 @@ int dclaw_step_batched(const dclaw_batch* batch, const dclaw_member* members, co
     if (nsm <= 0) return DCLAW_ERR_CUDA;
     double* w = (double*)work;
     unsigned int* counters = (unsigned int*)((char*)work + (batch->work_bytes - 256));
+    uint32_t* tflag = (uint32_t*)((char*)work + (batch->work_bytes - 256 - align256((size_t)batch->ntiles * 4)));
     const int cpsm = batch->cell_ctas_per_sm > 0 ? batch->cell_ctas_per_sm : 8;
+    const int TX = batch_tx(batch->tile_shape), TY = batch_ty(batch->tile_shape);
     unsigned g1 = (unsigned)(nsm * cpsm);
     if (g1 > batch->nrchunks) g1 = batch->nrchunks;
-    k_records_batch<<<g1, TPB, 0, s>>>(batch->nmembers, batch->nrchunks, members, params, clocks, q_in, b, w, counters);
+    k_records_batch<<<g1, TPB, 0, s>>>(batch->nmembers, batch->nrchunks, members, params, clocks, q_in, b, w, counters,
+                                       tflag, TX, TY);
     int rc = DCLAW_OK;
     switch (batch->tile_shape) {
-        case 0: rc = launch_tile_batch<batch_tx(0), batch_ty(0)>(batch, members, params, clocks, b, w, counters, nsm, s); break;
-        case 1: rc = launch_tile_batch<batch_tx(1), batch_ty(1)>(batch, members, params, clocks, b, w, counters, nsm, s); break;
-        default: rc = launch_tile_batch<batch_tx(2), batch_ty(2)>(batch, members, params, clocks, b, w, counters, nsm, s); break;
+        case 0: rc = launch_tile_batch<batch_tx(0), batch_ty(0)>(batch, members, params, clocks, b, w, counters, tflag, nsm, s); break;
+        case 1: rc = launch_tile_batch<batch_tx(1), batch_ty(1)>(batch, members, params, clocks, b, w, counters, tflag, nsm, s); break;
+        default: rc = launch_tile_batch<batch_tx(2), batch_ty(2)>(batch, members, params, clocks, b, w, counters, tflag, nsm, s); break;
     }
     if (rc != DCLAW_OK) return rc;
     unsigned g3 = (unsigned)(nsm * cpsm);
     if (g3 > batch->nschunks) g3 = batch->nschunks;
-    k_src2_batch<<<g3, TPB, 0, s>>>(batch->nmembers, batch->nschunks, members, params, clocks, q_out, w);
+    k_src2_batch<<<g3, TPB, 0, s>>>(batch->nmembers, batch->nschunks, members, params, clocks, q_out, w, tflag, TX, TY);
+    k_tick_batch<<<(unsigned)((batch->nmembers + TPB - 1) / TPB), TPB, 0, s>>>(batch->nmembers, params, clocks);
     return cuda_status();
 }
 

@@ -188,9 +188,10 @@ size_t dclaw_step_noalloc_max_cells(void);
  * reference's differentiable port: one simulation per particle,
  * gradient_particle_filter/pf_flume/flume_model.py:129-179, vmapped in
  * pf_flume/inference.py:96-108). All members advance together: one step of
- * the ensemble is three launches of persistent kernels (cell records, a
- * dynamic work queue over every member's tiles, src2 + each member's tick),
- * so a sequence of ensemble steps captures into one CUDA graph.
+ * the ensemble is four launches (cell records, a persistent kernel pulling
+ * every member's tiles from one work queue, src2, each member's tick), so a
+ * sequence of ensemble steps captures into one CUDA graph. Tiles with no wet
+ * cell within 3 cells are skipped (src2 writes their zeros).
  * Member m's state is 5 planes [5][my][mx] at q_off in the state arenas; its
  * bed is [my][mx] at b_off in the bed arena. */
 typedef struct dclaw_member {
