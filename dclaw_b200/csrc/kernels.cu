@@ -39,6 +39,10 @@ constexpr int MAX_DEVICES = 64;
 #define DCLAW_SRC2_KERNEL 1
 #endif
 constexpr int TILE_X = DCLAW_TILE_X, TILE_Y = DCLAW_TILE_Y;
+// resident blocks per SM the per-cell kernels (records, src2) are sized for
+#ifndef DCLAW_CELL_MINB
+#define DCLAW_CELL_MINB 4
+#endif
 
 __device__ __forceinline__ double warp_max(double v) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -204,7 +208,7 @@ __global__ void k_clock_init(dclaw_clock* clk, double t, double dt, double t_fin
 }
 
 // ---- fused step: K1 cell records + K2 tiles --------------------------------
-__global__ void __launch_bounds__(TPB) k_records(dclaw_params P, Geom g, const double* __restrict__ q_in,
+__global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_records(dclaw_params P, Geom g, const double* __restrict__ q_in,
                                                  const double* __restrict__ b, Rec R, dclaw_clock* clk,
                                                  uint32_t* __restrict__ tflag) {
     const long long n = (long long)g.PX * g.PY;
@@ -375,7 +379,7 @@ __global__ void __launch_bounds__(TILE_TPB, DCLAW_TILE_MINBLOCKS) k_tile(dclaw_p
 
 // src2 of every interior cell from the updated state; the last block
 // applies the tick rule
-__global__ void __launch_bounds__(TPB) k_src2_cells(dclaw_params P, Geom g, const double* __restrict__ q_star,
+__global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_src2_cells(dclaw_params P, Geom g, const double* __restrict__ q_star,
                                                     double* __restrict__ q_out, dclaw_clock* clk,
                                                     const uint32_t* __restrict__ tflag) {
     const long long n = (long long)g.mx * g.my;
@@ -423,7 +427,7 @@ __device__ __forceinline__ void load_member(const dclaw_member* __restrict__ mem
 // table (read through the cache; all threads of a block share the chunk, so
 // the search is uniform) and reads the member's entry and parameters in
 // place: no shared-memory broadcast and no barrier per chunk.
-__global__ void __launch_bounds__(TPB) k_records_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
+__global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_records_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
                                                        const dclaw_params* __restrict__ prm, dclaw_clock* clocks,
                                                        const double* __restrict__ q_in, const double* __restrict__ b,
                                                        double* __restrict__ work, unsigned int* counters,
@@ -501,7 +505,7 @@ __global__ void __launch_bounds__(TPB, 2) k_tile_batch(int nmem, uint32_t ntiles
     }
 }
 
-__global__ void __launch_bounds__(TPB) k_src2_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
+__global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_src2_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
                                                     const dclaw_params* __restrict__ prm, const dclaw_clock* clocks,
                                                     double* __restrict__ q_out, const double* __restrict__ work,
                                                     const uint32_t* __restrict__ tflag, int TX, int TY) {
