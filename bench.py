@@ -41,6 +41,11 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 BYTES_PER_CELL_UPDATE = 88  # read 5 state + 1 bed, write 5 state (FP64)
+# DRAM bytes (read + write) of one fused step measured by ncu on the 2048 x 2048
+# random-field case: k_records 357.4 MB + k_tile 170.1 MB + k_src2_cells 157.4 MB;
+# the case keeps its wet fraction at every size, so the bytes scale with the cell
+# count
+NCU_STEP_BYTES_2048 = 684.9e6
 METRIC = "cell-updates/sec on 1 B200 (plain vs batched); gradient/forward time ratio"
 
 
@@ -529,7 +534,8 @@ def run_ours(args):
                           "l2": "state 672 MB > L2, no flush", "order": case.params.order,
                           "transverse_waves": case.params.transverse_waves, "limiter": "MC"},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                            "frac": achieved / peak, "traffic": None,
+                            "frac": achieved / peak, "traffic": NCU_STEP_BYTES_2048 * cells / 2048 ** 2,
+                            "traffic_note": "bytes per step from the ncu capture at 2048^2, scaled by cells",
                             "kernel": "fused step k_records + k_tile + k_src2_cells (88 B/cell-update algorithmic)",
                             "peak_source": peak_kind},
                "clocks": clocks, "gpu_launches": 3 * args.steps, "status": status}
