@@ -213,6 +213,28 @@ def cfl_dt(q: torch.Tensor, p, grid: Grid, cfl: float) -> torch.Tensor:
     return cfl * min(grid.dx, grid.dy) / torch.clamp(smax, min=1.0e-6)
 
 
+def gate_bed(b_base: torch.Tensor, gate_shape: torch.Tensor, gate_t, gate_deg):
+    """Moving bed of a headgate release, as the port builds it
+    (differentiable_dclaw/dclaw_jax/solver.py:304-322): the closed gate is a
+    ridge `gate_shape` on top of `b_base`, lowered to cos(angle(t)) of its
+    height as the gate swings open, angle piecewise linear through
+    (gate_t, gate_deg) and held at the end values outside them. Returns
+    b(t) for `rollout` / `rollout_peak`; t may be a device tensor, so the bed
+    is rebuilt on the device without a host round trip."""
+    gt = torch.as_tensor(gate_t, dtype=torch.float64, device=b_base.device)
+    gd = torch.as_tensor(gate_deg, dtype=torch.float64, device=b_base.device)
+
+    def bed(t):
+        t = torch.as_tensor(t, dtype=torch.float64, device=b_base.device).reshape(1)
+        k = torch.clamp(torch.searchsorted(gt, t, right=True), 1, len(gt) - 1)
+        t0, t1, a0, a1 = gt[k - 1], gt[k], gd[k - 1], gd[k]
+        w = torch.clamp((t - t0) / (t1 - t0), 0.0, 1.0)
+        angle = torch.where(t <= gt[0], gd[0], torch.where(t >= gt[-1], gd[-1], a0 + w * (a1 - a0)))
+        return b_base + torch.cos(angle * (math.pi / 180.0)) * gate_shape
+
+    return bed
+
+
 def rollout(q0: torch.Tensor, b, p, grid: Grid, t_final: float, cfl: float = 0.4, bc_x: str = "wall",
             bc_y: str = "wall", n_steps: int = 2000, keep_states: bool = True):
     """Advance towards t_final over a fixed number of steps.
@@ -221,17 +243,21 @@ def rollout(q0: torch.Tensor, b, p, grid: Grid, t_final: float, cfl: float = 0.4
     rule (dt * cfl / Courant number of the last step, tick.f:490-526) and is
     clipped so that t never passes t_final (dt = 0 afterwards). Returns
     (q_final, t_reached, states, times) like the port; with keep_states=False
-    states/times are None.
+    states/times are None. `b` may be a function of t (a moving bed, e.g.
+    `gate_bed`): it is evaluated at the start of each step on the device and
+    h is left as it is when the bed moves, as GeoClaw does.
     """
-    if callable(b):
-        raise NotImplementedError("moving beds are not supported by the fused step")
+    moving = callable(b)
     prm = to_dclaw_params(p, bc_x, bc_y, cfl)
-    st = PatchStepper(_to_native(q0), _bed(b), prm, grid.dx, grid.dy)
+    st = PatchStepper(_to_native(q0), _bed(b, torch.zeros((), dtype=torch.float64, device=q0.device)), prm, grid.dx,
+                      grid.dy)
     dt0 = float(cfl_dt(q0, prm, grid, cfl))
     st.init_clock(dt0, t_final=float(t_final))
     states = torch.empty((n_steps,) + tuple(q0.shape), dtype=q0.dtype, device=q0.device) if keep_states else None
     hist = torch.empty((n_steps, 4), dtype=torch.float64, device=q0.device)
     for n in range(n_steps):
+        if moving:
+            st.b.copy_(b(st.clock[0]).t())
         st.step(1, history=hist[n:n + 1])
         if keep_states:
             states[n].copy_(st.state().permute(0, 2, 1))
@@ -246,11 +272,15 @@ def rollout_peak(q0: torch.Tensor, b, p, grid: Grid, t_final: float, cfl: float 
     Returns (q_final, t_reached, h_peak)."""
     if checkpoint_block is not None and n_steps % checkpoint_block:
         raise ValueError("n_steps must be a multiple of checkpoint_block")
+    moving = callable(b)
     prm = to_dclaw_params(p, bc_x, bc_y, cfl)
-    st = PatchStepper(_to_native(q0), _bed(b), prm, grid.dx, grid.dy)
+    st = PatchStepper(_to_native(q0), _bed(b, torch.zeros((), dtype=torch.float64, device=q0.device)), prm, grid.dx,
+                      grid.dy)
     st.init_clock(float(cfl_dt(q0, prm, grid, cfl)), t_final=float(t_final))
     hmax = st.state()[0].clone()
     for _ in range(n_steps):
+        if moving:
+            st.b.copy_(b(st.clock[0]).t())
         st.step(1)
         torch.maximum(hmax, st.state()[0], out=hmax)
     _lib.check(st.status(), "rollout_peak")
@@ -258,5 +288,5 @@ def rollout_peak(q0: torch.Tensor, b, p, grid: Grid, t_final: float, cfl: float 
     return _from_native(st.state()), t, hmax.t().contiguous()
 
 
-__all__ = ["Grid", "MaterialParams", "PatchStepper", "make_state", "step", "cfl_dt", "rollout", "rollout_peak",
+__all__ = ["Grid", "MaterialParams", "PatchStepper", "make_state", "step", "cfl_dt", "rollout", "rollout_peak", "gate_bed",
            "to_dclaw_params", "max_wave_speed"]
