@@ -146,7 +146,9 @@ class ClockSampler:
 def make_case(args, rank=0):
     from dclaw_b200 import workloads as W
 
-    return W.random_field_case(n=args.size, dx=args.dx, seed=args.seed + rank)
+    from dclaw_b200.replicas import replica_seed
+
+    return W.random_field_case(n=args.size, dx=args.dx, seed=replica_seed(args.seed, rank))
 
 
 def cpu_baseline(args, case, steps):
@@ -460,7 +462,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
-    from dclaw_b200 import _lib
+    from dclaw_b200.replicas import max_over_ranks
     from dclaw_b200.solver import PatchStepper
 
     case = make_case(args, rank)
@@ -489,11 +491,7 @@ def run_ours(args):
     e1.record(stream)
     barrier()
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1)
-    ms_t = torch.tensor([ms], device=dev)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms = float(ms_t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), dev)
     status = st.status()
     value = cells * args.steps * world / (ms / 1000.0)
 
@@ -514,11 +512,7 @@ def run_ours(args):
             cfl_h.copy_(st.clock, non_blocking=True)     # Courant number and next dt
         f1.record(stream)
         barrier()
-        e2e_ms = f0.elapsed_time(f1)
-        e_t = torch.tensor([e2e_ms], device=dev)
-        if world > 1:
-            dist.all_reduce(e_t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(e_t.item())
+        e2e_ms = max_over_ranks(f0.elapsed_time(f1), dev)
         h2d = qh.numel() * 8
         d2h = qh.numel() * 8 + cfl_h.numel() * 8
 
