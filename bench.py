@@ -343,7 +343,7 @@ def gradient_bench(args, dev):
             "grad": {"phi_deg": float(theta.grad[0]), "kref": float(theta.grad[1]), "m0": float(m0.grad),
                      "alpha_c": float(theta.grad[2]), "h0_l2": float(h.grad.norm())},
             "peak_mem_gb": torch.cuda.max_memory_allocated(dev) / 1e9,
-            "gpu_launches": {"adjoint_per_step": 16, "recompute_per_step": 3, "forward_per_step": 3},
+            "gpu_launches": {"adjoint_per_step": 17, "recompute_per_step": 3, "forward_per_step": 3},
             "note": "dt of each step chosen by the tick rule in the forward pass and replayed, not differentiated"}
 
 
@@ -448,7 +448,7 @@ def batched_gradient_bench(args, dev):
             "grad_member0": {"phi_deg": float(theta.grad[0, 0]), "kref": float(theta.grad[0, 1]),
                              "alpha_c": float(theta.grad[0, 2]), "mu": float(theta.grad[0, 3]),
                              "m0": float(m0.grad[0]), "block_volume": float(H.grad[0] / area[0])},
-            "gpu_launches": {"adjoint_per_step": 16, "recompute_per_step": 3, "forward_per_step": 3},
+            "gpu_launches": {"adjoint_per_step": 18, "recompute_per_step": 4, "forward_per_step": 4},
             "note": "every member's dt from its own tick rule, recorded and replayed, not differentiated"}
 
 

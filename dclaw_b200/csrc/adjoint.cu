@@ -6,8 +6,10 @@
 // (dS/dtheta)^T lam_out to the adjoints of the material parameters
 // theta = (phi [rad], kref, alpha_c, mu). The step's dt is data.
 //
-// One call is 16 data-parallel launches:
-//   forward recompute  b4step2, calc_taudir, setvars records of the rpn2
+// One call is 17 data-parallel launches and 3 memsets (the batched form: 18
+// launches, one of them zeroing):
+//   forward recompute  b4step2, the activity map of 16 x 16 blocks (a wet
+//                      cell within 4), calc_taudir, setvars records of the rpn2
 //                      states (tau and its partial derivatives, once per
 //                      cell state instead of once per interface side),
 //                      x/y solves, x/y fluxes
@@ -15,7 +17,9 @@
 //                      step, so every branch is the one the forward took)
 //   reverse            src2+update, x/y fluxes, x/y solves, calc_taudir,
 //                      b4step2, ghost gather, parameter sum
-// Every reverse stage gathers what later stages wrote (no atomics), and the
+// Reverse items in inactive blocks are skipped (their outputs are zeros or
+// unread; the reverse planes are zeroed first). Every reverse stage gathers
+// what later stages wrote (no atomics), and the
 // parameter adjoints are summed per block and then across blocks in a fixed
 // order, so results are bit-reproducible run to run.
 #include <cuda_runtime.h>
@@ -33,6 +37,10 @@ namespace adj {
 // resident blocks per SM the heavy reverse kernels' registers are sized for
 #ifndef DCLAW_ADJ_MINB
 #define DCLAW_ADJ_MINB 4
+#endif
+// resident blocks per SM the forward-recompute and light reverse kernels are sized for
+#ifndef DCLAW_ADJ_LIGHT_MINB
+#define DCLAW_ADJ_LIGHT_MINB 1
 #endif
 constexpr int ATPB = DCLAW_ADJ_TPB;
 constexpr int NWARP = ATPB / 32;
@@ -63,7 +71,7 @@ __device__ __forceinline__ void block_pbar(const double* pb, double* __restrict_
 }
 
 // ---- forward recompute (the staged step's stages A-D) ---------------------
-__global__ void __launch_bounds__(ATPB) k_fw_b4(dclaw_params P, Geom g, const double* __restrict__ q_in,
+__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_fw_b4(dclaw_params P, Geom g, const double* __restrict__ q_in,
                                                 const double* __restrict__ b, Work W, int32_t* status) {
     const long long n = (long long)g.PX * g.PY;
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -72,7 +80,30 @@ __global__ void __launch_bounds__(ATPB) k_fw_b4(dclaw_params P, Geom g, const do
     if (stage_b4(P, g, q_in, b, W, i, j)) flag(status, DCLAW_ERR_NAN);
 }
 
-__global__ void __launch_bounds__(ATPB) k_fw_taudir(dclaw_params P, Geom g, Work W) {
+// blocks of padded cells within ACT_REACH of a wet padded cell (act zeroed before)
+__device__ __forceinline__ void mark_active(const dclaw_params& P, const Geom& g, const Work& W, uint32_t* act,
+                                            int act_nx, int i, int j) {
+    if (!(W.qB[pidx(g, i, j)] > P.dry_tolerance)) return;
+    const int px = i + 1, py = j + 1;
+    const int act_ny = (g.PY + ACT_TILE - 1) / ACT_TILE;
+    int x0 = (px - ACT_REACH) / ACT_TILE, x1 = (px + ACT_REACH) / ACT_TILE;
+    int y0 = (py - ACT_REACH) / ACT_TILE, y1 = (py + ACT_REACH) / ACT_TILE;
+    if (px - ACT_REACH < 0) x0 = 0;
+    if (py - ACT_REACH < 0) y0 = 0;
+    if (x1 > act_nx - 1) x1 = act_nx - 1;
+    if (y1 > act_ny - 1) y1 = act_ny - 1;
+    for (int y = y0; y <= y1; ++y)
+        for (int x = x0; x <= x1; ++x) act[y * act_nx + x] = 1u;
+}
+
+__global__ void __launch_bounds__(ATPB) k_fw_mark(dclaw_params P, Geom g, Work W, uint32_t* act, int act_nx) {
+    const long long n = (long long)g.PX * g.PY;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    mark_active(P, g, W, act, act_nx, (int)(idx % g.PX) - 1, (int)(idx / g.PX) - 1);
+}
+
+__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_fw_taudir(dclaw_params P, Geom g, Work W) {
     const long long n = (long long)g.PX * g.PY;
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n) return;
@@ -82,7 +113,7 @@ __global__ void __launch_bounds__(ATPB) k_fw_taudir(dclaw_params P, Geom g, Work
 
 // DIR 0: rows r = 0..my+1, interfaces i = 0..mx+2; DIR 1: interfaces
 // k = 0..my+2, columns c = 0..mx+1 (the fast index is along x)
-__global__ void __launch_bounds__(ATPB) k_fw_svrec(dclaw_params P, Geom g, Work W, AdjWork A) {
+__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_fw_svrec(dclaw_params P, Geom g, Work W, AdjWork A) {
     const long long n = (long long)g.PX * g.PY;
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n) return;
@@ -91,7 +122,7 @@ __global__ void __launch_bounds__(ATPB) k_fw_svrec(dclaw_params P, Geom g, Work 
 }
 
 template <int DIR>
-__global__ void __launch_bounds__(ATPB) k_fw_riemann(dclaw_params P, Geom g, Work W, const double* __restrict__ sv) {
+__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_fw_riemann(dclaw_params P, Geom g, Work W, const double* __restrict__ sv) {
     const int nfast = DIR == 0 ? g.mx + 3 : g.mx + 2;
     const int nslow = DIR == 0 ? g.my + 2 : g.my + 3;
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -103,7 +134,7 @@ __global__ void __launch_bounds__(ATPB) k_fw_riemann(dclaw_params P, Geom g, Wor
 
 // DIR 0: rows 0..my+1, interfaces 1..mx+1; DIR 1: interfaces 1..my+1, columns 0..mx+1
 template <int DIR>
-__global__ void __launch_bounds__(ATPB) k_fw_flux(dclaw_params P, Geom g, Work W, const double* __restrict__ dtp) {
+__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_fw_flux(dclaw_params P, Geom g, Work W, const double* __restrict__ dtp) {
     const int nfast = DIR == 0 ? g.mx + 1 : g.mx + 2;
     const int nslow = DIR == 0 ? g.my + 2 : g.my + 1;
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -123,7 +154,7 @@ __global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_rv_src2(dclaw_params P
     double pb[NPB] = {0.0, 0.0, 0.0, 0.0};
     if (idx < n) {
         int i = (int)(idx % g.mx) + 1, j = (int)(idx / g.mx) + 1;
-        adj_item_src2(P, g, W, A, lam_out, i, j, *dtp, pb);
+        if (adj_active(A, i, j)) adj_item_src2(P, g, W, A, lam_out, i, j, *dtp, pb);
     }
     block_pbar(pb, part + (size_t)blockIdx.x * NPB);
 }
@@ -137,7 +168,7 @@ __global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_rv_flux(dclaw_params P
     if (idx >= (long long)nfast * nslow) return;
     int a = (int)(idx % nfast), s = (int)(idx / nfast);
     int r = DIR == 0 ? s : a, i = DIR == 0 ? a + 1 : s + 1;
-    adj_item_flux<DIR>(P, g, W, A, r, i, *dtp);
+    if (adj_active(A, DIR == 0 ? i : r, DIR == 0 ? r : i)) adj_item_flux<DIR>(P, g, W, A, r, i, *dtp);
 }
 
 template <int DIR>
@@ -150,39 +181,40 @@ __global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_rv_riemann(dclaw_param
     if (idx < (long long)nfast * nslow) {
         int a = (int)(idx % nfast), s = (int)(idx / nfast);
         int r = DIR == 0 ? s : a, i = DIR == 0 ? a : s;
-        if (!adj_item_riemann<DIR>(P, g, W, A, r, i, pb)) flag(status, DCLAW_ERR_UNSUPPORTED);
+        if (adj_active(A, DIR == 0 ? i : r, DIR == 0 ? r : i) && !adj_item_riemann<DIR>(P, g, W, A, r, i, pb))
+            flag(status, DCLAW_ERR_UNSUPPORTED);
     }
     block_pbar(pb, part + (size_t)blockIdx.x * NPB);
 }
 
-__global__ void __launch_bounds__(ATPB) k_rv_taudir(dclaw_params P, Geom g, Work W, AdjWork A,
+__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_rv_taudir(dclaw_params P, Geom g, Work W, AdjWork A,
                                                     double* __restrict__ part) {
     const long long n = (long long)g.PX * g.PY;
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double pb[NPB] = {0.0, 0.0, 0.0, 0.0};
     if (idx < n) {
         int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
-        adj_item_taudir(P, g, W, A, i, j, pb);
+        if (adj_active(A, i, j)) adj_item_taudir(P, g, W, A, i, j, pb);
     }
     block_pbar(pb, part + (size_t)blockIdx.x * NPB);
 }
 
-__global__ void __launch_bounds__(ATPB) k_rv_b4(dclaw_params P, Geom g, Work W, AdjWork A,
+__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_rv_b4(dclaw_params P, Geom g, Work W, AdjWork A,
                                                 const double* __restrict__ q_in) {
     const long long n = (long long)g.PX * g.PY;
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n) return;
     int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
-    adj_item_b4(P, g, W, A, q_in, i, j);
+    if (adj_active(A, i, j)) adj_item_b4(P, g, W, A, q_in, i, j);
 }
 
-__global__ void __launch_bounds__(ATPB) k_rv_gather(dclaw_params P, Geom g, Work W, AdjWork A,
+__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_rv_gather(dclaw_params P, Geom g, Work W, AdjWork A,
                                                     double* __restrict__ lam_in) {
     const long long n = (long long)g.mx * g.my;
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n) return;
     int i = (int)(idx % g.mx) + 1, j = (int)(idx / g.mx) + 1;
-    adj_item_gather(P, g, A, W, lam_in, i, j);
+    if (adj_active(A, i, j)) adj_item_gather(P, g, A, W, lam_in, i, j);
 }
 
 // pbar[k] += sum over the nb block partials, in block order (one block)
@@ -204,7 +236,8 @@ __global__ void __launch_bounds__(ATPB) k_rv_pbar(const double* __restrict__ par
 
 struct AdjLayout {
     StagedLayout S;
-    size_t off_lamq, off_xfb, off_yfb, off_xcb, off_ycb, off_tdq, off_qsb, off_sv, off_part;
+    size_t off_lamq, off_xfb, off_yfb, off_xcb, off_ycb, off_tdq, off_qsb, off_sv, off_part, off_act;
+    int act_nx, act_ny;
     long long nb_src2, nb_rx, nb_ry, nb_td, nparts;
     size_t total;
 };
@@ -227,6 +260,9 @@ __host__ __device__ inline AdjLayout adj_layout(int mx, int my) {
     L.off_qsb = o; o += align256((size_t)5 * L.S.npad * 8);
     L.off_sv = o; o += align256((size_t)NSV * L.S.npad * 8);
     L.off_part = o; o += align256((size_t)L.nparts * NPB * 8);
+    L.act_nx = (mx + 4 + ACT_TILE - 1) / ACT_TILE;
+    L.act_ny = (my + 4 + ACT_TILE - 1) / ACT_TILE;
+    L.off_act = o; o += align256((size_t)L.act_nx * L.act_ny * 4);
     L.total = o;
     return L;
 }
@@ -238,7 +274,7 @@ inline bool adj_sizes_ok(int mx, int my) {
 // ---- ensembles: the same stages over the chunks of every member -------------
 enum { SP_PAD = 0, SP_INT, SP_RX, SP_RY, SP_FX, SP_FY, NSPACE };
 enum {
-    OP_FW_B4, OP_FW_TAUDIR, OP_FW_SVREC, OP_FW_RX, OP_FW_RY, OP_FW_FX, OP_FW_FY,
+    OP_FW_B4, OP_FW_MARK, OP_FW_TAUDIR, OP_FW_SVREC, OP_FW_RX, OP_FW_RY, OP_FW_FX, OP_FW_FY,
     OP_RV_SRC2, OP_RV_FX, OP_RV_FY, OP_RV_RX, OP_RV_RY, OP_RV_TAUDIR, OP_RV_B4, OP_RV_GATHER
 };
 
@@ -251,6 +287,7 @@ struct OpTraits;
         static constexpr bool PBAR = pb;    \
     };
 DC_OP(OP_FW_B4, SP_PAD, false)
+DC_OP(OP_FW_MARK, SP_PAD, false)
 DC_OP(OP_FW_TAUDIR, SP_PAD, false)
 DC_OP(OP_FW_SVREC, SP_PAD, false)
 DC_OP(OP_FW_RX, SP_RX, false)
@@ -326,9 +363,10 @@ __global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_adj_batch(BatchArgs a,
         const AdjLayout L = adj_layout(mx, my);
         char* base = a.work + sM.work_off;
         const Work W = make_work(base, L.S);
+        uint32_t* act = (uint32_t*)(base + L.off_act);
         const AdjWork A{(double*)(base + L.off_lamq), (double*)(base + L.off_xfb), (double*)(base + L.off_yfb),
                         (double*)(base + L.off_xcb), (double*)(base + L.off_ycb), (double*)(base + L.off_tdq),
-                        (double*)(base + L.off_qsb), (double*)(base + L.off_sv)};
+                        (double*)(base + L.off_qsb), (double*)(base + L.off_sv), act, L.act_nx};
         const uint32_t lch = ch - sM.chunk0[SP];
         const long long idx = (long long)lch * ATPB + threadIdx.x;
         const double* q_in = a.q + sM.q_off;
@@ -339,19 +377,23 @@ __global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_adj_batch(BatchArgs a,
                 const int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
                 if (OP == OP_FW_B4) {
                     if (stage_b4(sP, g, q_in, a.b + sM.b_off, W, i, j) && a.status) atomicCAS(a.status + m, 0, DCLAW_ERR_NAN);
+                } else if (OP == OP_FW_MARK) {
+                    mark_active(sP, g, W, act, L.act_nx, i, j);
                 } else if (OP == OP_FW_TAUDIR) {
                     stage_taudir(sP, g, W, i, j);
                 } else if (OP == OP_FW_SVREC) {
                     adj_item_svrec(sP, g, W, A, i, j);
                 } else if (OP == OP_RV_TAUDIR) {
-                    adj_item_taudir(sP, g, W, A, i, j, pb);
+                    if (adj_active(A, i, j)) adj_item_taudir(sP, g, W, A, i, j, pb);
                 } else if (OP == OP_RV_B4) {
-                    adj_item_b4(sP, g, W, A, q_in, i, j);
+                    if (adj_active(A, i, j)) adj_item_b4(sP, g, W, A, q_in, i, j);
                 }
             } else if (SP == SP_INT) {
                 const int i = (int)(idx % mx) + 1, j = (int)(idx / mx) + 1;
-                if (OP == OP_RV_SRC2) adj_item_src2(sP, g, W, A, a.lam_out + sM.q_off, i, j, dt, pb);
-                else if (OP == OP_RV_GATHER) adj_item_gather(sP, g, A, W, a.lam_in + sM.q_off, i, j);
+                if (adj_active(A, i, j)) {
+                    if (OP == OP_RV_SRC2) adj_item_src2(sP, g, W, A, a.lam_out + sM.q_off, i, j, dt, pb);
+                    else if (OP == OP_RV_GATHER) adj_item_gather(sP, g, A, W, a.lam_in + sM.q_off, i, j);
+                }
             } else if (SP == SP_RX || SP == SP_RY) {
                 const int nfast = SP == SP_RX ? mx + 3 : mx + 2;
                 const int af = (int)(idx % nfast), as = (int)(idx / nfast);
@@ -359,7 +401,7 @@ __global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_adj_batch(BatchArgs a,
                 constexpr int DIR = SP == SP_RX ? 0 : 1;
                 if (OP == OP_FW_RX || OP == OP_FW_RY) {
                     stage_riemann<DIR>(sP, g, W, r, i, nullptr, A.sv);
-                } else {
+                } else if (adj_active(A, DIR == 0 ? i : r, DIR == 0 ? r : i)) {
                     if (!adj_item_riemann<DIR>(sP, g, W, A, r, i, pb) && a.status)
                         atomicCAS(a.status + m, 0, DCLAW_ERR_UNSUPPORTED);
                 }
@@ -369,7 +411,7 @@ __global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_adj_batch(BatchArgs a,
                 const int r = SP == SP_FX ? as : af, i = SP == SP_FX ? af + 1 : as + 1;
                 constexpr int DIR = SP == SP_FX ? 0 : 1;
                 if (OP == OP_FW_FX || OP == OP_FW_FY) stage_flux<DIR>(sP, g, W, r, i, DIR == 0 ? dt / g.dx : dt / g.dy, nullptr);
-                else adj_item_flux<DIR>(sP, g, W, A, r, i, dt);
+                else if (adj_active(A, DIR == 0 ? i : r, DIR == 0 ? r : i)) adj_item_flux<DIR>(sP, g, W, A, r, i, dt);
             }
         }
         if (OpTraits<OP>::PBAR) {
@@ -383,6 +425,19 @@ __global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_adj_batch(BatchArgs a,
         }
         __syncthreads();
     }
+}
+
+// zero member m's reverse planes, block partials, activity map and lam_in
+// (blockIdx.y = m)
+__global__ void __launch_bounds__(256) k_adj_batch_zero(BatchArgs a) {
+    const dclaw_adj_member M = a.mem[blockIdx.y];
+    const AdjLayout L = adj_layout(M.mx, M.my);
+    char* base = a.work + M.work_off;
+    double* p3[3] = {(double*)(base + L.off_lamq), (double*)(base + L.off_part), a.lam_in + M.q_off};
+    const size_t n3[3] = {(L.off_sv - L.off_lamq) / 8, (L.total - L.off_part) / 8, (size_t)5 * M.mx * M.my};
+    for (int k = 0; k < 3; ++k)
+        for (size_t x = (size_t)blockIdx.x * blockDim.x + threadIdx.x; x < n3[k]; x += (size_t)gridDim.x * blockDim.x)
+            p3[k][x] = 0.0;
 }
 
 // pbar[4 m + k] += member m's partials, summed as k_rv_pbar sums them
@@ -443,14 +498,21 @@ int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, doub
     Geom g{mx, my, mx + 4, my + 4, dx, dy};
     Work W = make_work(work, L.S);
     char* base = (char*)work;
+    uint32_t* act = (uint32_t*)(base + L.off_act);
     AdjWork A{(double*)(base + L.off_lamq), (double*)(base + L.off_xfb), (double*)(base + L.off_yfb),
               (double*)(base + L.off_xcb), (double*)(base + L.off_ycb), (double*)(base + L.off_tdq),
-              (double*)(base + L.off_qsb), (double*)(base + L.off_sv)};
+              (double*)(base + L.off_qsb), (double*)(base + L.off_sv), act, L.act_nx};
     double* part = (double*)(base + L.off_part);
+    // reverse planes, block partials, activity map and lam_in start at zero:
+    // the items of inactive blocks are skipped
+    cudaMemsetAsync(base + L.off_lamq, 0, L.off_sv - L.off_lamq, s);
+    cudaMemsetAsync(base + L.off_part, 0, L.total - L.off_part, s);
+    cudaMemsetAsync(lam_in, 0, (size_t)5 * mx * my * 8, s);
     const long long npad = (long long)L.S.npad, nint = (long long)mx * my;
     const long long nxf = (long long)(mx + 1) * (my + 2), nyf = (long long)(mx + 2) * (my + 1);
     // forward intermediates of this step
     k_fw_b4<<<nblk(npad), ATPB, 0, s>>>(P, g, q_in, b, W, status);
+    k_fw_mark<<<nblk(npad), ATPB, 0, s>>>(P, g, W, act, L.act_nx);
     k_fw_taudir<<<nblk(npad), ATPB, 0, s>>>(P, g, W);
     k_fw_svrec<<<nblk(npad), ATPB, 0, s>>>(P, g, W, A);
     k_fw_riemann<0><<<(unsigned)L.nb_rx, ATPB, 0, s>>>(P, g, W, A.sv);
@@ -518,6 +580,9 @@ int dclaw_step_adjoint_batched(const dclaw_adj_batch* batch, const dclaw_adj_mem
     int dev = 0, nsm = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     BatchArgs a{batch->nmembers, members, params, dt, q_in, b, lam_out, lam_in, (char*)work, status};
+    // reverse planes, partials, activity maps and lam_in start at zero: the
+    // items of inactive blocks are skipped
+    k_adj_batch_zero<<<dim3(64, (unsigned)batch->nmembers), 256, 0, s>>>(a);
     // persistent grids: a few blocks per SM, capped by the chunks of the space
     auto grid = [&](int sp) -> unsigned {
         uint32_t c = batch->nchunks[sp];
@@ -526,6 +591,7 @@ int dclaw_step_adjoint_batched(const dclaw_adj_batch* batch, const dclaw_adj_mem
     };
 #define DC_LAUNCH(op) k_adj_batch<op><<<grid(OpTraits<op>::SPACE), ATPB, 0, s>>>(a, batch->nchunks[OpTraits<op>::SPACE])
     DC_LAUNCH(OP_FW_B4);
+    DC_LAUNCH(OP_FW_MARK);
     DC_LAUNCH(OP_FW_TAUDIR);
     DC_LAUNCH(OP_FW_SVREC);
     DC_LAUNCH(OP_FW_RX);

@@ -1732,7 +1732,25 @@ struct AdjWork {
     double* tdq;   // NTD padded planes
     double* qsb;   // 5 padded planes
     double* sv;    // NSV padded planes: setvars records (svrec_cell)
+    // activity of ACT_TILE x ACT_TILE blocks of padded cells (nullable: all
+    // active): nonzero when a cell within ACT_REACH of the block is wet in
+    // the step's b4step2 state. Every reverse item whose cell lies in an
+    // inactive block has only dry cells within ACT_REACH: its outputs are
+    // zeros (dry-dry solves and dry cells have no adjoint form, a wave of
+    // zero norm takes no part in the limiter) or values no item reads, so
+    // with the reverse planes zeroed beforehand it can be skipped.
+    const uint32_t* act;
+    int act_nx;    // blocks per row of padded cells
 };
+
+constexpr int ACT_TILE = 16, ACT_REACH = 4;
+
+// whether the reverse items at padded cell (i, j) (interfaces: the cell on
+// their high side) may contribute
+DC_HD bool adj_active(const AdjWork& A, int i, int j) {
+    if (!A.act) return true;
+    return A.act[((j + 1) / ACT_TILE) * A.act_nx + (i + 1) / ACT_TILE] != 0u;
+}
 
 // padded cell (i, j), i in -1..mx+2, j in -1..my+2: setvars records
 DC_HD void adj_item_svrec(const dclaw_params& P, const Geom& g, const Work& W, const AdjWork& A, int i, int j) {

@@ -269,8 +269,9 @@ int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, doub
  * The reference differentiates its particle filters member by member with
  * jax.jacfwd / jax.grad under jax.vmap (gradient_particle_filter/pf_flume/
  * inference.py:96-108). Here the adjoint of one step of every member of an
- * ensemble of uneven patches runs as one sequence of 16 launches, each a
- * grid-stride loop over the chunks of all members' items. Each member has its
+ * ensemble of uneven patches runs as one sequence of 18 launches (a zeroing
+ * pass, then the stages), each a grid-stride loop over the chunks of all
+ * members' items. Each member has its
  * own parameters, dt and parameter adjoints; member k's results equal those of
  * dclaw_step_adjoint on member k alone, bit for bit.
  * Item spaces (chunk0 / nchunk index): 0 padded cells, 1 interior cells,
