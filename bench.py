@@ -496,23 +496,54 @@ def run_ours(args):
     value = cells * args.steps * world / (ms / 1000.0)
 
     # ---- end to end through the public patch-step API with host buffers ----
-    e2e_ms = None
+    e2e_ms = e2e_serial_ms = None
     h2d = d2h = 0
     if args.e2e_steps > 0:
         qh = st.state().cpu().pin_memory()
         cfl_h = torch.zeros(8, dtype=torch.float64).pin_memory()
-        barrier()
         f0 = torch.cuda.Event(enable_timing=True)
         f1 = torch.cuda.Event(enable_timing=True)
+        # the host-buffer step: the state stays in pinned host memory and
+        # every step uploads it, steps it and downloads the result, the
+        # copies pipelined against the compute band by band
+        st.step_host(qh)
+        barrier()
         f0.record(stream)
         for _ in range(args.e2e_steps):
-            st.qa.copy_(qh, non_blocking=True)           # that step's input state, host -> device
-            st.step(1)
-            qh.copy_(st.state(), non_blocking=True)      # the new state, device -> host
+            st.step_host(qh)                             # host state in, new host state out
             cfl_h.copy_(st.clock, non_blocking=True)     # Courant number and next dt
         f1.record(stream)
         barrier()
         e2e_ms = max_over_ranks(f0.elapsed_time(f1), dev)
+        # the same with whole-state copies around the device step, for comparison
+        barrier()
+        f0.record(stream)
+        for _ in range(args.e2e_steps):
+            st.qa.copy_(qh, non_blocking=True)
+            st.step(1)
+            qh.copy_(st.state(), non_blocking=True)
+            cfl_h.copy_(st.clock, non_blocking=True)
+        f1.record(stream)
+        barrier()
+        e2e_serial_ms = max_over_ranks(f0.elapsed_time(f1), dev)
+        # the floor: the same bytes copied both ways at once, nothing else
+        qh2 = torch.empty_like(qh).pin_memory()
+        up, down = torch.cuda.Stream(), torch.cuda.Stream()
+        barrier()
+        f0.record(stream)
+        for _ in range(args.e2e_steps):
+            up.wait_stream(stream)
+            down.wait_stream(stream)
+            with torch.cuda.stream(up):
+                st.qa.copy_(qh, non_blocking=True)
+            with torch.cuda.stream(down):
+                qh2.copy_(st.qb, non_blocking=True)
+            stream.wait_stream(up)
+            stream.wait_stream(down)
+        f1.record(stream)
+        barrier()
+        copy_floor_ms = max_over_ranks(f0.elapsed_time(f1), dev)
+        del qh2
         h2d = qh.numel() * 8
         d2h = qh.numel() * 8 + cfl_h.numel() * 8
 
@@ -535,8 +566,15 @@ def run_ours(args):
                "clocks": clocks, "gpu_launches": 3 * args.steps, "status": status}
         if e2e_ms is not None:
             out["e2e"] = {"value": cells * args.e2e_steps * world / (e2e_ms / 1000.0), "unit": "cell-updates/s",
-                          "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                          "api": "PatchStepper.step with pinned host state in/out every step"}
+                          "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.e2e_steps,
+                          "api": "PatchStepper.step_host (dclaw_step_host): pinned host state in and out every "
+                                 "step, copies pipelined by bands of tile rows",
+                          "serial_copies_value": cells * args.e2e_steps * world / (e2e_serial_ms / 1000.0),
+                          "serial_copies_note": "whole-state copy in, PatchStepper.step, whole-state copy out",
+                          "copy_floor_ms_per_step": copy_floor_ms / args.e2e_steps,
+                          "frac_of_copy_floor": copy_floor_ms / e2e_ms,
+                          "copy_floor_note": "the state copied host->device and device->host at once on two "
+                                             "streams, no compute: the PCIe bound of the e2e step"}
     if world > 1:
         dist.barrier()
     if rank == 0 and world == 1 and args.ensemble_members > 0:

@@ -37,6 +37,9 @@ SIGNATURES = {
     "dclaw_max_wave_speed": (_int, [_vp, _int, _int, _pp, _vp, _vp]),
     "dclaw_step_noalloc": (_int, [_vp, _vp, _vp, _int, _int, _dbl, _dbl, _pp, _vp, _vp]),
     "dclaw_step_noalloc_max_cells": (_sz, []),
+    "dclaw_step_host": (_int, [_vp, _vp, _vp, _int, _int, _dbl, _dbl, _pp, _vp, _vp, _sz, _int, _vp]),
+    "dclaw_step_host_workspace_bytes": (_sz, [_int, _int]),
+    "dclaw_step_host_bands": (_int, [_int, _int, _int, _vp, _int]),
     "dclaw_batch_tile_shapes": (_int, [_vp, _vp, _int]),
     "dclaw_batch_layout": (_int, [_int, _vp, _vp, _vp, _vp, _int, ctypes.POINTER(CMember), ctypes.POINTER(CBatch)]),
     "dclaw_step_batched": (_int, [ctypes.POINTER(CBatch), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

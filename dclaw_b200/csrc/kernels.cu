@@ -9,6 +9,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
+
 #include "stages.cuh"
 #include "tile.cuh"
 #include "workspace.cuh"
@@ -208,13 +210,15 @@ __global__ void k_clock_init(dclaw_clock* clk, double t, double dt, double t_fin
 }
 
 // ---- fused step: K1 cell records + K2 tiles --------------------------------
+// prow0 / nprow: the padded rows (0 .. my+3 for j = -1 .. my+2) this launch
+// covers, all of them by default
 __global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_records(dclaw_params P, Geom g, const double* __restrict__ q_in,
                                                  const double* __restrict__ b, Rec R, dclaw_clock* clk,
-                                                 uint32_t* __restrict__ tflag) {
-    const long long n = (long long)g.PX * g.PY;
+                                                 uint32_t* __restrict__ tflag, int prow0 = 0, int nprow = -1) {
+    const long long n = (long long)g.PX * (nprow < 0 ? g.PY : nprow);
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n) return;
-    int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
+    int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1 + prow0;
     if (cell_record(P, g, q_in, b, R, i, j)) flag_status(clk, DCLAW_ERR_NAN);
     if (tflag && R.get(R_H, pidx(g, i, j)) > 0.0)
         mark_tiles(tflag, clk->nsteps + 1u, i, j, TILE_X, TILE_Y, (g.mx + TILE_X - 1) / TILE_X,
@@ -363,13 +367,16 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
     return cfl;
 }
 
+// ty0: the first tile row of the launch (grid.y tile rows from there)
 template <int TX, int TY, bool WITH_SRC2>
 __global__ void __launch_bounds__(TILE_TPB, DCLAW_TILE_MINBLOCKS) k_tile(dclaw_params P, Geom g, Rec R, const double* __restrict__ b,
                                                  double* __restrict__ q_out, dclaw_clock* clk,
-                                                 uint32_t* __restrict__ brlog, const uint32_t* __restrict__ tflag) {
+                                                 uint32_t* __restrict__ brlog, const uint32_t* __restrict__ tflag,
+                                                 int ty0 = 0) {
     extern __shared__ double smem[];
-    const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
-    const bool active = !tflag || brlog || tflag[blockIdx.y * gridDim.x + blockIdx.x] == clk->nsteps + 1u;
+    const int ty = (int)blockIdx.y + ty0;
+    const int i0 = 1 + blockIdx.x * TX, j0 = 1 + ty * TY;
+    const bool active = !tflag || brlog || tflag[ty * gridDim.x + blockIdx.x] == clk->nsteps + 1u;
     bool nan;
     double cfl = tile_body<TX, TY, WITH_SRC2, TILE_TPB>(P, g, R, b, q_out, clk->dt, i0, j0, smem, brlog, nan, active);
     if (nan) flag_status(clk, DCLAW_ERR_NAN);
@@ -377,14 +384,15 @@ __global__ void __launch_bounds__(TILE_TPB, DCLAW_TILE_MINBLOCKS) k_tile(dclaw_p
     if (WITH_SRC2) last_block_tick(P, clk);
 }
 
-// src2 of every interior cell from the updated state; the last block
-// applies the tick rule
+// src2 of the interior cells c0 .. c0 + ncell - 1 (all by default) from the
+// updated state; with `tick` the last block applies the tick rule
 __global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_src2_cells(dclaw_params P, Geom g, const double* __restrict__ q_star,
                                                     double* __restrict__ q_out, dclaw_clock* clk,
-                                                    const uint32_t* __restrict__ tflag) {
-    const long long n = (long long)g.mx * g.my;
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx < n) {
+                                                    const uint32_t* __restrict__ tflag, long long c0 = 0,
+                                                    long long ncell = -1, int tick = 1) {
+    const long long n = ncell < 0 ? (long long)g.mx * g.my : ncell;
+    long long idx = c0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < c0 + n) {
         const int i = (int)(idx % g.mx) + 1, j = (int)(idx / g.mx) + 1;
         if (tile_active(tflag, clk->nsteps + 1u, i, j, TILE_X, TILE_Y, (g.mx + TILE_X - 1) / TILE_X)) {
             cell_src2(P, g, clk->dt, q_star, q_out, (size_t)idx);
@@ -393,7 +401,7 @@ __global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_src2_cells(dclaw_param
             for (int m = 0; m < 5; ++m) q_out[(size_t)m * plane + (size_t)idx] = 0.0;
         }
     }
-    last_block_tick(P, clk);
+    if (tick) last_block_tick(P, clk);
 }
 
 // ---- batched ensemble -------------------------------------------------------
@@ -731,6 +739,79 @@ inline bool sizes_ok(int mx, int my) {
     return mx >= 2 && my >= 2 && (long long)(mx + 4) * (my + 4) < (1LL << 40);
 }
 
+// ---- the host-buffer step: bands of tile rows ------------------------------
+// Band g holds tile rows T[g] .. T[g+1]-1 (cell rows 1 + T[g] TY .. T[g+1] TY).
+// Its tiles read the records of rows up to T[g+1] TY + 2 (and only those
+// records mark their flags); the record of row j reads the input rows
+// j - 1 .. j + 1. So once the input rows up to T[g+1] TY + 3 are on the
+// device, the band's records, tiles and src2 can run while later rows are
+// still uploading, and its rows can download while later bands compute.
+constexpr int MAX_HOST_BANDS = 64;
+
+inline int host_auto_bands(int mx, int my) {
+    const int nty = (my + TILE_Y - 1) / TILE_Y;
+    // about 40 MB of state per band: enough work per band to fill the GPU
+    // and few enough launches and copies, fine enough that the first upload
+    // and the last download (the parts that do not overlap) stay short. On
+    // the 4096^2 state (16 bands) the step then takes 1.07x the time of
+    // the bare copies both ways at once; 4 bands take 1.25x, 64 take 1.22x.
+    const double state = 40.0 * mx * (double)my;
+    int nb = (int)(state / 40.0e6) + 1;
+    if (nb > MAX_HOST_BANDS) nb = MAX_HOST_BANDS;
+    if (nb > nty) nb = nty;
+    return nb < 1 ? 1 : nb;
+}
+
+// first tile row of each band (first[0..nb], first[nb] = tile rows)
+inline void host_band_plan(int my, int nb, int* first) {
+    const int nty = (my + TILE_Y - 1) / TILE_Y;
+    for (int g = 0; g <= nb; ++g) first[g] = (int)((long long)g * nty / nb);
+}
+
+struct HostPipe {
+    cudaStream_t up = nullptr, down = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_end = nullptr;
+    cudaEvent_t ev_up[MAX_HOST_BANDS] = {}, ev_cmp[MAX_HOST_BANDS] = {};
+    bool ready = false;
+};
+static HostPipe g_pipe[MAX_DEVICES];
+static std::mutex g_pipe_mu;
+
+// the two copy streams and the events of the current device, created on
+// first use and kept for the process
+inline HostPipe* host_pipe() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return nullptr;
+    HostPipe& hp = g_pipe[dev];
+    if (!hp.ready) {
+        const unsigned fl = cudaEventDisableTiming;
+        bool ok = cudaStreamCreateWithFlags(&hp.up, cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaStreamCreateWithFlags(&hp.down, cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&hp.ev_start, fl) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&hp.ev_end, fl) == cudaSuccess;
+        for (int k = 0; ok && k < MAX_HOST_BANDS; ++k)
+            ok = cudaEventCreateWithFlags(&hp.ev_up[k], fl) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&hp.ev_cmp[k], fl) == cudaSuccess;
+        if (!ok) return nullptr;
+        hp.ready = true;
+    }
+    return &hp;
+}
+
+inline size_t host_state_bytes(int mx, int my) { return align256((size_t)5 * mx * my * 8); }
+
+// rows lo .. hi (1-based, inclusive) of the five planes of a state
+inline cudaError_t copy_rows(double* dst, const double* src, int mx, int my, int lo, int hi, cudaMemcpyKind kind,
+                             cudaStream_t s) {
+    if (lo > hi) return cudaSuccess;
+    const size_t plane = (size_t)mx * my, off = (size_t)(lo - 1) * mx, n = (size_t)(hi - lo + 1) * mx;
+    for (int m = 0; m < 5; ++m) {
+        cudaError_t e = cudaMemcpyAsync(dst + m * plane + off, src + m * plane + off, n * 8, kind, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 }  // namespace dclaw
 
 using namespace dclaw;
@@ -852,6 +933,94 @@ int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int m
                                                                             tflag);
     }
     return cuda_status();
+}
+
+size_t dclaw_step_host_workspace_bytes(int mx, int my) {
+    if (!sizes_ok(mx, my)) return 0;
+    return align256(layout(mx, my).total_fused) + 2 * host_state_bytes(mx, my);
+}
+
+int dclaw_step_host_bands(int mx, int my, int nbands, int32_t* first, int max) {
+    if (!sizes_ok(mx, my) || nbands < 0) return 0;
+    const int nty = (my + TILE_Y - 1) / TILE_Y;
+    int nb = nbands == 0 ? host_auto_bands(mx, my) : (nbands > nty ? nty : nbands);
+    if (nb > MAX_HOST_BANDS) nb = MAX_HOST_BANDS;
+    int f[MAX_HOST_BANDS + 1];
+    host_band_plan(my, nb, f);
+    for (int g = 0; first && g <= nb && g < max; ++g) first[g] = f[g];
+    return nb;
+}
+
+int dclaw_step_host(const double* q_in, double* q_out, const double* b, int mx, int my, double dx, double dy,
+                    const dclaw_params* p, dclaw_clock* clock, void* work, size_t work_bytes, int nbands,
+                    void* stream) {
+    if (!q_in || !q_out || !b || !p || !clock || !work || nbands < 0) return DCLAW_ERR_ARG;
+    if (!sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0)) return DCLAW_ERR_ARG;
+    int rc = dclaw_params_check(p);
+    if (rc) return rc;
+    if (work_bytes < dclaw_step_host_workspace_bytes(mx, my)) return DCLAW_ERR_WORKSPACE;
+    if (ensure_tile_smem_attr() != DCLAW_OK) return DCLAW_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_pipe_mu);
+    HostPipe* hp = host_pipe();
+    if (!hp) return DCLAW_ERR_CUDA;
+    int first[MAX_HOST_BANDS + 1];
+    const int nb = dclaw_step_host_bands(mx, my, nbands, first, MAX_HOST_BANDS + 1);
+    Layout L = layout(mx, my);
+    cudaStream_t s = (cudaStream_t)stream;
+    Geom g{mx, my, mx + 4, my + 4, dx, dy};
+    Rec R{(double*)((char*)work + L.off_rec), L.npad};
+    const dclaw_params P = *p;
+    using TG = TileGeom<TILE_X, TILE_Y>;
+    uint32_t* tflag = (uint32_t*)((char*)work + L.off_tflag);
+    double* qstar = (double*)((char*)work + L.off_qstar);
+    double* dq_in = (double*)((char*)work + align256(L.total_fused));
+    double* dq_out = (double*)((char*)dq_in + host_state_bytes(mx, my));
+    const int ntx = (mx + TILE_X - 1) / TILE_X;
+    cudaError_t e = cudaSuccess;
+    // the copy streams start after the work queued on the caller's stream
+    // (the previous step still reads the device copies)
+    if (e == cudaSuccess) e = cudaEventRecord(hp->ev_start, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(hp->up, hp->ev_start, 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(hp->down, hp->ev_start, 0);
+    // uploads: band g brings the input rows its compute needs
+    int lo = 1;
+    for (int k = 0; k < nb && e == cudaSuccess; ++k) {
+        const int hi = k == nb - 1 ? my : (first[k + 1] * TILE_Y + 3 < my ? first[k + 1] * TILE_Y + 3 : my);
+        e = copy_rows(dq_in, q_in, mx, my, lo, hi, cudaMemcpyHostToDevice, hp->up);
+        if (e == cudaSuccess) e = cudaEventRecord(hp->ev_up[k], hp->up);
+        lo = hi + 1 > lo ? hi + 1 : lo;
+    }
+    // compute on the caller's stream, downloads behind it
+    int ja = -1;
+    for (int k = 0; k < nb && e == cudaSuccess; ++k) {
+        e = cudaStreamWaitEvent(s, hp->ev_up[k], 0);
+        if (e != cudaSuccess) break;
+        const int jb = k == nb - 1 ? my + 2 : (first[k + 1] * TILE_Y + 2 < my + 2 ? first[k + 1] * TILE_Y + 2 : my + 2);
+        if (jb >= ja) {
+            const int nrow = jb - ja + 1;
+            k_records<<<nblocks((long long)g.PX * nrow), TPB, 0, s>>>(P, g, dq_in, b, R, clock, tflag, ja + 1, nrow);
+            ja = jb + 1;
+        }
+        const int nty = first[k + 1] - first[k];
+        const int r0 = 1 + first[k] * TILE_Y, r1 = first[k + 1] * TILE_Y < my ? first[k + 1] * TILE_Y : my;
+        if (nty > 0) {
+            dim3 grid(ntx, nty);
+            k_tile<TILE_X, TILE_Y, false><<<grid, TILE_TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, qstar, clock, nullptr,
+                                                                                 tflag, first[k]);
+            const long long nc = (long long)(r1 - r0 + 1) * mx;
+            k_src2_cells<<<nblocks(nc), TPB, 0, s>>>(P, g, qstar, dq_out, clock, tflag, (long long)(r0 - 1) * mx, nc,
+                                                     0);
+        }
+        if (k == nb - 1) k_tick<<<1, 32, 0, s>>>(P, clock);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaEventRecord(hp->ev_cmp[k], s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(hp->down, hp->ev_cmp[k], 0);
+        if (e == cudaSuccess && nty > 0) e = copy_rows(q_out, dq_out, mx, my, r0, r1, cudaMemcpyDeviceToHost, hp->down);
+    }
+    // the caller's stream resumes after the last download
+    if (e == cudaSuccess) e = cudaEventRecord(hp->ev_end, hp->down);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, hp->ev_end, 0);
+    return e == cudaSuccess ? cuda_status() : DCLAW_ERR_CUDA;
 }
 
 int dclaw_bc2amr(double* q, int mx, int my, int mbc, const dclaw_params* p, void* stream) {

@@ -170,6 +170,29 @@ class PatchStepper:
     def status(self) -> int:
         return self.read_clock().status
 
+    # ---- state in host memory ----------------------------------------------
+    def step_host(self, q_host: torch.Tensor, out: torch.Tensor | None = None, nbands: int = 0) -> None:
+        """One step of a (5, my, mx) float64 state held in host memory:
+        q_host -> out (q_host itself, in place, by default), with this
+        stepper's bed, parameters and clock. The copies overlap the compute
+        band by band when the host tensors are pinned. The stepper's device
+        state is not used. Returns once the step is queued on the current
+        stream; synchronize it before reading `out`."""
+        out = q_host if out is None else out
+        for t, name in ((q_host, "q_host"), (out, "out")):
+            if t.is_cuda or t.dtype != torch.float64 or not t.is_contiguous():
+                raise _lib.DClawError(f"{name} must be a contiguous float64 host tensor")
+            if tuple(t.shape) != (5, self.my, self.mx):
+                raise _lib.DClawError(f"{name} must have shape (5, my, mx) = (5, {self.my}, {self.mx})")
+        if getattr(self, "host_work", None) is None:
+            nbytes = self.lib.dclaw_step_host_workspace_bytes(self.mx, self.my)
+            self.host_work = torch.empty(nbytes, dtype=torch.uint8, device=self.qa.device)
+        rc = self.lib.dclaw_step_host(_lib.ptr(q_host), _lib.ptr(out), _lib.ptr(self.b), self.mx, self.my,
+                                      self.dx, self.dy, ctypes.byref(self.cp), _lib.ptr(self.clock),
+                                      _lib.ptr(self.host_work), self.host_work.numel(), int(nbands),
+                                      _lib.stream_ptr())
+        _lib.check(rc, "dclaw_step_host")
+
 
 # ---- differentiable-port style API ------------------------------------------
 def _to_native(q: torch.Tensor) -> torch.Tensor:

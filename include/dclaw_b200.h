@@ -182,6 +182,32 @@ int dclaw_step_noalloc(const double* q_in, double* q_out, const double* b, int m
                        void* stream);
 /* largest patch (padded cells) dclaw_step_noalloc accepts */
 size_t dclaw_step_noalloc_max_cells(void);
+/* dclaw_step on a state held in HOST memory: the reference's patch step
+ * works on host arrays (stepgrid passes q and aux to step2, step2.f90:9-10,
+ * then src2, src2.f90:27), and a host time loop that keeps the state there
+ * calls this once per step. q_in and q_out are (5, my, mx) host arrays (they
+ * may be the same array: the step then updates it in place); b, clock and
+ * work are on the device, work holding dclaw_step_host_workspace_bytes()
+ * (the step's workspace and a device copy of the state in and out). The
+ * step is pipelined by bands of tile rows: each band's input rows go up on
+ * one copy stream, its records, tiles and src2 run on `stream`, and its
+ * output rows come down on another copy stream, so that both copy
+ * directions and the compute overlap. Host memory must be page-locked
+ * (cudaHostAlloc / cudaHostRegister) for the copies to overlap; pageable
+ * memory gives the same result without the overlap. nbands = 0 picks the
+ * band count (about 40 MB of state per band, at most 64); a positive value
+ * asks for that many (capped by the tile rows and 64). The call returns once
+ * the work is queued; `stream` waits for the last download, so a
+ * synchronize on it (or on an event recorded after the call) means q_out and
+ * the clock are complete. Results are those of dclaw_step, bit for bit. */
+int dclaw_step_host(const double* q_in, double* q_out, const double* b, int mx, int my,
+                    double dx, double dy, const dclaw_params* p, dclaw_clock* clock,
+                    void* work, size_t work_bytes, int nbands, void* stream);
+size_t dclaw_step_host_workspace_bytes(int mx, int my);
+/* the band plan dclaw_step_host uses: returns the band count nb and writes
+ * the first tile row of each band to first[0..nb] (first[nb] = tile rows),
+ * at most `max` entries; 0 for an invalid size */
+int dclaw_step_host_bands(int mx, int my, int nbands, int32_t* first, int max);
 /* ---- batched ensemble -------------------------------------------------------
  * An ensemble of independent uniform patches of uneven sizes, each with its
  * own parameters and its own clock (the particle-filter use of the
