@@ -67,7 +67,8 @@ def parse():
     ap.add_argument("--ensemble-steps", type=int, default=10)
     ap.add_argument("--grad-steps", type=int, default=500,
                     help="steps of the 512 x 512 gradient case measured beside the plain step (0: skip)")
-    ap.add_argument("--checkpoint-block", type=int, default=0, help="0: ceil(sqrt(steps))")
+    ap.add_argument("--checkpoint-block", type=int, default=0,
+                    help="0: the smallest block whose checkpoints fit half of the free device memory")
     ap.add_argument("--bgrad-members", type=int, default=64,
                     help="members of the batched-gradient channel case (0: skip)")
     ap.add_argument("--bgrad-steps", type=int, default=200,
@@ -276,14 +277,15 @@ def ensemble_bench(args, dev):
 def gradient_bench(args, dev):
     """Gradient of a gauge loss over a 500-step run of the 512 x 512 case
     with respect to (phi, kref, m0, alpha_c) and the initial depth of every
-    cell, by the hand-written step adjoint with sqrt(N) checkpointing,
+    cell, by the hand-written step adjoint with time checkpointing (every
+    state kept when the run fits the memory budget),
     against the forward solve of the same run. Both are timed with CUDA
     events on the launching stream; the gradient's time covers its forward
     pass (with checkpoints), the loss and the whole backward pass."""
     import torch
 
     from dclaw_b200 import workloads as W
-    from dclaw_b200.adjoint import initial_state, rollout_states, theta_of
+    from dclaw_b200.adjoint import checkpoint_block_of, initial_state, rollout_states, theta_of
     from dclaw_b200.solver import PatchStepper
 
     c = W.gradient_case(nsteps=args.grad_steps)
@@ -301,10 +303,15 @@ def gradient_bench(args, dev):
 
     sel = gj * c.b.shape[1] + gi            # depth plane entries of the gauge cells
 
+    used_k = []
+
     def gauges(h, m0, theta):
         q0 = initial_state(h, m0, p)
-        return rollout_states(q0, theta, b, p, c.dx, c.dx, c.nsteps, c.out_steps, c.dt_initial,
-                              checkpoint_block=blk, select=sel)
+        out = rollout_states(q0, theta, b, p, c.dx, c.dx, c.nsteps, c.out_steps, c.dt_initial,
+                             checkpoint_block=blk, select=sel)
+        if out.grad_fn is not None:
+            used_k.append(checkpoint_block_of(out))
+        return out
 
     with torch.no_grad():
         target = gauges(h0, torch.tensor(c.m0, dtype=torch.float64, device=dev), theta_of(c.true_params, dev))
@@ -335,7 +342,7 @@ def gradient_bench(args, dev):
         torch.cuda.synchronize()
         grad_ms.append(e0.elapsed_time(e1))
     f, g = min(fwd_ms), min(grad_ms)
-    k = blk or math.ceil(math.sqrt(c.nsteps))
+    k = used_k[-1]
     mx, my = c.b.shape[1], c.b.shape[0]
     return {"workload": f"gauge_loss_{mx}x{my}_dx{c.dx}_{c.nsteps}steps", "gauges": len(c.gauges),
             "output_times": len(c.out_steps), "checkpoint_block": k, "forward_ms": f, "gradient_ms": g,
@@ -359,7 +366,8 @@ def batched_gradient_bench(args, dev):
     import torch
 
     from dclaw_b200 import workloads as W
-    from dclaw_b200.adjoint import ensemble_rollout_states, initial_state, rollout_states, theta_of
+    from dclaw_b200.adjoint import (checkpoint_block_of, ensemble_rollout_states, initial_state, rollout_states,
+                                    theta_of)
     from dclaw_b200.ensemble import EnsembleStepper, Member
 
     c = W.batched_gradient_case(n=args.bgrad_members, nsteps=args.bgrad_steps)
@@ -442,7 +450,8 @@ def batched_gradient_bench(args, dev):
     cells = sum(m.q.shape[1] * m.q.shape[2] for m in c.members)
     area = torch.tensor(c.block_area, dtype=torch.float64, device=dev)
     return {"workload": f"channels_{n}x1024_w128-256_dx0.05_{c.nsteps}steps", "members": n, "cells": cells,
-            "steps": c.nsteps, "forward_ms": min(fwd), "gradient_ms": grad_ms,
+            "steps": c.nsteps, "checkpoint_block": checkpoint_block_of(out), "forward_ms": min(fwd),
+            "gradient_ms": grad_ms,
             "gradient_over_forward": grad_ms / min(fwd), "unbatched_first2_gradient_ms": unb,
             "batched_gradient_ms_per_member": grad_ms / n, "peak_mem_gb": peak,
             "grad_member0": {"phi_deg": float(theta.grad[0, 0]), "kref": float(theta.grad[0, 1]),

@@ -10,8 +10,11 @@ sequence per step), wrapped in a `torch.autograd.Function` with the same
 sqrt(N) time checkpointing:
 
 * forward: run the fused step, record each step's dt on the device, keep the
-  state every k steps (k = ceil(sqrt(n_steps)) unless given) and the states
-  the caller asked for;
+  state every k steps and the states the caller asked for. Unless k is
+  given, it is the smallest block whose checkpoints fit half of the free
+  device memory (after the adjoint's workspace): every state (k = 1, no
+  recompute) when the run fits, as a 512 x 512 run of 500 steps (5 GB)
+  does in a B200's 180 GB, and at most ceil(sqrt(n_steps));
 * backward: for each block of k steps, last block first, recompute its
   states from its checkpoint with the recorded dts (bit-identical, so every
   branch is the one the forward took), then run the step adjoint backwards
@@ -82,9 +85,37 @@ class StepAdjoint:
         _lib.check(int(self.status.item()), "adjoint step")
 
 
-def _block(n_steps: int, checkpoint_block: int | None) -> int:
+# share of the device memory free when a differentiable run starts that its
+# checkpoints may take (the step adjoint's workspace is set aside first)
+CHECKPOINT_MEMORY_FRACTION = 0.5
+
+
+def checkpoint_block_for(n_steps: int, state_bytes: int, budget_bytes: float) -> int:
+    """The smallest block length k whose checkpoints fit the budget: the
+    forward pass keeps ceil(n/k) block inputs, the backward pass recomputes
+    a block's other k-1 states into a k-state buffer (none when k = 1). The
+    backward pass recomputes n - ceil(n/k) steps, so the smallest k that
+    fits is the cheapest: k = 1 (every state kept, nothing recomputed)
+    whenever the run's states fit, up to k = ceil(sqrt(n)), the memory
+    minimum of two-level checkpointing, which is returned when nothing
+    smaller fits."""
+    n = max(1, int(n_steps))
+    kmax = max(1, math.ceil(math.sqrt(n)))
+    for k in range(1, kmax):
+        nstates = -(-n // k) + (k if k > 1 else 0)
+        if nstates * state_bytes <= budget_bytes:
+            return k
+    return kmax
+
+
+def _block(n_steps: int, checkpoint_block: int | None, state_bytes: int = 0, reserve_bytes: int = 0,
+           device=None) -> int:
     if checkpoint_block is None:
-        return max(1, math.ceil(math.sqrt(n_steps)))
+        if state_bytes <= 0 or device is None or device.type != "cuda":
+            return max(1, math.ceil(math.sqrt(n_steps)))
+        free, _ = torch.cuda.mem_get_info(device)
+        budget = CHECKPOINT_MEMORY_FRACTION * max(0, free - reserve_bytes)
+        return checkpoint_block_for(n_steps, state_bytes, budget)
     if checkpoint_block < 1:
         raise ValueError("checkpoint_block must be >= 1")
     return int(checkpoint_block)
@@ -100,9 +131,10 @@ class _Rollout(torch.autograd.Function):
             st.init_clock(0.0, fixed_dt=True)
         else:
             st.init_clock(float(dt0), t_final=float(t_final), fixed_dt=bool(fixed_dt))
-        k = _block(n_steps, checkpoint_block)
+        lib = _lib.load()
+        k = _block(n_steps, checkpoint_block, q0.numel() * 8,
+                   lib.dclaw_adjoint_workspace_bytes(q0.shape[2], q0.shape[1]), q0.device)
         dts = torch.empty(n_steps, dtype=torch.float64, device=q0.device)
-        ckpt = []
         oshape = tuple(q0.shape) if select is None else tuple(select.shape)
         outs = torch.empty((len(out_steps),) + oshape, dtype=q0.dtype, device=q0.device)
         pick = (lambda t: t) if select is None else (lambda t: t.reshape(-1)[select])
@@ -111,15 +143,25 @@ class _Rollout(torch.autograd.Function):
             where.setdefault(n, []).append(idx)
         for idx in where.get(0, []):
             outs[idx].copy_(pick(q0.detach()))
+        # every block's first input in one allocation; the step before a
+        # block writes straight into its slot, the others ping-pong
+        store = torch.empty((max(1, -(-n_steps // k)),) + tuple(q0.shape), dtype=q0.dtype, device=q0.device)
+        store[0].copy_(st.qa)
+        ckpt = list(store.unbind(0))
+        src = ckpt[0]
         for n in range(n_steps):
-            if n % k == 0:
-                ckpt.append(st.state().clone())
+            nxt = (n + 1) // k
+            if (n + 1) % k == 0 and nxt < len(ckpt):
+                dst = ckpt[nxt]
+            else:
+                dst = st.qa if src is not st.qa else st.qb
             if dt_schedule is not None:
                 st.clock[1:2].copy_(dt_schedule[n:n + 1])
-            st.step(1)
+            st._launch(src, dst)
+            src = dst
             dts[n:n + 1].copy_(st.clock[3:4])   # dt the step used
             for idx in where.get(n + 1, []):
-                outs[idx].copy_(pick(st.state()))
+                outs[idx].copy_(pick(src))
         _lib.check(st.status(), "rollout forward")
         ctx.save_for_backward(b, dts)
         ctx.ckpt = ckpt
@@ -142,7 +184,7 @@ class _Rollout(torch.autograd.Function):
         lam = torch.zeros(shape, dtype=torch.float64, device=dev)
         lam2 = torch.empty_like(lam)
         pbar = torch.zeros(4, dtype=torch.float64, device=dev)
-        seg = torch.empty((k,) + tuple(shape), dtype=torch.float64, device=dev)
+        seg = torch.empty((k,) + tuple(shape), dtype=torch.float64, device=dev) if k > 1 else None
         g_out = g_out.contiguous() if g_out is not None else None
         sel = ctx.select
 
@@ -156,18 +198,18 @@ class _Rollout(torch.autograd.Function):
         for s in reversed(range(nblocks)):
             n0 = s * k
             n1 = min(n0 + k, n_steps)
-            # recompute the block's states n0 .. n1-1 with the recorded dts
-            seg[0].copy_(ctx.ckpt[s])
-            fw.qa.copy_(ctx.ckpt[s])
+            # recompute the block's states n0+1 .. n1-1 from its first input
+            # with the recorded dts, each step writing its slot of seg
+            states = [ctx.ckpt[s]]
             for n in range(n0 + 1, n1):
                 fw.clock[1:2].copy_(dts[n - 1:n])
-                fw.step(1)
-                seg[n - n0].copy_(fw.state())
+                fw._launch(states[-1], seg[n - n0])
+                states.append(seg[n - n0])
             for n in range(n1, n0, -1):
                 if g_out is not None:
                     for idx in where.get(n, []):
                         add_out(idx)
-                adj.vjp(seg[n - 1 - n0], dts[n - 1:n], lam, lam2, pbar)
+                adj.vjp(states[n - 1 - n0], dts[n - 1:n], lam, lam2, pbar)
                 lam, lam2 = lam2, lam
         if g_out is not None:
             for idx in where.get(0, []):
@@ -190,8 +232,10 @@ def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b: torch.Tensor, param
     (0 = q0), shape (len(out_steps), 5, my, mx). dt0 is the first dt; with
     fixed_dt every step uses it, otherwise the tick rule picks the next dt
     from the Courant number (clipped at t_final when t_final > 0). Gradients
-    reach q0 and theta through the hand-written step adjoint with sqrt(N)
-    checkpointing (checkpoint_block steps per block, default ceil(sqrt(n))).
+    reach q0 and theta through the hand-written step adjoint with time
+    checkpointing (checkpoint_block steps per block; by default the
+    smallest block whose checkpoints fit half of the free device memory,
+    `checkpoint_block_for`: 1, every state kept, when the run fits).
     dt_schedule (n_steps,) float64 device tensor: replay these dts instead
     (dt0, fixed_dt and t_final are then ignored) -- e.g. the dts of an
     earlier adaptive run, for finite-difference checks at a fixed schedule.
@@ -208,6 +252,12 @@ def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b: torch.Tensor, param
         dt_schedule = dt_schedule.contiguous()
     return _Rollout.apply(q0, theta, b.contiguous(), params, dx, dy, int(n_steps), tuple(int(n) for n in out_steps),
                           float(dt0), bool(fixed_dt), float(t_final), checkpoint_block, dt_schedule, select)
+
+
+def checkpoint_block_of(out: torch.Tensor) -> int:
+    """The checkpoint block length the differentiable run that produced
+    `out` (rollout_states or ensemble_rollout_states) chose."""
+    return int(out.grad_fn.meta[-1])
 
 
 def last_dts(out: torch.Tensor) -> torch.Tensor:
@@ -302,7 +352,9 @@ class _EnsembleRollout(torch.autograd.Function):
     def forward(ctx, q0, theta, members, n_steps, out_steps, checkpoint_block, fixed_dt, dt_schedule, select):
         st = _ensemble(members, theta, fixed_dt or dt_schedule is not None)
         st.qa.copy_(q0.detach())
-        k = _block(n_steps, checkpoint_block)
+        lib = _lib.load()
+        reserve = sum(lib.dclaw_adjoint_workspace_bytes(m.q.shape[2], m.q.shape[1]) for m in members)
+        k = _block(n_steps, checkpoint_block, st.qa.numel() * 8, reserve, q0.device)
         dts = torch.empty((n_steps, st.n), dtype=torch.float64, device=q0.device)
         oshape = tuple(q0.shape) if select is None else tuple(select.shape)
         outs = torch.empty((len(out_steps),) + oshape, dtype=q0.dtype, device=q0.device)
@@ -312,16 +364,25 @@ class _EnsembleRollout(torch.autograd.Function):
             where.setdefault(n, []).append(idx)
         for idx in where.get(0, []):
             outs[idx].copy_(pick(q0.detach()))
-        ckpt = []
+        # as in _Rollout (arenas zeroed: the gaps between members stay zero)
+        store = torch.zeros((max(1, -(-n_steps // k)),) + tuple(st.qa.shape), dtype=torch.float64,
+                            device=q0.device)
+        store[0].copy_(st.qa)
+        ckpt = list(store.unbind(0))
+        src = ckpt[0]
         for n in range(n_steps):
-            if n % k == 0:
-                ckpt.append(st.qa.clone())
+            nxt = (n + 1) // k
+            if (n + 1) % k == 0 and nxt < len(ckpt):
+                dst = ckpt[nxt]
+            else:
+                dst = st.qa if src is not st.qa else st.qb
             if dt_schedule is not None:
                 _clock_field(st, 1).copy_(dt_schedule[n])
-            st.step(1)
+            st._launch(src, dst)
+            src = dst
             dts[n].copy_(_clock_field(st, 3))
             for idx in where.get(n + 1, []):
-                outs[idx].copy_(pick(st.qa))
+                outs[idx].copy_(pick(src))
         for kk, s in enumerate(st.status()):
             _lib.check(s, f"ensemble rollout, member {kk}")
         ctx.save_for_backward(dts)
@@ -343,7 +404,7 @@ class _EnsembleRollout(torch.autograd.Function):
         lam = torch.zeros_like(fw.qa)
         lam2 = torch.zeros_like(lam)   # arena gaps between members stay zero
         pbar = torch.zeros((fw.n, 4), dtype=torch.float64, device=dev)
-        seg = torch.empty((k,) + tuple(fw.qa.shape), dtype=torch.float64, device=dev)
+        seg = torch.zeros((k,) + tuple(fw.qa.shape), dtype=torch.float64, device=dev) if k > 1 else None
         g_out = g_out.contiguous() if g_out is not None else None
         sel = ctx.select
 
@@ -356,17 +417,16 @@ class _EnsembleRollout(torch.autograd.Function):
         for s in reversed(range(len(ctx.ckpt))):
             n0 = s * k
             n1 = min(n0 + k, n_steps)
-            seg[0].copy_(ctx.ckpt[s])
-            fw.qa.copy_(ctx.ckpt[s])
+            states = [ctx.ckpt[s]]
             for n in range(n0 + 1, n1):
                 _clock_field(fw, 1).copy_(dts[n - 1])
-                fw.step(1)
-                seg[n - n0].copy_(fw.qa)
+                fw._launch(states[-1], seg[n - n0])
+                states.append(seg[n - n0])
             for n in range(n1, n0, -1):
                 if g_out is not None:
                     for idx in where.get(n, []):
                         add_out(idx)
-                adj.vjp(seg[n - 1 - n0], dts[n - 1], lam, lam2, pbar)
+                adj.vjp(states[n - 1 - n0], dts[n - 1], lam, lam2, pbar)
                 lam, lam2 = lam2, lam
         if g_out is not None:
             for idx in where.get(0, []):
@@ -392,7 +452,8 @@ def ensemble_rollout_states(q0: torch.Tensor, theta: torch.Tensor, members, n_st
     or fixed; dt_schedule (n_steps, n) replays recorded dts). select (int64
     CUDA tensor of arena indices): return only these entries per output
     step (gauges) instead of whole arenas. The backward pass runs the
-    batched step adjoint with sqrt(N) checkpointing.
+    batched step adjoint with time checkpointing (block length as in
+    `rollout_states`).
     """
     for n in out_steps:
         if not 0 <= n <= n_steps:

@@ -70,6 +70,20 @@ __device__ __forceinline__ void block_max_to(double v, unsigned long long* acc) 
 
 __device__ __forceinline__ void flag_status(dclaw_clock* clk, int code) { atomicCAS(&clk->status, 0, code); }
 
+// column and row of a flat index over rows of width w, in 32-bit arithmetic
+// when the index fits (a 64-bit division is a long instruction sequence,
+// a large share of a per-cell kernel's issue slots)
+__device__ __forceinline__ void split_index(long long idx, int w, int& col, int& row) {
+    if (idx <= 0xffffffffLL) {
+        const unsigned u = (unsigned)idx, q = u / (unsigned)w;
+        row = (int)q;
+        col = (int)(u - q * (unsigned)w);
+    } else {
+        row = (int)(idx / w);
+        col = (int)(idx - (long long)row * w);
+    }
+}
+
 // ---- tile activity flags ------------------------------------------------------
 // A tile is active in a step when a cell within distance 3 of it is wet after
 // b4step2 (the cells whose records the tile reads). k_records writes the
@@ -218,7 +232,10 @@ __global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_records(dclaw_params P
     const long long n = (long long)g.PX * (nprow < 0 ? g.PY : nprow);
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n) return;
-    int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1 + prow0;
+    int i, j;
+    split_index(idx, g.PX, i, j);
+    i -= 1;
+    j += prow0 - 1;
     if (cell_record(P, g, q_in, b, R, i, j)) flag_status(clk, DCLAW_ERR_NAN);
     if (tflag && R.get(R_H, pidx(g, i, j)) > 0.0)
         mark_tiles(tflag, clk->nsteps + 1u, i, j, TILE_X, TILE_Y, (g.mx + TILE_X - 1) / TILE_X,
@@ -393,7 +410,10 @@ __global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_src2_cells(dclaw_param
     const long long n = ncell < 0 ? (long long)g.mx * g.my : ncell;
     long long idx = c0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx < c0 + n) {
-        const int i = (int)(idx % g.mx) + 1, j = (int)(idx / g.mx) + 1;
+        int i, j;
+        split_index(idx, g.mx, i, j);
+        i += 1;
+        j += 1;
         if (tile_active(tflag, clk->nsteps + 1u, i, j, TILE_X, TILE_Y, (g.mx + TILE_X - 1) / TILE_X)) {
             cell_src2(P, g, clk->dt, q_star, q_out, (size_t)idx);
         } else {
@@ -449,7 +469,10 @@ __global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_records_batch(int nmem
         const Rec R{work + M.rec_off, npad};
         const size_t idx = (size_t)(ch - M.rchunk0) * TPB + threadIdx.x;
         if (idx < npad) {
-            int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
+            int i, j;
+            split_index((long long)idx, g.PX, i, j);
+            i -= 1;
+            j -= 1;
             if (cell_record(prm[m], g, q_in + M.q_off, b + M.b_off, R, i, j)) flag_status(clocks + m, DCLAW_ERR_NAN);
             if (R.get(R_H, pidx(g, i, j)) > 0.0)
                 mark_tiles(tflag + M.tile0, clocks[m].nsteps + 1u, i, j, TX, TY, (int)M.ntiles_x,
@@ -524,7 +547,10 @@ __global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_src2_batch(int nmem, u
         const size_t n = (size_t)g.mx * g.my;
         const size_t idx = (size_t)(ch - M.schunk0) * TPB + threadIdx.x;
         if (idx < n) {
-            const int i = (int)(idx % g.mx) + 1, j = (int)(idx / g.mx) + 1;
+            int i, j;
+            split_index((long long)idx, g.mx, i, j);
+            i += 1;
+            j += 1;
             if (tile_active(tflag + M.tile0, clocks[m].nsteps + 1u, i, j, TX, TY, (int)M.ntiles_x)) {
                 cell_src2(prm[m], g, clocks[m].dt, work + M.qs_off, q_out + M.q_off, idx);
             } else {

@@ -96,3 +96,28 @@ def test_step_vjp_matches_finite_differences(adj, name):
         fdp = (Lp(hh) - Lp(-hh)) / (2 * hh)
         assert abs(pb[k] - fdp) <= 1e-4 * abs(fdp) + 1e-12, \
             f"{pname}: AD {pb[k]:.10e} FD {fdp:.10e}"
+
+
+def test_checkpoint_block_follows_the_memory_budget():
+    """The default checkpoint block: every state kept (k = 1) when the run
+    fits the budget, else the smallest k whose ceil(n/k) block inputs plus
+    a k-state recompute buffer fit, never above ceil(sqrt(n))."""
+    from dclaw_b200.adjoint import checkpoint_block_for
+
+    state = 10_485_760                       # a 512 x 512 state
+    assert checkpoint_block_for(500, state, 500 * state) == 1
+    assert checkpoint_block_for(500, state, 80e9) == 1
+    # 500 states do not fit, 250 + 2 do
+    assert checkpoint_block_for(500, state, 300 * state) == 2
+    assert checkpoint_block_for(500, state, 252 * state) == 2
+    assert checkpoint_block_for(500, state, 251 * state) == 3
+    # nothing fits: the two-level minimum ceil(sqrt(n))
+    assert checkpoint_block_for(500, state, 0) == math.ceil(math.sqrt(500)) == 23
+    for n in [1, 2, 7, 100, 801]:
+        for budget in [0, 5 * state, 40 * state, 1e15]:
+            k = checkpoint_block_for(n, state, budget)
+            assert 1 <= k <= max(1, math.ceil(math.sqrt(n)))
+            if k < max(1, math.ceil(math.sqrt(n))):
+                assert (-(-n // k) + (k if k > 1 else 0)) * state <= budget
+            for j in range(1, k):
+                assert (-(-n // j) + (j if j > 1 else 0)) * state > budget
