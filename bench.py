@@ -271,7 +271,7 @@ def ensemble_bench(args, dev):
             "looped_graph": {"value": cells * K / (ms_lg / 1000.0), "ms_per_step": ms_lg / K},
             "vs_looped_eager": ms_le / ms_b, "vs_looped_graph": ms_lg / ms_b,
             "autotune": {k: tune[k] for k in ("tile_shape", "tile_ctas_per_sm", "ms")},
-            "gpu_launches": 4 * K, "status_nonzero": sum(1 for x in status_b if x)}
+            "gpu_launches": 6 * K, "status_nonzero": sum(1 for x in status_b if x)}
 
 
 def gradient_bench(args, dev):
@@ -457,7 +457,7 @@ def batched_gradient_bench(args, dev):
             "grad_member0": {"phi_deg": float(theta.grad[0, 0]), "kref": float(theta.grad[0, 1]),
                              "alpha_c": float(theta.grad[0, 2]), "mu": float(theta.grad[0, 3]),
                              "m0": float(m0.grad[0]), "block_volume": float(H.grad[0] / area[0])},
-            "gpu_launches": {"adjoint_per_step": 18, "recompute_per_step": 4, "forward_per_step": 4},
+            "gpu_launches": {"adjoint_per_step": 18, "recompute_per_step": 6, "forward_per_step": 6},
             "note": "every member's dt from its own tick rule, recorded and replayed, not differentiated"}
 
 

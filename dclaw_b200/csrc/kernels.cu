@@ -107,6 +107,59 @@ __device__ __forceinline__ void mark_tiles(uint32_t* __restrict__ tflag, uint32_
         for (int tx = x0; tx <= x1; ++tx) tflag[ty * ntx + tx] = epoch;
 }
 
+// The records in two passes. A wet padded cell is a ghost copy of a wet
+// interior cell within 2 of the edge (mirror or copy), and every tile whose
+// read range holds the ghost also holds its source, so the interior cells'
+// marks are all the marks. Pass 1 (the scan) reads every interior cell's
+// five fields -- the NaN check -- and marks; pass 2 builds the records of
+// the padded cells an active tile reads, and no others: far from the flow
+// a cell costs its 40 bytes of state and nothing more.
+// a cell's column and row are only worked out when it is wet (the marks);
+// a dry cell costs its five loads and the NaN test
+__device__ __forceinline__ bool scan_cell(const dclaw_params& P, const double* __restrict__ q, size_t plane,
+                                          size_t c, int mx, uint32_t* __restrict__ tflag, const dclaw_clock* clk,
+                                          int TX, int TY, int ntx, int nty) {
+    const double h = q[c], hu = q[plane + c], hv = q[2 * plane + c], hm = q[3 * plane + c], pb = q[4 * plane + c];
+    if (h > P.dry_tolerance) {
+        int i, j;
+        split_index((long long)c, mx, i, j);
+        mark_tiles(tflag, clk->nsteps + 1u, i + 1, j + 1, TX, TY, ntx, nty);
+    }
+    return (h != h) || (hu != hu) || (hv != hv) || (hm != hm) || (pb != pb);
+}
+
+// Pass 2 of the records works tile by tile: a tile builds the records of
+// the padded cells it owns -- its own cells, and the ghost cells beside it
+// when it lies on the patch edge -- when it or one of its eight neighbours
+// is active. A tile that reads a cell (within 3 of it) is the cell's owner
+// or a neighbour of the owner (tiles are wider than 3), so every record an
+// active tile reads is built, once.
+__device__ __forceinline__ bool near_active(const uint32_t* __restrict__ tflag, uint32_t epoch, int tx, int ty,
+                                            int ntx, int nty) {
+    bool act = false;
+    for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+            const int x = tx + dx, y = ty + dy;
+            if (x >= 0 && y >= 0 && x < ntx && y < nty) act |= tflag[y * ntx + x] == epoch;
+        }
+    return act;
+}
+
+// the records of the cells tile (tx, ty) owns (all threads of the CTA)
+template <int TX, int TY>
+__device__ __forceinline__ void tile_records(const dclaw_params& P, const Geom& g, const double* __restrict__ q_in,
+                                             const double* __restrict__ b, const Rec& R, int tx, int ty, int ntx,
+                                             int nty) {
+    const int i0 = 1 + tx * TX, j0 = 1 + ty * TY;
+    const int xa = tx == 0 ? -1 : i0, xb = tx == ntx - 1 ? g.mx + 2 : i0 + TX - 1;
+    const int ya = ty == 0 ? -1 : j0, yb = ty == nty - 1 ? g.my + 2 : j0 + TY - 1;
+    const int w = xb - xa + 1, n = w * (yb - ya + 1);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int r = k / w;
+        cell_record(P, g, q_in, b, R, xa + (k - r * w), ya + r);
+    }
+}
+
 __device__ __forceinline__ bool tile_active(const uint32_t* __restrict__ tflag, uint32_t epoch, int i, int j, int TX,
                                             int TY, int ntx) {
     return !tflag || tflag[((j - 1) / TY) * ntx + (i - 1) / TX] == epoch;
@@ -224,8 +277,9 @@ __global__ void k_clock_init(dclaw_clock* clk, double t, double dt, double t_fin
 }
 
 // ---- fused step: K1 cell records + K2 tiles --------------------------------
-// prow0 / nprow: the padded rows (0 .. my+3 for j = -1 .. my+2) this launch
-// covers, all of them by default
+// Records of every padded cell, and the marks. prow0 / nprow: the padded
+// rows (0 .. my+3 for j = -1 .. my+2) this launch covers, all of them by
+// default.
 __global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_records(dclaw_params P, Geom g, const double* __restrict__ q_in,
                                                  const double* __restrict__ b, Rec R, dclaw_clock* clk,
                                                  uint32_t* __restrict__ tflag, int prow0 = 0, int nprow = -1) {
@@ -455,29 +509,84 @@ __device__ __forceinline__ void load_member(const dclaw_member* __restrict__ mem
 // table (read through the cache; all threads of a block share the chunk, so
 // the search is uniform) and reads the member's entry and parameters in
 // place: no shared-memory broadcast and no barrier per chunk.
-__global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_records_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
-                                                       const dclaw_params* __restrict__ prm, dclaw_clock* clocks,
-                                                       const double* __restrict__ q_in, const double* __restrict__ b,
-                                                       double* __restrict__ work, unsigned int* counters,
-                                                       uint32_t* __restrict__ tflag, int TX, int TY) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) counters[0] = 0u;  // the tile queue of this step
-    for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-        const int m = find_member(nmem, ch, [&](int k) { return mem[k].rchunk0; });
+// the member owning chunk ch, starting from the previous chunk's member m
+// (grid-stride loops mostly stay inside one member: no search then)
+template <typename F>
+__device__ __forceinline__ int member_of(int nmem, uint32_t nchunks, uint32_t ch, int m, F first) {
+    if (m >= 0 && first(m) <= ch && ch < (m + 1 < nmem ? first(m + 1) : nchunks)) return m;
+    return find_member(nmem, ch, first);
+}
+
+// After the scan: the active tiles (for the tile kernel) and the tiles
+// whose records an active tile reads (for pass 2), each appended to its
+// list in one warp-aggregated atomic per warp. One thread per tile.
+__global__ void __launch_bounds__(TPB) k_list_batch(int nmem, uint32_t ntiles, const dclaw_member* __restrict__ mem,
+                                                    const dclaw_clock* clocks, const uint32_t* __restrict__ tflag,
+                                                    unsigned int* counters, uint32_t* __restrict__ list_act,
+                                                    uint32_t* __restrict__ list_rec) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    bool act = false, rec = false;
+    if (t < ntiles) {
+        const int m = find_member(nmem, t, [&](int k) { return mem[k].tile0; });
+        const dclaw_member& M = mem[m];
+        const uint32_t epoch = clocks[m].nsteps + 1u;
+        const int ntx = (int)M.ntiles_x, lt = (int)(t - M.tile0);
+        act = tflag[t] == epoch;
+        rec = act || near_active(tflag + M.tile0, epoch, lt % ntx, lt / ntx, ntx, (int)(M.ntiles / M.ntiles_x));
+    }
+    const int lane = threadIdx.x & 31;
+    const unsigned ba = __ballot_sync(0xffffffffu, act), br = __ballot_sync(0xffffffffu, rec);
+    unsigned base_a = 0, base_r = 0;
+    if (lane == 0) {
+        if (ba) base_a = atomicAdd(counters + 1, (unsigned)__popc(ba));
+        if (br) base_r = atomicAdd(counters + 2, (unsigned)__popc(br));
+    }
+    base_a = __shfl_sync(0xffffffffu, base_a, 0);
+    base_r = __shfl_sync(0xffffffffu, base_r, 0);
+    const unsigned below = (1u << lane) - 1u;
+    if (act) list_act[base_a + __popc(ba & below)] = t;
+    if (rec) list_rec[base_r + __popc(br & below)] = t;
+}
+
+// pass 2 of the records over the listed tiles (grid-stride over the list)
+template <int TX, int TY>
+__global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_records_tiles_batch(int nmem, uint32_t ntiles,
+                                                                              const dclaw_member* __restrict__ mem,
+                                                                              const dclaw_params* __restrict__ prm,
+                                                                              const double* __restrict__ q_in,
+                                                                              const double* __restrict__ b,
+                                                                              double* __restrict__ work,
+                                                                              const unsigned int* counters,
+                                                                              const uint32_t* __restrict__ list_rec) {
+    const uint32_t n = counters[2];
+    int m = -1;
+    for (uint32_t k = blockIdx.x; k < n; k += gridDim.x) {
+        const uint32_t t = list_rec[k];
+        m = member_of(nmem, ntiles, t, m, [&](int j) { return mem[j].tile0; });
         const dclaw_member& M = mem[m];
         const Geom g{M.mx, M.my, M.mx + 4, M.my + 4, M.dx, M.dy};
-        const size_t npad = (size_t)g.PX * g.PY;
-        const Rec R{work + M.rec_off, npad};
-        const size_t idx = (size_t)(ch - M.rchunk0) * TPB + threadIdx.x;
-        if (idx < npad) {
-            int i, j;
-            split_index((long long)idx, g.PX, i, j);
-            i -= 1;
-            j -= 1;
-            if (cell_record(prm[m], g, q_in + M.q_off, b + M.b_off, R, i, j)) flag_status(clocks + m, DCLAW_ERR_NAN);
-            if (R.get(R_H, pidx(g, i, j)) > 0.0)
-                mark_tiles(tflag + M.tile0, clocks[m].nsteps + 1u, i, j, TX, TY, (int)M.ntiles_x,
-                           (int)(M.ntiles / M.ntiles_x));
-        }
+        const Rec R{work + M.rec_off, (size_t)g.PX * g.PY};
+        const int ntx = (int)M.ntiles_x, lt = (int)(t - M.tile0);
+        tile_records<TX, TY>(prm[m], g, q_in + M.q_off, b + M.b_off, R, lt % ntx, lt / ntx, ntx,
+                             (int)(M.ntiles / M.ntiles_x));
+    }
+}
+
+// pass 1 of the two-pass records over every member's interior chunks
+__global__ void __launch_bounds__(TPB) k_scan_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
+                                                    const dclaw_params* __restrict__ prm, dclaw_clock* clocks,
+                                                    const double* __restrict__ q_in, unsigned int* counters,
+                                                    uint32_t* __restrict__ tflag, int TX, int TY) {
+    if (blockIdx.x == 0 && threadIdx.x < 3) counters[threadIdx.x] = 0u;  // tile queue and list lengths
+    int m = -1;
+    for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+        m = member_of(nmem, nchunks, ch, m, [&](int k) { return mem[k].schunk0; });
+        const dclaw_member& M = mem[m];
+        const size_t n = (size_t)M.mx * M.my;
+        const size_t idx = (size_t)(ch - M.schunk0) * TPB + threadIdx.x;
+        if (idx < n && scan_cell(prm[m], q_in + M.q_off, n, idx, M.mx, tflag + M.tile0, clocks + m, TX, TY,
+                                 (int)M.ntiles_x, (int)(M.ntiles / M.ntiles_x)))
+            flag_status(clocks + m, DCLAW_ERR_NAN);
     }
 }
 
@@ -485,28 +594,27 @@ template <int TX, int TY>
 __global__ void __launch_bounds__(TPB, 2) k_tile_batch(int nmem, uint32_t ntiles, const dclaw_member* __restrict__ mem,
                                                        const dclaw_params* __restrict__ prm, dclaw_clock* clocks,
                                                        const double* __restrict__ b, double* __restrict__ work,
-                                                       unsigned int* counters, const uint32_t* __restrict__ tflag) {
+                                                       unsigned int* counters, const uint32_t* __restrict__ list_act) {
     extern __shared__ double smem[];
     __shared__ dclaw_member sM;
     __shared__ dclaw_params sP;
     __shared__ unsigned int s_t;
     __shared__ int s_m;
     __shared__ double red[TPB / 32];
+    // the queue hands out the active tiles only (inactive tiles: no wet
+    // cell within 3; src2 writes their zeros)
+    const unsigned int nact = counters[1];
     int cur = -1;
     for (;;) {
         if (threadIdx.x == 0) {
-            s_t = atomicAdd(counters, 1u);
-            s_m = s_t < ntiles ? find_member(nmem, s_t, [&](int k) { return mem[k].tile0; }) : -1;
+            const unsigned int k = atomicAdd(counters, 1u);
+            s_t = k < nact ? list_act[k] : ntiles;
+            s_m = s_t < ntiles ? find_member(nmem, s_t, [&](int j) { return mem[j].tile0; }) : -1;
         }
         __syncthreads();
         const unsigned int t = s_t;
         const int m = s_m;
         if (t >= ntiles) break;
-        // inactive tiles (no wet cell within 3): src2 writes their zeros
-        if (tflag[t] != clocks[m].nsteps + 1u) {
-            __syncthreads();
-            continue;
-        }
         if (m != cur) {
             load_member(mem, prm, m, sM, sP);
             __syncthreads();
@@ -536,12 +644,14 @@ __global__ void __launch_bounds__(TPB, 2) k_tile_batch(int nmem, uint32_t ntiles
     }
 }
 
+template <int TX, int TY>
 __global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_src2_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
                                                     const dclaw_params* __restrict__ prm, const dclaw_clock* clocks,
                                                     double* __restrict__ q_out, const double* __restrict__ work,
-                                                    const uint32_t* __restrict__ tflag, int TX, int TY) {
+                                                    const uint32_t* __restrict__ tflag) {
+    int m = -1;
     for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-        const int m = find_member(nmem, ch, [&](int k) { return mem[k].schunk0; });
+        m = member_of(nmem, nchunks, ch, m, [&](int k) { return mem[k].schunk0; });
         const dclaw_member& M = mem[m];
         const Geom g{M.mx, M.my, M.mx + 4, M.my + 4, M.dx, M.dy};
         const size_t n = (size_t)g.mx * g.my;
@@ -583,13 +693,31 @@ inline int batch_tile_attr() {
 
 template <int TX, int TY>
 inline int launch_tile_batch(const dclaw_batch* B, const dclaw_member* mem, const dclaw_params* prm, dclaw_clock* clocks,
-                             const double* b, double* work, unsigned int* counters, const uint32_t* tflag, int nsm,
+                             const double* b, double* work, unsigned int* counters, const uint32_t* list_act, int nsm,
                              cudaStream_t s) {
     if (batch_tile_attr<TX, TY>() != DCLAW_OK) return DCLAW_ERR_CUDA;
     unsigned grid = (unsigned)(nsm * (B->tile_ctas_per_sm > 0 ? B->tile_ctas_per_sm : 2));
     if (grid > B->ntiles) grid = B->ntiles > 0 ? B->ntiles : 1;
     k_tile_batch<TX, TY><<<grid, TPB, TileGeom<TX, TY>::SMEM_BYTES, s>>>(B->nmembers, B->ntiles, mem, prm, clocks, b,
-                                                                        work, counters, tflag);
+                                                                        work, counters, list_act);
+    return DCLAW_OK;
+}
+
+// the records the active tiles read, the tiles, src2 (after the scan and
+// the lists)
+template <int TX, int TY>
+inline int launch_batch_tiles(const dclaw_batch* B, const dclaw_member* mem, const dclaw_params* prm,
+                              dclaw_clock* clocks, const double* q_in, double* q_out, const double* b, double* w,
+                              unsigned int* counters, const uint32_t* tflag, const uint32_t* list_act,
+                              const uint32_t* list_rec, int nsm, int cpsm, cudaStream_t s) {
+    unsigned g1 = (unsigned)(nsm * cpsm);
+    if (g1 > B->ntiles) g1 = B->ntiles > 0 ? B->ntiles : 1;
+    k_records_tiles_batch<TX, TY><<<g1, TPB, 0, s>>>(B->nmembers, B->ntiles, mem, prm, q_in, b, w, counters, list_rec);
+    int rc = launch_tile_batch<TX, TY>(B, mem, prm, clocks, b, w, counters, list_act, nsm, s);
+    if (rc != DCLAW_OK) return rc;
+    unsigned g3 = (unsigned)(nsm * cpsm);
+    if (g3 > B->nschunks) g3 = B->nschunks;
+    k_src2_batch<TX, TY><<<g3, TPB, 0, s>>>(B->nmembers, B->nschunks, mem, prm, clocks, q_out, w, tflag);
     return DCLAW_OK;
 }
 
@@ -1237,8 +1365,9 @@ int dclaw_batch_layout(int n, const int32_t* mx, const int32_t* my, const double
     batch->nschunks = sch;
     batch->q_doubles = q;
     batch->b_doubles = bb;
-    // + the tile activity flags, then the work-queue counters
-    batch->work_bytes = w * 8 + align256((size_t)tiles * 4) + 256;
+    // + the active-tile and record-tile lists, the tile activity flags, then
+    // the work-queue counters and list lengths
+    batch->work_bytes = w * 8 + 3 * align256((size_t)tiles * 4) + 256;
     return DCLAW_OK;
 }
 
@@ -1260,23 +1389,25 @@ int dclaw_step_batched(const dclaw_batch* batch, const dclaw_member* members, co
     if (nsm <= 0) return DCLAW_ERR_CUDA;
     double* w = (double*)work;
     unsigned int* counters = (unsigned int*)((char*)work + (batch->work_bytes - 256));
-    uint32_t* tflag = (uint32_t*)((char*)work + (batch->work_bytes - 256 - align256((size_t)batch->ntiles * 4)));
+    const size_t tbytes = align256((size_t)batch->ntiles * 4);
+    uint32_t* tflag = (uint32_t*)((char*)counters - tbytes);
+    uint32_t* list_rec = (uint32_t*)((char*)tflag - tbytes);
+    uint32_t* list_act = (uint32_t*)((char*)list_rec - tbytes);
     const int cpsm = batch->cell_ctas_per_sm > 0 ? batch->cell_ctas_per_sm : 8;
     const int TX = batch_tx(batch->tile_shape), TY = batch_ty(batch->tile_shape);
-    unsigned g1 = (unsigned)(nsm * cpsm);
-    if (g1 > batch->nrchunks) g1 = batch->nrchunks;
-    k_records_batch<<<g1, TPB, 0, s>>>(batch->nmembers, batch->nrchunks, members, params, clocks, q_in, b, w, counters,
-                                       tflag, TX, TY);
+    unsigned g0 = (unsigned)(nsm * cpsm);
+    if (g0 > batch->nschunks) g0 = batch->nschunks;
+    k_scan_batch<<<g0, TPB, 0, s>>>(batch->nmembers, batch->nschunks, members, params, clocks, q_in, counters, tflag,
+                                    TX, TY);
+    k_list_batch<<<(unsigned)((batch->ntiles + TPB - 1) / TPB), TPB, 0, s>>>(batch->nmembers, batch->ntiles, members,
+                                                                            clocks, tflag, counters, list_act, list_rec);
     int rc = DCLAW_OK;
     switch (batch->tile_shape) {
-        case 0: rc = launch_tile_batch<batch_tx(0), batch_ty(0)>(batch, members, params, clocks, b, w, counters, tflag, nsm, s); break;
-        case 1: rc = launch_tile_batch<batch_tx(1), batch_ty(1)>(batch, members, params, clocks, b, w, counters, tflag, nsm, s); break;
-        default: rc = launch_tile_batch<batch_tx(2), batch_ty(2)>(batch, members, params, clocks, b, w, counters, tflag, nsm, s); break;
+        case 0: rc = launch_batch_tiles<batch_tx(0), batch_ty(0)>(batch, members, params, clocks, q_in, q_out, b, w, counters, tflag, list_act, list_rec, nsm, cpsm, s); break;
+        case 1: rc = launch_batch_tiles<batch_tx(1), batch_ty(1)>(batch, members, params, clocks, q_in, q_out, b, w, counters, tflag, list_act, list_rec, nsm, cpsm, s); break;
+        default: rc = launch_batch_tiles<batch_tx(2), batch_ty(2)>(batch, members, params, clocks, q_in, q_out, b, w, counters, tflag, list_act, list_rec, nsm, cpsm, s); break;
     }
     if (rc != DCLAW_OK) return rc;
-    unsigned g3 = (unsigned)(nsm * cpsm);
-    if (g3 > batch->nschunks) g3 = batch->nschunks;
-    k_src2_batch<<<g3, TPB, 0, s>>>(batch->nmembers, batch->nschunks, members, params, clocks, q_out, w, tflag, TX, TY);
     k_tick_batch<<<(unsigned)((batch->nmembers + TPB - 1) / TPB), TPB, 0, s>>>(batch->nmembers, params, clocks);
     return cuda_status();
 }

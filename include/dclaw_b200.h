@@ -214,8 +214,10 @@ int dclaw_step_host_bands(int mx, int my, int nbands, int32_t* first, int max);
  * reference's differentiable port: one simulation per particle,
  * gradient_particle_filter/pf_flume/flume_model.py:129-179, vmapped in
  * pf_flume/inference.py:96-108). All members advance together: one step of
- * the ensemble is four launches (cell records, a persistent kernel pulling
- * every member's tiles from one work queue, src2, each member's tick), so a
+ * the ensemble is six launches (a scan of every cell that marks the active
+ * tiles, a list of the active tiles and of the tiles whose records they
+ * read, those records, a persistent kernel pulling the active tiles of
+ * every member from one work queue, src2, each member's tick), so a
  * sequence of ensemble steps captures into one CUDA graph. Tiles with no wet
  * cell within 3 cells are skipped (src2 writes their zeros).
  * Member m's state is 5 planes [5][my][mx] at q_off in the state arenas; its

@@ -61,8 +61,9 @@ def test_layout_covers_every_member(shape):
         rch += M.nrchunks
         sch += M.nschunks
     assert (cb.q_doubles, cb.b_doubles, cb.ntiles, cb.nrchunks, cb.nschunks) == (q, b, tiles, rch, sch)
-    # + one 32-bit activity flag per tile (256-byte aligned), then the work-queue counters
-    assert cb.work_bytes == 8 * w + -(-4 * tiles // 256) * 256 + 256
+    # + two tile lists (active tiles, tiles whose records are built) and one
+    # 32-bit activity flag per tile, each 256-byte aligned, then the counters
+    assert cb.work_bytes == 8 * w + 3 * (-(-4 * tiles // 256) * 256) + 256
 
 
 def test_layout_rejects_bad_members():
