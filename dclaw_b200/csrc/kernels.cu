@@ -573,10 +573,13 @@ __global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_records_tiles_batch(in
 }
 
 // pass 1 of the two-pass records over every member's interior chunks
+// It also writes the zero state into q_out for every cell: the cells of
+// inactive tiles keep it, src2 over the active tiles overwrites the others.
 __global__ void __launch_bounds__(TPB) k_scan_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
                                                     const dclaw_params* __restrict__ prm, dclaw_clock* clocks,
-                                                    const double* __restrict__ q_in, unsigned int* counters,
-                                                    uint32_t* __restrict__ tflag, int TX, int TY) {
+                                                    const double* __restrict__ q_in, double* __restrict__ q_out,
+                                                    unsigned int* counters, uint32_t* __restrict__ tflag, int TX,
+                                                    int TY) {
     if (blockIdx.x == 0 && threadIdx.x < 3) counters[threadIdx.x] = 0u;  // tile queue and list lengths
     int m = -1;
     for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
@@ -584,9 +587,13 @@ __global__ void __launch_bounds__(TPB) k_scan_batch(int nmem, uint32_t nchunks, 
         const dclaw_member& M = mem[m];
         const size_t n = (size_t)M.mx * M.my;
         const size_t idx = (size_t)(ch - M.schunk0) * TPB + threadIdx.x;
-        if (idx < n && scan_cell(prm[m], q_in + M.q_off, n, idx, M.mx, tflag + M.tile0, clocks + m, TX, TY,
-                                 (int)M.ntiles_x, (int)(M.ntiles / M.ntiles_x)))
-            flag_status(clocks + m, DCLAW_ERR_NAN);
+        if (idx < n) {
+            if (scan_cell(prm[m], q_in + M.q_off, n, idx, M.mx, tflag + M.tile0, clocks + m, TX, TY, (int)M.ntiles_x,
+                          (int)(M.ntiles / M.ntiles_x)))
+                flag_status(clocks + m, DCLAW_ERR_NAN);
+            double* qo = q_out + M.q_off + idx;
+            for (int f = 0; f < 5; ++f) qo[(size_t)f * n] = 0.0;
+        }
     }
 }
 
@@ -644,28 +651,28 @@ __global__ void __launch_bounds__(TPB, 2) k_tile_batch(int nmem, uint32_t ntiles
     }
 }
 
+// src2 of the active tiles' cells (grid-stride over the active list; the
+// scan has written the zeros of every other cell)
 template <int TX, int TY>
-__global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_src2_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
+__global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_src2_batch(int nmem, uint32_t ntiles, const dclaw_member* __restrict__ mem,
                                                     const dclaw_params* __restrict__ prm, const dclaw_clock* clocks,
                                                     double* __restrict__ q_out, const double* __restrict__ work,
-                                                    const uint32_t* __restrict__ tflag) {
+                                                    const unsigned int* counters,
+                                                    const uint32_t* __restrict__ list_act) {
+    const uint32_t nact = counters[1];
     int m = -1;
-    for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-        m = member_of(nmem, nchunks, ch, m, [&](int k) { return mem[k].schunk0; });
+    for (uint32_t k = blockIdx.x; k < nact; k += gridDim.x) {
+        const uint32_t t = list_act[k];
+        m = member_of(nmem, ntiles, t, m, [&](int j) { return mem[j].tile0; });
         const dclaw_member& M = mem[m];
         const Geom g{M.mx, M.my, M.mx + 4, M.my + 4, M.dx, M.dy};
-        const size_t n = (size_t)g.mx * g.my;
-        const size_t idx = (size_t)(ch - M.schunk0) * TPB + threadIdx.x;
-        if (idx < n) {
-            int i, j;
-            split_index((long long)idx, g.mx, i, j);
-            i += 1;
-            j += 1;
-            if (tile_active(tflag + M.tile0, clocks[m].nsteps + 1u, i, j, TX, TY, (int)M.ntiles_x)) {
-                cell_src2(prm[m], g, clocks[m].dt, work + M.qs_off, q_out + M.q_off, idx);
-            } else {
-                for (int f = 0; f < 5; ++f) q_out[M.q_off + (size_t)f * n + idx] = 0.0;
-            }
+        const int lt = (int)(t - M.tile0), ntx = (int)M.ntiles_x;
+        const int i0 = 1 + (lt % ntx) * TX, j0 = 1 + (lt / ntx) * TY;
+        const double dt = clocks[m].dt;
+        for (int c = threadIdx.x; c < TX * TY; c += blockDim.x) {
+            const int i = i0 + c % TX, j = j0 + c / TX;
+            if (i > g.mx || j > g.my) continue;
+            cell_src2(prm[m], g, dt, work + M.qs_off, q_out + M.q_off, (size_t)(j - 1) * g.mx + (size_t)(i - 1));
         }
     }
 }
@@ -716,8 +723,8 @@ inline int launch_batch_tiles(const dclaw_batch* B, const dclaw_member* mem, con
     int rc = launch_tile_batch<TX, TY>(B, mem, prm, clocks, b, w, counters, list_act, nsm, s);
     if (rc != DCLAW_OK) return rc;
     unsigned g3 = (unsigned)(nsm * cpsm);
-    if (g3 > B->nschunks) g3 = B->nschunks;
-    k_src2_batch<TX, TY><<<g3, TPB, 0, s>>>(B->nmembers, B->nschunks, mem, prm, clocks, q_out, w, tflag);
+    if (g3 > B->ntiles) g3 = B->ntiles > 0 ? B->ntiles : 1;
+    k_src2_batch<TX, TY><<<g3, TPB, 0, s>>>(B->nmembers, B->ntiles, mem, prm, clocks, q_out, w, counters, list_act);
     return DCLAW_OK;
 }
 
@@ -1397,8 +1404,8 @@ int dclaw_step_batched(const dclaw_batch* batch, const dclaw_member* members, co
     const int TX = batch_tx(batch->tile_shape), TY = batch_ty(batch->tile_shape);
     unsigned g0 = (unsigned)(nsm * cpsm);
     if (g0 > batch->nschunks) g0 = batch->nschunks;
-    k_scan_batch<<<g0, TPB, 0, s>>>(batch->nmembers, batch->nschunks, members, params, clocks, q_in, counters, tflag,
-                                    TX, TY);
+    k_scan_batch<<<g0, TPB, 0, s>>>(batch->nmembers, batch->nschunks, members, params, clocks, q_in, q_out, counters,
+                                    tflag, TX, TY);
     k_list_batch<<<(unsigned)((batch->ntiles + TPB - 1) / TPB), TPB, 0, s>>>(batch->nmembers, batch->ntiles, members,
                                                                             clocks, tflag, counters, list_act, list_rec);
     int rc = DCLAW_OK;
