@@ -41,6 +41,10 @@ constexpr int MAX_DEVICES = 64;
 #define DCLAW_SRC2_KERNEL 1
 #endif
 constexpr int TILE_X = DCLAW_TILE_X, TILE_Y = DCLAW_TILE_Y;
+// resident blocks per SM the ensemble's streaming scan is sized for
+#ifndef DCLAW_SCAN_MINB
+#define DCLAW_SCAN_MINB 4
+#endif
 // resident blocks per SM the per-cell kernels (records, src2) are sized for
 #ifndef DCLAW_CELL_MINB
 #define DCLAW_CELL_MINB 4
@@ -575,7 +579,7 @@ __global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_records_tiles_batch(in
 // pass 1 of the two-pass records over every member's interior chunks
 // It also writes the zero state into q_out for every cell: the cells of
 // inactive tiles keep it, src2 over the active tiles overwrites the others.
-__global__ void __launch_bounds__(TPB) k_scan_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
+__global__ void __launch_bounds__(TPB, DCLAW_SCAN_MINB) k_scan_batch(int nmem, uint32_t nchunks, const dclaw_member* __restrict__ mem,
                                                     const dclaw_params* __restrict__ prm, dclaw_clock* clocks,
                                                     const double* __restrict__ q_in, double* __restrict__ q_out,
                                                     unsigned int* counters, uint32_t* __restrict__ tflag, int TX,
