@@ -73,6 +73,10 @@ def parse():
                     help="members of the batched-gradient channel case (0: skip)")
     ap.add_argument("--bgrad-steps", type=int, default=200,
                     help="steps of the batched-gradient case (the case is defined over 800)")
+    ap.add_argument("--slab-steps", type=int, default=0,
+                    help="also step ONE patch of the case split into row slabs over the N ranks "
+                         "(strong scaling; halo exchange + Courant max per step); 0: skip")
+    ap.add_argument("--slab-count", type=int, default=8, help="slabs of the one-GPU slab measurement")
     ap.add_argument("--only", default="", choices=["", "batched", "gradient", "batched_gradient"],
                     help="run one side measurement alone and print its object (profiling runs)")
     return ap.parse_args()
@@ -461,6 +465,44 @@ def batched_gradient_bench(args, dev):
             "note": "every member's dt from its own tick rule, recorded and replayed, not differentiated"}
 
 
+def slab_bench(args, dev, rank, world, barrier):
+    """ONE patch of the case (the same on every rank) split into row slabs
+    over the ranks: halo exchange, own rows, Courant max, tick per step
+    (strong scaling). On one rank, the patch as `--slab-count` slabs stepped
+    one after another on the one GPU: the work the halos add."""
+    import torch
+
+    from dclaw_b200.replicas import max_over_ranks
+    from dclaw_b200.slabs import DistSlabs, LocalSlabs
+
+    case = make_case(args, 0)
+    q = torch.tensor(case.q, device=dev)
+    b = torch.tensor(case.b, device=dev)
+    if world > 1:
+        sl = DistSlabs(q, b, case.params, case.dx, case.dy)
+        nslab = world
+    else:
+        sl = LocalSlabs(q, b, case.params, case.dx, case.dy, args.slab_count)
+        nslab = args.slab_count
+    del q, b
+    sl.init_clock(case.dt_initial)
+    sl.step(args.warmup)
+    barrier()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sl.step(args.slab_steps)
+    e1.record(stream)
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1), dev)
+    cells = case.mx * case.my
+    return {"workload": f"random_field_{case.mx}x{case.my}_dx{case.dx}", "slabs": nslab, "ranks": world,
+            "halo_rows": 14, "steps": args.slab_steps, "ms_per_step": ms / args.slab_steps,
+            "value": cells * args.slab_steps / (ms / 1000.0), "unit": "cell-updates/s",
+            "scaling": "strong" if world > 1 else "one GPU, slabs in turn",
+            "gpu_launches_per_step_per_slab": 4}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -584,6 +626,10 @@ def run_ours(args):
                           "frac_of_copy_floor": copy_floor_ms / e2e_ms,
                           "copy_floor_note": "the state copied host->device and device->host at once on two "
                                              "streams, no compute: the PCIe bound of the e2e step"}
+    if args.slab_steps > 0:
+        sl = slab_bench(args, dev, rank, world, barrier)
+        if rank == 0:
+            out["one_patch_slabs"] = sl
     if world > 1:
         dist.barrier()
     if rank == 0 and world == 1 and args.ensemble_members > 0:

@@ -40,6 +40,9 @@ SIGNATURES = {
     "dclaw_step_host": (_int, [_vp, _vp, _vp, _int, _int, _dbl, _dbl, _pp, _vp, _vp, _sz, _int, _vp]),
     "dclaw_step_host_workspace_bytes": (_sz, [_int, _int]),
     "dclaw_step_host_bands": (_int, [_int, _int, _int, _vp, _int]),
+    "dclaw_rows_granule": (_int, []),
+    "dclaw_step_rows": (_int, [_vp, _vp, _vp, _int, _int, _dbl, _dbl, _pp, _vp, _vp, _sz, _int, _int, _vp]),
+    "dclaw_clock_tick": (_int, [_vp, _pp, _vp]),
     "dclaw_batch_tile_shapes": (_int, [_vp, _vp, _int]),
     "dclaw_batch_layout": (_int, [_int, _vp, _vp, _vp, _vp, _int, ctypes.POINTER(CMember), ctypes.POINTER(CBatch)]),
     "dclaw_step_batched": (_int, [ctypes.POINTER(CBatch), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -1188,6 +1188,52 @@ int dclaw_step_host(const double* q_in, double* q_out, const double* b, int mx, 
     return e == cudaSuccess ? cuda_status() : DCLAW_ERR_CUDA;
 }
 
+int dclaw_rows_granule(void) { return TILE_Y; }
+
+int dclaw_step_rows(const double* q_in, double* q_out, const double* b, int mx, int my, double dx, double dy,
+                    const dclaw_params* p, dclaw_clock* clock, void* work, size_t work_bytes, int row_first,
+                    int row_count, void* stream) {
+    if (!q_in || !q_out || !b || !p || !clock || !work || q_in == q_out) return DCLAW_ERR_ARG;
+    if (!sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0)) return DCLAW_ERR_ARG;
+    // whole tile rows: the first row starts a tile row and the range ends on
+    // a tile-row boundary or at the patch's last row
+    const int last = row_first + row_count - 1;
+    if (row_first < 1 || row_count < 1 || last > my || (row_first - 1) % TILE_Y != 0 ||
+        (last != my && last % TILE_Y != 0))
+        return DCLAW_ERR_ARG;
+    int rc = dclaw_params_check(p);
+    if (rc) return rc;
+    Layout L = layout(mx, my);
+    if (work_bytes < L.total_fused) return DCLAW_ERR_WORKSPACE;
+    if (ensure_tile_smem_attr() != DCLAW_OK) return DCLAW_ERR_CUDA;
+    cudaStream_t s = (cudaStream_t)stream;
+    Geom g{mx, my, mx + 4, my + 4, dx, dy};
+    Rec R{(double*)((char*)work + L.off_rec), L.npad};
+    const dclaw_params P = *p;
+    using TG = TileGeom<TILE_X, TILE_Y>;
+    uint32_t* tflag = (uint32_t*)((char*)work + L.off_tflag);
+    double* qstar = (double*)((char*)work + L.off_qstar);
+    // the records of the rows the range's tiles read (3 beyond it), the
+    // range's tiles, its cells' src2; no tick
+    const int ja = row_first - 3 > -1 ? row_first - 3 : -1, jb = last + 3 < my + 2 ? last + 3 : my + 2;
+    const int nrow = jb - ja + 1;
+    k_records<<<nblocks((long long)g.PX * nrow), TPB, 0, s>>>(P, g, q_in, b, R, clock, tflag, ja + 1, nrow);
+    const int ty0 = (row_first - 1) / TILE_Y, nty = (last - 1) / TILE_Y - ty0 + 1;
+    k_tile<TILE_X, TILE_Y, false><<<dim3((mx + TILE_X - 1) / TILE_X, nty), TILE_TPB, TG::SMEM_BYTES, s>>>(
+        P, g, R, b, qstar, clock, nullptr, tflag, ty0);
+    const long long nc = (long long)row_count * mx;
+    k_src2_cells<<<nblocks(nc), TPB, 0, s>>>(P, g, qstar, q_out, clock, tflag, (long long)(row_first - 1) * mx, nc, 0);
+    return cuda_status();
+}
+
+int dclaw_clock_tick(dclaw_clock* clock, const dclaw_params* p, void* stream) {
+    if (!clock || !p) return DCLAW_ERR_ARG;
+    int rc = dclaw_params_check(p);
+    if (rc) return rc;
+    k_tick<<<1, 32, 0, (cudaStream_t)stream>>>(*p, clock);
+    return cuda_status();
+}
+
 int dclaw_bc2amr(double* q, int mx, int my, int mbc, const dclaw_params* p, void* stream) {
     if (!q || !p || mbc != 2 || !sizes_ok(mx, my)) return DCLAW_ERR_ARG;
     int rc = dclaw_params_check(p);

@@ -204,6 +204,32 @@ int dclaw_step_host(const double* q_in, double* q_out, const double* b, int mx, 
                     double dx, double dy, const dclaw_params* p, dclaw_clock* clock,
                     void* work, size_t work_bytes, int nbands, void* stream);
 size_t dclaw_step_host_workspace_bytes(int mx, int my);
+/* ---- one patch over several GPUs (row slabs) ------------------------------
+ * A patch too large for one GPU splits into slabs of whole tile rows, one per
+ * GPU. Each GPU holds its rows plus a halo of dclaw_rows_granule() rows on
+ * each side that lies inside the patch (the step reads at most 4 rows away),
+ * as a patch of its own: its own mx x my_local state, bed and workspace, its
+ * edges at the patch's edges keeping the patch's boundary conditions. Per
+ * step every GPU receives its halo rows from its neighbours, calls
+ * dclaw_step_rows for its own rows, max-reduces clock->cfl_bits over the GPUs
+ * (the order-preserving bit pattern of the non-negative Courant number, so
+ * an integer max), and calls dclaw_clock_tick. The result equals dclaw_step
+ * on the whole patch, bit for bit, with the same dt: the reference's patch
+ * advance likewise computes cflgrid per patch and takes the largest for the
+ * level's next dt (GeoClaw's advanc, called from tick.f:333). */
+/* rows per tile row: row ranges of dclaw_step_rows start and end on multiples */
+int dclaw_rows_granule(void);
+/* dclaw_step for rows row_first .. row_first+row_count-1 (1-based) of the
+ * patch only: row_first - 1 is a multiple of dclaw_rows_granule(), and the
+ * range ends on one or at the last row. Those rows of q_out are written (the
+ * others are left as they are), their tiles' Courant number is max-reduced
+ * into clock->cfl_bits, and the clock is NOT ticked. Workspace: as dclaw_step. */
+int dclaw_step_rows(const double* q_in, double* q_out, const double* b, int mx, int my,
+                    double dx, double dy, const dclaw_params* p, dclaw_clock* clock,
+                    void* work, size_t work_bytes, int row_first, int row_count, void* stream);
+/* the tick rule after dclaw_step_rows: t += dt, cfl from cfl_bits, the next dt
+ * (tick.f:490-526), cfl_bits cleared */
+int dclaw_clock_tick(dclaw_clock* clock, const dclaw_params* p, void* stream);
 /* the band plan dclaw_step_host uses: returns the band count nb and writes
  * the first tile row of each band to first[0..nb] (first[nb] = tile rows),
  * at most `max` entries; 0 for an invalid size */
