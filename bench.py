@@ -309,10 +309,10 @@ def gradient_bench(args, dev):
 
     used_k = []
 
-    def gauges(h, m0, theta):
+    def gauges(h, m0, theta, block=blk):
         q0 = initial_state(h, m0, p)
         out = rollout_states(q0, theta, b, p, c.dx, c.dx, c.nsteps, c.out_steps, c.dt_initial,
-                             checkpoint_block=blk, select=sel)
+                             checkpoint_block=block, select=sel)
         if out.grad_fn is not None:
             used_k.append(checkpoint_block_of(out))
         return out
@@ -347,10 +347,27 @@ def gradient_bench(args, dev):
         grad_ms.append(e0.elapsed_time(e1))
     f, g = min(fwd_ms), min(grad_ms)
     k = used_k[-1]
+    # the same gradient with two-level sqrt(N) checkpoints (the memory
+    # minimum: every block's states recomputed once in the backward pass)
+    ksq = max(1, math.ceil(math.sqrt(c.nsteps)))
+    sq_ms = []
+    for _ in range(2):
+        hs = h0.clone().requires_grad_(True)
+        ms0 = torch.tensor(c.m0, dtype=torch.float64, device=dev, requires_grad=True)
+        ths = theta_of(p, dev).requires_grad_(True)
+        torch.cuda.synchronize()
+        e0 = ev()
+        ((gauges(hs, ms0, ths, ksq) - target) ** 2).sum().backward()
+        e1 = ev()
+        torch.cuda.synchronize()
+        sq_ms.append(e0.elapsed_time(e1))
+    same = bool(torch.equal(ths.grad, theta.grad) and torch.equal(hs.grad, h.grad))
     mx, my = c.b.shape[1], c.b.shape[0]
     return {"workload": f"gauge_loss_{mx}x{my}_dx{c.dx}_{c.nsteps}steps", "gauges": len(c.gauges),
             "output_times": len(c.out_steps), "checkpoint_block": k, "forward_ms": f, "gradient_ms": g,
             "gradient_over_forward": g / f, "loss": float(loss.detach()),
+            "sqrt_n_checkpoints": {"checkpoint_block": ksq, "gradient_ms": min(sq_ms),
+                                   "gradient_over_forward": min(sq_ms) / f, "same_gradient_bits": same},
             "grad": {"phi_deg": float(theta.grad[0]), "kref": float(theta.grad[1]), "m0": float(m0.grad),
                      "alpha_c": float(theta.grad[2]), "h0_l2": float(h.grad.norm())},
             "peak_mem_gb": torch.cuda.max_memory_allocated(dev) / 1e9,

@@ -163,23 +163,26 @@ class _Rollout(torch.autograd.Function):
             for idx in where.get(n + 1, []):
                 outs[idx].copy_(pick(src))
         _lib.check(st.status(), "rollout forward")
-        ctx.save_for_backward(b, dts)
-        ctx.ckpt = ckpt
+        # the block inputs are saved tensors: autograd frees them after the
+        # backward pass (unless the graph is retained), so a loop of gradient
+        # evaluations reuses one allocation instead of holding two
+        ctx.save_for_backward(b, dts, store)
         ctx.select = select
         ctx.meta = (prm, float(dx), float(dy), int(n_steps), tuple(out_steps), k)
         return outs
 
     @staticmethod
     def backward(ctx, g_out):
-        b, dts = ctx.saved_tensors
+        b, dts, store = ctx.saved_tensors
+        ckpt = list(store.unbind(0))
         prm, dx, dy, n_steps, out_steps, k = ctx.meta
         dev = b.device
-        shape = ctx.ckpt[0].shape
+        shape = ckpt[0].shape
         where = {}
         for idx, n in enumerate(out_steps):
             where.setdefault(n, []).append(idx)
         adj = StepAdjoint(b, prm, dx, dy)
-        fw = PatchStepper(ctx.ckpt[0], b, prm, dx, dy)
+        fw = PatchStepper(ckpt[0], b, prm, dx, dy)
         fw.init_clock(0.0, fixed_dt=True)
         lam = torch.zeros(shape, dtype=torch.float64, device=dev)
         lam2 = torch.empty_like(lam)
@@ -194,13 +197,13 @@ class _Rollout(torch.autograd.Function):
             else:
                 lam.view(-1).index_add_(0, sel.reshape(-1), g_out[idx].reshape(-1))
 
-        nblocks = len(ctx.ckpt)
+        nblocks = len(ckpt)
         for s in reversed(range(nblocks)):
             n0 = s * k
             n1 = min(n0 + k, n_steps)
             # recompute the block's states n0+1 .. n1-1 from its first input
             # with the recorded dts, each step writing its slot of seg
-            states = [ctx.ckpt[s]]
+            states = [ckpt[s]]
             for n in range(n0 + 1, n1):
                 fw.clock[1:2].copy_(dts[n - 1:n])
                 fw._launch(states[-1], seg[n - n0])
@@ -385,15 +388,15 @@ class _EnsembleRollout(torch.autograd.Function):
                 outs[idx].copy_(pick(src))
         for kk, s in enumerate(st.status()):
             _lib.check(s, f"ensemble rollout, member {kk}")
-        ctx.save_for_backward(dts)
-        ctx.ckpt = ckpt
+        ctx.save_for_backward(dts, store)
         ctx.select = select
         ctx.meta = (members, theta.detach(), int(n_steps), tuple(out_steps), k)
         return outs
 
     @staticmethod
     def backward(ctx, g_out):
-        (dts,) = ctx.saved_tensors
+        dts, store = ctx.saved_tensors
+        ckpt = list(store.unbind(0))
         members, theta, n_steps, out_steps, k = ctx.meta
         dev = dts.device
         where = {}
@@ -414,10 +417,10 @@ class _EnsembleRollout(torch.autograd.Function):
             else:
                 lam.index_add_(0, sel.reshape(-1), g_out[idx].reshape(-1))
 
-        for s in reversed(range(len(ctx.ckpt))):
+        for s in reversed(range(len(ckpt))):
             n0 = s * k
             n1 = min(n0 + k, n_steps)
-            states = [ctx.ckpt[s]]
+            states = [ckpt[s]]
             for n in range(n0 + 1, n1):
                 _clock_field(fw, 1).copy_(dts[n - 1])
                 fw._launch(states[-1], seg[n - n0])
