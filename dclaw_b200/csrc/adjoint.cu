@@ -259,9 +259,12 @@ __host__ __device__ inline AdjLayout adj_layout(int mx, int my) {
     L.off_tdq = o; o += align256((size_t)NTD * L.S.npad * 8);
     L.off_qsb = o; o += align256((size_t)5 * L.S.npad * 8);
     L.off_sv = o; o += align256((size_t)NSV * L.S.npad * 8);
-    L.off_part = o; o += align256((size_t)L.nparts * NPB * 8);
     L.act_nx = (mx + 4 + ACT_TILE - 1) / ACT_TILE;
     L.act_ny = (my + 4 + ACT_TILE - 1) / ACT_TILE;
+    // block partials: per 128-item chunk (single patch) or per activity
+    // block and reverse stage (ensembles), whichever needs more
+    const long long nbp = 4LL * L.act_nx * L.act_ny;
+    L.off_part = o; o += align256((size_t)(L.nparts > nbp ? L.nparts : nbp) * NPB * 8);
     L.off_act = o; o += align256((size_t)L.act_nx * L.act_ny * 4);
     L.total = o;
     return L;
@@ -328,128 +331,258 @@ struct BatchArgs {
     int32_t* status;
 };
 
-// One stage over the chunks of all members (grid-stride; every thread of a
-// block runs the same number of iterations, so the barriers are uniform).
+// ---- ensembles: the stages over lists of 16 x 16 activity blocks ------------
+// A batch step of mostly dry members works only where a member is wet:
+//   1. k_adj_batch_zero   each member's activity map, lam_in, list lengths
+//   2. k_adj_batch_scan   every interior cell; a wet one marks the blocks
+//                         within ACT_REACH (a wet ghost copies a wet interior
+//                         cell within 2 of the edge, whose marks cover the
+//                         ghost's: the padded grid ends 2 cells out)
+//   3. k_adj_batch_list   per member block: the active blocks, and the
+//                         blocks that are active or have an active neighbour
+//   4. the forward recompute and the zeroing of the reverse planes over the
+//      second list, the reverse stages over the first: every item an active
+//      item reads lies within 6 cells of it, inside the second list's
+//      blocks (16 wide), and its own inputs there come from those blocks
+//   5. k_adj_batch_pbar   each member's block partials, in block order.
+// Items are the ones the single-patch stages run; each writes its own slots,
+// so lam_in equals dclaw_step_adjoint member by member, bit for bit, and the
+// parameter adjoints agree to rounding (summed per block, not per chunk).
+constexpr int BLK_PBAR_OPS = 4;   // src2, x solves, y solves, calc_taudir
+
+__device__ __forceinline__ void batch_member_work(const BatchArgs& a, const dclaw_adj_member& M, AdjLayout& L, Work& W,
+                                                  AdjWork& A, uint32_t*& act) {
+    L = adj_layout(M.mx, M.my);
+    char* base = a.work + M.work_off;
+    W = make_work(base, L.S);
+    act = (uint32_t*)(base + L.off_act);
+    A = AdjWork{(double*)(base + L.off_lamq), (double*)(base + L.off_xfb), (double*)(base + L.off_yfb),
+                (double*)(base + L.off_xcb), (double*)(base + L.off_ycb), (double*)(base + L.off_tdq),
+                (double*)(base + L.off_qsb), (double*)(base + L.off_sv), act, L.act_nx};
+}
+
+// one item of stage OP at activity cell (ci, cj) (the padded cell whose
+// block decides the item's activity); false outside the item space
 template <int OP>
-__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_adj_batch(BatchArgs a, uint32_t nchunks) {
+__device__ __forceinline__ void block_item(const BatchArgs& a, int m, const dclaw_adj_member& M, const dclaw_params& P,
+                                           const Geom& g, const Work& W, const AdjWork& A, const AdjLayout& L,
+                                           int ci, int cj, double* pb) {
     constexpr int SP = OpTraits<OP>::SPACE;
+    const int mx = g.mx, my = g.my;
+    const double* q_in = a.q + M.q_off;
+    const double dt = a.dt[m];
+    if (SP == SP_PAD) {
+        if (ci < -1 || cj < -1 || ci > mx + 2 || cj > my + 2) return;
+        if (OP == OP_FW_B4) {
+            if (stage_b4(P, g, q_in, a.b + M.b_off, W, ci, cj) && a.status) atomicCAS(a.status + m, 0, DCLAW_ERR_NAN);
+        } else if (OP == OP_FW_TAUDIR) {
+            stage_taudir(P, g, W, ci, cj);
+        } else if (OP == OP_FW_SVREC) {
+            adj_item_svrec(P, g, W, A, ci, cj);
+        } else if (OP == OP_RV_TAUDIR) {
+            adj_item_taudir(P, g, W, A, ci, cj, pb);
+        } else if (OP == OP_RV_B4) {
+            adj_item_b4(P, g, W, A, q_in, ci, cj);
+        }
+    } else if (SP == SP_INT) {
+        if (ci < 1 || cj < 1 || ci > mx || cj > my) return;
+        if (OP == OP_RV_SRC2) adj_item_src2(P, g, W, A, a.lam_out + M.q_off, ci, cj, dt, pb);
+        else if (OP == OP_RV_GATHER) adj_item_gather(P, g, A, W, a.lam_in + M.q_off, ci, cj);
+    } else if (SP == SP_RX) {
+        if (ci < 0 || cj < 0 || ci > mx + 2 || cj > my + 1) return;
+        if (OP == OP_FW_RX) stage_riemann<0>(P, g, W, cj, ci, nullptr, A.sv);
+        else if (!adj_item_riemann<0>(P, g, W, A, cj, ci, pb) && a.status) atomicCAS(a.status + m, 0, DCLAW_ERR_UNSUPPORTED);
+    } else if (SP == SP_RY) {
+        if (ci < 0 || cj < 0 || ci > mx + 1 || cj > my + 2) return;
+        if (OP == OP_FW_RY) stage_riemann<1>(P, g, W, ci, cj, nullptr, A.sv);
+        else if (!adj_item_riemann<1>(P, g, W, A, ci, cj, pb) && a.status) atomicCAS(a.status + m, 0, DCLAW_ERR_UNSUPPORTED);
+    } else if (SP == SP_FX) {
+        if (ci < 1 || cj < 0 || ci > mx + 1 || cj > my + 1) return;
+        if (OP == OP_FW_FX) stage_flux<0>(P, g, W, cj, ci, dt / g.dx, nullptr);
+        else adj_item_flux<0>(P, g, W, A, cj, ci, dt);
+    } else {
+        if (ci < 0 || cj < 1 || ci > mx + 1 || cj > my + 1) return;
+        if (OP == OP_FW_FY) stage_flux<1>(P, g, W, ci, cj, dt / g.dy, nullptr);
+        else adj_item_flux<1>(P, g, W, A, ci, cj, dt);
+    }
+}
+
+// One stage over a list of (member, block) entries (grid-stride; every
+// thread of a CTA runs the same iterations, so the barriers are uniform).
+// A CTA of 128 threads covers a 16 x 16 block in two rows of 8.
+template <int OP>
+__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_adj_blocks(BatchArgs a, const uint64_t* __restrict__ list,
+                                                                     const unsigned int* __restrict__ count) {
     __shared__ dclaw_adj_member sM;
     __shared__ dclaw_params sP;
-    __shared__ int s_m;
+    __shared__ uint64_t s_e;
+    const unsigned int n = *count;
     int cur = -1;
-    for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-        if (threadIdx.x == 0) {
-            int lo = 0, hi = a.nmem - 1;
-            while (lo < hi) {
-                int mid = (lo + hi + 1) >> 1;
-                if (a.mem[mid].chunk0[SP] <= ch) lo = mid;
-                else hi = mid - 1;
-            }
-            s_m = lo;
-        }
+    for (unsigned int k = blockIdx.x; k < n; k += gridDim.x) {
+        if (threadIdx.x == 0) s_e = list[k];
         __syncthreads();
-        const int m = s_m;
+        const int m = (int)(s_e >> 32);
+        const int blk = (int)(s_e & 0xffffffffu);
         if (m != cur) {
             const int nM = (int)(sizeof(dclaw_adj_member) / 4), nP = (int)(sizeof(dclaw_params) / 4);
-            for (int k = threadIdx.x; k < nM + nP; k += blockDim.x) {
-                if (k < nM) reinterpret_cast<int*>(&sM)[k] = reinterpret_cast<const int*>(a.mem + m)[k];
-                else reinterpret_cast<int*>(&sP)[k - nM] = reinterpret_cast<const int*>(a.prm + m)[k - nM];
+            for (int j = threadIdx.x; j < nM + nP; j += blockDim.x) {
+                if (j < nM) reinterpret_cast<int*>(&sM)[j] = reinterpret_cast<const int*>(a.mem + m)[j];
+                else reinterpret_cast<int*>(&sP)[j - nM] = reinterpret_cast<const int*>(a.prm + m)[j - nM];
             }
             __syncthreads();
             cur = m;
         }
-        const int mx = sM.mx, my = sM.my;
-        const Geom g{mx, my, mx + 4, my + 4, sM.dx, sM.dy};
-        const AdjLayout L = adj_layout(mx, my);
-        char* base = a.work + sM.work_off;
-        const Work W = make_work(base, L.S);
-        uint32_t* act = (uint32_t*)(base + L.off_act);
-        const AdjWork A{(double*)(base + L.off_lamq), (double*)(base + L.off_xfb), (double*)(base + L.off_yfb),
-                        (double*)(base + L.off_xcb), (double*)(base + L.off_ycb), (double*)(base + L.off_tdq),
-                        (double*)(base + L.off_qsb), (double*)(base + L.off_sv), act, L.act_nx};
-        const uint32_t lch = ch - sM.chunk0[SP];
-        const long long idx = (long long)lch * ATPB + threadIdx.x;
-        const double* q_in = a.q + sM.q_off;
+        const Geom g{sM.mx, sM.my, sM.mx + 4, sM.my + 4, sM.dx, sM.dy};
+        AdjLayout L;
+        Work W;
+        AdjWork A;
+        uint32_t* act;
+        batch_member_work(a, sM, L, W, A, act);
+        const int bx = blk % L.act_nx, by = blk / L.act_nx;
+        const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
         double pb[NPB] = {0.0, 0.0, 0.0, 0.0};
-        if (idx < space_items(SP, mx, my)) {
-            const double dt = a.dt[m];
-            if (SP == SP_PAD) {
-                const int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
-                if (OP == OP_FW_B4) {
-                    if (stage_b4(sP, g, q_in, a.b + sM.b_off, W, i, j) && a.status) atomicCAS(a.status + m, 0, DCLAW_ERR_NAN);
-                } else if (OP == OP_FW_MARK) {
-                    mark_active(sP, g, W, act, L.act_nx, i, j);
-                } else if (OP == OP_FW_TAUDIR) {
-                    stage_taudir(sP, g, W, i, j);
-                } else if (OP == OP_FW_SVREC) {
-                    adj_item_svrec(sP, g, W, A, i, j);
-                } else if (OP == OP_RV_TAUDIR) {
-                    if (adj_active(A, i, j)) adj_item_taudir(sP, g, W, A, i, j, pb);
-                } else if (OP == OP_RV_B4) {
-                    if (adj_active(A, i, j)) adj_item_b4(sP, g, W, A, q_in, i, j);
-                }
-            } else if (SP == SP_INT) {
-                const int i = (int)(idx % mx) + 1, j = (int)(idx / mx) + 1;
-                if (adj_active(A, i, j)) {
-                    if (OP == OP_RV_SRC2) adj_item_src2(sP, g, W, A, a.lam_out + sM.q_off, i, j, dt, pb);
-                    else if (OP == OP_RV_GATHER) adj_item_gather(sP, g, A, W, a.lam_in + sM.q_off, i, j);
-                }
-            } else if (SP == SP_RX || SP == SP_RY) {
-                const int nfast = SP == SP_RX ? mx + 3 : mx + 2;
-                const int af = (int)(idx % nfast), as = (int)(idx / nfast);
-                const int r = SP == SP_RX ? as : af, i = SP == SP_RX ? af : as;
-                constexpr int DIR = SP == SP_RX ? 0 : 1;
-                if (OP == OP_FW_RX || OP == OP_FW_RY) {
-                    stage_riemann<DIR>(sP, g, W, r, i, nullptr, A.sv);
-                } else if (adj_active(A, DIR == 0 ? i : r, DIR == 0 ? r : i)) {
-                    if (!adj_item_riemann<DIR>(sP, g, W, A, r, i, pb) && a.status)
-                        atomicCAS(a.status + m, 0, DCLAW_ERR_UNSUPPORTED);
-                }
-            } else {
-                const int nfast = SP == SP_FX ? mx + 1 : mx + 2;
-                const int af = (int)(idx % nfast), as = (int)(idx / nfast);
-                const int r = SP == SP_FX ? as : af, i = SP == SP_FX ? af + 1 : as + 1;
-                constexpr int DIR = SP == SP_FX ? 0 : 1;
-                if (OP == OP_FW_FX || OP == OP_FW_FY) stage_flux<DIR>(sP, g, W, r, i, DIR == 0 ? dt / g.dx : dt / g.dy, nullptr);
-                else if (adj_active(A, DIR == 0 ? i : r, DIR == 0 ? r : i)) adj_item_flux<DIR>(sP, g, W, A, r, i, dt);
-            }
-        }
+        for (int h = 0; h < ACT_TILE; h += ATPB / ACT_TILE)
+            block_item<OP>(a, m, sM, sP, g, W, A, L, bx * ACT_TILE + tx - 1, by * ACT_TILE + ty + h - 1, pb);
         if (OpTraits<OP>::PBAR) {
-            // the member's block partials, in the single-patch call's order
-            double* part = (double*)(base + L.off_part);
-            const long long off = OP == OP_RV_SRC2 ? 0
-                                  : OP == OP_RV_RX ? L.nb_src2
-                                  : OP == OP_RV_RY ? L.nb_src2 + L.nb_rx
-                                                   : L.nb_src2 + L.nb_rx + L.nb_ry;
-            block_pbar(pb, part + (size_t)(off + lch) * NPB);
+            const int pidx = OP == OP_RV_SRC2 ? 0 : OP == OP_RV_RX ? 1 : OP == OP_RV_RY ? 2 : 3;
+            double* part = (double*)(a.work + sM.work_off + L.off_part);
+            block_pbar(pb, part + ((size_t)pidx * L.act_nx * L.act_ny + blk) * NPB);
         }
         __syncthreads();
     }
 }
 
-// zero member m's reverse planes, block partials, activity map and lam_in
-// (blockIdx.y = m)
-__global__ void __launch_bounds__(256) k_adj_batch_zero(BatchArgs a) {
-    const dclaw_adj_member M = a.mem[blockIdx.y];
-    const AdjLayout L = adj_layout(M.mx, M.my);
-    char* base = a.work + M.work_off;
-    double* p3[3] = {(double*)(base + L.off_lamq), (double*)(base + L.off_part), a.lam_in + M.q_off};
-    const size_t n3[3] = {(L.off_sv - L.off_lamq) / 8, (L.total - L.off_part) / 8, (size_t)5 * M.mx * M.my};
-    for (int k = 0; k < 3; ++k)
-        for (size_t x = (size_t)blockIdx.x * blockDim.x + threadIdx.x; x < n3[k]; x += (size_t)gridDim.x * blockDim.x)
-            p3[k][x] = 0.0;
+// zero the reverse planes of the listed blocks' items (the slots active
+// items read; the rest of the planes is never read)
+__global__ void __launch_bounds__(ATPB) k_adj_blocks_zero(BatchArgs a, const uint64_t* __restrict__ list,
+                                                          const unsigned int* __restrict__ count) {
+    const unsigned int n = *count;
+    for (unsigned int k = blockIdx.x; k < n; k += gridDim.x) {
+        const uint64_t e = list[k];
+        const int m = (int)(e >> 32), blk = (int)(e & 0xffffffffu);
+        const dclaw_adj_member& M = a.mem[m];
+        const Geom g{M.mx, M.my, M.mx + 4, M.my + 4, M.dx, M.dy};
+        AdjLayout L;
+        Work W;
+        AdjWork A;
+        uint32_t* act;
+        batch_member_work(a, M, L, W, A, act);
+        const int bx = blk % L.act_nx, by = blk / L.act_nx;
+        const int mx = g.mx, my = g.my;
+        const size_t nint = (size_t)mx * my, nxi = L.S.nxi, nyi = L.S.nyi, npad = L.S.npad;
+        for (int h = 0; h < ACT_TILE; h += ATPB / ACT_TILE) {
+            const int ci = bx * ACT_TILE + (threadIdx.x & 15) - 1, cj = by * ACT_TILE + (threadIdx.x >> 4) + h - 1;
+            if (ci >= 1 && cj >= 1 && ci <= mx && cj <= my) {
+                const size_t c = (size_t)(cj - 1) * mx + (size_t)(ci - 1);
+                for (int f = 0; f < 5; ++f) A.lamq[f * nint + c] = 0.0;
+            }
+            if (ci >= 0 && cj >= 0 && ci <= mx + 2 && cj <= my + 1) {
+                const size_t x = xidx(g, cj, ci);
+                for (int f = 0; f < NFB; ++f) A.xfb[f * nxi + x] = 0.0;
+                for (int f = 0; f < NCB; ++f) A.xcb[f * nxi + x] = 0.0;
+            }
+            if (ci >= 0 && cj >= 0 && ci <= mx + 1 && cj <= my + 2) {
+                const size_t y = yidx(g, cj, ci);
+                for (int f = 0; f < NFB; ++f) A.yfb[f * nyi + y] = 0.0;
+                for (int f = 0; f < NCB; ++f) A.ycb[f * nyi + y] = 0.0;
+            }
+            if (ci >= -1 && cj >= -1 && ci <= mx + 2 && cj <= my + 2) {
+                const size_t pp = pidx(g, ci, cj);
+                for (int f = 0; f < NTD; ++f) A.tdq[f * npad + pp] = 0.0;
+                for (int f = 0; f < 5; ++f) A.qsb[f * npad + pp] = 0.0;
+            }
+        }
+    }
 }
 
-// pbar[4 m + k] += member m's partials, summed as k_rv_pbar sums them
+// member m (blockIdx.y): activity map and lam_in to zero; block 0 of member
+// 0 clears the list lengths
+__global__ void __launch_bounds__(256) k_adj_batch_zero(BatchArgs a, unsigned int* counts) {
+    const dclaw_adj_member M = a.mem[blockIdx.y];
+    const AdjLayout L = adj_layout(M.mx, M.my);
+    uint32_t* act = (uint32_t*)(a.work + M.work_off + L.off_act);
+    double* lam = a.lam_in + M.q_off;
+    const size_t nact = (size_t)L.act_nx * L.act_ny, nl = (size_t)5 * M.mx * M.my;
+    const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+    for (size_t x = t0; x < nact; x += st) act[x] = 0u;
+    for (size_t x = t0; x < nl; x += st) lam[x] = 0.0;
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < 2) counts[threadIdx.x] = 0u;
+}
+
+// member m (blockIdx.y): a wet interior cell marks the blocks within ACT_REACH
+__global__ void __launch_bounds__(256) k_adj_batch_scan(BatchArgs a) {
+    const int m = blockIdx.y;
+    const dclaw_adj_member M = a.mem[m];
+    const double dry = a.prm[m].dry_tolerance;
+    const AdjLayout L = adj_layout(M.mx, M.my);
+    uint32_t* act = (uint32_t*)(a.work + M.work_off + L.off_act);
+    const double* h = a.q + M.q_off;
+    const size_t n = (size_t)M.mx * M.my;
+    const int act_ny = (M.my + 4 + ACT_TILE - 1) / ACT_TILE;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        if (!(h[c] > dry)) continue;
+        const int px = (int)(c % (size_t)M.mx) + 1 + 1, py = (int)(c / (size_t)M.mx) + 1 + 1;   // padded index i + 1
+        int x0 = px - ACT_REACH < 0 ? 0 : (px - ACT_REACH) / ACT_TILE, x1 = (px + ACT_REACH) / ACT_TILE;
+        int y0 = py - ACT_REACH < 0 ? 0 : (py - ACT_REACH) / ACT_TILE, y1 = (py + ACT_REACH) / ACT_TILE;
+        if (x1 > L.act_nx - 1) x1 = L.act_nx - 1;
+        if (y1 > act_ny - 1) y1 = act_ny - 1;
+        for (int y = y0; y <= y1; ++y)
+            for (int x = x0; x <= x1; ++x) act[y * L.act_nx + x] = 1u;
+    }
+}
+
+// member m (blockIdx.y): its active blocks into list_act and its blocks with
+// an active block among the 3 x 3 around them into list_dil (one
+// warp-aggregated atomic per warp and list)
+__global__ void __launch_bounds__(256) k_adj_batch_list(BatchArgs a, unsigned int* counts, uint64_t* list_act,
+                                                        uint64_t* list_dil) {
+    const int m = blockIdx.y;
+    const dclaw_adj_member M = a.mem[m];
+    const AdjLayout L = adj_layout(M.mx, M.my);
+    const uint32_t* act = (const uint32_t*)(a.work + M.work_off + L.off_act);
+    const int nx = L.act_nx, ny = L.act_ny, nb = nx * ny;
+    const int lane = threadIdx.x & 31;
+    for (int b0 = blockIdx.x * blockDim.x; b0 < nb; b0 += gridDim.x * blockDim.x) {
+        const int b = b0 + threadIdx.x;
+        bool on = false, dil = false;
+        if (b < nb) {
+            const int bx = b % nx, by = b / nx;
+            on = act[b] != 0u;
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int x = bx + dx, y = by + dy;
+                    if (x >= 0 && y >= 0 && x < nx && y < ny) dil |= act[y * nx + x] != 0u;
+                }
+        }
+        const unsigned ba = __ballot_sync(0xffffffffu, on), bd = __ballot_sync(0xffffffffu, dil);
+        unsigned base_a = 0, base_d = 0;
+        if (lane == 0) {
+            if (ba) base_a = atomicAdd(counts, (unsigned)__popc(ba));
+            if (bd) base_d = atomicAdd(counts + 1, (unsigned)__popc(bd));
+        }
+        base_a = __shfl_sync(0xffffffffu, base_a, 0);
+        base_d = __shfl_sync(0xffffffffu, base_d, 0);
+        const unsigned below = (1u << lane) - 1u;
+        const uint64_t e = ((uint64_t)m << 32) | (uint32_t)b;
+        if (on) list_act[base_a + __popc(ba & below)] = e;
+        if (dil) list_dil[base_d + __popc(bd & below)] = e;
+    }
+}
+
+// pbar[4 m + k] += member m's block partials of its active blocks, summed in
+// a fixed order (thread t: slots t, t + ATPB, ...; then the threads in order)
 __global__ void __launch_bounds__(ATPB) k_adj_batch_pbar(BatchArgs a, double* __restrict__ pbar) {
     __shared__ double red[NPB][ATPB];
     const int m = blockIdx.x;
     const dclaw_adj_member M = a.mem[m];
     const AdjLayout L = adj_layout(M.mx, M.my);
     const double* part = (const double*)(a.work + M.work_off + L.off_part);
+    const uint32_t* act = (const uint32_t*)(a.work + M.work_off + L.off_act);
+    const long long nb = (long long)L.act_nx * L.act_ny, ns = BLK_PBAR_OPS * nb;
     for (int k = 0; k < NPB; ++k) {
         double s = 0.0;
-        for (long long b = threadIdx.x; b < L.nparts; b += ATPB) s += part[b * NPB + k];
+        for (long long x = threadIdx.x; x < ns; x += ATPB)
+            if (act[x % nb]) s += part[x * NPB + k];
         red[k][threadIdx.x] = s;
     }
     __syncthreads();
@@ -541,7 +674,7 @@ int dclaw_adjoint_batch_layout(int n, const int32_t* mx, const int32_t* my, cons
                                const uint64_t* q_off, const uint64_t* b_off, dclaw_adj_member* members,
                                dclaw_adj_batch* batch) {
     if (n <= 0 || !mx || !my || !dx || !dy || !q_off || !b_off || !members || !batch) return DCLAW_ERR_ARG;
-    uint64_t w = 0;
+    uint64_t w = 0, nblocks = 0;
     uint64_t nch[NSPACE] = {0, 0, 0, 0, 0, 0};
     for (int k = 0; k < n; ++k) {
         if (!adj_sizes_ok(mx[k], my[k]) || !(dx[k] > 0.0) || !(dy[k] > 0.0)) return DCLAW_ERR_ARG;
@@ -553,7 +686,9 @@ int dclaw_adjoint_batch_layout(int n, const int32_t* mx, const int32_t* my, cons
         M.q_off = q_off[k];
         M.b_off = b_off[k];
         M.work_off = w;
-        w += align256(adj_layout(mx[k], my[k]).total);
+        const AdjLayout Lk = adj_layout(mx[k], my[k]);
+        w += align256(Lk.total);
+        nblocks += (uint64_t)Lk.act_nx * Lk.act_ny;
         for (int sp = 0; sp < NSPACE; ++sp) {
             const uint64_t c = nblk(space_items(sp, mx[k], my[k]));
             if (nch[sp] + c > 0xffffffffull) return DCLAW_ERR_TOO_LARGE;
@@ -562,10 +697,14 @@ int dclaw_adjoint_batch_layout(int n, const int32_t* mx, const int32_t* my, cons
             nch[sp] += c;
         }
     }
+    if (nblocks > 0xffffffffull) return DCLAW_ERR_TOO_LARGE;
     batch->nmembers = n;
     batch->chunk_items = ATPB;
     for (int sp = 0; sp < NSPACE; ++sp) batch->nchunks[sp] = (uint32_t)nch[sp];
-    batch->work_bytes = w;
+    batch->nblocks = (uint32_t)nblocks;
+    batch->pad_ = 0;
+    // + the two block lists and their lengths
+    batch->work_bytes = w + 2 * align256(nblocks * 8) + 256;
     return DCLAW_OK;
 }
 
@@ -580,33 +719,36 @@ int dclaw_step_adjoint_batched(const dclaw_adj_batch* batch, const dclaw_adj_mem
     int dev = 0, nsm = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     BatchArgs a{batch->nmembers, members, params, dt, q_in, b, lam_out, lam_in, (char*)work, status};
-    // reverse planes, partials, activity maps and lam_in start at zero: the
-    // items of inactive blocks are skipped
-    k_adj_batch_zero<<<dim3(64, (unsigned)batch->nmembers), 256, 0, s>>>(a);
-    // persistent grids: a few blocks per SM, capped by the chunks of the space
-    auto grid = [&](int sp) -> unsigned {
-        uint32_t c = batch->nchunks[sp];
-        uint32_t cap = (uint32_t)nsm * 8u;
-        return c < cap ? (c ? c : 1u) : cap;
-    };
-#define DC_LAUNCH(op) k_adj_batch<op><<<grid(OpTraits<op>::SPACE), ATPB, 0, s>>>(a, batch->nchunks[OpTraits<op>::SPACE])
-    DC_LAUNCH(OP_FW_B4);
-    DC_LAUNCH(OP_FW_MARK);
-    DC_LAUNCH(OP_FW_TAUDIR);
-    DC_LAUNCH(OP_FW_SVREC);
-    DC_LAUNCH(OP_FW_RX);
-    DC_LAUNCH(OP_FW_RY);
-    DC_LAUNCH(OP_FW_FX);
-    DC_LAUNCH(OP_FW_FY);
-    DC_LAUNCH(OP_RV_SRC2);
-    DC_LAUNCH(OP_RV_FX);
-    DC_LAUNCH(OP_RV_FY);
-    DC_LAUNCH(OP_RV_RX);
-    DC_LAUNCH(OP_RV_RY);
-    DC_LAUNCH(OP_RV_TAUDIR);
-    DC_LAUNCH(OP_RV_B4);
-    DC_LAUNCH(OP_RV_GATHER);
-#undef DC_LAUNCH
+    char* lists = (char*)work + (batch->work_bytes - 256 - 2 * align256((size_t)batch->nblocks * 8));
+    uint64_t* list_act = (uint64_t*)lists;
+    uint64_t* list_dil = (uint64_t*)(lists + align256((size_t)batch->nblocks * 8));
+    unsigned int* counts = (unsigned int*)((char*)work + (batch->work_bytes - 256));
+    const dim3 per_member(64, (unsigned)batch->nmembers);
+    k_adj_batch_zero<<<per_member, 256, 0, s>>>(a, counts);
+    k_adj_batch_scan<<<per_member, 256, 0, s>>>(a);
+    k_adj_batch_list<<<dim3(8, (unsigned)batch->nmembers), 256, 0, s>>>(a, counts, list_act, list_dil);
+    // persistent grids over the lists
+    const unsigned grid = (unsigned)nsm * 4u;
+    k_adj_blocks_zero<<<grid, ATPB, 0, s>>>(a, list_dil, counts + 1);
+#define DC_FW(op) k_adj_blocks<op><<<grid, ATPB, 0, s>>>(a, list_dil, counts + 1)
+#define DC_RV(op) k_adj_blocks<op><<<grid, ATPB, 0, s>>>(a, list_act, counts)
+    DC_FW(OP_FW_B4);
+    DC_FW(OP_FW_TAUDIR);
+    DC_FW(OP_FW_SVREC);
+    DC_FW(OP_FW_RX);
+    DC_FW(OP_FW_RY);
+    DC_FW(OP_FW_FX);
+    DC_FW(OP_FW_FY);
+    DC_RV(OP_RV_SRC2);
+    DC_RV(OP_RV_FX);
+    DC_RV(OP_RV_FY);
+    DC_RV(OP_RV_RX);
+    DC_RV(OP_RV_RY);
+    DC_RV(OP_RV_TAUDIR);
+    DC_RV(OP_RV_B4);
+    DC_RV(OP_RV_GATHER);
+#undef DC_FW
+#undef DC_RV
     k_adj_batch_pbar<<<batch->nmembers, ATPB, 0, s>>>(a, pbar);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DCLAW_OK : DCLAW_ERR_CUDA;

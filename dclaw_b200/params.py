@@ -120,7 +120,7 @@ class CAdjBatch(ctypes.Structure):
 
     _fields_ = [
         ("nmembers", ctypes.c_int32), ("chunk_items", ctypes.c_uint32), ("nchunks", ctypes.c_uint32 * 6),
-        ("work_bytes", ctypes.c_uint64),
+        ("nblocks", ctypes.c_uint32), ("pad_", ctypes.c_uint32), ("work_bytes", ctypes.c_uint64),
     ]
 
 

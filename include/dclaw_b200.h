@@ -323,11 +323,16 @@ int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, doub
  * The reference differentiates its particle filters member by member with
  * jax.jacfwd / jax.grad under jax.vmap (gradient_particle_filter/pf_flume/
  * inference.py:96-108). Here the adjoint of one step of every member of an
- * ensemble of uneven patches runs as one sequence of 18 launches (a zeroing
- * pass, then the stages), each a grid-stride loop over the chunks of all
- * members' items. Each member has its
- * own parameters, dt and parameter adjoints; member k's results equal those of
- * dclaw_step_adjoint on member k alone, bit for bit.
+ * ensemble of uneven patches runs as one sequence of 20 launches that work
+ * only where members are wet: a scan marks each member's 16 x 16 activity
+ * blocks (a wet cell within 4), a list kernel gathers the active blocks and
+ * the blocks beside them, the forward recompute and the zeroing of the
+ * reverse planes run over the second list and the reverse stages over the
+ * first, each a grid-stride loop of one CTA per listed block. Each member
+ * has its own parameters, dt and parameter adjoints; member k's lam_in
+ * equals dclaw_step_adjoint's on member k alone bit for bit, and its
+ * parameter adjoints agree to rounding (the block sums are grouped by
+ * activity block, not by 128-item chunk).
  * Item spaces (chunk0 / nchunk index): 0 padded cells, 1 interior cells,
  * 2 x-interface solves, 3 y-interface solves, 4 x-interface fluxes, 5 y-interface
  * fluxes. */
@@ -345,7 +350,9 @@ typedef struct dclaw_adj_batch {
     int32_t nmembers;
     uint32_t chunk_items;  /* items per chunk (threads per block) */
     uint32_t nchunks[6];   /* chunks of all members per item space */
-    uint64_t work_bytes;   /* adjoint workspace of the whole batch */
+    uint32_t nblocks;      /* 16 x 16 activity blocks of all members */
+    uint32_t pad_;
+    uint64_t work_bytes;   /* adjoint workspace of the whole batch (+ block lists) */
 } dclaw_adj_batch;
 
 /* host-side layout: members[0..n) (host array) from sizes, spacings and the

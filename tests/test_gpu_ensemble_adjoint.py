@@ -1,9 +1,12 @@
 """The batched step adjoint (dclaw_step_adjoint_batched through the C ABI)
 and the differentiable ensemble rollout, against the single-patch adjoint
-member by member: the batched launches run the same reverse stages on every
-member's own layout, parameters and dt, so state and parameter adjoints are
-bit-identical to dclaw_step_adjoint on each member alone, and so are whole
-checkpointed gradients. The single-patch adjoint is checked against finite
+member by member: the batched launches run the same item stages on every
+member's own layout, parameters and dt, over the 16 x 16 blocks where the
+member is wet (and the blocks beside them), so state adjoints and whole
+checkpointed state gradients are bit-identical to dclaw_step_adjoint on each
+member alone. The parameter adjoints are block sums grouped by activity
+block instead of by 128-item chunk: equal to 1e-12 relative, and the same
+bits from call to call. The single-patch adjoint is checked against finite
 differences in test_gpu_adjoint.py."""
 import numpy as np
 import pytest
@@ -41,9 +44,23 @@ def _advance(members, dev, n=12):
             for k, m in enumerate(members)]
 
 
-def test_batched_step_adjoint_matches_single_patch(cuda_device):
+def _close_params(a, b, what):
+    assert torch.allclose(a, b, rtol=1e-12, atol=0.0), f"{what}: {a.tolist()} vs {b.tolist()}"
+
+
+def _mostly_dry(seed=9):
+    """Long flumes whose release blocks cover a few of their 16 x 16 blocks,
+    so that most blocks are inactive and the list edges matter."""
+    out = []
+    for c in W.flume_ensemble(n=3, seed=seed, width_range=(40, 70), length_range=(300, 420)):
+        out.append(Member(c.q, c.b, c.params, c.dx, c.dy, 2.0e-3))
+    return out
+
+
+@pytest.mark.parametrize("which", ["uneven", "mostly_dry"])
+def test_batched_step_adjoint_matches_single_patch(cuda_device, which):
     dev = cuda_device
-    members = _advance(_members(), dev)
+    members = _advance(_members() if which == "uneven" else _mostly_dry(), dev)
     ens = EnsembleStepper(members, dev)
     adj = EnsembleStepAdjoint(ens)
     rng = np.random.default_rng(3)
@@ -54,6 +71,10 @@ def test_batched_step_adjoint_matches_single_patch(cuda_device):
     adj.vjp(ens.qa, dts, lam, lam_in, pbar)
     torch.cuda.synchronize()
     adj.check_status()
+    # a second call gives the same bits (fixed summation order)
+    lam_in2, pbar2 = torch.zeros_like(lam), torch.zeros_like(pbar)
+    adj.vjp(ens.qa, dts, lam, lam_in2, pbar2)
+    assert torch.equal(lam_in, lam_in2) and torch.equal(pbar, pbar2)
     for k, m in enumerate(members):
         o, c = ens.cm[k].q_off, m.q.size
         sa = StepAdjoint(torch.tensor(m.b, device=dev), m.params, m.dx, m.dy)
@@ -61,12 +82,13 @@ def test_batched_step_adjoint_matches_single_patch(cuda_device):
         pb = torch.zeros(4, dtype=torch.float64, device=dev)
         sa.vjp(ens.qa[o:o + c].view(m.q.shape), dts[k:k + 1], lam[o:o + c].view(m.q.shape).contiguous(), li, pb)
         assert torch.equal(lam_in[o:o + c].view(m.q.shape), li), f"member {k}: state adjoint differs"
-        assert torch.equal(pbar[k], pb), f"member {k}: parameter adjoint differs"
+        _close_params(pbar[k], pb, f"member {k}: parameter adjoint")
 
 
 def test_ensemble_gradient_matches_single_patch_gradients(cuda_device):
     """Per-member losses over output times; the batched checkpointed gradient
-    equals each member's unbatched rollout_states gradient, bit for bit."""
+    equals each member's unbatched rollout_states gradient: states and state
+    gradients bit for bit, parameter gradients to 1e-12."""
     dev = cuda_device
     members = _advance(_members(seed=9), dev, n=8)
     ens = EnsembleStepper(members, dev)
@@ -88,7 +110,7 @@ def test_ensemble_gradient_matches_single_patch_gradients(cuda_device):
         Lk.backward()
         assert torch.equal(o.detach()[:, off:off + c].view(ok.shape), ok.detach()), f"member {k}: states"
         assert torch.equal(q0.grad[off:off + c].view(m.q.shape), qk.grad), f"member {k}: state gradient"
-        assert torch.equal(theta.grad[k], tk.grad), f"member {k}: parameter gradient"
+        _close_params(theta.grad[k], tk.grad, f"member {k}: parameter gradient")
 
 
 def test_ensemble_select_outputs(cuda_device):
