@@ -333,7 +333,7 @@ def gradient_bench(args, dev):
         fwd_ms.append(e0.elapsed_time(e1))
     del st
     grad_ms = []
-    for _ in range(2):
+    for _ in range(3):
         h = h0.clone().requires_grad_(True)
         m0 = torch.tensor(c.m0, dtype=torch.float64, device=dev, requires_grad=True)
         theta = theta_of(p, dev).requires_grad_(True)
@@ -351,7 +351,7 @@ def gradient_bench(args, dev):
     # minimum: every block's states recomputed once in the backward pass)
     ksq = max(1, math.ceil(math.sqrt(c.nsteps)))
     sq_ms = []
-    for _ in range(2):
+    for _ in range(3):
         hs = h0.clone().requires_grad_(True)
         ms0 = torch.tensor(c.m0, dtype=torch.float64, device=dev, requires_grad=True)
         ths = theta_of(p, dev).requires_grad_(True)
@@ -371,7 +371,7 @@ def gradient_bench(args, dev):
             "grad": {"phi_deg": float(theta.grad[0]), "kref": float(theta.grad[1]), "m0": float(m0.grad),
                      "alpha_c": float(theta.grad[2]), "h0_l2": float(h.grad.norm())},
             "peak_mem_gb": torch.cuda.max_memory_allocated(dev) / 1e9,
-            "gpu_launches": {"adjoint_per_step": 17, "recompute_per_step": 3, "forward_per_step": 3},
+            "gpu_launches": {"adjoint_per_step": 21, "recompute_per_step": 3, "forward_per_step": 3},
             "note": "dt of each step chosen by the tick rule in the forward pass and replayed, not differentiated"}
 
 
@@ -478,7 +478,7 @@ def batched_gradient_bench(args, dev):
             "grad_member0": {"phi_deg": float(theta.grad[0, 0]), "kref": float(theta.grad[0, 1]),
                              "alpha_c": float(theta.grad[0, 2]), "mu": float(theta.grad[0, 3]),
                              "m0": float(m0.grad[0]), "block_volume": float(H.grad[0] / area[0])},
-            "gpu_launches": {"adjoint_per_step": 18, "recompute_per_step": 6, "forward_per_step": 6},
+            "gpu_launches": {"adjoint_per_step": 20, "recompute_per_step": 6, "forward_per_step": 6},
             "note": "every member's dt from its own tick rule, recorded and replayed, not differentiated"}
 
 

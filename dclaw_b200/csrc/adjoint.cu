@@ -6,10 +6,10 @@
 // (dS/dtheta)^T lam_out to the adjoints of the material parameters
 // theta = (phi [rad], kref, alpha_c, mu). The step's dt is data.
 //
-// One call is 17 data-parallel launches and 3 memsets (the batched form: 18
-// launches, one of them zeroing):
-//   forward recompute  b4step2, the activity map of 16 x 16 blocks (a wet
-//                      cell within 4), calc_taudir, setvars records of the rpn2
+// One call (a single patch, or every member of an ensemble) is 20
+// launches that work only where the flow is (see "ensembles" below: a
+// single patch runs as a one-member ensemble):
+//   forward recompute  b4step2, calc_taudir, setvars records of the rpn2
 //                      states (tau and its partial derivatives, once per
 //                      cell state instead of once per interface side),
 //                      x/y solves, x/y fluxes
@@ -17,12 +17,11 @@
 //                      step, so every branch is the one the forward took)
 //   reverse            src2+update, x/y fluxes, x/y solves, calc_taudir,
 //                      b4step2, ghost gather, parameter sum
-// Reverse items in inactive blocks are skipped (their outputs are zeros or
-// unread; the reverse planes are zeroed first). Every reverse stage gathers
-// what later stages wrote (no atomics), and the
+// Every reverse stage gathers what later stages wrote (no atomics), and the
 // parameter adjoints are summed per block and then across blocks in a fixed
 // order, so results are bit-reproducible run to run.
 #include <cuda_runtime.h>
+#include <string.h>
 
 #include "adjoint.cuh"
 #include "workspace.cuh"
@@ -38,23 +37,17 @@ namespace adj {
 #ifndef DCLAW_ADJ_MINB
 #define DCLAW_ADJ_MINB 4
 #endif
-// resident blocks per SM the forward-recompute and light reverse kernels are sized for
-#ifndef DCLAW_ADJ_LIGHT_MINB
-#define DCLAW_ADJ_LIGHT_MINB 1
-#endif
 constexpr int ATPB = DCLAW_ADJ_TPB;
-constexpr int NWARP = ATPB / 32;
+// threads of the block-list kernels: one per item of a 16 x 16 block
+constexpr int BTPB = 256;
 
 __host__ __device__ inline unsigned nblk(long long n) { return (unsigned)((n + ATPB - 1) / ATPB); }
 
-__device__ __forceinline__ void flag(int32_t* st, int code) {
-    if (st) atomicCAS(st, 0, code);
-}
-
 // Sum of the block's per-thread parameter adjoints, in a fixed order, into
-// dst[0..NPB). Every thread of the block must call it.
+// dst[0..NPB). Every thread of the block (NW warps) must call it.
+template <int NW>
 __device__ __forceinline__ void block_pbar(const double* pb, double* __restrict__ dst) {
-    __shared__ double red[NPB][NWARP];
+    __shared__ double red[NPB][NW];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < NPB; ++k) {
@@ -65,172 +58,8 @@ __device__ __forceinline__ void block_pbar(const double* pb, double* __restrict_
     __syncthreads();
     if (threadIdx.x < NPB) {
         double s = 0.0;
-        for (int w = 0; w < NWARP; ++w) s += red[threadIdx.x][w];
+        for (int w = 0; w < NW; ++w) s += red[threadIdx.x][w];
         dst[threadIdx.x] = s;
-    }
-}
-
-// ---- forward recompute (the staged step's stages A-D) ---------------------
-__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_fw_b4(dclaw_params P, Geom g, const double* __restrict__ q_in,
-                                                const double* __restrict__ b, Work W, int32_t* status) {
-    const long long n = (long long)g.PX * g.PY;
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n) return;
-    int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
-    if (stage_b4(P, g, q_in, b, W, i, j)) flag(status, DCLAW_ERR_NAN);
-}
-
-// blocks of padded cells within ACT_REACH of a wet padded cell (act zeroed before)
-__device__ __forceinline__ void mark_active(const dclaw_params& P, const Geom& g, const Work& W, uint32_t* act,
-                                            int act_nx, int i, int j) {
-    if (!(W.qB[pidx(g, i, j)] > P.dry_tolerance)) return;
-    const int px = i + 1, py = j + 1;
-    const int act_ny = (g.PY + ACT_TILE - 1) / ACT_TILE;
-    int x0 = (px - ACT_REACH) / ACT_TILE, x1 = (px + ACT_REACH) / ACT_TILE;
-    int y0 = (py - ACT_REACH) / ACT_TILE, y1 = (py + ACT_REACH) / ACT_TILE;
-    if (px - ACT_REACH < 0) x0 = 0;
-    if (py - ACT_REACH < 0) y0 = 0;
-    if (x1 > act_nx - 1) x1 = act_nx - 1;
-    if (y1 > act_ny - 1) y1 = act_ny - 1;
-    for (int y = y0; y <= y1; ++y)
-        for (int x = x0; x <= x1; ++x) act[y * act_nx + x] = 1u;
-}
-
-__global__ void __launch_bounds__(ATPB) k_fw_mark(dclaw_params P, Geom g, Work W, uint32_t* act, int act_nx) {
-    const long long n = (long long)g.PX * g.PY;
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n) return;
-    mark_active(P, g, W, act, act_nx, (int)(idx % g.PX) - 1, (int)(idx / g.PX) - 1);
-}
-
-__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_fw_taudir(dclaw_params P, Geom g, Work W) {
-    const long long n = (long long)g.PX * g.PY;
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n) return;
-    int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
-    stage_taudir(P, g, W, i, j);
-}
-
-// DIR 0: rows r = 0..my+1, interfaces i = 0..mx+2; DIR 1: interfaces
-// k = 0..my+2, columns c = 0..mx+1 (the fast index is along x)
-__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_fw_svrec(dclaw_params P, Geom g, Work W, AdjWork A) {
-    const long long n = (long long)g.PX * g.PY;
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n) return;
-    int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
-    adj_item_svrec(P, g, W, A, i, j);
-}
-
-template <int DIR>
-__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_fw_riemann(dclaw_params P, Geom g, Work W, const double* __restrict__ sv) {
-    const int nfast = DIR == 0 ? g.mx + 3 : g.mx + 2;
-    const int nslow = DIR == 0 ? g.my + 2 : g.my + 3;
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (long long)nfast * nslow) return;
-    int a = (int)(idx % nfast), s = (int)(idx / nfast);
-    int r = DIR == 0 ? s : a, i = DIR == 0 ? a : s;
-    stage_riemann<DIR>(P, g, W, r, i, nullptr, sv);
-}
-
-// DIR 0: rows 0..my+1, interfaces 1..mx+1; DIR 1: interfaces 1..my+1, columns 0..mx+1
-template <int DIR>
-__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_fw_flux(dclaw_params P, Geom g, Work W, const double* __restrict__ dtp) {
-    const int nfast = DIR == 0 ? g.mx + 1 : g.mx + 2;
-    const int nslow = DIR == 0 ? g.my + 2 : g.my + 1;
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (long long)nfast * nslow) return;
-    int a = (int)(idx % nfast), s = (int)(idx / nfast);
-    int r = DIR == 0 ? s : a, i = DIR == 0 ? a + 1 : s + 1;
-    const double dt = *dtp;
-    stage_flux<DIR>(P, g, W, r, i, DIR == 0 ? dt / g.dx : dt / g.dy, nullptr);
-}
-
-// ---- reverse stages -------------------------------------------------------
-__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_rv_src2(dclaw_params P, Geom g, Work W, AdjWork A,
-                                                  const double* __restrict__ lam_out, const double* __restrict__ dtp,
-                                                  double* __restrict__ part) {
-    const long long n = (long long)g.mx * g.my;
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    double pb[NPB] = {0.0, 0.0, 0.0, 0.0};
-    if (idx < n) {
-        int i = (int)(idx % g.mx) + 1, j = (int)(idx / g.mx) + 1;
-        if (adj_active(A, i, j)) adj_item_src2(P, g, W, A, lam_out, i, j, *dtp, pb);
-    }
-    block_pbar(pb, part + (size_t)blockIdx.x * NPB);
-}
-
-template <int DIR>
-__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_rv_flux(dclaw_params P, Geom g, Work W, AdjWork A,
-                                                  const double* __restrict__ dtp) {
-    const int nfast = DIR == 0 ? g.mx + 1 : g.mx + 2;
-    const int nslow = DIR == 0 ? g.my + 2 : g.my + 1;
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (long long)nfast * nslow) return;
-    int a = (int)(idx % nfast), s = (int)(idx / nfast);
-    int r = DIR == 0 ? s : a, i = DIR == 0 ? a + 1 : s + 1;
-    if (adj_active(A, DIR == 0 ? i : r, DIR == 0 ? r : i)) adj_item_flux<DIR>(P, g, W, A, r, i, *dtp);
-}
-
-template <int DIR>
-__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_rv_riemann(dclaw_params P, Geom g, Work W, AdjWork A,
-                                                     double* __restrict__ part, int32_t* status) {
-    const int nfast = DIR == 0 ? g.mx + 3 : g.mx + 2;
-    const int nslow = DIR == 0 ? g.my + 2 : g.my + 3;
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    double pb[NPB] = {0.0, 0.0, 0.0, 0.0};
-    if (idx < (long long)nfast * nslow) {
-        int a = (int)(idx % nfast), s = (int)(idx / nfast);
-        int r = DIR == 0 ? s : a, i = DIR == 0 ? a : s;
-        if (adj_active(A, DIR == 0 ? i : r, DIR == 0 ? r : i) && !adj_item_riemann<DIR>(P, g, W, A, r, i, pb))
-            flag(status, DCLAW_ERR_UNSUPPORTED);
-    }
-    block_pbar(pb, part + (size_t)blockIdx.x * NPB);
-}
-
-__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_rv_taudir(dclaw_params P, Geom g, Work W, AdjWork A,
-                                                    double* __restrict__ part) {
-    const long long n = (long long)g.PX * g.PY;
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    double pb[NPB] = {0.0, 0.0, 0.0, 0.0};
-    if (idx < n) {
-        int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
-        if (adj_active(A, i, j)) adj_item_taudir(P, g, W, A, i, j, pb);
-    }
-    block_pbar(pb, part + (size_t)blockIdx.x * NPB);
-}
-
-__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_rv_b4(dclaw_params P, Geom g, Work W, AdjWork A,
-                                                const double* __restrict__ q_in) {
-    const long long n = (long long)g.PX * g.PY;
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n) return;
-    int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
-    if (adj_active(A, i, j)) adj_item_b4(P, g, W, A, q_in, i, j);
-}
-
-__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_LIGHT_MINB) k_rv_gather(dclaw_params P, Geom g, Work W, AdjWork A,
-                                                    double* __restrict__ lam_in) {
-    const long long n = (long long)g.mx * g.my;
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n) return;
-    int i = (int)(idx % g.mx) + 1, j = (int)(idx / g.mx) + 1;
-    if (adj_active(A, i, j)) adj_item_gather(P, g, A, W, lam_in, i, j);
-}
-
-// pbar[k] += sum over the nb block partials, in block order (one block)
-__global__ void __launch_bounds__(ATPB) k_rv_pbar(const double* __restrict__ part, long long nb,
-                                                  double* __restrict__ pbar) {
-    __shared__ double red[NPB][ATPB];
-    for (int k = 0; k < NPB; ++k) {
-        double s = 0.0;
-        for (long long b = threadIdx.x; b < nb; b += ATPB) s += part[b * NPB + k];
-        red[k][threadIdx.x] = s;
-    }
-    __syncthreads();
-    if (threadIdx.x < NPB) {
-        double s = 0.0;
-        for (int t = 0; t < ATPB; ++t) s += red[threadIdx.x][t];
-        pbar[threadIdx.x] += s;
     }
 }
 
@@ -277,7 +106,7 @@ inline bool adj_sizes_ok(int mx, int my) {
 // ---- ensembles: the same stages over the chunks of every member -------------
 enum { SP_PAD = 0, SP_INT, SP_RX, SP_RY, SP_FX, SP_FY, NSPACE };
 enum {
-    OP_FW_B4, OP_FW_MARK, OP_FW_TAUDIR, OP_FW_SVREC, OP_FW_RX, OP_FW_RY, OP_FW_FX, OP_FW_FY,
+    OP_FW_B4, OP_FW_TAUDIR, OP_FW_SVREC, OP_FW_RX, OP_FW_RY, OP_FW_FX, OP_FW_FY,
     OP_RV_SRC2, OP_RV_FX, OP_RV_FY, OP_RV_RX, OP_RV_RY, OP_RV_TAUDIR, OP_RV_B4, OP_RV_GATHER
 };
 
@@ -290,7 +119,6 @@ struct OpTraits;
         static constexpr bool PBAR = pb;    \
     };
 DC_OP(OP_FW_B4, SP_PAD, false)
-DC_OP(OP_FW_MARK, SP_PAD, false)
 DC_OP(OP_FW_TAUDIR, SP_PAD, false)
 DC_OP(OP_FW_SVREC, SP_PAD, false)
 DC_OP(OP_FW_RX, SP_RX, false)
@@ -409,9 +237,10 @@ __device__ __forceinline__ void block_item(const BatchArgs& a, int m, const dcla
 
 // One stage over a list of (member, block) entries (grid-stride; every
 // thread of a CTA runs the same iterations, so the barriers are uniform).
-// A CTA of 128 threads covers a 16 x 16 block in two rows of 8.
+// A CTA has one thread per item of a 16 x 16 block; two CTAs per SM at up
+// to 128 registers a thread.
 template <int OP>
-__global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_adj_blocks(BatchArgs a, const uint64_t* __restrict__ list,
+__global__ void __launch_bounds__(BTPB, DCLAW_ADJ_MINB / 2) k_adj_blocks(BatchArgs a, const uint64_t* __restrict__ list,
                                                                      const unsigned int* __restrict__ count) {
     __shared__ dclaw_adj_member sM;
     __shared__ dclaw_params sP;
@@ -441,12 +270,11 @@ __global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_adj_blocks(BatchArgs a
         const int bx = blk % L.act_nx, by = blk / L.act_nx;
         const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
         double pb[NPB] = {0.0, 0.0, 0.0, 0.0};
-        for (int h = 0; h < ACT_TILE; h += ATPB / ACT_TILE)
-            block_item<OP>(a, m, sM, sP, g, W, A, L, bx * ACT_TILE + tx - 1, by * ACT_TILE + ty + h - 1, pb);
+        block_item<OP>(a, m, sM, sP, g, W, A, L, bx * ACT_TILE + tx - 1, by * ACT_TILE + ty - 1, pb);
         if (OpTraits<OP>::PBAR) {
             const int pidx = OP == OP_RV_SRC2 ? 0 : OP == OP_RV_RX ? 1 : OP == OP_RV_RY ? 2 : 3;
             double* part = (double*)(a.work + sM.work_off + L.off_part);
-            block_pbar(pb, part + ((size_t)pidx * L.act_nx * L.act_ny + blk) * NPB);
+            block_pbar<BTPB / 32>(pb, part + ((size_t)pidx * L.act_nx * L.act_ny + blk) * NPB);
         }
         __syncthreads();
     }
@@ -454,7 +282,7 @@ __global__ void __launch_bounds__(ATPB, DCLAW_ADJ_MINB) k_adj_blocks(BatchArgs a
 
 // zero the reverse planes of the listed blocks' items (the slots active
 // items read; the rest of the planes is never read)
-__global__ void __launch_bounds__(ATPB) k_adj_blocks_zero(BatchArgs a, const uint64_t* __restrict__ list,
+__global__ void __launch_bounds__(BTPB) k_adj_blocks_zero(BatchArgs a, const uint64_t* __restrict__ list,
                                                           const unsigned int* __restrict__ count) {
     const unsigned int n = *count;
     for (unsigned int k = blockIdx.x; k < n; k += gridDim.x) {
@@ -470,8 +298,8 @@ __global__ void __launch_bounds__(ATPB) k_adj_blocks_zero(BatchArgs a, const uin
         const int bx = blk % L.act_nx, by = blk / L.act_nx;
         const int mx = g.mx, my = g.my;
         const size_t nint = (size_t)mx * my, nxi = L.S.nxi, nyi = L.S.nyi, npad = L.S.npad;
-        for (int h = 0; h < ACT_TILE; h += ATPB / ACT_TILE) {
-            const int ci = bx * ACT_TILE + (threadIdx.x & 15) - 1, cj = by * ACT_TILE + (threadIdx.x >> 4) + h - 1;
+        {
+            const int ci = bx * ACT_TILE + (threadIdx.x & 15) - 1, cj = by * ACT_TILE + (threadIdx.x >> 4) - 1;
             if (ci >= 1 && cj >= 1 && ci <= mx && cj <= my) {
                 const size_t c = (size_t)(cj - 1) * mx + (size_t)(ci - 1);
                 for (int f = 0; f < 5; ++f) A.lamq[f * nint + c] = 0.0;
@@ -509,7 +337,8 @@ __global__ void __launch_bounds__(256) k_adj_batch_zero(BatchArgs a, unsigned in
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < 2) counts[threadIdx.x] = 0u;
 }
 
-// member m (blockIdx.y): a wet interior cell marks the blocks within ACT_REACH
+// member m (blockIdx.y): a wet interior cell marks the blocks within
+// ACT_REACH; every field of every cell is tested for NaN (status)
 __global__ void __launch_bounds__(256) k_adj_batch_scan(BatchArgs a) {
     const int m = blockIdx.y;
     const dclaw_adj_member M = a.mem[m];
@@ -519,8 +348,11 @@ __global__ void __launch_bounds__(256) k_adj_batch_scan(BatchArgs a) {
     const double* h = a.q + M.q_off;
     const size_t n = (size_t)M.mx * M.my;
     const int act_ny = (M.my + 4 + ACT_TILE - 1) / ACT_TILE;
+    bool nan = false;
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
-        if (!(h[c] > dry)) continue;
+        const double hc = h[c], f1 = h[n + c], f2 = h[2 * n + c], f3 = h[3 * n + c], f4 = h[4 * n + c];
+        nan |= (hc != hc) || (f1 != f1) || (f2 != f2) || (f3 != f3) || (f4 != f4);
+        if (!(hc > dry)) continue;
         const int px = (int)(c % (size_t)M.mx) + 1 + 1, py = (int)(c / (size_t)M.mx) + 1 + 1;   // padded index i + 1
         int x0 = px - ACT_REACH < 0 ? 0 : (px - ACT_REACH) / ACT_TILE, x1 = (px + ACT_REACH) / ACT_TILE;
         int y0 = py - ACT_REACH < 0 ? 0 : (py - ACT_REACH) / ACT_TILE, y1 = (py + ACT_REACH) / ACT_TILE;
@@ -529,6 +361,7 @@ __global__ void __launch_bounds__(256) k_adj_batch_scan(BatchArgs a) {
         for (int y = y0; y <= y1; ++y)
             for (int x = x0; x <= x1; ++x) act[y * L.act_nx + x] = 1u;
     }
+    if (nan && a.status) atomicCAS(a.status + m, 0, DCLAW_ERR_NAN);
 }
 
 // member m (blockIdx.y): its active blocks into list_act and its blocks with
@@ -593,6 +426,75 @@ __global__ void __launch_bounds__(ATPB) k_adj_batch_pbar(BatchArgs a, double* __
     }
 }
 
+// the step adjoint of nmem members over the block lists (all launches)
+inline void launch_block_adjoint(const BatchArgs& a, uint32_t nblocks, char* lists, unsigned int* counts, int nsm,
+                                 cudaStream_t s) {
+    uint64_t* list_act = (uint64_t*)lists;
+    uint64_t* list_dil = (uint64_t*)(lists + align256((size_t)nblocks * 8));
+    // the per-member kernels fill the GPU whether there is one member or many
+    int gx = 4 * nsm / (a.nmem > 0 ? a.nmem : 1);
+    gx = gx < 16 ? 16 : (gx > 512 ? 512 : gx);
+    const dim3 per_member((unsigned)gx, (unsigned)a.nmem);
+    k_adj_batch_zero<<<per_member, 256, 0, s>>>(a, counts);
+    k_adj_batch_scan<<<per_member, 256, 0, s>>>(a);
+    k_adj_batch_list<<<dim3(8, (unsigned)a.nmem), 256, 0, s>>>(a, counts, list_act, list_dil);
+    // persistent grids over the lists
+    const unsigned grid = (unsigned)nsm * 2u;
+    k_adj_blocks_zero<<<grid * 2u, BTPB, 0, s>>>(a, list_dil, counts + 1);
+#define DC_FW(op) k_adj_blocks<op><<<grid, BTPB, 0, s>>>(a, list_dil, counts + 1)
+#define DC_RV(op) k_adj_blocks<op><<<grid, BTPB, 0, s>>>(a, list_act, counts)
+    DC_FW(OP_FW_B4);
+    DC_FW(OP_FW_TAUDIR);
+    DC_FW(OP_FW_SVREC);
+    DC_FW(OP_FW_RX);
+    DC_FW(OP_FW_RY);
+    DC_FW(OP_FW_FX);
+    DC_FW(OP_FW_FY);
+    DC_RV(OP_RV_SRC2);
+    DC_RV(OP_RV_FX);
+    DC_RV(OP_RV_FY);
+    DC_RV(OP_RV_RX);
+    DC_RV(OP_RV_RY);
+    DC_RV(OP_RV_TAUDIR);
+    DC_RV(OP_RV_B4);
+    DC_RV(OP_RV_GATHER);
+#undef DC_FW
+#undef DC_RV
+}
+
+// the single patch as a one-member batch: its table entry and parameters,
+// written into the workspace tail by one thread
+__global__ void k_adj_single_setup(dclaw_adj_member M, dclaw_params P, dclaw_adj_member* mem, dclaw_params* prm) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        *mem = M;
+        *prm = P;
+    }
+}
+
+// tail of the single-patch workspace: member entry, parameters, two block
+// lists, list lengths
+struct SingleTail {
+    size_t off_mem, off_prm, off_lists, off_counts, total;
+};
+
+inline SingleTail single_tail(const AdjLayout& L) {
+    SingleTail T;
+    const size_t nb = (size_t)L.act_nx * L.act_ny;
+    size_t o = L.total;
+    T.off_mem = o; o += align256(sizeof(dclaw_adj_member));
+    T.off_prm = o; o += align256(sizeof(dclaw_params));
+    T.off_lists = o; o += 2 * align256(nb * 8);
+    T.off_counts = o; o += 256;
+    T.total = o;
+    return T;
+}
+
+inline int sm_count_adj() {
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return nsm;
+}
+
 }  // namespace adj
 }  // namespace dclaw
 
@@ -603,7 +505,7 @@ extern "C" {
 
 size_t dclaw_adjoint_workspace_bytes(int mx, int my) {
     if (!adj_sizes_ok(mx, my)) return 0;
-    return adj_layout(mx, my).total;
+    return single_tail(adj_layout(mx, my)).total;
 }
 
 int dclaw_adjoint_supported(const dclaw_params* p) {
@@ -625,47 +527,23 @@ int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, doub
     int rc = dclaw_adjoint_supported(p);
     if (rc) return rc;
     AdjLayout L = adj_layout(mx, my);
-    if (work_bytes < L.total) return DCLAW_ERR_WORKSPACE;
+    const SingleTail T = single_tail(L);
+    if (work_bytes < T.total) return DCLAW_ERR_WORKSPACE;
     cudaStream_t s = (cudaStream_t)stream;
-    const dclaw_params P = *p;
-    Geom g{mx, my, mx + 4, my + 4, dx, dy};
-    Work W = make_work(work, L.S);
     char* base = (char*)work;
-    uint32_t* act = (uint32_t*)(base + L.off_act);
-    AdjWork A{(double*)(base + L.off_lamq), (double*)(base + L.off_xfb), (double*)(base + L.off_yfb),
-              (double*)(base + L.off_xcb), (double*)(base + L.off_ycb), (double*)(base + L.off_tdq),
-              (double*)(base + L.off_qsb), (double*)(base + L.off_sv), act, L.act_nx};
-    double* part = (double*)(base + L.off_part);
-    // reverse planes, block partials, activity map and lam_in start at zero:
-    // the items of inactive blocks are skipped
-    cudaMemsetAsync(base + L.off_lamq, 0, L.off_sv - L.off_lamq, s);
-    cudaMemsetAsync(base + L.off_part, 0, L.total - L.off_part, s);
-    cudaMemsetAsync(lam_in, 0, (size_t)5 * mx * my * 8, s);
-    const long long npad = (long long)L.S.npad, nint = (long long)mx * my;
-    const long long nxf = (long long)(mx + 1) * (my + 2), nyf = (long long)(mx + 2) * (my + 1);
-    // forward intermediates of this step
-    k_fw_b4<<<nblk(npad), ATPB, 0, s>>>(P, g, q_in, b, W, status);
-    k_fw_mark<<<nblk(npad), ATPB, 0, s>>>(P, g, W, act, L.act_nx);
-    k_fw_taudir<<<nblk(npad), ATPB, 0, s>>>(P, g, W);
-    k_fw_svrec<<<nblk(npad), ATPB, 0, s>>>(P, g, W, A);
-    k_fw_riemann<0><<<(unsigned)L.nb_rx, ATPB, 0, s>>>(P, g, W, A.sv);
-    k_fw_riemann<1><<<(unsigned)L.nb_ry, ATPB, 0, s>>>(P, g, W, A.sv);
-    k_fw_flux<0><<<nblk(nxf), ATPB, 0, s>>>(P, g, W, dt);
-    k_fw_flux<1><<<nblk(nyf), ATPB, 0, s>>>(P, g, W, dt);
-    // reverse
-    double* part_src2 = part;
-    double* part_rx = part_src2 + (size_t)L.nb_src2 * NPB;
-    double* part_ry = part_rx + (size_t)L.nb_rx * NPB;
-    double* part_td = part_ry + (size_t)L.nb_ry * NPB;
-    k_rv_src2<<<(unsigned)L.nb_src2, ATPB, 0, s>>>(P, g, W, A, lam_out, dt, part_src2);
-    k_rv_flux<0><<<nblk(nxf), ATPB, 0, s>>>(P, g, W, A, dt);
-    k_rv_flux<1><<<nblk(nyf), ATPB, 0, s>>>(P, g, W, A, dt);
-    k_rv_riemann<0><<<(unsigned)L.nb_rx, ATPB, 0, s>>>(P, g, W, A, part_rx, status);
-    k_rv_riemann<1><<<(unsigned)L.nb_ry, ATPB, 0, s>>>(P, g, W, A, part_ry, status);
-    k_rv_taudir<<<(unsigned)L.nb_td, ATPB, 0, s>>>(P, g, W, A, part_td);
-    k_rv_b4<<<nblk(npad), ATPB, 0, s>>>(P, g, W, A, q_in);
-    k_rv_gather<<<nblk(nint), ATPB, 0, s>>>(P, g, W, A, lam_in);
-    k_rv_pbar<<<1, ATPB, 0, s>>>(part, L.nparts, pbar);
+    dclaw_adj_member M;
+    memset(&M, 0, sizeof(M));
+    M.mx = mx;
+    M.my = my;
+    M.dx = dx;
+    M.dy = dy;
+    dclaw_adj_member* mem = (dclaw_adj_member*)(base + T.off_mem);
+    dclaw_params* prm = (dclaw_params*)(base + T.off_prm);
+    k_adj_single_setup<<<1, 32, 0, s>>>(M, *p, mem, prm);
+    BatchArgs a{1, mem, prm, dt, q_in, b, lam_out, lam_in, base, status};
+    launch_block_adjoint(a, (uint32_t)((size_t)L.act_nx * L.act_ny), base + T.off_lists,
+                         (unsigned int*)(base + T.off_counts), sm_count_adj(), s);
+    k_adj_batch_pbar<<<1, ATPB, 0, s>>>(a, pbar);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DCLAW_OK : DCLAW_ERR_CUDA;
 }
@@ -720,35 +598,8 @@ int dclaw_step_adjoint_batched(const dclaw_adj_batch* batch, const dclaw_adj_mem
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     BatchArgs a{batch->nmembers, members, params, dt, q_in, b, lam_out, lam_in, (char*)work, status};
     char* lists = (char*)work + (batch->work_bytes - 256 - 2 * align256((size_t)batch->nblocks * 8));
-    uint64_t* list_act = (uint64_t*)lists;
-    uint64_t* list_dil = (uint64_t*)(lists + align256((size_t)batch->nblocks * 8));
     unsigned int* counts = (unsigned int*)((char*)work + (batch->work_bytes - 256));
-    const dim3 per_member(64, (unsigned)batch->nmembers);
-    k_adj_batch_zero<<<per_member, 256, 0, s>>>(a, counts);
-    k_adj_batch_scan<<<per_member, 256, 0, s>>>(a);
-    k_adj_batch_list<<<dim3(8, (unsigned)batch->nmembers), 256, 0, s>>>(a, counts, list_act, list_dil);
-    // persistent grids over the lists
-    const unsigned grid = (unsigned)nsm * 4u;
-    k_adj_blocks_zero<<<grid, ATPB, 0, s>>>(a, list_dil, counts + 1);
-#define DC_FW(op) k_adj_blocks<op><<<grid, ATPB, 0, s>>>(a, list_dil, counts + 1)
-#define DC_RV(op) k_adj_blocks<op><<<grid, ATPB, 0, s>>>(a, list_act, counts)
-    DC_FW(OP_FW_B4);
-    DC_FW(OP_FW_TAUDIR);
-    DC_FW(OP_FW_SVREC);
-    DC_FW(OP_FW_RX);
-    DC_FW(OP_FW_RY);
-    DC_FW(OP_FW_FX);
-    DC_FW(OP_FW_FY);
-    DC_RV(OP_RV_SRC2);
-    DC_RV(OP_RV_FX);
-    DC_RV(OP_RV_FY);
-    DC_RV(OP_RV_RX);
-    DC_RV(OP_RV_RY);
-    DC_RV(OP_RV_TAUDIR);
-    DC_RV(OP_RV_B4);
-    DC_RV(OP_RV_GATHER);
-#undef DC_FW
-#undef DC_RV
+    launch_block_adjoint(a, batch->nblocks, lists, counts, nsm, s);
     k_adj_batch_pbar<<<batch->nmembers, ATPB, 0, s>>>(a, pbar);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DCLAW_OK : DCLAW_ERR_CUDA;

@@ -255,6 +255,31 @@ def test_unsupported_options_are_refused(cuda_device):
         StepAdjoint(b, DClawParams(friction_forcing=True, manning_coefficient=0.03), 1.0, 1.0)
 
 
+def test_nan_anywhere_in_the_state_is_reported(cuda_device):
+    """A NaN in any field of any cell, near the flow or far from it, sets the
+    adjoint's status word (as the forward step's check4nans scan does); a
+    clean state leaves it at zero."""
+    from dclaw_b200 import _lib
+
+    dev = cuda_device
+    p, qn, bn = _small_flow(seed=3)
+    b = torch.tensor(bn, device=dev)
+    adj = StepAdjoint(b, p, 1.0, 1.0)
+    dtt = torch.tensor([0.01], dtype=torch.float64, device=dev)
+    lam = torch.ones(qn.shape, dtype=torch.float64, device=dev)
+    for where in [None, (3, 0, 0), (4, qn.shape[1] - 1, qn.shape[2] - 1)]:
+        q = torch.tensor(qn, device=dev)
+        if where is not None:
+            q[where] = float("nan")
+        adj.status.zero_()
+        adj.vjp(q, dtt, lam, torch.empty_like(lam), torch.zeros(4, dtype=torch.float64, device=dev))
+        if where is None:
+            adj.check_status()
+        else:
+            with pytest.raises(_lib.DClawError):
+                adj.check_status()
+
+
 def test_select_outputs_give_the_same_gradient(cuda_device):
     """Returning only selected entries (gauges) at the output steps gives the
     gradient of the same loss computed from whole output states."""
