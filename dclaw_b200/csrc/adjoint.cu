@@ -403,25 +403,30 @@ __global__ void __launch_bounds__(256) k_adj_batch_list(BatchArgs a, unsigned in
 }
 
 // pbar[4 m + k] += member m's block partials of its active blocks, summed in
-// a fixed order (thread t: slots t, t + ATPB, ...; then the threads in order)
-__global__ void __launch_bounds__(ATPB) k_adj_batch_pbar(BatchArgs a, double* __restrict__ pbar) {
-    __shared__ double red[NPB][ATPB];
+// a fixed order: thread t takes blocks t, t + BTPB, ... of each stage in
+// turn, all four parameters at once; then the threads in order
+__global__ void __launch_bounds__(BTPB) k_adj_batch_pbar(BatchArgs a, double* __restrict__ pbar) {
+    __shared__ double red[NPB][BTPB];
     const int m = blockIdx.x;
     const dclaw_adj_member M = a.mem[m];
     const AdjLayout L = adj_layout(M.mx, M.my);
     const double* part = (const double*)(a.work + M.work_off + L.off_part);
     const uint32_t* act = (const uint32_t*)(a.work + M.work_off + L.off_act);
-    const long long nb = (long long)L.act_nx * L.act_ny, ns = BLK_PBAR_OPS * nb;
-    for (int k = 0; k < NPB; ++k) {
-        double s = 0.0;
-        for (long long x = threadIdx.x; x < ns; x += ATPB)
-            if (act[x % nb]) s += part[x * NPB + k];
-        red[k][threadIdx.x] = s;
-    }
+    const int nb = L.act_nx * L.act_ny;
+    double sum[NPB] = {0.0, 0.0, 0.0, 0.0};
+    for (int p = 0; p < BLK_PBAR_OPS; ++p)
+        for (int b = threadIdx.x; b < nb; b += BTPB)
+            if (act[b]) {
+                const double* v = part + ((size_t)p * nb + b) * NPB;
+#pragma unroll
+                for (int k = 0; k < NPB; ++k) sum[k] += v[k];
+            }
+#pragma unroll
+    for (int k = 0; k < NPB; ++k) red[k][threadIdx.x] = sum[k];
     __syncthreads();
     if (threadIdx.x < NPB) {
         double s = 0.0;
-        for (int t = 0; t < ATPB; ++t) s += red[threadIdx.x][t];
+        for (int t = 0; t < BTPB; ++t) s += red[threadIdx.x][t];
         pbar[(size_t)m * NPB + threadIdx.x] += s;
     }
 }
@@ -543,7 +548,7 @@ int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, doub
     BatchArgs a{1, mem, prm, dt, q_in, b, lam_out, lam_in, base, status};
     launch_block_adjoint(a, (uint32_t)((size_t)L.act_nx * L.act_ny), base + T.off_lists,
                          (unsigned int*)(base + T.off_counts), sm_count_adj(), s);
-    k_adj_batch_pbar<<<1, ATPB, 0, s>>>(a, pbar);
+    k_adj_batch_pbar<<<1, BTPB, 0, s>>>(a, pbar);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DCLAW_OK : DCLAW_ERR_CUDA;
 }
@@ -600,7 +605,7 @@ int dclaw_step_adjoint_batched(const dclaw_adj_batch* batch, const dclaw_adj_mem
     char* lists = (char*)work + (batch->work_bytes - 256 - 2 * align256((size_t)batch->nblocks * 8));
     unsigned int* counts = (unsigned int*)((char*)work + (batch->work_bytes - 256));
     launch_block_adjoint(a, batch->nblocks, lists, counts, nsm, s);
-    k_adj_batch_pbar<<<batch->nmembers, ATPB, 0, s>>>(a, pbar);
+    k_adj_batch_pbar<<<batch->nmembers, BTPB, 0, s>>>(a, pbar);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DCLAW_OK : DCLAW_ERR_CUDA;
 }
