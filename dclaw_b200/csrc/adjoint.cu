@@ -235,6 +235,33 @@ __device__ __forceinline__ void block_item(const BatchArgs& a, int m, const dcla
     }
 }
 
+// In a listed block that is not active (a neighbour of active blocks) only
+// the items near an active block matter: whether activity cell (ci, cj) lies
+// within `margin` cells (Chebyshev) of one of the eight blocks around its
+// block that is active. Active items read at most 3 cells away; each
+// forward stage reads its inputs at most 2 cells further, so the margins
+// grow along the forward chain (all below the block width).
+__device__ __forceinline__ bool near_active_block(const uint32_t* __restrict__ act, int nx, int ny, int bx, int by,
+                                                  int ci, int cj, int margin) {
+    const int px = ci + 1, py = cj + 1;
+    for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+            const int x = bx + dx, y = by + dy;
+            if ((dx == 0 && dy == 0) || x < 0 || y < 0 || x >= nx || y >= ny || !act[y * nx + x]) continue;
+            const int ex = dx < 0 ? px - (bx * ACT_TILE - 1) : dx > 0 ? (bx + 1) * ACT_TILE - px : 0;
+            const int ey = dy < 0 ? py - (by * ACT_TILE - 1) : dy > 0 ? (by + 1) * ACT_TILE - py : 0;
+            if ((ex > ey ? ex : ey) <= margin) return true;
+        }
+    return false;
+}
+
+template <int OP>
+struct FwMargin {
+    static constexpr int value = OP == OP_FW_B4 ? 10 : (OP == OP_FW_TAUDIR || OP == OP_FW_SVREC) ? 8
+                                 : (OP == OP_FW_RX || OP == OP_FW_RY) ? 6 : 4;
+};
+constexpr int ZERO_MARGIN = 4;
+
 // One stage over a list of (member, block) entries (grid-stride; every
 // thread of a CTA runs the same iterations, so the barriers are uniform).
 // A CTA has one thread per item of a 16 x 16 block; two CTAs per SM at up
@@ -269,8 +296,13 @@ __global__ void __launch_bounds__(BTPB, DCLAW_ADJ_MINB / 2) k_adj_blocks(BatchAr
         batch_member_work(a, sM, L, W, A, act);
         const int bx = blk % L.act_nx, by = blk / L.act_nx;
         const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+        const int ci = bx * ACT_TILE + tx - 1, cj = by * ACT_TILE + ty - 1;
         double pb[NPB] = {0.0, 0.0, 0.0, 0.0};
-        block_item<OP>(a, m, sM, sP, g, W, A, L, bx * ACT_TILE + tx - 1, by * ACT_TILE + ty - 1, pb);
+        // forward stages run over active blocks and their neighbours; in a
+        // neighbour, only near the active ones
+        if (OpTraits<OP>::PBAR || OP >= OP_RV_SRC2 || act[blk] ||
+            near_active_block(act, L.act_nx, L.act_ny, bx, by, ci, cj, FwMargin<OP>::value))
+            block_item<OP>(a, m, sM, sP, g, W, A, L, ci, cj, pb);
         if (OpTraits<OP>::PBAR) {
             const int pidx = OP == OP_RV_SRC2 ? 0 : OP == OP_RV_RX ? 1 : OP == OP_RV_RY ? 2 : 3;
             double* part = (double*)(a.work + sM.work_off + L.off_part);
@@ -280,8 +312,11 @@ __global__ void __launch_bounds__(BTPB, DCLAW_ADJ_MINB / 2) k_adj_blocks(BatchAr
     }
 }
 
-// zero the reverse planes of the listed blocks' items (the slots active
-// items read; the rest of the planes is never read)
+// zero the reverse planes of the listed blocks that are not active: an
+// active block's items write every slot of theirs (each reverse item writes
+// all of its outputs) before a later stage reads them, so only the slots of
+// the inactive neighbours, which active items read near the block edges,
+// need zeros; the rest of the planes is never read
 __global__ void __launch_bounds__(BTPB) k_adj_blocks_zero(BatchArgs a, const uint64_t* __restrict__ list,
                                                           const unsigned int* __restrict__ count) {
     const unsigned int n = *count;
@@ -295,11 +330,12 @@ __global__ void __launch_bounds__(BTPB) k_adj_blocks_zero(BatchArgs a, const uin
         AdjWork A;
         uint32_t* act;
         batch_member_work(a, M, L, W, A, act);
+        if (act[blk]) continue;
         const int bx = blk % L.act_nx, by = blk / L.act_nx;
         const int mx = g.mx, my = g.my;
         const size_t nint = (size_t)mx * my, nxi = L.S.nxi, nyi = L.S.nyi, npad = L.S.npad;
-        {
-            const int ci = bx * ACT_TILE + (threadIdx.x & 15) - 1, cj = by * ACT_TILE + (threadIdx.x >> 4) - 1;
+        const int ci = bx * ACT_TILE + (threadIdx.x & 15) - 1, cj = by * ACT_TILE + (threadIdx.x >> 4) - 1;
+        if (near_active_block(act, L.act_nx, L.act_ny, bx, by, ci, cj, ZERO_MARGIN)) {
             if (ci >= 1 && cj >= 1 && ci <= mx && cj <= my) {
                 const size_t c = (size_t)(cj - 1) * mx + (size_t)(ci - 1);
                 for (int f = 0; f < 5; ++f) A.lamq[f * nint + c] = 0.0;
