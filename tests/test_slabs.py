@@ -132,3 +132,32 @@ def test_local_slabs_equal_the_whole_patch_step(cuda_device, n, mx, my, nslabs, 
     for s in sl.slabs:
         assert torch.equal(s.st.clock, ref.clock)
     assert not torch.equal(ref.state(), q0)
+
+
+def test_step_rows_argument_checks():
+    """dclaw_step_rows takes whole tile rows only and refuses bad ranges,
+    sizes and workspaces on the host, before any device work."""
+    import ctypes
+
+    from dclaw_b200 import _lib
+    from dclaw_b200.params import DClawParams
+
+    lib = _lib.load()
+    assert lib.dclaw_rows_granule() == G
+    mx, my = 50, 100
+    need = lib.dclaw_workspace_bytes(mx, my)
+    cp = DClawParams().to_c()
+    one, two = ctypes.c_void_p(256), ctypes.c_void_p(512)
+
+    def call(first, count, work=need, q_out=two):
+        return lib.dclaw_step_rows(one, q_out, one, mx, my, 1.0, 1.0, ctypes.byref(cp), one, one, work, first,
+                                   count, None)
+
+    assert call(2, 14) == 1           # does not start a tile row
+    assert call(1, 13) == 1           # does not end on one (and not at the last row)
+    assert call(0, 14) == 1
+    assert call(99, 14) == 1          # beyond the patch
+    assert call(1, 0) == 1
+    assert call(15, 28, q_out=one) == 1   # in place
+    assert call(15, 28, work=1024) == 5
+    assert lib.dclaw_clock_tick(None, ctypes.byref(cp), None) == 1
