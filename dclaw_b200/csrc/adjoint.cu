@@ -272,6 +272,8 @@ __global__ void __launch_bounds__(BTPB, DCLAW_ADJ_MINB / 2) k_adj_blocks(BatchAr
     __shared__ dclaw_adj_member sM;
     __shared__ dclaw_params sP;
     __shared__ uint64_t s_e;
+    __shared__ int s_list[BTPB];
+    __shared__ int s_n;
     const unsigned int n = *count;
     int cur = -1;
     for (unsigned int k = blockIdx.x; k < n; k += gridDim.x) {
@@ -298,11 +300,48 @@ __global__ void __launch_bounds__(BTPB, DCLAW_ADJ_MINB / 2) k_adj_blocks(BatchAr
         const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
         const int ci = bx * ACT_TILE + tx - 1, cj = by * ACT_TILE + ty - 1;
         double pb[NPB] = {0.0, 0.0, 0.0, 0.0};
-        // forward stages run over active blocks and their neighbours; in a
-        // neighbour, only near the active ones
-        if (OpTraits<OP>::PBAR || OP >= OP_RV_SRC2 || act[blk] ||
-            near_active_block(act, L.act_nx, L.act_ny, bx, by, ci, cj, FwMargin<OP>::value))
+        if (OP == OP_RV_RX || OP == OP_RV_RY) {
+            // the reverse of a dry-dry solve writes zeros (the forward
+            // skipped it): those items store their zeros here, the others
+            // are gathered into a dense list so that the warps running the
+            // reverse solver are full of them
+            constexpr int DIR = OP == OP_RV_RX ? 0 : 1;
+            const int mx = g.mx, my = g.my;
+            const bool valid = DIR == 0 ? (ci >= 0 && cj >= 0 && ci <= mx + 2 && cj <= my + 1)
+                                        : (ci >= 0 && cj >= 0 && ci <= mx + 1 && cj <= my + 2);
+            bool need = false;
+            if (valid) {
+                // x: row r = cj, interface i = ci (cells i-1, i); y: column r = ci, interface i = cj
+                const size_t pL = DIR == 0 ? pidx(g, ci - 1, cj) : pidx(g, ci, cj - 1);
+                const size_t pR = pidx(g, ci, cj);
+                need = !(W.qB[pL] <= sP.dry_tolerance && W.qB[pR] <= sP.dry_tolerance);
+                if (!need) {
+                    double* dst = DIR == 0 ? A.xcb : A.ycb;
+                    const size_t np = DIR == 0 ? W.nxi : W.nyi;
+                    const size_t oi = DIR == 0 ? xidx(g, cj, ci) : yidx(g, cj, ci);
+                    for (int k = 0; k < NCB; ++k) dst[(size_t)k * np + oi] = 0.0;
+                }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, need);
+            const int lane = threadIdx.x & 31;
+            if (threadIdx.x == 0) s_n = 0;
+            __syncthreads();
+            int base = 0;
+            if (lane == 0 && bal) base = atomicAdd(&s_n, __popc(bal));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (need) s_list[base + __popc(bal & ((1u << lane) - 1u))] = threadIdx.x;
+            __syncthreads();
+            if ((int)threadIdx.x < s_n) {
+                const int t = s_list[threadIdx.x];
+                block_item<OP>(a, m, sM, sP, g, W, A, L, bx * ACT_TILE + (t & 15) - 1, by * ACT_TILE + (t >> 4) - 1,
+                               pb);
+            }
+        } else if (OpTraits<OP>::PBAR || OP >= OP_RV_SRC2 || act[blk] ||
+                   near_active_block(act, L.act_nx, L.act_ny, bx, by, ci, cj, FwMargin<OP>::value)) {
+            // forward stages run over active blocks and their neighbours; in
+            // a neighbour, only near the active ones
             block_item<OP>(a, m, sM, sP, g, W, A, L, ci, cj, pb);
+        }
         if (OpTraits<OP>::PBAR) {
             const int pidx = OP == OP_RV_SRC2 ? 0 : OP == OP_RV_RX ? 1 : OP == OP_RV_RY ? 2 : 3;
             double* part = (double*)(a.work + sM.work_off + L.off_part);
