@@ -161,3 +161,27 @@ def test_step_rows_argument_checks():
     assert call(15, 28, q_out=one) == 1   # in place
     assert call(15, 28, work=1024) == 5
     assert lib.dclaw_clock_tick(None, ctypes.byref(cp), None) == 1
+
+
+@pytest.mark.gpu
+def test_dist_slabs_single_rank_equals_the_whole_patch_step(cuda_device):
+    """DistSlabs with no process group is one slab holding the whole patch:
+    its per-step calls (own rows, Courant bits, tick) equal dclaw_step."""
+    from dclaw_b200 import workloads as W
+    from dclaw_b200.slabs import DistSlabs
+    from dclaw_b200.solver import PatchStepper
+
+    dev = cuda_device
+    c = W.random_field_case(n=120, dx=0.5, seed=43)
+    q0 = torch.tensor(c.q, device=dev)
+    b = torch.tensor(c.b, device=dev)
+    ref = PatchStepper(q0, b, c.params, c.dx, c.dy)
+    ref.init_clock(c.dt_initial)
+    sl = DistSlabs(q0, b, c.params, c.dx, c.dy)
+    assert (sl.rank, sl.world) == (0, 1)
+    sl.init_clock(c.dt_initial)
+    ref.step(6)
+    sl.step(6)
+    torch.cuda.synchronize()
+    assert torch.equal(sl.own(), ref.state())
+    assert torch.equal(sl.slab.st.clock, ref.clock)
