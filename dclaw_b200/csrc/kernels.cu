@@ -915,10 +915,11 @@ constexpr int MAX_HOST_BANDS = 64;
 
 inline int host_auto_bands(int mx, int my) {
     const int nty = (my + TILE_Y - 1) / TILE_Y;
-    // about 40 MB of state per band in the middle of the plan: enough work
-    // per band to fill the GPU and few enough launches and copies (equal
-    // bands on the 4096^2 state: 16 bands took 1.07x the time of the bare
-    // copies both ways at once, 4 bands 1.25x, 64 bands 1.22x)
+    // about 40 MB of state per band: enough work per band to fill the GPU
+    // and few enough launches and copies, fine enough that the first upload
+    // and the last download (the parts that do not overlap) stay short. On
+    // the 4096^2 state (16 bands) the step then takes 1.07x the time of
+    // the bare copies both ways at once; 4 bands take 1.25x, 64 take 1.22x.
     const double state = 40.0 * mx * (double)my;
     int nb = (int)(state / 40.0e6) + 1;
     if (nb > MAX_HOST_BANDS) nb = MAX_HOST_BANDS;
@@ -926,39 +927,10 @@ inline int host_auto_bands(int mx, int my) {
     return nb < 1 ? 1 : nb;
 }
 
-// first tile row of each band (first[0..nb], first[nb] = tile rows): nb
-// equal bands
+// first tile row of each band (first[0..nb], first[nb] = tile rows)
 inline void host_band_plan(int my, int nb, int* first) {
     const int nty = (my + TILE_Y - 1) / TILE_Y;
     for (int g = 0; g <= nb; ++g) first[g] = (int)((long long)g * nty / nb);
-}
-
-// The automatic plan: bands of about nty / nb tile rows in the middle, and
-// sizes doubling from one tile row up to that at both ends, so that the first
-// upload (before any compute) and the last download (after it) are short.
-// Returns the band count (at most MAX_HOST_BANDS); equal bands when the patch
-// is too short for the ramps.
-inline int host_ramp_plan(int my, int nb, int* first) {
-    const int nty = (my + TILE_Y - 1) / TILE_Y;
-    const int S = nty / (nb > 0 ? nb : 1);
-    int ramp[16], nr = 0, rsum = 0;
-    for (int r = 1; r < S && nr < 16; r *= 2) {
-        ramp[nr++] = r;
-        rsum += r;
-    }
-    const int rem = nty - 2 * rsum;
-    int nmid = S > 0 ? (rem + S / 2) / S : 0;
-    if (nr == 0 || rem < S || nmid < 1 || 2 * nr + nmid > MAX_HOST_BANDS) {
-        host_band_plan(my, nb, first);
-        return nb;
-    }
-    int g = 0, at = 0;
-    first[g++] = 0;
-    for (int k = 0; k < nr; ++k) first[g++] = (at += ramp[k]);
-    for (int k = 1; k <= nmid; ++k) first[g++] = rsum + (int)((long long)k * rem / nmid);
-    at = rsum + rem;
-    for (int k = nr - 1; k >= 0; --k) first[g++] = (at += ramp[k]);
-    return g - 1;
 }
 
 struct HostPipe {
@@ -1139,8 +1111,7 @@ int dclaw_step_host_bands(int mx, int my, int nbands, int32_t* first, int max) {
     int nb = nbands == 0 ? host_auto_bands(mx, my) : (nbands > nty ? nty : nbands);
     if (nb > MAX_HOST_BANDS) nb = MAX_HOST_BANDS;
     int f[MAX_HOST_BANDS + 1];
-    if (nbands == 0) nb = host_ramp_plan(my, nb, f);
-    else host_band_plan(my, nb, f);
+    host_band_plan(my, nb, f);
     for (int g = 0; first && g <= nb && g < max; ++g) first[g] = f[g];
     return nb;
 }

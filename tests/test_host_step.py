@@ -38,16 +38,9 @@ def test_band_plan_covers_every_tile_row():
                 assert nb == min(nbands, nty, 64)
             assert first[0] == 0 and first[-1] == nty
             assert all(b > a for a, b in zip(first, first[1:]))      # every band holds a tile row
-    # the automatic choice: about 40 MB of state per band in the middle
-    # (17 tile rows at 4096^2), and sizes doubling from one tile row at both
-    # ends, so that the first upload and the last download are short
-    nb, first = _plan(lib, 4096, 4096, 0)
-    sizes = [b - a for a, b in zip(first, first[1:])]
-    assert sizes[:5] == [1, 2, 4, 8, 16] and sizes[-5:] == [16, 8, 4, 2, 1]
-    assert all(16 <= x <= 17 for x in sizes[5:-5]) and nb == 24
-    # too short for the ramps: equal bands
-    nb, first = _plan(lib, 100, 20000, 0)
-    assert [b - a for a, b in zip(first, first[1:])] == [476, 476, 477]
+    # the automatic choice: about 40 MB of state per band
+    nb, _ = _plan(lib, 4096, 4096, 0)
+    assert nb == int(40 * 4096 * 4096 / 40e6) + 1 == 17
     assert _plan(lib, 64, 64, 0)[0] == 1
     assert lib.dclaw_step_host_bands(1, 10, 0, None, 0) == 0
 
@@ -80,7 +73,6 @@ def _case(n, mx, my, seed):
 @pytest.mark.gpu
 @pytest.mark.parametrize("mx,my,nbands,inplace,pinned", [
     (200, 200, 0, True, True),
-    (2048, 2048, 0, False, True),       # the automatic plan with its ramps (13 bands)
     (200, 200, 1, False, True),
     (200, 200, 3, True, True),
     (200, 200, 15, False, True),        # one band per tile row
@@ -92,7 +84,7 @@ def test_host_step_matches_device_step(cuda_device, mx, my, nbands, inplace, pin
     from dclaw_b200.solver import PatchStepper
 
     dev = cuda_device
-    c, qn, bn = _case(max(200, mx, my), mx, my, 31)
+    c, qn, bn = _case(200, mx, my, 31)
     q0 = torch.tensor(qn, device=dev)
     b = torch.tensor(bn, device=dev)
     ref = PatchStepper(q0, b, c.params, c.dx, c.dy)
