@@ -42,10 +42,10 @@ sys.path.insert(0, str(ROOT))
 
 BYTES_PER_CELL_UPDATE = 88  # read 5 state + 1 bed, write 5 state (FP64)
 # DRAM bytes (read + write) of one fused step measured by ncu on the 2048 x 2048
-# random-field case: k_records 357.4 MB + k_tile 170.1 MB + k_src2_cells 157.4 MB;
+# random-field case: k_records 361.7 MB + k_tile 170.4 MB + k_src2_cells 158.9 MB;
 # the case keeps its wet fraction at every size, so the bytes scale with the cell
 # count
-NCU_STEP_BYTES_2048 = 684.9e6
+NCU_STEP_BYTES_2048 = 690.9e6
 METRIC = "cell-updates/sec on 1 B200 (plain vs batched); gradient/forward time ratio"
 
 

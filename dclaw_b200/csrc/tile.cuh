@@ -80,16 +80,6 @@ DC_HD bool cell_record(const dclaw_params& P, const Geom& g, const double* __res
     const size_t plane = (size_t)mx * my;
     const size_t c = (size_t)(sj - 1) * mx + (size_t)(si - 1);
     const size_t pi = pidx(g, i, j);
-    // calc_taudir's neighbour depths are loaded with the cell's own fields,
-    // so that a cell costs one memory round trip, not two
-    const bool ring = i >= 0 && j >= 0 && i <= mx + 1 && j <= my + 1;
-    double hL = 0.0, hR = 0.0, hB = 0.0, hT = 0.0;
-    if (ring) {
-        hL = qB_h(P, g, q_in, i - 1, j);
-        hR = qB_h(P, g, q_in, i + 1, j);
-        hB = qB_h(P, g, q_in, i, j - 1);
-        hT = qB_h(P, g, q_in, i, j + 1);
-    }
     // every field is read: a NaN anywhere in the state is reported, as the
     // reference's check4nans does before b4step2
     double h = q_in[c];
@@ -139,8 +129,10 @@ DC_HD bool cell_record(const dclaw_params& P, const Geom& g, const double* __res
         R.put(R_TAU2, pi, tau2);
     }
     // calc_taudir on the inner ghost ring and the interior
-    if (ring) {
+    if (i >= 0 && j >= 0 && i <= mx + 1 && j <= my + 1) {
         const double dry = P.dry_tolerance, gz = P.grav;
+        double hL = qB_h(P, g, q_in, i - 1, j), hR = qB_h(P, g, q_in, i + 1, j);
+        double hB = qB_h(P, g, q_in, i, j - 1), hT = qB_h(P, g, q_in, i, j + 1);
         if (!((h + hL + hB + hR + hT) < dry)) {
             double b = bed_at(g, b_in, i, j);
             double eta = h + b;
