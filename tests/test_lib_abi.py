@@ -55,3 +55,40 @@ def test_ctypes_struct_matches_header_size():
     # dclaw_params: 8 doubles + 2 int32 + ... checked by field offsets of the ctypes image
     assert ctypes.sizeof(CParams) % 8 == 0
     assert CParams.bc_lower.offset % 4 == 0
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """Every ctypes image of a header struct has the C compiler's size and
+    field offsets (a C probe compiled against include/dclaw_b200.h)."""
+    import shutil
+    import subprocess
+
+    import pytest
+
+    from dclaw_b200.params import CAdjBatch, CAdjMember, CBatch, CClock, CMember
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    images = {"dclaw_params": CParams, "dclaw_clock": CClock, "dclaw_member": CMember, "dclaw_batch": CBatch,
+              "dclaw_adj_member": CAdjMember, "dclaw_adj_batch": CAdjBatch}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "dclaw_b200.h"', "int main(void) {"]
+    for cname, img in images.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, *_ in img._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "probe"
+    subprocess.run([cc, "-I", str(HEADER.parent), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        if line:
+            cname, key, val = line.split()
+            got[(cname, key)] = int(val)
+    for cname, img in images.items():
+        assert got[(cname, "size")] == ctypes.sizeof(img), cname
+        for fname, *_ in img._fields_:
+            assert got[(cname, fname)] == getattr(img, fname).offset, f"{cname}.{fname}"
