@@ -12,13 +12,17 @@ sqrt(N) time checkpointing:
 * forward: run the fused step, record each step's dt on the device, keep the
   state every k steps and the states the caller asked for. Unless k is
   given, it is the smallest block whose checkpoints fit half of the free
-  device memory (after the adjoint's workspace): every state (k = 1, no
+  device memory (after the adjoint's two workspaces): every state (k = 1, no
   recompute) when the run fits, as a 512 x 512 run of 500 steps (5 GB)
   does in a B200's 180 GB, and at most ceil(sqrt(n_steps));
 * backward: for each block of k steps, last block first, recompute its
   states from its checkpoint with the recorded dts (bit-identical, so every
   branch is the one the forward took), then run the step adjoint backwards
   through the block, adding the caller's output gradients as it passes them.
+  Each step adjoint is queued in two parts: the part that does not read
+  the output adjoint (the forward recompute, `prepare`) runs on a side
+  stream one step ahead, in a second workspace, while the previous step's
+  reverse stages run on a high-priority stream.
 
 Time steps are data: the dt of each step (chosen by D-Claw's tick rule from
 the previous Courant number, or fixed) is recorded in the forward pass and
@@ -81,12 +85,68 @@ class StepAdjoint:
                                          _lib.ptr(self.status), _lib.stream_ptr())
         _lib.check(rc, "dclaw_step_adjoint")
 
+    def prepare(self, q_in: torch.Tensor, dt: torch.Tensor) -> None:
+        """The part of vjp that does not read lam_out (activity blocks and the
+        forward recompute into this object's workspace)."""
+        rc = self.lib.dclaw_step_adjoint_prepare(_lib.ptr(q_in), _lib.ptr(self.b), self.mx, self.my, self.dx,
+                                                 self.dy, _lib.ptr(dt), ctypes.byref(self.cp), _lib.ptr(self.work),
+                                                 self.work_bytes, _lib.ptr(self.status), _lib.stream_ptr())
+        _lib.check(rc, "dclaw_step_adjoint_prepare")
+
+    def reverse(self, q_in: torch.Tensor, dt: torch.Tensor, lam_out: torch.Tensor, lam_in: torch.Tensor,
+                pbar: torch.Tensor) -> None:
+        """The rest of vjp, after prepare with the same q_in and dt."""
+        rc = self.lib.dclaw_step_adjoint_reverse(_lib.ptr(q_in), _lib.ptr(self.b), self.mx, self.my, self.dx,
+                                                 self.dy, _lib.ptr(dt), ctypes.byref(self.cp), _lib.ptr(lam_out),
+                                                 _lib.ptr(lam_in), _lib.ptr(pbar), _lib.ptr(self.work),
+                                                 self.work_bytes, _lib.ptr(self.status), _lib.stream_ptr())
+        _lib.check(rc, "dclaw_step_adjoint_reverse")
+
     def check_status(self) -> None:
         _lib.check(int(self.status.item()), "adjoint step")
 
 
+def _reverse_block(adjs, steps, state_of, dt_of, lam, lam2, pbar, add_outs):
+    """The step adjoints of `steps` (descending step numbers), each step's
+    prepare queued on a side stream ahead of the previous step's reverse.
+
+    adjs: two adjoint objects (two workspaces), used alternately; state_of(n)
+    / dt_of(n): the input state and dt of step n; add_outs(n): adds the
+    output gradients at step count n into lam. The reverses run on a
+    high-priority stream, the prepares (which do not read lam) on a normal
+    one, so the prepare of step n-1 fills the SMs the reverse of step n
+    leaves idle. Returns the final (lam, lam2)."""
+    cur = torch.cuda.current_stream()
+    rev = torch.cuda.Stream(priority=-8)        # mapped to the device's highest priority
+    side = torch.cuda.Stream()
+    rev.wait_stream(cur)
+    side.wait_stream(cur)
+    last_rev = [None, None]               # the last reverse that used each workspace
+    with torch.cuda.stream(side):
+        adjs[steps[0] % 2].prepare(state_of(steps[0]), dt_of(steps[0]))
+    ev_prep = side.record_event()
+    for idx, n in enumerate(steps):
+        w = n % 2
+        with torch.cuda.stream(rev):
+            rev.wait_event(ev_prep)
+            add_outs(n, lam)
+            adjs[w].reverse(state_of(n), dt_of(n), lam, lam2, pbar)
+            last_rev[w] = rev.record_event()
+        if idx + 1 < len(steps):
+            n2 = steps[idx + 1]
+            with torch.cuda.stream(side):
+                if last_rev[n2 % 2] is not None:
+                    side.wait_event(last_rev[n2 % 2])
+                adjs[n2 % 2].prepare(state_of(n2), dt_of(n2))
+            ev_prep = side.record_event()
+        lam, lam2 = lam2, lam
+    cur.wait_stream(rev)
+    cur.wait_stream(side)
+    return lam, lam2
+
+
 # share of the device memory free when a differentiable run starts that its
-# checkpoints may take (the step adjoint's workspace is set aside first)
+# checkpoints may take (the step adjoint's two workspaces are set aside first)
 CHECKPOINT_MEMORY_FRACTION = 0.5
 
 
@@ -133,7 +193,7 @@ class _Rollout(torch.autograd.Function):
             st.init_clock(float(dt0), t_final=float(t_final), fixed_dt=bool(fixed_dt))
         lib = _lib.load()
         k = _block(n_steps, checkpoint_block, q0.numel() * 8,
-                   lib.dclaw_adjoint_workspace_bytes(q0.shape[2], q0.shape[1]), q0.device)
+                   2 * lib.dclaw_adjoint_workspace_bytes(q0.shape[2], q0.shape[1]), q0.device)
         dts = torch.empty(n_steps, dtype=torch.float64, device=q0.device)
         oshape = tuple(q0.shape) if select is None else tuple(select.shape)
         outs = torch.empty((len(out_steps),) + oshape, dtype=q0.dtype, device=q0.device)
@@ -181,7 +241,7 @@ class _Rollout(torch.autograd.Function):
         where = {}
         for idx, n in enumerate(out_steps):
             where.setdefault(n, []).append(idx)
-        adj = StepAdjoint(b, prm, dx, dy)
+        adjs = [StepAdjoint(b, prm, dx, dy), StepAdjoint(b, prm, dx, dy)]
         fw = PatchStepper(ckpt[0], b, prm, dx, dy)
         fw.init_clock(0.0, fixed_dt=True)
         lam = torch.zeros(shape, dtype=torch.float64, device=dev)
@@ -191,13 +251,23 @@ class _Rollout(torch.autograd.Function):
         g_out = g_out.contiguous() if g_out is not None else None
         sel = ctx.select
 
-        def add_out(idx):
+        def add_out(idx, target):
             if sel is None:
-                lam.add_(g_out[idx])
+                target.add_(g_out[idx])
             else:
-                lam.view(-1).index_add_(0, sel.reshape(-1), g_out[idx].reshape(-1))
+                target.view(-1).index_add_(0, sel.reshape(-1), g_out[idx].reshape(-1))
 
         nblocks = len(ckpt)
+        if k == 1:
+            # every state kept: the whole backward pass is one pipelined run
+            def add_outs1(n, target):
+                if g_out is not None:
+                    for idx in where.get(n, []):
+                        add_out(idx, target)
+
+            lam, lam2 = _reverse_block(adjs, list(range(n_steps, 0, -1)), lambda n: ckpt[n - 1],
+                                       lambda n: dts[n - 1:n], lam, lam2, pbar, add_outs1)
+            nblocks = 0
         for s in reversed(range(nblocks)):
             n0 = s * k
             n1 = min(n0 + k, n_steps)
@@ -208,17 +278,20 @@ class _Rollout(torch.autograd.Function):
                 fw.clock[1:2].copy_(dts[n - 1:n])
                 fw._launch(states[-1], seg[n - n0])
                 states.append(seg[n - n0])
-            for n in range(n1, n0, -1):
+
+            def add_outs(n, target):
                 if g_out is not None:
                     for idx in where.get(n, []):
-                        add_out(idx)
-                adj.vjp(states[n - 1 - n0], dts[n - 1:n], lam, lam2, pbar)
-                lam, lam2 = lam2, lam
+                        add_out(idx, target)
+
+            lam, lam2 = _reverse_block(adjs, list(range(n1, n0, -1)), lambda n: states[n - 1 - n0],
+                                       lambda n: dts[n - 1:n], lam, lam2, pbar, add_outs)
         if g_out is not None:
             for idx in where.get(0, []):
-                add_out(idx)
+                add_out(idx, lam)
         _lib.check(fw.status(), "rollout recompute")
-        adj.check_status()
+        for adj in adjs:
+            adj.check_status()
         scale = torch.tensor([_DEG, 1.0, 1.0, 1.0], dtype=torch.float64, device=dev)
         return lam, pbar * scale, None, None, None, None, None, None, None, None, None, None, None, None
 
@@ -321,6 +394,22 @@ class EnsembleStepAdjoint:
         self.work = torch.empty(self.batch.work_bytes, dtype=torch.uint8, device=dev)
         self.status = torch.zeros(self.n, dtype=torch.int32, device=dev)
 
+    def prepare(self, q_in: torch.Tensor, dts: torch.Tensor) -> None:
+        rc = self.lib.dclaw_step_adjoint_batched_prepare(ctypes.byref(self.batch), _lib.ptr(self.members_dev),
+                                                         _lib.ptr(self.params), _lib.ptr(dts), _lib.ptr(q_in),
+                                                         _lib.ptr(self.bed), _lib.ptr(self.work),
+                                                         _lib.ptr(self.status), _lib.stream_ptr())
+        _lib.check(rc, "dclaw_step_adjoint_batched_prepare")
+
+    def reverse(self, q_in: torch.Tensor, dts: torch.Tensor, lam_out: torch.Tensor, lam_in: torch.Tensor,
+                pbar: torch.Tensor) -> None:
+        rc = self.lib.dclaw_step_adjoint_batched_reverse(ctypes.byref(self.batch), _lib.ptr(self.members_dev),
+                                                         _lib.ptr(self.params), _lib.ptr(dts), _lib.ptr(q_in),
+                                                         _lib.ptr(self.bed), _lib.ptr(lam_out), _lib.ptr(lam_in),
+                                                         _lib.ptr(pbar), _lib.ptr(self.work),
+                                                         _lib.ptr(self.status), _lib.stream_ptr())
+        _lib.check(rc, "dclaw_step_adjoint_batched_reverse")
+
     def vjp(self, q_in: torch.Tensor, dts: torch.Tensor, lam_out: torch.Tensor, lam_in: torch.Tensor,
             pbar: torch.Tensor) -> None:
         rc = self.lib.dclaw_step_adjoint_batched(ctypes.byref(self.batch), _lib.ptr(self.members_dev),
@@ -356,7 +445,7 @@ class _EnsembleRollout(torch.autograd.Function):
         st = _ensemble(members, theta, fixed_dt or dt_schedule is not None)
         st.qa.copy_(q0.detach())
         lib = _lib.load()
-        reserve = sum(lib.dclaw_adjoint_workspace_bytes(m.q.shape[2], m.q.shape[1]) for m in members)
+        reserve = 2 * sum(lib.dclaw_adjoint_workspace_bytes(m.q.shape[2], m.q.shape[1]) for m in members)
         k = _block(n_steps, checkpoint_block, st.qa.numel() * 8, reserve, q0.device)
         dts = torch.empty((n_steps, st.n), dtype=torch.float64, device=q0.device)
         oshape = tuple(q0.shape) if select is None else tuple(select.shape)
@@ -403,7 +492,7 @@ class _EnsembleRollout(torch.autograd.Function):
         for idx, n in enumerate(out_steps):
             where.setdefault(n, []).append(idx)
         fw = _ensemble(members, theta, True)
-        adj = EnsembleStepAdjoint(fw)
+        adjs = [EnsembleStepAdjoint(fw), EnsembleStepAdjoint(fw)]
         lam = torch.zeros_like(fw.qa)
         lam2 = torch.zeros_like(lam)   # arena gaps between members stay zero
         pbar = torch.zeros((fw.n, 4), dtype=torch.float64, device=dev)
@@ -411,13 +500,24 @@ class _EnsembleRollout(torch.autograd.Function):
         g_out = g_out.contiguous() if g_out is not None else None
         sel = ctx.select
 
-        def add_out(idx):
+        def add_out(idx, target):
             if sel is None:
-                lam.add_(g_out[idx])
+                target.add_(g_out[idx])
             else:
-                lam.index_add_(0, sel.reshape(-1), g_out[idx].reshape(-1))
+                target.index_add_(0, sel.reshape(-1), g_out[idx].reshape(-1))
 
-        for s in reversed(range(len(ckpt))):
+        def add_outs(n, target):
+            if g_out is not None:
+                for idx in where.get(n, []):
+                    add_out(idx, target)
+
+        nblocks = len(ckpt)
+        if k == 1:
+            # every state kept: the whole backward pass is one pipelined run
+            lam, lam2 = _reverse_block(adjs, list(range(n_steps, 0, -1)), lambda n: ckpt[n - 1],
+                                       lambda n: dts[n - 1], lam, lam2, pbar, add_outs)
+            nblocks = 0
+        for s in reversed(range(nblocks)):
             n0 = s * k
             n1 = min(n0 + k, n_steps)
             states = [ckpt[s]]
@@ -425,18 +525,13 @@ class _EnsembleRollout(torch.autograd.Function):
                 _clock_field(fw, 1).copy_(dts[n - 1])
                 fw._launch(states[-1], seg[n - n0])
                 states.append(seg[n - n0])
-            for n in range(n1, n0, -1):
-                if g_out is not None:
-                    for idx in where.get(n, []):
-                        add_out(idx)
-                adj.vjp(states[n - 1 - n0], dts[n - 1], lam, lam2, pbar)
-                lam, lam2 = lam2, lam
-        if g_out is not None:
-            for idx in where.get(0, []):
-                add_out(idx)
+            lam, lam2 = _reverse_block(adjs, list(range(n1, n0, -1)), lambda n: states[n - 1 - n0],
+                                       lambda n: dts[n - 1], lam, lam2, pbar, add_outs)
+        add_outs(0, lam)
         for kk, st in enumerate(fw.status()):
             _lib.check(st, f"ensemble recompute, member {kk}")
-        adj.check_status()
+        for adj in adjs:
+            adj.check_status()
         scale = torch.tensor([_DEG, 1.0, 1.0, 1.0], dtype=torch.float64, device=dev)
         return lam, pbar * scale, None, None, None, None, None, None, None
 

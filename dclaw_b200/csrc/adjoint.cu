@@ -400,16 +400,22 @@ __global__ void __launch_bounds__(BTPB) k_adj_blocks_zero(BatchArgs a, const uin
 
 // member m (blockIdx.y): activity map and lam_in to zero; block 0 of member
 // 0 clears the list lengths
-__global__ void __launch_bounds__(256) k_adj_batch_zero(BatchArgs a, unsigned int* counts) {
+// (what & 1: the activity map and the list lengths; what & 2: lam_in)
+__global__ void __launch_bounds__(256) k_adj_batch_zero(BatchArgs a, unsigned int* counts, int what) {
     const dclaw_adj_member M = a.mem[blockIdx.y];
     const AdjLayout L = adj_layout(M.mx, M.my);
-    uint32_t* act = (uint32_t*)(a.work + M.work_off + L.off_act);
-    double* lam = a.lam_in + M.q_off;
-    const size_t nact = (size_t)L.act_nx * L.act_ny, nl = (size_t)5 * M.mx * M.my;
     const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
-    for (size_t x = t0; x < nact; x += st) act[x] = 0u;
-    for (size_t x = t0; x < nl; x += st) lam[x] = 0.0;
-    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < 2) counts[threadIdx.x] = 0u;
+    if (what & 1) {
+        uint32_t* act = (uint32_t*)(a.work + M.work_off + L.off_act);
+        const size_t nact = (size_t)L.act_nx * L.act_ny;
+        for (size_t x = t0; x < nact; x += st) act[x] = 0u;
+        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < 2) counts[threadIdx.x] = 0u;
+    }
+    if (what & 2) {
+        double* lam = a.lam_in + M.q_off;
+        const size_t nl = (size_t)5 * M.mx * M.my;
+        for (size_t x = t0; x < nl; x += st) lam[x] = 0.0;
+    }
 }
 
 // member m (blockIdx.y): a wet interior cell marks the blocks within
@@ -507,29 +513,36 @@ __global__ void __launch_bounds__(BTPB) k_adj_batch_pbar(BatchArgs a, double* __
 }
 
 // the step adjoint of nmem members over the block lists (all launches)
+// phase & 1: prepare (activity, lists, zeroing, forward recompute: none of
+// it reads lam_out); phase & 2: reverse (lam_in, the reverse stages)
+enum { PHASE_PREPARE = 1, PHASE_REVERSE = 2 };
 inline void launch_block_adjoint(const BatchArgs& a, uint32_t nblocks, char* lists, unsigned int* counts, int nsm,
-                                 cudaStream_t s) {
+                                 cudaStream_t s, int phase) {
     uint64_t* list_act = (uint64_t*)lists;
     uint64_t* list_dil = (uint64_t*)(lists + align256((size_t)nblocks * 8));
     // the per-member kernels fill the GPU whether there is one member or many
     int gx = 4 * nsm / (a.nmem > 0 ? a.nmem : 1);
     gx = gx < 16 ? 16 : (gx > 512 ? 512 : gx);
     const dim3 per_member((unsigned)gx, (unsigned)a.nmem);
-    k_adj_batch_zero<<<per_member, 256, 0, s>>>(a, counts);
-    k_adj_batch_scan<<<per_member, 256, 0, s>>>(a);
-    k_adj_batch_list<<<dim3(8, (unsigned)a.nmem), 256, 0, s>>>(a, counts, list_act, list_dil);
     // persistent grids over the lists
     const unsigned grid = (unsigned)nsm * 2u;
-    k_adj_blocks_zero<<<grid * 2u, BTPB, 0, s>>>(a, list_dil, counts + 1);
 #define DC_FW(op) k_adj_blocks<op><<<grid, BTPB, 0, s>>>(a, list_dil, counts + 1)
 #define DC_RV(op) k_adj_blocks<op><<<grid, BTPB, 0, s>>>(a, list_act, counts)
-    DC_FW(OP_FW_B4);
-    DC_FW(OP_FW_TAUDIR);
-    DC_FW(OP_FW_SVREC);
-    DC_FW(OP_FW_RX);
-    DC_FW(OP_FW_RY);
-    DC_FW(OP_FW_FX);
-    DC_FW(OP_FW_FY);
+    if (phase & PHASE_PREPARE) {
+        k_adj_batch_zero<<<per_member, 256, 0, s>>>(a, counts, 1);
+        k_adj_batch_scan<<<per_member, 256, 0, s>>>(a);
+        k_adj_batch_list<<<dim3(8, (unsigned)a.nmem), 256, 0, s>>>(a, counts, list_act, list_dil);
+        k_adj_blocks_zero<<<grid * 2u, BTPB, 0, s>>>(a, list_dil, counts + 1);
+        DC_FW(OP_FW_B4);
+        DC_FW(OP_FW_TAUDIR);
+        DC_FW(OP_FW_SVREC);
+        DC_FW(OP_FW_RX);
+        DC_FW(OP_FW_RY);
+        DC_FW(OP_FW_FX);
+        DC_FW(OP_FW_FY);
+    }
+    if (!(phase & PHASE_REVERSE)) return;
+    k_adj_batch_zero<<<per_member, 256, 0, s>>>(a, counts, 2);
     DC_RV(OP_RV_SRC2);
     DC_RV(OP_RV_FX);
     DC_RV(OP_RV_FY);
@@ -599,11 +612,14 @@ int dclaw_adjoint_supported(const dclaw_params* p) {
     return DCLAW_OK;
 }
 
-int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, double dx, double dy,
-                       const double* dt, const dclaw_params* p, const double* lam_out, double* lam_in,
-                       double* pbar, void* work, size_t work_bytes, int32_t* status, void* stream) {
-    if (!q_in || !b || !dt || !lam_out || !lam_in || !pbar || !work) return DCLAW_ERR_ARG;
-    if (lam_in == lam_out || !adj_sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0)) return DCLAW_ERR_ARG;
+// the single patch as a one-member batch over its workspace (phase: which
+// part of the step adjoint to queue)
+static int single_adjoint(const double* q_in, const double* b, int mx, int my, double dx, double dy,
+                          const double* dt, const dclaw_params* p, const double* lam_out, double* lam_in,
+                          double* pbar, void* work, size_t work_bytes, int32_t* status, void* stream, int phase) {
+    if (!q_in || !b || !dt || !work) return DCLAW_ERR_ARG;
+    if ((phase & PHASE_REVERSE) && (!lam_out || !lam_in || !pbar || lam_in == lam_out)) return DCLAW_ERR_ARG;
+    if (!adj_sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0)) return DCLAW_ERR_ARG;
     int rc = dclaw_adjoint_supported(p);
     if (rc) return rc;
     AdjLayout L = adj_layout(mx, my);
@@ -611,21 +627,44 @@ int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, doub
     if (work_bytes < T.total) return DCLAW_ERR_WORKSPACE;
     cudaStream_t s = (cudaStream_t)stream;
     char* base = (char*)work;
-    dclaw_adj_member M;
-    memset(&M, 0, sizeof(M));
-    M.mx = mx;
-    M.my = my;
-    M.dx = dx;
-    M.dy = dy;
     dclaw_adj_member* mem = (dclaw_adj_member*)(base + T.off_mem);
     dclaw_params* prm = (dclaw_params*)(base + T.off_prm);
-    k_adj_single_setup<<<1, 32, 0, s>>>(M, *p, mem, prm);
+    if (phase & PHASE_PREPARE) {
+        dclaw_adj_member M;
+        memset(&M, 0, sizeof(M));
+        M.mx = mx;
+        M.my = my;
+        M.dx = dx;
+        M.dy = dy;
+        k_adj_single_setup<<<1, 32, 0, s>>>(M, *p, mem, prm);
+    }
     BatchArgs a{1, mem, prm, dt, q_in, b, lam_out, lam_in, base, status};
     launch_block_adjoint(a, (uint32_t)((size_t)L.act_nx * L.act_ny), base + T.off_lists,
-                         (unsigned int*)(base + T.off_counts), sm_count_adj(), s);
-    k_adj_batch_pbar<<<1, BTPB, 0, s>>>(a, pbar);
+                         (unsigned int*)(base + T.off_counts), sm_count_adj(), s, phase);
+    if (phase & PHASE_REVERSE) k_adj_batch_pbar<<<1, BTPB, 0, s>>>(a, pbar);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DCLAW_OK : DCLAW_ERR_CUDA;
+}
+
+int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, double dx, double dy,
+                       const double* dt, const dclaw_params* p, const double* lam_out, double* lam_in,
+                       double* pbar, void* work, size_t work_bytes, int32_t* status, void* stream) {
+    return single_adjoint(q_in, b, mx, my, dx, dy, dt, p, lam_out, lam_in, pbar, work, work_bytes, status, stream,
+                          PHASE_PREPARE | PHASE_REVERSE);
+}
+
+int dclaw_step_adjoint_prepare(const double* q_in, const double* b, int mx, int my, double dx, double dy,
+                               const double* dt, const dclaw_params* p, void* work, size_t work_bytes,
+                               int32_t* status, void* stream) {
+    return single_adjoint(q_in, b, mx, my, dx, dy, dt, p, nullptr, nullptr, nullptr, work, work_bytes, status,
+                          stream, PHASE_PREPARE);
+}
+
+int dclaw_step_adjoint_reverse(const double* q_in, const double* b, int mx, int my, double dx, double dy,
+                               const double* dt, const dclaw_params* p, const double* lam_out, double* lam_in,
+                               double* pbar, void* work, size_t work_bytes, int32_t* status, void* stream) {
+    return single_adjoint(q_in, b, mx, my, dx, dy, dt, p, lam_out, lam_in, pbar, work, work_bytes, status, stream,
+                          PHASE_REVERSE);
 }
 
 int dclaw_adjoint_batch_layout(int n, const int32_t* mx, const int32_t* my, const double* dx, const double* dy,
@@ -666,23 +705,44 @@ int dclaw_adjoint_batch_layout(int n, const int32_t* mx, const int32_t* my, cons
     return DCLAW_OK;
 }
 
+static int batched_adjoint(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
+                           const dclaw_params* params, const double* dt, const double* q_in, const double* b,
+                           const double* lam_out, double* lam_in, double* pbar, void* work, int32_t* status,
+                           void* stream, int phase) {
+    if (!batch || !members || !params || !dt || !q_in || !b || !work) return DCLAW_ERR_ARG;
+    if ((phase & PHASE_REVERSE) && (!lam_out || !lam_in || !pbar || lam_in == lam_out)) return DCLAW_ERR_ARG;
+    if (batch->nmembers <= 0 || batch->chunk_items != (uint32_t)ATPB) return DCLAW_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    BatchArgs a{batch->nmembers, members, params, dt, q_in, b, lam_out, lam_in, (char*)work, status};
+    char* lists = (char*)work + (batch->work_bytes - 256 - 2 * align256((size_t)batch->nblocks * 8));
+    unsigned int* counts = (unsigned int*)((char*)work + (batch->work_bytes - 256));
+    launch_block_adjoint(a, batch->nblocks, lists, counts, sm_count_adj(), s, phase);
+    if (phase & PHASE_REVERSE) k_adj_batch_pbar<<<batch->nmembers, BTPB, 0, s>>>(a, pbar);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? DCLAW_OK : DCLAW_ERR_CUDA;
+}
+
 int dclaw_step_adjoint_batched(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
                                const dclaw_params* params, const double* dt, const double* q_in, const double* b,
                                const double* lam_out, double* lam_in, double* pbar, void* work, int32_t* status,
                                void* stream) {
-    if (!batch || !members || !params || !dt || !q_in || !b || !lam_out || !lam_in || !pbar || !work)
-        return DCLAW_ERR_ARG;
-    if (batch->nmembers <= 0 || batch->chunk_items != (uint32_t)ATPB || lam_in == lam_out) return DCLAW_ERR_ARG;
-    cudaStream_t s = (cudaStream_t)stream;
-    int dev = 0, nsm = 148;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    BatchArgs a{batch->nmembers, members, params, dt, q_in, b, lam_out, lam_in, (char*)work, status};
-    char* lists = (char*)work + (batch->work_bytes - 256 - 2 * align256((size_t)batch->nblocks * 8));
-    unsigned int* counts = (unsigned int*)((char*)work + (batch->work_bytes - 256));
-    launch_block_adjoint(a, batch->nblocks, lists, counts, nsm, s);
-    k_adj_batch_pbar<<<batch->nmembers, BTPB, 0, s>>>(a, pbar);
-    cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? DCLAW_OK : DCLAW_ERR_CUDA;
+    return batched_adjoint(batch, members, params, dt, q_in, b, lam_out, lam_in, pbar, work, status, stream,
+                           PHASE_PREPARE | PHASE_REVERSE);
+}
+
+int dclaw_step_adjoint_batched_prepare(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
+                                       const dclaw_params* params, const double* dt, const double* q_in,
+                                       const double* b, void* work, int32_t* status, void* stream) {
+    return batched_adjoint(batch, members, params, dt, q_in, b, nullptr, nullptr, nullptr, work, status, stream,
+                           PHASE_PREPARE);
+}
+
+int dclaw_step_adjoint_batched_reverse(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
+                                       const dclaw_params* params, const double* dt, const double* q_in,
+                                       const double* b, const double* lam_out, double* lam_in, double* pbar,
+                                       void* work, int32_t* status, void* stream) {
+    return batched_adjoint(batch, members, params, dt, q_in, b, lam_out, lam_in, pbar, work, status, stream,
+                           PHASE_REVERSE);
 }
 
 }  // extern "C"

@@ -318,6 +318,18 @@ int dclaw_adjoint_supported(const dclaw_params* p);
 int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, double dx, double dy,
                        const double* dt, const dclaw_params* p, const double* lam_out, double* lam_in,
                        double* pbar, void* work, size_t work_bytes, int32_t* status, void* stream);
+/* dclaw_step_adjoint in two parts. prepare queues what does not depend on
+ * lam_out (the activity blocks, the forward recompute of the step's
+ * intermediates into work); reverse, given the same q_in, b, dt, p and work
+ * after prepare, queues the reverse stages. A backward pass over many steps
+ * can prepare step n-1 in a second workspace (on another stream) while step
+ * n's reverse runs; the results are those of dclaw_step_adjoint, bit for bit. */
+int dclaw_step_adjoint_prepare(const double* q_in, const double* b, int mx, int my, double dx, double dy,
+                               const double* dt, const dclaw_params* p, void* work, size_t work_bytes,
+                               int32_t* status, void* stream);
+int dclaw_step_adjoint_reverse(const double* q_in, const double* b, int mx, int my, double dx, double dy,
+                               const double* dt, const dclaw_params* p, const double* lam_out, double* lam_in,
+                               double* pbar, void* work, size_t work_bytes, int32_t* status, void* stream);
 
 /* ---- adjoint of one step of an ensemble ---------------------------------------
  * The reference differentiates its particle filters member by member with
@@ -369,6 +381,14 @@ int dclaw_step_adjoint_batched(const dclaw_adj_batch* batch, const dclaw_adj_mem
                                const dclaw_params* params, const double* dt, const double* q_in, const double* b,
                                const double* lam_out, double* lam_in, double* pbar, void* work, int32_t* status,
                                void* stream);
+/* the two parts of dclaw_step_adjoint_batched, as for the single patch */
+int dclaw_step_adjoint_batched_prepare(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
+                                       const dclaw_params* params, const double* dt, const double* q_in,
+                                       const double* b, void* work, int32_t* status, void* stream);
+int dclaw_step_adjoint_batched_reverse(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
+                                       const dclaw_params* params, const double* dt, const double* q_in,
+                                       const double* b, const double* lam_out, double* lam_in, double* pbar,
+                                       void* work, int32_t* status, void* stream);
 
 /* initialise a device clock: t, dt, t_final, fixed_dt; counters cleared */
 int dclaw_clock_init(dclaw_clock* clock, double t, double dt, double t_final, int fixed_dt,
