@@ -106,38 +106,55 @@ class StepAdjoint:
         _lib.check(int(self.status.item()), "adjoint step")
 
 
-def _reverse_block(adjs, steps, state_of, dt_of, lam, lam2, pbar, add_outs):
-    """The step adjoints of `steps` (descending step numbers), each step's
-    prepare queued on a side stream ahead of the previous step's reverse.
+def _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, dt_of, lam, lam2, pbar, add_outs):
+    """The step adjoints of steps n_steps .. 1, each step's prepare queued on
+    a side stream ahead of the previous step's reverse.
 
-    adjs: two adjoint objects (two workspaces), used alternately; state_of(n)
-    / dt_of(n): the input state and dt of step n; add_outs(n): adds the
-    output gradients at step count n into lam. The reverses run on a
-    high-priority stream, the prepares (which do not read lam) on a normal
-    one, so the prepare of step n-1 fills the SMs the reverse of step n
-    leaves idle. Returns the final (lam, lam2)."""
+    adjs: two adjoint objects (two workspaces), used alternately. ckpt[s] is
+    the input of step s k + 1 (block s); with k > 1 the block's other inputs
+    are recomputed into segs[s % 2] by recompute(s, seg), queued on the
+    reverse stream after the reverses of block s + 1 (so that its kernels,
+    persistent ones among them, never hold SMs the reverses wait for; the
+    buffer's previous user, block s + 2, is done by then). dt_of(n): step
+    n's dt; add_outs(n, lam): adds the output gradients at step count n.
+    The reverses run on a high-priority stream and the prepares (which do
+    not read lam) on a normal one, so they fill the SMs the reverses leave
+    idle. Returns the final (lam, lam2)."""
     cur = torch.cuda.current_stream()
     rev = torch.cuda.Stream(priority=-8)        # mapped to the device's highest priority
     side = torch.cuda.Stream()
     rev.wait_stream(cur)
     side.wait_stream(cur)
     last_rev = [None, None]               # the last reverse that used each workspace
+
+    def state_of(n):
+        s, j = (n - 1) // k, (n - 1) % k
+        return ckpt[s] if j == 0 else segs[s % 2][j]
+
+    def prepare(n):
+        # on the side stream, after the block's recompute when n is its top step
+        s = (n - 1) // k
+        if k > 1 and (n == n_steps or n % k == 0):
+            with torch.cuda.stream(rev):
+                recompute(s, segs[s % 2])
+            side.wait_event(rev.record_event())
+        if last_rev[n % 2] is not None:
+            side.wait_event(last_rev[n % 2])
+        adjs[n % 2].prepare(state_of(n), dt_of(n))
+
     with torch.cuda.stream(side):
-        adjs[steps[0] % 2].prepare(state_of(steps[0]), dt_of(steps[0]))
+        prepare(n_steps)
     ev_prep = side.record_event()
-    for idx, n in enumerate(steps):
+    for n in range(n_steps, 0, -1):
         w = n % 2
         with torch.cuda.stream(rev):
             rev.wait_event(ev_prep)
             add_outs(n, lam)
             adjs[w].reverse(state_of(n), dt_of(n), lam, lam2, pbar)
             last_rev[w] = rev.record_event()
-        if idx + 1 < len(steps):
-            n2 = steps[idx + 1]
+        if n > 1:
             with torch.cuda.stream(side):
-                if last_rev[n2 % 2] is not None:
-                    side.wait_event(last_rev[n2 % 2])
-                adjs[n2 % 2].prepare(state_of(n2), dt_of(n2))
+                prepare(n - 1)
             ev_prep = side.record_event()
         lam, lam2 = lam2, lam
     cur.wait_stream(rev)
@@ -257,35 +274,24 @@ class _Rollout(torch.autograd.Function):
             else:
                 target.view(-1).index_add_(0, sel.reshape(-1), g_out[idx].reshape(-1))
 
-        nblocks = len(ckpt)
-        if k == 1:
-            # every state kept: the whole backward pass is one pipelined run
-            def add_outs1(n, target):
-                if g_out is not None:
-                    for idx in where.get(n, []):
-                        add_out(idx, target)
+        segs = [seg, torch.empty_like(seg)] if k > 1 else None
 
-            lam, lam2 = _reverse_block(adjs, list(range(n_steps, 0, -1)), lambda n: ckpt[n - 1],
-                                       lambda n: dts[n - 1:n], lam, lam2, pbar, add_outs1)
-            nblocks = 0
-        for s in reversed(range(nblocks)):
-            n0 = s * k
-            n1 = min(n0 + k, n_steps)
-            # recompute the block's states n0+1 .. n1-1 from its first input
-            # with the recorded dts, each step writing its slot of seg
-            states = [ckpt[s]]
+        def recompute(s, buf):
+            # the block's states n0+1 .. n1-1 from its first input, with the recorded dts
+            n0, n1 = s * k, min(s * k + k, n_steps)
+            src = ckpt[s]
             for n in range(n0 + 1, n1):
                 fw.clock[1:2].copy_(dts[n - 1:n])
-                fw._launch(states[-1], seg[n - n0])
-                states.append(seg[n - n0])
+                fw._launch(src, buf[n - n0])
+                src = buf[n - n0]
 
-            def add_outs(n, target):
-                if g_out is not None:
-                    for idx in where.get(n, []):
-                        add_out(idx, target)
+        def add_outs(n, target):
+            if g_out is not None:
+                for idx in where.get(n, []):
+                    add_out(idx, target)
 
-            lam, lam2 = _reverse_block(adjs, list(range(n1, n0, -1)), lambda n: states[n - 1 - n0],
-                                       lambda n: dts[n - 1:n], lam, lam2, pbar, add_outs)
+        lam, lam2 = _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, lambda n: dts[n - 1:n], lam,
+                                        lam2, pbar, add_outs)
         if g_out is not None:
             for idx in where.get(0, []):
                 add_out(idx, lam)
@@ -511,22 +517,18 @@ class _EnsembleRollout(torch.autograd.Function):
                 for idx in where.get(n, []):
                     add_out(idx, target)
 
-        nblocks = len(ckpt)
-        if k == 1:
-            # every state kept: the whole backward pass is one pipelined run
-            lam, lam2 = _reverse_block(adjs, list(range(n_steps, 0, -1)), lambda n: ckpt[n - 1],
-                                       lambda n: dts[n - 1], lam, lam2, pbar, add_outs)
-            nblocks = 0
-        for s in reversed(range(nblocks)):
-            n0 = s * k
-            n1 = min(n0 + k, n_steps)
-            states = [ckpt[s]]
+        segs = [seg, torch.zeros_like(seg)] if k > 1 else None
+
+        def recompute(s, buf):
+            n0, n1 = s * k, min(s * k + k, n_steps)
+            src = ckpt[s]
             for n in range(n0 + 1, n1):
                 _clock_field(fw, 1).copy_(dts[n - 1])
-                fw._launch(states[-1], seg[n - n0])
-                states.append(seg[n - n0])
-            lam, lam2 = _reverse_block(adjs, list(range(n1, n0, -1)), lambda n: states[n - 1 - n0],
-                                       lambda n: dts[n - 1], lam, lam2, pbar, add_outs)
+                fw._launch(src, buf[n - n0])
+                src = buf[n - n0]
+
+        lam, lam2 = _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, lambda n: dts[n - 1], lam, lam2,
+                                        pbar, add_outs)
         add_outs(0, lam)
         for kk, st in enumerate(fw.status()):
             _lib.check(st, f"ensemble recompute, member {kk}")
