@@ -255,6 +255,33 @@ def test_unsupported_options_are_refused(cuda_device):
         StepAdjoint(b, DClawParams(friction_forcing=True, manning_coefficient=0.03), 1.0, 1.0)
 
 
+def test_prepare_then_reverse_equals_the_whole_step_adjoint(cuda_device):
+    """dclaw_step_adjoint_prepare + _reverse (the two parts the backward
+    pass overlaps) give dclaw_step_adjoint's bits, with another step
+    prepared in a second workspace in between."""
+    p, qn, bn = _small_flow(seed=4)
+    dev = cuda_device
+    b = torch.tensor(bn, device=dev)
+    rng = np.random.default_rng(8)
+    q1 = torch.tensor(qn, device=dev)
+    q2 = torch.tensor(qn * (1.0 + 0.01 * rng.standard_normal(qn.shape)).clip(min=0.0), device=dev)
+    lam = torch.tensor(rng.standard_normal(qn.shape), device=dev)
+    dt1 = torch.tensor([0.02], dtype=torch.float64, device=dev)
+    dt2 = torch.tensor([0.015], dtype=torch.float64, device=dev)
+    ref = StepAdjoint(b, p, 1.0, 1.0)
+    li_ref, pb_ref = torch.empty_like(lam), torch.zeros(4, dtype=torch.float64, device=dev)
+    ref.vjp(q1, dt1, lam, li_ref, pb_ref)
+    a, other = StepAdjoint(b, p, 1.0, 1.0), StepAdjoint(b, p, 1.0, 1.0)
+    li, pb = torch.empty_like(lam), torch.zeros(4, dtype=torch.float64, device=dev)
+    a.prepare(q1, dt1)
+    other.prepare(q2, dt2)
+    a.reverse(q1, dt1, lam, li, pb)
+    torch.cuda.synchronize()
+    for x in (ref, a, other):
+        x.check_status()
+    assert torch.equal(li, li_ref) and torch.equal(pb, pb_ref)
+
+
 def test_nan_anywhere_in_the_state_is_reported(cuda_device):
     """A NaN in any field of any cell, near the flow or far from it, sets the
     adjoint's status word (as the forward step's check4nans scan does); a
