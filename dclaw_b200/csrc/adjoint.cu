@@ -605,10 +605,9 @@ int dclaw_adjoint_supported(const dclaw_params* p) {
     if (!p) return DCLAW_ERR_ARG;
     int rc = dclaw_params_check(p);
     if (rc) return rc;
-    // no adjoint form: the rare-wave corrector's branch structure, Manning
-    // friction and src2method 2's data-dependent substeps
-    if (p->rarecorrectortest || (p->friction_forcing && p->manning_coefficient > 0.0) || p->src2method == 2)
-        return DCLAW_ERR_UNSUPPORTED;
+    // no adjoint form: the rare-wave corrector's branch structure and
+    // src2method 2's data-dependent substeps
+    if (p->rarecorrectortest || p->src2method == 2) return DCLAW_ERR_UNSUPPORTED;
     return DCLAW_OK;
 }
 

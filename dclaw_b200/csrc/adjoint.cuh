@@ -1393,7 +1393,7 @@ DC_HD void mp_update_relax_b(const dclaw_params& P, double phi, double dt, doubl
 
 // src2_cell reverse: q[5] the cell state before src2 (after the update);
 // qb[5] on entry the adjoint of the output state, replaced by the adjoint of
-// the input state. Returns false for Manning friction (no adjoint form).
+// the input state. Always true.
 DC_HD bool src2_cell_b(const dclaw_params& P, double phi, double dt, const double q[5], double qb[5], double& phib,
                        double* pbar) {
     const double rs = P.rho_s, rf = P.rho_f;
@@ -1405,7 +1405,6 @@ DC_HD bool src2_cell_b(const dclaw_params& P, double phi, double dt, const doubl
     double hu0 = q[1], hv0 = q[2], hm0 = q[3], p0 = q[4];
     double rhoh = hm0 * rs + (h - hm0) * rf;
     if (hm0 < 0.0) return true;  // identity
-    if (P.friction_forcing && P.manning_coefficient > 0.0) return false;
     const double gz = P.grav;
     double h1 = h, hu1 = hu0, hv1 = hv0, hm1 = hm0, p1 = p0, u1, v1, m1;
     qfix(P, h1, hu1, hv1, hm1, p1, u1, v1, m1, gz);
@@ -1434,9 +1433,53 @@ DC_HD bool src2_cell_b(const dclaw_params& P, double phi, double dt, const doubl
         for (int k = 0; k < 5; ++k) qb[k] = 0.0;
         return true;
     }
-    // outputs (h3, h3 u3, h3 v3, h3 m3, p3)
-    double h3b = qb[0] + qb[1] * u3 + qb[2] * v3 + qb[3] * m3;
-    double u3b = qb[1] * h3, v3b = qb[2] * h3, m3b = qb[3] * h3, p3b = qb[4];
+    // outputs (h3, h3 u3, h3 v3, h3 m3, p3), or Manning's update of them
+    // (src2.f90:271-289): hu, hv divided by 1 + dt gamma, gamma =
+    // |(hu, hv)| g cm^2 / h^(7/3), cm constant or (dd_manning) a tanh ramp
+    // in h, then qfix
+    double h3b, u3b, v3b, m3b, p3b;
+    if (P.friction_forcing && P.manning_coefficient > 0.0 && h3 <= P.friction_depth) {
+        const double hM = h3, huM = h3 * u3, hvM = h3 * v3, hmM = h3 * m3, pM = p3;
+        double cm = P.manning_coefficient, th = 0.0;
+        if (P.dd_manning) {
+            th = em::d_tanh(300.0 * (hM - 0.05));
+            cm = P.manning_max + (P.manning_coefficient - P.manning_max) * 0.5 * (1.0 + th);
+        }
+        const double N = sqrt(sq(huM) + sq(hvM));
+        const double gamma = N * (gz * sq(cm)) / (em::d_pow_7_3(hM));
+        const double D = 1.0 + dt * gamma;
+        const double hu5 = huM / D, hv5 = hvM / D;
+        // qfix(hM, hu5, hv5, hmM, pM) -> the outputs
+        double hb = qb[0], hu5b = qb[1], hv5b = qb[2], hmMb = qb[3], pMb = qb[4];
+        qfix_b(P, hM, hu5, hv5, hmM, pM, gz, hb, hu5b, hv5b, hmMb, pMb, 0.0, 0.0, 0.0);
+        // hu5 = huM / D, hv5 = hvM / D
+        double huMb = hu5b / D, hvMb = hv5b / D;
+        const double Db = -(hu5b * hu5 + hv5b * hv5) / D;
+        const double gammab = Db * dt;
+        // gamma = N g cm^2 h^(-7/3)
+        if (N > 0.0) {
+            const double Nb = gammab * gamma / N;
+            huMb += Nb * huM / N;
+            hvMb += Nb * hvM / N;
+            hb -= gammab * gamma * (7.0 / 3.0) / hM;
+            if (P.dd_manning) {
+                const double cmb = gammab * 2.0 * gamma / cm;
+                hb += cmb * (P.manning_coefficient - P.manning_max) * 0.5 * 300.0 * (1.0 - th * th);
+            }
+        }
+        // (hM, huM, hvM, hmM, pM) = (h3, h3 u3, h3 v3, h3 m3, p3)
+        h3b = hb + huMb * u3 + hvMb * v3 + hmMb * m3;
+        u3b = huMb * h3;
+        v3b = hvMb * h3;
+        m3b = hmMb * h3;
+        p3b = pMb;
+    } else {
+        h3b = qb[0] + qb[1] * u3 + qb[2] * v3 + qb[3] * m3;
+        u3b = qb[1] * h3;
+        v3b = qb[2] * h3;
+        m3b = qb[3] * h3;
+        p3b = qb[4];
+    }
     double rhohb = 0.0;
     double h1b, u2b, v2b, m1b, p1b;
     if (P.src2method != -1) {

@@ -313,7 +313,8 @@ int dclaw_batch_reset(const dclaw_batch* batch, void* work, void* stream);
  * work: dclaw_adjoint_workspace_bytes(mx, my) bytes. */
 size_t dclaw_adjoint_workspace_bytes(int mx, int my);
 /* DCLAW_OK when the options have an adjoint form; DCLAW_ERR_UNSUPPORTED for
- * the rare-wave corrector test and for Manning friction */
+ * the rare-wave corrector test and for src2method 2 (FE_4quad's data-dependent
+ * substeps); Manning friction (constant or dd_manning) has its reverse */
 int dclaw_adjoint_supported(const dclaw_params* p);
 int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, double dx, double dy,
                        const double* dt, const dclaw_params* p, const double* lam_out, double* lam_in,

@@ -301,10 +301,18 @@ Stat check_rpt2(Rng& r, int n) {
     return st;
 }
 
-// src2 on one cell, with phi, kref, alpha_c, mu as extra inputs
-Stat check_src2(Rng& r, int n, int method, bool still) {
+// src2 on one cell, with phi, kref, alpha_c, mu as extra inputs; manning:
+// 1 Manning friction with a constant coefficient, 2 depth-dependent
+Stat check_src2(Rng& r, int n, int method, bool still, int manning = 0) {
     dclaw_params P0 = default_params();
     P0.src2method = method;
+    if (manning) {
+        P0.friction_forcing = 1;
+        P0.manning_coefficient = 0.06;
+        P0.friction_depth = 1.0e6;
+        P0.dd_manning = manning == 2 ? 1 : 0;
+        P0.manning_max = 0.1;
+    }
     Stat st;
     const double dt = 0.01;
     auto f = [&](const Vec& x) {
@@ -340,7 +348,8 @@ extern "C" {
 
 // which: 0 qfix, 1 qfix_cmass, 2 setvars, 3 setvars<all>, 4 setvars<all> alphamethod 1,
 // 5 riemanntype, 6 riemann wet, 7 riemann dry side / wall, 8 riemann at rest, 9 riemann src2method -1,
-// 10..13 limiter 1..4, 14 rpt2, 15 src2 m0, 16 src2 m1, 17 src2 m-1, 18 src2 at rest
+// 10..13 limiter 1..4, 14 rpt2, 15 src2 m0, 16 src2 m1, 17 src2 m-1, 18 src2 at rest,
+// 19 src2 with Manning friction, 20 with depth-dependent Manning friction
 int adj_check_local(int which, int seed, int n, double* maxerr, int* skipped) {
     Rng r((uint64_t)seed * 7919u + (uint64_t)which);
     Stat st;
@@ -361,6 +370,8 @@ int adj_check_local(int which, int seed, int n, double* maxerr, int* skipped) {
         case 16: st = check_src2(r, n, 1, false); break;
         case 17: st = check_src2(r, n, -1, false); break;
         case 18: st = check_src2(r, n, 0, true); break;
+        case 19: st = check_src2(r, n, 0, false, 1); break;
+        case 20: st = check_src2(r, n, 0, false, 2); break;
         default: return -1;
     }
     *maxerr = st.maxerr;

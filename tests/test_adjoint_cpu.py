@@ -64,6 +64,9 @@ CASES = {
     "minmod": dict(seed=11, p=DClawParams(limiter=1)),
     "superbee": dict(seed=12, p=DClawParams(limiter=2)),
     "alphamethod1": dict(seed=13, p=DClawParams(alphamethod=1)),
+    "manning": dict(seed=14, p=DClawParams(friction_forcing=True, manning_coefficient=0.06)),
+    "dd_manning": dict(seed=15, p=DClawParams(friction_forcing=True, manning_coefficient=0.04, dd_manning=True,
+                                              manning_max=0.1, friction_depth=0.8)),
     "at_rest": dict(seed=3, moving=False),
 }
 

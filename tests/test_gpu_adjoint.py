@@ -252,7 +252,9 @@ def test_unsupported_options_are_refused(cuda_device):
     with pytest.raises(_lib.DClawError):
         StepAdjoint(b, DClawParams(rarecorrectortest=True), 1.0, 1.0)
     with pytest.raises(_lib.DClawError):
-        StepAdjoint(b, DClawParams(friction_forcing=True, manning_coefficient=0.03), 1.0, 1.0)
+        StepAdjoint(b, DClawParams(src2method=2, alphamethod=1), 1.0, 1.0)
+    # Manning friction has its reverse
+    StepAdjoint(b, DClawParams(friction_forcing=True, manning_coefficient=0.03), 1.0, 1.0)
 
 
 def test_prepare_then_reverse_equals_the_whole_step_adjoint(cuda_device):
