@@ -262,12 +262,29 @@ struct FwMargin {
 };
 constexpr int ZERO_MARGIN = 4;
 
+// resident CTAs per SM of the block kernels; the stages of the set
+// DCLAW_ADJ_HEAVY_SET (1: reverse solves, 2: and reverse fluxes, 3: and
+// reverse src2) take DCLAW_ADJ_HEAVY_MINB instead
+#ifndef DCLAW_ADJ_HEAVY_MINB
+#define DCLAW_ADJ_HEAVY_MINB (DCLAW_ADJ_MINB / 2)
+#endif
+#ifndef DCLAW_ADJ_HEAVY_SET
+#define DCLAW_ADJ_HEAVY_SET 0
+#endif
+template <int OP>
+struct BlkMinB {
+    static constexpr bool heavy = (DCLAW_ADJ_HEAVY_SET >= 1 && (OP == OP_RV_RX || OP == OP_RV_RY)) ||
+                                  (DCLAW_ADJ_HEAVY_SET >= 2 && (OP == OP_RV_FX || OP == OP_RV_FY)) ||
+                                  (DCLAW_ADJ_HEAVY_SET >= 3 && OP == OP_RV_SRC2);
+    static constexpr int value = heavy ? DCLAW_ADJ_HEAVY_MINB : DCLAW_ADJ_MINB / 2;
+};
+
 // One stage over a list of (member, block) entries (grid-stride; every
 // thread of a CTA runs the same iterations, so the barriers are uniform).
 // A CTA has one thread per item of a 16 x 16 block; two CTAs per SM at up
 // to 128 registers a thread.
 template <int OP>
-__global__ void __launch_bounds__(BTPB, DCLAW_ADJ_MINB / 2) k_adj_blocks(BatchArgs a, const uint64_t* __restrict__ list,
+__global__ void __launch_bounds__(BTPB, BlkMinB<OP>::value) k_adj_blocks(BatchArgs a, const uint64_t* __restrict__ list,
                                                                      const unsigned int* __restrict__ count) {
     __shared__ dclaw_adj_member sM;
     __shared__ dclaw_params sP;
