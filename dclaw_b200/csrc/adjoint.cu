@@ -43,6 +43,30 @@ constexpr int BTPB = 256;
 
 __host__ __device__ inline unsigned nblk(long long n) { return (unsigned)((n + ATPB - 1) / ATPB); }
 
+// Programmatic dependent launch: a kernel launched with the
+// programmatic-serialization attribute may start while the kernel before
+// it on the stream drains; it waits here, before reading anything, until
+// that kernel has completed and its writes are visible (a no-op for a
+// kernel launched without the attribute). A CTA that has no work left
+// lets the next kernel start launching.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // Sum of the block's per-thread parameter adjoints, in a fixed order, into
 // dst[0..NPB). Every thread of the block (NW warps) must call it.
 template <int NW>
@@ -291,6 +315,7 @@ __global__ void __launch_bounds__(BTPB, BlkMinB<OP>::value) k_adj_blocks(BatchAr
     __shared__ uint64_t s_e;
     __shared__ int s_list[BTPB];
     __shared__ int s_n;
+    pdl_wait();
     const unsigned int n = *count;
     int cur = -1;
     for (unsigned int k = blockIdx.x; k < n; k += gridDim.x) {
@@ -366,6 +391,7 @@ __global__ void __launch_bounds__(BTPB, BlkMinB<OP>::value) k_adj_blocks(BatchAr
         }
         __syncthreads();
     }
+    pdl_trigger();
 }
 
 // zero the reverse planes of the listed blocks that are not active: an
@@ -419,6 +445,7 @@ __global__ void __launch_bounds__(BTPB) k_adj_blocks_zero(BatchArgs a, const uin
 // 0 clears the list lengths
 // (what & 1: the activity map and the list lengths; what & 2: lam_in)
 __global__ void __launch_bounds__(256) k_adj_batch_zero(BatchArgs a, unsigned int* counts, int what) {
+    pdl_wait();
     const dclaw_adj_member M = a.mem[blockIdx.y];
     const AdjLayout L = adj_layout(M.mx, M.my);
     const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
@@ -433,6 +460,7 @@ __global__ void __launch_bounds__(256) k_adj_batch_zero(BatchArgs a, unsigned in
         const size_t nl = (size_t)5 * M.mx * M.my;
         for (size_t x = t0; x < nl; x += st) lam[x] = 0.0;
     }
+    pdl_trigger();
 }
 
 // member m (blockIdx.y): a wet interior cell marks the blocks within
@@ -505,6 +533,7 @@ __global__ void __launch_bounds__(256) k_adj_batch_list(BatchArgs a, unsigned in
 // turn, all four parameters at once; then the threads in order
 __global__ void __launch_bounds__(BTPB) k_adj_batch_pbar(BatchArgs a, double* __restrict__ pbar) {
     __shared__ double red[NPB][BTPB];
+    pdl_wait();
     const int m = blockIdx.x;
     const dclaw_adj_member M = a.mem[m];
     const AdjLayout L = adj_layout(M.mx, M.my);
@@ -559,7 +588,11 @@ inline void launch_block_adjoint(const BatchArgs& a, uint32_t nblocks, char* lis
         DC_FW(OP_FW_FY);
     }
     if (!(phase & PHASE_REVERSE)) return;
-    k_adj_batch_zero<<<per_member, 256, 0, s>>>(a, counts, 2);
+    // the reverse chain: each kernel launched as the one before it drains
+#undef DC_RV
+#define DC_RV(op) launch_pdl(k_adj_blocks<op>, dim3(grid), dim3(BTPB), s, a, (const uint64_t*)list_act, \
+                             (const unsigned int*)counts)
+    launch_pdl(k_adj_batch_zero, per_member, dim3(256), s, a, counts, 2);
     DC_RV(OP_RV_SRC2);
     DC_RV(OP_RV_FX);
     DC_RV(OP_RV_FY);
@@ -657,7 +690,7 @@ static int single_adjoint(const double* q_in, const double* b, int mx, int my, d
     BatchArgs a{1, mem, prm, dt, q_in, b, lam_out, lam_in, base, status};
     launch_block_adjoint(a, (uint32_t)((size_t)L.act_nx * L.act_ny), base + T.off_lists,
                          (unsigned int*)(base + T.off_counts), sm_count_adj(), s, phase);
-    if (phase & PHASE_REVERSE) k_adj_batch_pbar<<<1, BTPB, 0, s>>>(a, pbar);
+    if (phase & PHASE_REVERSE) launch_pdl(k_adj_batch_pbar, dim3(1), dim3(BTPB), s, a, pbar);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DCLAW_OK : DCLAW_ERR_CUDA;
 }
@@ -733,7 +766,7 @@ static int batched_adjoint(const dclaw_adj_batch* batch, const dclaw_adj_member*
     char* lists = (char*)work + (batch->work_bytes - 256 - 2 * align256((size_t)batch->nblocks * 8));
     unsigned int* counts = (unsigned int*)((char*)work + (batch->work_bytes - 256));
     launch_block_adjoint(a, batch->nblocks, lists, counts, sm_count_adj(), s, phase);
-    if (phase & PHASE_REVERSE) k_adj_batch_pbar<<<batch->nmembers, BTPB, 0, s>>>(a, pbar);
+    if (phase & PHASE_REVERSE) launch_pdl(k_adj_batch_pbar, dim3((unsigned)batch->nmembers), dim3(BTPB), s, a, pbar);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DCLAW_OK : DCLAW_ERR_CUDA;
 }
