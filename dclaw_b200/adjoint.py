@@ -106,7 +106,7 @@ class StepAdjoint:
         _lib.check(int(self.status.item()), "adjoint step")
 
 
-def _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, dt_of, lam, lam2, pbar, add_outs):
+def _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, dt_of, lam, lam2, pbar, add_outs, bed_for=None):
     """The step adjoints of steps n_steps .. 1, each step's prepare queued on
     a side stream ahead of the previous step's reverse.
 
@@ -116,7 +116,9 @@ def _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, dt_of, lam, lam
     reverse stream after the reverses of block s + 1 (so that its kernels,
     persistent ones among them, never hold SMs the reverses wait for; the
     buffer's previous user, block s + 2, is done by then). dt_of(n): step
-    n's dt; add_outs(n, lam): adds the output gradients at step count n.
+    n's dt; add_outs(n, lam): adds the output gradients at step count n;
+    bed_for(n, adj) (a moving bed): fills adj's bed with step n's, on the
+    side stream once adj's workspace is free.
     The reverses run on a high-priority stream and the prepares (which do
     not read lam) on a normal one, so they fill the SMs the reverses leave
     idle. Returns the final (lam, lam2)."""
@@ -140,6 +142,8 @@ def _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, dt_of, lam, lam
             side.wait_event(rev.record_event())
         if last_rev[n % 2] is not None:
             side.wait_event(last_rev[n % 2])
+        if bed_for is not None:
+            bed_for(n, adjs[n % 2])
         adjs[n % 2].prepare(state_of(n), dt_of(n))
 
     with torch.cuda.stream(side):
@@ -203,6 +207,11 @@ class _Rollout(torch.autograd.Function):
     def forward(ctx, q0, theta, b, params, dx, dy, n_steps, out_steps, dt0, fixed_dt, t_final, checkpoint_block,
                 dt_schedule, select):
         prm = with_theta(params, theta.detach().cpu())
+        # a moving bed: a function of the simulated time, evaluated before
+        # every step (the port's step(q, bed(t), ...) loop)
+        bed_fn = b if callable(b) else None
+        if bed_fn is not None:
+            b = bed_fn(torch.zeros((), dtype=torch.float64, device=q0.device)).contiguous()
         st = PatchStepper(q0.detach(), b, prm, dx, dy)
         if dt_schedule is not None:
             st.init_clock(0.0, fixed_dt=True)
@@ -212,6 +221,7 @@ class _Rollout(torch.autograd.Function):
         k = _block(n_steps, checkpoint_block, q0.numel() * 8,
                    2 * lib.dclaw_adjoint_workspace_bytes(q0.shape[2], q0.shape[1]), q0.device)
         dts = torch.empty(n_steps, dtype=torch.float64, device=q0.device)
+        t_start = torch.empty(n_steps if bed_fn is not None else 0, dtype=torch.float64, device=q0.device)
         oshape = tuple(q0.shape) if select is None else tuple(select.shape)
         outs = torch.empty((len(out_steps),) + oshape, dtype=q0.dtype, device=q0.device)
         pick = (lambda t: t) if select is None else (lambda t: t.reshape(-1)[select])
@@ -234,6 +244,9 @@ class _Rollout(torch.autograd.Function):
                 dst = st.qa if src is not st.qa else st.qb
             if dt_schedule is not None:
                 st.clock[1:2].copy_(dt_schedule[n:n + 1])
+            if bed_fn is not None:
+                t_start[n:n + 1].copy_(st.clock[0:1])
+                st.b.copy_(bed_fn(st.clock[0]))
             st._launch(src, dst)
             src = dst
             dts[n:n + 1].copy_(st.clock[3:4])   # dt the step used
@@ -243,23 +256,28 @@ class _Rollout(torch.autograd.Function):
         # the block inputs are saved tensors: autograd frees them after the
         # backward pass (unless the graph is retained), so a loop of gradient
         # evaluations reuses one allocation instead of holding two
-        ctx.save_for_backward(b, dts, store)
+        ctx.save_for_backward(b, dts, store, t_start)
+        ctx.bed_fn = bed_fn
         ctx.select = select
         ctx.meta = (prm, float(dx), float(dy), int(n_steps), tuple(out_steps), k)
         return outs
 
     @staticmethod
     def backward(ctx, g_out):
-        b, dts, store = ctx.saved_tensors
+        b, dts, store, t_start = ctx.saved_tensors
         ckpt = list(store.unbind(0))
         prm, dx, dy, n_steps, out_steps, k = ctx.meta
+        bed_fn = ctx.bed_fn
         dev = b.device
         shape = ckpt[0].shape
         where = {}
         for idx, n in enumerate(out_steps):
             where.setdefault(n, []).append(idx)
-        adjs = [StepAdjoint(b, prm, dx, dy), StepAdjoint(b, prm, dx, dy)]
-        fw = PatchStepper(ckpt[0], b, prm, dx, dy)
+        # with a moving bed each workspace and the recompute keep their own
+        # bed, refilled with the step's bed(t) before they use it
+        own = (lambda x: x.clone()) if bed_fn is not None else (lambda x: x)
+        adjs = [StepAdjoint(own(b), prm, dx, dy), StepAdjoint(own(b), prm, dx, dy)]
+        fw = PatchStepper(ckpt[0], own(b), prm, dx, dy)
         fw.init_clock(0.0, fixed_dt=True)
         lam = torch.zeros(shape, dtype=torch.float64, device=dev)
         lam2 = torch.empty_like(lam)
@@ -282,6 +300,8 @@ class _Rollout(torch.autograd.Function):
             src = ckpt[s]
             for n in range(n0 + 1, n1):
                 fw.clock[1:2].copy_(dts[n - 1:n])
+                if bed_fn is not None:
+                    fw.b.copy_(bed_fn(t_start[n - 1]))
                 fw._launch(src, buf[n - n0])
                 src = buf[n - n0]
 
@@ -290,8 +310,11 @@ class _Rollout(torch.autograd.Function):
                 for idx in where.get(n, []):
                     add_out(idx, target)
 
+        def bed_for(n, adj):
+            adj.b.copy_(bed_fn(t_start[n - 1]))
+
         lam, lam2 = _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, lambda n: dts[n - 1:n], lam,
-                                        lam2, pbar, add_outs)
+                                        lam2, pbar, add_outs, bed_for if bed_fn is not None else None)
         if g_out is not None:
             for idx in where.get(0, []):
                 add_out(idx, lam)
@@ -302,7 +325,7 @@ class _Rollout(torch.autograd.Function):
         return lam, pbar * scale, None, None, None, None, None, None, None, None, None, None, None, None
 
 
-def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b: torch.Tensor, params: DClawParams, dx: float,
+def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams, dx: float,
                    dy: float, n_steps: int, out_steps: Sequence[int], dt0: float, fixed_dt: bool = False,
                    t_final: float = 0.0, checkpoint_block: int | None = None,
                    dt_schedule: torch.Tensor | None = None, select: torch.Tensor | None = None) -> torch.Tensor:
@@ -310,7 +333,10 @@ def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b: torch.Tensor, param
 
     q0: (5, my, mx) float64 CUDA tensor (x fastest), theta: (4,) float64
     tensor (phi [deg], kref, alpha_c, mu) overriding those fields of params,
-    b: (my, mx). Returns the states after each step count in out_steps
+    b: (my, mx), or a moving bed: a function of the simulated time (a 0-dim
+    float64 device tensor) returning the (my, mx) bed, evaluated before every
+    step as the port's loops do (e.g. `solver.gate_bed`); the bed itself is
+    not differentiated. Returns the states after each step count in out_steps
     (0 = q0), shape (len(out_steps), 5, my, mx). dt0 is the first dt; with
     fixed_dt every step uses it, otherwise the tick rule picks the next dt
     from the Courant number (clipped at t_final when t_final > 0). Gradients
@@ -332,7 +358,8 @@ def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b: torch.Tensor, param
         if dt_schedule.shape != (n_steps,) or dt_schedule.dtype != torch.float64 or not dt_schedule.is_cuda:
             raise ValueError("dt_schedule must be a (n_steps,) float64 CUDA tensor")
         dt_schedule = dt_schedule.contiguous()
-    return _Rollout.apply(q0, theta, b.contiguous(), params, dx, dy, int(n_steps), tuple(int(n) for n in out_steps),
+    return _Rollout.apply(q0, theta, b if callable(b) else b.contiguous(), params, dx, dy, int(n_steps),
+                          tuple(int(n) for n in out_steps),
                           float(dt0), bool(fixed_dt), float(t_final), checkpoint_block, dt_schedule, select)
 
 

@@ -160,6 +160,59 @@ def test_rollout_gradient_matches_finite_differences(cuda_device, mode):
         _close(float(gt[k]) * scale, _fd(lambda h: Lf(q00, th0 + h * e), eps0=4e-6), f"theta[{k}]")
 
 
+def test_rollout_gradient_with_a_moving_gate_bed(cuda_device):
+    """The port's flume runs step under a moving gate, bed(t) (gate_bed):
+    the differentiable run evaluates the bed before every step, its states
+    equal stepping with the bed rebuilt each step, and its gradients match
+    finite differences at the recorded dt schedule, with every state kept
+    and with checkpoint blocks."""
+    from dclaw_b200.solver import PatchStepper, gate_bed
+
+    dev = cuda_device
+    p, qn, bn = _small_flow(seed=5)
+    b0 = torch.tensor(bn, device=dev)
+    ridge = torch.zeros_like(b0)
+    ridge[:, 10:12] = 0.5                        # a gate across the flow, opening over 0.2 s (10 steps)
+    bed = gate_bed(b0, ridge, [0.0, 0.2], [0.0, 90.0])
+    n, outs = 16, [8, 16]
+    wts = torch.tensor(_loss_weights(qn, len(outs), seed=4), device=dev)
+    res = []
+    for blk in (1, 4):
+        q0 = torch.tensor(qn, device=dev, requires_grad=True)
+        theta = theta_of(p, dev).requires_grad_(True)
+        L, o = _run_loss(q0, theta, bed, p, 1.0, n, outs, wts, dt0=0.02, fixed_dt=True, checkpoint_block=blk)
+        L.backward()
+        res.append((o.detach(), q0.grad.clone(), theta.grad.clone()))
+    assert all(torch.equal(x, y) for x, y in zip(res[0], res[1])), "checkpoint blocks differ"
+    o, gq, gt = res[0]
+    # the forward states: the fused step with the bed rebuilt before every step
+    st = PatchStepper(torch.tensor(qn, device=dev), bed(torch.zeros((), dtype=torch.float64, device=dev)), p,
+                      1.0, 1.0)
+    st.init_clock(0.02, fixed_dt=True)
+    for k in range(n):
+        st.b.copy_(bed(st.clock[0]))
+        st.step(1)
+        if k + 1 == 8:
+            assert torch.equal(st.state(), o[0])
+    assert torch.equal(st.state(), o[1])
+    # gradients against finite differences
+    sched = torch.full((n,), 0.02, dtype=torch.float64, device=dev)
+
+    def Lf(qq, th):
+        with torch.no_grad():
+            return float(_run_loss(qq, th, bed, p, 1.0, n, outs, wts, dt0=0.0, dt_schedule=sched)[0])
+
+    rng = np.random.default_rng(11)
+    d = rng.standard_normal(qn.shape) * (np.abs(qn) + 1e-3)
+    d[:, qn[0] <= 10 * p.dry_tolerance] = 0.0
+    d = torch.tensor(d, device=dev)
+    q00, th0 = torch.tensor(qn, device=dev), theta_of(p, dev)
+    _close(float((gq * d).sum()), _fd(lambda e: Lf(q00 + e * d, th0)), "state")
+    e0 = torch.zeros(4, dtype=torch.float64, device=dev)
+    e0[0] = 1.0
+    _close(float(gt[0]), _fd(lambda h: Lf(q00, th0 + h * e0), eps0=4e-6), "phi")
+
+
 def test_checkpoint_block_gives_identical_gradients(cuda_device):
     dev = cuda_device
     p, qn, bn = _small_flow(seed=2)
