@@ -568,7 +568,9 @@ def run_ours(args):
     h2d = d2h = 0
     if args.e2e_steps > 0:
         qh = st.state().cpu().pin_memory()
-        cfl_h = torch.zeros(8, dtype=torch.float64).pin_memory()
+        from dclaw_b200.params import CLOCK_DOUBLES
+
+        cfl_h = torch.zeros(CLOCK_DOUBLES, dtype=torch.float64).pin_memory()
         f0 = torch.cuda.Event(enable_timing=True)
         f1 = torch.cuda.Event(enable_timing=True)
         # the host-buffer step: the state stays in pinned host memory and

@@ -34,6 +34,7 @@ SIGNATURES = {
     "dclaw_src2": (_int, [_vp, _vp, _int, _int, _int, _dbl, _dbl, _dbl, _dbl, _pp, _vp]),
     "dclaw_step": (_int, [_vp, _vp, _vp, _int, _int, _dbl, _dbl, _pp, _vp, _vp, _sz, _vp, _vp]),
     "dclaw_clock_init": (_int, [_vp, _dbl, _dbl, _dbl, _int, _vp]),
+    "dclaw_clock_set_obs": (_int, [_vp, _dbl, _vp]),
     "dclaw_max_wave_speed": (_int, [_vp, _int, _int, _pp, _vp, _vp]),
     "dclaw_step_noalloc": (_int, [_vp, _vp, _vp, _int, _int, _dbl, _dbl, _pp, _vp, _vp]),
     "dclaw_step_noalloc_max_cells": (_sz, []),

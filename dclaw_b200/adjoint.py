@@ -205,7 +205,7 @@ def _block(n_steps: int, checkpoint_block: int | None, state_bytes: int = 0, res
 class _Rollout(torch.autograd.Function):
     @staticmethod
     def forward(ctx, q0, theta, b, params, dx, dy, n_steps, out_steps, dt0, fixed_dt, t_final, checkpoint_block,
-                dt_schedule, select):
+                dt_schedule, select, obs_dt):
         prm = with_theta(params, theta.detach().cpu())
         # a moving bed: a function of the simulated time, evaluated before
         # every step (the port's step(q, bed(t), ...) loop)
@@ -216,7 +216,7 @@ class _Rollout(torch.autograd.Function):
         if dt_schedule is not None:
             st.init_clock(0.0, fixed_dt=True)
         else:
-            st.init_clock(float(dt0), t_final=float(t_final), fixed_dt=bool(fixed_dt))
+            st.init_clock(float(dt0), t_final=float(t_final), fixed_dt=bool(fixed_dt), t_obs=float(obs_dt))
         lib = _lib.load()
         k = _block(n_steps, checkpoint_block, q0.numel() * 8,
                    2 * lib.dclaw_adjoint_workspace_bytes(q0.shape[2], q0.shape[1]), q0.device)
@@ -322,13 +322,14 @@ class _Rollout(torch.autograd.Function):
         for adj in adjs:
             adj.check_status()
         scale = torch.tensor([_DEG, 1.0, 1.0, 1.0], dtype=torch.float64, device=dev)
-        return lam, pbar * scale, None, None, None, None, None, None, None, None, None, None, None, None
+        return lam, pbar * scale, None, None, None, None, None, None, None, None, None, None, None, None, None
 
 
 def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams, dx: float,
                    dy: float, n_steps: int, out_steps: Sequence[int], dt0: float, fixed_dt: bool = False,
                    t_final: float = 0.0, checkpoint_block: int | None = None,
-                   dt_schedule: torch.Tensor | None = None, select: torch.Tensor | None = None) -> torch.Tensor:
+                   dt_schedule: torch.Tensor | None = None, select: torch.Tensor | None = None,
+                   obs_dt: float = 0.0) -> torch.Tensor:
     """Differentiable run of n_steps fused steps on one patch.
 
     q0: (5, my, mx) float64 CUDA tensor (x fastest), theta: (4,) float64
@@ -350,6 +351,9 @@ def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams
     select (int64 CUDA tensor of flat indices into the (5, my, mx) state):
     return only these entries at each output step, shape (len(out_steps),
     *select.shape) -- e.g. gauge cells' depths -- instead of whole states.
+    obs_dt > 0 (with the tick rule): every dt is also clipped at the next
+    multiple of obs_dt, so that the run lands on each observation time, as
+    the port's flume loop does (pf_flume/flume_model.py:152-153).
     """
     for n in out_steps:
         if not 0 <= n <= n_steps:
@@ -360,7 +364,8 @@ def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams
         dt_schedule = dt_schedule.contiguous()
     return _Rollout.apply(q0, theta, b if callable(b) else b.contiguous(), params, dx, dy, int(n_steps),
                           tuple(int(n) for n in out_steps),
-                          float(dt0), bool(fixed_dt), float(t_final), checkpoint_block, dt_schedule, select)
+                          float(dt0), bool(fixed_dt), float(t_final), checkpoint_block, dt_schedule, select,
+                          float(obs_dt))
 
 
 def checkpoint_block_of(out: torch.Tensor) -> int:

@@ -252,6 +252,17 @@ __global__ void __launch_bounds__(TPB) k_final(dclaw_params P, Geom g, Work W, d
     if (stage_finalize(P, g, W, q_out, i, j, clk->dt)) flag_status(clk, DCLAW_ERR_NAN);
 }
 
+// the next dt after the tick rule's choice dtn: clipped at the next
+// observation time (with the tick rule and t_obs > 0), then at t_final
+__device__ __forceinline__ double clip_next_dt(const dclaw_clock* clk, double dtn) {
+    if (!clk->fixed_dt && clk->t_obs > 0.0) {
+        const double tn = (floor(clk->t / clk->t_obs + 1.0e-9) + 1.0) * clk->t_obs;
+        dtn = fmin2(dtn, tn - clk->t);
+    }
+    if (clk->t_final > 0.0) dtn = fmax2(fmin2(dtn, clk->t_final - clk->t), 0.0);
+    return dtn;
+}
+
 __global__ void k_tick(dclaw_params P, dclaw_clock* clk) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double cfl = __longlong_as_double((long long)clk->cfl_bits);
@@ -260,9 +271,7 @@ __global__ void k_tick(dclaw_params P, dclaw_clock* clk) {
     clk->dt_last = dt;
     clk->t = clk->t + dt;
     clk->nsteps = clk->nsteps + 1;
-    double dtn = clk->fixed_dt ? dt : tick_next_dt(P, dt, cfl);
-    if (clk->t_final > 0.0) dtn = fmax2(fmin2(dtn, clk->t_final - clk->t), 0.0);
-    clk->dt = dtn;
+    clk->dt = clip_next_dt(clk, clk->fixed_dt ? dt : tick_next_dt(P, dt, cfl));
     clk->cfl_bits = 0ull;
 }
 
@@ -278,6 +287,13 @@ __global__ void k_clock_init(dclaw_clock* clk, double t, double dt, double t_fin
     clk->blocks_done = 0;
     clk->status = 0;
     clk->fixed_dt = fixed_dt;
+    clk->t_obs = 0.0;
+}
+
+__global__ void k_clock_set_obs(dclaw_clock* clk, double t_obs) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    clk->t_obs = t_obs;
+    clk->dt = clip_next_dt(clk, clk->dt);
 }
 
 // ---- fused step: K1 cell records + K2 tiles --------------------------------
@@ -307,9 +323,7 @@ __device__ __forceinline__ void tick_device(const dclaw_params& P, dclaw_clock* 
     clk->dt_last = dt;
     clk->t = clk->t + dt;
     clk->nsteps = clk->nsteps + 1;
-    double dtn = clk->fixed_dt ? dt : tick_next_dt(P, dt, cfl);
-    if (clk->t_final > 0.0) dtn = fmax2(fmin2(dtn, clk->t_final - clk->t), 0.0);
-    clk->dt = dtn;
+    clk->dt = clip_next_dt(clk, clk->fixed_dt ? dt : tick_next_dt(P, dt, cfl));
     clk->cfl_bits = 0ull;
     clk->blocks_done = 0u;
 }
@@ -1063,6 +1077,12 @@ size_t dclaw_workspace_bytes(int mx, int my) {
 int dclaw_clock_init(dclaw_clock* clock, double t, double dt, double t_final, int fixed_dt, void* stream) {
     if (!clock) return DCLAW_ERR_ARG;
     k_clock_init<<<1, 32, 0, (cudaStream_t)stream>>>(clock, t, dt, t_final, fixed_dt);
+    return cuda_status();
+}
+
+int dclaw_clock_set_obs(dclaw_clock* clock, double t_obs, void* stream) {
+    if (!clock || !(t_obs >= 0.0)) return DCLAW_ERR_ARG;
+    k_clock_set_obs<<<1, 32, 0, (cudaStream_t)stream>>>(clock, t_obs);
     return cuda_status();
 }
 

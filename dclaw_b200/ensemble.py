@@ -33,18 +33,25 @@ class Member:
     dy: float
     dt_initial: float
     t_final: float = 0.0
+    t_obs: float = 0.0   # observation interval every dt is clipped at (tick rule); 0: off
 
 
-def clock_array(dts, t_finals, fixed_dt: bool = False) -> np.ndarray:
-    """Host image of n initialised clocks (t = 0) as float64 words."""
+def clock_array(dts, t_finals, fixed_dt: bool = False, t_obs=None) -> np.ndarray:
+    """Host image of n initialised clocks (t = 0) as float64 words. t_obs
+    (per member, 0: off): the observation interval every dt is also clipped
+    at (with the tick rule), as the device clock's tick does."""
     n = len(dts)
     arr = (CClock * n)()
     for k in range(n):
         dt, tf = float(dts[k]), float(t_finals[k])
+        to = float(t_obs[k]) if t_obs is not None else 0.0
+        if not fixed_dt and to > 0.0:
+            dt = min(dt, (np.floor(0.0 / to + 1.0e-9) + 1.0) * to - 0.0)
         arr[k].t = 0.0
         arr[k].t_final = tf
         arr[k].dt = max(min(dt, tf), 0.0) if tf > 0.0 else dt
         arr[k].fixed_dt = int(fixed_dt)
+        arr[k].t_obs = to
     return np.frombuffer(bytes(arr), dtype=np.float64).copy()
 
 
@@ -77,7 +84,8 @@ class EnsembleStepper:
         params = (CParams * self.n)(*[m.params.to_c() for m in members])
         self.params = torch.frombuffer(bytearray(bytes(params)), dtype=torch.uint8).to(self.device)
         self.clocks = torch.tensor(clock_array([m.dt_initial for m in members], [m.t_final for m in members],
-                                               fixed_dt), device=self.device)
+                                               fixed_dt, [getattr(m, "t_obs", 0.0) for m in members]),
+                                   device=self.device)
         self.graph = None
 
     def _layout(self, tile_shape: int) -> None:

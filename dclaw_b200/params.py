@@ -72,6 +72,7 @@ class CClock(ctypes.Structure):
         ("blocks_done", ctypes.c_uint32),
         ("status", ctypes.c_int32),
         ("fixed_dt", ctypes.c_int32),
+        ("t_obs", ctypes.c_double),
     ]
 
 

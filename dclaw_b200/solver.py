@@ -118,9 +118,16 @@ class PatchStepper:
         self.graph_steps = 0
 
     # ---- clock -------------------------------------------------------------
-    def init_clock(self, dt: float, t: float = 0.0, t_final: float = 0.0, fixed_dt: bool = False) -> None:
+    def init_clock(self, dt: float, t: float = 0.0, t_final: float = 0.0, fixed_dt: bool = False,
+                   t_obs: float = 0.0) -> None:
+        """t_obs > 0: with the tick rule every dt is also clipped at the next
+        multiple of t_obs, so that t lands on each observation time (the
+        port's flume loop)."""
         _lib.check(self.lib.dclaw_clock_init(_lib.ptr(self.clock), float(t), float(dt), float(t_final),
                                              int(fixed_dt), _lib.stream_ptr()), "clock init")
+        if t_obs > 0.0:
+            _lib.check(self.lib.dclaw_clock_set_obs(_lib.ptr(self.clock), float(t_obs), _lib.stream_ptr()),
+                       "clock observation interval")
 
     def read_clock(self) -> CClock:
         buf = self.clock.cpu().numpy().tobytes()

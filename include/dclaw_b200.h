@@ -113,6 +113,11 @@ typedef struct dclaw_clock {
     uint32_t blocks_done;/* internal counter */
     int32_t status;      /* DCLAW_OK or DCLAW_ERR_NAN */
     int32_t fixed_dt;    /* 1: keep dt constant (no tick rule) */
+    double t_obs;        /* > 0 (with the tick rule): every dt is also clipped at
+                            the next multiple of t_obs, so t lands on each
+                            observation time: dt <= (floor(t / t_obs + 1e-9) + 1)
+                            t_obs - t, the port's flume loop
+                            (pf_flume/flume_model.py:152-153); 0: off */
 } dclaw_clock;
 
 /* ---- library info and parameters ---------------------------------------- */
@@ -391,9 +396,11 @@ int dclaw_step_adjoint_batched_reverse(const dclaw_adj_batch* batch, const dclaw
                                        const double* b, const double* lam_out, double* lam_in, double* pbar,
                                        void* work, int32_t* status, void* stream);
 
-/* initialise a device clock: t, dt, t_final, fixed_dt; counters cleared */
+/* initialise a device clock: t, dt, t_final, fixed_dt; counters cleared, t_obs 0 */
 int dclaw_clock_init(dclaw_clock* clock, double t, double dt, double t_final, int fixed_dt,
                      void* stream);
+/* set the clock's observation interval (0: off) and clip its next dt by it */
+int dclaw_clock_set_obs(dclaw_clock* clock, double t_obs, void* stream);
 /* max over cells of |u|+sqrt(g h) (interior layout) written to *smax (device double) */
 int dclaw_max_wave_speed(const double* q, int mx, int my, const dclaw_params* p, double* smax,
                          void* stream);

@@ -1691,6 +1691,9 @@ int oracle_threads(int n) {
  * mx x my interior state q (5 SoA planes, in/out) over bed b (mx*my).
  * dt_hist/cfl_hist (nullable) receive each step's dt and Courant number.
  * fixed_dt != 0 keeps dt constant. t_final > 0 clips dt so t <= t_final.
+ * t_obs > 0 (with the tick rule) first clips dt at the next multiple of
+ * t_obs, (floor(t/t_obs + 1e-9) + 1) t_obs - t, the differentiable port's
+ * observation clamp (pf_flume/flume_model.py:152-153).
  * parallel != 0 uses the OpenMP step2 (bit-identical to the serial one).
  * xlog/ylog (nullable): branch bits of the LAST step, sized
  * (my+2)*(mx+1) and (mx+2)*(my+1).
@@ -1699,7 +1702,7 @@ int oracle_threads(int n) {
 int oracle_run(const dclaw_params* prm, int mx, int my, double dx, double dy, double* q,
                const double* b, int nsteps, double dt_initial, double t_final, int fixed_dt,
                int parallel, double* dt_hist, double* cfl_hist, uint32_t* xlog, uint32_t* ylog,
-               double* t_out) {
+               double* t_out, double t_obs) {
     Model M = make_model(prm);
     Patch pt(mx, my);
     put_state(pt, q);
@@ -1709,6 +1712,7 @@ int oracle_run(const dclaw_params* prm, int mx, int my, double dx, double dy, do
     int status = 0;
     for (int n = 0; n < nsteps; ++n) {
         double dtn = dt;
+        if (!fixed_dt && t_obs > 0.0) dtn = fmin2(dtn, (std::floor(t / t_obs + 1.0e-9) + 1.0) * t_obs - t);
         if (t_final > 0.0) dtn = fmax2(fmin2(dtn, t_final - t), 0.0);
         bc2amr(M.p, pt);
         if (has_nan(pt)) { status = 3; break; }

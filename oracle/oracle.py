@@ -57,7 +57,7 @@ class Oracle:
         L.oracle_run.restype = ctypes.c_int
         L.oracle_run.argtypes = [ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                  ctypes.c_double, _dp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
-                                 ctypes.c_int, ctypes.c_int, _dp, _dp, _up, _up, _dp]
+                                 ctypes.c_int, ctypes.c_int, _dp, _dp, _up, _up, _dp, ctypes.c_double]
         L.oracle_threads.restype = ctypes.c_int
         L.oracle_threads.argtypes = [ctypes.c_int]
         for name in ("oracle_bc2amr",):
@@ -91,8 +91,9 @@ class Oracle:
 
     def run(self, p: DClawParams, q: np.ndarray, b: np.ndarray, dx: float, dy: float, nsteps: int,
             dt_initial: float, t_final: float = 0.0, fixed_dt: bool = False, parallel: bool = True,
-            branch_log: bool = False, libm: str = "glibc"):
-        """Advance q (5, my, mx) by nsteps; returns dict(q, dt, cfl, t, status, xlog, ylog)."""
+            branch_log: bool = False, libm: str = "glibc", t_obs: float = 0.0):
+        """Advance q (5, my, mx) by nsteps; returns dict(q, dt, cfl, t, status, xlog, ylog).
+        t_obs > 0 clips each dt at the next multiple of t_obs (tick rule only)."""
         self.set_libm(libm)
         q = np.ascontiguousarray(q, dtype=np.float64).copy()
         b = np.ascontiguousarray(b, dtype=np.float64)
@@ -105,7 +106,7 @@ class Oracle:
         cp = p.to_c()
         st = self.lib.oracle_run(ctypes.byref(cp), mx, my, dx, dy, _ptr(q), _ptr(b), nsteps, dt_initial,
                                  t_final, int(fixed_dt), int(parallel), _ptr(dt_hist), _ptr(cfl_hist),
-                                 _ptr(xlog, _up), _ptr(ylog, _up), _ptr(t_out))
+                                 _ptr(xlog, _up), _ptr(ylog, _up), _ptr(t_out), float(t_obs))
         return dict(q=q, dt=dt_hist[:nsteps], cfl=cfl_hist[:nsteps], t=float(t_out[0]), status=st,
                     xlog=xlog, ylog=ylog)
 

@@ -213,6 +213,44 @@ def test_rollout_gradient_with_a_moving_gate_bed(cuda_device):
     _close(float(gt[0]), _fd(lambda h: Lf(q00, th0 + h * e0), eps0=4e-6), "phi")
 
 
+def test_rollout_with_observation_interval(cuda_device):
+    """rollout_states(obs_dt=...) steps with the clock clipping dt at every
+    observation time: its states equal the fused step's with that clock,
+    its dt schedule lands on the observation times, and the recorded
+    schedule replays the same run for the gradient."""
+    from dclaw_b200.solver import PatchStepper
+
+    dev = cuda_device
+    p, qn, bn = _small_flow(seed=3)
+    b = torch.tensor(bn, device=dev)
+    n, outs, t_obs = 24, [12, 24], 0.03
+    wts = torch.tensor(_loss_weights(qn, len(outs), seed=2), device=dev)
+    q0 = torch.tensor(qn, device=dev, requires_grad=True)
+    theta = theta_of(p, dev).requires_grad_(True)
+    L, o = _run_loss(q0, theta, b, p, 1.0, n, outs, wts, dt0=0.02, obs_dt=t_obs)
+    sched = last_dts(o).clone()
+    L.backward()
+    st = PatchStepper(torch.tensor(qn, device=dev), b, p, 1.0, 1.0)
+    st.init_clock(0.02, t_obs=t_obs)
+    st.step(12)
+    assert torch.equal(st.state(), o[0])
+    st.step(12)
+    assert torch.equal(st.state(), o[1])
+    t = st.read_clock().t
+    tt = np.cumsum(sched.cpu().numpy())
+    assert tt[-1] == t
+    assert all(np.abs(tt - m * t_obs).min() < 1e-9 for m in range(1, int(t / t_obs + 1e-9) + 1))
+    with torch.no_grad():
+        L2, _ = _run_loss(torch.tensor(qn, device=dev), theta_of(p, dev), b, p, 1.0, n, outs, wts, dt0=0.0,
+                          dt_schedule=sched)
+    assert float(L2) == float(L)
+    q1 = torch.tensor(qn, device=dev, requires_grad=True)
+    th1 = theta_of(p, dev).requires_grad_(True)
+    L3, _ = _run_loss(q1, th1, b, p, 1.0, n, outs, wts, dt0=0.0, dt_schedule=sched)
+    L3.backward()
+    assert torch.equal(q1.grad, q0.grad) and torch.equal(th1.grad, theta.grad)
+
+
 def test_checkpoint_block_gives_identical_gradients(cuda_device):
     dev = cuda_device
     p, qn, bn = _small_flow(seed=2)

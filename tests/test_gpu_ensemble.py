@@ -35,7 +35,7 @@ def _single(members, nsteps, dev):
     res = []
     for m in members:
         ps = PatchStepper(torch.from_numpy(m.q).to(dev), torch.from_numpy(m.b).to(dev), m.params, m.dx, m.dy)
-        ps.init_clock(m.dt_initial, t_final=m.t_final)
+        ps.init_clock(m.dt_initial, t_final=m.t_final, t_obs=m.t_obs)
         ps.step(nsteps)
         c = ps.read_clock()
         res.append((ps.state().cpu().numpy(), (c.t, c.dt, c.cfl, c.nsteps, c.status)))
@@ -71,6 +71,21 @@ def test_batched_one_cta_per_sm_and_t_final():
     ens = EnsembleStepper(members, dev)
     ens.batch.tile_ctas_per_sm = 1
     ens.step(12)
+    torch.cuda.synchronize()
+    _check(ens, ref)
+
+
+def test_batched_observation_intervals():
+    """Per-member observation intervals (and t_final) clip each member's dt as
+    the single-patch clock does."""
+    import dataclasses
+
+    dev = torch.device("cuda:0")
+    members = [dataclasses.replace(m, t_obs=to) for m, to in
+               zip(_members(seed=9, t_final=0.4), [0.05, 0.0, 0.013, 0.1, 0.02, 0.07, 0.0])]
+    ref = _single(members, 30, dev)
+    ens = EnsembleStepper(members, dev)
+    ens.step(30)
     torch.cuda.synchronize()
     _check(ens, ref)
 

@@ -85,6 +85,34 @@ def test_variants(cuda_device, oracle, variant):
     check(c, 40, oracle)
 
 
+def test_observation_clamp(cuda_device, oracle):
+    """With an observation interval the clock clips every dt at the next
+    multiple of it, (floor(t/t_obs + 1e-9) + 1) t_obs - t, as the port's
+    flume loop does (pf_flume/flume_model.py:152-153): dt history, Courant
+    numbers and state bit for bit with the oracle, and t lands on every
+    observation time it passes."""
+    from dclaw_b200.solver import PatchStepper
+
+    c = W.slope_runout(n=96)
+    n, t_obs = 60, 0.25
+    st = PatchStepper(torch.tensor(c.q, device=cuda_device), torch.tensor(c.b, device=cuda_device), c.params,
+                      c.dx, c.dy)
+    st.init_clock(c.dt_initial, t_obs=t_obs)
+    hist = torch.zeros((n, 4), dtype=torch.float64, device=cuda_device)
+    st.step(n, history=hist)
+    h = hist.cpu().numpy()
+    o = oracle.run(c.params, c.q, c.b, c.dx, c.dy, n, c.dt_initial, libm="portable", t_obs=t_obs)
+    free = oracle.run(c.params, c.q, c.b, c.dx, c.dy, n, c.dt_initial, libm="portable")
+    assert np.array_equal(h[:, 3], o["dt"]) and np.array_equal(h[:, 2], o["cfl"])
+    assert np.array_equal(st.state().cpu().numpy(), o["q"])
+    assert not np.array_equal(o["dt"], free["dt"])
+    t = h[:, 0]
+    assert t[-1] == o["t"]
+    stops = [m for m in range(1, int(t[-1] / t_obs + 1e-9) + 1)]
+    assert len(stops) >= 8
+    assert all(np.abs(t - m * t_obs).min() < 1e-9 for m in stops)
+
+
 def test_random_field_small(cuda_device, oracle):
     check(W.random_field_case(n=256, dx=0.5, seed=5), 30, oracle)
 

@@ -133,3 +133,21 @@ def test_src2method2_keeps_rho_h(oracle, libm):
     assert np.abs(rhoh1 - rhoh0)[wet].max() <= 1e-12 * rhoh0[wet].max()
     assert np.abs(qo[3] / qo[0] - qi[3] / qi[0])[wet].max() > 1e-4     # m moved
     assert np.abs(qo[4] - qi[4])[wet].max() > 1.0                       # p moved
+
+
+def test_observation_clamp_lands_on_observation_times(oracle):
+    """t_obs clips each tick-rule dt at the next multiple of t_obs (the
+    port's flume loop, pf_flume/flume_model.py:152-153): t reaches every
+    observation time it passes, and no step is longer than the free run's
+    rule would make it from the same Courant number."""
+    c = W.slope_runout(n=48)
+    t_obs = 0.25
+    o = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 40, c.dt_initial, libm="portable", t_obs=t_obs)
+    assert o["status"] == 0
+    t = np.cumsum(o["dt"])
+    assert t[-1] == o["t"]
+    stops = list(range(1, int(t[-1] / t_obs + 1e-9) + 1))
+    assert len(stops) >= 4
+    assert all(np.abs(t - m * t_obs).min() < 1e-9 for m in stops)
+    rule = np.minimum(o["dt"][:-1] * c.params.cfl_desired / o["cfl"][:-1], c.params.dt_max)
+    assert np.all(o["dt"][1:] <= rule) and np.any(o["dt"][1:] < rule)
