@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(BTPB, BlkMinB<OP>::value) k_adj_blocks(BatchAr
     __shared__ dclaw_params sP;
     __shared__ uint64_t s_e;
     __shared__ int s_list[BTPB];
-    __shared__ int s_n;
+    __shared__ int s_wcnt[BTPB / 32];
     pdl_wait();
     const unsigned int n = *count;
     int cur = -1;
@@ -364,16 +364,21 @@ __global__ void __launch_bounds__(BTPB, BlkMinB<OP>::value) k_adj_blocks(BatchAr
                     for (int k = 0; k < NCB; ++k) dst[(size_t)k * np + oi] = 0.0;
                 }
             }
+            // the list is in thread order (warp counts summed in warp
+            // order), so each item lands on the same thread every run and
+            // the block's parameter partial is bit-reproducible
             const unsigned bal = __ballot_sync(0xffffffffu, need);
-            const int lane = threadIdx.x & 31;
-            if (threadIdx.x == 0) s_n = 0;
+            const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+            if (lane == 0) s_wcnt[wid] = __popc(bal);
             __syncthreads();
-            int base = 0;
-            if (lane == 0 && bal) base = atomicAdd(&s_n, __popc(bal));
-            base = __shfl_sync(0xffffffffu, base, 0);
+            int base = 0, tot = 0;
+            for (int w = 0; w < BTPB / 32; ++w) {
+                base += w < wid ? s_wcnt[w] : 0;
+                tot += s_wcnt[w];
+            }
             if (need) s_list[base + __popc(bal & ((1u << lane) - 1u))] = threadIdx.x;
             __syncthreads();
-            if ((int)threadIdx.x < s_n) {
+            if ((int)threadIdx.x < tot) {
                 const int t = s_list[threadIdx.x];
                 block_item<OP>(a, m, sM, sP, g, W, A, L, bx * ACT_TILE + (t & 15) - 1, by * ACT_TILE + (t >> 4) - 1,
                                pb);
