@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-band-rows", type=int, default=256,
+                    help="rows of the one-thread CPU sample (one step)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--json-out", default="")
     ap.add_argument("--ensemble-members", type=int, default=256,
@@ -158,6 +160,8 @@ def make_case(args, rank=0):
 
 def cpu_baseline(args, case, steps):
     """Oracle (CPU restatement) on `steps` full steps of the same case."""
+    import numpy as np
+
     from oracle import Oracle
 
     o = Oracle()
@@ -166,9 +170,25 @@ def cpu_baseline(args, case, steps):
     r = o.run(case.params, case.q, case.b, case.dx, case.dy, steps, case.dt_initial, parallel=True)
     el = time.perf_counter() - t0
     cells = case.mx * case.my * steps
-    return {"value": cells / el, "unit": "cell-updates/s", "cores": cores, "kind": "port",
-            "sample": f"first {steps} steps of the {case.mx}x{case.my} workload from its initial state "
-                      f"({el:.1f} s, OpenMP, oracle/dclaw_oracle.cpp)", "status": r["status"]}
+    out = {"value": cells / el, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+           "sample": f"first {steps} steps of the {case.mx}x{case.my} workload from its initial state "
+                     f"({el:.1f} s, OpenMP, oracle/dclaw_oracle.cpp)", "status": r["status"]}
+    # one thread, on a band of rows of the same field (the same band, all
+    # threads, beside it for the scaling)
+    band = min(case.my, max(1, args.cpu_band_rows))
+    qb, bb = np.ascontiguousarray(case.q[:, :band, :]), np.ascontiguousarray(case.b[:band, :])
+    timing = {}
+    for n in (1, cores):
+        o.threads(n)
+        t0 = time.perf_counter()
+        o.run(case.params, qb, bb, case.dx, case.dy, 1, case.dt_initial, parallel=True)
+        timing[n] = time.perf_counter() - t0
+    o.threads(cores)
+    out["one_thread"] = {"value": case.mx * band / timing[1], "unit": "cell-updates/s", "cores": 1,
+                         "all_threads_same_sample": case.mx * band / timing[cores],
+                         "sample": f"1 step of rows 1..{band} of the same field ({case.mx}x{band}, walls at the "
+                                   f"band's edges; {timing[1]:.1f} s on 1 thread, {timing[cores]:.2f} s on {cores})"}
+    return out
 
 
 def run_reference(args):

@@ -44,6 +44,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -180,12 +181,19 @@ struct Patch {
 };
 
 // digclaw_module.f90:500-719 (bed_normal = 0: theta = 0, gz = grav)
+// Cells are independent (each reads q and aux 1..3, writes its own aux
+// 4..6), so rows run on OpenMP threads, each with its own copy of the model
+// for the module-global phi the reference overwrites per cell (:557); the
+// global ends as the last cell's, as in the serial loop.
 void calc_taudir(Model& M, Patch& pt, double dx, double dy) {
     const dclaw_params& P = M.p;
     const int mx = pt.mx, my = pt.my;
     const double dry = P.dry_tolerance;
     double gz = P.grav;
+#pragma omp parallel for schedule(static)
     for (int j = 2 - MBC; j <= my + MBC - 1; ++j) {
+        Model Mrow = M;
+        Model& M = Mrow;
         for (int i = 2 - MBC; i <= mx + MBC - 1; ++i) {
             double theta = 0.0;
             double u, v, m, chi, rho;
@@ -269,6 +277,7 @@ void calc_taudir(Model& M, Patch& pt, double dx, double dy) {
             }
         }
     }
+    M.phi = pt.A(I_PHI, mx + MBC - 1, my + MBC - 1);
 }
 
 // b4step2.f90:7-113 (check4nans is reported by the driver; setaux is not re-run:
@@ -277,6 +286,8 @@ void b4step2(Model& M, Patch& pt, double dx, double dy) {
     const dclaw_params& P = M.p;
     const int mx = pt.mx, my = pt.my;
     double gz = P.grav;
+    // per-cell passes: rows on OpenMP threads
+#pragma omp parallel for schedule(static)
     for (int j = 1 - MBC; j <= my + MBC; ++j) {
         for (int i = 1 - MBC; i <= mx + MBC; ++i) {
             double u, v, m, chi, rho;
@@ -285,6 +296,7 @@ void b4step2(Model& M, Patch& pt, double dx, double dy) {
             pt.Q(I_BDIF, i, j) = fmax2(pt.Q(I_BDIF, i, j), 0.0);
         }
     }
+#pragma omp parallel for schedule(static)
     for (int j = 1 - MBC; j <= my + MBC; ++j) {
         for (int i = 1 - MBC; i <= mx + MBC; ++i) {
             if (pt.Q(1, i, j) > 0.0) {
@@ -1095,18 +1107,28 @@ double step2_serial(Model& M, Patch& pt, Fluxes& F, double dx, double dy, double
 // Same arithmetic, same per-element summation order, split into phases that
 // OpenMP can run concurrently: every sum keeps the operand order of the
 // serial sweep (x-sweep row j-1 before row j, y-sweep column i-1 before i).
+// zero n doubles on the OpenMP threads (the flux and increment arrays are
+// hundreds of MB on large patches; a serial fill would bound the scaling)
+static void par_zero(double* p, size_t n) {
+    const long long nn = (long long)n;
+#pragma omp parallel for schedule(static)
+    for (long long k = 0; k < nn; ++k) p[k] = 0.0;
+}
+
 double step2_parallel(Model& M, Patch& pt, Fluxes& F, double dx, double dy, double dt,
                       uint32_t* xlog, uint32_t* ylog) {
     const int mx = pt.mx, my = pt.my;
     double dtdx = dt / dx, dtdy = dt / dy;
     const size_t LX = (size_t)mx + 2 * MBC, LY = (size_t)my + 2 * MBC;
     // per-slice transverse increments, side 1 and side 2 (gaddm == gaddp)
-    std::vector<double> Gx((size_t)(my + 2) * 2 * LX * MEQN);
+    const size_t nGx = (size_t)(my + 2) * 2 * LX * MEQN;
+    std::unique_ptr<double[]> Gx(new double[nGx]);
+    par_zero(Gx.get(), nGx);
     std::vector<double> cflx(my + 2), cfly(mx + 2);
-    std::fill(F.fm.begin(), F.fm.end(), 0.0);
-    std::fill(F.fp.begin(), F.fp.end(), 0.0);
-    std::fill(F.gm.begin(), F.gm.end(), 0.0);
-    std::fill(F.gp.begin(), F.gp.end(), 0.0);
+    par_zero(F.fm.data(), F.fm.size());
+    par_zero(F.fp.data(), F.fp.size());
+    par_zero(F.gm.data(), F.gm.size());
+    par_zero(F.gp.data(), F.gp.size());
 #pragma omp parallel
     {
         Slice sx(mx);
@@ -1137,8 +1159,10 @@ double step2_parallel(Model& M, Patch& pt, Fluxes& F, double dx, double dy, doub
                 F.gm[F.at(m, i, j)] = acc;
                 F.gp[F.at(m, i, j)] = acc;
             }
-    std::vector<double>().swap(Gx);
-    std::vector<double> Gy((size_t)(mx + 2) * 2 * LY * MEQN);
+    Gx.reset();
+    const size_t nGy = (size_t)(mx + 2) * 2 * LY * MEQN;
+    std::unique_ptr<double[]> Gy(new double[nGy]);
+    par_zero(Gy.get(), nGy);
 #pragma omp parallel
     {
         Slice sy(my);
@@ -1585,8 +1609,11 @@ void setaux(const dclaw_params& P, Patch& pt, const double* b_interior) {
 }
 
 bool has_nan(Patch& pt) {
-    for (double x : pt.q) if (std::isnan(x)) return true;
-    return false;
+    const long long n = (long long)pt.q.size();
+    int found = 0;
+#pragma omp parallel for schedule(static) reduction(| : found)
+    for (long long k = 0; k < n; ++k) found |= std::isnan(pt.q[k]) ? 1 : 0;
+    return found != 0;
 }
 
 // tick.f:490-526 with stepgrid's dtnew = dt*cfl_desired/cflgrid
