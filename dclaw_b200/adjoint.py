@@ -205,7 +205,7 @@ def _block(n_steps: int, checkpoint_block: int | None, state_bytes: int = 0, res
 class _Rollout(torch.autograd.Function):
     @staticmethod
     def forward(ctx, q0, theta, b, params, dx, dy, n_steps, out_steps, dt0, fixed_dt, t_final, checkpoint_block,
-                dt_schedule, select, obs_dt):
+                dt_schedule, select, obs_dt, n_obs):
         prm = with_theta(params, theta.detach().cpu())
         # a moving bed: a function of the simulated time, evaluated before
         # every step (the port's step(q, bed(t), ...) loop)
@@ -214,7 +214,9 @@ class _Rollout(torch.autograd.Function):
             b = bed_fn(torch.zeros((), dtype=torch.float64, device=q0.device)).contiguous()
         st = PatchStepper(q0.detach(), b, prm, dx, dy)
         if dt_schedule is not None:
-            st.init_clock(0.0, fixed_dt=True)
+            # a replayed schedule keeps the observation interval for the
+            # record (a fixed-dt clock is not clipped by it)
+            st.init_clock(0.0, fixed_dt=True, t_obs=float(obs_dt) if n_obs else 0.0)
         else:
             st.init_clock(float(dt0), t_final=float(t_final), fixed_dt=bool(fixed_dt), t_obs=float(obs_dt))
         lib = _lib.load()
@@ -223,7 +225,15 @@ class _Rollout(torch.autograd.Function):
         dts = torch.empty(n_steps, dtype=torch.float64, device=q0.device)
         t_start = torch.empty(n_steps if bed_fn is not None else 0, dtype=torch.float64, device=q0.device)
         oshape = tuple(q0.shape) if select is None else tuple(select.shape)
-        outs = torch.empty((len(out_steps),) + oshape, dtype=q0.dtype, device=q0.device)
+        if n_obs:
+            # observation slots: filled on the device when the clock lands
+            # on an observation time; slots the run does not reach stay 0
+            outs = torch.zeros((n_obs,) + oshape, dtype=q0.dtype, device=q0.device)
+            obs_step = torch.full((n_obs,), -1, dtype=torch.int32, device=q0.device)
+            sel64 = None if select is None else select.reshape(-1).to(torch.int64).contiguous()
+            nsel = q0.numel() if select is None else sel64.numel()
+        else:
+            outs = torch.empty((len(out_steps),) + oshape, dtype=q0.dtype, device=q0.device)
         pick = (lambda t: t) if select is None else (lambda t: t.reshape(-1)[select])
         where = {}
         for idx, n in enumerate(out_steps):
@@ -252,7 +262,15 @@ class _Rollout(torch.autograd.Function):
             dts[n:n + 1].copy_(st.clock[3:4])   # dt the step used
             for idx in where.get(n + 1, []):
                 outs[idx].copy_(pick(src))
+            if n_obs:
+                _lib.check(lib.dclaw_obs_record(_lib.ptr(st.clock), 1, None, _lib.ptr(src), _lib.ptr(sel64), nsel,
+                                                n_obs, n + 1, _lib.ptr(outs), _lib.ptr(obs_step),
+                                                _lib.stream_ptr()), "observation record")
         _lib.check(st.status(), "rollout forward")
+        if n_obs:
+            # the step each slot was recorded at (-1: not reached) stands in
+            # for the output steps of the backward pass
+            out_steps = tuple(int(v) for v in obs_step.cpu().tolist())
         # the block inputs are saved tensors: autograd frees them after the
         # backward pass (unless the graph is retained), so a loop of gradient
         # evaluations reuses one allocation instead of holding two
@@ -260,6 +278,7 @@ class _Rollout(torch.autograd.Function):
         ctx.bed_fn = bed_fn
         ctx.select = select
         ctx.meta = (prm, float(dx), float(dy), int(n_steps), tuple(out_steps), k)
+        ctx.obs_steps = tuple(out_steps) if n_obs else None
         return outs
 
     @staticmethod
@@ -322,7 +341,7 @@ class _Rollout(torch.autograd.Function):
         for adj in adjs:
             adj.check_status()
         scale = torch.tensor([_DEG, 1.0, 1.0, 1.0], dtype=torch.float64, device=dev)
-        return lam, pbar * scale, None, None, None, None, None, None, None, None, None, None, None, None, None
+        return lam, pbar * scale, None, None, None, None, None, None, None, None, None, None, None, None, None, None
 
 
 def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams, dx: float,
@@ -365,7 +384,42 @@ def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams
     return _Rollout.apply(q0, theta, b if callable(b) else b.contiguous(), params, dx, dy, int(n_steps),
                           tuple(int(n) for n in out_steps),
                           float(dt0), bool(fixed_dt), float(t_final), checkpoint_block, dt_schedule, select,
-                          float(obs_dt))
+                          float(obs_dt), 0)
+
+
+def rollout_observations(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams, dx: float, dy: float,
+                         n_steps: int, obs_dt: float, n_obs: int, dt0: float, t_end: float = 0.0,
+                         select: torch.Tensor | None = None, checkpoint_block: int | None = None,
+                         dt_schedule: torch.Tensor | None = None) -> torch.Tensor:
+    """Differentiable run that records observations at fixed times, as the
+    port's flume loop does (pf_flume/flume_model.py:150-158): every tick-rule
+    dt is clipped at the next multiple of obs_dt (and at t_end when
+    t_end > 0), and after a step that lands on (k+1) obs_dt with dt > 0,
+    slot k receives the state (or its `select` entries). Returns
+    (n_obs, 5, my, mx) or (n_obs, *select.shape); slots the n_steps steps
+    do not reach stay 0 and take no gradient. `observation_steps(out)`
+    gives the step each slot was recorded at. The other arguments are those
+    of `rollout_states`; dt_schedule replays recorded dts (the slots then
+    follow the replayed times)."""
+    if not obs_dt > 0.0 or int(n_obs) < 1:
+        raise ValueError("obs_dt must be > 0 and n_obs >= 1")
+    if dt_schedule is not None:
+        if dt_schedule.shape != (n_steps,) or dt_schedule.dtype != torch.float64 or not dt_schedule.is_cuda:
+            raise ValueError("dt_schedule must be a (n_steps,) float64 CUDA tensor")
+        dt_schedule = dt_schedule.contiguous()
+    return _Rollout.apply(q0, theta, b if callable(b) else b.contiguous(), params, dx, dy, int(n_steps), (),
+                          float(dt0), False, float(t_end), checkpoint_block, dt_schedule, select, float(obs_dt),
+                          int(n_obs))
+
+
+def observation_steps(out: torch.Tensor) -> list:
+    """The step count each observation slot of `rollout_observations` or
+    `ensemble_rollout_observations` was recorded at (-1: not reached); for
+    an ensemble, one list per slot with an entry per member."""
+    steps = getattr(out.grad_fn, "obs_steps", None)
+    if steps is None:
+        raise ValueError("not the output of a differentiable observation run")
+    return list(steps)
 
 
 def checkpoint_block_of(out: torch.Tensor) -> int:
@@ -398,8 +452,8 @@ def initial_state(h0: torch.Tensor, m0: torch.Tensor, params: DClawParams, p_rat
     return torch.where(wet.unsqueeze(0), q, torch.zeros_like(q))
 
 
-__all__ = ["StepAdjoint", "rollout_states", "theta_of", "with_theta", "initial_state", "last_dts", "THETA_NAMES",
-           "EnsembleStepAdjoint", "ensemble_rollout_states", "ensemble_last_dts"]
+__all__ = ["StepAdjoint", "rollout_states", "rollout_observations", "observation_steps", "theta_of", "with_theta", "initial_state", "last_dts", "THETA_NAMES",
+           "EnsembleStepAdjoint", "ensemble_rollout_states", "ensemble_rollout_observations", "ensemble_last_dts"]
 
 
 # ---- ensembles -----------------------------------------------------------------
@@ -466,7 +520,8 @@ def _ensemble(members, theta, fixed_dt: bool):
     from .ensemble import EnsembleStepper, Member
 
     th = theta.detach().cpu().tolist()
-    mem = [Member(m.q, m.b, with_theta(m.params, th[k]), m.dx, m.dy, m.dt_initial, m.t_final)
+    mem = [Member(m.q, m.b, with_theta(m.params, th[k]), m.dx, m.dy, m.dt_initial, m.t_final,
+                  getattr(m, "t_obs", 0.0))
            for k, m in enumerate(members)]
     return EnsembleStepper(mem, theta.device, fixed_dt=fixed_dt)
 
@@ -479,7 +534,8 @@ def _clock_field(st, k: int) -> torch.Tensor:
 
 class _EnsembleRollout(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, q0, theta, members, n_steps, out_steps, checkpoint_block, fixed_dt, dt_schedule, select):
+    def forward(ctx, q0, theta, members, n_steps, out_steps, checkpoint_block, fixed_dt, dt_schedule, select,
+                n_obs):
         st = _ensemble(members, theta, fixed_dt or dt_schedule is not None)
         st.qa.copy_(q0.detach())
         lib = _lib.load()
@@ -487,7 +543,21 @@ class _EnsembleRollout(torch.autograd.Function):
         k = _block(n_steps, checkpoint_block, st.qa.numel() * 8, reserve, q0.device)
         dts = torch.empty((n_steps, st.n), dtype=torch.float64, device=q0.device)
         oshape = tuple(q0.shape) if select is None else tuple(select.shape)
-        outs = torch.empty((len(out_steps),) + oshape, dtype=q0.dtype, device=q0.device)
+        if n_obs:
+            # observation slots per gauge entry, each filled when its own
+            # member's clock lands on an observation time
+            sel64 = select.reshape(-1).to(torch.int64).contiguous()
+            sel_h = sel64.cpu().numpy()
+            offs = np.array([st.cm[k].q_off for k in range(st.n)], dtype=np.int64)
+            ends = offs + 5 * st.mx.astype(np.int64) * st.my.astype(np.int64)
+            mem_h = np.searchsorted(offs, sel_h, side="right") - 1
+            if (mem_h < 0).any() or (sel_h >= ends[np.maximum(mem_h, 0)]).any():
+                raise ValueError("select holds arena entries outside every member")
+            member = torch.tensor(mem_h, dtype=torch.int32, device=q0.device)
+            outs = torch.zeros((n_obs,) + oshape, dtype=q0.dtype, device=q0.device)
+            obs_step = torch.full((n_obs, st.n), -1, dtype=torch.int32, device=q0.device)
+        else:
+            outs = torch.empty((len(out_steps),) + oshape, dtype=q0.dtype, device=q0.device)
         pick = (lambda t: t) if select is None else (lambda t: t[select])
         where = {}
         for idx, n in enumerate(out_steps):
@@ -513,11 +583,27 @@ class _EnsembleRollout(torch.autograd.Function):
             dts[n].copy_(_clock_field(st, 3))
             for idx in where.get(n + 1, []):
                 outs[idx].copy_(pick(src))
+            if n_obs:
+                _lib.check(lib.dclaw_obs_record(_lib.ptr(st.clocks), st.n, _lib.ptr(member), _lib.ptr(src),
+                                                _lib.ptr(sel64), sel64.numel(), n_obs, n + 1, _lib.ptr(outs),
+                                                _lib.ptr(obs_step), _lib.stream_ptr()), "observation record")
         for kk, s in enumerate(st.status()):
             _lib.check(s, f"ensemble rollout, member {kk}")
         ctx.save_for_backward(dts, store)
         ctx.select = select
         ctx.meta = (members, theta.detach(), int(n_steps), tuple(out_steps), k)
+        ctx.obs_steps = None
+        if n_obs:
+            steps = obs_step.cpu().numpy()
+            ctx.obs_steps = tuple(tuple(int(v) for v in row) for row in steps)
+            # backward: at step n, slot k's entries of the members recorded then
+            obs_where = {}
+            for kk in range(n_obs):
+                for n in sorted(set(int(v) for v in steps[kk] if v >= 0)):
+                    ents = np.nonzero(steps[kk][mem_h] == n)[0]
+                    obs_where.setdefault(n, []).append((kk, torch.tensor(ents, dtype=torch.int64,
+                                                                         device=q0.device)))
+            ctx.obs_where = obs_where
         return outs
 
     @staticmethod
@@ -544,10 +630,17 @@ class _EnsembleRollout(torch.autograd.Function):
             else:
                 target.index_add_(0, sel.reshape(-1), g_out[idx].reshape(-1))
 
+        obs_where = getattr(ctx, "obs_where", None) if ctx.obs_steps is not None else None
+        sel_flat = sel.reshape(-1) if sel is not None else None
+
         def add_outs(n, target):
-            if g_out is not None:
-                for idx in where.get(n, []):
-                    add_out(idx, target)
+            if g_out is None:
+                return
+            for idx in where.get(n, []):
+                add_out(idx, target)
+            if obs_where is not None:
+                for kk, ents in obs_where.get(n, []):
+                    target.index_add_(0, sel_flat[ents], g_out[kk].reshape(-1)[ents])
 
         segs = [seg, torch.zeros_like(seg)] if k > 1 else None
 
@@ -567,7 +660,7 @@ class _EnsembleRollout(torch.autograd.Function):
         for adj in adjs:
             adj.check_status()
         scale = torch.tensor([_DEG, 1.0, 1.0, 1.0], dtype=torch.float64, device=dev)
-        return lam, pbar * scale, None, None, None, None, None, None, None
+        return lam, pbar * scale, None, None, None, None, None, None, None, None
 
 
 def ensemble_rollout_states(q0: torch.Tensor, theta: torch.Tensor, members, n_steps: int, out_steps,
@@ -593,7 +686,28 @@ def ensemble_rollout_states(q0: torch.Tensor, theta: torch.Tensor, members, n_st
     if dt_schedule is not None and dt_schedule.shape != (n_steps, len(members)):
         raise ValueError("dt_schedule must be (n_steps, n_members)")
     return _EnsembleRollout.apply(q0, theta, list(members), int(n_steps), tuple(int(n) for n in out_steps),
-                                  checkpoint_block, bool(fixed_dt), dt_schedule, select)
+                                  checkpoint_block, bool(fixed_dt), dt_schedule, select, 0)
+
+
+def ensemble_rollout_observations(q0: torch.Tensor, theta: torch.Tensor, members, n_steps: int, n_obs: int,
+                                  select: torch.Tensor, checkpoint_block: int | None = None,
+                                  dt_schedule: torch.Tensor | None = None) -> torch.Tensor:
+    """The batched form of `rollout_observations`, the particle filter's
+    vmapped flume loop (pf_flume/inference.py:96-108 over
+    pf_flume/flume_model.py:150-158): every member steps with its own tick
+    rule clipped at the multiples of its `Member.t_obs` (and at its
+    t_final), and each gauge entry of `select` (arena indices) is recorded
+    into slot k when its own member lands on (k+1) t_obs. Returns
+    (n_obs, *select.shape); entries of slots a member does not reach stay 0.
+    `observation_steps(out)` gives, per slot, each member's step."""
+    if int(n_obs) < 1 or select is None:
+        raise ValueError("n_obs >= 1 and a select of gauge entries are required")
+    if not any(getattr(m, "t_obs", 0.0) > 0.0 for m in members):
+        raise ValueError("no member has an observation interval (Member.t_obs)")
+    if dt_schedule is not None and dt_schedule.shape != (n_steps, len(members)):
+        raise ValueError("dt_schedule must be (n_steps, n_members)")
+    return _EnsembleRollout.apply(q0, theta, list(members), int(n_steps), (), checkpoint_block, False,
+                                  dt_schedule, select, int(n_obs))
 
 
 def ensemble_last_dts(out: torch.Tensor) -> torch.Tensor:

@@ -849,6 +849,33 @@ __global__ void __launch_bounds__(TPB) k_src2_padded(dclaw_params P, int mx, int
     q[pc] = a; q[npad + pc] = b; q[2 * npad + pc] = c; q[3 * npad + pc] = d; q[4 * npad + pc] = e;
 }
 
+// observation slot of clock c after its step, or -1: the flume loop's
+// k = round(t / dt_obs) - 1 (round half to even) and its hit test
+// |t - (k+1) dt_obs| < 1e-9 with dt > 0 (pf_flume/flume_model.py:155-157)
+__device__ __forceinline__ long long obs_slot(const dclaw_clock* c, int n_obs) {
+    const double to = c->t_obs;
+    if (!(to > 0.0) || !(c->dt_last > 0.0)) return -1;
+    const double kr = rint(c->t / to) - 1.0;
+    if (!(kr >= 0.0) || !(kr < (double)n_obs)) return -1;
+    const long long k = (long long)kr;
+    return fabs(c->t - (double)(k + 1) * to) < 1.0e-9 ? k : -1;
+}
+
+__global__ void __launch_bounds__(TPB) k_obs_record(const dclaw_clock* __restrict__ clocks, int n_clocks,
+                                                    const int32_t* __restrict__ member, const double* __restrict__ q,
+                                                    const int64_t* __restrict__ sel, long long nsel, int n_obs,
+                                                    int step, double* __restrict__ out, int32_t* __restrict__ out_step) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nsel; e += stride) {
+        const long long k = obs_slot(clocks + (member ? member[e] : 0), n_obs);
+        if (k >= 0) out[k * nsel + e] = q[sel ? sel[e] : e];
+    }
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n_clocks; c += stride) {
+        const long long k = obs_slot(clocks + c, n_obs);
+        if (k >= 0) out_step[k * n_clocks + c] = step;
+    }
+}
+
 __global__ void __launch_bounds__(TPB) k_wave_speed(dclaw_params P, int mx, int my, const double* __restrict__ q,
                                                    unsigned long long* acc) {
     const long long n = (long long)mx * my;
@@ -1321,6 +1348,19 @@ int dclaw_src2(double* q, const double* aux, int mx, int my, int mbc, double dx,
     int rc = dclaw_params_check(p);
     if (rc) return rc;
     k_src2_padded<<<nblocks((long long)mx * my), TPB, 0, (cudaStream_t)stream>>>(*p, mx, my, dt, q);
+    return cuda_status();
+}
+
+int dclaw_obs_record(const dclaw_clock* clocks, int n_clocks, const int32_t* member, const double* q,
+                     const int64_t* select, int64_t n_select, int n_obs, int step, double* out,
+                     int32_t* out_step, void* stream) {
+    if (!clocks || n_clocks <= 0 || !q || n_select <= 0 || n_obs <= 0 || !out || !out_step) return DCLAW_ERR_ARG;
+    if (n_clocks > 1 && !member) return DCLAW_ERR_ARG;
+    const long long work = n_select > n_clocks ? (long long)n_select : (long long)n_clocks;
+    long long nb = (work + TPB - 1) / TPB;
+    if (nb > 4096) nb = 4096;
+    k_obs_record<<<(unsigned)nb, TPB, 0, (cudaStream_t)stream>>>(clocks, n_clocks, member, q, select,
+                                                                 (long long)n_select, n_obs, step, out, out_step);
     return cuda_status();
 }
 

@@ -401,6 +401,17 @@ int dclaw_clock_init(dclaw_clock* clock, double t, double dt, double t_final, in
                      void* stream);
 /* set the clock's observation interval (0: off) and clip its next dt by it */
 int dclaw_clock_set_obs(dclaw_clock* clock, double t_obs, void* stream);
+/* Observation record after a step (the flume loop of the differentiable port,
+   pf_flume/flume_model.py:154-158): for each clock c of n_clocks whose t lands on
+   an observation time, |t - (k+1) t_obs| < 1e-9 with k = rint(t / t_obs) - 1 in
+   0..n_obs-1, and whose last dt was positive, slot k of `out` (n_obs rows of
+   n_select doubles) receives the state entries q[select[e]] of the entries e of
+   that clock (member[e]; member NULL: all entries belong to clock 0; select
+   NULL: entry e is q[e]), and out_step[k * n_clocks + c] = step. Other slots
+   are left as they are. Clocks with t_obs = 0 record nothing. */
+int dclaw_obs_record(const dclaw_clock* clocks, int n_clocks, const int32_t* member, const double* q,
+                     const int64_t* select, int64_t n_select, int n_obs, int step, double* out,
+                     int32_t* out_step, void* stream);
 /* max over cells of |u|+sqrt(g h) (interior layout) written to *smax (device double) */
 int dclaw_max_wave_speed(const double* q, int mx, int my, const dclaw_params* p, double* smax,
                          void* stream);

@@ -243,12 +243,69 @@ def test_rollout_with_observation_interval(cuda_device):
     with torch.no_grad():
         L2, _ = _run_loss(torch.tensor(qn, device=dev), theta_of(p, dev), b, p, 1.0, n, outs, wts, dt0=0.0,
                           dt_schedule=sched)
-    assert float(L2) == float(L)
+    assert float(L2) == float(L.detach())
     q1 = torch.tensor(qn, device=dev, requires_grad=True)
     th1 = theta_of(p, dev).requires_grad_(True)
     L3, _ = _run_loss(q1, th1, b, p, 1.0, n, outs, wts, dt0=0.0, dt_schedule=sched)
     L3.backward()
     assert torch.equal(q1.grad, q0.grad) and torch.equal(th1.grad, theta.grad)
+
+
+def test_rollout_observations(cuda_device):
+    """rollout_observations records slot k when t lands on (k+1) obs_dt (the
+    port's flume loop): the slots equal the fused step's states at those
+    steps, slots past the run stay 0, and the gradient of a loss over the
+    slots matches finite differences at the recorded dt schedule (which
+    replays the same landings)."""
+    from dclaw_b200.adjoint import observation_steps, rollout_observations
+    from dclaw_b200.solver import PatchStepper
+
+    dev = cuda_device
+    p, qn, bn = _small_flow(seed=6)
+    p = p.replace(cfl_desired=0.4)
+    b = torch.tensor(bn, device=dev)
+    n, obs_dt, n_obs = 30, 0.05, 40
+    rng = np.random.default_rng(9)
+    sel = torch.tensor(rng.choice(qn.size, 40, replace=False), device=dev)
+    wts = torch.tensor(rng.standard_normal((n_obs, 40)), device=dev)
+    q0 = torch.tensor(qn, device=dev, requires_grad=True)
+    theta = theta_of(p, dev).requires_grad_(True)
+    o = rollout_observations(q0, theta, b, p, 1.0, 1.0, n, obs_dt, n_obs, 0.02, select=sel)
+    steps = observation_steps(o)
+    sched = last_dts(o).clone()
+    L = (o * wts).sum()
+    L.backward()
+    # the slots against stepping one step at a time with the same clock
+    st = PatchStepper(torch.tensor(qn, device=dev), b, p, 1.0, 1.0)
+    st.init_clock(0.02, t_obs=obs_dt)
+    got = {}
+    for k in range(n):
+        st.step(1)
+        c = st.read_clock()
+        j = int(np.rint(c.t / obs_dt)) - 1
+        if c.dt_last > 0 and 0 <= j < n_obs and abs(c.t - (j + 1) * obs_dt) < 1e-9:
+            got[j] = (k + 1, st.state().reshape(-1)[sel].clone())
+    assert len(got) >= 4 and any(s < 0 for s in steps)
+    for j in range(n_obs):
+        if j in got:
+            assert steps[j] == got[j][0] and torch.equal(o.detach()[j], got[j][1])
+        else:
+            assert steps[j] == -1 and not o.detach()[j].any()
+
+    def Lf(qq, th):
+        with torch.no_grad():
+            oo = rollout_observations(qq, th, b, p, 1.0, 1.0, n, obs_dt, n_obs, 0.0, select=sel, dt_schedule=sched)
+            return float((oo * wts).sum())
+
+    assert Lf(q0.detach(), theta.detach()) == float(L.detach())
+    d = rng.standard_normal(qn.shape) * (np.abs(qn) + 1e-3)
+    d[:, qn[0] <= 10 * p.dry_tolerance] = 0.0
+    d = torch.tensor(d, device=dev)
+    q00, th0 = q0.detach(), theta.detach()
+    _close(float((q0.grad * d).sum()), _fd(lambda e: Lf(q00 + e * d, th0)), "state")
+    e0 = torch.zeros(4, dtype=torch.float64, device=dev)
+    e0[0] = 1.0
+    _close(float(theta.grad[0]), _fd(lambda h: Lf(q00, th0 + h * e0), eps0=4e-6), "phi")
 
 
 def test_checkpoint_block_gives_identical_gradients(cuda_device):

@@ -13,7 +13,8 @@ import pytest
 import torch
 
 from dclaw_b200 import workloads as W
-from dclaw_b200.adjoint import (EnsembleStepAdjoint, StepAdjoint, ensemble_rollout_states, rollout_states,
+from dclaw_b200.adjoint import (EnsembleStepAdjoint, StepAdjoint, ensemble_rollout_observations,
+                                ensemble_rollout_states, observation_steps, rollout_observations, rollout_states,
                                 theta_of)
 from dclaw_b200.ensemble import EnsembleStepper, Member
 
@@ -134,3 +135,40 @@ def test_ensemble_select_outputs(cuda_device):
         res.append((o.detach(), q0.grad.clone(), theta.grad.clone()))
     for a, b in zip(res[0], res[1]):
         assert torch.equal(a, b)
+
+
+def test_ensemble_observations_match_single_patch(cuda_device):
+    """Per-member observation intervals: each member's gauge entries land in
+    its own slots at its own steps, bit for bit as rollout_observations on
+    the member alone, with the same state gradients and parameter gradients
+    to 1e-12."""
+    import dataclasses
+
+    dev = cuda_device
+    members = [dataclasses.replace(m, t_obs=to) for m, to in
+               zip(_advance(_members(seed=4), dev, n=6), [0.01, 0.02, 0.015, 0.03, 0.01])]
+    ens = EnsembleStepper(members, dev)
+    rng = np.random.default_rng(12)
+    n, n_obs, per = 24, 8, 6
+    picks = [rng.choice(m.q.size, per, replace=False) for m in members]
+    sel = torch.tensor(np.concatenate([ens.cm[k].q_off + picks[k] for k in range(len(members))]), device=dev)
+    wts = torch.tensor(rng.standard_normal((n_obs, sel.numel())), device=dev)
+    q0 = ens.qa.clone().requires_grad_(True)
+    theta = torch.stack([theta_of(m.params, dev) for m in members]).requires_grad_(True)
+    o = ensemble_rollout_observations(q0, theta, members, n, n_obs, sel, checkpoint_block=5)
+    steps = observation_steps(o)
+    (o * wts).sum().backward()
+    assert any(s >= 0 for row in steps for s in row)
+    for k, m in enumerate(members):
+        cols = slice(k * per, (k + 1) * per)
+        qk = torch.tensor(m.q, device=dev, requires_grad=True)
+        tk = theta_of(m.params, dev).requires_grad_(True)
+        sk = torch.tensor(picks[k], device=dev)
+        ok = rollout_observations(qk, tk, torch.tensor(m.b, device=dev), m.params, m.dx, m.dy, n, m.t_obs, n_obs,
+                                  m.dt_initial, select=sk, checkpoint_block=3)
+        assert [row[k] for row in steps] == observation_steps(ok), f"member {k}: steps"
+        assert torch.equal(o.detach()[:, cols], ok.detach()), f"member {k}: observations"
+        (ok * wts[:, cols]).sum().backward()
+        off, c = ens.cm[k].q_off, m.q.size
+        assert torch.equal(q0.grad[off:off + c].view(m.q.shape), qk.grad), f"member {k}: state gradient"
+        _close_params(theta.grad[k], tk.grad, f"member {k}: parameter gradient")

@@ -51,6 +51,23 @@ def test_host_side_helpers():
     assert lib.dclaw_error_string(3) == b"NaN in the state"
 
 
+def test_observation_record_argument_checks():
+    """dclaw_obs_record refuses bad arguments before any device work."""
+    lib = _lib.load()
+    fake = ctypes.c_void_p(256)   # never dereferenced: every call below fails its checks
+    null = ctypes.c_void_p(0)
+    args = dict(clocks=fake, n=1, member=null, q=fake, sel=null, nsel=10, n_obs=4, step=1, out=fake, ostep=fake)
+
+    def call(**kw):
+        a = dict(args, **kw)
+        return lib.dclaw_obs_record(a["clocks"], a["n"], a["member"], a["q"], a["sel"], a["nsel"], a["n_obs"],
+                                    a["step"], a["out"], a["ostep"], null)
+
+    for bad in (dict(clocks=null), dict(n=0), dict(q=null), dict(nsel=0), dict(n_obs=0), dict(out=null),
+                dict(ostep=null), dict(n=3)):      # several clocks need a member map
+        assert call(**bad) == 1, bad
+
+
 def test_ctypes_struct_matches_header_size():
     # dclaw_params: 8 doubles + 2 int32 + ... checked by field offsets of the ctypes image
     assert ctypes.sizeof(CParams) % 8 == 0
