@@ -849,6 +849,23 @@ __global__ void __launch_bounds__(TPB) k_src2_padded(dclaw_params P, int mx, int
     q[pc] = a; q[npad + pc] = b; q[2 * npad + pc] = c; q[3 * npad + pc] = d; q[4 * npad + pc] = e;
 }
 
+// Fortran cell-major arrays (nfa fields per cell) <-> field planes: one
+// thread per cell; a warp's reads cover its cells' contiguous records, its
+// writes are contiguous within each plane
+__global__ void __launch_bounds__(TPB) k_fields_soa(const double* __restrict__ a, int nfa, int nf, long long ncell,
+                                                    double* __restrict__ planes) {
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell;
+         c += (long long)gridDim.x * blockDim.x)
+        for (int f = 0; f < nf; ++f) planes[(long long)f * ncell + c] = a[c * nfa + f];
+}
+
+__global__ void __launch_bounds__(TPB) k_fields_aos(const double* __restrict__ planes, int nf, int nfa, long long ncell,
+                                                    double* __restrict__ a) {
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell;
+         c += (long long)gridDim.x * blockDim.x)
+        for (int f = 0; f < nf; ++f) a[c * nfa + f] = planes[(long long)f * ncell + c];
+}
+
 // observation slot of clock c after its step, or -1: the flume loop's
 // k = round(t / dt_obs) - 1 (round half to even) and its hit test
 // |t - (k+1) dt_obs| < 1e-9 with dt > 0 (pf_flume/flume_model.py:155-157)
@@ -1361,6 +1378,26 @@ int dclaw_obs_record(const dclaw_clock* clocks, int n_clocks, const int32_t* mem
     if (nb > 4096) nb = 4096;
     k_obs_record<<<(unsigned)nb, TPB, 0, (cudaStream_t)stream>>>(clocks, n_clocks, member, q, select,
                                                                  (long long)n_select, n_obs, step, out, out_step);
+    return cuda_status();
+}
+
+int dclaw_fields_from_fortran(const double* fortran, int nf_fortran, int nf, int mx, int my, int mbc,
+                              double* planes, void* stream) {
+    if (!fortran || !planes || nf < 1 || nf > nf_fortran || mx < 1 || my < 1 || mbc < 0) return DCLAW_ERR_ARG;
+    const long long ncell = (long long)(mx + 2 * mbc) * (my + 2 * mbc);
+    long long nb = (ncell + TPB - 1) / TPB;
+    if (nb > 65535) nb = 65535;
+    k_fields_soa<<<(unsigned)nb, TPB, 0, (cudaStream_t)stream>>>(fortran, nf_fortran, nf, ncell, planes);
+    return cuda_status();
+}
+
+int dclaw_fields_to_fortran(const double* planes, int nf, int nf_fortran, int mx, int my, int mbc,
+                            double* fortran, void* stream) {
+    if (!fortran || !planes || nf < 1 || nf > nf_fortran || mx < 1 || my < 1 || mbc < 0) return DCLAW_ERR_ARG;
+    const long long ncell = (long long)(mx + 2 * mbc) * (my + 2 * mbc);
+    long long nb = (ncell + TPB - 1) / TPB;
+    if (nb > 65535) nb = 65535;
+    k_fields_aos<<<(unsigned)nb, TPB, 0, (cudaStream_t)stream>>>(planes, nf, nf_fortran, ncell, fortran);
     return cuda_status();
 }
 

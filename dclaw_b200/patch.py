@@ -77,5 +77,30 @@ class Patch:
         _lib.check(self.lib.dclaw_src2(_lib.ptr(q), _lib.ptr(aux), self.mx, self.my, MBC, dx, dy, t, dt,
                                        ctypes.byref(self.cp), _lib.stream_ptr()), "src2")
 
+    def from_fortran(self, a: torch.Tensor, nf: int) -> torch.Tensor:
+        """The first nf fields of a Fortran patch array a(nf_fortran,
+        1-mbc:mx+mbc, 1-mbc:my+mbc) -- here a contiguous float64 CUDA tensor
+        of shape (my+4, mx+4, nf_fortran), the same memory -- as the padded
+        (nf, my+4, mx+4) planes the patch calls take (q: nf 5 of meqn 7;
+        aux: nf 6 of maux)."""
+        my, mx = self.my + 2 * MBC, self.mx + 2 * MBC
+        if a.dim() != 3 or tuple(a.shape[:2]) != (my, mx) or not a.is_contiguous() or a.dtype != torch.float64:
+            raise _lib.DClawError("a must be a contiguous float64 (my+4, mx+4, nf_fortran) tensor")
+        out = torch.empty((nf, my, mx), dtype=torch.float64, device=a.device)
+        _lib.check(self.lib.dclaw_fields_from_fortran(_lib.ptr(a), int(a.shape[2]), int(nf), self.mx, self.my, MBC,
+                                                      _lib.ptr(out), _lib.stream_ptr()), "fields from Fortran layout")
+        return out
+
+    def to_fortran(self, planes: torch.Tensor, a: torch.Tensor) -> None:
+        """Write the padded planes back into fields 1..nf of the Fortran patch
+        array a (shape (my+4, mx+4, nf_fortran)); its other fields are kept."""
+        nf = int(planes.shape[0])
+        self._shape_check(planes, nf, "planes")
+        my, mx = self.my + 2 * MBC, self.mx + 2 * MBC
+        if a.dim() != 3 or tuple(a.shape[:2]) != (my, mx) or not a.is_contiguous() or a.dtype != torch.float64:
+            raise _lib.DClawError("a must be a contiguous float64 (my+4, mx+4, nf_fortran) tensor")
+        _lib.check(self.lib.dclaw_fields_to_fortran(_lib.ptr(planes), nf, int(a.shape[2]), self.mx, self.my, MBC,
+                                                    _lib.ptr(a), _lib.stream_ptr()), "fields to Fortran layout")
+
     def status(self) -> int:
         return CClock.from_buffer_copy(self.clock.cpu().numpy().tobytes()).status

@@ -412,6 +412,19 @@ int dclaw_clock_set_obs(dclaw_clock* clock, double t_obs, void* stream);
 int dclaw_obs_record(const dclaw_clock* clocks, int n_clocks, const int32_t* member, const double* q,
                      const int64_t* select, int64_t n_select, int n_obs, int step, double* out,
                      int32_t* out_step, void* stream);
+/* Fortran-layout adapters for the patch calls. A Fortran patch array
+   a(nf_fortran, 1-mbc:mx+mbc, 1-mbc:my+mbc) (field fastest; D-Claw's
+   q(meqn=7, ...) and aux(maux, ...), digclaw_module.f90:96-110) and the patch
+   calls' padded structure-of-arrays form (nf planes of (my+2mbc)(mx+2mbc), x
+   fastest) hold the same cells. from_fortran copies fields 1..nf of each cell
+   into the planes; to_fortran copies the planes back into fields 1..nf and
+   leaves fields nf+1..nf_fortran as they are (for q: hchi and bdif, which stay
+   zero without segregation and entrainment). Device pointers;
+   nf <= nf_fortran. */
+int dclaw_fields_from_fortran(const double* fortran, int nf_fortran, int nf, int mx, int my, int mbc,
+                              double* planes, void* stream);
+int dclaw_fields_to_fortran(const double* planes, int nf, int nf_fortran, int mx, int my, int mbc,
+                            double* fortran, void* stream);
 /* max over cells of |u|+sqrt(g h) (interior layout) written to *smax (device double) */
 int dclaw_max_wave_speed(const double* q, int mx, int my, const dclaw_params* p, double* smax,
                          void* stream);

@@ -223,6 +223,49 @@ def test_patch_calls(cuda_device, oracle):
     assert P.status() == 0
 
 
+def test_fortran_layout_adapters(cuda_device, oracle):
+    """q(meqn=7, ...) and aux(maux=10, ...) in Fortran cell-major order into
+    the patch calls' planes and back: the fields match, the extra fields
+    are kept, and a b4step2 + step2 + src2 pass through the adapters gives
+    the oracle's state."""
+    from dclaw_b200.patch import Patch
+
+    c = W.slope_runout(n=48)
+    mx, my = c.mx, c.my
+    dev = cuda_device
+    rng = np.random.default_rng(3)
+    r = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 10, c.dt_initial, libm="portable")
+    qpad = np.zeros((5, my + 4, mx + 4))
+    qpad[:, 2:-2, 2:-2] = r["q"]
+    qf = np.zeros((my + 4, mx + 4, 7))
+    qf[..., :5] = np.moveaxis(qpad, 0, -1)
+    qf[..., 5:] = rng.standard_normal((my + 4, mx + 4, 2))
+    P = Patch(c.params, mx, my)
+    qf_d = torch.tensor(qf, device=dev)
+    planes = P.from_fortran(qf_d, 5)
+    assert torch.equal(planes.cpu(), torch.tensor(qpad))
+    auxf = torch.tensor(rng.standard_normal((my + 4, mx + 4, 10)), device=dev)
+    aux_planes = P.from_fortran(auxf, 6)
+    assert torch.equal(aux_planes, auxf[..., :6].permute(2, 0, 1))
+    # a patch step through the adapters against the oracle's patch calls
+    aux = torch.zeros((6, my + 4, mx + 4), dtype=torch.float64, device=dev)
+    aux[0, 2:-2, 2:-2] = torch.tensor(c.b, device=dev)
+    P.setaux(aux)
+    P.bc2amr(planes)
+    P.b4step2(planes, aux, c.dx, c.dy)
+    P.step2(planes, aux, c.dx, c.dy, 0.01)
+    P.src2(planes, aux, c.dx, c.dy, 0.0, 0.01)
+    P.to_fortran(planes, qf_d)
+    back = qf_d.cpu().numpy()
+    assert np.array_equal(back[..., 5:], qf[..., 5:])
+    assert np.array_equal(np.moveaxis(back[..., :5], -1, 0), planes.cpu().numpy())
+    aux_o = oracle.setaux(c.params, c.b)
+    qo, aux_o = oracle.b4step2(c.params, oracle.bc2amr(c.params, qpad), aux_o, c.dx, c.dy, libm="portable")
+    qo = oracle.step2(c.params, qo, aux_o, c.dx, c.dy, 0.01, libm="portable")["q"]
+    qo = oracle.src2(c.params, qo, aux_o, 0.01, libm="portable")
+    assert np.array_equal(planes.cpu().numpy()[:, 2:-2, 2:-2], qo[:, 2:-2, 2:-2])
+
+
 def test_graph_replay_matches_eager(cuda_device):
     from dclaw_b200.solver import PatchStepper
 

@@ -68,6 +68,19 @@ def test_observation_record_argument_checks():
         assert call(**bad) == 1, bad
 
 
+def test_fortran_adapter_argument_checks():
+    lib = _lib.load()
+    fake, null = ctypes.c_void_p(256), ctypes.c_void_p(0)
+    for fn in (lib.dclaw_fields_from_fortran, lib.dclaw_fields_to_fortran):
+        for a, nfa, nf, mx, my, mbc, b in ((null, 7, 5, 8, 8, 2, fake), (fake, 7, 5, 8, 8, 2, null),
+                                            (fake, 4, 5, 8, 8, 2, fake), (fake, 7, 0, 8, 8, 2, fake),
+                                            (fake, 7, 5, 0, 8, 2, fake), (fake, 7, 5, 8, 8, -1, fake)):
+            if fn is lib.dclaw_fields_to_fortran:
+                assert fn(b, nf, nfa, mx, my, mbc, a, null) == 1
+            else:
+                assert fn(a, nfa, nf, mx, my, mbc, b, null) == 1
+
+
 def test_ctypes_struct_matches_header_size():
     # dclaw_params: 8 doubles + 2 int32 + ... checked by field offsets of the ctypes image
     assert ctypes.sizeof(CParams) % 8 == 0
