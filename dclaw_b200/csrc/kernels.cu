@@ -45,9 +45,19 @@ constexpr int TILE_X = DCLAW_TILE_X, TILE_Y = DCLAW_TILE_Y;
 #ifndef DCLAW_SCAN_MINB
 #define DCLAW_SCAN_MINB 4
 #endif
-// resident blocks per SM the per-cell kernels (records, src2) are sized for
+// resident blocks per SM the ensemble's per-cell kernels (records of the
+// listed tiles, src2) are sized for
 #ifndef DCLAW_CELL_MINB
 #define DCLAW_CELL_MINB 4
+#endif
+// resident blocks per SM the single-patch per-cell kernels (k_records,
+// k_src2_cells) are sized for: on the 4096^2 random field 6 (40 registers,
+// with spills) steps 1.9 % faster than 4 (64 registers), 5 1.2 % and 8
+// (32 registers) 0.8 %; 3 and 2 (80 and 110 registers, no spills) 4 % and
+// 10 % slower. The ensemble's per-cell kernels are fastest at 4 (6 is 5 %
+// slower there).
+#ifndef DCLAW_PLAIN_CELL_MINB
+#define DCLAW_PLAIN_CELL_MINB 6
 #endif
 
 __device__ __forceinline__ double warp_max(double v) {
@@ -300,7 +310,7 @@ __global__ void k_clock_set_obs(dclaw_clock* clk, double t_obs) {
 // Records of every padded cell, and the marks. prow0 / nprow: the padded
 // rows (0 .. my+3 for j = -1 .. my+2) this launch covers, all of them by
 // default.
-__global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_records(dclaw_params P, Geom g, const double* __restrict__ q_in,
+__global__ void __launch_bounds__(TPB, DCLAW_PLAIN_CELL_MINB) k_records(dclaw_params P, Geom g, const double* __restrict__ q_in,
                                                  const double* __restrict__ b, Rec R, dclaw_clock* clk,
                                                  uint32_t* __restrict__ tflag, int prow0 = 0, int nprow = -1) {
     const long long n = (long long)g.PX * (nprow < 0 ? g.PY : nprow);
@@ -475,7 +485,7 @@ __global__ void __launch_bounds__(TILE_TPB, DCLAW_TILE_MINBLOCKS) k_tile(dclaw_p
 
 // src2 of the interior cells c0 .. c0 + ncell - 1 (all by default) from the
 // updated state; with `tick` the last block applies the tick rule
-__global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_src2_cells(dclaw_params P, Geom g, const double* __restrict__ q_star,
+__global__ void __launch_bounds__(TPB, DCLAW_PLAIN_CELL_MINB) k_src2_cells(dclaw_params P, Geom g, const double* __restrict__ q_star,
                                                     double* __restrict__ q_out, dclaw_clock* clk,
                                                     const uint32_t* __restrict__ tflag, long long c0 = 0,
                                                     long long ncell = -1, int tick = 1) {
