@@ -646,7 +646,8 @@ def run_ours(args):
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                "config": {"workload": f"random_field_{case.mx}x{case.my}_dx{case.dx}",
                           "cells_per_gpu": cells, "parallelism": f"replicas{world}",
-                          "l2": "state 672 MB > L2, no flush", "order": case.params.order,
+                          "l2": f"state {40 * cells / 1e6:.0f} MB {'>' if 40 * cells > 126e6 else '<'} L2 (126 MB),"
+                                f" no flush", "order": case.params.order,
                           "transverse_waves": case.params.transverse_waves, "limiter": "MC"},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": NCU_STEP_BYTES_2048 * cells / 2048 ** 2,
