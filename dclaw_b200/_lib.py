@@ -36,6 +36,8 @@ SIGNATURES = {
     "dclaw_clock_init": (_int, [_vp, _dbl, _dbl, _dbl, _int, _vp]),
     "dclaw_clock_set_obs": (_int, [_vp, _dbl, _vp]),
     "dclaw_obs_record": (_int, [_vp, _int, _vp, _vp, _vp, ctypes.c_int64, _int, _int, _vp, _vp, _vp]),
+    "dclaw_peak_update": (_int, [_vp, _vp, _vp, ctypes.c_int64, _int, _vp]),
+    "dclaw_peak_adjoint": (_int, [_vp, _vp, ctypes.c_int64, _int, _vp, _vp]),
     "dclaw_fields_from_fortran": (_int, [_vp, _int, _int, _int, _int, _int, _vp, _vp]),
     "dclaw_fields_to_fortran": (_int, [_vp, _int, _int, _int, _int, _int, _vp, _vp]),
     "dclaw_max_wave_speed": (_int, [_vp, _int, _int, _pp, _vp, _vp]),

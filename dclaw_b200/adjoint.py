@@ -205,7 +205,7 @@ def _block(n_steps: int, checkpoint_block: int | None, state_bytes: int = 0, res
 class _Rollout(torch.autograd.Function):
     @staticmethod
     def forward(ctx, q0, theta, b, params, dx, dy, n_steps, out_steps, dt0, fixed_dt, t_final, checkpoint_block,
-                dt_schedule, select, obs_dt, n_obs):
+                dt_schedule, select, obs_dt, n_obs, peak):
         prm = with_theta(params, theta.detach().cpu())
         # a moving bed: a function of the simulated time, evaluated before
         # every step (the port's step(q, bed(t), ...) loop)
@@ -225,7 +225,12 @@ class _Rollout(torch.autograd.Function):
         dts = torch.empty(n_steps, dtype=torch.float64, device=q0.device)
         t_start = torch.empty(n_steps if bed_fn is not None else 0, dtype=torch.float64, device=q0.device)
         oshape = tuple(q0.shape) if select is None else tuple(select.shape)
-        if n_obs:
+        plane = q0.shape[1] * q0.shape[2]
+        if peak:
+            # running peak depth from q0's, and the step that set it
+            outs = q0.detach()[0].clone()
+            argstep = torch.zeros(outs.shape, dtype=torch.int32, device=q0.device)
+        elif n_obs:
             # observation slots: filled on the device when the clock lands
             # on an observation time; slots the run does not reach stay 0
             outs = torch.zeros((n_obs,) + oshape, dtype=q0.dtype, device=q0.device)
@@ -262,6 +267,9 @@ class _Rollout(torch.autograd.Function):
             dts[n:n + 1].copy_(st.clock[3:4])   # dt the step used
             for idx in where.get(n + 1, []):
                 outs[idx].copy_(pick(src))
+            if peak:
+                _lib.check(lib.dclaw_peak_update(_lib.ptr(src), _lib.ptr(outs), _lib.ptr(argstep), plane, n + 1,
+                                                 _lib.stream_ptr()), "peak update")
             if n_obs:
                 _lib.check(lib.dclaw_obs_record(_lib.ptr(st.clock), 1, None, _lib.ptr(src), _lib.ptr(sel64), nsel,
                                                 n_obs, n + 1, _lib.ptr(outs), _lib.ptr(obs_step),
@@ -279,6 +287,7 @@ class _Rollout(torch.autograd.Function):
         ctx.select = select
         ctx.meta = (prm, float(dx), float(dy), int(n_steps), tuple(out_steps), k)
         ctx.obs_steps = tuple(out_steps) if n_obs else None
+        ctx.peak_arg = argstep if peak else None
         return outs
 
     @staticmethod
@@ -324,24 +333,30 @@ class _Rollout(torch.autograd.Function):
                 fw._launch(src, buf[n - n0])
                 src = buf[n - n0]
 
+        peak_arg = ctx.peak_arg
+        lib = _lib.load()
+
         def add_outs(n, target):
-            if g_out is not None:
-                for idx in where.get(n, []):
-                    add_out(idx, target)
+            if g_out is None:
+                return
+            for idx in where.get(n, []):
+                add_out(idx, target)
+            if peak_arg is not None:
+                _lib.check(lib.dclaw_peak_adjoint(_lib.ptr(g_out), _lib.ptr(peak_arg), peak_arg.numel(), n,
+                                                  _lib.ptr(target), _lib.stream_ptr()), "peak adjoint")
 
         def bed_for(n, adj):
             adj.b.copy_(bed_fn(t_start[n - 1]))
 
         lam, lam2 = _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, lambda n: dts[n - 1:n], lam,
                                         lam2, pbar, add_outs, bed_for if bed_fn is not None else None)
-        if g_out is not None:
-            for idx in where.get(0, []):
-                add_out(idx, lam)
+        add_outs(0, lam)
         _lib.check(fw.status(), "rollout recompute")
         for adj in adjs:
             adj.check_status()
         scale = torch.tensor([_DEG, 1.0, 1.0, 1.0], dtype=torch.float64, device=dev)
-        return lam, pbar * scale, None, None, None, None, None, None, None, None, None, None, None, None, None, None
+        return (lam, pbar * scale, None, None, None, None, None, None, None, None, None, None, None, None, None, None,
+                None)
 
 
 def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams, dx: float,
@@ -384,7 +399,7 @@ def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams
     return _Rollout.apply(q0, theta, b if callable(b) else b.contiguous(), params, dx, dy, int(n_steps),
                           tuple(int(n) for n in out_steps),
                           float(dt0), bool(fixed_dt), float(t_final), checkpoint_block, dt_schedule, select,
-                          float(obs_dt), 0)
+                          float(obs_dt), 0, False)
 
 
 def rollout_observations(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams, dx: float, dy: float,
@@ -409,7 +424,26 @@ def rollout_observations(q0: torch.Tensor, theta: torch.Tensor, b, params: DClaw
         dt_schedule = dt_schedule.contiguous()
     return _Rollout.apply(q0, theta, b if callable(b) else b.contiguous(), params, dx, dy, int(n_steps), (),
                           float(dt0), False, float(t_end), checkpoint_block, dt_schedule, select, float(obs_dt),
-                          int(n_obs))
+                          int(n_obs), False)
+
+
+def rollout_peak(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams, dx: float, dy: float,
+                 n_steps: int, dt0: float, t_final: float = 0.0, fixed_dt: bool = False,
+                 checkpoint_block: int | None = None, dt_schedule: torch.Tensor | None = None) -> torch.Tensor:
+    """Differentiable running peak depth over n_steps steps, the loss input
+    of the port's rollout_peak (differentiable_dclaw/dclaw_jax/solver.py:
+    357-388, differentiated by jax.grad): max over q0 and every step's state
+    of h, per cell, shape (my, mx). Its gradient reaches q0 and theta
+    through the step that set each cell's peak (ties: the earliest step).
+    The other arguments are those of `rollout_states` (the bed is not
+    differentiated)."""
+    if dt_schedule is not None:
+        if dt_schedule.shape != (n_steps,) or dt_schedule.dtype != torch.float64 or not dt_schedule.is_cuda:
+            raise ValueError("dt_schedule must be a (n_steps,) float64 CUDA tensor")
+        dt_schedule = dt_schedule.contiguous()
+    return _Rollout.apply(q0, theta, b if callable(b) else b.contiguous(), params, dx, dy, int(n_steps), (),
+                          float(dt0), bool(fixed_dt), float(t_final), checkpoint_block, dt_schedule, None, 0.0, 0,
+                          True)
 
 
 def observation_steps(out: torch.Tensor) -> list:
@@ -452,7 +486,7 @@ def initial_state(h0: torch.Tensor, m0: torch.Tensor, params: DClawParams, p_rat
     return torch.where(wet.unsqueeze(0), q, torch.zeros_like(q))
 
 
-__all__ = ["StepAdjoint", "rollout_states", "rollout_observations", "observation_steps", "theta_of", "with_theta", "initial_state", "last_dts", "THETA_NAMES",
+__all__ = ["StepAdjoint", "rollout_states", "rollout_observations", "observation_steps", "rollout_peak", "theta_of", "with_theta", "initial_state", "last_dts", "THETA_NAMES",
            "EnsembleStepAdjoint", "ensemble_rollout_states", "ensemble_rollout_observations", "ensemble_last_dts"]
 
 

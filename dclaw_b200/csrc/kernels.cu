@@ -868,6 +868,25 @@ __global__ void __launch_bounds__(TPB) k_src2_padded(dclaw_params P, int mx, int
     q[pc] = a; q[npad + pc] = b; q[2 * npad + pc] = c; q[3 * npad + pc] = d; q[4 * npad + pc] = e;
 }
 
+// running peak of a plane and the step that set it; the adjoint adds the
+// peak's adjoint at that step
+__global__ void __launch_bounds__(TPB) k_peak_update(const double* __restrict__ h, double* __restrict__ hmax,
+                                                     int32_t* __restrict__ arg, long long n, int step) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double v = h[i];
+        if (v > hmax[i]) {
+            hmax[i] = v;
+            arg[i] = step;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(TPB) k_peak_adjoint(const double* __restrict__ g, const int32_t* __restrict__ arg,
+                                                      long long n, int step, double* __restrict__ lam) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (arg[i] == step) lam[i] += g[i];
+}
+
 // Fortran cell-major arrays (nfa fields per cell) <-> field planes: one
 // thread per cell; a warp's reads cover its cells' contiguous records, its
 // writes are contiguous within each plane
@@ -1398,6 +1417,23 @@ int dclaw_obs_record(const dclaw_clock* clocks, int n_clocks, const int32_t* mem
     if (nb > 4096) nb = 4096;
     k_obs_record<<<(unsigned)nb, TPB, 0, (cudaStream_t)stream>>>(clocks, n_clocks, member, q, select,
                                                                  (long long)n_select, n_obs, step, out, out_step);
+    return cuda_status();
+}
+
+int dclaw_peak_update(const double* h, double* hmax, int32_t* argstep, int64_t n, int step, void* stream) {
+    if (!h || !hmax || !argstep || n <= 0) return DCLAW_ERR_ARG;
+    long long nb = ((long long)n + TPB - 1) / TPB;
+    if (nb > 65535) nb = 65535;
+    k_peak_update<<<(unsigned)nb, TPB, 0, (cudaStream_t)stream>>>(h, hmax, argstep, (long long)n, step);
+    return cuda_status();
+}
+
+int dclaw_peak_adjoint(const double* g, const int32_t* argstep, int64_t n, int step, double* lam_h,
+                       void* stream) {
+    if (!g || !argstep || !lam_h || n <= 0) return DCLAW_ERR_ARG;
+    long long nb = ((long long)n + TPB - 1) / TPB;
+    if (nb > 65535) nb = 65535;
+    k_peak_adjoint<<<(unsigned)nb, TPB, 0, (cudaStream_t)stream>>>(g, argstep, (long long)n, step, lam_h);
     return cuda_status();
 }
 

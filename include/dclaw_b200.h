@@ -412,6 +412,14 @@ int dclaw_clock_set_obs(dclaw_clock* clock, double t_obs, void* stream);
 int dclaw_obs_record(const dclaw_clock* clocks, int n_clocks, const int32_t* member, const double* q,
                      const int64_t* select, int64_t n_select, int n_obs, int step, double* out,
                      int32_t* out_step, void* stream);
+/* Running peak of a plane for the differentiable peak-depth run (the port's
+   rollout_peak, differentiable_dclaw/dclaw_jax/solver.py:357-388): where
+   h[i] > hmax[i], hmax[i] = h[i] and argstep[i] = step. peak_adjoint adds
+   g[i] to lam_h[i] where argstep[i] == step (the gradient of a maximum goes
+   to the step that set it; ties to the earliest). n entries, device pointers. */
+int dclaw_peak_update(const double* h, double* hmax, int32_t* argstep, int64_t n, int step, void* stream);
+int dclaw_peak_adjoint(const double* g, const int32_t* argstep, int64_t n, int step, double* lam_h,
+                       void* stream);
 /* Fortran-layout adapters for the patch calls. A Fortran patch array
    a(nf_fortran, 1-mbc:mx+mbc, 1-mbc:my+mbc) (field fastest; D-Claw's
    q(meqn=7, ...) and aux(maux, ...), digclaw_module.f90:96-110) and the patch

@@ -308,6 +308,53 @@ def test_rollout_observations(cuda_device):
     _close(float(theta.grad[0]), _fd(lambda h: Lf(q00, th0 + h * e0), eps0=4e-6), "phi")
 
 
+def test_rollout_peak_gradient(cuda_device):
+    """adjoint.rollout_peak, the loss input of the port's rollout_peak: the
+    running peak depth equals the maximum over stepped states, bit for bit,
+    with every state kept and with checkpoint blocks. Its gradient is the
+    gradient of the same loss over rollout_states outputs with each cell's
+    term taken at the step that set its peak (rollout_states' gradients are
+    checked against finite differences above; finite differences of a
+    maximum straddle its kinks wherever two steps nearly tie)."""
+    from dclaw_b200.adjoint import rollout_peak
+    from dclaw_b200.solver import PatchStepper
+
+    dev = cuda_device
+    p, qn, bn = _small_flow(seed=8)
+    b = torch.tensor(bn, device=dev)
+    n = 16
+    rng = np.random.default_rng(21)
+    w = torch.tensor(rng.standard_normal(qn.shape[1:]), device=dev)
+    res = []
+    for blk in (1, 4):
+        q0 = torch.tensor(qn, device=dev, requires_grad=True)
+        theta = theta_of(p, dev).requires_grad_(True)
+        hp = rollout_peak(q0, theta, b, p, 1.0, 1.0, n, 0.02, fixed_dt=True, checkpoint_block=blk)
+        (hp * w).sum().backward()
+        res.append((hp.detach(), q0.grad.clone(), theta.grad.clone()))
+    assert all(torch.equal(x, y) for x, y in zip(res[0], res[1])), "checkpoint blocks differ"
+    hp, gq, gt = res[0]
+    st = PatchStepper(torch.tensor(qn, device=dev), b, p, 1.0, 1.0)
+    st.init_clock(0.02, fixed_dt=True)
+    ref = torch.tensor(qn[0], device=dev)
+    arg = torch.zeros(ref.shape, dtype=torch.int64, device=dev)
+    for k in range(n):
+        st.step(1)
+        h = st.state()[0]
+        arg = torch.where(h > ref, torch.full_like(arg, k + 1), arg)
+        ref = torch.maximum(ref, h)
+    assert torch.equal(hp, ref)
+    assert len(torch.unique(arg)) > 3
+    # the same loss with each cell's term at the step that set its peak
+    q1 = torch.tensor(qn, device=dev, requires_grad=True)
+    th1 = theta_of(p, dev).requires_grad_(True)
+    o = rollout_states(q1, th1, b, p, 1.0, 1.0, n, list(range(n + 1)), 0.02, fixed_dt=True)
+    mask = (arg.unsqueeze(0) == torch.arange(n + 1, device=dev).view(-1, 1, 1)).to(torch.float64)
+    (o[:, 0] * mask * w).sum().backward()
+    assert torch.allclose(gq, q1.grad, rtol=1e-12, atol=1e-300)
+    assert torch.allclose(gt, th1.grad, rtol=1e-12, atol=0.0)
+
+
 def test_checkpoint_block_gives_identical_gradients(cuda_device):
     dev = cuda_device
     p, qn, bn = _small_flow(seed=2)

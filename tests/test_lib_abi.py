@@ -68,6 +68,15 @@ def test_observation_record_argument_checks():
         assert call(**bad) == 1, bad
 
 
+def test_peak_argument_checks():
+    lib = _lib.load()
+    fake, null = ctypes.c_void_p(256), ctypes.c_void_p(0)
+    assert lib.dclaw_peak_update(null, fake, fake, 10, 1, null) == 1
+    assert lib.dclaw_peak_update(fake, fake, fake, 0, 1, null) == 1
+    assert lib.dclaw_peak_adjoint(fake, null, 10, 1, fake, null) == 1
+    assert lib.dclaw_peak_adjoint(fake, fake, 10, 1, null, null) == 1
+
+
 def test_fortran_adapter_argument_checks():
     lib = _lib.load()
     fake, null = ctypes.c_void_p(256), ctypes.c_void_p(0)
