@@ -56,18 +56,18 @@ SIGNATURES = {
     "dclaw_adjoint_workspace_bytes": (_sz, [_int, _int]),
     "dclaw_adjoint_supported": (_int, [_pp]),
     "dclaw_step_adjoint_prepare": (_int, [_vp, _vp, _int, _int, _dbl, _dbl, _vp, _pp, _vp, _sz, _vp, _vp]),
-    "dclaw_step_adjoint_reverse": (_int, [_vp, _vp, _int, _int, _dbl, _dbl, _vp, _pp, _vp, _vp, _vp, _vp, _sz,
-                                          _vp, _vp]),
+    "dclaw_step_adjoint_reverse": (_int, [_vp, _vp, _int, _int, _dbl, _dbl, _vp, _pp, _vp, _vp, _vp, _vp, _vp,
+                                          _sz, _vp, _vp]),
     "dclaw_step_adjoint_batched_prepare": (_int, [ctypes.POINTER(CAdjBatch), _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                                   _vp]),
     "dclaw_step_adjoint_batched_reverse": (_int, [ctypes.POINTER(CAdjBatch), _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                                                  _vp, _vp, _vp, _vp]),
-    "dclaw_step_adjoint": (_int, [_vp, _vp, _int, _int, _dbl, _dbl, _vp, _pp, _vp, _vp, _vp, _vp, _sz, _vp,
+                                                  _vp, _vp, _vp, _vp, _vp]),
+    "dclaw_step_adjoint": (_int, [_vp, _vp, _int, _int, _dbl, _dbl, _vp, _pp, _vp, _vp, _vp, _vp, _vp, _sz, _vp,
                                   _vp]),
     "dclaw_adjoint_batch_layout": (_int, [_int, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(CAdjMember),
                                           ctypes.POINTER(CAdjBatch)]),
     "dclaw_step_adjoint_batched": (_int, [ctypes.POINTER(CAdjBatch), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                                          _vp, _vp]),
+                                          _vp, _vp, _vp]),
 }
 
 _lib = None

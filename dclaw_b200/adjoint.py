@@ -78,10 +78,11 @@ class StepAdjoint:
         self.status = torch.zeros(1, dtype=torch.int32, device=b.device)
 
     def vjp(self, q_in: torch.Tensor, dt: torch.Tensor, lam_out: torch.Tensor, lam_in: torch.Tensor,
-            pbar: torch.Tensor) -> None:
+            pbar: torch.Tensor, bbar: torch.Tensor | None = None) -> None:
+        """bbar ((my, mx), accumulated, optional): += the bed's adjoint."""
         rc = self.lib.dclaw_step_adjoint(_lib.ptr(q_in), _lib.ptr(self.b), self.mx, self.my, self.dx, self.dy,
                                          _lib.ptr(dt), ctypes.byref(self.cp), _lib.ptr(lam_out), _lib.ptr(lam_in),
-                                         _lib.ptr(pbar), _lib.ptr(self.work), self.work_bytes,
+                                         _lib.ptr(pbar), _lib.ptr(bbar), _lib.ptr(self.work), self.work_bytes,
                                          _lib.ptr(self.status), _lib.stream_ptr())
         _lib.check(rc, "dclaw_step_adjoint")
 
@@ -94,19 +95,21 @@ class StepAdjoint:
         _lib.check(rc, "dclaw_step_adjoint_prepare")
 
     def reverse(self, q_in: torch.Tensor, dt: torch.Tensor, lam_out: torch.Tensor, lam_in: torch.Tensor,
-                pbar: torch.Tensor) -> None:
+                pbar: torch.Tensor, bbar: torch.Tensor | None = None) -> None:
         """The rest of vjp, after prepare with the same q_in and dt."""
         rc = self.lib.dclaw_step_adjoint_reverse(_lib.ptr(q_in), _lib.ptr(self.b), self.mx, self.my, self.dx,
                                                  self.dy, _lib.ptr(dt), ctypes.byref(self.cp), _lib.ptr(lam_out),
-                                                 _lib.ptr(lam_in), _lib.ptr(pbar), _lib.ptr(self.work),
-                                                 self.work_bytes, _lib.ptr(self.status), _lib.stream_ptr())
+                                                 _lib.ptr(lam_in), _lib.ptr(pbar), _lib.ptr(bbar),
+                                                 _lib.ptr(self.work), self.work_bytes, _lib.ptr(self.status),
+                                                 _lib.stream_ptr())
         _lib.check(rc, "dclaw_step_adjoint_reverse")
 
     def check_status(self) -> None:
         _lib.check(int(self.status.item()), "adjoint step")
 
 
-def _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, dt_of, lam, lam2, pbar, add_outs, bed_for=None):
+def _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, dt_of, lam, lam2, pbar, add_outs, bed_for=None,
+                        bbar=None):
     """The step adjoints of steps n_steps .. 1, each step's prepare queued on
     a side stream ahead of the previous step's reverse.
 
@@ -118,7 +121,8 @@ def _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, dt_of, lam, lam
     buffer's previous user, block s + 2, is done by then). dt_of(n): step
     n's dt; add_outs(n, lam): adds the output gradients at step count n;
     bed_for(n, adj) (a moving bed): fills adj's bed with step n's, on the
-    side stream once adj's workspace is free.
+    side stream once adj's workspace is free. bbar (optional): accumulates
+    the bed's adjoint over the steps.
     The reverses run on a high-priority stream and the prepares (which do
     not read lam) on a normal one, so they fill the SMs the reverses leave
     idle. Returns the final (lam, lam2)."""
@@ -154,7 +158,7 @@ def _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, dt_of, lam, lam
         with torch.cuda.stream(rev):
             rev.wait_event(ev_prep)
             add_outs(n, lam)
-            adjs[w].reverse(state_of(n), dt_of(n), lam, lam2, pbar)
+            adjs[w].reverse(state_of(n), dt_of(n), lam, lam2, pbar, bbar)
             last_rev[w] = rev.record_event()
         if n > 1:
             with torch.cuda.stream(side):
@@ -212,6 +216,7 @@ class _Rollout(torch.autograd.Function):
         bed_fn = b if callable(b) else None
         if bed_fn is not None:
             b = bed_fn(torch.zeros((), dtype=torch.float64, device=q0.device)).contiguous()
+        b = b.detach()
         st = PatchStepper(q0.detach(), b, prm, dx, dy)
         if dt_schedule is not None:
             # a replayed schedule keeps the observation interval for the
@@ -348,14 +353,16 @@ class _Rollout(torch.autograd.Function):
         def bed_for(n, adj):
             adj.b.copy_(bed_fn(t_start[n - 1]))
 
+        # the bed's gradient, for a fixed bed that requires one
+        bbar = torch.zeros_like(b) if bed_fn is None and ctx.needs_input_grad[2] else None
         lam, lam2 = _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, lambda n: dts[n - 1:n], lam,
-                                        lam2, pbar, add_outs, bed_for if bed_fn is not None else None)
+                                        lam2, pbar, add_outs, bed_for if bed_fn is not None else None, bbar)
         add_outs(0, lam)
         _lib.check(fw.status(), "rollout recompute")
         for adj in adjs:
             adj.check_status()
         scale = torch.tensor([_DEG, 1.0, 1.0, 1.0], dtype=torch.float64, device=dev)
-        return (lam, pbar * scale, None, None, None, None, None, None, None, None, None, None, None, None, None, None,
+        return (lam, pbar * scale, bbar, None, None, None, None, None, None, None, None, None, None, None, None, None,
                 None)
 
 
@@ -370,9 +377,12 @@ def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams
     tensor (phi [deg], kref, alpha_c, mu) overriding those fields of params,
     b: (my, mx), or a moving bed: a function of the simulated time (a 0-dim
     float64 device tensor) returning the (my, mx) bed, evaluated before every
-    step as the port's loops do (e.g. `solver.gate_bed`); the bed itself is
-    not differentiated. Returns the states after each step count in out_steps
-    (0 = q0), shape (len(out_steps), 5, my, mx). dt0 is the first dt; with
+    step as the port's loops do (e.g. `solver.gate_bed`). A fixed bed that
+    requires grad gets its gradient (through calc_taudir's surface slopes
+    and the solver's bed step), as the port's rollout_peak is differentiated
+    with respect to the whole bed; a moving bed is not differentiated.
+    Returns the states after each step count in out_steps (0 = q0), shape
+    (len(out_steps), 5, my, mx). dt0 is the first dt; with
     fixed_dt every step uses it, otherwise the tick rule picks the next dt
     from the Courant number (clipped at t_final when t_final > 0). Gradients
     reach q0 and theta through the hand-written step adjoint with time
@@ -433,10 +443,10 @@ def rollout_peak(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams, 
     """Differentiable running peak depth over n_steps steps, the loss input
     of the port's rollout_peak (differentiable_dclaw/dclaw_jax/solver.py:
     357-388, differentiated by jax.grad): max over q0 and every step's state
-    of h, per cell, shape (my, mx). Its gradient reaches q0 and theta
-    through the step that set each cell's peak (ties: the earliest step).
-    The other arguments are those of `rollout_states` (the bed is not
-    differentiated)."""
+    of h, per cell, shape (my, mx). Its gradient reaches q0, theta and a
+    fixed bed that requires grad through the step that set each cell's peak
+    (ties: the earliest step). The other arguments are those of
+    `rollout_states`."""
     if dt_schedule is not None:
         if dt_schedule.shape != (n_steps,) or dt_schedule.dtype != torch.float64 or not dt_schedule.is_cuda:
             raise ValueError("dt_schedule must be a (n_steps,) float64 CUDA tensor")
@@ -528,21 +538,21 @@ class EnsembleStepAdjoint:
         _lib.check(rc, "dclaw_step_adjoint_batched_prepare")
 
     def reverse(self, q_in: torch.Tensor, dts: torch.Tensor, lam_out: torch.Tensor, lam_in: torch.Tensor,
-                pbar: torch.Tensor) -> None:
+                pbar: torch.Tensor, bbar: torch.Tensor | None = None) -> None:
         rc = self.lib.dclaw_step_adjoint_batched_reverse(ctypes.byref(self.batch), _lib.ptr(self.members_dev),
                                                          _lib.ptr(self.params), _lib.ptr(dts), _lib.ptr(q_in),
                                                          _lib.ptr(self.bed), _lib.ptr(lam_out), _lib.ptr(lam_in),
-                                                         _lib.ptr(pbar), _lib.ptr(self.work),
+                                                         _lib.ptr(pbar), _lib.ptr(bbar), _lib.ptr(self.work),
                                                          _lib.ptr(self.status), _lib.stream_ptr())
         _lib.check(rc, "dclaw_step_adjoint_batched_reverse")
 
     def vjp(self, q_in: torch.Tensor, dts: torch.Tensor, lam_out: torch.Tensor, lam_in: torch.Tensor,
-            pbar: torch.Tensor) -> None:
+            pbar: torch.Tensor, bbar: torch.Tensor | None = None) -> None:
         rc = self.lib.dclaw_step_adjoint_batched(ctypes.byref(self.batch), _lib.ptr(self.members_dev),
                                                  _lib.ptr(self.params), _lib.ptr(dts), _lib.ptr(q_in),
                                                  _lib.ptr(self.bed), _lib.ptr(lam_out), _lib.ptr(lam_in),
-                                                 _lib.ptr(pbar), _lib.ptr(self.work), _lib.ptr(self.status),
-                                                 _lib.stream_ptr())
+                                                 _lib.ptr(pbar), _lib.ptr(bbar), _lib.ptr(self.work),
+                                                 _lib.ptr(self.status), _lib.stream_ptr())
         _lib.check(rc, "dclaw_step_adjoint_batched")
 
     def check_status(self) -> None:

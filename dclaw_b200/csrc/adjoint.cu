@@ -110,7 +110,7 @@ __host__ __device__ inline AdjLayout adj_layout(int mx, int my) {
     L.off_xcb = o; o += align256((size_t)NCB * L.S.nxi * 8);
     L.off_ycb = o; o += align256((size_t)NCB * L.S.nyi * 8);
     L.off_tdq = o; o += align256((size_t)NTD * L.S.npad * 8);
-    L.off_qsb = o; o += align256((size_t)5 * L.S.npad * 8);
+    L.off_qsb = o; o += align256((size_t)NQSB * L.S.npad * 8);
     L.off_sv = o; o += align256((size_t)NSV * L.S.npad * 8);
     L.act_nx = (mx + 4 + ACT_TILE - 1) / ACT_TILE;
     L.act_ny = (my + 4 + ACT_TILE - 1) / ACT_TILE;
@@ -179,6 +179,7 @@ struct BatchArgs {
     const double* b;
     const double* lam_out;
     double* lam_in;
+    double* bbar;   // += the beds' adjoints (bed layout), or null
     char* work;
     int32_t* status;
 };
@@ -239,7 +240,10 @@ __device__ __forceinline__ void block_item(const BatchArgs& a, int m, const dcla
     } else if (SP == SP_INT) {
         if (ci < 1 || cj < 1 || ci > mx || cj > my) return;
         if (OP == OP_RV_SRC2) adj_item_src2(P, g, W, A, a.lam_out + M.q_off, ci, cj, dt, pb);
-        else if (OP == OP_RV_GATHER) adj_item_gather(P, g, A, W, a.lam_in + M.q_off, ci, cj);
+        else if (OP == OP_RV_GATHER) {
+            adj_item_gather(P, g, A, W, a.lam_in + M.q_off, ci, cj);
+            if (a.bbar) adj_item_gather_bed(g, A, W, a.bbar + M.b_off, ci, cj);
+        }
     } else if (SP == SP_RX) {
         if (ci < 0 || cj < 0 || ci > mx + 2 || cj > my + 1) return;
         if (OP == OP_FW_RX) stage_riemann<0>(P, g, W, cj, ci, nullptr, A.sv);
@@ -440,7 +444,7 @@ __global__ void __launch_bounds__(BTPB) k_adj_blocks_zero(BatchArgs a, const uin
             if (ci >= -1 && cj >= -1 && ci <= mx + 2 && cj <= my + 2) {
                 const size_t pp = pidx(g, ci, cj);
                 for (int f = 0; f < NTD; ++f) A.tdq[f * npad + pp] = 0.0;
-                for (int f = 0; f < 5; ++f) A.qsb[f * npad + pp] = 0.0;
+                for (int f = 0; f < NQSB; ++f) A.qsb[f * npad + pp] = 0.0;
             }
         }
     }
@@ -670,7 +674,8 @@ int dclaw_adjoint_supported(const dclaw_params* p) {
 // part of the step adjoint to queue)
 static int single_adjoint(const double* q_in, const double* b, int mx, int my, double dx, double dy,
                           const double* dt, const dclaw_params* p, const double* lam_out, double* lam_in,
-                          double* pbar, void* work, size_t work_bytes, int32_t* status, void* stream, int phase) {
+                          double* pbar, double* bbar, void* work, size_t work_bytes, int32_t* status, void* stream,
+                          int phase) {
     if (!q_in || !b || !dt || !work) return DCLAW_ERR_ARG;
     if ((phase & PHASE_REVERSE) && (!lam_out || !lam_in || !pbar || lam_in == lam_out)) return DCLAW_ERR_ARG;
     if (!adj_sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0)) return DCLAW_ERR_ARG;
@@ -692,7 +697,7 @@ static int single_adjoint(const double* q_in, const double* b, int mx, int my, d
         M.dy = dy;
         k_adj_single_setup<<<1, 32, 0, s>>>(M, *p, mem, prm);
     }
-    BatchArgs a{1, mem, prm, dt, q_in, b, lam_out, lam_in, base, status};
+    BatchArgs a{1, mem, prm, dt, q_in, b, lam_out, lam_in, bbar, base, status};
     launch_block_adjoint(a, (uint32_t)((size_t)L.act_nx * L.act_ny), base + T.off_lists,
                          (unsigned int*)(base + T.off_counts), sm_count_adj(), s, phase);
     if (phase & PHASE_REVERSE) launch_pdl(k_adj_batch_pbar, dim3(1), dim3(BTPB), s, a, pbar);
@@ -702,23 +707,24 @@ static int single_adjoint(const double* q_in, const double* b, int mx, int my, d
 
 int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, double dx, double dy,
                        const double* dt, const dclaw_params* p, const double* lam_out, double* lam_in,
-                       double* pbar, void* work, size_t work_bytes, int32_t* status, void* stream) {
-    return single_adjoint(q_in, b, mx, my, dx, dy, dt, p, lam_out, lam_in, pbar, work, work_bytes, status, stream,
-                          PHASE_PREPARE | PHASE_REVERSE);
+                       double* pbar, double* bbar, void* work, size_t work_bytes, int32_t* status, void* stream) {
+    return single_adjoint(q_in, b, mx, my, dx, dy, dt, p, lam_out, lam_in, pbar, bbar, work, work_bytes, status,
+                          stream, PHASE_PREPARE | PHASE_REVERSE);
 }
 
 int dclaw_step_adjoint_prepare(const double* q_in, const double* b, int mx, int my, double dx, double dy,
                                const double* dt, const dclaw_params* p, void* work, size_t work_bytes,
                                int32_t* status, void* stream) {
-    return single_adjoint(q_in, b, mx, my, dx, dy, dt, p, nullptr, nullptr, nullptr, work, work_bytes, status,
-                          stream, PHASE_PREPARE);
+    return single_adjoint(q_in, b, mx, my, dx, dy, dt, p, nullptr, nullptr, nullptr, nullptr, work, work_bytes,
+                          status, stream, PHASE_PREPARE);
 }
 
 int dclaw_step_adjoint_reverse(const double* q_in, const double* b, int mx, int my, double dx, double dy,
                                const double* dt, const dclaw_params* p, const double* lam_out, double* lam_in,
-                               double* pbar, void* work, size_t work_bytes, int32_t* status, void* stream) {
-    return single_adjoint(q_in, b, mx, my, dx, dy, dt, p, lam_out, lam_in, pbar, work, work_bytes, status, stream,
-                          PHASE_REVERSE);
+                               double* pbar, double* bbar, void* work, size_t work_bytes, int32_t* status,
+                               void* stream) {
+    return single_adjoint(q_in, b, mx, my, dx, dy, dt, p, lam_out, lam_in, pbar, bbar, work, work_bytes, status,
+                          stream, PHASE_REVERSE);
 }
 
 int dclaw_adjoint_batch_layout(int n, const int32_t* mx, const int32_t* my, const double* dx, const double* dy,
@@ -761,13 +767,13 @@ int dclaw_adjoint_batch_layout(int n, const int32_t* mx, const int32_t* my, cons
 
 static int batched_adjoint(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
                            const dclaw_params* params, const double* dt, const double* q_in, const double* b,
-                           const double* lam_out, double* lam_in, double* pbar, void* work, int32_t* status,
-                           void* stream, int phase) {
+                           const double* lam_out, double* lam_in, double* pbar, double* bbar, void* work,
+                           int32_t* status, void* stream, int phase) {
     if (!batch || !members || !params || !dt || !q_in || !b || !work) return DCLAW_ERR_ARG;
     if ((phase & PHASE_REVERSE) && (!lam_out || !lam_in || !pbar || lam_in == lam_out)) return DCLAW_ERR_ARG;
     if (batch->nmembers <= 0 || batch->chunk_items != (uint32_t)ATPB) return DCLAW_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
-    BatchArgs a{batch->nmembers, members, params, dt, q_in, b, lam_out, lam_in, (char*)work, status};
+    BatchArgs a{batch->nmembers, members, params, dt, q_in, b, lam_out, lam_in, bbar, (char*)work, status};
     char* lists = (char*)work + (batch->work_bytes - 256 - 2 * align256((size_t)batch->nblocks * 8));
     unsigned int* counts = (unsigned int*)((char*)work + (batch->work_bytes - 256));
     launch_block_adjoint(a, batch->nblocks, lists, counts, sm_count_adj(), s, phase);
@@ -778,24 +784,24 @@ static int batched_adjoint(const dclaw_adj_batch* batch, const dclaw_adj_member*
 
 int dclaw_step_adjoint_batched(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
                                const dclaw_params* params, const double* dt, const double* q_in, const double* b,
-                               const double* lam_out, double* lam_in, double* pbar, void* work, int32_t* status,
-                               void* stream) {
-    return batched_adjoint(batch, members, params, dt, q_in, b, lam_out, lam_in, pbar, work, status, stream,
+                               const double* lam_out, double* lam_in, double* pbar, double* bbar, void* work,
+                               int32_t* status, void* stream) {
+    return batched_adjoint(batch, members, params, dt, q_in, b, lam_out, lam_in, pbar, bbar, work, status, stream,
                            PHASE_PREPARE | PHASE_REVERSE);
 }
 
 int dclaw_step_adjoint_batched_prepare(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
                                        const dclaw_params* params, const double* dt, const double* q_in,
                                        const double* b, void* work, int32_t* status, void* stream) {
-    return batched_adjoint(batch, members, params, dt, q_in, b, nullptr, nullptr, nullptr, work, status, stream,
-                           PHASE_PREPARE);
+    return batched_adjoint(batch, members, params, dt, q_in, b, nullptr, nullptr, nullptr, nullptr, work, status,
+                           stream, PHASE_PREPARE);
 }
 
 int dclaw_step_adjoint_batched_reverse(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
                                        const dclaw_params* params, const double* dt, const double* q_in,
                                        const double* b, const double* lam_out, double* lam_in, double* pbar,
-                                       void* work, int32_t* status, void* stream) {
-    return batched_adjoint(batch, members, params, dt, q_in, b, lam_out, lam_in, pbar, work, status, stream,
+                                       double* bbar, void* work, int32_t* status, void* stream) {
+    return batched_adjoint(batch, members, params, dt, q_in, b, lam_out, lam_in, pbar, bbar, work, status, stream,
                            PHASE_REVERSE);
 }
 

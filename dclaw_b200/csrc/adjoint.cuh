@@ -1544,8 +1544,10 @@ DC_HD bool src2_cell_b(const dclaw_params& P, double phi, double dt, const doubl
 // Stage B reverse on cell (i, j): tdb = adjoints of (fs, taudir_x,
 // taudir_y). Accumulates the cell's qB adjoint into qb[5] and the adjoints of
 // the neighbours' depths into nb[4] (left, right, bottom, top).
+// bedb[5] += adjoints of the beds of the cell and of its neighbours L, R,
+// B, T (eta = h + b enters the driving forces)
 DC_HD void stage_taudir_b(const dclaw_params& P, const Geom& g, const Work& W, int i, int j, const double tdb[3],
-                          double qb[5], double nb[4], double* pbar) {
+                          double qb[5], double nb[4], double* pbar, double bedb[5]) {
     if (i < 0 || j < 0 || i > g.mx + 1 || j > g.my + 1) return;
     const size_t pi = pidx(g, i, j);
     const double dry = P.dry_tolerance;
@@ -1666,14 +1668,16 @@ DC_HD void stage_taudir_b(const dclaw_params& P, const Geom& g, const Work& W, i
     // eta source
     double eta0b = 0.0;
     if (esrc == 0) eta0b += etab; else if (esrc == 1) etaLb += etab; else etaBb += etab;
-    auto nbeta = [&](bool mm, double eb, double& hNb) {
-        if (mm) eta0b += eb; else hNb += eb;  // etaN0 = hN + bN
+    auto nbeta = [&](bool mm, double eb, double& hNb, double& bNb) {
+        if (mm) eta0b += eb;   // etaN replaced by eta0
+        else { hNb += eb; bNb += eb; }  // etaN0 = hN + bN
     };
-    nbeta(mL, etaLb, hLb);
-    nbeta(mR, etaRb, hRb);
-    nbeta(mB, etaBb, hBb);
-    nbeta(mT, etaTb, hTb);
+    nbeta(mL, etaLb, hLb, bedb[1]);
+    nbeta(mR, etaRb, hRb, bedb[2]);
+    nbeta(mB, etaBb, hBb, bedb[3]);
+    nbeta(mT, etaTb, hTb, bedb[4]);
     double h_b = eta0b;  // eta0 = h + b
+    bedb[0] += eta0b;
     // setvars and qfix
     double phib = 0.0, ub = 0.0, vb = 0.0, mb = 0.0, pb = 0.0;
     SetVars ob{};
@@ -1763,8 +1767,9 @@ DC_HD void stage_b4_b(const dclaw_params& P, const Geom& g, const double* __rest
 namespace dclaw {
 
 constexpr int NFB = 47;  // FluxB: self 15, left 12, right 12, a2l 4, a2r 4
-constexpr int NCB = 14;  // CellB of both sides: q[5], fs, taudir
-constexpr int NTD = 9;   // taudir reverse: qb[5], neighbour depths[4]
+constexpr int NCB = 16;  // CellB of both sides: q[5], fs, taudir; then the beds of L and R
+constexpr int NTD = 14;  // taudir reverse: qb[5], neighbour depths[4], beds of the cell and L, R, B, T
+constexpr int NQSB = 6;  // per padded cell: its source cell's q adjoint (5), its bed's adjoint
 
 struct AdjWork {
     double* lamq;  // 5 interior planes
@@ -1773,7 +1778,7 @@ struct AdjWork {
     double* xcb;   // NCB x-interface planes
     double* ycb;   // NCB y-interface planes
     double* tdq;   // NTD padded planes
-    double* qsb;   // 5 padded planes
+    double* qsb;   // NQSB padded planes
     double* sv;    // NSV padded planes: setvars records (svrec_cell)
     // activity of ACT_TILE x ACT_TILE blocks of padded cells (nullable: all
     // active): nonzero when a cell within ACT_REACH of the block is wet in
@@ -1861,6 +1866,8 @@ DC_HD bool adj_item_riemann(const dclaw_params& P, const Geom& g, const Work& W,
     dst[(size_t)6 * np + oi] = Lc.taudir;
     dst[(size_t)12 * np + oi] = Rc.fs;
     dst[(size_t)13 * np + oi] = Rc.taudir;
+    dst[(size_t)14 * np + oi] = Lc.b;
+    dst[(size_t)15 * np + oi] = Rc.b;
     return ok;
 }
 
@@ -1894,10 +1901,12 @@ DC_HD void adj_item_taudir(const dclaw_params& P, const Geom& g, const Work& W, 
         }
     }
     double qb[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, nb[4] = {0.0, 0.0, 0.0, 0.0};
-    stage_taudir_b(P, g, W, i, j, tdb, qb, nb, pbar);
+    double bedb[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    stage_taudir_b(P, g, W, i, j, tdb, qb, nb, pbar, bedb);
     const size_t pi = pidx(g, i, j);
     for (int k = 0; k < 5; ++k) A.tdq[(size_t)k * W.npad + pi] = qb[k];
     for (int k = 0; k < 4; ++k) A.tdq[(size_t)(5 + k) * W.npad + pi] = nb[k];
+    for (int k = 0; k < 5; ++k) A.tdq[(size_t)(9 + k) * W.npad + pi] = bedb[k];
 }
 
 DC_HD void adj_item_b4(const dclaw_params& P, const Geom& g, const Work& W, const AdjWork& A,
@@ -1952,6 +1961,23 @@ DC_HD void adj_item_b4(const dclaw_params& P, const Geom& g, const Work& W, cons
     int si, sj;
     stage_b4_b(P, g, q_in, i, j, qb, sb, si, sj);
     for (int k = 0; k < 5; ++k) A.qsb[(size_t)k * np + pi] = sb[k];
+    // the cell's bed: the solver sides it takes (x and y), its own
+    // calc_taudir stencil and its neighbours'
+    double bb = 0.0;
+    if (j >= 0 && j <= my + 1) {
+        if (i + 1 >= 0 && i + 1 <= mx + 2) bb += A.xcb[(size_t)14 * nx + xidx(g, j, i + 1)];
+        if (i >= 0 && i <= mx + 2) bb += A.xcb[(size_t)15 * nx + xidx(g, j, i)];
+    }
+    if (i >= 0 && i <= mx + 1) {
+        if (j + 1 >= 0 && j + 1 <= my + 2) bb += A.ycb[(size_t)14 * ny + yidx(g, j + 1, i)];
+        if (j >= 0 && j <= my + 2) bb += A.ycb[(size_t)15 * ny + yidx(g, j, i)];
+    }
+    bb += A.tdq[(size_t)9 * np + pi];
+    if (i + 1 <= mx + 2) bb += A.tdq[(size_t)10 * np + pidx(g, i + 1, j)];
+    if (i - 1 >= -1) bb += A.tdq[(size_t)11 * np + pidx(g, i - 1, j)];
+    if (j + 1 <= my + 2) bb += A.tdq[(size_t)12 * np + pidx(g, i, j + 1)];
+    if (j - 1 >= -1) bb += A.tdq[(size_t)13 * np + pidx(g, i, j - 1)];
+    A.qsb[(size_t)5 * np + pi] = bb;
 }
 
 // interior source index of padded coordinate x (bc2amr mapping)
@@ -1982,6 +2008,25 @@ DC_HD void adj_item_gather(const dclaw_params& P, const Geom& g, const AdjWork& 
             for (int a = 0; a < ni; ++a) s += A.qsb[(size_t)m * W.npad + pidx(g, ci[a], cj[b])];
         lam_in[(size_t)m * plane + c] = s;
     }
+}
+
+// interior cell (i, j): bbar += the adjoint of its bed, summed over the
+// padded cells whose bed is a copy of it (the ghost bed is the nearest
+// interior cell's, whatever the boundary condition)
+DC_HD void adj_item_gather_bed(const Geom& g, const AdjWork& A, const Work& W, double* __restrict__ bbar, int i,
+                               int j) {
+    const int mx = g.mx, my = g.my;
+    int ci[3], cj[3], ni = 1, nj = 1;
+    ci[0] = i;
+    cj[0] = j;
+    if (i == 1) { ci[ni++] = -1; ci[ni++] = 0; }
+    if (i == mx) { ci[ni++] = mx + 1; ci[ni++] = mx + 2; }
+    if (j == 1) { cj[nj++] = -1; cj[nj++] = 0; }
+    if (j == my) { cj[nj++] = my + 1; cj[nj++] = my + 2; }
+    double s = 0.0;
+    for (int b = 0; b < nj; ++b)
+        for (int a = 0; a < ni; ++a) s += A.qsb[(size_t)5 * W.npad + pidx(g, ci[a], cj[b])];
+    bbar[(size_t)(j - 1) * mx + (size_t)(i - 1)] += s;
 }
 
 }  // namespace dclaw

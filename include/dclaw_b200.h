@@ -311,6 +311,9 @@ int dclaw_batch_reset(const dclaw_batch* batch, void* work, void* stream);
  * double; dt is data, not differentiated) from q_in (interior layout, 5
  * planes) over bed b. pbar (DEVICE, 4 doubles, ACCUMULATED) receives
  * (dS/dtheta)^T lam_out for theta = (phi [radians], kref, alpha_c, mu).
+ * bbar (DEVICE, mx*my doubles, ACCUMULATED, nullable) receives (dS/db)^T
+ * lam_out, the adjoint of the bed (through calc_taudir's surface slopes and
+ * the solver's bed step; the ghost beds are copies of the nearest cells).
  * At branches (dry tolerance, limiter regimes, wall and static-friction
  * tests, min/max picks) the adjoint follows the branch the forward step
  * took. Results are bit-reproducible (no atomics in the sums). status
@@ -323,7 +326,7 @@ size_t dclaw_adjoint_workspace_bytes(int mx, int my);
 int dclaw_adjoint_supported(const dclaw_params* p);
 int dclaw_step_adjoint(const double* q_in, const double* b, int mx, int my, double dx, double dy,
                        const double* dt, const dclaw_params* p, const double* lam_out, double* lam_in,
-                       double* pbar, void* work, size_t work_bytes, int32_t* status, void* stream);
+                       double* pbar, double* bbar, void* work, size_t work_bytes, int32_t* status, void* stream);
 /* dclaw_step_adjoint in two parts. prepare queues what does not depend on
  * lam_out (the activity blocks, the forward recompute of the step's
  * intermediates into work); reverse, given the same q_in, b, dt, p and work
@@ -335,7 +338,8 @@ int dclaw_step_adjoint_prepare(const double* q_in, const double* b, int mx, int 
                                int32_t* status, void* stream);
 int dclaw_step_adjoint_reverse(const double* q_in, const double* b, int mx, int my, double dx, double dy,
                                const double* dt, const dclaw_params* p, const double* lam_out, double* lam_in,
-                               double* pbar, void* work, size_t work_bytes, int32_t* status, void* stream);
+                               double* pbar, double* bbar, void* work, size_t work_bytes, int32_t* status,
+                               void* stream);
 
 /* ---- adjoint of one step of an ensemble ---------------------------------------
  * The reference differentiates its particle filters member by member with
@@ -380,13 +384,14 @@ int dclaw_adjoint_batch_layout(int n, const int32_t* mx, const int32_t* my, cons
                                dclaw_adj_batch* batch);
 /* batch: host; members, params, dt (one per member), status (one int32 per
  * member, nullable), pbar (4 per member, accumulated): DEVICE arrays.
- * q_in, lam_out, lam_in: state-shaped arenas; b: bed arena; work:
+ * q_in, lam_out, lam_in: state-shaped arenas; b: bed arena; bbar (nullable,
+ * accumulated): bed-shaped arena of the beds' adjoints; work:
  * batch->work_bytes. Members whose options have no adjoint form get
  * DCLAW_ERR_UNSUPPORTED in their status word. */
 int dclaw_step_adjoint_batched(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
                                const dclaw_params* params, const double* dt, const double* q_in, const double* b,
-                               const double* lam_out, double* lam_in, double* pbar, void* work, int32_t* status,
-                               void* stream);
+                               const double* lam_out, double* lam_in, double* pbar, double* bbar, void* work,
+                               int32_t* status, void* stream);
 /* the two parts of dclaw_step_adjoint_batched, as for the single patch */
 int dclaw_step_adjoint_batched_prepare(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
                                        const dclaw_params* params, const double* dt, const double* q_in,
@@ -394,7 +399,7 @@ int dclaw_step_adjoint_batched_prepare(const dclaw_adj_batch* batch, const dclaw
 int dclaw_step_adjoint_batched_reverse(const dclaw_adj_batch* batch, const dclaw_adj_member* members,
                                        const dclaw_params* params, const double* dt, const double* q_in,
                                        const double* b, const double* lam_out, double* lam_in, double* pbar,
-                                       void* work, int32_t* status, void* stream);
+                                       double* bbar, void* work, int32_t* status, void* stream);
 
 /* initialise a device clock: t, dt, t_final, fixed_dt; counters cleared, t_obs 0 */
 int dclaw_clock_init(dclaw_clock* clock, double t, double dt, double t_final, int fixed_dt,

@@ -38,7 +38,7 @@ class Adj:
         self.lib.adj_step_fwd.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                           ctypes.c_double, _dp, _dp, ctypes.c_double, _dp]
         self.lib.adj_step_vjp.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
-                                          ctypes.c_double, _dp, _dp, ctypes.c_double, _dp, _dp, _dp]
+                                          ctypes.c_double, _dp, _dp, ctypes.c_double, _dp, _dp, _dp, _dp]
 
     def local(self, name: str, seed: int = 1, n: int = 1000):
         err = ctypes.c_double()
@@ -58,13 +58,16 @@ class Adj:
                               out.ctypes.data_as(_dp))
         return out
 
-    def vjp(self, p, q, b, dx, dy, dt, lam):
+    def vjp(self, p, q, b, dx, dy, dt, lam, bed=False):
+        """lam_in, pbar (and the bed's adjoint with bed=True)."""
         q = np.ascontiguousarray(q, dtype=np.float64)
         lam = np.ascontiguousarray(lam, dtype=np.float64)
         li = np.zeros_like(q)
         pb = np.zeros(4)
+        bb = np.zeros(q.shape[1:]) if bed else None
         cp = p.to_c()
         rc = self.lib.adj_step_vjp(ctypes.byref(cp), q.shape[2], q.shape[1], dx, dy, self._p(q), self._p(b), dt,
-                                   self._p(lam), li.ctypes.data_as(_dp), pb.ctypes.data_as(_dp))
+                                   self._p(lam), li.ctypes.data_as(_dp), pb.ctypes.data_as(_dp),
+                                   bb.ctypes.data_as(_dp) if bed else None)
         assert rc == 0
-        return li, pb
+        return (li, pb, bb) if bed else (li, pb)

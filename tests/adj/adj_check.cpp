@@ -425,13 +425,13 @@ int adj_step_fwd(const dclaw_params* P, int mx, int my, double dx, double dy, co
 
 // adjoint of one step: lam_in = (dS/dq)^T lam_out, pbar += (dS/dtheta)^T lam_out
 int adj_step_vjp(const dclaw_params* P, int mx, int my, double dx, double dy, const double* q, const double* b,
-                 double dt, const double* lam_out, double* lam_in, double* pbar) {
+                 double dt, const double* lam_out, double* lam_in, double* pbar, double* bbar) {
     Geom g{mx, my, mx + 4, my + 4, dx, dy};
     HostWork H(mx, my);
     forward_stages(*P, g, q, b, H, dt);
     const Work& W = H.W;
     std::vector<double> lamq(5 * (size_t)mx * my), xfb(NFB * W.nxi), yfb(NFB * W.nyi), xcb(NCB * W.nxi),
-        ycb(NCB * W.nyi), tdq(NTD * W.npad), qsb(5 * W.npad), sv(NSV * W.npad);
+        ycb(NCB * W.nyi), tdq(NTD * W.npad), qsb(NQSB * W.npad), sv(NSV * W.npad);
     AdjWork A{lamq.data(), xfb.data(), yfb.data(), xcb.data(), ycb.data(), tdq.data(), qsb.data(), sv.data()};
     for (int j = -1; j <= my + 2; ++j)
         for (int i = -1; i <= mx + 2; ++i) adj_item_svrec(*P, g, W, A, i, j);
@@ -452,6 +452,9 @@ int adj_step_vjp(const dclaw_params* P, int mx, int my, double dx, double dy, co
         for (int i = -1; i <= mx + 2; ++i) adj_item_b4(*P, g, W, A, q, i, j);
     for (int j = 1; j <= my; ++j)
         for (int i = 1; i <= mx; ++i) adj_item_gather(*P, g, A, W, lam_in, i, j);
+    if (bbar)
+        for (int j = 1; j <= my; ++j)
+            for (int i = 1; i <= mx; ++i) adj_item_gather_bed(g, A, W, bbar, i, j);
     return ok ? 0 : 2;
 }
 

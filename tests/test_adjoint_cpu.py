@@ -101,6 +101,30 @@ def test_step_vjp_matches_finite_differences(adj, name):
             f"{pname}: AD {pb[k]:.10e} FD {fdp:.10e}"
 
 
+@pytest.mark.parametrize("name", ["wet", "dry30", "dry50", "order1", "transverse1", "at_rest", "manning"])
+def test_step_vjp_bed_matches_finite_differences(adj, name):
+    """The bed's adjoint (calc_taudir's surface slopes, the solver's bed
+    step, ghost beds copied from the nearest cells) against central
+    differences of the host step; lam_in and pbar are unchanged by asking
+    for it."""
+    p, q, b = _case(**CASES[name])
+    dx, dt = 1.0, 0.02
+    rng = np.random.default_rng(200)
+    lam = rng.standard_normal(q.shape)
+    li0, pb0 = adj.vjp(p, q, b, dx, dx, dt, lam)
+    li, pb, bb = adj.vjp(p, q, b, dx, dx, dt, lam, bed=True)
+    assert np.array_equal(li, li0) and np.array_equal(pb, pb0)
+    db = rng.standard_normal(b.shape)
+
+    def L(bed):
+        return float((lam * adj.step(p, q, bed, dx, dx, dt)).sum())
+
+    eps = 1e-6
+    fd = (L(b + eps * db) - L(b - eps * db)) / (2 * eps)
+    ad = float((bb * db).sum())
+    assert abs(ad - fd) <= 1e-6 * max(abs(fd), 1e-3), f"bed: AD {ad:.12e} FD {fd:.12e}"
+
+
 def test_checkpoint_block_follows_the_memory_budget():
     """The default checkpoint block: every state kept (k = 1) when the run
     fits the budget, else the smallest k whose ceil(n/k) block inputs plus

@@ -54,6 +54,14 @@ def test_step_adjoint_matches_host_build(cuda_device, host_adj, name):
     assert np.array_equal(li, li_h), f"max |diff| {np.abs(li - li_h).max():.3e}"
     pb = pbar.cpu().numpy()
     assert np.allclose(pb, pb_h, rtol=1e-12, atol=1e-300), (pb, pb_h)
+    # the bed's adjoint: bit for bit with the host build, nothing else changed
+    _, _, bb_h = host_adj.vjp(p, q, b, dx, dx, dt, lam, bed=True)
+    lam_in_b = torch.empty_like(lam_in)
+    pbar_b = torch.zeros(4, dtype=torch.float64, device=dev)
+    bbar = torch.zeros(b.shape, dtype=torch.float64, device=dev)
+    adj.vjp(torch.tensor(q, device=dev), dtt, torch.tensor(lam, device=dev), lam_in_b, pbar_b, bbar)
+    assert torch.equal(lam_in_b, lam_in) and torch.equal(pbar_b, pbar)
+    assert np.array_equal(bbar.cpu().numpy(), bb_h), f"bed: max |diff| {np.abs(bbar.cpu().numpy() - bb_h).max():.3e}"
     # a second call gives the same bits (no atomics in the sums)
     pbar2 = torch.zeros(4, dtype=torch.float64, device=dev)
     lam_in2 = torch.empty_like(lam_in)
@@ -158,6 +166,37 @@ def test_rollout_gradient_matches_finite_differences(cuda_device, mode):
         e = torch.zeros(4, dtype=torch.float64, device=dev)
         e[k] = scale
         _close(float(gt[k]) * scale, _fd(lambda h: Lf(q00, th0 + h * e), eps0=4e-6), f"theta[{k}]")
+
+
+def test_rollout_bed_gradient(cuda_device):
+    """The gradient with respect to a fixed bed over a checkpointed run
+    matches finite differences at the fixed dt, and is the same with every
+    state kept and with checkpoint blocks."""
+    dev = cuda_device
+    p, qn, bn = _small_flow(seed=12)
+    n, outs = 16, [8, 16]
+    wts = torch.tensor(_loss_weights(qn, len(outs), seed=6), device=dev)
+    res = []
+    for blk in (1, 4):
+        q0 = torch.tensor(qn, device=dev, requires_grad=True)
+        theta = theta_of(p, dev)
+        b = torch.tensor(bn, device=dev, requires_grad=True)
+        L, o = _run_loss(q0, theta, b, p, 1.0, n, outs, wts, dt0=0.02, fixed_dt=True, checkpoint_block=blk)
+        L.backward()
+        res.append((b.grad.clone(), q0.grad.clone()))
+    assert torch.equal(res[0][0], res[1][0]) and torch.equal(res[0][1], res[1][1])
+    gb = res[0][0]
+    assert gb.abs().max() > 0
+
+    def Lf(bb):
+        with torch.no_grad():
+            return float(_run_loss(torch.tensor(qn, device=dev), theta_of(p, dev), bb, p, 1.0, n, outs, wts,
+                                   dt0=0.02, fixed_dt=True)[0])
+
+    rng = np.random.default_rng(14)
+    db = torch.tensor(rng.standard_normal(bn.shape), device=dev)
+    b0 = torch.tensor(bn, device=dev)
+    _close(float((gb * db).sum()), _fd(lambda e: Lf(b0 + e * db)), "bed")
 
 
 def test_rollout_gradient_with_a_moving_gate_bed(cuda_device):
