@@ -211,7 +211,7 @@ __device__ __forceinline__ void batch_member_work(const BatchArgs& a, const dcla
     act = (uint32_t*)(base + L.off_act);
     A = AdjWork{(double*)(base + L.off_lamq), (double*)(base + L.off_xfb), (double*)(base + L.off_yfb),
                 (double*)(base + L.off_xcb), (double*)(base + L.off_ycb), (double*)(base + L.off_tdq),
-                (double*)(base + L.off_qsb), (double*)(base + L.off_sv), act, L.act_nx};
+                (double*)(base + L.off_qsb), (double*)(base + L.off_sv), act, L.act_nx, a.bbar != nullptr};
 }
 
 // one item of stage OP at activity cell (ci, cj) (the padded cell whose
@@ -365,7 +365,8 @@ __global__ void __launch_bounds__(BTPB, BlkMinB<OP>::value) k_adj_blocks(BatchAr
                     double* dst = DIR == 0 ? A.xcb : A.ycb;
                     const size_t np = DIR == 0 ? W.nxi : W.nyi;
                     const size_t oi = DIR == 0 ? xidx(g, cj, ci) : yidx(g, cj, ci);
-                    for (int k = 0; k < NCB; ++k) dst[(size_t)k * np + oi] = 0.0;
+                    const int nz = A.bed ? NCB : NCB_Q;
+                    for (int k = 0; k < nz; ++k) dst[(size_t)k * np + oi] = 0.0;
                 }
             }
             // the list is in thread order (warp counts summed in warp
@@ -434,17 +435,17 @@ __global__ void __launch_bounds__(BTPB) k_adj_blocks_zero(BatchArgs a, const uin
             if (ci >= 0 && cj >= 0 && ci <= mx + 2 && cj <= my + 1) {
                 const size_t x = xidx(g, cj, ci);
                 for (int f = 0; f < NFB; ++f) A.xfb[f * nxi + x] = 0.0;
-                for (int f = 0; f < NCB; ++f) A.xcb[f * nxi + x] = 0.0;
+                for (int f = 0; f < NCB_Q; ++f) A.xcb[f * nxi + x] = 0.0;
             }
             if (ci >= 0 && cj >= 0 && ci <= mx + 1 && cj <= my + 2) {
                 const size_t y = yidx(g, cj, ci);
                 for (int f = 0; f < NFB; ++f) A.yfb[f * nyi + y] = 0.0;
-                for (int f = 0; f < NCB; ++f) A.ycb[f * nyi + y] = 0.0;
+                for (int f = 0; f < NCB_Q; ++f) A.ycb[f * nyi + y] = 0.0;
             }
             if (ci >= -1 && cj >= -1 && ci <= mx + 2 && cj <= my + 2) {
                 const size_t pp = pidx(g, ci, cj);
-                for (int f = 0; f < NTD; ++f) A.tdq[f * npad + pp] = 0.0;
-                for (int f = 0; f < NQSB; ++f) A.qsb[f * npad + pp] = 0.0;
+                for (int f = 0; f < NTD_Q; ++f) A.tdq[f * npad + pp] = 0.0;
+                for (int f = 0; f < NQSB_Q; ++f) A.qsb[f * npad + pp] = 0.0;
             }
         }
     }

@@ -1770,6 +1770,8 @@ constexpr int NFB = 47;  // FluxB: self 15, left 12, right 12, a2l 4, a2r 4
 constexpr int NCB = 16;  // CellB of both sides: q[5], fs, taudir; then the beds of L and R
 constexpr int NTD = 14;  // taudir reverse: qb[5], neighbour depths[4], beds of the cell and L, R, B, T
 constexpr int NQSB = 6;  // per padded cell: its source cell's q adjoint (5), its bed's adjoint
+// the planes that need zeros in inactive blocks (all but the bed planes)
+constexpr int NCB_Q = 14, NTD_Q = 9, NQSB_Q = 5;
 
 struct AdjWork {
     double* lamq;  // 5 interior planes
@@ -1789,6 +1791,11 @@ struct AdjWork {
     // with the reverse planes zeroed beforehand it can be skipped.
     const uint32_t* act;
     int act_nx;    // blocks per row of padded cells
+    // the beds' adjoints are wanted: the bed planes are written (solver
+    // sides, calc_taudir) and summed (adj_item_b4, adj_item_gather_bed).
+    // They are not zeroed in inactive blocks: their readers take only items
+    // of active blocks (the others' bed adjoints are zeros).
+    bool bed = false;
 };
 
 constexpr int ACT_TILE = 16, ACT_REACH = 4;
@@ -1866,8 +1873,10 @@ DC_HD bool adj_item_riemann(const dclaw_params& P, const Geom& g, const Work& W,
     dst[(size_t)6 * np + oi] = Lc.taudir;
     dst[(size_t)12 * np + oi] = Rc.fs;
     dst[(size_t)13 * np + oi] = Rc.taudir;
-    dst[(size_t)14 * np + oi] = Lc.b;
-    dst[(size_t)15 * np + oi] = Rc.b;
+    if (A.bed) {
+        dst[(size_t)14 * np + oi] = Lc.b;
+        dst[(size_t)15 * np + oi] = Rc.b;
+    }
     return ok;
 }
 
@@ -1906,7 +1915,8 @@ DC_HD void adj_item_taudir(const dclaw_params& P, const Geom& g, const Work& W, 
     const size_t pi = pidx(g, i, j);
     for (int k = 0; k < 5; ++k) A.tdq[(size_t)k * W.npad + pi] = qb[k];
     for (int k = 0; k < 4; ++k) A.tdq[(size_t)(5 + k) * W.npad + pi] = nb[k];
-    for (int k = 0; k < 5; ++k) A.tdq[(size_t)(9 + k) * W.npad + pi] = bedb[k];
+    if (A.bed)
+        for (int k = 0; k < 5; ++k) A.tdq[(size_t)(9 + k) * W.npad + pi] = bedb[k];
 }
 
 DC_HD void adj_item_b4(const dclaw_params& P, const Geom& g, const Work& W, const AdjWork& A,
@@ -1961,22 +1971,24 @@ DC_HD void adj_item_b4(const dclaw_params& P, const Geom& g, const Work& W, cons
     int si, sj;
     stage_b4_b(P, g, q_in, i, j, qb, sb, si, sj);
     for (int k = 0; k < 5; ++k) A.qsb[(size_t)k * np + pi] = sb[k];
+    if (!A.bed) return;
     // the cell's bed: the solver sides it takes (x and y), its own
-    // calc_taudir stencil and its neighbours'
+    // calc_taudir stencil and its neighbours' (items of active blocks only:
+    // the others' bed adjoints are zeros and their planes are not zeroed)
     double bb = 0.0;
     if (j >= 0 && j <= my + 1) {
-        if (i + 1 >= 0 && i + 1 <= mx + 2) bb += A.xcb[(size_t)14 * nx + xidx(g, j, i + 1)];
-        if (i >= 0 && i <= mx + 2) bb += A.xcb[(size_t)15 * nx + xidx(g, j, i)];
+        if (i + 1 >= 0 && i + 1 <= mx + 2 && adj_active(A, i + 1, j)) bb += A.xcb[(size_t)14 * nx + xidx(g, j, i + 1)];
+        if (i >= 0 && i <= mx + 2 && adj_active(A, i, j)) bb += A.xcb[(size_t)15 * nx + xidx(g, j, i)];
     }
     if (i >= 0 && i <= mx + 1) {
-        if (j + 1 >= 0 && j + 1 <= my + 2) bb += A.ycb[(size_t)14 * ny + yidx(g, j + 1, i)];
-        if (j >= 0 && j <= my + 2) bb += A.ycb[(size_t)15 * ny + yidx(g, j, i)];
+        if (j + 1 >= 0 && j + 1 <= my + 2 && adj_active(A, i, j + 1)) bb += A.ycb[(size_t)14 * ny + yidx(g, j + 1, i)];
+        if (j >= 0 && j <= my + 2 && adj_active(A, i, j)) bb += A.ycb[(size_t)15 * ny + yidx(g, j, i)];
     }
-    bb += A.tdq[(size_t)9 * np + pi];
-    if (i + 1 <= mx + 2) bb += A.tdq[(size_t)10 * np + pidx(g, i + 1, j)];
-    if (i - 1 >= -1) bb += A.tdq[(size_t)11 * np + pidx(g, i - 1, j)];
-    if (j + 1 <= my + 2) bb += A.tdq[(size_t)12 * np + pidx(g, i, j + 1)];
-    if (j - 1 >= -1) bb += A.tdq[(size_t)13 * np + pidx(g, i, j - 1)];
+    if (adj_active(A, i, j)) bb += A.tdq[(size_t)9 * np + pi];
+    if (i + 1 <= mx + 2 && adj_active(A, i + 1, j)) bb += A.tdq[(size_t)10 * np + pidx(g, i + 1, j)];
+    if (i - 1 >= -1 && adj_active(A, i - 1, j)) bb += A.tdq[(size_t)11 * np + pidx(g, i - 1, j)];
+    if (j + 1 <= my + 2 && adj_active(A, i, j + 1)) bb += A.tdq[(size_t)12 * np + pidx(g, i, j + 1)];
+    if (j - 1 >= -1 && adj_active(A, i, j - 1)) bb += A.tdq[(size_t)13 * np + pidx(g, i, j - 1)];
     A.qsb[(size_t)5 * np + pi] = bb;
 }
 
@@ -2025,7 +2037,8 @@ DC_HD void adj_item_gather_bed(const Geom& g, const AdjWork& A, const Work& W, d
     if (j == my) { cj[nj++] = my + 1; cj[nj++] = my + 2; }
     double s = 0.0;
     for (int b = 0; b < nj; ++b)
-        for (int a = 0; a < ni; ++a) s += A.qsb[(size_t)5 * W.npad + pidx(g, ci[a], cj[b])];
+        for (int a = 0; a < ni; ++a)
+            if (adj_active(A, ci[a], cj[b])) s += A.qsb[(size_t)5 * W.npad + pidx(g, ci[a], cj[b])];
     bbar[(size_t)(j - 1) * mx + (size_t)(i - 1)] += s;
 }
 

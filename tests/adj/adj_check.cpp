@@ -433,6 +433,7 @@ int adj_step_vjp(const dclaw_params* P, int mx, int my, double dx, double dy, co
     std::vector<double> lamq(5 * (size_t)mx * my), xfb(NFB * W.nxi), yfb(NFB * W.nyi), xcb(NCB * W.nxi),
         ycb(NCB * W.nyi), tdq(NTD * W.npad), qsb(NQSB * W.npad), sv(NSV * W.npad);
     AdjWork A{lamq.data(), xfb.data(), yfb.data(), xcb.data(), ycb.data(), tdq.data(), qsb.data(), sv.data()};
+    A.bed = bbar != nullptr;
     for (int j = -1; j <= my + 2; ++j)
         for (int i = -1; i <= mx + 2; ++i) adj_item_svrec(*P, g, W, A, i, j);
     for (int j = 1; j <= my; ++j)
