@@ -560,14 +560,19 @@ class EnsembleStepAdjoint:
             _lib.check(int(st), f"ensemble adjoint, member {k}")
 
 
-def _ensemble(members, theta, fixed_dt: bool):
+def _ensemble(members, theta, fixed_dt: bool, bed: torch.Tensor | None = None):
     from .ensemble import EnsembleStepper, Member
 
     th = theta.detach().cpu().tolist()
     mem = [Member(m.q, m.b, with_theta(m.params, th[k]), m.dx, m.dy, m.dt_initial, m.t_final,
                   getattr(m, "t_obs", 0.0))
            for k, m in enumerate(members)]
-    return EnsembleStepper(mem, theta.device, fixed_dt=fixed_dt)
+    st = EnsembleStepper(mem, theta.device, fixed_dt=fixed_dt)
+    if bed is not None:
+        if bed.shape != st.bed.shape:
+            raise ValueError(f"bed must be the ensemble's bed arena, shape {tuple(st.bed.shape)}")
+        st.bed.copy_(bed.detach())
+    return st
 
 
 def _clock_field(st, k: int) -> torch.Tensor:
@@ -579,8 +584,9 @@ def _clock_field(st, k: int) -> torch.Tensor:
 class _EnsembleRollout(torch.autograd.Function):
     @staticmethod
     def forward(ctx, q0, theta, members, n_steps, out_steps, checkpoint_block, fixed_dt, dt_schedule, select,
-                n_obs):
-        st = _ensemble(members, theta, fixed_dt or dt_schedule is not None)
+                n_obs, bed):
+        st = _ensemble(members, theta, fixed_dt or dt_schedule is not None, bed)
+        ctx.bed = None if bed is None else bed.detach()
         st.qa.copy_(q0.detach())
         lib = _lib.load()
         reserve = 2 * sum(lib.dclaw_adjoint_workspace_bytes(m.q.shape[2], m.q.shape[1]) for m in members)
@@ -659,8 +665,10 @@ class _EnsembleRollout(torch.autograd.Function):
         where = {}
         for idx, n in enumerate(out_steps):
             where.setdefault(n, []).append(idx)
-        fw = _ensemble(members, theta, True)
+        fw = _ensemble(members, theta, True, ctx.bed)
         adjs = [EnsembleStepAdjoint(fw), EnsembleStepAdjoint(fw)]
+        # the bed arena's gradient, when the run was given one that requires grad
+        bbar = torch.zeros_like(fw.bed) if ctx.bed is not None and ctx.needs_input_grad[10] else None
         lam = torch.zeros_like(fw.qa)
         lam2 = torch.zeros_like(lam)   # arena gaps between members stay zero
         pbar = torch.zeros((fw.n, 4), dtype=torch.float64, device=dev)
@@ -697,19 +705,20 @@ class _EnsembleRollout(torch.autograd.Function):
                 src = buf[n - n0]
 
         lam, lam2 = _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, lambda n: dts[n - 1], lam, lam2,
-                                        pbar, add_outs)
+                                        pbar, add_outs, None, bbar)
         add_outs(0, lam)
         for kk, st in enumerate(fw.status()):
             _lib.check(st, f"ensemble recompute, member {kk}")
         for adj in adjs:
             adj.check_status()
         scale = torch.tensor([_DEG, 1.0, 1.0, 1.0], dtype=torch.float64, device=dev)
-        return lam, pbar * scale, None, None, None, None, None, None, None, None
+        return lam, pbar * scale, None, None, None, None, None, None, None, None, bbar
 
 
 def ensemble_rollout_states(q0: torch.Tensor, theta: torch.Tensor, members, n_steps: int, out_steps,
                             checkpoint_block: int | None = None, fixed_dt: bool = False,
-                            dt_schedule: torch.Tensor | None = None, select: torch.Tensor | None = None) -> torch.Tensor:
+                            dt_schedule: torch.Tensor | None = None, select: torch.Tensor | None = None,
+                            bed: torch.Tensor | None = None) -> torch.Tensor:
     """Differentiable run of an ensemble (the batched form of `rollout_states`).
 
     members: list of `ensemble.Member` (bed, parameters, spacing, first dt;
@@ -722,7 +731,9 @@ def ensemble_rollout_states(q0: torch.Tensor, theta: torch.Tensor, members, n_st
     CUDA tensor of arena indices): return only these entries per output
     step (gauges) instead of whole arenas. The backward pass runs the
     batched step adjoint with time checkpointing (block length as in
-    `rollout_states`).
+    `rollout_states`). bed (optional): the bed arena (an `EnsembleStepper`'s
+    `bed` layout) to step over instead of the members' beds; when it
+    requires grad it gets every member's bed gradient.
     """
     for n in out_steps:
         if not 0 <= n <= n_steps:
@@ -730,12 +741,13 @@ def ensemble_rollout_states(q0: torch.Tensor, theta: torch.Tensor, members, n_st
     if dt_schedule is not None and dt_schedule.shape != (n_steps, len(members)):
         raise ValueError("dt_schedule must be (n_steps, n_members)")
     return _EnsembleRollout.apply(q0, theta, list(members), int(n_steps), tuple(int(n) for n in out_steps),
-                                  checkpoint_block, bool(fixed_dt), dt_schedule, select, 0)
+                                  checkpoint_block, bool(fixed_dt), dt_schedule, select, 0, bed)
 
 
 def ensemble_rollout_observations(q0: torch.Tensor, theta: torch.Tensor, members, n_steps: int, n_obs: int,
                                   select: torch.Tensor, checkpoint_block: int | None = None,
-                                  dt_schedule: torch.Tensor | None = None) -> torch.Tensor:
+                                  dt_schedule: torch.Tensor | None = None,
+                                  bed: torch.Tensor | None = None) -> torch.Tensor:
     """The batched form of `rollout_observations`, the particle filter's
     vmapped flume loop (pf_flume/inference.py:96-108 over
     pf_flume/flume_model.py:150-158): every member steps with its own tick
@@ -751,7 +763,7 @@ def ensemble_rollout_observations(q0: torch.Tensor, theta: torch.Tensor, members
     if dt_schedule is not None and dt_schedule.shape != (n_steps, len(members)):
         raise ValueError("dt_schedule must be (n_steps, n_members)")
     return _EnsembleRollout.apply(q0, theta, list(members), int(n_steps), (), checkpoint_block, False,
-                                  dt_schedule, select, int(n_obs))
+                                  dt_schedule, select, int(n_obs), bed)
 
 
 def ensemble_last_dts(out: torch.Tensor) -> torch.Tensor:

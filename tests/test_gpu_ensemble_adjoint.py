@@ -172,3 +172,34 @@ def test_ensemble_observations_match_single_patch(cuda_device):
         off, c = ens.cm[k].q_off, m.q.size
         assert torch.equal(q0.grad[off:off + c].view(m.q.shape), qk.grad), f"member {k}: state gradient"
         _close_params(theta.grad[k], tk.grad, f"member {k}: parameter gradient")
+
+
+def test_ensemble_bed_gradient_matches_single_patch(cuda_device):
+    """A bed arena that requires grad: each member's bed gradient from the
+    batched adjoint equals rollout_states' on the member alone, bit for bit,
+    and stepping over the given arena equals stepping over the members'
+    own beds."""
+    dev = cuda_device
+    members = _advance(_members(seed=6), dev, n=6)
+    ens = EnsembleStepper(members, dev)
+    n, outs = 10, [4, 10]
+    rng = np.random.default_rng(5)
+    wts = torch.tensor(rng.standard_normal((len(outs), ens.qa.numel())), device=dev)
+    q0 = ens.qa.clone().requires_grad_(True)
+    theta = torch.stack([theta_of(m.params, dev) for m in members])
+    bed = ens.bed.clone().requires_grad_(True)
+    o = ensemble_rollout_states(q0, theta, members, n, outs, checkpoint_block=4, bed=bed)
+    o_plain = ensemble_rollout_states(ens.qa.clone(), theta, members, n, outs, checkpoint_block=4)
+    assert torch.equal(o.detach(), o_plain.detach())
+    (o * wts).sum().backward()
+    assert bed.grad is not None and bed.grad.abs().max() > 0
+    for k, m in enumerate(members):
+        off, c = ens.cm[k].q_off, m.q.size
+        ob, cb = ens.cm[k].b_off, m.b.size
+        qk = torch.tensor(m.q, device=dev, requires_grad=True)
+        bk = torch.tensor(m.b, device=dev, requires_grad=True)
+        ok = rollout_states(qk, theta_of(m.params, dev), bk, m.params, m.dx, m.dy, n, outs, m.dt_initial,
+                            checkpoint_block=3)
+        (ok * wts[:, off:off + c].view((len(outs),) + m.q.shape)).sum().backward()
+        assert torch.equal(bed.grad[ob:ob + cb].view(m.b.shape), bk.grad), f"member {k}: bed gradient"
+        assert torch.equal(q0.grad[off:off + c].view(m.q.shape), qk.grad), f"member {k}: state gradient"
