@@ -59,22 +59,29 @@ def parse():
     ap.add_argument("--dx", type=float, default=0.5)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=0,
+                    help="timed oracle steps of the CPU baseline (0: --steps, the reference arm's sample)")
     ap.add_argument("--cpu-band-rows", type=int, default=256,
                     help="rows of the one-thread CPU sample (one step)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--json-out", default="")
     ap.add_argument("--ensemble-members", type=int, default=256,
                     help="members of the batched flume ensemble measured beside the plain step (0: skip)")
-    ap.add_argument("--ensemble-steps", type=int, default=10)
+    ap.add_argument("--ensemble-steps", type=int, default=2000,
+                    help="steps of the batched ensemble run (the case is defined over 2000)")
+    ap.add_argument("--ensemble-window", type=int, default=10,
+                    help="steps of the batched-vs-looped comparison windows (early and late in the run)")
     ap.add_argument("--grad-steps", type=int, default=500,
                     help="steps of the 512 x 512 gradient case measured beside the plain step (0: skip)")
     ap.add_argument("--checkpoint-block", type=int, default=0,
                     help="0: the smallest block whose checkpoints fit half of the free device memory")
     ap.add_argument("--bgrad-members", type=int, default=64,
                     help="members of the batched-gradient channel case (0: skip)")
-    ap.add_argument("--bgrad-steps", type=int, default=200,
+    ap.add_argument("--bgrad-steps", type=int, default=800,
                     help="steps of the batched-gradient case (the case is defined over 800)")
+    ap.add_argument("--full-steps", type=int, default=200,
+                    help="steps of the whole-run leg of the plain case from its initial state "
+                         "(the case is defined over 200; 0: skip)")
     ap.add_argument("--slab-steps", type=int, default=0,
                     help="also step ONE patch of the case split into row slabs over the N ranks "
                          "(strong scaling; halo exchange + Courant max per step); 0: skip")
@@ -158,23 +165,53 @@ def make_case(args, rank=0):
     return W.random_field_case(n=args.size, dx=args.dx, seed=replica_seed(args.seed, rank))
 
 
-def cpu_baseline(args, case, steps):
-    """Oracle (CPU restatement) on `steps` full steps of the same case."""
-    import numpy as np
+def workload_config(case, world=1):
+    """The `config` object of both arms (the same keys and values)."""
+    cells = case.mx * case.my
+    return {"workload": f"random_field_{case.mx}x{case.my}_dx{case.dx}", "cells_per_gpu": cells,
+            "parallelism": f"replicas{world}",
+            "l2": f"state {40 * cells / 1e6:.0f} MB {'>' if 40 * cells > 126e6 else '<'} L2 (126 MB), no flush",
+            "order": case.params.order, "transverse_waves": case.params.transverse_waves, "limiter": "MC"}
 
+
+def oracle_sample(case, warmup, steps):
+    """The CPU sample both arms time: the oracle (the CPU restatement of the
+    reference Fortran, OpenMP over all host cores) advances the case by
+    `warmup` untimed steps from its initial state, then `steps` timed full
+    steps from there. Returns (cell-updates/s, seconds, cores, status)."""
     from oracle import Oracle
 
     o = Oracle()
     cores = o.threads(os.cpu_count() or 1)
+    q, dt = case.q, case.dt_initial
+    if warmup:
+        r = o.run(case.params, case.q, case.b, case.dx, case.dy, warmup, case.dt_initial, parallel=True)
+        # the timed steps continue from the warm-up state, starting at the
+        # warm-up's last dt
+        q, dt = r["q"], float(r["dt"][-1])
     t0 = time.perf_counter()
-    r = o.run(case.params, case.q, case.b, case.dx, case.dy, steps, case.dt_initial, parallel=True)
+    r2 = o.run(case.params, q, case.b, case.dx, case.dy, steps, dt, parallel=True)
     el = time.perf_counter() - t0
-    cells = case.mx * case.my * steps
-    out = {"value": cells / el, "unit": "cell-updates/s", "cores": cores, "kind": "port",
-           "sample": f"first {steps} steps of the {case.mx}x{case.my} workload from its initial state "
-                     f"({el:.1f} s, OpenMP, oracle/dclaw_oracle.cpp)", "status": r["status"]}
-    # one thread, on a band of rows of the same field (the same band, all
-    # threads, beside it for the scaling)
+    return case.mx * case.my * steps / el, el, cores, r2["status"]
+
+
+def oracle_sample_text(case, warmup, steps, el):
+    return (f"steps {warmup + 1}..{warmup + steps} of the {case.mx}x{case.my} workload ({warmup} untimed warm-up "
+            f"steps from its initial state, then {steps} timed full steps, {el:.1f} s; oracle/dclaw_oracle.cpp, "
+            f"OpenMP)")
+
+
+def cpu_baseline(args, case, warmup, steps):
+    """The reference arm's sample (oracle_sample) timed on this box, and a
+    one-thread figure on a band of rows of the same field beside it."""
+    import numpy as np
+
+    from oracle import Oracle
+
+    v, el, cores, status = oracle_sample(case, warmup, steps)
+    out = {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+           "sample": oracle_sample_text(case, warmup, steps, el), "status": status}
+    o = Oracle()
     band = min(case.my, max(1, args.cpu_band_rows))
     qb, bb = np.ascontiguousarray(case.q[:, :band, :]), np.ascontiguousarray(case.b[:band, :])
     timing = {}
@@ -196,54 +233,43 @@ def run_reference(args):
     if rank != 0:
         return
     case = make_case(args)
-    from oracle import Oracle
-
-    o = Oracle()
-    cores = o.threads(os.cpu_count() or 1)
-    # warm-up steps advance the state; the timed steps continue from it
-    r = o.run(case.params, case.q, case.b, case.dx, case.dy, args.warmup, case.dt_initial, parallel=True)
-    dt_next = float(r["dt"][-1]) if args.warmup else case.dt_initial
-    t0 = time.perf_counter()
-    r2 = o.run(case.params, r["q"], case.b, case.dx, case.dy, args.steps, dt_next, parallel=True)
-    el = time.perf_counter() - t0
-    cells = case.mx * case.my * args.steps
-    v = cells / el
+    v, el, cores, status = oracle_sample(case, args.warmup, args.steps)
     line = {"metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": f"random_field_{case.mx}x{case.my}_dx{case.dx}", "steps_per_sample": 1,
-                       "threads": cores},
+            "impl": "reference", "config": workload_config(case, args.gpus),
             "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port",
-                             "sample": f"{args.steps} full steps of the {case.mx}x{case.my} workload after "
-                                       f"{args.warmup} warm-up steps (oracle/dclaw_oracle.cpp, OpenMP)"},
+                             "sample": oracle_sample_text(case, args.warmup, args.steps, el)},
             "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "status": r2["status"]}
+            "status": status}
     print(json.dumps(line), flush=True)
 
 
 def ensemble_bench(args, dev):
     """Batched flume ensemble (uneven channels, per-member parameters and dt)
-    against looping the plain patch step over its members. Both forms run the
-    same members from the same state for the same number of steps; the
-    batched form replays one captured CUDA graph of the persistent ensemble
-    kernels after autotuning, the looped form calls the plain step member by
-    member (eagerly, and captured into one CUDA graph of all its launches)."""
+    over its whole run (--ensemble-steps, 2000 by default, from the initial
+    state), replayed from one captured CUDA graph of the persistent ensemble
+    kernels after autotuning. Beside it, two windows of --ensemble-window
+    steps -- the first steps of the run and the last ones, where the flows
+    have spread -- are also run by looping the plain patch step over the
+    members from the same states and clocks (eagerly, and captured into one
+    CUDA graph of all its launches)."""
     import torch
 
     from dclaw_b200 import workloads as W
     from dclaw_b200.ensemble import EnsembleStepper, Member
+    from dclaw_b200.params import CLOCK_DOUBLES
     from dclaw_b200.solver import PatchStepper
 
-    K = max(2, args.ensemble_steps + args.ensemble_steps % 2)
+    K = max(2, args.ensemble_window + args.ensemble_window % 2)
+    nrep = max(2, -(-args.ensemble_steps // K))
+    N = nrep * K
     cases = W.flume_ensemble(n=args.ensemble_members, seed=args.seed)
     members = [Member(c.q, c.b, c.params, c.dx, c.dy, c.dt_initial) for c in cases]
     cells = sum(c.mx * c.my for c in cases)
     ens = EnsembleStepper(members, dev)
-    tune = ens.autotune(steps=2)
-    ens.step(args.warmup)
+    tune = ens.autotune(steps=2)      # leaves the state and clocks at the start
     ens.capture(K)
-    ens.replay(1)
     torch.cuda.synchronize()
 
     def timed(fn):
@@ -256,46 +282,72 @@ def ensemble_bench(args, dev):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    ms_b = timed(lambda: ens.replay(1))
+    def snapshot():
+        return ([ens.state(k).clone() for k in range(ens.n)], ens.clocks.view(ens.n, CLOCK_DOUBLES).clone())
+
+    snap_early = snapshot()
+    ms_early = timed(lambda: ens.replay(1))
+    ms_mid = timed(lambda: ens.replay(nrep - 2))
+    snap_late = snapshot()
+    ms_late = timed(lambda: ens.replay(1))
     status_b = ens.status()
+    ms_run = ms_early + ms_mid + ms_late
+    beds = [torch.from_numpy(m.b).to(dev) for m in members]
     del ens
-    steppers = []
-    for m in members:
-        ps = PatchStepper(torch.from_numpy(m.q).to(dev), torch.from_numpy(m.b).to(dev), m.params, m.dx, m.dy)
-        ps.init_clock(m.dt_initial)
-        steppers.append(ps)
-    for _ in range(args.warmup):
-        for ps in steppers:
-            ps.step(1)
+    torch.cuda.empty_cache()
 
-    def loop_eager():
-        for _ in range(K):
-            for ps in steppers:
-                ps.step(1)
+    def looped(snap):
+        states, clocks = snap
+        steppers = []
+        for k, m in enumerate(members):
+            ps = PatchStepper(states[k], beds[k], m.params, m.dx, m.dy)
+            ps.clock.copy_(clocks[k])
+            steppers.append(ps)
 
-    ms_le = timed(loop_eager)
-    s = torch.cuda.Stream()
-    s.wait_stream(torch.cuda.current_stream())
-    g = torch.cuda.CUDAGraph()
-    with torch.cuda.stream(s):
-        with torch.cuda.graph(g, stream=s):
-            for _ in range(K // 2):
+        def reset():
+            for k, ps in enumerate(steppers):
+                ps.qa.copy_(states[k])
+                ps.clock.copy_(clocks[k])
+
+        def loop_eager():
+            for _ in range(K):
                 for ps in steppers:
-                    ps._launch(ps.qa, ps.qb)
-                for ps in steppers:
-                    ps._launch(ps.qb, ps.qa)
-    torch.cuda.current_stream().wait_stream(s)
-    g.replay()
-    ms_lg = timed(g.replay)
-    del g
-    v_b = cells * K / (ms_b / 1000.0)
+                    ps.step(1)
+
+        ms_le = timed(loop_eager)
+        reset()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                for _ in range(K // 2):
+                    for ps in steppers:
+                        ps._launch(ps.qa, ps.qb)
+                    for ps in steppers:
+                        ps._launch(ps.qb, ps.qa)
+        torch.cuda.current_stream().wait_stream(s)
+        reset()
+        ms_lg = timed(g.replay)
+        del g, steppers
+        torch.cuda.empty_cache()
+        return ms_le, ms_lg
+
+    def window(first, ms_b, snap):
+        ms_le, ms_lg = looped(snap)
+        return {"steps": [first + 1, first + K], "batched_ms_per_step": ms_b / K,
+                "batched_value": cells * K / (ms_b / 1000.0),
+                "looped_eager_ms_per_step": ms_le / K, "looped_graph_ms_per_step": ms_lg / K,
+                "vs_looped_eager": ms_le / ms_b, "vs_looped_graph": ms_lg / ms_b}
+
+    early = window(0, ms_early, snap_early)
+    late = window(N - K, ms_late, snap_late)
     return {"workload": f"flume_ensemble_{len(members)}_dx0.05", "members": len(members), "cells": cells,
-            "steps": K, "value": v_b, "unit": "cell-updates/s", "ms_per_step": ms_b / K,
-            "looped_eager": {"value": cells * K / (ms_le / 1000.0), "ms_per_step": ms_le / K},
-            "looped_graph": {"value": cells * K / (ms_lg / 1000.0), "ms_per_step": ms_lg / K},
-            "vs_looped_eager": ms_le / ms_b, "vs_looped_graph": ms_lg / ms_b,
+            "steps": N, "value": cells * N / (ms_run / 1000.0), "unit": "cell-updates/s", "ms_per_step": ms_run / N,
+            "note": "the whole run from the initial state, one graph of the ensemble step replayed",
+            "early_window": early, "late_window": late,
             "autotune": {k: tune[k] for k in ("tile_shape", "tile_ctas_per_sm", "ms")},
-            "gpu_launches": 6 * K, "status_nonzero": sum(1 for x in status_b if x)}
+            "gpu_launches": 6 * N, "status_nonzero": sum(1 for x in status_b if x)}
 
 
 def gradient_bench(args, dev):
@@ -616,26 +668,44 @@ def run_ours(args):
         f1.record(stream)
         barrier()
         e2e_serial_ms = max_over_ranks(f0.elapsed_time(f1), dev)
-        # the floor: the same bytes copied both ways at once, nothing else
+        # a lower bound: the state's upload alone and its download alone,
+        # whole-state copies with nothing else running; the step moves both,
+        # so it cannot take less than the slower of the two
         qh2 = torch.empty_like(qh).pin_memory()
-        up, down = torch.cuda.Stream(), torch.cuda.Stream()
-        barrier()
-        f0.record(stream)
-        for _ in range(args.e2e_steps):
-            up.wait_stream(stream)
-            down.wait_stream(stream)
-            with torch.cuda.stream(up):
-                st.qa.copy_(qh, non_blocking=True)
-            with torch.cuda.stream(down):
-                qh2.copy_(st.qb, non_blocking=True)
-            stream.wait_stream(up)
-            stream.wait_stream(down)
-        f1.record(stream)
-        barrier()
-        copy_floor_ms = max_over_ranks(f0.elapsed_time(f1), dev)
+        one_way = {}
+        for name, fn in (("h2d", lambda: st.qb.copy_(qh, non_blocking=True)),
+                         ("d2h", lambda: qh2.copy_(st.qb, non_blocking=True))):
+            fn()
+            barrier()
+            f0.record(stream)
+            for _ in range(args.e2e_steps):
+                fn()
+            f1.record(stream)
+            barrier()
+            one_way[name] = max_over_ranks(f0.elapsed_time(f1), dev) / args.e2e_steps
         del qh2
         h2d = qh.numel() * 8
         d2h = qh.numel() * 8 + cfl_h.numel() * 8
+
+    # ---- the case over its whole stated run, from its initial state ----
+    full = None
+    if args.full_steps > 0:
+        fs = PatchStepper(torch.tensor(case.q, device=dev), b, case.params, case.dx, case.dy)
+        fs.init_clock(case.dt_initial)
+        barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        fs.step(args.full_steps)
+        f1.record(stream)
+        barrier()
+        full_ms = max_over_ranks(f0.elapsed_time(f1), dev)
+        full = {"steps": args.full_steps, "value": cells * args.full_steps * world / (full_ms / 1000.0),
+                "unit": "cell-updates/s", "ms_per_step": full_ms / args.full_steps,
+                "t_end": fs.read_clock().t, "wet_fraction_end": float((fs.state()[0] > 0).double().mean()),
+                "status": fs.status(),
+                "note": "steps 1..N of the case from its initial state (no warm-up steps on the state)"}
+        del fs
 
     peak, peak_kind = load_peaks()
     achieved = BYTES_PER_CELL_UPDATE * cells / (ms / 1000.0 / args.steps) / 1e9
@@ -644,17 +714,15 @@ def run_ours(args):
         out = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": {"workload": f"random_field_{case.mx}x{case.my}_dx{case.dx}",
-                          "cells_per_gpu": cells, "parallelism": f"replicas{world}",
-                          "l2": f"state {40 * cells / 1e6:.0f} MB {'>' if 40 * cells > 126e6 else '<'} L2 (126 MB),"
-                                f" no flush", "order": case.params.order,
-                          "transverse_waves": case.params.transverse_waves, "limiter": "MC"},
+               "config": workload_config(case, world),
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": NCU_STEP_BYTES_2048 * cells / 2048 ** 2,
                             "traffic_note": "bytes per step from the ncu capture at 2048^2, scaled by cells",
                             "kernel": "fused step k_records + k_tile + k_src2_cells (88 B/cell-update algorithmic)",
                             "peak_source": peak_kind},
-               "clocks": clocks, "gpu_launches": 3 * args.steps, "status": status}
+               "clocks": clocks, "gpu_launches": 5 * args.steps, "status": status}
+        if full is not None:
+            out["full_run"] = full
         if e2e_ms is not None:
             out["e2e"] = {"value": cells * args.e2e_steps * world / (e2e_ms / 1000.0), "unit": "cell-updates/s",
                           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.e2e_steps,
@@ -662,10 +730,12 @@ def run_ours(args):
                                  "step, copies pipelined by bands of tile rows",
                           "serial_copies_value": cells * args.e2e_steps * world / (e2e_serial_ms / 1000.0),
                           "serial_copies_note": "whole-state copy in, PatchStepper.step, whole-state copy out",
-                          "copy_floor_ms_per_step": copy_floor_ms / args.e2e_steps,
-                          "frac_of_copy_floor": copy_floor_ms / e2e_ms,
-                          "copy_floor_note": "the state copied host->device and device->host at once on two "
-                                             "streams, no compute: the PCIe bound of the e2e step"}
+                          "copy_bound_ms_per_step": max(one_way.values()),
+                          "h2d_alone_ms": one_way["h2d"], "d2h_alone_ms": one_way["d2h"],
+                          "frac_of_copy_bound": max(one_way.values()) / (e2e_ms / args.e2e_steps),
+                          "copy_bound_note": "the slower of the state's upload alone and its download alone "
+                                             "(whole-state copies, nothing else running): a lower bound on a "
+                                             "step that moves both"}
     if args.slab_steps > 0:
         sl = slab_bench(args, dev, rank, world, barrier)
         if rank == 0:
@@ -681,7 +751,7 @@ def run_ours(args):
     if rank == 0 and world == 1 and args.bgrad_members > 0 and args.bgrad_steps > 0:
         out["batched_gradient"] = batched_gradient_bench(args, dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(args, case, args.cpu_steps)
+        out["cpu_baseline"] = cpu_baseline(args, case, args.warmup, args.cpu_steps or args.steps)
     if rank == 0:
         print(json.dumps(out), flush=True)
         if args.json_out:

@@ -586,7 +586,6 @@ class _EnsembleRollout(torch.autograd.Function):
     def forward(ctx, q0, theta, members, n_steps, out_steps, checkpoint_block, fixed_dt, dt_schedule, select,
                 n_obs, bed):
         st = _ensemble(members, theta, fixed_dt or dt_schedule is not None, bed)
-        ctx.bed = None if bed is None else bed.detach()
         st.qa.copy_(q0.detach())
         lib = _lib.load()
         reserve = 2 * sum(lib.dclaw_adjoint_workspace_bytes(m.q.shape[2], m.q.shape[1]) for m in members)
@@ -639,7 +638,10 @@ class _EnsembleRollout(torch.autograd.Function):
                                                 _lib.ptr(obs_step), _lib.stream_ptr()), "observation record")
         for kk, s in enumerate(st.status()):
             _lib.check(s, f"ensemble rollout, member {kk}")
-        ctx.save_for_backward(dts, store)
+        # the bed goes through save_for_backward (None when absent) so that an
+        # in-place change between forward and backward raises autograd's
+        # version error instead of silently changing the recompute
+        ctx.save_for_backward(dts, store, bed)
         ctx.select = select
         ctx.meta = (members, theta.detach(), int(n_steps), tuple(out_steps), k)
         ctx.obs_steps = None
@@ -658,17 +660,18 @@ class _EnsembleRollout(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g_out):
-        dts, store = ctx.saved_tensors
+        dts, store, bed = ctx.saved_tensors
+        bed = None if bed is None else bed.detach()
         ckpt = list(store.unbind(0))
         members, theta, n_steps, out_steps, k = ctx.meta
         dev = dts.device
         where = {}
         for idx, n in enumerate(out_steps):
             where.setdefault(n, []).append(idx)
-        fw = _ensemble(members, theta, True, ctx.bed)
+        fw = _ensemble(members, theta, True, bed)
         adjs = [EnsembleStepAdjoint(fw), EnsembleStepAdjoint(fw)]
         # the bed arena's gradient, when the run was given one that requires grad
-        bbar = torch.zeros_like(fw.bed) if ctx.bed is not None and ctx.needs_input_grad[10] else None
+        bbar = torch.zeros_like(fw.bed) if bed is not None and ctx.needs_input_grad[10] else None
         lam = torch.zeros_like(fw.qa)
         lam2 = torch.zeros_like(lam)   # arena gaps between members stay zero
         pbar = torch.zeros((fw.n, 4), dtype=torch.float64, device=dev)

@@ -9,6 +9,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "stages.cuh"
@@ -24,6 +25,11 @@ constexpr int TPB = 256;
 #endif
 constexpr int TILE_TPB = DCLAW_TILE_TPB;
 constexpr int MAX_DEVICES = 64;
+// One-time per-device set-up (function attributes, the SM count, symbol
+// addresses) is filled under this lock and published through atomics, so
+// host threads making their first calls on a device at the same time do not
+// race on the caches.
+static std::mutex g_setup_mu;
 // tile of the fused step: with 16 x 14 the flux phases of k_tile fit in one
 // round of 256 threads (256 and 252 cells) and the solves in two
 #ifndef DCLAW_TILE_X
@@ -515,6 +521,126 @@ __global__ void __launch_bounds__(SRC2_TPB, SRC2_MINB) k_src2_cells(dclaw_params
     if (tick) last_block_tick(P, clk);
 }
 
+// ---- single patch over tile lists -------------------------------------------
+// dclaw_step without a branch log: the records, tiles and src2 run only
+// where the flow is. (1) k_scan_patch reads every interior cell's five
+// fields (the NaN check), marks the tiles whose read range holds a wet cell
+// and writes the zero state into q_out; (2) k_list_patch lists the active
+// tiles and the tiles that are active or next to one; (3) k_records_list
+// builds the records of the second list's tiles (every record an active tile
+// reads, once); (4) k_tile_list, a persistent kernel, takes the active tiles
+// from a queue; (5) k_src2_list overwrites the zeros of the active tiles'
+// cells with src2 of the updated state, and its last block applies the tick.
+// Each cell's arithmetic is that of the full-grid kernels, so the results
+// are the same bits; far from the flow a cell costs its 80 bytes of scan.
+__global__ void __launch_bounds__(TPB, DCLAW_SCAN_MINB) k_scan_patch(dclaw_params P, int mx, int my,
+                                                                    const double* __restrict__ q_in,
+                                                                    double* __restrict__ q_out, dclaw_clock* clk,
+                                                                    unsigned int* counters,
+                                                                    uint32_t* __restrict__ tflag) {
+    if (blockIdx.x == 0 && threadIdx.x < 3) counters[threadIdx.x] = 0u;  // tile queue and list lengths
+    const size_t n = (size_t)mx * my;
+    const int ntx = (mx + TILE_X - 1) / TILE_X, nty = (my + TILE_Y - 1) / TILE_Y;
+    bool nan = false;
+    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+        if (scan_cell(P, q_in, n, idx, mx, tflag, clk, TILE_X, TILE_Y, ntx, nty)) nan = true;
+        for (int f = 0; f < 5; ++f) q_out[(size_t)f * n + idx] = 0.0;
+    }
+    if (nan) flag_status(clk, DCLAW_ERR_NAN);
+}
+
+__global__ void __launch_bounds__(TPB) k_list_patch(int ntx, int nty, const dclaw_clock* clk,
+                                                    const uint32_t* __restrict__ tflag, unsigned int* counters,
+                                                    uint32_t* __restrict__ list_act, uint32_t* __restrict__ list_rec) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t ntiles = (uint32_t)ntx * (uint32_t)nty;
+    const uint32_t epoch = clk->nsteps + 1u;
+    bool act = false, rec = false;
+    if (t < ntiles) {
+        act = tflag[t] == epoch;
+        rec = act || near_active(tflag, epoch, (int)(t % ntx), (int)(t / ntx), ntx, nty);
+    }
+    const int lane = threadIdx.x & 31;
+    const unsigned ba = __ballot_sync(0xffffffffu, act), br = __ballot_sync(0xffffffffu, rec);
+    unsigned base_a = 0, base_r = 0;
+    if (lane == 0) {
+        if (ba) base_a = atomicAdd(counters + 1, (unsigned)__popc(ba));
+        if (br) base_r = atomicAdd(counters + 2, (unsigned)__popc(br));
+    }
+    base_a = __shfl_sync(0xffffffffu, base_a, 0);
+    base_r = __shfl_sync(0xffffffffu, base_r, 0);
+    const unsigned below = (1u << lane) - 1u;
+    if (act) list_act[base_a + __popc(ba & below)] = t;
+    if (rec) list_rec[base_r + __popc(br & below)] = t;
+}
+
+__global__ void __launch_bounds__(TPB, DCLAW_PLAIN_CELL_MINB) k_records_list(dclaw_params P, Geom g,
+                                                                            const double* __restrict__ q_in,
+                                                                            const double* __restrict__ b, Rec R,
+                                                                            const unsigned int* counters,
+                                                                            const uint32_t* __restrict__ list_rec) {
+    const uint32_t n = counters[2];
+    const int ntx = (g.mx + TILE_X - 1) / TILE_X, nty = (g.my + TILE_Y - 1) / TILE_Y;
+    for (uint32_t k = blockIdx.x; k < n; k += gridDim.x) {
+        const uint32_t t = list_rec[k];
+        tile_records<TILE_X, TILE_Y>(P, g, q_in, b, R, (int)(t % ntx), (int)(t / ntx), ntx, nty);
+    }
+}
+
+// persistent: each CTA takes active tiles from the queue until it is empty;
+// the Courant number is max-reduced once per CTA at the end
+__global__ void __launch_bounds__(TILE_TPB, DCLAW_TILE_MINBLOCKS) k_tile_list(dclaw_params P, Geom g, Rec R,
+                                                                             const double* __restrict__ b,
+                                                                             double* __restrict__ q_star,
+                                                                             dclaw_clock* clk, unsigned int* counters,
+                                                                             const uint32_t* __restrict__ list_act) {
+    extern __shared__ double smem[];
+    __shared__ uint32_t s_t;
+    const unsigned int nact = counters[1];
+    const uint32_t ntx = (uint32_t)((g.mx + TILE_X - 1) / TILE_X);
+    const double dt = clk->dt;
+    double cfl = 0.0;
+    bool nan_any = false;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const unsigned int k = atomicAdd(counters, 1u);
+            s_t = k < nact ? list_act[k] : 0xffffffffu;
+        }
+        __syncthreads();
+        const uint32_t t = s_t;
+        if (t == 0xffffffffu) break;
+        const int i0 = 1 + (int)(t % ntx) * TILE_X, j0 = 1 + (int)(t / ntx) * TILE_Y;
+        bool nan;
+        const double c = tile_body<TILE_X, TILE_Y, false, TILE_TPB>(P, g, R, b, q_star, dt, i0, j0, smem, nullptr, nan);
+        cfl = fmax2(cfl, c);
+        nan_any = nan_any || nan;
+        // the next tile's staging overwrites shared memory and s_t
+        __syncthreads();
+    }
+    if (nan_any) flag_status(clk, DCLAW_ERR_NAN);
+    block_max_to(cfl, reinterpret_cast<unsigned long long*>(&clk->cfl_bits));
+}
+
+__global__ void __launch_bounds__(SRC2_TPB, SRC2_MINB) k_src2_list(dclaw_params P, Geom g,
+                                                                  const double* __restrict__ q_star,
+                                                                  double* __restrict__ q_out, dclaw_clock* clk,
+                                                                  const unsigned int* counters,
+                                                                  const uint32_t* __restrict__ list_act) {
+    const uint32_t nact = counters[1];
+    const uint32_t ntx = (uint32_t)((g.mx + TILE_X - 1) / TILE_X);
+    const double dt = clk->dt;
+    for (uint32_t k = blockIdx.x; k < nact; k += gridDim.x) {
+        const uint32_t t = list_act[k];
+        const int i0 = 1 + (int)(t % ntx) * TILE_X, j0 = 1 + (int)(t / ntx) * TILE_Y;
+        for (int c = threadIdx.x; c < TILE_X * TILE_Y; c += blockDim.x) {
+            const int i = i0 + c % TILE_X, j = j0 + c / TILE_X;
+            if (i > g.mx || j > g.my) continue;
+            cell_src2(P, g, dt, q_star, q_out, (size_t)(j - 1) * g.mx + (size_t)(i - 1));
+        }
+    }
+    last_block_tick(P, clk);
+}
+
 // ---- batched ensemble -------------------------------------------------------
 constexpr int NBATCH_SHAPES = 3;
 __host__ __device__ constexpr int batch_tx(int k) { return k == 0 ? 16 : (k == 1 ? 13 : 16); }
@@ -723,14 +849,17 @@ __global__ void __launch_bounds__(TPB) k_tick_batch(int nmem, const dclaw_params
 
 template <int TX, int TY>
 inline int batch_tile_attr() {
-    static bool done[MAX_DEVICES] = {};
+    static std::atomic<bool> done[MAX_DEVICES];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return DCLAW_ERR_CUDA;
-    if (!done[dev]) {
-        if (cudaFuncSetAttribute(k_tile_batch<TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)TileGeom<TX, TY>::SMEM_BYTES) != cudaSuccess)
-            return DCLAW_ERR_CUDA;
-        done[dev] = true;
+    if (!done[dev].load(std::memory_order_acquire)) {
+        std::lock_guard<std::mutex> lock(g_setup_mu);
+        if (!done[dev].load(std::memory_order_relaxed)) {
+            if (cudaFuncSetAttribute(k_tile_batch<TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)TileGeom<TX, TY>::SMEM_BYTES) != cudaSuccess)
+                return DCLAW_ERR_CUDA;
+            done[dev].store(true, std::memory_order_release);
+        }
     }
     return DCLAW_OK;
 }
@@ -766,11 +895,15 @@ inline int launch_batch_tiles(const dclaw_batch* B, const dclaw_member* mem, con
 }
 
 inline int sm_count() {
-    static int n[MAX_DEVICES] = {};
+    static std::atomic<int> n[MAX_DEVICES];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return 0;
-    if (!n[dev]) cudaDeviceGetAttribute(&n[dev], cudaDevAttrMultiProcessorCount, dev);
-    return n[dev];
+    int v = n[dev].load(std::memory_order_relaxed);
+    if (!v) {
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+        n[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
 }
 
 // ---- patch calls (padded layout) ------------------------------------------
@@ -957,7 +1090,7 @@ inline unsigned src2_blocks(long long n) { return (unsigned)((n + SRC2_TPB - 1) 
 
 struct Layout : StagedLayout {
     size_t total_staged;
-    size_t off_rec, off_qstar, off_tflag, total_fused;
+    size_t off_rec, off_qstar, off_tflag, off_list_act, off_list_rec, off_counters, total_fused;
 };
 
 inline Layout layout(int mx, int my) {
@@ -969,7 +1102,12 @@ inline Layout layout(int mx, int my) {
     L.off_qstar = align256((size_t)NREC * L.npad * 8);
     L.off_tflag = L.off_qstar + align256((size_t)5 * mx * my * 8);
     const size_t ntiles = (size_t)((mx + TILE_X - 1) / TILE_X) * (size_t)((my + TILE_Y - 1) / TILE_Y);
-    L.total_fused = L.off_tflag + align256(ntiles * 4);
+    // the tile lists of the step without a branch log, then the queue and
+    // list counters
+    L.off_list_act = L.off_tflag + align256(ntiles * 4);
+    L.off_list_rec = L.off_list_act + align256(ntiles * 4);
+    L.off_counters = L.off_list_rec + align256(ntiles * 4);
+    L.total_fused = L.off_counters + 256;
     L.total = L.total_staged > L.total_fused ? L.total_staged : L.total_fused;
     return L;
 }
@@ -982,17 +1120,21 @@ inline int cuda_status() {
 // the tile kernel's dynamic shared memory above 48 KB must be opted into
 // once per device (function attributes belong to the device's context)
 inline int ensure_tile_smem_attr() {
-    static bool done[MAX_DEVICES] = {};
+    static std::atomic<bool> done[MAX_DEVICES];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return DCLAW_ERR_CUDA;
-    if (!done[dev]) {
-        const int bytes = (int)TileGeom<TILE_X, TILE_Y>::SMEM_BYTES;
-        if (cudaFuncSetAttribute(k_tile<TILE_X, TILE_Y, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 bytes) != cudaSuccess ||
-            cudaFuncSetAttribute(k_tile<TILE_X, TILE_Y, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 bytes) != cudaSuccess)
-            return DCLAW_ERR_CUDA;
-        done[dev] = true;
+    if (!done[dev].load(std::memory_order_acquire)) {
+        std::lock_guard<std::mutex> lock(g_setup_mu);
+        if (!done[dev].load(std::memory_order_relaxed)) {
+            const int bytes = (int)TileGeom<TILE_X, TILE_Y>::SMEM_BYTES;
+            if (cudaFuncSetAttribute(k_tile<TILE_X, TILE_Y, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     bytes) != cudaSuccess ||
+                cudaFuncSetAttribute(k_tile<TILE_X, TILE_Y, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     bytes) != cudaSuccess ||
+                cudaFuncSetAttribute(k_tile_list, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
+                return DCLAW_ERR_CUDA;
+            done[dev].store(true, std::memory_order_release);
+        }
     }
     return DCLAW_OK;
 }
@@ -1189,8 +1331,35 @@ int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int m
         cudaMemsetAsync(branch_log, 0, nlog * sizeof(uint32_t), s);
     }
     uint32_t* tflag = (uint32_t*)((char*)work + L.off_tflag);
+    const int ntx = (mx + TILE_X - 1) / TILE_X, nty = (my + TILE_Y - 1) / TILE_Y;
+    if (!branch_log) {
+        // over the tile lists (the branch log needs every interface's bits,
+        // so it keeps the full-grid kernels below)
+        const int nsm = sm_count();
+        if (nsm <= 0) return DCLAW_ERR_CUDA;
+        unsigned int* counters = (unsigned int*)((char*)work + L.off_counters);
+        uint32_t* list_act = (uint32_t*)((char*)work + L.off_list_act);
+        uint32_t* list_rec = (uint32_t*)((char*)work + L.off_list_rec);
+        double* qstar = (double*)((char*)work + L.off_qstar);
+        const long long ncell = (long long)mx * my;
+        const unsigned ntiles = (unsigned)ntx * (unsigned)nty;
+        unsigned g0 = (unsigned)(nsm * DCLAW_SCAN_MINB * 2);
+        if ((long long)g0 * TPB > ncell) g0 = nblocks(ncell);
+        k_scan_patch<<<g0, TPB, 0, s>>>(P, mx, my, q_in, q_out, clock, counters, tflag);
+        k_list_patch<<<(ntiles + TPB - 1) / TPB, TPB, 0, s>>>(ntx, nty, clock, tflag, counters, list_act, list_rec);
+        unsigned g1 = (unsigned)(nsm * DCLAW_PLAIN_CELL_MINB);
+        if (g1 > ntiles) g1 = ntiles;
+        k_records_list<<<g1, TPB, 0, s>>>(P, g, q_in, b, R, counters, list_rec);
+        unsigned g2 = (unsigned)(nsm * DCLAW_TILE_MINBLOCKS);
+        if (g2 > ntiles) g2 = ntiles;
+        k_tile_list<<<g2, TILE_TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, qstar, clock, counters, list_act);
+        unsigned g3 = (unsigned)(nsm * SRC2_MINB);
+        if (g3 > ntiles) g3 = ntiles;
+        k_src2_list<<<g3, SRC2_TPB, 0, s>>>(P, g, qstar, q_out, clock, counters, list_act);
+        return cuda_status();
+    }
     k_records<<<nblocks((long long)L.npad), TPB, 0, s>>>(P, g, q_in, b, R, clock, tflag);
-    dim3 grid((mx + TILE_X - 1) / TILE_X, (my + TILE_Y - 1) / TILE_Y);
+    dim3 grid(ntx, nty);
     if (DCLAW_SRC2_KERNEL) {
         double* qstar = (double*)((char*)work + L.off_qstar);
         k_tile<TILE_X, TILE_Y, false><<<grid, TILE_TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, qstar, clock, branch_log,
@@ -1476,7 +1645,7 @@ int dclaw_max_wave_speed(const double* q, int mx, int my, const dclaw_params* p,
 namespace dclaw {
 constexpr size_t NOALLOC_MAX_CELLS = (size_t)1 << 18;
 static __device__ __align__(256) double g_noalloc_scratch[(size_t)NREC * NOALLOC_MAX_CELLS];
-static double* g_noalloc_addr[MAX_DEVICES] = {};
+static std::atomic<double*> g_noalloc_addr[MAX_DEVICES];
 }  // namespace dclaw
 
 extern "C" {
@@ -1492,11 +1661,18 @@ int dclaw_step_noalloc(const double* q_in, double* q_out, const double* b, int m
     if (rc) return rc;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return DCLAW_ERR_CUDA;
-    if (!g_noalloc_addr[dev]) {
-        // set-up on first use on this device (this device is current here)
-        void* addr = nullptr;
-        if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return DCLAW_ERR_CUDA;
-        g_noalloc_addr[dev] = static_cast<double*>(addr);
+    double* scratch = g_noalloc_addr[dev].load(std::memory_order_acquire);
+    if (!scratch) {
+        // set-up on first use on this device (this device is current here),
+        // under the set-up lock so that concurrent first calls agree
+        std::lock_guard<std::mutex> lock(g_setup_mu);
+        scratch = g_noalloc_addr[dev].load(std::memory_order_relaxed);
+        if (!scratch) {
+            void* addr = nullptr;
+            if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return DCLAW_ERR_CUDA;
+            scratch = static_cast<double*>(addr);
+            g_noalloc_addr[dev].store(scratch, std::memory_order_release);
+        }
     }
     if (ensure_tile_smem_attr() != DCLAW_OK) return DCLAW_ERR_CUDA;
     // every record plane a tile reads is written by k_records in the same
@@ -1506,7 +1682,7 @@ int dclaw_step_noalloc(const double* q_in, double* q_out, const double* b, int m
     cudaStream_t s = (cudaStream_t)stream;
     Geom g{mx, my, mx + 4, my + 4, dx, dy};
     const size_t npad = (size_t)(mx + 4) * (my + 4);
-    Rec R{g_noalloc_addr[dev], npad};
+    Rec R{scratch, npad};
     const dclaw_params P = *p;
     k_records<<<nblocks((long long)npad), TPB, 0, s>>>(P, g, q_in, b, R, clock, nullptr);
     dim3 grid((mx + TILE_X - 1) / TILE_X, (my + TILE_Y - 1) / TILE_Y);

@@ -177,7 +177,9 @@ int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int m
  * larger patches return DCLAW_ERR_TOO_LARGE without launching anything.
  * It never calls cudaMalloc/cudaFree. The first call on a device looks up
  * the array's device address (with that device current) and should come
- * before any stream capture on that device. All calls on a device share the
+ * before any stream capture on that device; first calls from several host
+ * threads at once are safe (the look-up runs under a lock, once per
+ * device). All calls on a device share the
  * one array: calls whose work overlaps on the GPU (different streams, or
  * different host threads without ordering) race and must not be issued.
  * Arguments and results are those of dclaw_step without the workspace and

@@ -1699,8 +1699,44 @@ double oracle_elementary(int which, double x) {
         case 3: return dclaw::em::d_tanh(x);
         case 4: return dclaw::em::d_pow_7_3(x);
         case 5: return dclaw::em::d_log(x);
+        case 6: return dclaw::em::d_expm1(x);
         default: return 0.0;
     }
+}
+
+/* glibc's value of the same function (the libm the Fortran build calls) */
+static double glibc_elementary(int which, double x) {
+    switch (which) {
+        case 0: return std::exp(x);
+        case 1: return std::atan(x);
+        case 2: return std::tan(x);
+        case 3: return std::tanh(x);
+        case 4: return std::pow(x, 7.0 / 3.0);
+        case 5: return std::log(x);
+        case 6: return std::expm1(x);
+        default: return 0.0;
+    }
+}
+
+/* Number of arguments, of n drawn uniformly from [lo, hi) by a seeded
+ * xorshift generator, at which the portable function `which` and glibc's
+ * differ in any bit. */
+long long oracle_libm_mismatches(int which, double lo, double hi, long long n, unsigned long long seed) {
+    unsigned long long s = seed ? seed : 88172645463325252ull;
+    long long bad = 0;
+    for (long long i = 0; i < n; ++i) {
+        s ^= s << 13;
+        s ^= s >> 7;
+        s ^= s << 17;
+        const double u = (double)(s >> 11) * (1.0 / 9007199254740992.0);
+        const double x = lo + (hi - lo) * u;
+        const double a = oracle_elementary(which, x), b = glibc_elementary(which, x);
+        uint64_t ba, bb;
+        std::memcpy(&ba, &a, 8);
+        std::memcpy(&bb, &b, 8);
+        if (ba != bb) ++bad;
+    }
+    return bad;
 }
 
 int oracle_threads(int n) {

@@ -72,6 +72,9 @@ class Oracle:
         L.oracle_set_libm.argtypes = [ctypes.c_int]
         L.oracle_elementary.restype = ctypes.c_double
         L.oracle_elementary.argtypes = [ctypes.c_int, ctypes.c_double]
+        L.oracle_libm_mismatches.restype = ctypes.c_longlong
+        L.oracle_libm_mismatches.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_longlong,
+                                             ctypes.c_ulonglong]
         L.oracle_qfix.argtypes = [ctypes.POINTER(CParams), _dp, _dp]
         L.oracle_setvars.argtypes = [ctypes.POINTER(CParams), _dp, _dp]
 
@@ -85,9 +88,16 @@ class Oracle:
             raise ValueError(libm)
         self.lib.oracle_set_libm(1 if libm == "portable" else 0)
 
+    ELEMENTARY = ["exp", "atan", "tan", "tanh", "pow73", "log", "expm1"]
+
     def elementary(self, name: str, x: float) -> float:
-        """The portable elementary function `name` (exp, atan, tan, tanh, pow73, log) at x."""
-        return self.lib.oracle_elementary(["exp", "atan", "tan", "tanh", "pow73", "log"].index(name), float(x))
+        """The portable elementary function `name` (exp, atan, tan, tanh, pow73, log, expm1) at x."""
+        return self.lib.oracle_elementary(self.ELEMENTARY.index(name), float(x))
+
+    def libm_mismatches(self, name: str, lo: float, hi: float, n: int, seed: int = 1) -> int:
+        """How many of n seeded uniform arguments in [lo, hi) give the portable
+        function `name` and glibc's different bits."""
+        return self.lib.oracle_libm_mismatches(self.ELEMENTARY.index(name), float(lo), float(hi), int(n), int(seed))
 
     def run(self, p: DClawParams, q: np.ndarray, b: np.ndarray, dx: float, dy: float, nsteps: int,
             dt_initial: float, t_final: float = 0.0, fixed_dt: bool = False, parallel: bool = True,

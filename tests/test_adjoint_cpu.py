@@ -68,6 +68,8 @@ CASES = {
     "dd_manning": dict(seed=15, p=DClawParams(friction_forcing=True, manning_coefficient=0.04, dd_manning=True,
                                               manning_max=0.1, friction_depth=0.8)),
     "at_rest": dict(seed=3, moving=False),
+    # b4step2's speed limit (b4step2.f90:74-100) acting on the faster cells
+    "speed_limit": dict(seed=16, p=DClawParams(speed_limit=0.6)),
 }
 
 

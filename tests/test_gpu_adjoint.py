@@ -87,40 +87,45 @@ def _loss_weights(q, n_out, seed=5):
     return w / sc[None, :, None, None]
 
 
-def _fd(f, eps0=1e-6, agree=1e-5, tries=5):
+def _fd(f, eps0=1e-6, down=4, up=3):
     """Central difference (f(e) - f(-e)) / 2e and its uncertainty.
 
-    Estimates at e, 2e and 4e are compared; where they disagree by more than
-    `agree` a kink of the forward map lies within the step (limiter regimes,
-    the dry tolerance and min/max picks put kinks within 1e-6 relative of
-    ordinary states, and a step that straddles one measures a chord, not the
-    derivative the adjoint gives), so e is halved. Returns (estimate at e,
-    spread of the three estimates) for the first step that settles, else for
-    the one with the smallest spread. Truncation error is far below the
-    spread, which measures the estimate's rounding noise: every perturbed
-    run rounds its elementary functions afresh, step after step, and that
-    noise divided by e grows as e shrinks."""
+    Estimates are taken at e = eps0 * 2^k for k = -down .. up, and the
+    window of three neighbours (e, 2e, 4e) whose estimates agree best is
+    kept: returns (estimate at that window's middle step, spread of its
+    three estimates). Two errors pull the step size in opposite ways. A
+    step that straddles a kink of the forward map (limiter regimes, the dry
+    tolerance and min/max picks put kinks within 1e-6 relative of ordinary
+    states) measures a chord, not the derivative the adjoint gives, so
+    smaller steps help; rounding noise (every perturbed run rounds its
+    elementary functions afresh, step after step) divided by e grows as e
+    shrinks, so larger steps help. The spread is the estimate's
+    uncertainty; the caller checks it against its tolerance rather than
+    widening the tolerance by it."""
     def cd(e):
         return (f(e) - f(-e)) / (2 * e)
 
-    e = eps0
-    vals = {2 * e: cd(2 * e), 4 * e: cd(4 * e)}
+    es = [eps0 * 2.0**k for k in range(-down, up + 1)]
+    vals = [cd(e) for e in es]
     best = None
-    for _ in range(tries):
-        vals[e] = cd(e)
-        three = [vals[e], vals[2 * e], vals[4 * e]]
+    for k in range(len(es) - 2):
+        three = vals[k:k + 3]
+        mid = three[1]
         spread = max(three) - min(three)
-        if best is None or spread < best[1]:
-            best = (vals[e], spread)
-        if spread <= agree * abs(vals[e]):
-            break
-        e *= 0.5
-    return best
+        rel = spread / max(abs(mid), 1e-300)
+        if best is None or rel < best[2]:
+            best = (mid, spread, rel)
+    return best[0], best[1]
 
 
 def _close(ad, fd, what, rtol=1e-6):
-    est, noise = fd
-    assert abs(ad - est) <= rtol * abs(est) + noise, f"{what}: AD {ad:.12e} FD {est:.12e} (noise {noise:.2e})"
+    """AD against a finite difference to rtol, with the finite difference
+    itself settled to a quarter of rtol (its spread over three step sizes)."""
+    est, spread = fd
+    msg = f"{what}: AD {ad:.12e} FD {est:.12e} (FD spread {spread:.2e}, {spread / max(abs(est), 1e-300):.2e} rel)"
+    print(msg)
+    assert spread <= 0.25 * rtol * abs(est), "finite differences did not settle: " + msg
+    assert abs(ad - est) <= rtol * abs(est), msg
 
 
 def _run_loss(q0, theta, b, p, dx, n, outs, wts, **kw):

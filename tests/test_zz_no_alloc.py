@@ -31,13 +31,19 @@ def _clock(dev, dt):
     return clk
 
 
-def test_noalloc_matches_workspace_step_on_two_calls():
+# 200 x 200 uses a sixth of the scratch; 508 x 508 fills it exactly
+# ((508 + 4)^2 = 2^18 padded cells), where a wrong size check or plane stride
+# would first reach past the array
+@pytest.mark.parametrize("n", [200, 508])
+def test_noalloc_matches_workspace_step_on_two_calls(n):
     assert torch.cuda.is_available()
     lib = _lib.load()
     dev = torch.device("cuda:0")
-    c = W.random_field_case(n=200, dx=0.5, seed=21)
+    c = W.random_field_case(n=n, dx=0.5, seed=21)
     mx, my = c.mx, c.my
     assert (mx + 4) * (my + 4) <= lib.dclaw_step_noalloc_max_cells()
+    if n == 508:
+        assert (mx + 4) * (my + 4) == lib.dclaw_step_noalloc_max_cells()
     cp = c.params.to_c()
     q0 = torch.tensor(c.q, device=dev)
     b = torch.tensor(c.b, device=dev)
@@ -67,12 +73,15 @@ def test_noalloc_matches_workspace_step_on_two_calls():
     assert torch.equal(clk_a[:4], clk_b[:4])  # t, next dt, Courant number, dt used
     assert int(clk_b.cpu().numpy().view(np.int32)[14]) == 0  # status word
     assert (qb2[0] > 0).sum().item() > 1000
+    # the second call also moved the state (not a copy of the first result)
+    assert not torch.equal(qb2, qb1)
 
 
-def test_noalloc_rejects_oversized_patch():
+# far beyond the limit, and one row beyond it (512 x 513 padded cells)
+@pytest.mark.parametrize("mx,my", [(600, 600), (508, 509)])
+def test_noalloc_rejects_oversized_patch(mx, my):
     lib = _lib.load()
     dev = torch.device("cuda:0")
-    mx = my = 600  # (604)^2 padded cells > 2^18
     cp = W.slope_runout(n=16).params.to_c()
     q = torch.zeros((5, my, mx), dtype=torch.float64, device=dev)
     out = torch.empty_like(q)
