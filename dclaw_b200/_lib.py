@@ -26,6 +26,7 @@ SIGNATURES = {
     "dclaw_error_string": (ctypes.c_char_p, [_int]),
     "dclaw_params_default": (None, [_pp]),
     "dclaw_params_check": (_int, [_pp]),
+    "dclaw_params_check_5": (_int, [_pp]),
     "dclaw_workspace_bytes": (_sz, [_int, _int]),
     "dclaw_bc2amr": (_int, [_vp, _int, _int, _int, _pp, _vp]),
     "dclaw_setaux": (_int, [_vp, _int, _int, _int, _pp, _vp]),
@@ -41,6 +42,8 @@ SIGNATURES = {
     "dclaw_fields_from_fortran": (_int, [_vp, _int, _int, _int, _int, _int, _vp, _vp]),
     "dclaw_fields_to_fortran": (_int, [_vp, _int, _int, _int, _int, _int, _vp, _vp]),
     "dclaw_max_wave_speed": (_int, [_vp, _int, _int, _pp, _vp, _vp]),
+    "dclaw_step_full": (_int, [_vp, _vp, _vp, _vp, _int, _int, _dbl, _dbl, _pp, _vp, _vp, _sz, _vp, _vp]),
+    "dclaw_step_full_workspace_bytes": (_sz, [_int, _int]),
     "dclaw_step_noalloc": (_int, [_vp, _vp, _vp, _int, _int, _dbl, _dbl, _pp, _vp, _vp]),
     "dclaw_step_noalloc_max_cells": (_sz, []),
     "dclaw_step_host": (_int, [_vp, _vp, _vp, _int, _int, _dbl, _dbl, _pp, _vp, _vp, _sz, _int, _vp]),

@@ -663,7 +663,7 @@ size_t dclaw_adjoint_workspace_bytes(int mx, int my) {
 
 int dclaw_adjoint_supported(const dclaw_params* p) {
     if (!p) return DCLAW_ERR_ARG;
-    int rc = dclaw_params_check(p);
+    int rc = dclaw_params_check_5(p);
     if (rc) return rc;
     // no adjoint form: the rare-wave corrector's branch structure and
     // src2method 2's data-dependent substeps

@@ -12,6 +12,7 @@
 #include <atomic>
 #include <mutex>
 
+#include "full_state.cuh"
 #include "stages.cuh"
 #include "tile.cuh"
 #include "workspace.cuh"
@@ -277,6 +278,79 @@ __global__ void __launch_bounds__(TPB) k_final(dclaw_params P, Geom g, Work W, d
     if (stage_finalize(P, g, W, q_out, i, j, clk->dt)) flag_status(clk, DCLAW_ERR_NAN);
 }
 
+// ---- the full-state step (segregation, entrainment) -------------------------
+__global__ void __launch_bounds__(TPB) k_full_b4(dclaw_params P, Geom g, const double* __restrict__ q_in,
+                                                 const double* __restrict__ b, WorkF W, dclaw_clock* clk) {
+    const long long n = (long long)g.PX * g.PY;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
+    if (full_b4(P, g, q_in, b, W, i, j)) flag_status(clk, DCLAW_ERR_NAN);
+}
+
+__global__ void __launch_bounds__(TPB) k_full_taudir(dclaw_params P, Geom g, WorkF W) {
+    const long long n = (long long)g.PX * g.PY;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
+    full_taudir(P, g, W, i, j);
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(TPB) k_full_riemann(dclaw_params P, Geom g, WorkF W, dclaw_clock* clk,
+                                                      uint32_t* __restrict__ brlog) {
+    const int nfast = DIR == 0 ? g.mx + 3 : g.mx + 2;
+    const int nslow = DIR == 0 ? g.my + 2 : g.my + 3;
+    const long long n = (long long)nfast * nslow;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double cflv = 0.0;
+    if (idx < n) {
+        int a = (int)(idx % nfast), s = (int)(idx / nfast);
+        int r = DIR == 0 ? s : a;
+        int i = DIR == 0 ? a : s;
+        const int nlen = DIR == 0 ? g.mx : g.my;
+        uint32_t bits = 0;
+        double smax = full_riemann<DIR>(P, g, W, r, i, &bits);
+        if (i >= 1 && i <= nlen + 1) {
+            const double dt = clk->dt;
+            const double dtdx = DIR == 0 ? dt / g.dx : dt / g.dy;
+            cflv = dtdx * smax;
+            if (brlog) {
+                size_t off = DIR == 0 ? (size_t)r * (g.mx + 1) + (size_t)(i - 1)
+                                      : (size_t)(g.my + 2) * (g.mx + 1) + (size_t)r * (g.my + 1) + (size_t)(i - 1);
+                brlog[off] = bits;
+            }
+        }
+        if (!(cflv == cflv)) cflv = 0.0;
+    }
+    block_max_to(cflv, reinterpret_cast<unsigned long long*>(&clk->cfl_bits));
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(TPB) k_full_flux(dclaw_params P, Geom g, WorkF W, const dclaw_clock* clk,
+                                                   uint32_t* __restrict__ brlog) {
+    const int nfast = DIR == 0 ? g.mx + 1 : g.mx + 2;
+    const int nslow = DIR == 0 ? g.my + 2 : g.my + 1;
+    const long long n = (long long)nfast * nslow;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    int a = (int)(idx % nfast), s = (int)(idx / nfast);
+    int r = DIR == 0 ? s : a;
+    int i = DIR == 0 ? a + 1 : s + 1;
+    const double dt = clk->dt;
+    const double dtdx = DIR == 0 ? dt / g.dx : dt / g.dy;
+    uint32_t bits = 0;
+    full_flux<DIR>(P, g, W, r, i, dtdx, brlog ? &bits : nullptr);
+    if (brlog) {
+        size_t off = DIR == 0 ? (size_t)r * (g.mx + 1) + (size_t)(i - 1)
+                              : (size_t)(g.my + 2) * (g.mx + 1) + (size_t)r * (g.my + 1) + (size_t)(i - 1);
+        brlog[off] |= bits;
+    }
+}
+
+__global__ void __launch_bounds__(TPB) k_full_final(dclaw_params P, Geom g, WorkF W, const double* __restrict__ he,
+                                                    double* __restrict__ q_out, dclaw_clock* clk);
+
 // the next dt after the tick rule's choice dtn: clipped at the next
 // observation time (with the tick rule and t_obs > 0), then at t_final
 __device__ __forceinline__ double clip_next_dt(const dclaw_clock* clk, double dtn) {
@@ -364,6 +438,18 @@ __device__ __forceinline__ void last_block_tick(const dclaw_params& P, dclaw_clo
             tick_device(P, clk);
         }
     }
+}
+
+// update + src2 of the full state; the last block applies the tick
+__global__ void __launch_bounds__(TPB) k_full_final(dclaw_params P, Geom g, WorkF W, const double* __restrict__ he,
+                                                    double* __restrict__ q_out, dclaw_clock* clk) {
+    const long long n = (long long)g.mx * g.my;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < n) {
+        int i = (int)(idx % g.mx) + 1, j = (int)(idx / g.mx) + 1;
+        if (full_finalize(P, g, W, he, q_out, i, j, clk->dt)) flag_status(clk, DCLAW_ERR_NAN);
+    }
+    last_block_tick(P, clk);
 }
 
 // One tile of the fused step (all threads of the CTA call it). smem holds
@@ -1272,12 +1358,20 @@ void dclaw_params_default(dclaw_params* p) {
     p->cfl_desired = 0.9;
     p->cfl_max = 1.0;
     p->dt_max = 1.0e99;
+    p->beta_seg = 0.0;
+    p->delta_kr_order = 2.0;
+    p->chie = 0.5;
+    p->me = 0.65;
+    p->entrainment_rate = 0.2;
+    p->entrainment_method = 1;
 }
 
 int dclaw_params_check(const dclaw_params* p) {
     if (!p) return DCLAW_ERR_ARG;
-    if (p->bed_normal != 0 || p->entrainment != 0 || p->segregation != 0 || p->curvature != 0)
-        return DCLAW_ERR_UNSUPPORTED;
+    if (p->bed_normal != 0 || p->curvature != 0) return DCLAW_ERR_UNSUPPORTED;
+    if ((p->entrainment != 0 && p->entrainment != 1) || (p->segregation != 0 && p->segregation != 1))
+        return DCLAW_ERR_ARG;
+    if (p->entrainment_method != 0 && p->entrainment_method != 1) return DCLAW_ERR_ARG;
     if (p->src2method < -1 || p->src2method > 2) return DCLAW_ERR_UNSUPPORTED;
     if (p->alphamethod != 0 && p->alphamethod != 1) return DCLAW_ERR_ARG;
     // the setrun writer's parameter conflict check (src/python/dclaw/data.py:362-365)
@@ -1291,6 +1385,13 @@ int dclaw_params_check(const dclaw_params* p) {
     }
     if (!(p->grav > 0.0) || !(p->dry_tolerance > 0.0) || !(p->rho_f > 0.0) || !(p->rho_s > 0.0)) return DCLAW_ERR_ARG;
     if (!(p->alpha_c > 0.0) || !(p->cfl_desired > 0.0) || !(p->dt_max > 0.0)) return DCLAW_ERR_ARG;
+    return DCLAW_OK;
+}
+
+int dclaw_params_check_5(const dclaw_params* p) {
+    const int rc = dclaw_params_check(p);
+    if (rc) return rc;
+    if (p->entrainment != 0 || p->segregation != 0) return DCLAW_ERR_UNSUPPORTED;
     return DCLAW_OK;
 }
 
@@ -1316,7 +1417,7 @@ int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int m
                void* stream) {
     if (!q_in || !q_out || !b || !p || !clock || !work || q_in == q_out) return DCLAW_ERR_ARG;
     if (!sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0)) return DCLAW_ERR_ARG;
-    int rc = dclaw_params_check(p);
+    int rc = dclaw_params_check_5(p);
     if (rc) return rc;
     Layout L = layout(mx, my);
     if (work_bytes < L.total_fused) return DCLAW_ERR_WORKSPACE;
@@ -1393,7 +1494,7 @@ int dclaw_step_host(const double* q_in, double* q_out, const double* b, int mx, 
                     void* stream) {
     if (!q_in || !q_out || !b || !p || !clock || !work || nbands < 0) return DCLAW_ERR_ARG;
     if (!sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0)) return DCLAW_ERR_ARG;
-    int rc = dclaw_params_check(p);
+    int rc = dclaw_params_check_5(p);
     if (rc) return rc;
     if (work_bytes < dclaw_step_host_workspace_bytes(mx, my)) return DCLAW_ERR_WORKSPACE;
     if (ensure_tile_smem_attr() != DCLAW_OK) return DCLAW_ERR_CUDA;
@@ -1473,7 +1574,7 @@ int dclaw_step_rows(const double* q_in, double* q_out, const double* b, int mx, 
     if (row_first < 1 || row_count < 1 || last > my || (row_first - 1) % TILE_Y != 0 ||
         (last != my && last % TILE_Y != 0))
         return DCLAW_ERR_ARG;
-    int rc = dclaw_params_check(p);
+    int rc = dclaw_params_check_5(p);
     if (rc) return rc;
     Layout L = layout(mx, my);
     if (work_bytes < L.total_fused) return DCLAW_ERR_WORKSPACE;
@@ -1500,7 +1601,7 @@ int dclaw_step_rows(const double* q_in, double* q_out, const double* b, int mx, 
 
 int dclaw_clock_tick(dclaw_clock* clock, const dclaw_params* p, void* stream) {
     if (!clock || !p) return DCLAW_ERR_ARG;
-    int rc = dclaw_params_check(p);
+    int rc = dclaw_params_check_5(p);
     if (rc) return rc;
     k_tick<<<1, 32, 0, (cudaStream_t)stream>>>(*p, clock);
     return cuda_status();
@@ -1508,7 +1609,7 @@ int dclaw_clock_tick(dclaw_clock* clock, const dclaw_params* p, void* stream) {
 
 int dclaw_bc2amr(double* q, int mx, int my, int mbc, const dclaw_params* p, void* stream) {
     if (!q || !p || mbc != 2 || !sizes_ok(mx, my)) return DCLAW_ERR_ARG;
-    int rc = dclaw_params_check(p);
+    int rc = dclaw_params_check_5(p);
     if (rc) return rc;
     k_bc2amr<<<nblocks((long long)(mx + 4) * (my + 4)), TPB, 0, (cudaStream_t)stream>>>(*p, mx, my, q);
     return cuda_status();
@@ -1524,7 +1625,7 @@ int dclaw_b4step2(double* q, double* aux, int mx, int my, int mbc, double dx, do
                   const dclaw_params* p, dclaw_clock* clock, void* stream) {
     (void)t; (void)dt;
     if (!q || !aux || !p || mbc != 2 || !sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0)) return DCLAW_ERR_ARG;
-    int rc = dclaw_params_check(p);
+    int rc = dclaw_params_check_5(p);
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
     const size_t npad = (size_t)(mx + 4) * (my + 4);
@@ -1544,7 +1645,7 @@ int dclaw_step2(double* q, const double* aux, int mx, int my, int mbc, double dx
                 void* stream) {
     if (!q || !aux || !p || !clock || !work || mbc != 2 || !sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0))
         return DCLAW_ERR_ARG;
-    int rc = dclaw_params_check(p);
+    int rc = dclaw_params_check_5(p);
     if (rc) return rc;
     Layout L = layout(mx, my);
     if (work_bytes < L.total_staged) return DCLAW_ERR_WORKSPACE;
@@ -1570,7 +1671,7 @@ int dclaw_src2(double* q, const double* aux, int mx, int my, int mbc, double dx,
                const dclaw_params* p, void* stream) {
     (void)aux; (void)dx; (void)dy; (void)t;
     if (!q || !p || mbc != 2 || !sizes_ok(mx, my)) return DCLAW_ERR_ARG;
-    int rc = dclaw_params_check(p);
+    int rc = dclaw_params_check_5(p);
     if (rc) return rc;
     k_src2_padded<<<nblocks((long long)mx * my), TPB, 0, (cudaStream_t)stream>>>(*p, mx, my, dt, q);
     return cuda_status();
@@ -1636,6 +1737,44 @@ int dclaw_max_wave_speed(const double* q, int mx, int my, const dclaw_params* p,
 
 }  // extern "C"
 
+extern "C" {
+
+size_t dclaw_step_full_workspace_bytes(int mx, int my) {
+    if (!sizes_ok(mx, my)) return 0;
+    return full_layout(mx, my).total;
+}
+
+int dclaw_step_full(const double* q_in, double* q_out, const double* b, const double* h_e, int mx, int my,
+                    double dx, double dy, const dclaw_params* p, dclaw_clock* clock, void* work, size_t work_bytes,
+                    uint32_t* branch_log, void* stream) {
+    if (!q_in || !q_out || !b || !p || !clock || !work || q_in == q_out) return DCLAW_ERR_ARG;
+    if (!sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0)) return DCLAW_ERR_ARG;
+    int rc = dclaw_params_check(p);
+    if (rc) return rc;
+    if (p->entrainment == 1 && p->entrainment_method == 0 && !h_e) return DCLAW_ERR_ARG;
+    const FullLayout L = full_layout(mx, my);
+    if (work_bytes < L.total) return DCLAW_ERR_WORKSPACE;
+    cudaStream_t s = (cudaStream_t)stream;
+    Geom g{mx, my, mx + 4, my + 4, dx, dy};
+    WorkF W = make_work_full(work, L);
+    const dclaw_params P = *p;
+    if (branch_log) {
+        size_t nlog = (size_t)(my + 2) * (mx + 1) + (size_t)(mx + 2) * (my + 1);
+        cudaMemsetAsync(branch_log, 0, nlog * sizeof(uint32_t), s);
+    }
+    const long long npad = (long long)g.PX * g.PY;
+    k_full_b4<<<nblocks(npad), TPB, 0, s>>>(P, g, q_in, b, W, clock);
+    k_full_taudir<<<nblocks(npad), TPB, 0, s>>>(P, g, W);
+    k_full_riemann<0><<<nblocks((long long)(mx + 3) * (my + 2)), TPB, 0, s>>>(P, g, W, clock, branch_log);
+    k_full_riemann<1><<<nblocks((long long)(mx + 2) * (my + 3)), TPB, 0, s>>>(P, g, W, clock, branch_log);
+    k_full_flux<0><<<nblocks((long long)(mx + 1) * (my + 2)), TPB, 0, s>>>(P, g, W, clock, branch_log);
+    k_full_flux<1><<<nblocks((long long)(mx + 2) * (my + 1)), TPB, 0, s>>>(P, g, W, clock, branch_log);
+    k_full_final<<<nblocks((long long)mx * my), TPB, 0, s>>>(P, g, W, h_e, q_out, clock);
+    return cuda_status();
+}
+
+}  // extern "C"
+
 // ---- allocation-free variant of the fused step ------------------------------
 // Scratch for the per-cell records of one patch of at most
 // NOALLOC_MAX_CELLS padded cells, in a fixed device array of this library
@@ -1657,7 +1796,7 @@ int dclaw_step_noalloc(const double* q_in, double* q_out, const double* b, int m
     if (!q_in || !q_out || !b || !p || !clock || q_in == q_out) return DCLAW_ERR_ARG;
     if (!sizes_ok(mx, my) || !(dx > 0.0) || !(dy > 0.0)) return DCLAW_ERR_ARG;
     if ((size_t)(mx + 4) * (size_t)(my + 4) > NOALLOC_MAX_CELLS) return DCLAW_ERR_TOO_LARGE;
-    int rc = dclaw_params_check(p);
+    int rc = dclaw_params_check_5(p);
     if (rc) return rc;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return DCLAW_ERR_CUDA;

@@ -121,13 +121,16 @@ struct SetVars {
     double rho, kperm, alphainv, m_eq, tanpsi, tau;
 };
 
-// setvars with segregation = 0 (kr_chi = 1). `phi` is the basal friction angle.
+// setvars. `phi` is the basal friction angle, chi the species fraction
+// (read only with segregation = 1: kperm times 10^(delta_kr_order 2 (chi -
+// 1/2)), digclaw_module.f90:418-431; kr_chi = 1 otherwise).
 template <bool NEED_ALL>
 DC_BIG SetVars setvars(const dclaw_params& P, double phi, double h, double u, double v,
-                                           double m, double p, double gz) {
+                                           double m, double p, double gz, double chi = 0.0) {
     SetVars o;
     o.rho = m * (P.rho_s - P.rho_f) + P.rho_f;
     double kr_chi = 1.0;
+    if (NEED_ALL && P.segregation == 1) kr_chi = em::d_pow(10.0, P.delta_kr_order * 2.0 * (chi - 0.5));
     if (NEED_ALL) o.kperm = kr_chi * P.kref * em::d_exp(-(m - P.mref) / (0.04));
     else o.kperm = 0.0;
     double sig_eff = fmax2(0.0, o.rho * gz * h - p);
@@ -249,14 +252,23 @@ struct Side {
     double b, taudir, fs;     // bed, static-friction direction and factor of safety
     // setvars outputs for this state (rho, tau), valid when h >= drytol
     double rho_sv, tau_sv;
+    double chi;               // species fraction; read only for the species waves
+};
+
+// The species (hchi) components of the waves, for the full-state step:
+// waves 1 and 5 after the middle-wave merge (wave 2's is merged too).
+struct ChiWaves {
+    double w1c, w5c;
 };
 
 // riemann_dig2_aug_sswave_ez with the wall / inundation preprocessing of
 // rpn2 (the dry-dry skip is done by the caller). bed_normal = 0: theta = 0.
 // L and R carry setvars (rho, tau) of their states; the mirrored ghost of a
 // wall problem has the same closures as its source because setvars depends
-// on the velocity only through u^2 + v^2.
-DC_BIG Waves riemann_solve(const dclaw_params& P, Side L, Side R, uint32_t* br) {
+// on the velocity only through u^2 + v^2. With cw, the species waves are
+// computed too from L.chi, R.chi (riemannsolvers_dclaw.f:463-468, merged at
+// :495-510; the dry side takes the wet side's chi, rpn2_dclaw.f:197,226).
+DC_BIG Waves riemann_solve(const dclaw_params& P, Side L, Side R, uint32_t* br, ChiWaves* cw = nullptr) {
     const double grav = P.grav;
     const double drytol = P.dry_tolerance;
     double wall1 = 1.0, wall2 = 1.0, wall3 = 1.0;
@@ -265,10 +277,16 @@ DC_BIG Waves riemann_solve(const dclaw_params& P, Side L, Side R, uint32_t* br) 
     double hmL = L.hm, hmR = R.hm, pL = L.p, pR = R.p, bL = L.b, bR = R.b;
     double uL = L.un, uR = R.un, vL = L.ut, vR = R.ut, mL = L.m, mR = R.m;
     double rhoL_sv = L.rho_sv, tauL_sv = L.tau_sv, rhoR_sv = R.rho_sv, tauR_sv = R.tau_sv;
+    double chiL = 0.0, chiR = 0.0;
+    if (cw) {
+        chiL = L.chi;
+        chiR = R.chi;
+    }
     if (hR <= drytol) {
         hR = 0.0;
         pR = 0.0;
         mR = mL;
+        chiR = chiL;
         RType t = riemanntype(hL, hL, uL, -uL, drytol, grav);
         double hstartest = fmax2(hL, t.hm);
         if (hstartest + bL < bR) {
@@ -282,6 +300,7 @@ DC_BIG Waves riemann_solve(const dclaw_params& P, Side L, Side R, uint32_t* br) 
         hL = 0.0;
         pL = 0.0;
         mL = mR;
+        chiL = chiR;
         RType t = riemanntype(hR, hR, -uR, uR, drytol, grav);
         double hstartest = fmax2(hR, t.hm);
         if (hstartest + bR < bL) {
@@ -461,12 +480,25 @@ DC_BIG Waves riemann_solve(const dclaw_params& P, Side L, Side R, uint32_t* br) 
     double fw53 = fw13 * gammaR * rhoR * grav * 1.0;
     double fw52;
 
+    double fw61 = 0.0, fw63 = 0.0, fw62 = 0.0;
+    if (cw) {
+        const double alpha_seg = 1.0 - P.beta_seg;
+        const double seg_L = chiL * hL * uL * (1.0 + (1.0 - alpha_seg) * (1.0 - chiL));
+        const double seg_R = chiR * hR * uR * (1.0 + (1.0 - alpha_seg) * (1.0 - chiR));
+        fw61 = fw11 * chiL * (1.0 + (1.0 - alpha_seg) * (1.0 - chiL));
+        fw63 = fw13 * chiR * (1.0 + (1.0 - alpha_seg) * (1.0 - chiR));
+        fw62 = seg_R - seg_L - fw61 - fw63;
+    }
     double hustar_interface = huL + fw11;
     if (!is_static) {
         double u_interface = hustar_interface / hstarHLL;
         del4 = -gamma * rho * gz * u_interface * (hR - hL) + grg * del1 + u_interface * (pR - pL);
     }
     fw52 = del4 - fw53 - fw51;
+    if (cw) {
+        if (hustar_interface <= 0.0) fw61 = fw61 + fw62;
+        else fw63 = fw63 + fw62;
+    }
     if (hustar_interface <= 0.0) {
         if (br) *br |= BR_REVERT_L;
         fw31 = fw31 + fw32;
@@ -482,6 +514,10 @@ DC_BIG Waves riemann_solve(const dclaw_params& P, Side L, Side R, uint32_t* br) 
     w.w1h = fw11 * wall1; w.w1n = fw21 * wall1; w.w1t = fw31 * wall1; w.w1m = fw41 * wall1; w.w1p = fw51 * wall1;
     w.w2h = fw12 * wall2; w.w2n = fw22 * wall2;
     w.w5h = fw13 * wall3; w.w5n = fw23 * wall3; w.w5t = fw33 * wall3; w.w5m = fw43 * wall3; w.w5p = fw53 * wall3;
+    if (cw) {
+        cw->w1c = fw61 * wall1;
+        cw->w5c = fw63 * wall3;
+    }
     return w;
 }
 
@@ -489,16 +525,23 @@ DC_BIG Waves riemann_solve(const dclaw_params& P, Side L, Side R, uint32_t* br) 
 // rpt2 for one fluctuation. cell = the imp cell (A2 state: h, hn, ht, hm),
 // b = its bed, topo1/topo3 = bed of the neighbours below/above in the
 // transverse direction. asdq in (h, n, t, hm, p). Outputs bm/bp in the same
-// order. Returns false when the split is skipped.
+// order. Returns false when the split is skipped. With bmp6 (the
+// full-state step) the species component is split too: bmp6[0], bmp6[1]
+// receive its B-, B+ parts, with r(6, 1) = r(6, 3) = chi = hchi / h
+// (rpt2_dclaw.f:104,208-215,244-258); b is then the bed less the bed change.
 DC_BIG bool rpt2_split(const dclaw_params& P, double h, double hn, double ht, double hm,
                                           double b, double topo1, double topo3, const double asdq[5],
-                                          double bm[5], double bp[5]) {
+                                          double bm[5], double bp[5], double hchi = 0.0,
+                                          double* bmp6 = nullptr) {
     for (int k = 0; k < 5; ++k) { bm[k] = 0.0; bp[k] = 0.0; }
+    if (bmp6) { bmp6[0] = 0.0; bmp6[1] = 0.0; }
     if (h <= P.dry_tolerance) return false;
     const double g = P.grav;
     double u = hn / h;
     double v = ht / h;
     double m = hm / h;
+    double chi = 0.0;
+    if (bmp6) chi = hchi / h;
     double eta = h + b;
     double rho = m * P.rho_s + (1.0 - m) * P.rho_f;
     double gamma;
@@ -512,15 +555,17 @@ DC_BIG bool rpt2_split(const dclaw_params& P, double h, double hn, double ht, do
     double beta2 = -u * delf1 + delf2;
     double beta3 = (delf3 - s1 * delf1) / (s3 - s1);
     double r5 = gamma * rho * g;
-    // wave 1: r = (1, u, s1, m, r5)
+    // wave 1: r = (1, u, s1, m, r5, chi)
     {
         double sb = 1.0 * s1 * beta1;
         if ((s1 < 0.0) && (eta >= topo1)) {
             bm[0] = bm[0] + sb * 1.0; bm[1] = bm[1] + sb * u; bm[2] = bm[2] + sb * s1;
             bm[3] = bm[3] + sb * m; bm[4] = bm[4] + sb * r5;
+            if (bmp6) bmp6[0] = bmp6[0] + sb * chi;
         } else if ((s1 > 0.0) && (eta >= topo3)) {
             bp[0] = bp[0] + sb * 1.0; bp[1] = bp[1] + sb * u; bp[2] = bp[2] + sb * s1;
             bp[3] = bp[3] + sb * m; bp[4] = bp[4] + sb * r5;
+            if (bmp6) bmp6[1] = bmp6[1] + sb * chi;
         }
     }
     // wave 2: r = (0, 1, 0, 0, 0): only the normal-momentum component is nonzero
@@ -529,15 +574,17 @@ DC_BIG bool rpt2_split(const dclaw_params& P, double h, double hn, double ht, do
         if ((s2 < 0.0) && (eta >= topo1)) bm[1] = bm[1] + sb * 1.0;
         else if ((s2 > 0.0) && (eta >= topo3)) bp[1] = bp[1] + sb * 1.0;
     }
-    // wave 3: r = (1, u, s3, m, r5)
+    // wave 3: r = (1, u, s3, m, r5, chi)
     {
         double sb = 1.0 * s3 * beta3;
         if ((s3 < 0.0) && (eta >= topo1)) {
             bm[0] = bm[0] + sb * 1.0; bm[1] = bm[1] + sb * u; bm[2] = bm[2] + sb * s3;
             bm[3] = bm[3] + sb * m; bm[4] = bm[4] + sb * r5;
+            if (bmp6) bmp6[0] = bmp6[0] + sb * chi;
         } else if ((s3 > 0.0) && (eta >= topo3)) {
             bp[0] = bp[0] + sb * 1.0; bp[1] = bp[1] + sb * u; bp[2] = bp[2] + sb * s3;
             bp[3] = bp[3] + sb * m; bp[4] = bp[4] + sb * r5;
+            if (bmp6) bmp6[1] = bmp6[1] + sb * chi;
         }
     }
     return true;
@@ -584,10 +631,10 @@ DC_HD void mp_update_relax(const dclaw_params& P, double phi, double dt, double&
 // dtm unassigned (branch vnorm == 0 or m == m_eq, mp_update.f90:225-249),
 // dtm = dtr, the whole remaining time.
 DC_BIG double mp_update_fe4quad(const dclaw_params& P, double phi, double dtr, double& h, double u, double v,
-                                double& m, double& p, double rhoh, double gz) {
+                                double& m, double& p, double rhoh, double gz, double chi = 0.0) {
     const double rs = P.rho_s, rf = P.rho_f, mu = P.mu;
     const double vnorm = sqrt(sq(u) + sq(v));
-    SetVars sv = setvars<true>(P, phi, h, u, v, m, p, gz);
+    SetVars sv = setvars<true>(P, phi, h, u, v, m, p, gz, chi);
     const double h0 = h, m_0 = m;
     const double rho0 = m_0 * (rs - rf) + rf;
     const double p_eq0 = rf * gz * h0;

@@ -107,33 +107,38 @@ DC_HD bool stage_b4(const dclaw_params& P, const Geom& g, const double* __restri
 // Stage B. calc_taudir on cell (i, j) of the padded patch. Cells of the outer
 // ghost ring keep fsphi = taudir = 0 (setaux zeroes them, calc_taudir covers
 // only 2-mbc..m+mbc-1).
-DC_HD void stage_taudir(const dclaw_params& P, const Geom& g, const Work& W, int i, int j) {
+// qB: the b4step2 state's padded planes (h, hu, hv, hm, pb first), td the
+// three output planes, bed(pi) the bed of padded cell pi (the bed less the
+// bed change on the full state: digclaw_module.f90:555-613).
+template <typename Bed>
+DC_HD void taudir_cell(const dclaw_params& P, const Geom& g, const double* __restrict__ qB, size_t npad,
+                       double* td, Bed bed, int i, int j) {
     const size_t pi = pidx(g, i, j);
-    double* fs = W.td;
-    double* tx = W.td + W.npad;
-    double* ty = W.td + 2 * W.npad;
+    double* fs = td;
+    double* tx = td + npad;
+    double* ty = td + 2 * npad;
     if (i < 0 || j < 0 || i > g.mx + 1 || j > g.my + 1) {
         fs[pi] = 0.0; tx[pi] = 0.0; ty[pi] = 0.0;
         return;
     }
     const double dry = P.dry_tolerance;
     const double gz = P.grav;
-    const double* qh = W.qB;
+    const double* qh = qB;
     // the qB state is already admissible: qfix leaves h of every cell as is
     double h = qh[pi];
-    double hu = W.qB[W.npad + pi], hv = W.qB[2 * W.npad + pi];
-    double hm = W.qB[3 * W.npad + pi], p = W.qB[4 * W.npad + pi];
+    double hu = qB[npad + pi], hv = qB[2 * npad + pi];
+    double hm = qB[3 * npad + pi], p = qB[4 * npad + pi];
     const size_t pL = pidx(g, i - 1, j), pR = pidx(g, i + 1, j), pB = pidx(g, i, j - 1), pT = pidx(g, i, j + 1);
     double hL = qh[pL], hR = qh[pR], hB = qh[pB], hT = qh[pT];
-    double b = W.bP[pi];
+    double b = bed(pi);
     double eta = h + b;
-    double etaL = hL + W.bP[pL];
+    double etaL = hL + bed(pL);
     if (hL < dry) etaL = fmin2(etaL, eta);
-    double etaR = hR + W.bP[pR];
+    double etaR = hR + bed(pR);
     if (hR < dry) etaR = fmin2(etaR, eta);
-    double etaB = hB + W.bP[pB];
+    double etaB = hB + bed(pB);
     if (hB < dry) etaB = fmin2(etaB, eta);
-    double etaT = hT + W.bP[pT];
+    double etaT = hT + bed(pT);
     if (hT < dry) etaT = fmin2(etaT, eta);
     if (h < dry) {
         eta = fmin2(etaL, eta);
@@ -178,6 +183,11 @@ DC_HD void stage_taudir(const dclaw_params& P, const Geom& g, const Work& W, int
         else ofs = 0.0;
     }
     fs[pi] = ofs; tx[pi] = otx; ty[pi] = oty;
+}
+
+DC_HD void stage_taudir(const dclaw_params& P, const Geom& g, const Work& W, int i, int j) {
+    const double* bP = W.bP;
+    taudir_cell(P, g, W.qB, W.npad, W.td, [bP](size_t q) { return bP[q]; }, i, j);
 }
 
 // ---------------------------------------------------------------------------
@@ -305,10 +315,11 @@ DC_HD double limiter_phi(int mth, double r, uint32_t& code) {
     return wl;
 }
 
-DC_HD void limit_family(int mth, int mw, double s, const double Wm[5], double Wi[5], const double Wp[5],
+template <int N = 5>
+DC_HD void limit_family(int mth, int mw, double s, const double* Wm, double* Wi, const double* Wp,
                         uint32_t* br) {
     double wnorm2 = 0.0, dotl = 0.0, dotr = 0.0;
-    for (int m = 0; m < 5; ++m) {
+    for (int m = 0; m < N; ++m) {
         wnorm2 = wnorm2 + sq(Wi[m]);
         dotl = dotl + Wm[m] * Wi[m];
         dotr = dotr + Wi[m] * Wp[m];
@@ -324,7 +335,7 @@ DC_HD void limit_family(int mth, int mw, double s, const double Wm[5], double Wi
     uint32_t code;
     double wl = limiter_phi(mth, r, code);
     if (br) *br |= br_lim(mw, code);
-    for (int m = 0; m < 5; ++m) Wi[m] = wl * Wi[m];
+    for (int m = 0; m < N; ++m) Wi[m] = wl * Wi[m];
 }
 
 // expand the compact waves at one interface into q-ordered 5-vectors

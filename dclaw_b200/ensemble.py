@@ -64,7 +64,7 @@ class EnsembleStepper:
         self.n = len(members)
         self.device = torch.device(device)
         for m in members:
-            _lib.check(self.lib.dclaw_params_check(ctypes.byref(m.params.to_c())), "member parameters")
+            _lib.check(self.lib.dclaw_params_check_5(ctypes.byref(m.params.to_c())), "member parameters")
         self.mx = np.array([m.q.shape[2] for m in members], dtype=np.int32)
         self.my = np.array([m.q.shape[1] for m in members], dtype=np.int32)
         self.dxs = np.array([m.dx for m in members], dtype=np.float64)

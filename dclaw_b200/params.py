@@ -55,6 +55,13 @@ class CParams(ctypes.Structure):
         ("cfl_desired", ctypes.c_double),
         ("cfl_max", ctypes.c_double),
         ("dt_max", ctypes.c_double),
+        ("beta_seg", ctypes.c_double),
+        ("delta_kr_order", ctypes.c_double),
+        ("chie", ctypes.c_double),
+        ("me", ctypes.c_double),
+        ("entrainment_rate", ctypes.c_double),
+        ("entrainment_method", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
     ]
 
 
@@ -165,6 +172,14 @@ class DClawParams:
     entrainment: int = 0
     segregation: int = 0
     curvature: int = 0
+    # segregation and entrainment (data.py:338-347; the full-state step only)
+    beta_seg: float = 0.0
+    chi0: float = 0.5            # initial species fraction (qinit.f90:219-226); initial states only
+    chie: float = 0.5
+    delta_kr_order: float = 2.0
+    me: float = 0.65
+    entrainment_rate: float = 0.2
+    entrainment_method: int = 1
     # clawdata
     order: int = 2
     transverse_waves: int = 2
@@ -191,6 +206,8 @@ class DClawParams:
                 c.phi = deg * float(self.phi)
             elif name == "theta_input":
                 c.theta_input = deg * float(self.theta_input)
+            elif name == "pad_":
+                continue
             else:
                 v = getattr(self, name)
                 setattr(c, name, int(v) if isinstance(v, bool) else v)

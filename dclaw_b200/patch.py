@@ -30,7 +30,7 @@ class Patch:
         self.lib = _lib.load()
         self.params = params
         self.cp = params.to_c()
-        _lib.check(self.lib.dclaw_params_check(ctypes.byref(self.cp)), "parameter check")
+        _lib.check(self.lib.dclaw_params_check_5(ctypes.byref(self.cp)), "parameter check")
         self.mx, self.my = int(mx), int(my)
         self.work_bytes = self.lib.dclaw_workspace_bytes(self.mx, self.my)
         self.work = torch.empty(self.work_bytes, dtype=torch.uint8, device=device)

@@ -90,24 +90,39 @@ def _require_cuda(t: torch.Tensor, name: str) -> None:
 class PatchStepper:
     """One uniform patch on the device, advanced by the fused step.
 
-    q: (5, my, mx) float64 CUDA tensor (x fastest), b: (my, mx).
+    q: (5, my, mx) float64 CUDA tensor (x fastest), b: (my, mx). A (7, my,
+    mx) state -- the reference's whole q (h, hu, hv, hm, pb, hchi, bdif) --
+    runs the full-state step (dclaw_step_full) instead, which also does
+    segregation and entrainment; h_e (my, mx) is then the erodible depth
+    (required with entrainment).
     """
 
     def __init__(self, q: torch.Tensor, b: torch.Tensor, params: DClawParams, dx: float, dy: float,
-                 branch_log: bool = False):
+                 branch_log: bool = False, h_e: torch.Tensor | None = None):
         _require_cuda(q, "q")
         _require_cuda(b, "b")
         self.lib = _lib.load()
         self.params = params
         self.cp = params.to_c()
-        _lib.check(self.lib.dclaw_params_check(ctypes.byref(self.cp)), "parameter check")
+        self.full = q.shape[0] == 7
+        if q.shape[0] not in (5, 7):
+            raise _lib.DClawError("q must have 5 fields (h, hu, hv, hm, pb) or 7 (+ hchi, bdif)")
+        check = self.lib.dclaw_params_check if self.full else self.lib.dclaw_params_check_5
+        _lib.check(check(ctypes.byref(self.cp)), "parameter check")
         _, self.my, self.mx = q.shape
         self.dx, self.dy = float(dx), float(dy)
         dev = q.device
         self.qa = q.contiguous().clone()
         self.qb = torch.empty_like(self.qa)
         self.b = b.contiguous()
-        self.work_bytes = self.lib.dclaw_workspace_bytes(self.mx, self.my)
+        self.h_e = None
+        if h_e is not None:
+            _require_cuda(h_e, "h_e")
+            self.h_e = h_e.contiguous()
+        if self.full:
+            self.work_bytes = self.lib.dclaw_step_full_workspace_bytes(self.mx, self.my)
+        else:
+            self.work_bytes = self.lib.dclaw_workspace_bytes(self.mx, self.my)
         if self.work_bytes == 0:
             raise _lib.DClawError("invalid patch size")
         self.work = torch.empty(self.work_bytes, dtype=torch.uint8, device=dev)
@@ -135,6 +150,13 @@ class PatchStepper:
 
     # ---- stepping ----------------------------------------------------------
     def _launch(self, src: torch.Tensor, dst: torch.Tensor) -> None:
+        if self.full:
+            rc = self.lib.dclaw_step_full(_lib.ptr(src), _lib.ptr(dst), _lib.ptr(self.b), _lib.ptr(self.h_e),
+                                          self.mx, self.my, self.dx, self.dy, ctypes.byref(self.cp),
+                                          _lib.ptr(self.clock), _lib.ptr(self.work), self.work_bytes,
+                                          _lib.ptr(self.brlog), _lib.stream_ptr())
+            _lib.check(rc, "dclaw_step_full")
+            return
         rc = self.lib.dclaw_step(_lib.ptr(src), _lib.ptr(dst), _lib.ptr(self.b), self.mx, self.my, self.dx,
                                  self.dy, ctypes.byref(self.cp), _lib.ptr(self.clock), _lib.ptr(self.work),
                                  self.work_bytes, _lib.ptr(self.brlog), _lib.stream_ptr())
@@ -185,6 +207,8 @@ class PatchStepper:
         band by band when the host tensors are pinned. The stepper's device
         state is not used. Returns once the step is queued on the current
         stream; synchronize it before reading `out`."""
+        if self.full:
+            raise _lib.DClawError("step_host takes the five-field state")
         out = q_host if out is None else out
         for t, name in ((q_host, "q_host"), (out, "out")):
             if t.is_cuda or t.dtype != torch.float64 or not t.is_contiguous():

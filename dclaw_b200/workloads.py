@@ -73,6 +73,48 @@ def slope_runout(n: int = 200, dx: float = 1.0, nsteps: int = 1000, params: DCla
     return Case("slope_runout_200", q, b, dx, dx, p, nsteps, 0.01)
 
 
+def full_state(q: np.ndarray, params: DClawParams) -> np.ndarray:
+    """The reference's whole state (7, my, mx) = (h, hu, hv, hm, pb, hchi,
+    bdif) from a five-field one: hchi = chi0 h where segregation is on, as
+    qinit sets it (qinit.f90:219-226), else 0; no bed eroded yet (bdif = 0)."""
+    z = np.zeros_like(q[0])
+    hchi = params.chi0 * q[0] if params.segregation == 1 else z
+    return np.concatenate([q, hchi[None], z[None]])
+
+
+@dataclasses.dataclass
+class FullCase:
+    """A case on the whole state, with the erodible depth of entrainment."""
+
+    name: str
+    q: np.ndarray        # (7, my, mx)
+    b: np.ndarray
+    h_e: np.ndarray      # (my, mx) erodible depth aux(i_ent)
+    dx: float
+    dy: float
+    params: DClawParams
+    nsteps: int
+    dt_initial: float
+
+
+def slope_runout_full(n: int = 200, segregation: int = 1, entrainment: int = 1, beta_seg: float = 0.3,
+                      erodible: float = 0.5, params: DClawParams | None = None) -> FullCase:
+    """The slope-runout case on the whole state: with segregation a mixture of
+    half and half species (chi0 = 0.5) and a species flux coefficient
+    beta_seg; with entrainment (method 0, ent_dclaw4) an erodible layer of
+    `erodible` m on the slope below the release (x in [60, 150] of 200),
+    solid fraction me = 0.65."""
+    base = slope_runout(n=n)
+    p = (params or base.params).replace(segregation=segregation, beta_seg=beta_seg, entrainment=entrainment,
+                                        entrainment_method=0)
+    x = (np.arange(n) + 0.5) * base.dx
+    X = np.broadcast_to(x[None, :], base.b.shape)
+    L = n * base.dx
+    h_e = np.where((X >= 0.3 * L) & (X <= 0.75 * L), erodible, 0.0)
+    return FullCase(f"slope_runout_full_{n}", full_state(base.q, p), base.b, np.ascontiguousarray(h_e),
+                    base.dx, base.dy, p, base.nsteps, base.dt_initial)
+
+
 def gaussian_random_field(n: int, dx: float, rms: float, slope: float, seed: int) -> np.ndarray:
     """Isotropic Gaussian random field with power spectrum ~ k^slope (slope -3),
     zero mean, scaled to the given RMS."""

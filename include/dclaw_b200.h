@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define DCLAW_ABI_VERSION 1
+#define DCLAW_ABI_VERSION 2
 
 /* return / status codes */
 #define DCLAW_OK 0
@@ -81,8 +81,8 @@ typedef struct dclaw_params {
     int32_t alphamethod;          /* 0 or 1 */
     int32_t rarecorrectortest;    /* 0/1 */
     int32_t bed_normal;           /* must be 0 */
-    int32_t entrainment;          /* must be 0 */
-    int32_t segregation;          /* must be 0 */
+    int32_t entrainment;          /* 0, or 1 on the full-state step only (dclaw_step_full) */
+    int32_t segregation;          /* 0, or 1 on the full-state step only (dclaw_step_full) */
     int32_t curvature;            /* must be 0 */
     /* clawdata */
     int32_t order;                /* method(2): 1 or 2 */
@@ -93,6 +93,17 @@ typedef struct dclaw_params {
     double cfl_desired;
     double cfl_max;
     double dt_max;
+    /* segregation and entrainment (dclaw_data, src/python/dclaw/data.py:338-347);
+     * read only by dclaw_step_full */
+    double beta_seg;              /* species flux: alpha_seg = 1 - beta_seg (riemannsolvers_dclaw.f:88,464-468) */
+    double delta_kr_order;        /* segregation = 1: kperm times 10^(delta_kr_order 2 (chi - 1/2))
+                                     (digclaw_module.f90:418-431) */
+    double chie;                  /* species fraction of entrained material (entrainment.f90:87) */
+    double me;                    /* solid fraction of the erodible layer (entrainment.f90:59) */
+    double entrainment_rate;      /* entrainment.f90:66-73 */
+    int32_t entrainment_method;   /* 0: ent_dclaw4 (entrainment.f90:27-100); 1: none, as the
+                                     reference's method 1 (src2.f90:256-262) */
+    int32_t pad_;
 } dclaw_params;
 
 /*
@@ -127,6 +138,12 @@ const char* dclaw_error_string(int code);
 void dclaw_params_default(dclaw_params* p);
 /* host-side validation; returns DCLAW_OK, DCLAW_ERR_ARG or DCLAW_ERR_UNSUPPORTED */
 int dclaw_params_check(const dclaw_params* p);
+/* dclaw_params_check, and DCLAW_ERR_UNSUPPORTED for segregation or
+ * entrainment: the entry points on the five-field state (h, hu, hv, hm, pb)
+ * carry no species fraction hchi and no bed change; those options need the
+ * full-state step dclaw_step_full. (Ensemble members of dclaw_step_batched
+ * must pass this check too.) */
+int dclaw_params_check_5(const dclaw_params* p);
 /* bytes of device workspace the step entry points need for an mx x my patch */
 size_t dclaw_workspace_bytes(int mx, int my);
 
@@ -165,6 +182,30 @@ int dclaw_src2(double* q, const double* aux, int mx, int my, int mbc, double dx,
 int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int my,
                double dx, double dy, const dclaw_params* p, dclaw_clock* clock,
                void* work, size_t work_bytes, uint32_t* branch_log, void* stream);
+/* The step on the reference's whole state, for segregation and entrainment.
+ * The reference carries q(7) = (h, hu, hv, hm, pb, hchi, bdif)
+ * (digclaw_module.f90:96-102); this entry point takes and returns those
+ * seven fields as (7, my, mx) planes (interior, x fastest, device):
+ * hchi = h chi (species fraction chi, clipped to [0, 1] by qfix), bdif = the
+ * bed eroded so far (the step sees the bed b - bdif). It is stepgrid's patch
+ * step like dclaw_step (b4step2.f90:7, step2 and src2.f90:27 with tick's dt
+ * rule) with every option of dclaw_step plus
+ *   segregation = 1: kperm times 10^(delta_kr_order 2 (chi - 1/2)) in setvars
+ *                    (digclaw_module.f90:418-431); the species waves use
+ *                    alpha_seg = 1 - beta_seg (riemannsolvers_dclaw.f:88,463-468)
+ *                    whatever segregation is, as the reference's do;
+ *   entrainment = 1, entrainment_method = 0: ent_dclaw4 in src2
+ *                    (src2.f90:252-262, entrainment.f90:27-100), eroding
+ *                    up to h_e - bdif, h_e (my, mx) on the device = the
+ *                    erodible depth aux(i_ent) (required then; nullable
+ *                    otherwise).
+ * With hchi = bdif = 0 and both options off it returns dclaw_step's bits for
+ * the first five fields. work holds dclaw_step_full_workspace_bytes(mx, my);
+ * branch_log as for dclaw_step. One launch per stage (seven). */
+int dclaw_step_full(const double* q_in, double* q_out, const double* b, const double* h_e, int mx, int my,
+                    double dx, double dy, const dclaw_params* p, dclaw_clock* clock, void* work,
+                    size_t work_bytes, uint32_t* branch_log, void* stream);
+size_t dclaw_step_full_workspace_bytes(int mx, int my);
 /* Allocation-free variant of dclaw_step. No counterpart in the reference:
  * it exists for callers that drive the step from code with no device
  * allocator of their own -- a Fortran time loop bound through iso_c_binding

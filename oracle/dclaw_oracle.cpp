@@ -59,7 +59,7 @@ constexpr int MBC = 2;
 // q indices (digclaw_module.f90:96-102), 1-based as in Fortran
 constexpr int I_H = 1, I_HU = 2, I_HV = 3, I_HM = 4, I_PB = 5, I_HCHI = 6, I_BDIF = 7;
 // aux indices for a Cartesian run (digclaw_module.f90:83-110)
-constexpr int I_PHI = 2, I_THETA = 3, I_FSPHI = 4, I_TAUDIR_X = 5, I_TAUDIR_Y = 6;
+constexpr int I_PHI = 2, I_THETA = 3, I_FSPHI = 4, I_TAUDIR_X = 5, I_TAUDIR_Y = 6, I_ENT = 7;
 
 // branch bits, shared meaning with the CUDA path
 constexpr uint32_t BR_DRY = 1u << 0, BR_WALL = 1u << 1, BR_SONIC = 1u << 2, BR_STATIC = 1u << 3,
@@ -79,6 +79,7 @@ inline double E_tan(double x) { return g_portable_libm ? dclaw::em::d_tan(x) : s
 inline double E_tanh(double x) { return g_portable_libm ? dclaw::em::d_tanh(x) : std::tanh(x); }
 inline double E_pow73(double x) { return g_portable_libm ? dclaw::em::d_pow_7_3(x) : std::pow(x, 7.0 / 3.0); }
 inline double E_log(double x) { return g_portable_libm ? dclaw::em::d_log(x) : std::log(x); }
+inline double E_pow(double x, double y) { return g_portable_libm ? dclaw::em::d_pow(x, y) : std::pow(x, y); }
 // Fortran MAX/MIN with two arguments
 inline double fmax2(double a, double b) { return a > b ? a : b; }
 inline double fmin2(double a, double b) { return a < b ? a : b; }
@@ -135,13 +136,14 @@ void qfix_cmass(const Model& M, double& h, double& m, double& p, double& rho, do
     hm = h * m;
 }
 
-// digclaw_module.f90:394-491 (segregation = 0: kr_chi = 1)
-void setvars(const Model& M, double h, double u, double v, double m, double p, double /*chi*/,
+// digclaw_module.f90:394-491
+void setvars(const Model& M, double h, double u, double v, double m, double p, double chi,
              double gz, double& rho, double& kperm, double& alphainv, double& m_eq,
              double& tanpsi, double& tau) {
     const dclaw_params& P = M.p;
     rho = m * (P.rho_s - P.rho_f) + P.rho_f;
     double kr_chi = 1.0;
+    if (P.segregation == 1) kr_chi = E_pow(10.0, P.delta_kr_order * 2.0 * (chi - 0.5));
     kperm = kr_chi * P.kref * E_exp(-(m - P.mref) / (0.04));
     double sig_eff = fmax2(0.0, rho * gz * h - p);
     double sig_0 = 0.0;
@@ -401,7 +403,7 @@ void riemann_dig2_aug_sswave_ez(Model& M, double hL, double hR, double huL, doub
     double gzR = grav * std::cos(thetaR);
     double theta = 0.5 * (thetaL + thetaR);
     double gz = grav * std::cos(theta);
-    double alpha_seg = 1.0 - 0.0; // beta_seg = 0 (segregation off)
+    double alpha_seg = 1.0 - P.beta_seg;  // riemannsolvers_dclaw.f:88
 
     double rhoL, rhoR, tauL, tauR, kperm, alphainv, m_eq, tanpsi, h, v, mbar;
     (void)v; (void)mbar;
@@ -1478,6 +1480,39 @@ void mp_update_FE_4quad(Model& M, double dt, double& h, double u, double v, doub
 }
 
 // src2.f90:27-306 (bed_normal = 0, curvature = 0, entrainment = 0)
+// entrainment.f90:27-100 (its hm is local: the caller's is not updated)
+void ent_dclaw4(const Model& M, double dt, double& h, double& u, double& v, double& m, double& p, double& rho,
+                double& hchi, double gz, double tau, double b_x, double b_y, double& b_eroded, double b_remaining) {
+    const dclaw_params& P = M.p;
+    (void)b_x; (void)b_y;
+    double coeff;
+    if (P.friction_forcing) coeff = P.manning_coefficient;
+    else coeff = 0.0;
+    double vnorm = std::sqrt(sq(u) + sq(v));
+    double vlow = 0.1;
+    if (vnorm > vlow) {
+        if (b_remaining > 0.0) {
+            double rhoe = P.me * P.rho_s + (1.0 - P.me) * P.rho_f;
+            double beta = fmax2(1.0 - m, 0.1);
+            double visc = beta * vnorm * 2.0 * P.mu * (1.0 - m) / (E_tanh(h + 1.0e-2));
+            double gamma = rho * beta * (sq(vnorm)) * (beta * gz * sq(coeff)) / (E_pow(E_tanh(h + 1.0e-2), 1.0 / 3.0));
+            double t1bot = visc + gamma + tau;
+            double t2top = fmin2(t1bot, (1.0 - beta * P.entrainment_rate) * tau);
+            double prat = p / (rho * h);
+            double dh = P.entrainment_rate * dt * (t1bot - t2top) / (rhoe * beta * vnorm);
+            dh = fmin2(dh, b_remaining);
+            h = h + dh;
+            double hm = h * m + dh * P.me;
+            m = hm / h;
+            hchi = hchi + dh * P.chie;
+            double hrho = hm * P.rho_s + (h - hm) * P.rho_f;
+            rho = hrho / h;
+            b_eroded = b_eroded + dh;
+            p = prat * hrho;
+        }
+    }
+}
+
 void src2(Model& M, Patch& pt, double dt) {
     const dclaw_params& P = M.p;
     const int mx = pt.mx, my = pt.my;
@@ -1543,6 +1578,17 @@ void src2(Model& M, Patch& pt, double dt) {
                 continue;
             }
             setvars(Mt, h, u, v, m, p, chi, gz, rho, kperm, alphainv, m_eq, tanpsi, tau);
+            if (P.entrainment == 1) {
+                // src2.f90:252-262. ent_dclaw4 is also handed the bed slopes
+                // b_x, b_y (src2.f90:133-147) but never reads them.
+                const double b_x = 0.0, b_y = 0.0;
+                double b_eroded = pt.Q(I_BDIF, i, j);
+                double b_remaining = pt.A(I_ENT, i, j) - b_eroded;
+                if (P.entrainment_method == 0) {
+                    ent_dclaw4(Mt, dt, h, u, v, m, p, rho, hchi, gz, tau, b_x, b_y, b_eroded, b_remaining);
+                    pt.Q(I_BDIF, i, j) = b_eroded;
+                }
+            }
             if (P.friction_forcing && coeffmanning > 0.0) {
                 if (h <= P.friction_depth) {
                     double cm = coeffmanning;
@@ -1641,6 +1687,27 @@ void get_state(Patch& pt, double* q_soa) {
         for (int i = 1; i <= mx; ++i) {
             size_t c = (size_t)(j - 1) * mx + (i - 1);
             for (int m = 1; m <= 5; ++m) q_soa[(m - 1) * plane + c] = pt.Q(m, i, j);
+        }
+}
+
+// the whole state, 7 interior planes (h, hu, hv, hm, pb, hchi, bdif)
+void put_state_full(Patch& pt, const double* q_soa) {
+    const int mx = pt.mx, my = pt.my;
+    const size_t plane = (size_t)mx * my;
+    for (int j = 1; j <= my; ++j)
+        for (int i = 1; i <= mx; ++i) {
+            size_t c = (size_t)(j - 1) * mx + (i - 1);
+            for (int m = 1; m <= MEQN; ++m) pt.Q(m, i, j) = q_soa[(m - 1) * plane + c];
+        }
+}
+
+void get_state_full(Patch& pt, double* q_soa) {
+    const int mx = pt.mx, my = pt.my;
+    const size_t plane = (size_t)mx * my;
+    for (int j = 1; j <= my; ++j)
+        for (int i = 1; i <= mx; ++i) {
+            size_t c = (size_t)(j - 1) * mx + (i - 1);
+            for (int m = 1; m <= MEQN; ++m) q_soa[(m - 1) * plane + c] = pt.Q(m, i, j);
         }
 }
 
@@ -1762,14 +1829,18 @@ int oracle_threads(int n) {
  * (my+2)*(mx+1) and (mx+2)*(my+1).
  * Returns 0, or 3 if a NaN appeared (the step where it appeared is not taken).
  */
-int oracle_run(const dclaw_params* prm, int mx, int my, double dx, double dy, double* q,
-               const double* b, int nsteps, double dt_initial, double t_final, int fixed_dt,
-               int parallel, double* dt_hist, double* cfl_hist, uint32_t* xlog, uint32_t* ylog,
-               double* t_out, double t_obs) {
+static int run_patch(const dclaw_params* prm, int mx, int my, double dx, double dy, double* q,
+                     const double* b, const double* h_e, bool full, int nsteps, double dt_initial,
+                     double t_final, int fixed_dt, int parallel, double* dt_hist, double* cfl_hist,
+                     uint32_t* xlog, uint32_t* ylog, double* t_out, double t_obs) {
     Model M = make_model(prm);
     Patch pt(mx, my);
-    put_state(pt, q);
+    if (full) put_state_full(pt, q);
+    else put_state(pt, q);
     setaux(M.p, pt, b);
+    if (h_e)
+        for (int j = 1; j <= my; ++j)
+            for (int i = 1; i <= mx; ++i) pt.A(I_ENT, i, j) = h_e[(size_t)(j - 1) * mx + (i - 1)];
     Fluxes F(mx, my);
     double t = 0.0, dt = dt_initial;
     int status = 0;
@@ -1790,9 +1861,28 @@ int oracle_run(const dclaw_params* prm, int mx, int my, double dx, double dy, do
         t = t + dtn;
         if (!fixed_dt) dt = next_dt(M.p, dtn, cfl);
     }
-    get_state(pt, q);
+    if (full) get_state_full(pt, q);
+    else get_state(pt, q);
     if (t_out) *t_out = t;
     return status;
+}
+
+int oracle_run(const dclaw_params* prm, int mx, int my, double dx, double dy, double* q,
+               const double* b, int nsteps, double dt_initial, double t_final, int fixed_dt,
+               int parallel, double* dt_hist, double* cfl_hist, uint32_t* xlog, uint32_t* ylog,
+               double* t_out, double t_obs) {
+    return run_patch(prm, mx, my, dx, dy, q, b, nullptr, false, nsteps, dt_initial, t_final, fixed_dt, parallel,
+                     dt_hist, cfl_hist, xlog, ylog, t_out, t_obs);
+}
+
+/* the whole state: q holds 7 planes (h, hu, hv, hm, pb, hchi, bdif); h_e
+ * (nullable) the erodible depth aux(i_ent) of the interior cells */
+int oracle_run_full(const dclaw_params* prm, int mx, int my, double dx, double dy, double* q,
+                    const double* b, const double* h_e, int nsteps, double dt_initial, double t_final,
+                    int fixed_dt, int parallel, double* dt_hist, double* cfl_hist, uint32_t* xlog,
+                    uint32_t* ylog, double* t_out) {
+    return run_patch(prm, mx, my, dx, dy, q, b, h_e, true, nsteps, dt_initial, t_final, fixed_dt, parallel,
+                     dt_hist, cfl_hist, xlog, ylog, t_out, 0.0);
 }
 
 /* Patch-call oracles on the padded SoA layout (5 q planes, 6 aux planes). */

@@ -58,6 +58,10 @@ class Oracle:
         L.oracle_run.argtypes = [ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                  ctypes.c_double, _dp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                  ctypes.c_int, ctypes.c_int, _dp, _dp, _up, _up, _dp, ctypes.c_double]
+        L.oracle_run_full.restype = ctypes.c_int
+        L.oracle_run_full.argtypes = [ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                      ctypes.c_double, _dp, _dp, _dp, ctypes.c_int, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp, _dp, _up, _up, _dp]
         L.oracle_threads.restype = ctypes.c_int
         L.oracle_threads.argtypes = [ctypes.c_int]
         for name in ("oracle_bc2amr",):
@@ -117,6 +121,28 @@ class Oracle:
         st = self.lib.oracle_run(ctypes.byref(cp), mx, my, dx, dy, _ptr(q), _ptr(b), nsteps, dt_initial,
                                  t_final, int(fixed_dt), int(parallel), _ptr(dt_hist), _ptr(cfl_hist),
                                  _ptr(xlog, _up), _ptr(ylog, _up), _ptr(t_out), float(t_obs))
+        return dict(q=q, dt=dt_hist[:nsteps], cfl=cfl_hist[:nsteps], t=float(t_out[0]), status=st,
+                    xlog=xlog, ylog=ylog)
+
+    def run_full(self, p: DClawParams, q: np.ndarray, b: np.ndarray, dx: float, dy: float, nsteps: int,
+                 dt_initial: float, h_e: np.ndarray | None = None, t_final: float = 0.0, fixed_dt: bool = False,
+                 parallel: bool = True, branch_log: bool = False, libm: str = "glibc"):
+        """The whole state: q (7, my, mx) = (h, hu, hv, hm, pb, hchi, bdif);
+        h_e (my, mx): the erodible depth (entrainment). Same results as run()."""
+        self.set_libm(libm)
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        he = None if h_e is None else np.ascontiguousarray(h_e, dtype=np.float64)
+        _, my, mx = q.shape
+        dt_hist = np.zeros(max(nsteps, 1))
+        cfl_hist = np.zeros(max(nsteps, 1))
+        xlog = np.zeros((my + 2, mx + 1), dtype=np.uint32) if branch_log else None
+        ylog = np.zeros((mx + 2, my + 1), dtype=np.uint32) if branch_log else None
+        t_out = np.zeros(1)
+        cp = p.to_c()
+        st = self.lib.oracle_run_full(ctypes.byref(cp), mx, my, dx, dy, _ptr(q), _ptr(b), _ptr(he), nsteps,
+                                      dt_initial, t_final, int(fixed_dt), int(parallel), _ptr(dt_hist),
+                                      _ptr(cfl_hist), _ptr(xlog, _up), _ptr(ylog, _up), _ptr(t_out))
         return dict(q=q, dt=dt_hist[:nsteps], cfl=cfl_hist[:nsteps], t=float(t_out[0]), status=st,
                     xlog=xlog, ylog=ylog)
 

@@ -36,6 +36,25 @@ class Emu:
                            _dp, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp, _dp, _up,
                            _dp]
         self.lib.emu_run_fused.argtypes = self.lib.emu_run_fused.argtypes + [ctypes.c_int] * 3
+        self.lib.emu_run_full.restype = ctypes.c_int
+        self.lib.emu_run_full.argtypes = [ctypes.POINTER(CParams), ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                          ctypes.c_double, _dp, _dp, _dp, ctypes.c_int, ctypes.c_double, _dp, _dp,
+                                          _up]
+
+    def run_full(self, p, q, b, dx, dy, nsteps, dt_initial, h_e=None):
+        """The full-state stages (7 fields) on the host."""
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        he = None if h_e is None else np.ascontiguousarray(h_e, dtype=np.float64)
+        _, my, mx = q.shape
+        dth = np.zeros(max(nsteps, 1))
+        cfh = np.zeros(max(nsteps, 1))
+        br = np.zeros((my + 2) * (mx + 1) + (mx + 2) * (my + 1), dtype=np.uint32)
+        cp = p.to_c()
+        st = self.lib.emu_run_full(ctypes.byref(cp), mx, my, dx, dy, q.ctypes.data_as(_dp), b.ctypes.data_as(_dp),
+                                   None if he is None else he.ctypes.data_as(_dp), nsteps, dt_initial,
+                                   dth.ctypes.data_as(_dp), cfh.ctypes.data_as(_dp), br.ctypes.data_as(_up))
+        return dict(q=q, dt=dth[:nsteps], cfl=cfh[:nsteps], status=st, br=br)
 
     def run(self, p, q, b, dx, dy, nsteps, dt_initial, t_final=0.0, fixed_dt=False, fused=False, tile=(16, 14),
             src2_in_tile=False):

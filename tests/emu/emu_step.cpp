@@ -7,6 +7,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <vector>
+#include "../../dclaw_b200/csrc/full_state.cuh"
 #include "../../dclaw_b200/csrc/stages.cuh"
 #include "../../dclaw_b200/csrc/tile.cuh"
 
@@ -172,4 +173,68 @@ extern "C" int emu_run_fused(const dclaw_params* P, int mx, int my, double dx, d
     DCLAW_EMU_TILE(13, 14)
     DCLAW_EMU_TILE(8, 8)
     return -1;
+}
+
+// The full-state step (full_state.cuh) in the kernels' launch order.
+extern "C" int emu_run_full(const dclaw_params* P, int mx, int my, double dx, double dy, double* q, const double* b,
+                            const double* he, int nsteps, double dt_initial, double* dt_hist, double* cfl_hist,
+                            uint32_t* brlog) {
+    Geom g{mx, my, mx + 4, my + 4, dx, dy};
+    const FullLayout L = full_layout(mx, my);
+    std::vector<unsigned char> mem(L.total);
+    WorkF W = make_work_full(mem.data(), L);
+    const size_t nq = (size_t)NQF * mx * my;
+    std::vector<double> qa(q, q + nq), qb(nq);
+    double dt = dt_initial;
+    int status = 0;
+    for (int n = 0; n < nsteps; ++n) {
+        uint32_t* br = (n == nsteps - 1 && brlog) ? brlog : nullptr;
+        for (int j = -1; j <= my + 2; ++j)
+            for (int i = -1; i <= mx + 2; ++i)
+                if (full_b4(*P, g, qa.data(), b, W, i, j)) status = DCLAW_ERR_NAN;
+        if (status) break;
+        for (int j = -1; j <= my + 2; ++j)
+            for (int i = -1; i <= mx + 2; ++i) full_taudir(*P, g, W, i, j);
+        double cfl = 0.0;
+        for (int r = 0; r <= my + 1; ++r)
+            for (int i = 0; i <= mx + 2; ++i) {
+                uint32_t bits = 0;
+                double s = full_riemann<0>(*P, g, W, r, i, &bits);
+                if (i >= 1 && i <= mx + 1) {
+                    cfl = fmax2(cfl, (dt / dx) * s);
+                    if (br) br[(size_t)r * (mx + 1) + (i - 1)] = bits;
+                }
+            }
+        for (int c = 0; c <= mx + 1; ++c)
+            for (int k = 0; k <= my + 2; ++k) {
+                uint32_t bits = 0;
+                double s = full_riemann<1>(*P, g, W, c, k, &bits);
+                if (k >= 1 && k <= my + 1) {
+                    cfl = fmax2(cfl, (dt / dy) * s);
+                    if (br) br[(size_t)(my + 2) * (mx + 1) + (size_t)c * (my + 1) + (k - 1)] = bits;
+                }
+            }
+        for (int r = 0; r <= my + 1; ++r)
+            for (int i = 1; i <= mx + 1; ++i) {
+                uint32_t bits = 0;
+                full_flux<0>(*P, g, W, r, i, dt / dx, br ? &bits : nullptr);
+                if (br) br[(size_t)r * (mx + 1) + (i - 1)] |= bits;
+            }
+        for (int c = 0; c <= mx + 1; ++c)
+            for (int k = 1; k <= my + 1; ++k) {
+                uint32_t bits = 0;
+                full_flux<1>(*P, g, W, c, k, dt / dy, br ? &bits : nullptr);
+                if (br) br[(size_t)(my + 2) * (mx + 1) + (size_t)c * (my + 1) + (k - 1)] |= bits;
+            }
+        for (int j = 1; j <= my; ++j)
+            for (int i = 1; i <= mx; ++i)
+                if (full_finalize(*P, g, W, he, qb.data(), i, j, dt)) status = DCLAW_ERR_NAN;
+        qa.swap(qb);
+        if (dt_hist) dt_hist[n] = dt;
+        if (cfl_hist) cfl_hist[n] = cfl;
+        dt = tick_next_dt(*P, dt, cfl);
+        if (status) break;
+    }
+    memcpy(q, qa.data(), sizeof(double) * nq);
+    return status;
 }

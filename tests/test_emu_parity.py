@@ -75,3 +75,53 @@ def test_fused_tile_shapes_and_partial_tiles(oracle, emu, tile, src2_in_tile):
                  src2_in_tile=src2_in_tile)
     assert np.array_equal(r1["q"], r2["q"])
     assert np.array_equal(np.concatenate([r1["xlog"].ravel(), r1["ylog"].ravel()]), r2["br"])
+
+
+# ---- the full-state step (segregation, entrainment) --------------------------
+FULL_VARIANTS = {
+    "extras_zero": dict(segregation=0, entrainment=0),
+    "segregation": dict(),
+    "segregation_beta0": dict(beta_seg=0.0),
+    "entrainment_only": dict(segregation=0),
+    "both_manning": dict(friction_forcing=True, manning_coefficient=0.03),
+    "both_src2m1": dict(src2method=1),
+    "both_swe": dict(src2method=-1),
+    "both_src2m2": dict(src2method=2, alphamethod=1),
+    "both_order1": dict(order=1, transverse_waves=0),
+    "both_extrap": dict(bc_lower=("extrap", "wall"), bc_upper=("extrap", "extrap")),
+    "entrainment_method1": dict(entrainment_method=1),
+}
+
+
+@pytest.mark.parametrize("variant", sorted(FULL_VARIANTS))
+def test_full_state_stages(oracle, emu, variant):
+    """The full-state stages (dclaw_b200/csrc/full_state.cuh) on the host
+    against the oracle's seven-field step: state (hchi and bdif included),
+    dt/Courant histories and branch bits, bit for bit."""
+    kw = dict(FULL_VARIANTS[variant])
+    seg = kw.pop("segregation", 1)
+    ent = kw.pop("entrainment", 1)
+    c = W.slope_runout_full(n=96, segregation=seg, entrainment=ent)
+    p = c.params.replace(**kw)
+    r1 = oracle.run_full(p, c.q, c.b, c.dx, c.dy, 60, c.dt_initial, h_e=c.h_e, branch_log=True, libm="portable")
+    r2 = emu.run_full(p, c.q, c.b, c.dx, c.dy, 60, c.dt_initial, h_e=c.h_e)
+    assert r1["status"] == r2["status"] == 0
+    assert np.array_equal(r1["q"], r2["q"])
+    assert np.array_equal(r1["dt"], r2["dt"]) and np.array_equal(r1["cfl"], r2["cfl"])
+    assert np.array_equal(np.concatenate([r1["xlog"].ravel(), r1["ylog"].ravel()]), r2["br"])
+    if seg:
+        chi = r1["q"][5][r1["q"][0] > 0] / r1["q"][0][r1["q"][0] > 0]
+        assert chi.min() >= 0.0 and chi.max() <= 1.0
+    if ent and p.entrainment_method == 0:
+        assert r1["q"][6].max() > 0.0 and r1["q"][6].max() <= c.h_e.max()
+    else:
+        assert not r1["q"][6].any()
+
+
+def test_full_state_without_extras_is_the_five_field_step(oracle):
+    """hchi = bdif = 0 with both options off: the oracle's seven-field run
+    gives the five-field run's bits and keeps the extra fields zero."""
+    c = W.slope_runout(n=96)
+    a = oracle.run(c.params, c.q, c.b, c.dx, c.dy, 40, c.dt_initial, libm="portable")
+    f = oracle.run_full(c.params, W.full_state(c.q, c.params), c.b, c.dx, c.dy, 40, c.dt_initial, libm="portable")
+    assert np.array_equal(a["q"], f["q"][:5]) and not f["q"][5:].any()

@@ -28,7 +28,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_host_side_helpers():
     lib = _lib.load()
-    assert lib.dclaw_abi_version() == 1
+    assert lib.dclaw_abi_version() == 2
     p = CParams()
     lib.dclaw_params_default(ctypes.byref(p))
     assert p.grav == 9.81 and p.limiter == 4 and p.order == 2
