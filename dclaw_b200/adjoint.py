@@ -109,7 +109,7 @@ class StepAdjoint:
 
 
 def _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, dt_of, lam, lam2, pbar, add_outs, bed_for=None,
-                        bbar=None):
+                        bbar=None, after_reverse=None):
     """The step adjoints of steps n_steps .. 1, each step's prepare queued on
     a side stream ahead of the previous step's reverse.
 
@@ -122,7 +122,9 @@ def _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, dt_of, lam, lam
     n's dt; add_outs(n, lam): adds the output gradients at step count n;
     bed_for(n, adj) (a moving bed): fills adj's bed with step n's, on the
     side stream once adj's workspace is free. bbar (optional): accumulates
-    the bed's adjoint over the steps.
+    the bed's adjoint over the steps; after_reverse(n) (optional) runs on
+    the reverse stream right after step n's reverse (a moving bed's
+    parameters take that step's bed adjoint from bbar there).
     The reverses run on a high-priority stream and the prepares (which do
     not read lam) on a normal one, so they fill the SMs the reverses leave
     idle. Returns the final (lam, lam2)."""
@@ -159,6 +161,8 @@ def _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, dt_of, lam, lam
             rev.wait_event(ev_prep)
             add_outs(n, lam)
             adjs[w].reverse(state_of(n), dt_of(n), lam, lam2, pbar, bbar)
+            if after_reverse is not None:
+                after_reverse(n)
             last_rev[w] = rev.record_event()
         if n > 1:
             with torch.cuda.stream(side):
@@ -209,7 +213,7 @@ def _block(n_steps: int, checkpoint_block: int | None, state_bytes: int = 0, res
 class _Rollout(torch.autograd.Function):
     @staticmethod
     def forward(ctx, q0, theta, b, params, dx, dy, n_steps, out_steps, dt0, fixed_dt, t_final, checkpoint_block,
-                dt_schedule, select, obs_dt, n_obs, peak):
+                dt_schedule, select, obs_dt, n_obs, peak, *bed_params):
         prm = with_theta(params, theta.detach().cpu())
         # a moving bed: a function of the simulated time, evaluated before
         # every step (the port's step(q, bed(t), ...) loop)
@@ -287,7 +291,7 @@ class _Rollout(torch.autograd.Function):
         # the block inputs are saved tensors: autograd frees them after the
         # backward pass (unless the graph is retained), so a loop of gradient
         # evaluations reuses one allocation instead of holding two
-        ctx.save_for_backward(b, dts, store, t_start)
+        ctx.save_for_backward(b, dts, store, t_start, *bed_params)
         ctx.bed_fn = bed_fn
         ctx.select = select
         ctx.meta = (prm, float(dx), float(dy), int(n_steps), tuple(out_steps), k)
@@ -297,7 +301,7 @@ class _Rollout(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g_out):
-        b, dts, store, t_start = ctx.saved_tensors
+        b, dts, store, t_start, *bed_params = ctx.saved_tensors
         ckpt = list(store.unbind(0))
         prm, dx, dy, n_steps, out_steps, k = ctx.meta
         bed_fn = ctx.bed_fn
@@ -355,22 +359,42 @@ class _Rollout(torch.autograd.Function):
 
         # the bed's gradient, for a fixed bed that requires one
         bbar = torch.zeros_like(b) if bed_fn is None and ctx.needs_input_grad[2] else None
+        # a moving bed's parameters: each step's bed adjoint, through the
+        # step's bed b(t_n) = bed_fn(t_n), summed over the steps
+        pgrads = [None] * len(bed_params)
+        after = None
+        want = [i for i, t in enumerate(bed_params) if ctx.needs_input_grad[17 + i]]
+        if bed_fn is not None and want:
+            bbar = torch.zeros_like(b)
+            pgrads = [torch.zeros_like(t) if i in want else None for i, t in enumerate(bed_params)]
+
+            def after(n):
+                with torch.enable_grad():
+                    bn = bed_fn(t_start[n - 1])
+                    gs = torch.autograd.grad(bn, [bed_params[i] for i in want], bbar, allow_unused=True)
+                for i, gi in zip(want, gs):
+                    if gi is not None:
+                        pgrads[i].add_(gi)
+                bbar.zero_()
+
         lam, lam2 = _pipelined_backward(adjs, n_steps, k, ckpt, segs, recompute, lambda n: dts[n - 1:n], lam,
-                                        lam2, pbar, add_outs, bed_for if bed_fn is not None else None, bbar)
+                                        lam2, pbar, add_outs, bed_for if bed_fn is not None else None, bbar, after)
+        if bed_fn is not None:
+            bbar = None
         add_outs(0, lam)
         _lib.check(fw.status(), "rollout recompute")
         for adj in adjs:
             adj.check_status()
         scale = torch.tensor([_DEG, 1.0, 1.0, 1.0], dtype=torch.float64, device=dev)
         return (lam, pbar * scale, bbar, None, None, None, None, None, None, None, None, None, None, None, None, None,
-                None)
+                None, *pgrads)
 
 
 def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams, dx: float,
                    dy: float, n_steps: int, out_steps: Sequence[int], dt0: float, fixed_dt: bool = False,
                    t_final: float = 0.0, checkpoint_block: int | None = None,
                    dt_schedule: torch.Tensor | None = None, select: torch.Tensor | None = None,
-                   obs_dt: float = 0.0) -> torch.Tensor:
+                   obs_dt: float = 0.0, bed_params: Sequence[torch.Tensor] = ()) -> torch.Tensor:
     """Differentiable run of n_steps fused steps on one patch.
 
     q0: (5, my, mx) float64 CUDA tensor (x fastest), theta: (4,) float64
@@ -380,7 +404,10 @@ def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams
     step as the port's loops do (e.g. `solver.gate_bed`). A fixed bed that
     requires grad gets its gradient (through calc_taudir's surface slopes
     and the solver's bed step), as the port's rollout_peak is differentiated
-    with respect to the whole bed; a moving bed is not differentiated.
+    with respect to the whole bed. A moving bed is differentiated with
+    respect to bed_params, the tensors the function reads (for `gate_bed`:
+    the gate's ridge, its times and its angles, as tensors that require
+    grad): each step's bed adjoint goes back through that step's b(t_n).
     Returns the states after each step count in out_steps (0 = q0), shape
     (len(out_steps), 5, my, mx). dt0 is the first dt; with
     fixed_dt every step uses it, otherwise the tick rule picks the next dt
@@ -409,13 +436,14 @@ def rollout_states(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams
     return _Rollout.apply(q0, theta, b if callable(b) else b.contiguous(), params, dx, dy, int(n_steps),
                           tuple(int(n) for n in out_steps),
                           float(dt0), bool(fixed_dt), float(t_final), checkpoint_block, dt_schedule, select,
-                          float(obs_dt), 0, False)
+                          float(obs_dt), 0, False, *tuple(bed_params))
 
 
 def rollout_observations(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams, dx: float, dy: float,
                          n_steps: int, obs_dt: float, n_obs: int, dt0: float, t_end: float = 0.0,
                          select: torch.Tensor | None = None, checkpoint_block: int | None = None,
-                         dt_schedule: torch.Tensor | None = None) -> torch.Tensor:
+                         dt_schedule: torch.Tensor | None = None,
+                         bed_params: Sequence[torch.Tensor] = ()) -> torch.Tensor:
     """Differentiable run that records observations at fixed times, as the
     port's flume loop does (pf_flume/flume_model.py:150-158): every tick-rule
     dt is clipped at the next multiple of obs_dt (and at t_end when
@@ -434,12 +462,13 @@ def rollout_observations(q0: torch.Tensor, theta: torch.Tensor, b, params: DClaw
         dt_schedule = dt_schedule.contiguous()
     return _Rollout.apply(q0, theta, b if callable(b) else b.contiguous(), params, dx, dy, int(n_steps), (),
                           float(dt0), False, float(t_end), checkpoint_block, dt_schedule, select, float(obs_dt),
-                          int(n_obs), False)
+                          int(n_obs), False, *tuple(bed_params))
 
 
 def rollout_peak(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams, dx: float, dy: float,
                  n_steps: int, dt0: float, t_final: float = 0.0, fixed_dt: bool = False,
-                 checkpoint_block: int | None = None, dt_schedule: torch.Tensor | None = None) -> torch.Tensor:
+                 checkpoint_block: int | None = None, dt_schedule: torch.Tensor | None = None,
+                 bed_params: Sequence[torch.Tensor] = ()) -> torch.Tensor:
     """Differentiable running peak depth over n_steps steps, the loss input
     of the port's rollout_peak (differentiable_dclaw/dclaw_jax/solver.py:
     357-388, differentiated by jax.grad): max over q0 and every step's state
@@ -453,7 +482,7 @@ def rollout_peak(q0: torch.Tensor, theta: torch.Tensor, b, params: DClawParams, 
         dt_schedule = dt_schedule.contiguous()
     return _Rollout.apply(q0, theta, b if callable(b) else b.contiguous(), params, dx, dy, int(n_steps), (),
                           float(dt0), bool(fixed_dt), float(t_final), checkpoint_block, dt_schedule, None, 0.0, 0,
-                          True)
+                          True, *tuple(bed_params))
 
 
 def observation_steps(out: torch.Tensor) -> list:

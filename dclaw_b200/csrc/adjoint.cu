@@ -667,7 +667,7 @@ int dclaw_adjoint_supported(const dclaw_params* p) {
     if (rc) return rc;
     // no adjoint form: the rare-wave corrector's branch structure and
     // src2method 2's data-dependent substeps
-    if (p->rarecorrectortest || p->src2method == 2) return DCLAW_ERR_UNSUPPORTED;
+    if (p->src2method == 2) return DCLAW_ERR_UNSUPPORTED;
     return DCLAW_OK;
 }
 

@@ -367,10 +367,11 @@ DC_HD void zero_sideb(SideB& s) {
 }
 
 // riemann_solve reverse: wb adjoints of the 15 wave outputs; accumulates
-// into Lb, Rb. Returns false for the rare-wave corrector (no adjoint).
+// into Lb, Rb. With the rare-wave corrector (riemannsolvers_dclaw.f:
+// 169-195, 365-386) it follows the forward's choice of the middle speed
+// (s1m, s2m or their mean) and of the eigenvector system.
 DC_HD bool riemann_solve_b(const dclaw_params& P, const Side& L, const Side& R, const Waves& wb, SideB& Lb,
                            SideB& Rb) {
-    if (P.rarecorrectortest) return false;
     const double grav = P.grav;
     const double drytol = P.dry_tolerance;
     double wall1 = 1.0, wall2 = 1.0, wall3 = 1.0;
@@ -448,6 +449,29 @@ DC_HD bool riemann_solve_b(const dclaw_params& P, const Side& L, const Side& R, 
     double Dd = sE2 - sE1;
     double Qh = (huL - huR + sE2 * hR - sE1 * hL) / Dd;
     double hstarHLL = fmax2(Qh, 0.0);
+    // the middle speed: the mean of sw1, sw3 (rsel 0) or the corrector's s1m
+    // (1), s2m (2) or their mean (3); the corrector's eigenvectors when rc
+    double sw2 = 0.5 * (sw3 + sw1);
+    int rsel = 0;
+    bool rc = false;
+    if (P.rarecorrectortest) {
+        double sdelta = sw3 - sw1;
+        double raremin = 0.5, raremax = 0.9;
+        if (rt.rare1 && sE1 * rt.s1m < 0.0) raremin = 0.2;
+        if (rt.rare2 && sE2 * rt.s2m < 0.0) raremin = 0.2;
+        if (rt.rare1 || rt.rare2) {
+            double sghm = sqrt(geps * rt.hm);
+            double rare1st = 3.0 * (cL - sghm);
+            double rare2st = 3.0 * (cR - sghm);
+            if (fmax2(rare1st, rare2st) > raremin * sdelta && fmax2(rare1st, rare2st) < raremax * sdelta) {
+                rc = true;
+                if (rare1st > rare2st) { sw2 = rt.s1m; rsel = 1; }
+                else if (rare2st > rare1st) { sw2 = rt.s2m; rsel = 2; }
+                else { sw2 = 0.5 * (rt.s1m + rt.s2m); rsel = 3; }
+            }
+        }
+        if (hstarHLL < fmin2(hL, hR) / 5.0) rc = false;
+    }
     double delb = (bR - bL);
     double hbar = 0.5 * (hL + hR);
     double s1s2bar = 0.25 * sq(uL + uR) - gz * hbar;
@@ -517,10 +541,26 @@ DC_HD bool riemann_solve_b(const dclaw_params& P, const Side& L, const Side& R, 
             ts0 = 0.5 * (tA + tB);
         }
     }
-    double a = sw1, c = sw3;
+    double a = sw1, c = sw3, bb = sw2;
     double D = c - a;
-    double beta1 = (c * del0 - del1) / D;
-    double beta3 = (del1 - a * del0) / D;
+    double beta1, beta2 = 0.0, beta3, D1 = 0.0, D2 = 0.0, D3 = 0.0;
+    if (!rc) {
+        beta1 = (c * del0 - del1) / D;
+        beta3 = (del1 - a * del0) / D;
+    } else {
+        // the corrector's system needs del2 = del2a - source2dx - tausource
+        double tsrc = 0.0;
+        if (tcase == 1) tsrc = xs;
+        else if (tcase == 2) tsrc = fsign(ts0, xs);
+        if (wallprob) tsrc = 0.0;
+        const double del2 = xs - tsrc;
+        D1 = sq(a) - a * bb - a * c + bb * c;
+        D2 = a * bb - a * c - sq(bb) + bb * c;
+        D3 = a * bb - a * c - bb * c + sq(c);
+        beta1 = (bb * c * del0 - (bb + c) * del1 + del2) / D1;
+        beta2 = (-a * c * del0 + (a + c) * del1 - del2) / D2;
+        beta3 = (a * bb * del0 - (a + bb) * del1 + del2) / D3;
+    }
     double fw11 = beta1 * sw1;
     double fw13 = beta3 * sw3;
     double hustar = huL + fw11;
@@ -532,7 +572,8 @@ DC_HD bool riemann_solve_b(const dclaw_params& P, const Side& L, const Side& R, 
     double sw1b = wb.s1 * wall1, sw2b = wb.s2 * wall2, sw3b = wb.s5 * wall3;
     double fw11b = wb.w1h * wall1, fw21b = wb.w1n * wall1, fw31b = wb.w1t * wall1, fw41b = wb.w1m * wall1,
            fw51b = wb.w1p * wall1;
-    double fw22b = wb.w2n * wall2;  // fw12 = beta2 * 0
+    double fw12b = wb.w2h * wall2;  // fw12 = beta2 R(1,2): 0 without the corrector
+    double fw22b = wb.w2n * wall2;
     double fw13b = wb.w5h * wall3, fw23b = wb.w5n * wall3, fw33b = wb.w5t * wall3, fw43b = wb.w5m * wall3,
            fw53b = wb.w5p * wall3;
     double fw32b, fw42b, fw52b;
@@ -582,26 +623,62 @@ DC_HD bool riemann_solve_b(const dclaw_params& P, const Side& L, const Side& R, 
     // fw11 = beta1 sw1, fw21 = beta1 sw1^2, fw22 = beta2, fw13 = beta3 sw3, fw23 = beta3 sw3^2
     double beta1b = fw11b * sw1 + fw21b * sq(sw1);
     sw1b += fw11b * beta1 + fw21b * beta1 * 2.0 * sw1;
-    double beta2b = fw22b;
+    double beta2b;
+    if (!rc) {
+        beta2b = fw22b;
+    } else {
+        // fw12 = beta2 sw2, fw22 = beta2 sw2^2
+        beta2b = fw12b * sw2 + fw22b * sq(sw2);
+        sw2b += fw12b * beta2 + fw22b * beta2 * 2.0 * sw2;
+    }
     double beta3b = fw13b * sw3 + fw23b * sq(sw3);
     sw3b += fw13b * beta3 + fw23b * beta3 * 2.0 * sw3;
-    // beta1 = (c del0 - del1)/D, beta3 = (del1 - a del0)/D, beta2 = a c del0 - (a+c) del1 + del2
-    double ab_ = 0.0, cb_ = 0.0, del2b = 0.0;
-    cb_ += beta1b * (del0 - beta1) / D;
-    ab_ += beta1b * beta1 / D;
-    del0b += beta1b * c / D;
-    del1b -= beta1b / D;
-    ab_ += beta3b * (beta3 - del0) / D;
-    cb_ -= beta3b * beta3 / D;
-    del1b += beta3b / D;
-    del0b -= beta3b * a / D;
-    ab_ += beta2b * (c * del0 - del1);
-    cb_ += beta2b * (a * del0 - del1);
-    del0b += beta2b * a * c;
-    del1b -= beta2b * (a + c);
-    del2b += beta2b;
+    double ab_ = 0.0, cb_ = 0.0, bbb_ = 0.0, del2b = 0.0;
+    if (!rc) {
+        // beta1 = (c del0 - del1)/D, beta3 = (del1 - a del0)/D, beta2 = a c del0 - (a+c) del1 + del2
+        cb_ += beta1b * (del0 - beta1) / D;
+        ab_ += beta1b * beta1 / D;
+        del0b += beta1b * c / D;
+        del1b -= beta1b / D;
+        ab_ += beta3b * (beta3 - del0) / D;
+        cb_ -= beta3b * beta3 / D;
+        del1b += beta3b / D;
+        del0b -= beta3b * a / D;
+        ab_ += beta2b * (c * del0 - del1);
+        cb_ += beta2b * (a * del0 - del1);
+        del0b += beta2b * a * c;
+        del1b -= beta2b * (a + c);
+        del2b += beta2b;
+    } else {
+        // beta_i = N_i / D_i of the corrector's system (riemannsolvers_dclaw.f:378-385)
+        const double N1b = beta1b / D1, N2b = beta2b / D2, N3b = beta3b / D3;
+        const double D1b = -beta1b * beta1 / D1, D2b = -beta2b * beta2 / D2, D3b = -beta3b * beta3 / D3;
+        // N1 = bb c del0 - (bb + c) del1 + del2
+        bbb_ += N1b * (c * del0 - del1);
+        cb_ += N1b * (bb * del0 - del1);
+        del0b += N1b * bb * c;
+        del1b -= N1b * (bb + c);
+        del2b += N1b;
+        // N2 = -a c del0 + (a + c) del1 - del2
+        ab_ += N2b * (-c * del0 + del1);
+        cb_ += N2b * (-a * del0 + del1);
+        del0b -= N2b * a * c;
+        del1b += N2b * (a + c);
+        del2b -= N2b;
+        // N3 = a bb del0 - (a + bb) del1 + del2
+        ab_ += N3b * (bb * del0 - del1);
+        bbb_ += N3b * (a * del0 - del1);
+        del0b += N3b * a * bb;
+        del1b -= N3b * (a + bb);
+        del2b += N3b;
+        // D1 = a^2 - a bb - a c + bb c, D2 = a bb - a c - bb^2 + bb c, D3 = a bb - a c - bb c + c^2
+        ab_ += D1b * (2.0 * a - bb - c) + D2b * (bb - c) + D3b * (bb - c);
+        bbb_ += D1b * (c - a) + D2b * (a - 2.0 * bb + c) + D3b * (a - c);
+        cb_ += D1b * (bb - a) + D2b * (bb - a) + D3b * (2.0 * c - a - bb);
+    }
     sw1b += ab_;
     sw3b += cb_;
+    sw2b += bbb_;
     // del2 = (del2a - source2dx) - tausource
     del2ab += del2b;
     source2dxb -= del2b;
@@ -721,9 +798,18 @@ DC_HD bool riemann_solve_b(const dclaw_params& P, const Side& L, const Side& R, 
         hLb -= Qb * sE1 / Dd;
     }
     // sw2, sw3, sw1
-    sw3b += 0.5 * sw2b;
-    sw1b += 0.5 * sw2b;
     double s1mb = 0.0, s2mb = 0.0;
+    if (rsel == 0) {
+        sw3b += 0.5 * sw2b;
+        sw1b += 0.5 * sw2b;
+    } else if (rsel == 1) {
+        s1mb += sw2b;
+    } else if (rsel == 2) {
+        s2mb += sw2b;
+    } else {
+        s1mb += 0.5 * sw2b;
+        s2mb += 0.5 * sw2b;
+    }
     if (sE2 > rt.s1m) sE2b += sw3b; else s1mb += sw3b;
     if (sE1 < rt.s2m) sE1b += sw1b; else s2mb += sw1b;
     riemanntype_b(hL, hR, uL, uR, drytol, geps, 0.0, s1mb, s2mb, hLb, hRb, uLb, uRb);

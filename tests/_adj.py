@@ -17,7 +17,8 @@ _dp = ctypes.POINTER(ctypes.c_double)
 LOCAL_CHECKS = ["qfix", "qfix_cmass", "setvars", "setvars_all", "setvars_all_alphamethod1", "riemanntype",
                 "riemann_wet", "riemann_dry_side_or_wall", "riemann_at_rest", "riemann_src2method_-1",
                 "limiter_minmod", "limiter_superbee", "limiter_vanleer", "limiter_mc", "rpt2", "src2_method0",
-                "src2_method1", "src2_method-1", "src2_at_rest", "src2_manning", "src2_dd_manning"]
+                "src2_method1", "src2_method-1", "src2_at_rest", "src2_manning", "src2_dd_manning",
+                "riemann_rare_corrector"]
 
 
 def build() -> Path:

@@ -70,6 +70,8 @@ CASES = {
     "at_rest": dict(seed=3, moving=False),
     # b4step2's speed limit (b4step2.f90:74-100) acting on the faster cells
     "speed_limit": dict(seed=16, p=DClawParams(speed_limit=0.6)),
+    # the rare-wave corrector (riemannsolvers_dclaw.f:169-195)
+    "rare_corrector": dict(seed=17, p=DClawParams(rarecorrectortest=True)),
 }
 
 

@@ -266,6 +266,47 @@ def test_rollout_gradient_with_a_moving_gate_bed(cuda_device):
     _close(float(gt[0]), _fd(lambda h: Lf(q00, th0 + h * e0), eps0=4e-6), "phi")
 
 
+def test_gate_parameter_gradients(cuda_device):
+    """The port differentiates its flume runs with respect to the gate
+    (gate_bed's ridge, opening times and angles, differentiable_dclaw/
+    dclaw_jax/solver.py:304-322). With bed_params the moving bed's step
+    adjoints go back through every step's b(t_n): the gradients of the
+    ridge height, an opening time and an angle match finite differences at
+    the recorded schedule."""
+    from dclaw_b200.solver import gate_bed
+
+    dev = cuda_device
+    p, qn, bn = _small_flow(seed=5)
+    b0 = torch.tensor(bn, device=dev)
+    ridge = torch.zeros_like(b0)
+    ridge[:, 10:12] = 1.0
+    n, outs = 16, [8, 16]
+    wts = torch.tensor(_loss_weights(qn, len(outs), seed=4), device=dev)
+    sched = torch.full((n,), 0.02, dtype=torch.float64, device=dev)
+
+    def run(amp, gt, gd):
+        bed = gate_bed(b0, amp * ridge, gt, gd)
+        q0 = torch.tensor(qn, device=dev)
+        return _run_loss(q0, theta_of(p, dev), bed, p, 1.0, n, outs, wts, dt0=0.0, dt_schedule=sched,
+                         bed_params=(amp, gt, gd))[0]
+
+    amp = torch.tensor(0.5, dtype=torch.float64, device=dev, requires_grad=True)
+    gt = torch.tensor([0.013, 0.231], dtype=torch.float64, device=dev, requires_grad=True)
+    gd = torch.tensor([0.0, 90.0], dtype=torch.float64, device=dev, requires_grad=True)
+    L = run(amp, gt, gd)
+    L.backward()
+    a0, t0, d0 = amp.detach(), gt.detach(), gd.detach()
+
+    def Lf(a, t, d):
+        with torch.no_grad():
+            return float(run(a, t, d))
+
+    e1 = torch.tensor([0.0, 1.0], dtype=torch.float64, device=dev)
+    _close(float(amp.grad), _fd(lambda e: Lf(a0 + e, t0, d0), eps0=1e-6), "ridge height")
+    _close(float(gt.grad[1]), _fd(lambda e: Lf(a0, t0 + e * e1, d0), eps0=1e-6), "opening time")
+    _close(float(gd.grad[1]), _fd(lambda e: Lf(a0, t0, d0 + e * e1), eps0=1e-4), "opening angle")
+
+
 def test_rollout_with_observation_interval(cuda_device):
     """rollout_states(obs_dt=...) steps with the clock clipping dt at every
     observation time: its states equal the fused step's with that clock,
@@ -498,11 +539,12 @@ def test_unsupported_options_are_refused(cuda_device):
 
     b = torch.zeros((8, 8), dtype=torch.float64, device=cuda_device)
     with pytest.raises(_lib.DClawError):
-        StepAdjoint(b, DClawParams(rarecorrectortest=True), 1.0, 1.0)
-    with pytest.raises(_lib.DClawError):
         StepAdjoint(b, DClawParams(src2method=2, alphamethod=1), 1.0, 1.0)
-    # Manning friction has its reverse
+    with pytest.raises(_lib.DClawError):
+        StepAdjoint(b, DClawParams(segregation=1), 1.0, 1.0)
+    # Manning friction and the rare-wave corrector have their reverses
     StepAdjoint(b, DClawParams(friction_forcing=True, manning_coefficient=0.03), 1.0, 1.0)
+    StepAdjoint(b, DClawParams(rarecorrectortest=True), 1.0, 1.0)
 
 
 def test_prepare_then_reverse_equals_the_whole_step_adjoint(cuda_device):
