@@ -546,27 +546,6 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
                 if (ok) cfl = fmax2(cfl, dtd * s);
             }
             __syncthreads();
-            // the limiter phase, in rounds of whole slices: each interface's
-            // limited fluctuations are computed once into registers, then
-            // written over its waves (which no later item of the round reads)
-            {
-                using LG = LimGeom<TX, TY>;
-                const int per = LG::per(dir), nlim = LG::count(dir);
-                const int round = (NT / per) * per;
-                for (int base = 0; base < nlim; base += round) {
-                    double lv[15];
-                    uint32_t lb = 0;
-                    int w = -1;
-                    if (tid < round && base + tid < nlim)
-                        w = tile_limit<TX, TY>(P, g, M, dir, base + tid, i0, j0, dtd, lv, brlog ? &lb : nullptr);
-                    __syncthreads();
-                    if (w >= 0) {
-                        tile_lim_store(M, w, lv);
-                        if (brlog) M.bits[w] |= lb;
-                    }
-                    __syncthreads();
-                }
-            }
             const int ncell = dir == 0 ? (TY + 2) * TX : TY * (TX + 2);
             for (int it = tid; it < ncell; it += NT) tile_flux<TX, TY>(P, g, R, M, dir, it, i0, j0, dtd, brlog);
             __syncthreads();

@@ -421,54 +421,6 @@ DC_HD size_t ylog_off(const Geom& g, int c, int k) {
     return (size_t)(g.my + 2) * (g.mx + 1) + (size_t)c * (g.my + 1) + (size_t)(k - 1);
 }
 
-// ---- the limiter phase: each interface of the flux phase once --------------
-// Limiter items of sweep dir: x, slices = rows j0-1..j0+TY, interfaces
-// i0..i0+TX along each; y, slices = columns i0-1..i0+TX, interfaces
-// j0..j0+TY. The item index runs slice by slice, so that a round of whole
-// slices only reads waves of its own slices (the limiter's neighbours lie
-// along the slice).
-template <int TX, int TY>
-struct LimGeom {
-    static constexpr int PER_X = TX + 1, PER_Y = TY + 1;
-    static constexpr int NX = (TY + 2) * PER_X, NY = (TX + 2) * PER_Y;
-    DC_HD static int per(int dir) { return dir == 0 ? PER_X : PER_Y; }
-    DC_HD static int count(int dir) { return dir == 0 ? NX : NY; }
-};
-
-// Limited fluctuations of limiter item li: out = (amdq[5], apdq[5],
-// cqxx[5]) of the interface, *bits the limiter regime / upwind / wet4 bits.
-// Returns the interface's wave-item index (its slot in M.A), or -1 when the
-// flux phase does not use it (outside the patch).
-template <int TX, int TY>
-DC_HD int tile_limit(const dclaw_params& P, const Geom& g, const TileMem& M, int dir, int li, int i0, int j0,
-                     double dtdx, double out[15], uint32_t* bits) {
-    using LG = LimGeom<TX, TY>;
-    const int per = LG::per(dir);
-    const int sl = (dir == 0 ? j0 - 1 : i0 - 1) + li / per;
-    const int a = (dir == 0 ? i0 : j0) + li % per;
-    const int nslice = dir == 0 ? g.my : g.mx, nlen = dir == 0 ? g.mx : g.my;
-    if (sl < 0 || sl > nslice + 1 || a < 1 || a > nlen + 1) return -1;
-    auto witem = [&](int k) -> int {
-        return dir == 0 ? (sl - (j0 - 1)) * (TX + 3) + (k - (i0 - 1)) : (k - (j0 - 1)) * (TX + 2) + (sl - (i0 - 1));
-    };
-    auto hcell = [&](int aa) -> double { return dir == 0 ? M.h(aa, sl) : M.h(sl, aa); };
-    const double h0[4] = {hcell(a - 2), hcell(a - 1), hcell(a), hcell(a + 1)};
-    iface_limited(P, M, dir, witem(a - 1), witem(a), witem(a + 1), h0, dtdx, out, out + 5, out + 10, bits);
-    return witem(a);
-}
-
-DC_HD void tile_lim_store(const TileMem& M, int w, const double v[15]) {
-    for (int k = 0; k < 15; ++k) M.A[(size_t)k * M.NA + w] = v[k];
-}
-
-DC_HD void tile_lim_load(const TileMem& M, int w, double am[5], double ap[5], double cq[5]) {
-    for (int k = 0; k < 5; ++k) {
-        am[k] = M.A[(size_t)k * M.NA + w];
-        ap[k] = M.A[(size_t)(5 + k) * M.NA + w];
-        cq[k] = M.A[(size_t)(10 + k) * M.NA + w];
-    }
-}
-
 // Sweep flux phase for one cell of the sweep (dir 0: cell (c, r) of rows
 // j0-1..j0+TY, columns i0..i0+TX-1; dir 1: cell (c, j) of columns
 // i0-1..i0+TX, rows j0..j0+TY-1). Computes the fluxes of its own interface
@@ -489,15 +441,19 @@ DC_HD void tile_flux(const dclaw_params& P, const Geom& g, const Rec& R, const T
     auto witem = [&](int k) -> int {
         return dir == 0 ? (r - (j0 - 1)) * (TX + 3) + (k - (i0 - 1)) : (k - (j0 - 1)) * (TX + 2) + (c - (i0 - 1));
     };
+    auto hcell = [&](int aa) -> double { return dir == 0 ? M.h(aa, r) : M.h(c, aa); };
     const double half = 0.5 * dtdx;
     const bool last = dir == 0 ? (c == (i0 + TX - 1 < mx ? i0 + TX - 1 : mx)) : (r == (j0 + TY - 1 < my ? j0 + TY - 1 : my));
     const bool in_tile = dir == 0 ? (r >= j0 && r <= j0 + TY - 1 && r <= my) : (c >= i0 && c <= i0 + TX - 1 && c <= mx);
     uint32_t b_own = 0, b_next = 0;
-    // own interface a (between cells a-1 and a) and the next one a+1, as the
-    // limiter phase left them in M.A (their limiter bits are in M.bits)
+    uint32_t* pb_own = log ? &b_own : nullptr;
+    uint32_t* pb_next = log ? &b_next : nullptr;
+    // own interface a (between cells a-1 and a) and the next one a+1
     double am0[5], ap0[5], cq0[5], am1[5], ap1[5], cq1[5];
-    tile_lim_load(M, witem(a), am0, ap0, cq0);
-    tile_lim_load(M, witem(a + 1), am1, ap1, cq1);
+    double h0[4] = {hcell(a - 2), hcell(a - 1), hcell(a), hcell(a + 1)};
+    double h1[4] = {h0[1], h0[2], h0[3], hcell(a + 2)};
+    iface_limited(P, M, dir, witem(a - 1), witem(a), witem(a + 1), h0, dtdx, am0, ap0, cq0, pb_own);
+    iface_limited(P, M, dir, witem(a), witem(a + 1), witem(a + 2), h1, dtdx, am1, ap1, cq1, pb_next);
     const bool ord2 = P.order != 1;
     auto fadd = [&](const double* am, const double* ap, const double* cq, double fm[5], double fp[5]) {
         for (int m = 0; m < 5; ++m) {
@@ -557,9 +513,11 @@ DC_HD void tile_flux(const dclaw_params& P, const Geom& g, const Rec& R, const T
         if (log) {
             // splits the reference logs but the interior update does not use
             double Xm[5], Xp[5];
-            if (a == 1) {   // imp = 1 at interface 1 (this cell's own) uses cell 0
+            if (a == 1) {   // imp = 1 at interface 1 uses cell 0
                 double s0[5];
-                for (int m = 0; m < 5; ++m) s0[m] = fold ? am0[m] + cq0[m] : am0[m];
+                double amx[5], apx[5], cqx[5], hx[4] = {hcell(-1), hcell(0), hcell(1), hcell(2)};
+                iface_limited(P, M, dir, witem(0), witem(1), witem(2), hx, dtdx, amx, apx, cqx, nullptr);
+                for (int m = 0; m < 5; ++m) s0[m] = fold ? amx[m] + cqx[m] : amx[m];
                 int ci = dir == 0 ? 0 : c, cj = dir == 0 ? r : 0;
                 if (split_cell(P, R, g, M, dir, ci, cj, s0, half, Xm, Xp)) b_own |= BR_RPT1;
             }

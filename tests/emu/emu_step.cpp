@@ -129,21 +129,6 @@ static int run_fused(const dclaw_params* P, int mx, int my, double dx, double dy
                         double s = tile_riemann(*P, g, R, M, dir, it, i0, j0, TX, TY, ok);
                         if (ok) cfl = fmax2(cfl, dtd * s);
                     }
-                    {
-                        // the limiter phase: every item computed before any is stored
-                        const int nlim = LimGeom<TX, TY>::count(dir);
-                        std::vector<double> lv((size_t)nlim * 15);
-                        std::vector<uint32_t> lb(nlim, 0u);
-                        std::vector<int> lw(nlim);
-                        for (int li = 0; li < nlim; ++li)
-                            lw[li] = tile_limit<TX, TY>(*P, g, M, dir, li, i0, j0, dtd, &lv[15 * (size_t)li],
-                                                        br ? &lb[li] : nullptr);
-                        for (int li = 0; li < nlim; ++li)
-                            if (lw[li] >= 0) {
-                                tile_lim_store(M, lw[li], &lv[15 * (size_t)li]);
-                                if (br) M.bits[lw[li]] |= lb[li];
-                            }
-                    }
                     const int ncell = dir == 0 ? (TY + 2) * TX : TY * (TX + 2);
                     for (int it = 0; it < ncell; ++it) tile_flux<TX, TY>(*P, g, R, M, dir, it, i0, j0, dtd, br);
                     if (dir == 0) {

@@ -88,48 +88,40 @@ def _loss_weights(q, n_out, seed=5):
 
 
 def _fd(f, eps0=1e-6, down=4, up=8):
-    """Fourth-order central difference (8 (f(e) - f(-e)) - (f(2e) - f(-2e)))
-    / 12e and its uncertainty.
+    """Central difference (f(e) - f(-e)) / 2e and its uncertainty.
 
-    Estimates are taken at e = eps0 * 2^k for k = -down .. up, and the
-    window of three neighbours (e, 2e, 4e) whose estimates agree best is
-    kept: returns (estimate at that window's middle step, spread of its
-    three estimates). Two errors pull the step size in opposite ways. A
-    step that straddles a kink of the forward map (limiter regimes, the dry
-    tolerance and min/max picks put kinks within 1e-6 relative of ordinary
-    states) measures a chord, not the derivative the adjoint gives, so
-    smaller steps help; rounding noise (every perturbed run rounds its
-    elementary functions afresh, step after step) divided by e grows as e
-    shrinks, so larger steps help, and the fourth-order stencil keeps the
-    truncation error of large steps small. The spread is the estimate's
-    uncertainty; the caller checks it against its tolerance rather than
-    widening the tolerance by it."""
+    Estimates are taken at e = eps0 * 2^k for k = -down .. up, and the pair
+    of neighbouring step sizes (e, 2e) whose estimates agree best is kept:
+    returns (estimate at e, |difference of the pair|). Two errors pull the
+    step size in opposite ways. A step that straddles a kink of the forward
+    map (limiter regimes, the dry tolerance and min/max picks put kinks
+    within 1e-6 relative of ordinary states) measures a chord, not the
+    derivative the adjoint gives, so smaller steps help; rounding noise
+    (every perturbed run rounds its elementary functions afresh, step after
+    step) divided by e grows as e shrinks, so larger steps help. Two step
+    sizes that agree bound the estimate's error; the caller checks that
+    bound against its tolerance rather than widening the tolerance by it."""
     cache = {}
 
-    def fv(e):
+    def cd(e):
         if e not in cache:
-            cache[e] = f(e)
+            cache[e] = (f(e) - f(-e)) / (2 * e)
         return cache[e]
 
-    def cd(e):
-        return (8.0 * (fv(e) - fv(-e)) - (fv(2 * e) - fv(-2 * e))) / (12.0 * e)
-
     es = [eps0 * 2.0**k for k in range(-down, up + 1)]
-    vals = [cd(e) for e in es]
     best = None
-    for k in range(len(es) - 2):
-        three = vals[k:k + 3]
-        mid = three[1]
-        spread = max(three) - min(three)
-        rel = spread / max(abs(mid), 1e-300)
+    for k in range(len(es) - 1):
+        lo, hi = cd(es[k]), cd(es[k + 1])
+        spread = abs(hi - lo)
+        rel = spread / max(abs(lo), 1e-300)
         if best is None or rel < best[2]:
-            best = (mid, spread, rel)
+            best = (lo, spread, rel)
     return best[0], best[1]
 
 
 def _close(ad, fd, what, rtol=1e-6):
     """AD against a finite difference to rtol, with the finite difference
-    itself settled to a quarter of rtol (its spread over three step sizes)."""
+    itself settled to a quarter of rtol (two step sizes agreeing to that)."""
     est, spread = fd
     msg = f"{what}: AD {ad:.12e} FD {est:.12e} (FD spread {spread:.2e}, {spread / max(abs(est), 1e-300):.2e} rel)"
     print(msg)
