@@ -369,9 +369,13 @@ class _Rollout(torch.autograd.Function):
             pgrads = [torch.zeros_like(t) if i in want else None for i, t in enumerate(bed_params)]
 
             def after(n):
+                # retain_graph: bed_fn may close over tensors computed from
+                # the parameters outside it (a gate shape amp * ridge), whose
+                # graph every step's bed shares
                 with torch.enable_grad():
                     bn = bed_fn(t_start[n - 1])
-                    gs = torch.autograd.grad(bn, [bed_params[i] for i in want], bbar, allow_unused=True)
+                    gs = torch.autograd.grad(bn, [bed_params[i] for i in want], bbar, allow_unused=True,
+                                             retain_graph=True)
                 for i, gi in zip(want, gs):
                     if gi is not None:
                         pgrads[i].add_(gi)
