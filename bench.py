@@ -41,11 +41,27 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 BYTES_PER_CELL_UPDATE = 88  # read 5 state + 1 bed, write 5 state (FP64)
-# DRAM bytes (read + write) of one fused step measured by ncu on the 2048 x 2048
-# random-field case: k_records 361.7 MB + k_tile 170.4 MB + k_src2_cells 158.9 MB;
-# the case keeps its wet fraction at every size, so the bytes scale with the cell
-# count
-NCU_STEP_BYTES_2048 = 690.9e6
+# One step over tile lists as ncu counts it (one launch of each kernel, after
+# the warm-up steps): DRAM bytes read + written and warp instructions issued
+# (smsp__inst_executed.sum), on the workload the numbers are quoted for
+NCU_STEP = {
+    "cells": 2048 * 2048,
+    "command": "ncu --metrics gpu__time_duration.sum,smsp__inst_executed.sum,dram__bytes_read.sum,"
+               "dram__bytes_write.sum --clock-control none -k regex:k_ python bench.py --size 2048 --steps 3 "
+               "--warmup 3 --e2e-steps 0 --no-cpu-baseline --ensemble-members 0 --grad-steps 0 "
+               "--bgrad-members 0 --full-steps 0",
+    "kernels": {  # name: (DRAM bytes, warp instructions) per launch
+        "k_scan_patch": (285.3e6, 12.72e6),
+        "k_list_patch": (0.081e6, 0.119e6),
+        "k_records_list": (185.4e6, 71.14e6),
+        "k_tile_list": (174.5e6, 424.1e6),
+        "k_src2_list": (56.19e6, 87.88e6),
+    },
+    # k_tile_list, --set full: active lanes per warp instruction, FP64 pipe
+    "k_tile_list_lanes": 21.97,
+    "k_tile_list_fp64_pipe": 0.258,
+}
+SMS, SCHEDULERS_PER_SM = 148, 4
 METRIC = "cell-updates/sec on 1 B200 (plain vs batched); gradient/forward time ratio"
 
 
@@ -708,7 +724,26 @@ def run_ours(args):
         del fs
 
     peak, peak_kind = load_peaks()
-    achieved = BYTES_PER_CELL_UPDATE * cells / (ms / 1000.0 / args.steps) / 1e9
+    step_s = ms / 1000.0 / args.steps
+    achieved = BYTES_PER_CELL_UPDATE * cells / step_s / 1e9
+    scale = cells / NCU_STEP["cells"]
+    traffic = sum(v[0] for v in NCU_STEP["kernels"].values()) * scale
+    # the issue ceiling: every scheduler issuing one warp instruction per
+    # cycle at the SM clock sampled during the timed region
+    inst = sum(v[1] for v in NCU_STEP["kernels"].values()) * scale
+    sm_hz = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    issue_peak = SMS * SCHEDULERS_PER_SM * sm_hz
+    lanes = NCU_STEP["k_tile_list_lanes"]
+    issue = {"bound": "issue", "achieved": inst / step_s / 1e9, "peak": issue_peak / 1e9,
+             "unit": "G warp-instructions/s", "frac": inst / step_s / issue_peak, "inst_per_step": inst,
+             "peak_note": f"{SMS} SMs x {SCHEDULERS_PER_SM} schedulers x 1 warp instruction per cycle at the "
+                          f"sampled SM clock",
+             "lane_frac": inst * lanes / step_s / (32 * issue_peak),
+             "lane_note": f"thread instructions (k_tile_list's {lanes:.2f} active lanes per warp instruction "
+                          f"applied to the step) over 32 lanes per issue slot",
+             "k_tile_list_fp64_pipe": NCU_STEP["k_tile_list_fp64_pipe"],
+             "source": "smsp__inst_executed.sum per kernel from ncu at "
+                       f"{int(NCU_STEP['cells'] ** 0.5)}^2, scaled by cells"}
     out = None
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
@@ -716,10 +751,14 @@ def run_ours(args):
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                "config": workload_config(case, world),
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                            "frac": achieved / peak, "traffic": NCU_STEP_BYTES_2048 * cells / 2048 ** 2,
-                            "traffic_note": "bytes per step from the ncu capture at 2048^2, scaled by cells",
-                            "kernel": "fused step k_records + k_tile + k_src2_cells (88 B/cell-update algorithmic)",
+                            "frac": achieved / peak, "traffic": traffic,
+                            "traffic_note": f"DRAM bytes read + written per step from ncu at "
+                                            f"{int(NCU_STEP['cells'] ** 0.5)}^2, scaled by cells",
+                            "algorithmic_bytes": BYTES_PER_CELL_UPDATE * cells,
+                            "kernel": "the step over tile lists: k_scan_patch + k_list_patch + k_records_list + "
+                                      "k_tile_list + k_src2_list (88 B/cell-update algorithmic)",
                             "peak_source": peak_kind},
+               "issue_roofline": issue,
                "clocks": clocks, "gpu_launches": 5 * args.steps, "status": status}
         if full is not None:
             out["full_run"] = full

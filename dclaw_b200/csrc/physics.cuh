@@ -529,32 +529,54 @@ DC_BIG Waves riemann_solve(const dclaw_params& P, Side L, Side R, uint32_t* br, 
 // full-state step) the species component is split too: bmp6[0], bmp6[1]
 // receive its B-, B+ parts, with r(6, 1) = r(6, 3) = chi = hchi / h
 // (rpt2_dclaw.f:104,208-215,244-258); b is then the bed less the bed change.
-DC_BIG bool rpt2_split(const dclaw_params& P, double h, double hn, double ht, double hm,
-                                          double b, double topo1, double topo3, const double asdq[5],
-                                          double bm[5], double bp[5], double hchi = 0.0,
-                                          double* bmp6 = nullptr) {
-    for (int k = 0; k < 5; ++k) { bm[k] = 0.0; bp[k] = 0.0; }
-    if (bmp6) { bmp6[0] = 0.0; bmp6[1] = 0.0; }
-    if (h <= P.dry_tolerance) return false;
+// The cell part of rpt2_split: the primitives and eigenvalues of the
+// Jacobian of the cell the fluctuation splits in. ok is false where the
+// reference returns zero waves (a dry cell, or eta below both transverse
+// neighbours' beds). One cell part serves every fluctuation split there.
+struct Rpt2Cell {
+    bool ok;
+    double u, m, chi, eta, r5, s1, s2, s3, s31;
+};
+
+DC_HD Rpt2Cell rpt2_cell(const dclaw_params& P, double h, double hn, double ht, double hm, double b, double topo1,
+                         double topo3, double hchi = 0.0, bool with_chi = false) {
+    Rpt2Cell c;
+    c.ok = false;
+    c.u = c.m = c.chi = c.eta = c.r5 = c.s1 = c.s2 = c.s3 = c.s31 = 0.0;
+    if (h <= P.dry_tolerance) return c;
     const double g = P.grav;
-    double u = hn / h;
+    c.u = hn / h;
     double v = ht / h;
-    double m = hm / h;
-    double chi = 0.0;
-    if (bmp6) chi = hchi / h;
-    double eta = h + b;
-    double rho = m * P.rho_s + (1.0 - m) * P.rho_f;
+    c.m = hm / h;
+    if (with_chi) c.chi = hchi / h;
+    c.eta = h + b;
+    double rho = c.m * P.rho_s + (1.0 - c.m) * P.rho_f;
     double gamma;
     if (P.src2method == -1) gamma = P.rho_f / rho;
     else gamma = 0.25 * (P.rho_f + 3.0 * rho) / rho;
-    if (eta < fmin2(topo1, topo3)) return false;
+    if (c.eta < fmin2(topo1, topo3)) return c;
+    c.ok = true;
     double sgh = sqrt(g * h);
-    double s1 = v - sgh, s2 = v, s3 = v + sgh;
+    c.s1 = v - sgh;
+    c.s2 = v;
+    c.s3 = v + sgh;
+    c.s31 = c.s3 - c.s1;
+    c.r5 = gamma * rho * g;
+    return c;
+}
+
+// The fluctuation part of rpt2_split: asdq split into bm/bp with the cell
+// part c (bmp6: the species row, with_chi in rpt2_cell).
+DC_HD bool rpt2_apply(const Rpt2Cell& c, double topo1, double topo3, const double asdq[5], double bm[5],
+                      double bp[5], double* bmp6 = nullptr) {
+    for (int k = 0; k < 5; ++k) { bm[k] = 0.0; bp[k] = 0.0; }
+    if (bmp6) { bmp6[0] = 0.0; bmp6[1] = 0.0; }
+    if (!c.ok) return false;
+    const double u = c.u, m = c.m, chi = c.chi, eta = c.eta, r5 = c.r5, s1 = c.s1, s2 = c.s2, s3 = c.s3;
     double delf1 = asdq[0], delf2 = asdq[1], delf3 = asdq[2];
-    double beta1 = (s3 * delf1 - delf3) / (s3 - s1);
+    double beta1 = (s3 * delf1 - delf3) / c.s31;
     double beta2 = -u * delf1 + delf2;
-    double beta3 = (delf3 - s1 * delf1) / (s3 - s1);
-    double r5 = gamma * rho * g;
+    double beta3 = (delf3 - s1 * delf1) / c.s31;
     // wave 1: r = (1, u, s1, m, r5, chi)
     {
         double sb = 1.0 * s1 * beta1;
@@ -588,6 +610,14 @@ DC_BIG bool rpt2_split(const dclaw_params& P, double h, double hn, double ht, do
         }
     }
     return true;
+}
+
+DC_BIG bool rpt2_split(const dclaw_params& P, double h, double hn, double ht, double hm,
+                                          double b, double topo1, double topo3, const double asdq[5],
+                                          double bm[5], double bp[5], double hchi = 0.0,
+                                          double* bmp6 = nullptr) {
+    const Rpt2Cell c = rpt2_cell(P, h, hn, ht, hm, b, topo1, topo3, hchi, bmp6 != nullptr);
+    return rpt2_apply(c, topo1, topo3, asdq, bm, bp, bmp6);
 }
 
 // ---------------------------------------------------------------------------

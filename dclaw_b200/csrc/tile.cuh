@@ -407,6 +407,34 @@ DC_HD bool split_cell(const dclaw_params& P, const Rec& R, const Geom& g, const 
     return done;
 }
 
+// the two fluctuations a cell splits in one sweep (A-dq of its next
+// interface, A+dq of its own), with the cell's Jacobian computed once:
+// the same bits as two split_cell calls
+DC_HD void split_cell2(const dclaw_params& P, const Rec& R, const Geom& g, const TileMem& M, int dir, int ci,
+                       int cj, const double src1[5], const double src2[5], double half, double U1m[5],
+                       double U1p[5], double U2m[5], double U2p[5], bool& d1, bool& d2) {
+    const bool y = dir != 0;
+    double h, hn, ht, hm;
+    rec_a2(P, R, g, M, ci, cj, dir, h, hn, ht, hm);
+    double topo1, topo3;
+    if (!y) { topo1 = M.bed(ci, cj - 1); topo3 = M.bed(ci, cj + 1); }
+    else { topo1 = M.bed(ci - 1, cj); topo3 = M.bed(ci + 1, cj); }
+    const Rpt2Cell cell = rpt2_cell(P, h, hn, ht, hm, M.bed(ci, cj), topo1, topo3);
+    auto one = [&](const double* src, double* Um, double* Up) -> bool {
+        double asdq[5] = {src[0], y ? src[2] : src[1], y ? src[1] : src[2], src[3], src[4]}, bm[5], bp[5];
+        bool done = rpt2_apply(cell, topo1, topo3, asdq, bm, bp);
+        double bmq[5] = {bm[0], y ? bm[2] : bm[1], y ? bm[1] : bm[2], bm[3], bm[4]};
+        double bpq[5] = {bp[0], y ? bp[2] : bp[1], y ? bp[1] : bp[2], bp[3], bp[4]};
+        for (int m = 0; m < 5; ++m) {
+            Um[m] = half * bmq[m];
+            Up[m] = half * bpq[m];
+        }
+        return done;
+    };
+    d1 = one(src1, U1m, U1p);
+    d2 = one(src2, U2m, U2p);
+}
+
 DC_HD void bits_or(uint32_t* log, size_t off, uint32_t b) {
     if (!log || !b) return;
 #if defined(__CUDA_ARCH__)
@@ -420,6 +448,22 @@ DC_HD size_t xlog_off(const Geom& g, int r, int k) { return (size_t)r * (g.mx + 
 DC_HD size_t ylog_off(const Geom& g, int c, int k) {
     return (size_t)(g.my + 2) * (g.mx + 1) + (size_t)c * (g.my + 1) + (size_t)(k - 1);
 }
+
+// Limited waves and fluctuations of x-interface a (between cells a-1 and a)
+// on row r, packed as v = (amdq[5], apdq[5], cqxx[5]); the limiter's bits
+// go to *bits. a and its neighbours a-1, a+1 lie in the x item grid.
+template <int TX, int TY>
+DC_HD void tile_x_iface(const dclaw_params& P, const TileMem& M, int r, int a, int i0, int j0, double dtdx,
+                        double v[15], uint32_t* bits) {
+    auto witem = [&](int k) -> int { return (r - (j0 - 1)) * (TX + 3) + (k - (i0 - 1)); };
+    const double h0[4] = {M.h(a - 2, r), M.h(a - 1, r), M.h(a, r), M.h(a + 1, r)};
+    iface_limited(P, M, 0, witem(a - 1), witem(a), witem(a + 1), h0, dtdx, v, v + 5, v + 10, bits);
+}
+
+template <int TX, int TY>
+DC_HD void tile_flux_cell(const dclaw_params& P, const Geom& g, const Rec& R, const TileMem& M, int dir, int c,
+                          int r, int i0, int j0, double dtdx, const double* v0, const double* v1, uint32_t lb0,
+                          uint32_t lb1, uint32_t* log);
 
 // Sweep flux phase for one cell of the sweep (dir 0: cell (c, r) of rows
 // j0-1..j0+TY, columns i0..i0+TX-1; dir 1: cell (c, j) of columns
@@ -435,25 +479,40 @@ DC_HD void tile_flux(const dclaw_params& P, const Geom& g, const Rec& R, const T
     const int mx = g.mx, my = g.my;
     if (c < (dir == 0 ? 1 : 0) || c > (dir == 0 ? mx : mx + 1)) return;
     if (r < (dir == 0 ? 0 : 1) || r > (dir == 0 ? my + 1 : my)) return;
-    // position along the sweep and the item-grid index of an interface
+    const int a = dir == 0 ? c : r;                 // this cell along the sweep
+    auto witem = [&](int k) -> int {
+        return dir == 0 ? (r - (j0 - 1)) * (TX + 3) + (k - (i0 - 1)) : (k - (j0 - 1)) * (TX + 2) + (c - (i0 - 1));
+    };
+    auto hcell = [&](int aa) -> double { return dir == 0 ? M.h(aa, r) : M.h(c, aa); };
+    // own interface a (between cells a-1 and a) and the next one a+1
+    double v0[15], v1[15];
+    uint32_t b0 = 0, b1 = 0;
+    const double h0[4] = {hcell(a - 2), hcell(a - 1), hcell(a), hcell(a + 1)};
+    const double h1[4] = {h0[1], h0[2], h0[3], hcell(a + 2)};
+    iface_limited(P, M, dir, witem(a - 1), witem(a), witem(a + 1), h0, dtdx, v0, v0 + 5, v0 + 10,
+                  log ? &b0 : nullptr);
+    iface_limited(P, M, dir, witem(a), witem(a + 1), witem(a + 2), h1, dtdx, v1, v1 + 5, v1 + 10,
+                  log ? &b1 : nullptr);
+    tile_flux_cell<TX, TY>(P, g, R, M, dir, c, r, i0, j0, dtdx, v0, v1, b0, b1, log);
+}
+
+// The rest of tile_flux for cell (c, r), given the limited fluctuations of
+// its own interface (v0, limiter bits lb0) and of the next one (v1, lb1).
+template <int TX, int TY>
+DC_HD void tile_flux_cell(const dclaw_params& P, const Geom& g, const Rec& R, const TileMem& M, int dir, int c,
+                          int r, int i0, int j0, double dtdx, const double* v0, const double* v1, uint32_t lb0,
+                          uint32_t lb1, uint32_t* log) {
+    const int mx = g.mx, my = g.my;
     const int a = dir == 0 ? c : r;                 // this cell along the sweep
     const int nlen = dir == 0 ? mx : my;
     auto witem = [&](int k) -> int {
         return dir == 0 ? (r - (j0 - 1)) * (TX + 3) + (k - (i0 - 1)) : (k - (j0 - 1)) * (TX + 2) + (c - (i0 - 1));
     };
-    auto hcell = [&](int aa) -> double { return dir == 0 ? M.h(aa, r) : M.h(c, aa); };
     const double half = 0.5 * dtdx;
     const bool last = dir == 0 ? (c == (i0 + TX - 1 < mx ? i0 + TX - 1 : mx)) : (r == (j0 + TY - 1 < my ? j0 + TY - 1 : my));
     const bool in_tile = dir == 0 ? (r >= j0 && r <= j0 + TY - 1 && r <= my) : (c >= i0 && c <= i0 + TX - 1 && c <= mx);
-    uint32_t b_own = 0, b_next = 0;
-    uint32_t* pb_own = log ? &b_own : nullptr;
-    uint32_t* pb_next = log ? &b_next : nullptr;
-    // own interface a (between cells a-1 and a) and the next one a+1
-    double am0[5], ap0[5], cq0[5], am1[5], ap1[5], cq1[5];
-    double h0[4] = {hcell(a - 2), hcell(a - 1), hcell(a), hcell(a + 1)};
-    double h1[4] = {h0[1], h0[2], h0[3], hcell(a + 2)};
-    iface_limited(P, M, dir, witem(a - 1), witem(a), witem(a + 1), h0, dtdx, am0, ap0, cq0, pb_own);
-    iface_limited(P, M, dir, witem(a), witem(a + 1), witem(a + 2), h1, dtdx, am1, ap1, cq1, pb_next);
+    uint32_t b_own = lb0, b_next = lb1;
+    const double *am0 = v0, *ap0 = v0 + 5, *cq0 = v0 + 10, *am1 = v1, *ap1 = v1 + 5, *cq1 = v1 + 10;
     const bool ord2 = P.order != 1;
     auto fadd = [&](const double* am, const double* ap, const double* cq, double fm[5], double fp[5]) {
         for (int m = 0; m < 5; ++m) {
@@ -506,18 +565,16 @@ DC_HD void tile_flux(const dclaw_params& P, const Geom& g, const Rec& R, const T
             src1[m] = fold ? am1[m] + cq1[m] : am1[m];   // A-dq at the next interface (imp = 1)
             src2[m] = fold ? ap0[m] - cq0[m] : ap0[m];   // A+dq at the own interface (imp = 2)
         }
-        bool d1 = split_cell(P, R, g, M, dir, c, r, src1, half, U1m, U1p);
-        bool d2 = split_cell(P, R, g, M, dir, c, r, src2, half, U2m, U2p);
+        bool d1, d2;
+        split_cell2(P, R, g, M, dir, c, r, src1, src2, half, U1m, U1p, U2m, U2p, d1, d2);
         if (d1) b_next |= BR_RPT1;
         if (d2) b_own |= BR_RPT2;
         if (log) {
             // splits the reference logs but the interior update does not use
             double Xm[5], Xp[5];
-            if (a == 1) {   // imp = 1 at interface 1 uses cell 0
+            if (a == 1) {   // imp = 1 at interface 1 (this cell's own) uses cell 0
                 double s0[5];
-                double amx[5], apx[5], cqx[5], hx[4] = {hcell(-1), hcell(0), hcell(1), hcell(2)};
-                iface_limited(P, M, dir, witem(0), witem(1), witem(2), hx, dtdx, amx, apx, cqx, nullptr);
-                for (int m = 0; m < 5; ++m) s0[m] = fold ? amx[m] + cqx[m] : amx[m];
+                for (int m = 0; m < 5; ++m) s0[m] = fold ? am0[m] + cq0[m] : am0[m];
                 int ci = dir == 0 ? 0 : c, cj = dir == 0 ? r : 0;
                 if (split_cell(P, R, g, M, dir, ci, cj, s0, half, Xm, Xp)) b_own |= BR_RPT1;
             }

@@ -17,7 +17,7 @@ numbers combine the same way:
   and every rank applies the tick rule (`dclaw_clock_tick`).
 
 One step reads at most 4 rows away (a record reads its neighbours' depths,
-a tile reads records 3 rows beyond it), so a halo of one tile row (14
+a tile reads records 3 rows beyond it), so a halo of one tile row (13
 rows) is exact: every rank's rows and dt equal the whole-patch step's, bit
 for bit. A slab's halo rows go stale during its step and are refreshed by
 the next exchange.

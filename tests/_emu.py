@@ -56,7 +56,7 @@ class Emu:
                                    dth.ctypes.data_as(_dp), cfh.ctypes.data_as(_dp), br.ctypes.data_as(_up))
         return dict(q=q, dt=dth[:nsteps], cfl=cfh[:nsteps], status=st, br=br)
 
-    def run(self, p, q, b, dx, dy, nsteps, dt_initial, t_final=0.0, fixed_dt=False, fused=False, tile=(16, 14),
+    def run(self, p, q, b, dx, dy, nsteps, dt_initial, t_final=0.0, fixed_dt=False, fused=False, tile=(14, 13),
             src2_in_tile=False):
         q = np.ascontiguousarray(q, dtype=np.float64).copy()
         b = np.ascontiguousarray(b, dtype=np.float64)

@@ -129,8 +129,25 @@ static int run_fused(const dclaw_params* P, int mx, int my, double dx, double dy
                         double s = tile_riemann(*P, g, R, M, dir, it, i0, j0, TX, TY, ok);
                         if (ok) cfl = fmax2(cfl, dtd * s);
                     }
-                    const int ncell = dir == 0 ? (TY + 2) * TX : TY * (TX + 2);
-                    for (int it = 0; it < ncell; ++it) tile_flux<TX, TY>(*P, g, R, M, dir, it, i0, j0, dtd, br);
+                    if (dir == 0 && TX + 1 <= 16) {
+                        // the kernels' x-sweep for tiles up to 15 wide: each
+                        // interface limited once, a cell given its own and
+                        // its next interface's results
+                        for (int rr = 0; rr < TY + 2; ++rr) {
+                            const int r = j0 - 1 + rr;
+                            if (r < 0 || r > my + 1) continue;
+                            std::vector<double> v(16 * 15, 0.0);
+                            std::vector<uint32_t> lb(16, 0u);
+                            for (int k = 0; k <= TX && i0 + k <= mx + 1; ++k)
+                                tile_x_iface<TX, TY>(*P, M, r, i0 + k, i0, j0, dtd, &v[15 * k], br ? &lb[k] : nullptr);
+                            for (int k = 0; k < TX && i0 + k <= mx; ++k)
+                                tile_flux_cell<TX, TY>(*P, g, R, M, 0, i0 + k, r, i0, j0, dtd, &v[15 * k],
+                                                       &v[15 * (k + 1)], lb[k], lb[k + 1], br);
+                        }
+                    } else {
+                        const int ncell = dir == 0 ? (TY + 2) * TX : TY * (TX + 2);
+                        for (int it = 0; it < ncell; ++it) tile_flux<TX, TY>(*P, g, R, M, dir, it, i0, j0, dtd, br);
+                    }
                     if (dir == 0) {
                         std::vector<double> T((size_t)(TY + 1) * TX * 5);
                         std::vector<char> v((size_t)(TY + 1) * TX);
@@ -171,6 +188,7 @@ extern "C" int emu_run_fused(const dclaw_params* P, int mx, int my, double dx, d
     DCLAW_EMU_TILE(16, 16)
     DCLAW_EMU_TILE(16, 14)
     DCLAW_EMU_TILE(13, 14)
+    DCLAW_EMU_TILE(14, 13)
     DCLAW_EMU_TILE(8, 8)
     return -1;
 }

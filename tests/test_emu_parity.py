@@ -62,7 +62,7 @@ def test_random_field_small(oracle, emu, fused):
 
 
 @pytest.mark.parametrize("src2_in_tile", [False, True])
-@pytest.mark.parametrize("tile", [(13, 14), (16, 16), (16, 14), (8, 8)])
+@pytest.mark.parametrize("tile", [(14, 13), (13, 14), (16, 16), (16, 14), (8, 8)])
 def test_fused_tile_shapes_and_partial_tiles(oracle, emu, tile, src2_in_tile):
     """Tile shapes of the fused step on a patch whose sizes are not multiples
     of the tile."""

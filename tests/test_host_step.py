@@ -18,9 +18,6 @@ from dclaw_b200 import _lib
 from dclaw_b200 import workloads as W
 from dclaw_b200.params import DClawParams
 
-TILE_Y = 14      # tile rows of the fused step (kernels.cu TILE_Y)
-
-
 def _plan(lib, mx, my, nbands):
     first = (ctypes.c_int32 * 66)()
     nb = lib.dclaw_step_host_bands(mx, my, nbands, first, 66)
@@ -29,8 +26,9 @@ def _plan(lib, mx, my, nbands):
 
 def test_band_plan_covers_every_tile_row():
     lib = _lib.load()
+    tile_y = lib.dclaw_rows_granule()      # cells per tile row of the fused step
     for mx, my in [(2, 2), (37, 53), (200, 200), (513, 1000), (4096, 4096), (100, 20000)]:
-        nty = -(-my // TILE_Y)
+        nty = -(-my // tile_y)
         for nbands in [0, 1, 2, 3, 7, 64, 1000]:
             nb, first = _plan(lib, mx, my, nbands)
             assert 1 <= nb <= min(64, nty)
@@ -75,9 +73,9 @@ def _case(n, mx, my, seed):
     (200, 200, 0, True, True),
     (200, 200, 1, False, True),
     (200, 200, 3, True, True),
-    (200, 200, 15, False, True),        # one band per tile row
+    (200, 200, 16, False, True),        # one band per tile row (13-row tiles)
     (200, 200, 500, True, False),       # capped at the tile rows; pageable memory
-    (173, 131, 4, False, True),         # ragged: last tile row partial
+    (173, 131, 4, False, True),         # ragged: last tile row partial (131 = 10 x 13 + 1)
     (96, 190, 5, True, True),
 ])
 def test_host_step_matches_device_step(cuda_device, mx, my, nbands, inplace, pinned):

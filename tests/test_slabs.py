@@ -19,7 +19,7 @@ import torch.multiprocessing as mp
 
 from dclaw_b200.slabs import Slab, _halo_counts, exchange_halos, slab_plan
 
-G = 14
+G = 14      # a granule for the plan tests (slab_plan takes any)
 
 
 def test_slab_plan_covers_rows_with_aligned_halos():
@@ -143,7 +143,8 @@ def test_step_rows_argument_checks():
     from dclaw_b200.params import DClawParams
 
     lib = _lib.load()
-    assert lib.dclaw_rows_granule() == G
+    g = lib.dclaw_rows_granule()      # cells per tile row of the fused step
+    assert 4 <= g <= 50
     mx, my = 50, 100
     need = lib.dclaw_workspace_bytes(mx, my)
     cp = DClawParams().to_c()
@@ -153,13 +154,13 @@ def test_step_rows_argument_checks():
         return lib.dclaw_step_rows(one, q_out, one, mx, my, 1.0, 1.0, ctypes.byref(cp), one, one, work, first,
                                    count, None)
 
-    assert call(2, 14) == 1           # does not start a tile row
-    assert call(1, 13) == 1           # does not end on one (and not at the last row)
-    assert call(0, 14) == 1
-    assert call(99, 14) == 1          # beyond the patch
+    assert call(2, g) == 1            # does not start a tile row
+    assert call(1, g - 1) == 1        # does not end on one (and not at the last row)
+    assert call(0, g) == 1
+    assert call(99, g) == 1           # beyond the patch
     assert call(1, 0) == 1
-    assert call(15, 28, q_out=one) == 1   # in place
-    assert call(15, 28, work=1024) == 5
+    assert call(g + 1, 2 * g, q_out=one) == 1   # in place
+    assert call(g + 1, 2 * g, work=1024) == 5
     assert lib.dclaw_clock_tick(None, ctypes.byref(cp), None) == 1
 
 
