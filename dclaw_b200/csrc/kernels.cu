@@ -477,7 +477,8 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
     const int tid = threadIdx.x;
     M.hi0 = i0 - 3;
     M.hj0 = j0 - 3;
-    M.hw = TX + 6;
+    M.hw = TG::HW;
+    M.hv = TX + 6;
     const double dtdx = dt / g.dx, dtdy = dt / g.dy;
     if (!active) {
         // flagged inactive: with src2 in this kernel its cells' zeros are
@@ -548,27 +549,34 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
                 if (ok) cfl = fmax2(cfl, dtd * s);
             }
             __syncthreads();
+            // A half-warp per slice (x: a row, y: a column), lane k on
+            // interface k of it. Each interface is limited once; a cell
+            // takes its own interface's fluctuations and, from the next
+            // lane, those of the next interface (a cell limited both
+            // before). Every thread reaches the shuffles.
             constexpr bool XPAIR = TX + 1 <= 16 && (TY + 2) * 16 <= NT && NT % 32 == 0;
-            if (XPAIR && dir == 0) {
-                // x-sweep: a half-warp per row, lane k on interface i0+k
-                // (k <= TX). Each interface is limited once; a cell takes
-                // its own interface's fluctuations and, from the next
-                // lane, those of the next interface (a cell limited both
-                // before). Every thread reaches the shuffles.
-                const int rr = tid >> 4, k = tid & 15;
-                const int r = j0 - 1 + rr, a = i0 + k;
-                const bool row_ok = rr < TY + 2 && r >= 0 && r <= g.my + 1;
+            constexpr bool YPAIR = TY + 1 <= 16 && (TX + 2) * 16 <= NT && NT % 32 == 0;
+            if ((XPAIR && dir == 0) || (YPAIR && dir == 1)) {
+                const int sl = tid >> 4, k = tid & 15;
+                const int nsl = dir == 0 ? TY + 2 : TX + 2, span = dir == 0 ? TX : TY;
+                const int s = (dir == 0 ? j0 : i0) - 1 + sl, a = (dir == 0 ? i0 : j0) + k;
+                const int smax = dir == 0 ? g.my + 1 : g.mx + 1, amax = dir == 0 ? g.mx : g.my;
+                const bool sl_ok = sl < nsl && s >= 0 && s <= smax;
                 double v[15];
                 uint32_t lb = 0;
-                if (row_ok && k <= TX && a <= g.mx + 1)
-                    tile_x_iface<TX, TY>(P, M, r, a, i0, j0, dtd, v, brlog ? &lb : nullptr);
-                else
+                if (sl_ok && k <= span && a <= amax + 1) {
+                    if (dir == 0) tile_x_iface<TX, TY>(P, M, s, a, i0, j0, dtd, v, brlog ? &lb : nullptr);
+                    else tile_y_iface<TX, TY>(P, M, s, a, i0, j0, dtd, v, brlog ? &lb : nullptr);
+                } else {
                     for (int m = 0; m < 15; ++m) v[m] = 0.0;
+                }
                 double vn[15];
                 for (int m = 0; m < 15; ++m) vn[m] = __shfl_down_sync(0xffffffffu, v[m], 1);
                 const uint32_t lbn = __shfl_down_sync(0xffffffffu, lb, 1);
-                if (row_ok && k < TX && a <= g.mx)
-                    tile_flux_cell<TX, TY>(P, g, R, M, 0, a, r, i0, j0, dtd, v, vn, lb, lbn, brlog);
+                if (sl_ok && k < span && a <= amax) {
+                    if (dir == 0) tile_flux_cell<TX, TY>(P, g, R, M, 0, a, s, i0, j0, dtd, v, vn, lb, lbn, brlog);
+                    else tile_flux_cell<TX, TY>(P, g, R, M, 1, s, a, i0, j0, dtd, v, vn, lb, lbn, brlog);
+                }
             } else {
                 const int ncell = dir == 0 ? (TY + 2) * TX : TY * (TX + 2);
                 for (int it = tid; it < ncell; it += NT) tile_flux<TX, TY>(P, g, R, M, dir, it, i0, j0, dtd, brlog);

@@ -186,13 +186,21 @@ DC_HD bool cell_record(const dclaw_params& P, const Geom& g, const double* __res
 // ---------------------------------------------------------------------------
 template <int TX, int TY>
 struct TileGeom {
-    static constexpr int NA = (TY + 2) * (TX + 3) > (TX + 2) * (TY + 3) ? (TY + 2) * (TX + 3) : (TX + 2) * (TY + 3);
     static constexpr int NXW = (TY + 2) * (TX + 3);   // x solves: rows j0-1..j0+TY, ifaces i0-1..i0+TX+1
     static constexpr int NYW = (TX + 2) * (TY + 3);   // y solves: cols i0-1..i0+TX, ifaces j0-1..j0+TY+1
+    // The y solves' waves are stored column by column (y_slot), with an odd
+    // pitch: the solves write them along rows and the flux phase reads them
+    // down columns, both without shared-memory bank conflicts.
+    static constexpr int YP = (TY + 3) | 1;
+    static constexpr int NYS = (TX + 2) * YP;
+    static constexpr int NA = NXW > NYS ? NXW : NYS;  // wave slots of either sweep
     static constexpr int NB = TY * (TX + 1);          // x-fluxes of tile rows, ifaces i0..i0+TX
     static constexpr int NC = (TY + 2) * TX;          // G1x/G2x rows j0-1..j0+TY (then T/gm/gp rows j0..j0+TY)
-    static constexpr int ND = (TX + 2) * TY;          // G1y/G2y cols i0-1..i0+TX, rows j0..j0+TY-1
-    static constexpr int NHB = (TX + 6) * (TY + 6);    // h and bed of cells within 3 of the tile
+    static constexpr int ND = (TX + 2) * TY;          // G1y/G2y cols i0-1..i0+TX, rows j0..j0+TY-1 (by column)
+    // h and bed of cells within 3 of the tile, rows of an odd pitch (one
+    // unused column when TX + 6 is even): read along rows and down columns
+    static constexpr int HW = (TX + 6) | 1;
+    static constexpr int NHB = HW * (TY + 6);
     static constexpr size_t SMEM_DOUBLES = (size_t)NW * NA + 10 * NB + 10 * NC + 10 * ND + 2 * NHB;
     // + branch bits of the sweep's items, the list of items that need a
     // solve, and its length
@@ -203,14 +211,15 @@ struct TileMem {
     double* A;   // NW planes of NA
     double* B;   // [NB][10]
     double* C;   // [NC][10]
-    double* D;   // [ND][10]
-    double* H;   // record h of cells (i0-3..i0+TX+2) x (j0-3..j0+TY+2)
+    double* D;   // [ND][10], column by column
+    double* H;   // record h of cells (i0-3..i0+TX+2) x (j0-3..j0+TY+2), row pitch hw
     double* Bd;  // bed of the same cells
     uint32_t* bits;  // NA Riemann branch bits of the current sweep
     int* list;       // NA: items of the current sweep that need a solve
     int* nlist;      // length of the list
     int NA;
-    int hi0, hj0, hw;  // origin and width of the H/Bd block
+    int hi0, hj0, hw;  // origin and row pitch of the H/Bd block
+    int hv;            // staged cells per row (TX + 6)
     DC_HD double h(int i, int j) const { return H[(j - hj0) * hw + (i - hi0)]; }
     DC_HD double bed(int i, int j) const { return Bd[(j - hj0) * hw + (i - hi0)]; }
 };
@@ -219,6 +228,7 @@ struct TileMem {
 // returns whether the cell is wet. Cells outside the padded patch are never
 // read and are left unset.
 DC_HD bool tile_stage_hb(const Geom& g, const Rec& R, const double* b_in, const TileMem& M, int it) {
+    if (it % M.hw >= M.hv) return false;  // the pitch's unused column
     int i = M.hi0 + it % M.hw, j = M.hj0 + it / M.hw;
     if (i < -1 || i > g.mx + 2 || j < -1 || j > g.my + 2) return false;
     double h = R.get(R_H, pidx(g, i, j));
@@ -226,6 +236,11 @@ DC_HD bool tile_stage_hb(const Geom& g, const Rec& R, const double* b_in, const 
     M.Bd[it] = bed_at(g, b_in, i, j);
     return h > 0.0;
 }
+
+// Slot of y-interface k (between rows k-1 and k) of column c in the wave
+// planes: column-major with the odd pitch TileGeom::YP. The x-sweep's slot
+// of an item is the item.
+DC_HD int y_slot(int TY, int i0, int j0, int c, int k) { return (c - (i0 - 1)) * ((TY + 3) | 1) + (k - (j0 - 1)); }
 
 // Solver side of a record cell after one (A1) or two (A2) qfix passes
 DC_HD Side rec_side(const dclaw_params& P, const Rec& R, const Geom& g, const TileMem& M, int i, int j, int dir,
@@ -326,8 +341,9 @@ DC_HD double tile_riemann(const dclaw_params& P, const Geom& g, const Rec& R, co
     }
     const double vals[NW] = {w.s1, w.s2, w.s5, w.w1h, w.w1n, w.w1t, w.w1m, w.w1p,
                              w.w2h, w.w2n, w.w5h, w.w5n, w.w5t, w.w5m, w.w5p};
-    for (int f = 0; f < NW; ++f) M.A[(size_t)f * M.NA + item] = vals[f];
-    M.bits[item] = bits;
+    const int slot = dir == 0 ? item : y_slot(TY, i0, j0, sl, k);
+    for (int f = 0; f < NW; ++f) M.A[(size_t)f * M.NA + slot] = vals[f];
+    M.bits[slot] = bits;
     return fmax2(fmax2(fabs(w.s1), fabs(w.s2)), fabs(w.s5));
 }
 
@@ -460,6 +476,15 @@ DC_HD void tile_x_iface(const dclaw_params& P, const TileMem& M, int r, int a, i
     iface_limited(P, M, 0, witem(a - 1), witem(a), witem(a + 1), h0, dtdx, v, v + 5, v + 10, bits);
 }
 
+// The same for y-interface a (between rows a-1 and a) of column c.
+template <int TX, int TY>
+DC_HD void tile_y_iface(const dclaw_params& P, const TileMem& M, int c, int a, int i0, int j0, double dtdy,
+                        double v[15], uint32_t* bits) {
+    auto witem = [&](int k) -> int { return y_slot(TY, i0, j0, c, k); };
+    const double h0[4] = {M.h(c, a - 2), M.h(c, a - 1), M.h(c, a), M.h(c, a + 1)};
+    iface_limited(P, M, 1, witem(a - 1), witem(a), witem(a + 1), h0, dtdy, v, v + 5, v + 10, bits);
+}
+
 template <int TX, int TY>
 DC_HD void tile_flux_cell(const dclaw_params& P, const Geom& g, const Rec& R, const TileMem& M, int dir, int c,
                           int r, int i0, int j0, double dtdx, const double* v0, const double* v1, uint32_t lb0,
@@ -481,7 +506,7 @@ DC_HD void tile_flux(const dclaw_params& P, const Geom& g, const Rec& R, const T
     if (r < (dir == 0 ? 0 : 1) || r > (dir == 0 ? my + 1 : my)) return;
     const int a = dir == 0 ? c : r;                 // this cell along the sweep
     auto witem = [&](int k) -> int {
-        return dir == 0 ? (r - (j0 - 1)) * (TX + 3) + (k - (i0 - 1)) : (k - (j0 - 1)) * (TX + 2) + (c - (i0 - 1));
+        return dir == 0 ? (r - (j0 - 1)) * (TX + 3) + (k - (i0 - 1)) : y_slot(TY, i0, j0, c, k);
     };
     auto hcell = [&](int aa) -> double { return dir == 0 ? M.h(aa, r) : M.h(c, aa); };
     // own interface a (between cells a-1 and a) and the next one a+1
@@ -506,7 +531,7 @@ DC_HD void tile_flux_cell(const dclaw_params& P, const Geom& g, const Rec& R, co
     const int a = dir == 0 ? c : r;                 // this cell along the sweep
     const int nlen = dir == 0 ? mx : my;
     auto witem = [&](int k) -> int {
-        return dir == 0 ? (r - (j0 - 1)) * (TX + 3) + (k - (i0 - 1)) : (k - (j0 - 1)) * (TX + 2) + (c - (i0 - 1));
+        return dir == 0 ? (r - (j0 - 1)) * (TX + 3) + (k - (i0 - 1)) : y_slot(TY, i0, j0, c, k);
     };
     const double half = 0.5 * dtdx;
     const bool last = dir == 0 ? (c == (i0 + TX - 1 < mx ? i0 + TX - 1 : mx)) : (r == (j0 + TY - 1 < my ? j0 + TY - 1 : my));
@@ -587,7 +612,7 @@ DC_HD void tile_flux_cell(const dclaw_params& P, const Geom& g, const Rec& R, co
         }
     }
     double* G = dir == 0 ? M.C + (size_t)((r - (j0 - 1)) * TX + (c - i0)) * 10
-                         : M.D + (size_t)((r - j0) * (TX + 2) + (c - (i0 - 1))) * 10;
+                         : M.D + (size_t)((c - (i0 - 1)) * TY + (r - j0)) * 10;
     for (int m = 0; m < 5; ++m) {
         G[m] = (0.0 - U1m[m]) - U2m[m];
         G[5 + m] = (0.0 - U1p[m]) - U2p[m];
@@ -637,9 +662,9 @@ DC_HD bool tile_final(const dclaw_params& P, const Geom& g, const Rec& R, const 
     }
     const double* Fx0 = M.B + (size_t)((j - j0) * (TX + 1) + (i - i0)) * 10;       // iface i
     const double* Fx1 = Fx0 + 10;                                                   // iface i+1
-    const double* Gy_im = M.D + (size_t)((j - j0) * (TX + 2) + (i - 1 - (i0 - 1))) * 10;  // column i-1
-    const double* Gy_i = Gy_im + 10;
-    const double* Gy_ip = Gy_im + 20;
+    const double* Gy_im = M.D + (size_t)((i - 1 - (i0 - 1)) * TY + (j - j0)) * 10;  // column i-1
+    const double* Gy_i = Gy_im + (size_t)10 * TY;
+    const double* Gy_ip = Gy_im + (size_t)20 * TY;
     const double* C0 = M.C + (size_t)((j - j0) * TX + (i - i0)) * 10;       // y-iface j
     const double* C1 = M.C + (size_t)((j + 1 - j0) * TX + (i - i0)) * 10;   // y-iface j+1
     double qn[5];

@@ -101,7 +101,8 @@ static int run_fused(const dclaw_params* P, int mx, int my, double dx, double dy
     M.Bd = M.H + TG::NHB;
     M.bits = bits.data();
     M.NA = TG::NA;
-    M.hw = TX + 6;
+    M.hw = TG::HW;
+    M.hv = TX + 6;
     std::vector<double> qa(q, q + 5 * (size_t)mx * my), qb(5 * (size_t)mx * my), qs(5 * (size_t)mx * my);
     double t = 0.0, dt = t_final > 0.0 ? fmax2(fmin2(dt_initial, t_final), 0.0) : dt_initial;
     int status = 0;
@@ -129,20 +130,30 @@ static int run_fused(const dclaw_params* P, int mx, int my, double dx, double dy
                         double s = tile_riemann(*P, g, R, M, dir, it, i0, j0, TX, TY, ok);
                         if (ok) cfl = fmax2(cfl, dtd * s);
                     }
-                    if (dir == 0 && TX + 1 <= 16) {
-                        // the kernels' x-sweep for tiles up to 15 wide: each
-                        // interface limited once, a cell given its own and
-                        // its next interface's results
-                        for (int rr = 0; rr < TY + 2; ++rr) {
-                            const int r = j0 - 1 + rr;
-                            if (r < 0 || r > my + 1) continue;
+                    // the kernels' flux phase: for slices up to 15 cells
+                    // (x: TX + 1 <= 16, y: TY + 1 <= 16, and a half-warp per
+                    // slice within 256 threads) each interface is limited
+                    // once and a cell is given its own and its next
+                    // interface's results
+                    const bool pair = dir == 0 ? (TX + 1 <= 16 && (TY + 2) * 16 <= 256)
+                                               : (TY + 1 <= 16 && (TX + 2) * 16 <= 256);
+                    if (pair) {
+                        const int nsl = dir == 0 ? TY + 2 : TX + 2, span = dir == 0 ? TX : TY;
+                        const int smax = dir == 0 ? my + 1 : mx + 1, amax = dir == 0 ? mx : my;
+                        for (int sl = 0; sl < nsl; ++sl) {
+                            const int s = (dir == 0 ? j0 : i0) - 1 + sl, a0 = dir == 0 ? i0 : j0;
+                            if (s < 0 || s > smax) continue;
                             std::vector<double> v(16 * 15, 0.0);
                             std::vector<uint32_t> lb(16, 0u);
-                            for (int k = 0; k <= TX && i0 + k <= mx + 1; ++k)
-                                tile_x_iface<TX, TY>(*P, M, r, i0 + k, i0, j0, dtd, &v[15 * k], br ? &lb[k] : nullptr);
-                            for (int k = 0; k < TX && i0 + k <= mx; ++k)
-                                tile_flux_cell<TX, TY>(*P, g, R, M, 0, i0 + k, r, i0, j0, dtd, &v[15 * k],
+                            for (int k = 0; k <= span && a0 + k <= amax + 1; ++k) {
+                                if (dir == 0) tile_x_iface<TX, TY>(*P, M, s, a0 + k, i0, j0, dtd, &v[15 * k], br ? &lb[k] : nullptr);
+                                else tile_y_iface<TX, TY>(*P, M, s, a0 + k, i0, j0, dtd, &v[15 * k], br ? &lb[k] : nullptr);
+                            }
+                            for (int k = 0; k < span && a0 + k <= amax; ++k) {
+                                const int c = dir == 0 ? a0 + k : s, r = dir == 0 ? s : a0 + k;
+                                tile_flux_cell<TX, TY>(*P, g, R, M, dir, c, r, i0, j0, dtd, &v[15 * k],
                                                        &v[15 * (k + 1)], lb[k], lb[k + 1], br);
+                            }
                         }
                     } else {
                         const int ncell = dir == 0 ? (TY + 2) * TX : TY * (TX + 2);
