@@ -45,21 +45,22 @@ BYTES_PER_CELL_UPDATE = 88  # read 5 state + 1 bed, write 5 state (FP64)
 # the warm-up steps): DRAM bytes read + written and warp instructions issued
 # (smsp__inst_executed.sum), on the workload the numbers are quoted for
 NCU_STEP = {
-    "cells": 2048 * 2048,
+    "cells": 4096 * 4096,
     "command": "ncu --metrics gpu__time_duration.sum,smsp__inst_executed.sum,dram__bytes_read.sum,"
-               "dram__bytes_write.sum --clock-control none -k regex:k_ python bench.py --size 2048 --steps 3 "
+               "dram__bytes_write.sum --clock-control none -k regex:k_ python bench.py --size 4096 --steps 3 "
                "--warmup 3 --e2e-steps 0 --no-cpu-baseline --ensemble-members 0 --grad-steps 0 "
                "--bgrad-members 0 --full-steps 0",
-    "kernels": {  # name: (DRAM bytes, warp instructions) per launch
-        "k_scan_patch": (285.3e6, 12.72e6),
-        "k_list_patch": (0.081e6, 0.119e6),
-        "k_records_list": (185.4e6, 71.14e6),
-        "k_tile_list": (174.5e6, 424.1e6),
-        "k_src2_list": (56.19e6, 87.88e6),
+    "kernels": {  # name: (DRAM bytes, warp instructions) per launch, the mean of the 6 launches
+        "k_scan_patch": (1294.0e6, 48.61e6),
+        "k_list_patch": (0.4e6, 0.55e6),
+        "k_records_list": (771.7e6, 280.61e6),
+        "k_tile_list": (763.1e6, 1426.81e6),
+        "k_src2_list": (317.8e6, 373.32e6),
     },
-    # k_tile_list, --set full: active lanes per warp instruction, FP64 pipe
-    "k_tile_list_lanes": 21.97,
-    "k_tile_list_fp64_pipe": 0.258,
+    # k_tile_list, --set full on the 2048^2 case: active lanes per warp
+    # instruction, FP64 pipe active
+    "k_tile_list_lanes": 20.84,
+    "k_tile_list_fp64_pipe": 0.298,
 }
 SMS, SCHEDULERS_PER_SM = 148, 4
 METRIC = "cell-updates/sec on 1 B200 (plain vs batched); gradient/forward time ratio"
@@ -743,7 +744,7 @@ def run_ours(args):
                           f"applied to the step) over 32 lanes per issue slot",
              "k_tile_list_fp64_pipe": NCU_STEP["k_tile_list_fp64_pipe"],
              "source": "smsp__inst_executed.sum per kernel from ncu at "
-                       f"{int(NCU_STEP['cells'] ** 0.5)}^2, scaled by cells"}
+                       f"{int(NCU_STEP['cells'] ** 0.5)}^2, scaled by cells (x1 on that workload)"}
     out = None
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
@@ -753,7 +754,8 @@ def run_ours(args):
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": traffic,
                             "traffic_note": f"DRAM bytes read + written per step from ncu at "
-                                            f"{int(NCU_STEP['cells'] ** 0.5)}^2, scaled by cells",
+                                            f"{int(NCU_STEP['cells'] ** 0.5)}^2, scaled by cells (x1 on that "
+                                            f"workload)",
                             "algorithmic_bytes": BYTES_PER_CELL_UPDATE * cells,
                             "kernel": "the step over tile lists: k_scan_patch + k_list_patch + k_records_list + "
                                       "k_tile_list + k_src2_list (88 B/cell-update algorithmic)",
