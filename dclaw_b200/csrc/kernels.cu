@@ -49,6 +49,11 @@ static std::mutex g_setup_mu;
 #ifndef DCLAW_SRC2_KERNEL
 #define DCLAW_SRC2_KERNEL 1
 #endif
+// the same choice for the step over tile lists: k_src2_list (1), or src2 and
+// the tick in k_tile_list (0)
+#ifndef DCLAW_LIST_SRC2_KERNEL
+#define DCLAW_LIST_SRC2_KERNEL 1
+#endif
 constexpr int TILE_X = DCLAW_TILE_X, TILE_Y = DCLAW_TILE_Y;
 // resident blocks per SM the ensemble's streaming scan is sized for
 #ifndef DCLAW_SCAN_MINB
@@ -707,10 +712,13 @@ __global__ void __launch_bounds__(TPB, DCLAW_PLAIN_CELL_MINB) k_records_list(dcl
 }
 
 // persistent: each CTA takes active tiles from the queue until it is empty;
-// the Courant number is max-reduced once per CTA at the end
+// the Courant number is max-reduced once per CTA at the end. WITH_SRC2:
+// q_out receives the state after src2 and the last CTA applies the tick
+// (no k_src2_list); otherwise the pre-src2 state.
+template <bool WITH_SRC2>
 __global__ void __launch_bounds__(TILE_TPB, DCLAW_TILE_MINBLOCKS) k_tile_list(dclaw_params P, Geom g, Rec R,
                                                                              const double* __restrict__ b,
-                                                                             double* __restrict__ q_star,
+                                                                             double* __restrict__ q_out,
                                                                              dclaw_clock* clk, unsigned int* counters,
                                                                              const uint32_t* __restrict__ list_act) {
     extern __shared__ double smem[];
@@ -730,7 +738,8 @@ __global__ void __launch_bounds__(TILE_TPB, DCLAW_TILE_MINBLOCKS) k_tile_list(dc
         if (t == 0xffffffffu) break;
         const int i0 = 1 + (int)(t % ntx) * TILE_X, j0 = 1 + (int)(t / ntx) * TILE_Y;
         bool nan;
-        const double c = tile_body<TILE_X, TILE_Y, false, TILE_TPB>(P, g, R, b, q_star, dt, i0, j0, smem, nullptr, nan);
+        const double c =
+            tile_body<TILE_X, TILE_Y, WITH_SRC2, TILE_TPB>(P, g, R, b, q_out, dt, i0, j0, smem, nullptr, nan);
         cfl = fmax2(cfl, c);
         nan_any = nan_any || nan;
         // the next tile's staging overwrites shared memory and s_t
@@ -738,6 +747,7 @@ __global__ void __launch_bounds__(TILE_TPB, DCLAW_TILE_MINBLOCKS) k_tile_list(dc
     }
     if (nan_any) flag_status(clk, DCLAW_ERR_NAN);
     block_max_to(cfl, reinterpret_cast<unsigned long long*>(&clk->cfl_bits));
+    if (WITH_SRC2) last_block_tick(P, clk);
 }
 
 __global__ void __launch_bounds__(SRC2_TPB, SRC2_MINB) k_src2_list(dclaw_params P, Geom g,
@@ -1251,7 +1261,9 @@ inline int ensure_tile_smem_attr() {
                                      bytes) != cudaSuccess ||
                 cudaFuncSetAttribute(k_tile<TILE_X, TILE_Y, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      bytes) != cudaSuccess ||
-                cudaFuncSetAttribute(k_tile_list, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
+                cudaFuncSetAttribute(k_tile_list<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+                    cudaSuccess ||
+                cudaFuncSetAttribute(k_tile_list<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
                 return DCLAW_ERR_CUDA;
             done[dev].store(true, std::memory_order_release);
         }
@@ -1487,7 +1499,11 @@ int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int m
         k_records_list<<<g1, TPB, 0, s>>>(P, g, q_in, b, R, counters, list_rec);
         unsigned g2 = (unsigned)(nsm * DCLAW_TILE_MINBLOCKS);
         if (g2 > ntiles) g2 = ntiles;
-        k_tile_list<<<g2, TILE_TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, qstar, clock, counters, list_act);
+        if (!DCLAW_LIST_SRC2_KERNEL) {
+            k_tile_list<true><<<g2, TILE_TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, q_out, clock, counters, list_act);
+            return cuda_status();
+        }
+        k_tile_list<false><<<g2, TILE_TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, qstar, clock, counters, list_act);
         unsigned g3 = (unsigned)(nsm * SRC2_MINB);
         if (g3 > ntiles) g3 = ntiles;
         k_src2_list<<<g3, SRC2_TPB, 0, s>>>(P, g, qstar, q_out, clock, counters, list_act);
