@@ -99,6 +99,9 @@ def parse():
     ap.add_argument("--full-steps", type=int, default=200,
                     help="steps of the whole-run leg of the plain case from its initial state "
                          "(the case is defined over 200; 0: skip)")
+    ap.add_argument("--variant-steps", type=int, default=10,
+                    help="timed steps of each option variant of the plain case (src2method 2, Manning, order 1, "
+                         "the full state with segregation and entrainment); 0: skip")
     ap.add_argument("--slab-steps", type=int, default=0,
                     help="also step ONE patch of the case split into row slabs over the N ranks "
                          "(strong scaling; halo exchange + Courant max per step); 0: skip")
@@ -571,6 +574,52 @@ def batched_gradient_bench(args, dev):
             "note": "every member's dt from its own tick rule, recorded and replayed, not differentiated"}
 
 
+def variants_bench(args, dev, case, plain_ms):
+    """The plain case's state under option variants of the step, each from
+    the case's initial state: `warmup` untimed steps, then `--variant-steps`
+    timed ones (CUDA events on the launching stream). The full-state variant
+    steps the seven-field state (dclaw_step_full) with segregation (chi0 =
+    0.5, beta_seg 0.3) and entrainment (ent_dclaw4, method 0) over an
+    erodible layer of 0.5 m under every cell."""
+    import torch
+
+    from dclaw_b200 import workloads as W
+    from dclaw_b200.solver import PatchStepper
+
+    cells = case.mx * case.my
+    b = torch.tensor(case.b, device=dev)
+    out = {"steps": args.variant_steps, "warmup": args.warmup, "unit": "cell-updates/s",
+           "plain_ms_per_step": plain_ms}
+    runs = {"src2method2": (dict(src2method=2, alphamethod=1), False),
+            "manning": (dict(friction_forcing=True, manning_coefficient=0.03), False),
+            "order1_no_transverse": (dict(order=1, transverse_waves=0), False),
+            "full_state_segregation_entrainment": (dict(segregation=1, beta_seg=0.3, entrainment=1,
+                                                        entrainment_method=0), True)}
+    for name, (kw, full) in runs.items():
+        p = case.params.replace(**kw)
+        if full:
+            q = torch.tensor(W.full_state(case.q, p), device=dev)
+            he = torch.full((case.my, case.mx), 0.5, dtype=torch.float64, device=dev)
+            st = PatchStepper(q, b, p, case.dx, case.dy, h_e=he)
+        else:
+            st = PatchStepper(torch.tensor(case.q, device=dev), b, p, case.dx, case.dy)
+        st.init_clock(case.dt_initial)
+        st.step(args.warmup)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st.step(args.variant_steps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.variant_steps
+        out[name] = {"ms_per_step": ms, "value": cells / (ms / 1000.0), "vs_plain_time": ms / plain_ms,
+                     "launches_per_step": 7 if full else 5, "status": st.status()}
+        del st
+        torch.cuda.empty_cache()
+    return out
+
+
 def slab_bench(args, dev, rank, world, barrier):
     """ONE patch of the case (the same on every rank) split into row slabs
     over the ranks: halo exchange, own rows, Courant max, tick per step
@@ -783,6 +832,8 @@ def run_ours(args):
             out["one_patch_slabs"] = sl
     if world > 1:
         dist.barrier()
+    if rank == 0 and world == 1 and args.variant_steps > 0:
+        out["variants"] = variants_bench(args, dev, case, ms / args.steps)
     if rank == 0 and world == 1 and args.ensemble_members > 0:
         del st
         torch.cuda.empty_cache()
