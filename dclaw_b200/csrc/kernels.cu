@@ -54,6 +54,10 @@ static std::mutex g_setup_mu;
 #ifndef DCLAW_LIST_SRC2_KERNEL
 #define DCLAW_LIST_SRC2_KERNEL 1
 #endif
+// and for the ensemble step: k_src2_batch (1), or src2 in k_tile_batch (0)
+#ifndef DCLAW_BATCH_SRC2_KERNEL
+#define DCLAW_BATCH_SRC2_KERNEL 1
+#endif
 constexpr int TILE_X = DCLAW_TILE_X, TILE_Y = DCLAW_TILE_Y;
 // resident blocks per SM the ensemble's streaming scan is sized for
 #ifndef DCLAW_SCAN_MINB
@@ -894,7 +898,8 @@ template <int TX, int TY>
 __global__ void __launch_bounds__(TPB, 2) k_tile_batch(int nmem, uint32_t ntiles, const dclaw_member* __restrict__ mem,
                                                        const dclaw_params* __restrict__ prm, dclaw_clock* clocks,
                                                        const double* __restrict__ b, double* __restrict__ work,
-                                                       unsigned int* counters, const uint32_t* __restrict__ list_act) {
+                                                       unsigned int* counters, const uint32_t* __restrict__ list_act,
+                                                       double* __restrict__ q_out) {
     extern __shared__ double smem[];
     __shared__ dclaw_member sM;
     __shared__ dclaw_params sP;
@@ -925,8 +930,11 @@ __global__ void __launch_bounds__(TPB, 2) k_tile_batch(int nmem, uint32_t ntiles
         const unsigned int lt = t - sM.tile0;
         const int i0 = 1 + (int)(lt % sM.ntiles_x) * TX, j0 = 1 + (int)(lt / sM.ntiles_x) * TY;
         bool nan;
-        double cfl = tile_body<TX, TY, false, TPB>(sP, g, R, b + sM.b_off, work + sM.qs_off, clocks[m].dt, i0, j0, smem,
-                                              nullptr, nan);
+        // with src2 in this kernel the tile writes the member's new state,
+        // otherwise its pre-src2 state (k_src2_batch follows)
+        double* dst = DCLAW_BATCH_SRC2_KERNEL ? work + sM.qs_off : q_out + sM.q_off;
+        double cfl = tile_body<TX, TY, !DCLAW_BATCH_SRC2_KERNEL, TPB>(sP, g, R, b + sM.b_off, dst, clocks[m].dt, i0, j0,
+                                                                     smem, nullptr, nan);
         if (nan) flag_status(clocks + m, DCLAW_ERR_NAN);
         // block max of this tile's Courant number into member m's clock
         cfl = warp_max(cfl);
@@ -997,12 +1005,12 @@ inline int batch_tile_attr() {
 template <int TX, int TY>
 inline int launch_tile_batch(const dclaw_batch* B, const dclaw_member* mem, const dclaw_params* prm, dclaw_clock* clocks,
                              const double* b, double* work, unsigned int* counters, const uint32_t* list_act, int nsm,
-                             cudaStream_t s) {
+                             cudaStream_t s, double* q_out = nullptr) {
     if (batch_tile_attr<TX, TY>() != DCLAW_OK) return DCLAW_ERR_CUDA;
     unsigned grid = (unsigned)(nsm * (B->tile_ctas_per_sm > 0 ? B->tile_ctas_per_sm : 2));
     if (grid > B->ntiles) grid = B->ntiles > 0 ? B->ntiles : 1;
     k_tile_batch<TX, TY><<<grid, TPB, TileGeom<TX, TY>::SMEM_BYTES, s>>>(B->nmembers, B->ntiles, mem, prm, clocks, b,
-                                                                        work, counters, list_act);
+                                                                        work, counters, list_act, q_out);
     return DCLAW_OK;
 }
 
@@ -1016,8 +1024,9 @@ inline int launch_batch_tiles(const dclaw_batch* B, const dclaw_member* mem, con
     unsigned g1 = (unsigned)(nsm * cpsm);
     if (g1 > B->ntiles) g1 = B->ntiles > 0 ? B->ntiles : 1;
     k_records_tiles_batch<TX, TY><<<g1, TPB, 0, s>>>(B->nmembers, B->ntiles, mem, prm, q_in, b, w, counters, list_rec);
-    int rc = launch_tile_batch<TX, TY>(B, mem, prm, clocks, b, w, counters, list_act, nsm, s);
+    int rc = launch_tile_batch<TX, TY>(B, mem, prm, clocks, b, w, counters, list_act, nsm, s, q_out);
     if (rc != DCLAW_OK) return rc;
+    if (!DCLAW_BATCH_SRC2_KERNEL) return DCLAW_OK;
     unsigned g3 = (unsigned)(nsm * cpsm);
     if (g3 > B->ntiles) g3 = B->ntiles > 0 ? B->ntiles : 1;
     k_src2_batch<TX, TY><<<g3, TPB, 0, s>>>(B->nmembers, B->ntiles, mem, prm, clocks, q_out, w, counters, list_act);
