@@ -68,6 +68,14 @@ constexpr int TILE_X = DCLAW_TILE_X, TILE_Y = DCLAW_TILE_Y;
 #ifndef DCLAW_CELL_MINB
 #define DCLAW_CELL_MINB 4
 #endif
+// threads per CTA of those two (one tile's cells per CTA pass), with the
+// register budget of DCLAW_CELL_MINB blocks of 256 threads. 192 (as the
+// single patch's) measured 3 % slower on the 256-flume ensemble.
+#ifndef DCLAW_BATCH_CELL_TPB
+#define DCLAW_BATCH_CELL_TPB 256
+#endif
+constexpr int BATCH_CELL_TPB = DCLAW_BATCH_CELL_TPB;
+constexpr int BATCH_CELL_MINB = DCLAW_CELL_MINB * 256 / DCLAW_BATCH_CELL_TPB;
 // resident blocks per SM the single-patch per-cell kernels (k_records,
 // k_src2_cells) are sized for: on the 4096^2 random field 6 (40 registers,
 // with spills) steps 1.9 % faster than 4 (64 registers), 5 1.2 % and 8
@@ -77,15 +85,25 @@ constexpr int TILE_X = DCLAW_TILE_X, TILE_Y = DCLAW_TILE_Y;
 #ifndef DCLAW_PLAIN_CELL_MINB
 #define DCLAW_PLAIN_CELL_MINB 6
 #endif
-// threads per CTA of k_src2_cells (its register budget is that of
-// DCLAW_PLAIN_CELL_MINB blocks of 256 threads whatever the CTA size).
-// Smaller CTAs retire their dry warps sooner, but measured on the 4096^2
-// field 128 threads step as fast as 256 and 64 threads 1 % slower.
+// threads per CTA of k_src2_list and k_src2_cells (the register budget is
+// that of DCLAW_PLAIN_CELL_MINB blocks of 256 threads whatever the CTA
+// size). k_src2_list gives each CTA one tile's 14 x 13 = 182 cells per
+// pass, which 192 threads cover in six warps (256 left two warps idle):
+// with the records likewise the step takes 3.87 ms on the 4096^2 field
+// against 3.96 ms at 256, with the same bits.
 #ifndef DCLAW_SRC2_TPB
-#define DCLAW_SRC2_TPB 256
+#define DCLAW_SRC2_TPB 192
 #endif
 constexpr int SRC2_TPB = DCLAW_SRC2_TPB;
 constexpr int SRC2_MINB = DCLAW_PLAIN_CELL_MINB * 256 / DCLAW_SRC2_TPB;
+// threads per CTA of k_records_list (one tile's records per CTA pass, 182
+// for an interior tile), with the register budget of DCLAW_PLAIN_CELL_MINB
+// blocks of 256 threads
+#ifndef DCLAW_RECORDS_TPB
+#define DCLAW_RECORDS_TPB 192
+#endif
+constexpr int RECORDS_TPB = DCLAW_RECORDS_TPB;
+constexpr int RECORDS_MINB = DCLAW_PLAIN_CELL_MINB * 256 / DCLAW_RECORDS_TPB;
 
 __device__ __forceinline__ double warp_max(double v) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -702,7 +720,7 @@ __global__ void __launch_bounds__(TPB) k_list_patch(int ntx, int nty, const dcla
     if (rec) list_rec[base_r + __popc(br & below)] = t;
 }
 
-__global__ void __launch_bounds__(TPB, DCLAW_PLAIN_CELL_MINB) k_records_list(dclaw_params P, Geom g,
+__global__ void __launch_bounds__(RECORDS_TPB, RECORDS_MINB) k_records_list(dclaw_params P, Geom g,
                                                                             const double* __restrict__ q_in,
                                                                             const double* __restrict__ b, Rec R,
                                                                             const unsigned int* counters,
@@ -847,7 +865,7 @@ __global__ void __launch_bounds__(TPB) k_list_batch(int nmem, uint32_t ntiles, c
 
 // pass 2 of the records over the listed tiles (grid-stride over the list)
 template <int TX, int TY>
-__global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_records_tiles_batch(int nmem, uint32_t ntiles,
+__global__ void __launch_bounds__(BATCH_CELL_TPB, BATCH_CELL_MINB) k_records_tiles_batch(int nmem, uint32_t ntiles,
                                                                               const dclaw_member* __restrict__ mem,
                                                                               const dclaw_params* __restrict__ prm,
                                                                               const double* __restrict__ q_in,
@@ -955,7 +973,7 @@ __global__ void __launch_bounds__(TPB, 2) k_tile_batch(int nmem, uint32_t ntiles
 // src2 of the active tiles' cells (grid-stride over the active list; the
 // scan has written the zeros of every other cell)
 template <int TX, int TY>
-__global__ void __launch_bounds__(TPB, DCLAW_CELL_MINB) k_src2_batch(int nmem, uint32_t ntiles, const dclaw_member* __restrict__ mem,
+__global__ void __launch_bounds__(BATCH_CELL_TPB, BATCH_CELL_MINB) k_src2_batch(int nmem, uint32_t ntiles, const dclaw_member* __restrict__ mem,
                                                     const dclaw_params* __restrict__ prm, const dclaw_clock* clocks,
                                                     double* __restrict__ q_out, const double* __restrict__ work,
                                                     const unsigned int* counters,
@@ -1023,13 +1041,15 @@ inline int launch_batch_tiles(const dclaw_batch* B, const dclaw_member* mem, con
                               const uint32_t* list_rec, int nsm, int cpsm, cudaStream_t s) {
     unsigned g1 = (unsigned)(nsm * cpsm);
     if (g1 > B->ntiles) g1 = B->ntiles > 0 ? B->ntiles : 1;
-    k_records_tiles_batch<TX, TY><<<g1, TPB, 0, s>>>(B->nmembers, B->ntiles, mem, prm, q_in, b, w, counters, list_rec);
+    k_records_tiles_batch<TX, TY><<<g1, BATCH_CELL_TPB, 0, s>>>(B->nmembers, B->ntiles, mem, prm, q_in, b, w, counters,
+                                                                 list_rec);
     int rc = launch_tile_batch<TX, TY>(B, mem, prm, clocks, b, w, counters, list_act, nsm, s, q_out);
     if (rc != DCLAW_OK) return rc;
     if (!DCLAW_BATCH_SRC2_KERNEL) return DCLAW_OK;
     unsigned g3 = (unsigned)(nsm * cpsm);
     if (g3 > B->ntiles) g3 = B->ntiles > 0 ? B->ntiles : 1;
-    k_src2_batch<TX, TY><<<g3, TPB, 0, s>>>(B->nmembers, B->ntiles, mem, prm, clocks, q_out, w, counters, list_act);
+    k_src2_batch<TX, TY><<<g3, BATCH_CELL_TPB, 0, s>>>(B->nmembers, B->ntiles, mem, prm, clocks, q_out, w, counters,
+                                                        list_act);
     return DCLAW_OK;
 }
 
@@ -1503,9 +1523,9 @@ int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int m
         if ((long long)g0 * TPB > ncell) g0 = nblocks(ncell);
         k_scan_patch<<<g0, TPB, 0, s>>>(P, mx, my, q_in, q_out, clock, counters, tflag);
         k_list_patch<<<(ntiles + TPB - 1) / TPB, TPB, 0, s>>>(ntx, nty, clock, tflag, counters, list_act, list_rec);
-        unsigned g1 = (unsigned)(nsm * DCLAW_PLAIN_CELL_MINB);
+        unsigned g1 = (unsigned)(nsm * RECORDS_MINB);
         if (g1 > ntiles) g1 = ntiles;
-        k_records_list<<<g1, TPB, 0, s>>>(P, g, q_in, b, R, counters, list_rec);
+        k_records_list<<<g1, RECORDS_TPB, 0, s>>>(P, g, q_in, b, R, counters, list_rec);
         unsigned g2 = (unsigned)(nsm * DCLAW_TILE_MINBLOCKS);
         if (g2 > ntiles) g2 = ntiles;
         if (!DCLAW_LIST_SRC2_KERNEL) {
