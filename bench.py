@@ -627,6 +627,7 @@ def slab_bench(args, dev, rank, world, barrier):
     one after another on the one GPU: the work the halos add."""
     import torch
 
+    from dclaw_b200 import _lib
     from dclaw_b200.replicas import max_over_ranks
     from dclaw_b200.slabs import DistSlabs, LocalSlabs
 
@@ -652,7 +653,7 @@ def slab_bench(args, dev, rank, world, barrier):
     ms = max_over_ranks(e0.elapsed_time(e1), dev)
     cells = case.mx * case.my
     return {"workload": f"random_field_{case.mx}x{case.my}_dx{case.dx}", "slabs": nslab, "ranks": world,
-            "halo_rows": 14, "steps": args.slab_steps, "ms_per_step": ms / args.slab_steps,
+            "halo_rows": _lib.load().dclaw_rows_granule(), "steps": args.slab_steps, "ms_per_step": ms / args.slab_steps,
             "value": cells * args.slab_steps / (ms / 1000.0), "unit": "cell-updates/s",
             "scaling": "strong" if world > 1 else "one GPU, slabs in turn",
             "gpu_launches_per_step_per_slab": 4}
