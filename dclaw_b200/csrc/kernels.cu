@@ -32,9 +32,11 @@ constexpr int MAX_DEVICES = 64;
 // race on the caches.
 static std::mutex g_setup_mu;
 // tile of the fused step: with 14 x 13 the solves of each sweep fit in one
-// round of 256 threads (255 and 256 interfaces) and the flux phases too (210
-// and 208 cells). On the 4096^2 random field it steps 2 % faster than 16 x 14
-// (whose solves take two rounds) and 7 % faster than 12 x 14.
+// round of 256 threads (255 and 256 interfaces), and the flux phases' half-
+// warp per slice does too (15 rows, 16 columns). Before the flux phases
+// exchanged interfaces between lanes, 14 x 13 stepped the 4096^2 random
+// field 2 % faster than 16 x 14 (whose solves take two rounds) and 7 %
+// faster than 12 x 14.
 #ifndef DCLAW_TILE_X
 #define DCLAW_TILE_X 14
 #endif
