@@ -77,6 +77,26 @@ def test_fused_tile_shapes_and_partial_tiles(oracle, emu, tile, src2_in_tile):
     assert np.array_equal(np.concatenate([r1["xlog"].ravel(), r1["ylog"].ravel()]), r2["br"])
 
 
+@pytest.mark.parametrize("tile", [(14, 13), (16, 14)])
+@pytest.mark.parametrize("shape", [(2, 2), (17, 3), (3, 17), (13, 14), (14, 15), (27, 29)])
+def test_fused_small_patches(oracle, emu, tile, shape):
+    """Patches smaller than, equal to or just over one tile, and thin strips,
+    around the wettest cell of a random field: the flux phase with each
+    interface limited once (14 x 13) and with each cell limiting both of
+    its interfaces (16 x 14) give the oracle's state and branch bits."""
+    c = W.random_field_case(n=128, dx=0.5, seed=4)
+    my, mx = shape
+    j, i = np.unravel_index(np.argmax(c.q[0]), c.q[0].shape)
+    j0, i0 = max(0, j - my // 2), max(0, i - mx // 2)
+    q = c.q[:, j0:j0 + my, i0:i0 + mx].copy()
+    b = c.b[j0:j0 + my, i0:i0 + mx].copy()
+    assert q[0].max() > 0.0
+    r1 = oracle.run(c.params, q, b, c.dx, c.dy, 10, c.dt_initial, branch_log=True, libm="portable")
+    r2 = emu.run(c.params, q, b, c.dx, c.dy, 10, c.dt_initial, fused=True, tile=tile)
+    assert np.array_equal(r1["q"], r2["q"])
+    assert np.array_equal(np.concatenate([r1["xlog"].ravel(), r1["ylog"].ravel()]), r2["br"])
+
+
 # ---- the full-state step (segregation, entrainment) --------------------------
 FULL_VARIANTS = {
     "extras_zero": dict(segregation=0, entrainment=0),
