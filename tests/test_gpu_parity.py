@@ -133,6 +133,20 @@ def test_random_field_small(cuda_device, oracle):
     check(W.random_field_case(n=256, dx=0.5, seed=5), 30, oracle)
 
 
+@pytest.mark.parametrize("shape", [(2, 2), (17, 3), (3, 17), (13, 14), (14, 15), (27, 29)])
+def test_small_patches(cuda_device, oracle, shape):
+    """Patches smaller than, equal to or just over one 14 x 13 tile, and thin
+    strips, cut around the wettest cell of a random field: bit for bit
+    against the oracle through the full-grid and the tile-list kernels."""
+    c = W.random_field_case(n=128, dx=0.5, seed=4)
+    my, mx = shape
+    j, i = np.unravel_index(np.argmax(c.q[0]), c.q[0].shape)
+    j0, i0 = max(0, j - my // 2), max(0, i - mx // 2)
+    q = np.ascontiguousarray(c.q[:, j0:j0 + my, i0:i0 + mx])
+    b = np.ascontiguousarray(c.b[j0:j0 + my, i0:i0 + mx])
+    check(W.Case("small", q, b, c.dx, c.dy, c.params, 10, c.dt_initial), 10, oracle, glibc_steps=0)
+
+
 def test_dry_tile_fast_path(cuda_device, oracle):
     """Without a branch log the fused step skips tiles whose cells within 3 are
     all dry; the result must not change (mostly dry 384 x 384 random field)."""
