@@ -310,13 +310,41 @@ __global__ void __launch_bounds__(TPB) k_final(dclaw_params P, Geom g, Work W, d
 }
 
 // ---- the full-state step (segregation, entrainment) -------------------------
+// Without a branch log the stages after b4 skip what no active cell reads.
+// A tile is active when a wet padded cell lies within 3 of its cells (the
+// fused step's marks, step-numbered in tflag). A cell of an inactive tile
+// has only dry cells within 3: every interface within 2 of it is dry-dry,
+// so its waves and fluxes are exact zeros and its new state is zero with
+// the eroded depth passed through, which the final stage writes without
+// reading any flux. An interface's flux is read by the updates of the cells
+// within one row (x) or column (y) of its two cells; its waves by its own
+// flux and its two neighbours' along the slice. Each is computed when one
+// of those readers is, so nothing skipped is ever read.
+__device__ __forceinline__ bool full_any_active(const uint32_t* __restrict__ tflag, uint32_t epoch, const Geom& g,
+                                                int ia, int ib, int ja, int jb) {
+    ia = ia < 1 ? 1 : ia;
+    ja = ja < 1 ? 1 : ja;
+    ib = ib > g.mx ? g.mx : ib;
+    jb = jb > g.my ? g.my : jb;
+    if (ia > ib || ja > jb) return false;
+    const int ntx = (g.mx + TILE_X - 1) / TILE_X;
+    for (int ty = (ja - 1) / TILE_Y; ty <= (jb - 1) / TILE_Y; ++ty)
+        for (int tx = (ia - 1) / TILE_X; tx <= (ib - 1) / TILE_X; ++tx)
+            if (tflag[ty * ntx + tx] == epoch) return true;
+    return false;
+}
+
 __global__ void __launch_bounds__(TPB) k_full_b4(dclaw_params P, Geom g, const double* __restrict__ q_in,
-                                                 const double* __restrict__ b, WorkF W, dclaw_clock* clk) {
+                                                 const double* __restrict__ b, WorkF W, dclaw_clock* clk,
+                                                 uint32_t* __restrict__ tflag) {
     const long long n = (long long)g.PX * g.PY;
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n) return;
     int i = (int)(idx % g.PX) - 1, j = (int)(idx / g.PX) - 1;
     if (full_b4(P, g, q_in, b, W, i, j)) flag_status(clk, DCLAW_ERR_NAN);
+    if (tflag && W.qB[pidx(g, i, j)] > 0.0)
+        mark_tiles(tflag, clk->nsteps + 1u, i, j, TILE_X, TILE_Y, (g.mx + TILE_X - 1) / TILE_X,
+                   (g.my + TILE_Y - 1) / TILE_Y);
 }
 
 __global__ void __launch_bounds__(TPB) k_full_taudir(dclaw_params P, Geom g, WorkF W) {
@@ -329,7 +357,8 @@ __global__ void __launch_bounds__(TPB) k_full_taudir(dclaw_params P, Geom g, Wor
 
 template <int DIR>
 __global__ void __launch_bounds__(TPB) k_full_riemann(dclaw_params P, Geom g, WorkF W, dclaw_clock* clk,
-                                                      uint32_t* __restrict__ brlog) {
+                                                      uint32_t* __restrict__ brlog,
+                                                      const uint32_t* __restrict__ tflag) {
     const int nfast = DIR == 0 ? g.mx + 3 : g.mx + 2;
     const int nslow = DIR == 0 ? g.my + 2 : g.my + 3;
     const long long n = (long long)nfast * nslow;
@@ -340,26 +369,33 @@ __global__ void __launch_bounds__(TPB) k_full_riemann(dclaw_params P, Geom g, Wo
         int r = DIR == 0 ? s : a;
         int i = DIR == 0 ? a : s;
         const int nlen = DIR == 0 ? g.mx : g.my;
-        uint32_t bits = 0;
-        double smax = full_riemann<DIR>(P, g, W, r, i, &bits);
-        if (i >= 1 && i <= nlen + 1) {
-            const double dt = clk->dt;
-            const double dtdx = DIR == 0 ? dt / g.dx : dt / g.dy;
-            cflv = dtdx * smax;
-            if (brlog) {
-                size_t off = DIR == 0 ? (size_t)r * (g.mx + 1) + (size_t)(i - 1)
-                                      : (size_t)(g.my + 2) * (g.mx + 1) + (size_t)r * (g.my + 1) + (size_t)(i - 1);
-                brlog[off] = bits;
+        // read by the fluxes at i-1, i, i+1 of the slice: cells i-2..i+1 along
+        // it, one slice either side (a skipped interface is dry-dry: no speed)
+        const uint32_t ep = clk->nsteps + 1u;
+        const bool need = !tflag || (DIR == 0 ? full_any_active(tflag, ep, g, i - 2, i + 1, r - 1, r + 1)
+                                              : full_any_active(tflag, ep, g, r - 1, r + 1, i - 2, i + 1));
+        if (need) {
+            uint32_t bits = 0;
+            double smax = full_riemann<DIR>(P, g, W, r, i, &bits);
+            if (i >= 1 && i <= nlen + 1) {
+                const double dt = clk->dt;
+                const double dtdx = DIR == 0 ? dt / g.dx : dt / g.dy;
+                cflv = dtdx * smax;
+                if (brlog) {
+                    size_t off = DIR == 0 ? (size_t)r * (g.mx + 1) + (size_t)(i - 1)
+                                          : (size_t)(g.my + 2) * (g.mx + 1) + (size_t)r * (g.my + 1) + (size_t)(i - 1);
+                    brlog[off] = bits;
+                }
             }
+            if (!(cflv == cflv)) cflv = 0.0;
         }
-        if (!(cflv == cflv)) cflv = 0.0;
     }
     block_max_to(cflv, reinterpret_cast<unsigned long long*>(&clk->cfl_bits));
 }
 
 template <int DIR>
 __global__ void __launch_bounds__(TPB) k_full_flux(dclaw_params P, Geom g, WorkF W, const dclaw_clock* clk,
-                                                   uint32_t* __restrict__ brlog) {
+                                                   uint32_t* __restrict__ brlog, const uint32_t* __restrict__ tflag) {
     const int nfast = DIR == 0 ? g.mx + 1 : g.mx + 2;
     const int nslow = DIR == 0 ? g.my + 2 : g.my + 1;
     const long long n = (long long)nfast * nslow;
@@ -368,6 +404,13 @@ __global__ void __launch_bounds__(TPB) k_full_flux(dclaw_params P, Geom g, WorkF
     int a = (int)(idx % nfast), s = (int)(idx / nfast);
     int r = DIR == 0 ? s : a;
     int i = DIR == 0 ? a + 1 : s + 1;
+    // read by the updates of cells i-1, i along the slice, one slice either side
+    if (tflag) {
+        const uint32_t ep = clk->nsteps + 1u;
+        if (!(DIR == 0 ? full_any_active(tflag, ep, g, i - 1, i, r - 1, r + 1)
+                       : full_any_active(tflag, ep, g, r - 1, r + 1, i - 1, i)))
+            return;
+    }
     const double dt = clk->dt;
     const double dtdx = DIR == 0 ? dt / g.dx : dt / g.dy;
     uint32_t bits = 0;
@@ -380,7 +423,8 @@ __global__ void __launch_bounds__(TPB) k_full_flux(dclaw_params P, Geom g, WorkF
 }
 
 __global__ void __launch_bounds__(TPB) k_full_final(dclaw_params P, Geom g, WorkF W, const double* __restrict__ he,
-                                                    double* __restrict__ q_out, dclaw_clock* clk);
+                                                    double* __restrict__ q_out, dclaw_clock* clk,
+                                                    const uint32_t* __restrict__ tflag);
 
 // the next dt after the tick rule's choice dtn: clipped at the next
 // observation time (with the tick rule and t_obs > 0), then at t_final
@@ -473,12 +517,20 @@ __device__ __forceinline__ void last_block_tick(const dclaw_params& P, dclaw_clo
 
 // update + src2 of the full state; the last block applies the tick
 __global__ void __launch_bounds__(TPB) k_full_final(dclaw_params P, Geom g, WorkF W, const double* __restrict__ he,
-                                                    double* __restrict__ q_out, dclaw_clock* clk) {
+                                                    double* __restrict__ q_out, dclaw_clock* clk,
+                                                    const uint32_t* __restrict__ tflag) {
     const long long n = (long long)g.mx * g.my;
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx < n) {
         int i = (int)(idx % g.mx) + 1, j = (int)(idx / g.mx) + 1;
-        if (full_finalize(P, g, W, he, q_out, i, j, clk->dt)) flag_status(clk, DCLAW_ERR_NAN);
+        if (tflag && !full_any_active(tflag, clk->nsteps + 1u, g, i, i, j, j)) {
+            // a cell of an inactive tile: zero, its eroded depth passed through
+            const size_t plane = (size_t)g.mx * g.my;
+            for (int f = 0; f < F_BDIF; ++f) q_out[(size_t)f * plane + (size_t)idx] = 0.0;
+            q_out[(size_t)F_BDIF * plane + (size_t)idx] = W.qB[(size_t)F_BDIF * W.npad + pidx(g, i, j)];
+        } else if (full_finalize(P, g, W, he, q_out, i, j, clk->dt)) {
+            flag_status(clk, DCLAW_ERR_NAN);
+        }
     }
     last_block_tick(P, clk);
 }
@@ -1820,9 +1872,15 @@ int dclaw_max_wave_speed(const double* q, int mx, int my, const dclaw_params* p,
 
 extern "C" {
 
+// the full-state workspace: the staged planes (full_layout), then the tile
+// flags of the skip
+inline size_t full_tflag_bytes(int mx, int my) {
+    return align256((size_t)((mx + TILE_X - 1) / TILE_X) * (size_t)((my + TILE_Y - 1) / TILE_Y) * 4);
+}
+
 size_t dclaw_step_full_workspace_bytes(int mx, int my) {
     if (!sizes_ok(mx, my)) return 0;
-    return full_layout(mx, my).total;
+    return full_layout(mx, my).total + full_tflag_bytes(mx, my);
 }
 
 int dclaw_step_full(const double* q_in, double* q_out, const double* b, const double* h_e, int mx, int my,
@@ -1834,23 +1892,25 @@ int dclaw_step_full(const double* q_in, double* q_out, const double* b, const do
     if (rc) return rc;
     if (p->entrainment == 1 && p->entrainment_method == 0 && !h_e) return DCLAW_ERR_ARG;
     const FullLayout L = full_layout(mx, my);
-    if (work_bytes < L.total) return DCLAW_ERR_WORKSPACE;
+    if (work_bytes < L.total + full_tflag_bytes(mx, my)) return DCLAW_ERR_WORKSPACE;
     cudaStream_t s = (cudaStream_t)stream;
     Geom g{mx, my, mx + 4, my + 4, dx, dy};
     WorkF W = make_work_full(work, L);
+    // with a branch log every interface is computed (its bits are logged)
+    uint32_t* tflag = branch_log ? nullptr : (uint32_t*)((char*)work + L.total);
     const dclaw_params P = *p;
     if (branch_log) {
         size_t nlog = (size_t)(my + 2) * (mx + 1) + (size_t)(mx + 2) * (my + 1);
         cudaMemsetAsync(branch_log, 0, nlog * sizeof(uint32_t), s);
     }
     const long long npad = (long long)g.PX * g.PY;
-    k_full_b4<<<nblocks(npad), TPB, 0, s>>>(P, g, q_in, b, W, clock);
+    k_full_b4<<<nblocks(npad), TPB, 0, s>>>(P, g, q_in, b, W, clock, tflag);
     k_full_taudir<<<nblocks(npad), TPB, 0, s>>>(P, g, W);
-    k_full_riemann<0><<<nblocks((long long)(mx + 3) * (my + 2)), TPB, 0, s>>>(P, g, W, clock, branch_log);
-    k_full_riemann<1><<<nblocks((long long)(mx + 2) * (my + 3)), TPB, 0, s>>>(P, g, W, clock, branch_log);
-    k_full_flux<0><<<nblocks((long long)(mx + 1) * (my + 2)), TPB, 0, s>>>(P, g, W, clock, branch_log);
-    k_full_flux<1><<<nblocks((long long)(mx + 2) * (my + 1)), TPB, 0, s>>>(P, g, W, clock, branch_log);
-    k_full_final<<<nblocks((long long)mx * my), TPB, 0, s>>>(P, g, W, h_e, q_out, clock);
+    k_full_riemann<0><<<nblocks((long long)(mx + 3) * (my + 2)), TPB, 0, s>>>(P, g, W, clock, branch_log, tflag);
+    k_full_riemann<1><<<nblocks((long long)(mx + 2) * (my + 3)), TPB, 0, s>>>(P, g, W, clock, branch_log, tflag);
+    k_full_flux<0><<<nblocks((long long)(mx + 1) * (my + 2)), TPB, 0, s>>>(P, g, W, clock, branch_log, tflag);
+    k_full_flux<1><<<nblocks((long long)(mx + 2) * (my + 1)), TPB, 0, s>>>(P, g, W, clock, branch_log, tflag);
+    k_full_final<<<nblocks((long long)mx * my), TPB, 0, s>>>(P, g, W, h_e, q_out, clock, tflag);
     return cuda_status();
 }
 
