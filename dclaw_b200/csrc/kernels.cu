@@ -1369,13 +1369,14 @@ constexpr int MAX_HOST_BANDS = 64;
 
 inline int host_auto_bands(int mx, int my) {
     const int nty = (my + TILE_Y - 1) / TILE_Y;
-    // about 40 MB of state per band: enough work per band to fill the GPU
+    // about 28 MB of state per band: enough work per band to fill the GPU
     // and few enough launches and copies, fine enough that the first upload
     // and the last download (the parts that do not overlap) stay short. On
-    // the 4096^2 state (16 bands) the step then takes 1.07x the time of
-    // the bare copies both ways at once; 4 bands take 1.25x, 64 take 1.22x.
+    // the 4096^2 state (24 bands) the step then takes 15.2 ms, 1.03x the
+    // bare copies both ways at once (14.7 ms); 12, 17, 20, 28 and 32 bands
+    // took 15.7, 15.5, 15.2, 15.5 and 15.6 ms, 4 bands 1.25x, 64 bands 1.22x.
     const double state = 40.0 * mx * (double)my;
-    int nb = (int)(state / 40.0e6) + 1;
+    int nb = (int)(state / 28.0e6) + 1;
     if (nb > MAX_HOST_BANDS) nb = MAX_HOST_BANDS;
     if (nb > nty) nb = nty;
     return nb < 1 ? 1 : nb;

@@ -243,7 +243,7 @@ size_t dclaw_step_noalloc_max_cells(void);
  * directions and the compute overlap. Host memory must be page-locked
  * (cudaHostAlloc / cudaHostRegister) for the copies to overlap; pageable
  * memory gives the same result without the overlap. nbands = 0 picks the
- * band count (about 40 MB of state per band, at most 64); a positive value
+ * band count (about 28 MB of state per band, at most 64); a positive value
  * asks for that many (capped by the tile rows and 64). The call returns once
  * the work is queued; `stream` waits for the last download, so a
  * synchronize on it (or on an event recorded after the call) means q_out and

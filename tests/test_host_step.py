@@ -36,9 +36,9 @@ def test_band_plan_covers_every_tile_row():
                 assert nb == min(nbands, nty, 64)
             assert first[0] == 0 and first[-1] == nty
             assert all(b > a for a, b in zip(first, first[1:]))      # every band holds a tile row
-    # the automatic choice: about 40 MB of state per band
+    # the automatic choice: about 28 MB of state per band
     nb, _ = _plan(lib, 4096, 4096, 0)
-    assert nb == int(40 * 4096 * 4096 / 40e6) + 1 == 17
+    assert nb == int(40 * 4096 * 4096 / 28e6) + 1 == 24
     assert _plan(lib, 64, 64, 0)[0] == 1
     assert lib.dclaw_step_host_bands(1, 10, 0, None, 0) == 0
 
