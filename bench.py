@@ -656,7 +656,7 @@ def slab_bench(args, dev, rank, world, barrier):
             "halo_rows": _lib.load().dclaw_rows_granule(), "steps": args.slab_steps, "ms_per_step": ms / args.slab_steps,
             "value": cells * args.slab_steps / (ms / 1000.0), "unit": "cell-updates/s",
             "scaling": "strong" if world > 1 else "one GPU, slabs in turn",
-            "gpu_launches_per_step_per_slab": 4}
+            "gpu_launches_per_step_per_slab": 5}
 
 
 def run_ours(args):

@@ -733,32 +733,44 @@ __global__ void __launch_bounds__(SRC2_TPB, SRC2_MINB) k_src2_cells(dclaw_params
 // cells with src2 of the updated state, and its last block applies the tick.
 // Each cell's arithmetic is that of the full-grid kernels, so the results
 // are the same bits; far from the flow a cell costs its 80 bytes of scan.
+// cells [s0, s1) are scanned, cells [z0, z1) of q_out zeroed (linear
+// interior indices; the whole patch for dclaw_step, a row range and the rows
+// within 3 of it for dclaw_step_rows)
 __global__ void __launch_bounds__(TPB, DCLAW_SCAN_MINB) k_scan_patch(dclaw_params P, int mx, int my,
                                                                     const double* __restrict__ q_in,
                                                                     double* __restrict__ q_out, dclaw_clock* clk,
                                                                     unsigned int* counters,
-                                                                    uint32_t* __restrict__ tflag) {
+                                                                    uint32_t* __restrict__ tflag, size_t s0,
+                                                                    size_t s1, size_t z0, size_t z1) {
     if (blockIdx.x == 0 && threadIdx.x < 3) counters[threadIdx.x] = 0u;  // tile queue and list lengths
     const size_t n = (size_t)mx * my;
     const int ntx = (mx + TILE_X - 1) / TILE_X, nty = (my + TILE_Y - 1) / TILE_Y;
+    const size_t lo = s0 < z0 ? s0 : z0, hi = s1 > z1 ? s1 : z1;
     bool nan = false;
-    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
-        if (scan_cell(P, q_in, n, idx, mx, tflag, clk, TILE_X, TILE_Y, ntx, nty)) nan = true;
-        for (int f = 0; f < 5; ++f) q_out[(size_t)f * n + idx] = 0.0;
+    for (size_t idx = lo + (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < hi;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        if (idx >= s0 && idx < s1 && scan_cell(P, q_in, n, idx, mx, tflag, clk, TILE_X, TILE_Y, ntx, nty)) nan = true;
+        if (idx >= z0 && idx < z1)
+            for (int f = 0; f < 5; ++f) q_out[(size_t)f * n + idx] = 0.0;
     }
     if (nan) flag_status(clk, DCLAW_ERR_NAN);
 }
 
+// active tiles of tile rows ty0..ty1, and the tiles of rows ty0-1..ty1+1
+// that are active or next to one (the whole patch: 0..nty-1)
 __global__ void __launch_bounds__(TPB) k_list_patch(int ntx, int nty, const dclaw_clock* clk,
                                                     const uint32_t* __restrict__ tflag, unsigned int* counters,
-                                                    uint32_t* __restrict__ list_act, uint32_t* __restrict__ list_rec) {
+                                                    uint32_t* __restrict__ list_act, uint32_t* __restrict__ list_rec,
+                                                    int ty0, int ty1) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t ntiles = (uint32_t)ntx * (uint32_t)nty;
     const uint32_t epoch = clk->nsteps + 1u;
     bool act = false, rec = false;
     if (t < ntiles) {
-        act = tflag[t] == epoch;
-        rec = act || near_active(tflag, epoch, (int)(t % ntx), (int)(t / ntx), ntx, nty);
+        const int ty = (int)(t / ntx);
+        const bool flag = tflag[t] == epoch;
+        act = flag && ty >= ty0 && ty <= ty1;
+        rec = ty >= ty0 - 1 && ty <= ty1 + 1 && (flag || near_active(tflag, epoch, (int)(t % ntx), ty, ntx, nty));
     }
     const int lane = threadIdx.x & 31;
     const unsigned ba = __ballot_sync(0xffffffffu, act), br = __ballot_sync(0xffffffffu, rec);
@@ -830,7 +842,8 @@ __global__ void __launch_bounds__(SRC2_TPB, SRC2_MINB) k_src2_list(dclaw_params 
                                                                   const double* __restrict__ q_star,
                                                                   double* __restrict__ q_out, dclaw_clock* clk,
                                                                   const unsigned int* counters,
-                                                                  const uint32_t* __restrict__ list_act) {
+                                                                  const uint32_t* __restrict__ list_act,
+                                                                  int tick = 1) {
     const uint32_t nact = counters[1];
     const uint32_t ntx = (uint32_t)((g.mx + TILE_X - 1) / TILE_X);
     const double dt = clk->dt;
@@ -843,7 +856,7 @@ __global__ void __launch_bounds__(SRC2_TPB, SRC2_MINB) k_src2_list(dclaw_params 
             cell_src2(P, g, dt, q_star, q_out, (size_t)(j - 1) * g.mx + (size_t)(i - 1));
         }
     }
-    last_block_tick(P, clk);
+    if (tick) last_block_tick(P, clk);
 }
 
 // ---- batched ensemble -------------------------------------------------------
@@ -1576,8 +1589,10 @@ int dclaw_step(const double* q_in, double* q_out, const double* b, int mx, int m
         const unsigned ntiles = (unsigned)ntx * (unsigned)nty;
         unsigned g0 = (unsigned)(nsm * DCLAW_SCAN_MINB * 2);
         if ((long long)g0 * TPB > ncell) g0 = nblocks(ncell);
-        k_scan_patch<<<g0, TPB, 0, s>>>(P, mx, my, q_in, q_out, clock, counters, tflag);
-        k_list_patch<<<(ntiles + TPB - 1) / TPB, TPB, 0, s>>>(ntx, nty, clock, tflag, counters, list_act, list_rec);
+        k_scan_patch<<<g0, TPB, 0, s>>>(P, mx, my, q_in, q_out, clock, counters, tflag, 0, (size_t)ncell, 0,
+                                        (size_t)ncell);
+        k_list_patch<<<(ntiles + TPB - 1) / TPB, TPB, 0, s>>>(ntx, nty, clock, tflag, counters, list_act, list_rec, 0,
+                                                             nty - 1);
         unsigned g1 = (unsigned)(nsm * RECORDS_MINB);
         if (g1 > ntiles) g1 = ntiles;
         k_records_list<<<g1, RECORDS_TPB, 0, s>>>(P, g, q_in, b, R, counters, list_rec);
@@ -1720,16 +1735,36 @@ int dclaw_step_rows(const double* q_in, double* q_out, const double* b, int mx, 
     using TG = TileGeom<TILE_X, TILE_Y>;
     uint32_t* tflag = (uint32_t*)((char*)work + L.off_tflag);
     double* qstar = (double*)((char*)work + L.off_qstar);
-    // the records of the rows the range's tiles read (3 beyond it), the
-    // range's tiles, its cells' src2; no tick
-    const int ja = row_first - 3 > -1 ? row_first - 3 : -1, jb = last + 3 < my + 2 ? last + 3 : my + 2;
-    const int nrow = jb - ja + 1;
-    k_records<<<nblocks((long long)g.PX * nrow), TPB, 0, s>>>(P, g, q_in, b, R, clock, tflag, ja + 1, nrow);
-    const int ty0 = (row_first - 1) / TILE_Y, nty = (last - 1) / TILE_Y - ty0 + 1;
-    k_tile<TILE_X, TILE_Y, false><<<dim3((mx + TILE_X - 1) / TILE_X, nty), TILE_TPB, TG::SMEM_BYTES, s>>>(
-        P, g, R, b, qstar, clock, nullptr, tflag, ty0);
-    const long long nc = (long long)row_count * mx;
-    k_src2_cells<<<src2_blocks(nc), SRC2_TPB, 0, s>>>(P, g, qstar, q_out, clock, tflag, (long long)(row_first - 1) * mx, nc, 0);
+    // dclaw_step's kernels over tile lists, restricted to the range: the scan
+    // of its rows and the 3 either side (the cells its tiles' marks depend
+    // on; the range's rows of q_out are zeroed), the active tiles of its
+    // tile rows, the records of those and their neighbours (one tile row
+    // beyond, 13 >= 3 rows), the tiles, their cells' src2; no tick
+    const int sm = sm_count();
+    if (sm <= 0) return DCLAW_ERR_CUDA;
+    unsigned int* counters = (unsigned int*)((char*)work + L.off_counters);
+    uint32_t* list_act = (uint32_t*)((char*)work + L.off_list_act);
+    uint32_t* list_rec = (uint32_t*)((char*)work + L.off_list_rec);
+    const int ntx = (mx + TILE_X - 1) / TILE_X, ntyp = (my + TILE_Y - 1) / TILE_Y;
+    const unsigned ntiles = (unsigned)ntx * (unsigned)ntyp;
+    const int ty0 = (row_first - 1) / TILE_Y, ty1 = (last - 1) / TILE_Y;
+    const int sa = row_first - 3 > 1 ? row_first - 3 : 1, sb = last + 3 < my ? last + 3 : my;
+    const long long nscan = (long long)(sb - sa + 1) * mx;
+    unsigned g0 = (unsigned)(sm * DCLAW_SCAN_MINB * 2);
+    if ((long long)g0 * TPB > nscan) g0 = nblocks(nscan);
+    k_scan_patch<<<g0, TPB, 0, s>>>(P, mx, my, q_in, q_out, clock, counters, tflag, (size_t)(sa - 1) * mx,
+                                    (size_t)sb * mx, (size_t)(row_first - 1) * mx, (size_t)last * mx);
+    k_list_patch<<<(ntiles + TPB - 1) / TPB, TPB, 0, s>>>(ntx, ntyp, clock, tflag, counters, list_act, list_rec, ty0,
+                                                         ty1);
+    unsigned g1 = (unsigned)(sm * RECORDS_MINB);
+    if (g1 > ntiles) g1 = ntiles;
+    k_records_list<<<g1, RECORDS_TPB, 0, s>>>(P, g, q_in, b, R, counters, list_rec);
+    unsigned g2 = (unsigned)(sm * DCLAW_TILE_MINBLOCKS);
+    if (g2 > ntiles) g2 = ntiles;
+    k_tile_list<false><<<g2, TILE_TPB, TG::SMEM_BYTES, s>>>(P, g, R, b, qstar, clock, counters, list_act);
+    unsigned g3 = (unsigned)(sm * SRC2_MINB);
+    if (g3 > ntiles) g3 = ntiles;
+    k_src2_list<<<g3, SRC2_TPB, 0, s>>>(P, g, qstar, q_out, clock, counters, list_act, 0);
     return cuda_status();
 }
 
