@@ -551,7 +551,8 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
     M.D = M.C + (size_t)10 * TG::NC;
     M.H = M.D + (size_t)10 * TG::ND;
     M.Bd = M.H + TG::NHB;
-    M.bits = reinterpret_cast<uint32_t*>(M.Bd + TG::NHB);
+    M.T5 = M.Bd + TG::NHB;
+    M.bits = reinterpret_cast<uint32_t*>(M.T5 + (size_t)5 * TG::NTS);
     M.list = reinterpret_cast<int*>(M.bits + TG::NA);
     M.nlist = M.list + TG::NA;
     M.NA = TG::NA;
@@ -580,6 +581,7 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
     // within distance 3 are all dry stays dry: all its interfaces are
     // dry-dry (skipped) and src2 zeroes dry cells
     bool any = false;
+    if (tid == 0) *M.nlist = 0;  // the x-sweep's solve list (the y-sweep's is reset after the x solves)
     for (int it = tid; it < TG::NHB; it += NT)
         if (tile_stage_hb(g, R, b, M, it)) any = true;
     any = __syncthreads_or(any) != 0;
@@ -606,8 +608,6 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
             // solve twice. The other items store zero waves here. Each
             // item writes only its own slots and the Courant number is a
             // max, so the list's order changes no result.
-            if (tid == 0) *M.nlist = 0;
-            __syncthreads();
             const int lane = tid & 31;
             for (int it0 = 0; it0 < nsolve; it0 += NT) {
                 const int it = it0 + tid;
@@ -630,6 +630,9 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
                 if (ok) cfl = fmax2(cfl, dtd * s);
             }
             __syncthreads();
+            // every thread has read this sweep's list length: reset it for the
+            // next sweep, whose list is built after two more barriers
+            if (tid == 0) *M.nlist = 0;
             // A half-warp per slice (x: a row, y: a column), lane k on
             // interface k of it. Each interface is limited once; a cell
             // takes its own interface's fluctuations and, from the next
@@ -664,13 +667,14 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
             }
             __syncthreads();
             if (dir == 0) {
-                double T0[5], T1[5];
-                const int nT = (TY + 1) * TX;
-                bool v0 = tid < nT && tile_T<TX, TY>(g, M, tid, i0, j0, T0);
-                bool v1 = tid + NT < nT && tile_T<TX, TY>(g, M, tid + NT, i0, j0, T1);
-                __syncthreads();
-                if (v0) tile_T_store<TX, TY>(M, tid, T0);
-                if (v1) tile_T_store<TX, TY>(M, tid + NT, T1);
+                // T into its own buffer (the y-sweep's flux phase reads it
+                // and writes gm/gp over C), so no barrier between the
+                // reads of C and the stores
+                const int nT = TG::NTS;
+                for (int it = tid; it < nT; it += NT) {
+                    double T0[5];
+                    if (tile_T<TX, TY>(g, M, it, i0, j0, T0)) tile_T_store<TX, TY>(M, it, T0);
+                }
                 __syncthreads();
             }
         }

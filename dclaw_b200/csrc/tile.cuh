@@ -195,13 +195,14 @@ struct TileGeom {
     static constexpr int NYS = (TX + 2) * YP;
     static constexpr int NA = NXW > NYS ? NXW : NYS;  // wave slots of either sweep
     static constexpr int NB = TY * (TX + 1);          // x-fluxes of tile rows, ifaces i0..i0+TX
-    static constexpr int NC = (TY + 2) * TX;          // G1x/G2x rows j0-1..j0+TY (then T/gm/gp rows j0..j0+TY)
+    static constexpr int NC = (TY + 2) * TX;          // G1x/G2x rows j0-1..j0+TY (then gm/gp rows j0..j0+TY)
     static constexpr int ND = (TX + 2) * TY;          // G1y/G2y cols i0-1..i0+TX, rows j0..j0+TY-1 (by column)
     // h and bed of cells within 3 of the tile, rows of an odd pitch (one
     // unused column when TX + 6 is even): read along rows and down columns
     static constexpr int HW = (TX + 6) | 1;
     static constexpr int NHB = HW * (TY + 6);
-    static constexpr size_t SMEM_DOUBLES = (size_t)NW * NA + 10 * NB + 10 * NC + 10 * ND + 2 * NHB;
+    static constexpr int NTS = (TY + 1) * TX;         // T of tile columns, y-interfaces j0..j0+TY
+    static constexpr size_t SMEM_DOUBLES = (size_t)NW * NA + 10 * NB + 10 * NC + 10 * ND + 2 * NHB + 5 * NTS;
     // + branch bits of the sweep's items, the list of items that need a
     // solve, and its length
     static constexpr size_t SMEM_BYTES = SMEM_DOUBLES * 8 + 4 * (size_t)NA + 4 * (size_t)NA + 16;
@@ -214,6 +215,7 @@ struct TileMem {
     double* D;   // [ND][10], column by column
     double* H;   // record h of cells (i0-3..i0+TX+2) x (j0-3..j0+TY+2), row pitch hw
     double* Bd;  // bed of the same cells
+    double* T5;  // [NTS][5]: T(k, c) of the x-sweep, read by the y-sweep's flux phase
     uint32_t* bits;  // NA Riemann branch bits of the current sweep
     int* list;       // NA: items of the current sweep that need a solve
     int* nlist;      // length of the list
@@ -564,16 +566,18 @@ DC_HD void tile_flux_cell(const dclaw_params& P, const Geom& g, const Rec& R, co
             // gm/gp = T + faddm_y/faddp_y in region C slot (r, c)
             fadd(am0, ap0, cq0, fm, fp);
             double* slot = M.C + (size_t)((r - j0) * TX + (c - i0)) * 10;
+            const double* ts = M.T5 + (size_t)((r - j0) * TX + (c - i0)) * 5;
             for (int m = 0; m < 5; ++m) {
-                double t = slot[m];
+                double t = ts[m];
                 slot[m] = t + fm[m];
                 slot[5 + m] = t + fp[m];
             }
             if (last) {
                 fadd(am1, ap1, cq1, fm, fp);
                 slot = M.C + (size_t)((r + 1 - j0) * TX + (c - i0)) * 10;
+                ts = M.T5 + (size_t)((r + 1 - j0) * TX + (c - i0)) * 5;
                 for (int m = 0; m < 5; ++m) {
-                    double t = slot[m];
+                    double t = ts[m];
                     slot[m] = t + fm[m];
                     slot[5 + m] = t + fp[m];
                 }
@@ -639,7 +643,7 @@ DC_HD bool tile_T(const Geom& g, const TileMem& M, int item, int i0, int j0, dou
 
 template <int TX, int TY>
 DC_HD void tile_T_store(const TileMem& M, int item, const double T[5]) {
-    double* slot = M.C + (size_t)item * 10;  // slot (k - j0, c - i0) == item
+    double* slot = M.T5 + (size_t)item * 5;  // slot (k - j0, c - i0) == item
     for (int m = 0; m < 5; ++m) slot[m] = T[m];
 }
 

@@ -99,6 +99,7 @@ static int run_fused(const dclaw_params* P, int mx, int my, double dx, double dy
     M.D = M.C + (size_t)10 * TG::NC;
     M.H = M.D + (size_t)10 * TG::ND;
     M.Bd = M.H + TG::NHB;
+    M.T5 = M.Bd + TG::NHB;
     M.bits = bits.data();
     M.NA = TG::NA;
     M.hw = TG::HW;
