@@ -596,19 +596,17 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
             for (int m = 0; m < 5; ++m) q_out[(size_t)m * plane + c] = 0.0;
         }
     } else {
-        // the two sweeps share one copy of the solver, limiter and rpt2 code
-#pragma unroll 1
-        for (int dir = 0; dir < 2; ++dir) {
+        // Items that need a solve are gathered into a dense list first, so
+        // that every warp of the solve loop is full of them: wet interfaces
+        // cluster in space, and handing items out by index leaves warps of
+        // dry items idle at the barrier while others solve twice. The other
+        // items store zero waves here. Each item writes only its own slots
+        // and the Courant number is a max, so the list's order changes no
+        // result. The x-sweep's list is built after the staging, the
+        // y-sweep's beside the T phase (neither reads what the other writes).
+        const int lane = tid & 31;
+        auto build_list = [&](int dir) {
             const int nsolve = dir == 0 ? TG::NXW : TG::NYW;
-            const double dtd = dir == 0 ? dtdx : dtdy;
-            // Items that need a solve are gathered into a dense list first,
-            // so that every warp of the solve loop is full of them: wet
-            // interfaces cluster in space, and handing items out by index
-            // leaves warps of dry items idle at the barrier while others
-            // solve twice. The other items store zero waves here. Each
-            // item writes only its own slots and the Courant number is a
-            // max, so the list's order changes no result.
-            const int lane = tid & 31;
             for (int it0 = 0; it0 < nsolve; it0 += NT) {
                 const int it = it0 + tid;
                 bool need = it < nsolve && tile_needs_solve(P, g, M, dir, it, i0, j0, TX);
@@ -622,7 +620,13 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
                 base = __shfl_sync(0xffffffffu, base, 0);
                 if (need) M.list[base + __popc(bal & ((1u << lane) - 1u))] = it;
             }
-            __syncthreads();
+        };
+        build_list(0);
+        // the two sweeps share one copy of the solver, limiter and rpt2 code
+#pragma unroll 1
+        for (int dir = 0; dir < 2; ++dir) {
+            const double dtd = dir == 0 ? dtdx : dtdy;
+            __syncthreads();  // this sweep's list is complete
             const int nneed = *M.nlist;
             for (int w = tid; w < nneed; w += NT) {
                 bool ok;
@@ -631,7 +635,7 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
             }
             __syncthreads();
             // every thread has read this sweep's list length: reset it for the
-            // next sweep, whose list is built after two more barriers
+            // next sweep, whose list is built after one more barrier
             if (tid == 0) *M.nlist = 0;
             // A half-warp per slice (x: a row, y: a column), lane k on
             // interface k of it. Each interface is limited once; a cell
@@ -675,7 +679,9 @@ __device__ __forceinline__ double tile_body(const dclaw_params& P, const Geom& g
                     double T0[5];
                     if (tile_T<TX, TY>(g, M, it, i0, j0, T0)) tile_T_store<TX, TY>(M, it, T0);
                 }
-                __syncthreads();
+                // the x waves are no longer read: the y-sweep's zero waves
+                // and list go in beside T
+                build_list(1);
             }
         }
         for (int it = tid; it < TX * TY; it += NT)
@@ -814,27 +820,34 @@ __global__ void __launch_bounds__(TILE_TPB, DCLAW_TILE_MINBLOCKS) k_tile_list(dc
                                                                              dclaw_clock* clk, unsigned int* counters,
                                                                              const uint32_t* __restrict__ list_act) {
     extern __shared__ double smem[];
-    __shared__ uint32_t s_t;
+    // the tile of this pass and the next one's, claimed at the start of this
+    // pass: the barrier that ends a pass also publishes the next index
+    __shared__ uint32_t s_t[2];
     const unsigned int nact = counters[1];
     const uint32_t ntx = (uint32_t)((g.mx + TILE_X - 1) / TILE_X);
     const double dt = clk->dt;
     double cfl = 0.0;
     bool nan_any = false;
-    for (;;) {
+    if (threadIdx.x == 0) {
+        const unsigned int k = atomicAdd(counters, 1u);
+        s_t[0] = k < nact ? list_act[k] : 0xffffffffu;
+    }
+    __syncthreads();
+    for (int pass = 0;; ++pass) {
+        const uint32_t t = s_t[pass & 1];
+        if (t == 0xffffffffu) break;
+        // s_t[(pass + 1) & 1] was last read before the previous pass's barrier
         if (threadIdx.x == 0) {
             const unsigned int k = atomicAdd(counters, 1u);
-            s_t = k < nact ? list_act[k] : 0xffffffffu;
+            s_t[(pass + 1) & 1] = k < nact ? list_act[k] : 0xffffffffu;
         }
-        __syncthreads();
-        const uint32_t t = s_t;
-        if (t == 0xffffffffu) break;
         const int i0 = 1 + (int)(t % ntx) * TILE_X, j0 = 1 + (int)(t / ntx) * TILE_Y;
         bool nan;
         const double c =
             tile_body<TILE_X, TILE_Y, WITH_SRC2, TILE_TPB>(P, g, R, b, q_out, dt, i0, j0, smem, nullptr, nan);
         cfl = fmax2(cfl, c);
         nan_any = nan_any || nan;
-        // the next tile's staging overwrites shared memory and s_t
+        // the next tile's staging overwrites shared memory
         __syncthreads();
     }
     if (nan_any) flag_status(clk, DCLAW_ERR_NAN);
