@@ -51,16 +51,16 @@ NCU_STEP = {
                "--warmup 3 --e2e-steps 0 --no-cpu-baseline --ensemble-members 0 --grad-steps 0 "
                "--bgrad-members 0 --full-steps 0 --variant-steps 0",
     "kernels": {  # name: (DRAM bytes, warp instructions) per launch, the mean of the 6 launches
-        "k_scan_patch": (1294.2e6, 48.61e6),
-        "k_list_patch": (0.4e6, 0.55e6),
-        "k_records_list": (839.7e6, 276.57e6),
-        "k_tile_list": (765.7e6, 1426.80e6),
-        "k_src2_list": (325.7e6, 372.79e6),
+        "k_scan_patch": (1295.4e6, 56.82e6),
+        "k_list_patch": (0.4e6, 0.59e6),
+        "k_records_list": (839.8e6, 276.57e6),
+        "k_tile_list": (754.6e6, 1410.10e6),
+        "k_src2_list": (325.6e6, 372.82e6),
     },
     # k_tile_list, --set full on the 2048^2 case: active lanes per warp
     # instruction, FP64 pipe active
-    "k_tile_list_lanes": 20.84,
-    "k_tile_list_fp64_pipe": 0.298,
+    "k_tile_list_lanes": 20.74,
+    "k_tile_list_fp64_pipe": 0.303,
 }
 SMS, SCHEDULERS_PER_SM = 148, 4
 METRIC = "cell-updates/sec on 1 B200 (plain vs batched); gradient/forward time ratio"
